@@ -1,0 +1,358 @@
+"""Headline benchmark: full decode of a variable-partitioned 200M uint64 piecewise-linear column.
+
+One step = one full decode of the column (persistent work-stealing kernel, TMA-staged input).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl glc|reference] [--n VALUES]
+
+Workload (``config.workload``): 200,000,000 uint64 values, piecewise linear with segment
+lengths ~ Poisson(50,000), slope U{1..10^6}, intercept jump U{0..2^40}, noise U[0, 2^b) with
+b in {0,4,8,16,24} (seeded synthetic data standing in for the reference's SOSD datasets),
+compressed with the device split/merge partitioner.  The compressed column and the output are
+both larger than L2 (126 MB), so no L2 flush is needed between steps.
+
+``value`` = decoded bytes (8 B x values, the reference's decode GB/s definition, app/Main.cu)
+/ device time, inputs resident in HBM.  ``e2e`` = the same through the public C ABI with host
+buffers: every step deserializes the host (pinned) blob onto the device and decodes into pinned
+host memory.  ``roofline`` = algorithmic bytes (compressed bytes read + decoded bytes written)
+per decode launch / its CUDA-event duration, against the measured HBM copy bandwidth.
+
+With N > 1 (torchrun, one process per GPU) every rank decodes its own column (columns are
+independent; no data-path collective): weak scaling, value = all ranks' bytes / max rank time.
+
+``--impl reference`` times the reference's own CPU decoder (directRandomAccessCPU, compiled from
+the reference sources into oracle/_ref; the CPU oracle when that is absent) on this host's cores
+over bounded samples of the same workload; rank 0 only.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "g-leco_b200"))
+
+METRIC = "decode GB/s"
+UNIT = "GB/s"
+WORKLOAD = "piecewise_u64_200M_variable"
+DEFAULT_N = 200_000_000
+PROFILE_NOTE = os.path.join(ROOT, "profiles", "decode_piecewise_u64_200M.md")
+
+
+def measured_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def profiled_traffic_per_value():
+    """DRAM bytes per decoded value from the committed ncu summary (one capture), or None."""
+    try:
+        with open(PROFILE_NOTE) as f:
+            for line in f:
+                if line.startswith("traffic_bytes_per_value:"):
+                    return float(line.split(":", 1)[1].strip())
+    except OSError:
+        pass
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons, sampled every 200 ms while running."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for name, val in zip(names, parts[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def make_values(n: int, rank: int) -> np.ndarray:
+    from glc import workloads as W
+    return W.piecewise_linear(n, seed=42 + rank)
+
+
+def cpu_baseline_decode(values: np.ndarray, blob_maker, threads: int, budget_s: float = 20.0):
+    """Time the reference's host decoder on a bounded prefix sample; returns a dict."""
+    import oracle
+    sample_n = min(len(values), 16_000_000)
+    sample = np.ascontiguousarray(values[:sample_n])
+    blob = blob_maker(sample)
+    pos = np.arange(sample_n, dtype=np.int32)
+    kind = "reference" if oracle.ref_available() else "port"
+    with tempfile.TemporaryDirectory() as td:
+        if kind == "reference":
+            chunks = np.array_split(pos, threads)
+            paths = []
+            for k, ch in enumerate(chunks):
+                pp = os.path.join(td, f"pos{k}.bin")
+                ch.tofile(pp)
+                paths.append(pp)
+            bp = os.path.join(td, "blob.bin")
+            with open(bp, "wb") as f:
+                f.write(blob)
+            env = dict(os.environ, GLC_REF_CPU_ONLY="1")
+            t0 = time.perf_counter()
+            procs = [subprocess.Popen([oracle.REF_HARNESS, "hostdecode", "u64", bp, paths[k],
+                                       os.path.join(td, f"out{k}.bin"), "1"], stdout=subprocess.PIPE,
+                                      stderr=subprocess.PIPE, env=env) for k in range(len(paths))]
+            for p in procs:
+                p.wait()
+            wall = time.perf_counter() - t0
+            secs = max(float(p.stdout.read().decode().strip().splitlines()[-1]) for p in procs)
+            out = np.concatenate([np.fromfile(os.path.join(td, f"out{k}.bin"), np.uint64) for k in range(len(paths))])
+            ok = bool(np.array_equal(out, sample))
+        else:
+            col = oracle.deserialize(blob, "u64")
+            t0 = time.perf_counter()
+            out = oracle.decode_full(col)
+            secs = time.perf_counter() - t0
+            wall = secs
+            ok = bool(np.array_equal(out, sample))
+            threads = 1
+    gbs = sample_n * 8 / secs / 1e9
+    return {"value": round(gbs, 4), "unit": UNIT, "cores": threads, "kind": kind,
+            "sample": f"full decode of the first {sample_n:,} values of the workload (all positions, "
+                      f"{'directRandomAccessCPU' if kind == 'reference' else 'oracle decode'}), "
+                      f"{threads} process(es); wall {wall:.2f} s; bit-exact={ok}"}
+
+
+def run_reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    import oracle
+    n = min(args.n, 200_000_000)
+    threads = os.cpu_count() or 1
+    values = make_values(min(n, 16_000_000), 0)
+    # blob of the sample: the reference's own CPU partitioner (restated) and the format's fit
+    def make_blob(sample):
+        s, e = oracle.ref_partition_cpu(sample)
+        return oracle.serialize(oracle.compress(sample, starts=s, ends=e))
+    blob = make_blob(values)
+    maker = lambda sample: blob  # noqa: E731
+    results = []
+    for step in range(args.warmup + args.steps):
+        r = cpu_baseline_decode(values, maker, threads)
+        if step >= args.warmup:
+            results.append(r)
+    val = float(np.median([r["value"] for r in results]))
+    line = {"impl": "reference", "metric": METRIC, "value": val, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "values": n, "sample_values": len(values)},
+            "cpu_baseline": {**results[-1], "value": val},
+            "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="glc", choices=["glc", "reference"])
+    ap.add_argument("--n", type=int, default=DEFAULT_N)
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference_arm(args)
+
+    import torch
+    import torch.distributed as dist
+
+    import glc
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.current_stream(dev)
+    sh = stream.cuda_stream
+    ctx = glc.Context(local)
+
+    n = args.n
+    values = make_values(n, rank)
+    d_in = torch.from_numpy(values.view(np.int64)).to(dev)
+    torch.cuda.synchronize(dev)
+    t0 = time.perf_counter()
+    col = glc.compress_device(ctx, glc.U64, d_in.data_ptr(), n, glc.VARIABLE, stream=sh)
+    torch.cuda.synchronize(dev)
+    compress_s = time.perf_counter() - t0
+    info = col.info()
+    del d_in
+    out = torch.empty(n, dtype=torch.int64, device=dev)
+
+    def step():
+        glc.decompress_into(ctx, col, out.data_ptr(), glc.SRC_PACKED, stream=sh)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize(dev)
+    ok = bool(np.array_equal(out.cpu().numpy().view(np.uint64), values))
+
+    clocks = ClockSampler(local)
+    clocks.start()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(args.steps):
+        step()
+    ev1.record(stream)
+    torch.cuda.synchronize(dev)
+    ms = ev0.elapsed_time(ev1)
+    if world > 1:
+        dist.barrier()
+    clk = clocks.stop()
+    t_max = torch.tensor([ms], device=dev, dtype=torch.float64)
+    if world > 1:
+        dist.all_reduce(t_max, op=dist.ReduceOp.MAX)
+    ms_max = float(t_max.item())
+    ms_per_step = ms_max / args.steps
+    decoded_bytes = n * 8
+    value = decoded_bytes * world / (ms_per_step / 1e3) / 1e9
+
+    # roofline of the decode kernel (one launch per step)
+    algo_bytes = info.compressed_size_bytes + decoded_bytes
+    achieved = algo_bytes / (ms / args.steps / 1e3) / 1e9
+    peak, peak_kind = measured_peak()
+    tpv = profiled_traffic_per_value()
+
+    # end to end through the C ABI with host buffers: host blob -> device -> decode -> host
+    blob = glc.serialize_host(ctx, col)
+    h_blob = torch.from_numpy(np.frombuffer(blob, np.uint8).copy()).pin_memory()
+    h_out = torch.empty(n, dtype=torch.int64).pin_memory()
+    lib = ctx.lib
+    import ctypes
+
+    def e2e_step():
+        h = ctypes.c_void_p()
+        ctx.check(lib.glc_deserialize(ctx.handle, glc.U64, ctypes.c_void_p(h_blob.data_ptr()), len(blob), glc.HOST_IN,
+                                      0, 0, ctypes.byref(h), ctypes.c_void_p(sh)))
+        c2 = glc.Column(ctx, h)
+        glc.decompress_into(ctx, c2, h_out.data_ptr(), glc.SRC_PACKED, stream=sh, host_out=True)
+        c2.free()
+
+    e2e_step()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.e2e_steps):
+        e2e_step()
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    e2e_ms = torch.tensor([e0.elapsed_time(e1) / args.e2e_steps], device=dev, dtype=torch.float64)
+    if world > 1:
+        dist.all_reduce(e2e_ms, op=dist.ReduceOp.MAX)
+    e2e_ok = bool(np.array_equal(h_out.numpy().view(np.uint64), values))
+    e2e_value = decoded_bytes * world / (float(e2e_ms.item()) / 1e3) / 1e9
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            threads = 1
+            cpu = cpu_baseline_decode(values, lambda s: glc.serialize_host(
+                ctx, glc.compress_device(ctx, glc.U64, s.ctypes.data, len(s), glc.VARIABLE, host=True)), threads)
+        except Exception as ex:  # reported, never fatal
+            cpu = {"value": None, "unit": UNIT, "cores": 1, "kind": "reference", "sample": f"failed: {ex}"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": round(value, 2), "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(ms_per_step, 4), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "values": n, "partitions": info.num_partitions,
+                       "bits_per_value": round(info.total_bits / n, 3),
+                       "compressed_bytes": info.compressed_size_bytes,
+                       "compression_ratio": round(decoded_bytes / info.compressed_size_bytes, 3),
+                       "l2": "inputs and output larger than L2 (no flush)", "parallelism": f"replicas{world}",
+                       "compress_s": round(compress_s, 3), "bit_exact": ok and e2e_ok},
+            "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                         "frac": round(achieved / peak, 4), "peak_kind": peak_kind,
+                         "traffic": (round(tpv * n) if tpv else None),
+                         "algorithmic_bytes": algo_bytes},
+            "e2e": {"value": round(e2e_value, 3), "unit": UNIT, "h2d_bytes_per_step": len(blob),
+                    "d2h_bytes_per_step": decoded_bytes},
+            "gpu_launches": args.steps,
+            "clocks": clk,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    col.free()
+    ctx.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

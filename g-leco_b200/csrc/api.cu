@@ -1,0 +1,624 @@
+// api.cu -- the C ABI (include/glc.h): contexts, columns, compress / decode / random access,
+// pre-unpack and the version-5 blob.  Orchestration only; the kernels live in the other .cu
+// files.  Nothing here exits the process or falls back to host computation: every failure is a
+// glc_status with a message (the reference calls exit() on any CUDA error,
+// core/CudaUtils.cuh:5-13).
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include "glc_internal.h"
+
+using namespace glc;
+
+namespace {
+
+struct BlobHeader {  // core/InternalTypes.cuh:39-63 (120 bytes, 4 trailing pad bytes)
+  uint32_t magic, version, total_values, num_partitions;
+  uint64_t start_off, end_off, types_off, params_off, bits_off, offsets_off, errb_off, delta_off;
+  uint64_t params_size, delta_size;
+  uint32_t type_size, checksum;
+  uint32_t reserved[3];
+  uint32_t pad;
+};
+static_assert(sizeof(BlobHeader) == 120, "blob header layout");
+constexpr uint32_t kMagic = 0x4F43454C;
+
+uint64_t align8(uint64_t x) { return (x + 7) & ~7ull; }
+
+// api/G-LeCo.cuh:87-100: rotate-add (the build without SSE4.2) or byte-wise CRC32C from 0.
+uint32_t header_checksum(const uint8_t* p, size_t n, int crc32c) {
+  uint32_t c = 0;
+  if (!crc32c) {
+    for (size_t i = 0; i < n; i++) { c += p[i]; c = (c << 1) | (c >> 31); }
+    return c;
+  }
+  for (size_t i = 0; i < n; i++) {
+    c ^= p[i];
+    for (int k = 0; k < 8; k++) c = (c >> 1) ^ (0x82F63B78u & (0u - (c & 1u)));
+  }
+  return c;
+}
+
+void fill_layout(BlobHeader& h, int64_t P, int64_t total_bits, int type_size, int64_t n) {
+  std::memset(&h, 0, sizeof h);
+  h.magic = kMagic;
+  h.version = 5;
+  h.total_values = (uint32_t)n;
+  h.num_partitions = (uint32_t)P;
+  uint64_t off = sizeof(BlobHeader);
+  off = align8(off); h.start_off = off; off += 4 * (uint64_t)P;
+  off = align8(off); h.end_off = off; off += 4 * (uint64_t)P;
+  off = align8(off); h.types_off = off; off += 4 * (uint64_t)P;
+  off = align8(off); h.params_off = off; h.params_size = 32 * (uint64_t)P; off += 32 * (uint64_t)P;
+  off = align8(off); h.bits_off = off; off += 4 * (uint64_t)P;
+  off = align8(off); h.offsets_off = off; off += 8 * (uint64_t)P;
+  off = align8(off); h.errb_off = off; off += 8 * (uint64_t)P;
+  off = align8(off); h.delta_off = off;
+  h.delta_size = (uint64_t)(total_bits + 7) / 8;
+  h.type_size = (uint32_t)type_size;
+}
+
+uint64_t blob_total(const BlobHeader& h) { return align8(h.delta_off + h.delta_size); }
+
+glc_status fail(glc_ctx* ctx, glc_status st, const std::string& msg) {
+  if (ctx) ctx->err = msg;
+  return st;
+}
+
+glc_status cuda_fail(glc_ctx* ctx, cudaError_t e, const char* where) {
+  if (e == cudaErrorMemoryAllocation) return fail(ctx, GLC_ERR_OOM, std::string(where) + ": out of device memory");
+  return fail(ctx, GLC_ERR_CUDA, std::string(where) + ": " + cudaGetErrorString(e));
+}
+
+#define CK(call, where)                                  \
+  do {                                                   \
+    cudaError_t e_ = (call);                             \
+    if (e_ != cudaSuccess) return cuda_fail(ctx, e_, where); \
+  } while (0)
+
+cudaStream_t pick(glc_ctx* ctx, glc_stream s) { return s ? (cudaStream_t)s : ctx->own_stream; }
+
+bool valid_dtype(int d) { return d >= GLC_I32 && d <= GLC_U32; }
+
+void free_column_arrays(glc_column* c) {
+  void* ptrs[] = {c->d_start, c->d_end, c->d_types, c->d_params, c->d_bits, c->d_offs, c->d_err,
+                  c->d_words, c->d_plain, c->d_desc, c->d_tiles};
+  for (void* p : ptrs)
+    if (p) cudaFree(p);
+  c->d_start = c->d_end = c->d_types = c->d_bits = nullptr;
+  c->d_params = nullptr;
+  c->d_offs = c->d_err = c->d_plain = nullptr;
+  c->d_words = nullptr;
+  c->d_desc = nullptr;
+  c->d_tiles = nullptr;
+}
+
+// Metadata arrays for P partitions and the decode tile table.
+cudaError_t alloc_meta(glc_column* c) {
+  const int64_t P = c->P > 0 ? c->P : 1;
+  cudaError_t e;
+  if ((e = cudaMalloc(&c->d_start, 4 * P)) != cudaSuccess) return e;
+  if ((e = cudaMalloc(&c->d_end, 4 * P)) != cudaSuccess) return e;
+  if ((e = cudaMalloc(&c->d_types, 4 * P)) != cudaSuccess) return e;
+  if ((e = cudaMalloc(&c->d_params, 32 * P)) != cudaSuccess) return e;
+  if ((e = cudaMalloc(&c->d_bits, 4 * P)) != cudaSuccess) return e;
+  if ((e = cudaMalloc(&c->d_offs, 8 * P)) != cudaSuccess) return e;
+  if ((e = cudaMalloc(&c->d_err, 8 * P)) != cudaSuccess) return e;
+  if ((e = cudaMalloc(&c->d_desc, sizeof(PartDesc) * P)) != cudaSuccess) return e;
+  c->ntiles = (c->n + kDecodeTile - 1) / kDecodeTile;
+  if ((e = cudaMalloc(&c->d_tiles, sizeof(TileInfo) * (c->ntiles + 1))) != cudaSuccess) return e;
+  return cudaSuccess;
+}
+
+void set_word_counts(glc_column* c) {
+  c->nwords = (c->total_bits + 31) / 32;
+  c->nwords_alloc = ((c->nwords + 3) & ~3ll) + 8;  // decoders read up to 3 words past a field
+}
+
+int64_t reported_size(int64_t P, int64_t total_bits) {  // api/G-LeCo.cuh:589-603
+  return 64 * P + 120 + (total_bits + 7) / 8;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* glc_status_string(glc_status s) {
+  switch (s) {
+    case GLC_OK: return "ok";
+    case GLC_ERR_INVALID_ARG: return "invalid argument";
+    case GLC_ERR_BAD_BLOB: return "bad blob";
+    case GLC_ERR_OOM: return "out of memory";
+    case GLC_ERR_CUDA: return "CUDA error";
+    case GLC_ERR_TIMEOUT: return "device wait timed out";
+    case GLC_ERR_BUDGET: return "memory budget exceeded";
+    case GLC_ERR_UNSUPPORTED: return "unsupported for this column";
+  }
+  return "unknown status";
+}
+
+const char* glc_last_error(const glc_ctx* ctx) { return ctx ? ctx->err.c_str() : "no context"; }
+
+glc_status glc_create(glc_ctx** out, int device) {
+  if (!out) return GLC_ERR_INVALID_ARG;
+  *out = nullptr;
+  glc_ctx* ctx = new (std::nothrow) glc_ctx();
+  if (!ctx) return GLC_ERR_OOM;
+  cudaError_t e;
+  if (device < 0) {
+    if ((e = cudaGetDevice(&device)) != cudaSuccess) { delete ctx; return GLC_ERR_CUDA; }
+  }
+  if ((e = cudaSetDevice(device)) != cudaSuccess) { delete ctx; return GLC_ERR_CUDA; }
+  ctx->device = device;
+  if ((e = cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, device)) != cudaSuccess ||
+      (e = cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking)) != cudaSuccess ||
+      (e = cudaMalloc(&ctx->d_flags, sizeof(int) * kFlagWords)) != cudaSuccess ||
+      (e = cudaMemset(ctx->d_flags, 0, sizeof(int) * kFlagWords)) != cudaSuccess ||
+      (e = cudaMalloc(&ctx->d_stats, sizeof(int64_t) * 16)) != cudaSuccess ||
+      (e = cudaMallocHost(&ctx->h_stats, sizeof(int64_t) * 16)) != cudaSuccess) {
+    glc_destroy(ctx);
+    return e == cudaErrorMemoryAllocation ? GLC_ERR_OOM : GLC_ERR_CUDA;
+  }
+  *out = ctx;
+  return GLC_OK;
+}
+
+glc_status glc_destroy(glc_ctx* ctx) {
+  if (!ctx) return GLC_ERR_INVALID_ARG;
+  cudaSetDevice(ctx->device);
+  if (ctx->own_stream) cudaStreamSynchronize(ctx->own_stream);
+  if (ctx->d_flags) cudaFree(ctx->d_flags);
+  if (ctx->d_stats) cudaFree(ctx->d_stats);
+  if (ctx->h_stats) cudaFreeHost(ctx->h_stats);
+  if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
+  delete ctx;
+  return GLC_OK;
+}
+
+glc_status glc_sync(glc_ctx* ctx, glc_stream stream) {
+  if (!ctx) return GLC_ERR_INVALID_ARG;
+  cudaSetDevice(ctx->device);
+  cudaStream_t s = pick(ctx, stream);
+  CK(cudaStreamSynchronize(s), "sync");
+  int code = 0;
+  CK(cudaMemcpy(&code, ctx->d_flags + kFlagError, sizeof(int), cudaMemcpyDeviceToHost), "sync: read error flag");
+  if (code != DEVERR_NONE) {
+    cudaMemset(ctx->d_flags + kFlagError, 0, sizeof(int));
+    return fail(ctx, code == DEVERR_TIMEOUT ? GLC_ERR_TIMEOUT : GLC_ERR_CUDA, "a device-side wait gave up");
+  }
+  return GLC_OK;
+}
+
+glc_status glc_column_free(glc_column* col) {
+  if (!col) return GLC_ERR_INVALID_ARG;
+  if (col->ctx) cudaSetDevice(col->ctx->device);
+  free_column_arrays(col);
+  delete col;
+  return GLC_OK;
+}
+
+glc_status glc_column_get_info(const glc_column* c, glc_column_info* info) {
+  if (!c || !info) return GLC_ERR_INVALID_ARG;
+  info->dtype = c->dtype;
+  info->total_values = c->n;
+  info->num_partitions = c->P;
+  info->total_bits = c->total_bits;
+  info->compressed_size_bytes = c->reported_size;
+  info->fixed_partition_len = c->fixed_len;
+  info->has_packed = (c->d_words != nullptr) ? 1 : 0;
+  info->has_preunpacked = (c->d_plain != nullptr) ? 1 : 0;
+  info->d_start_indices = c->d_start;
+  info->d_end_indices = c->d_end;
+  info->d_model_types = c->d_types;
+  info->d_model_params = c->d_params;
+  info->d_delta_bits = c->d_bits;
+  info->d_delta_array_bit_offsets = c->d_offs;
+  info->d_error_bounds = c->d_err;
+  info->delta_array = c->d_words;
+  info->d_plain_deltas = c->d_plain;
+  return GLC_OK;
+}
+
+// ---------------------------------------------------------------------------------------
+// compress
+// ---------------------------------------------------------------------------------------
+static glc_status compress_impl(glc_ctx* ctx, glc_dtype dtype, const void* dev_values, int64_t n,
+                                glc_partitioning mode, int32_t fixed_len, glc_column* c, cudaStream_t s) {
+  c->ctx = ctx;
+  c->dtype = dtype;
+  c->n = n;
+  int32_t* tmp_s = nullptr;
+  int32_t* tmp_e = nullptr;
+  if (mode == GLC_PART_FIXED) {
+    c->P = (n + fixed_len - 1) / fixed_len;
+    c->fixed_len = fixed_len;
+  } else {
+    std::string perr;
+    int64_t P = 0;
+    cudaError_t e = launch_partition_variable(ctx, dtype, dev_values, n, &tmp_s, &tmp_e, &P, s, &perr);
+    if (e != cudaSuccess) return perr.empty() ? cuda_fail(ctx, e, "variable partitioner") : fail(ctx, GLC_ERR_CUDA, perr);
+    c->P = P;
+    c->fixed_len = 0;
+  }
+  CK(alloc_meta(c), "compress: metadata allocation");
+  if (mode == GLC_PART_FIXED) {
+    CK(launch_fixed_partitions(c->d_start, c->d_end, n, fixed_len, c->P, s), "compress: fixed partitions");
+  } else {
+    CK(cudaMemcpyAsync(c->d_start, tmp_s, 4 * c->P, cudaMemcpyDeviceToDevice, s), "compress: partition copy");
+    CK(cudaMemcpyAsync(c->d_end, tmp_e, 4 * c->P, cudaMemcpyDeviceToDevice, s), "compress: partition copy");
+    cudaFreeAsync(tmp_s, s);
+    cudaFreeAsync(tmp_e, s);
+  }
+  const size_t sb = fit_scratch_bytes(nullptr, n, c->P);
+  void* scratch = nullptr;
+  CK(cudaMallocAsync(&scratch, sb, s), "compress: scratch allocation");
+  cudaError_t e = launch_fit(dtype, dev_values, c, scratch, sb, ctx->d_stats, s);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(ctx->h_stats, ctx->d_stats, 2 * sizeof(int64_t), cudaMemcpyDeviceToHost, s);
+  cudaFreeAsync(scratch, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "compress: fit");
+  c->total_bits = ctx->h_stats[0];
+  c->max_bits = (int32_t)ctx->h_stats[1];
+  set_word_counts(c);
+  CK(cudaMalloc(&c->d_words, 4 * c->nwords_alloc), "compress: word allocation");
+  CK(launch_pack(dtype, dev_values, c, s), "compress: pack");
+  CK(launch_desc_and_tiles(c, s), "compress: tables");
+  c->reported_size = reported_size(c->P, c->total_bits);
+  return GLC_OK;
+}
+
+glc_status glc_compress(glc_ctx* ctx, glc_dtype dtype, const void* values, int64_t n, int flags,
+                        glc_partitioning mode, int32_t fixed_partition_len, glc_column** out,
+                        int64_t* compressed_size_bytes, glc_stream stream) {
+  if (!ctx || !out) return fail(ctx, GLC_ERR_INVALID_ARG, "null context or output");
+  *out = nullptr;
+  if (!valid_dtype(dtype)) return fail(ctx, GLC_ERR_INVALID_ARG, "unknown dtype");
+  if (n < 0 || n > 0x7fffffffll) return fail(ctx, GLC_ERR_INVALID_ARG, "n must be in [0, 2^31)");
+  if (n > 0 && !values) return fail(ctx, GLC_ERR_INVALID_ARG, "null values");
+  if (mode != GLC_PART_FIXED && mode != GLC_PART_VARIABLE) return fail(ctx, GLC_ERR_INVALID_ARG, "unknown partitioning");
+  if (mode == GLC_PART_FIXED && fixed_partition_len <= 0)
+    return fail(ctx, GLC_ERR_INVALID_ARG, "fixed partition length must be positive");
+  cudaSetDevice(ctx->device);
+  cudaStream_t s = pick(ctx, stream);
+  glc_column* c = new (std::nothrow) glc_column();
+  if (!c) return fail(ctx, GLC_ERR_OOM, "host allocation");
+  c->ctx = ctx;
+  c->dtype = dtype;
+  if (n == 0) {  // api/G-LeCo.cuh:355-371: an empty object, size 0
+    c->n = 0;
+    c->P = 0;
+    set_word_counts(c);
+    if (compressed_size_bytes) *compressed_size_bytes = 0;
+    c->reported_size = 0;
+    *out = c;
+    return GLC_OK;
+  }
+  const void* dev_values = values;
+  void* staged = nullptr;
+  if (flags & GLC_HOST_IN) {
+    const size_t bytes = (size_t)n * dtype_size(dtype);
+    cudaError_t e = cudaMallocAsync(&staged, bytes, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(staged, values, bytes, cudaMemcpyHostToDevice, s);
+    if (e != cudaSuccess) {
+      if (staged) cudaFreeAsync(staged, s);
+      delete c;
+      return cuda_fail(ctx, e, "compress: input upload");
+    }
+    dev_values = staged;
+  }
+  glc_status st = compress_impl(ctx, dtype, dev_values, n, mode, fixed_partition_len, c, s);
+  if (staged) cudaFreeAsync(staged, s);
+  if (st != GLC_OK) {
+    cudaStreamSynchronize(s);
+    free_column_arrays(c);
+    delete c;
+    return st;
+  }
+  if (compressed_size_bytes) *compressed_size_bytes = c->reported_size;
+  *out = c;
+  return GLC_OK;
+}
+
+glc_status glc_partition_variable(glc_ctx* ctx, glc_dtype dtype, const void* values, int64_t n, int flags,
+                                  int32_t* starts, int32_t* ends, int64_t cap, int64_t* num_partitions,
+                                  glc_stream stream) {
+  if (!ctx || !num_partitions) return fail(ctx, GLC_ERR_INVALID_ARG, "null argument");
+  if (!valid_dtype(dtype) || n < 0 || n > 0x7fffffffll) return fail(ctx, GLC_ERR_INVALID_ARG, "bad dtype or n");
+  cudaSetDevice(ctx->device);
+  cudaStream_t s = pick(ctx, stream);
+  *num_partitions = 0;
+  if (n == 0) return GLC_OK;
+  const void* dev_values = values;
+  void* staged = nullptr;
+  if (flags & GLC_HOST_IN) {
+    const size_t bytes = (size_t)n * dtype_size(dtype);
+    CK(cudaMallocAsync(&staged, bytes, s), "partition: upload");
+    CK(cudaMemcpyAsync(staged, values, bytes, cudaMemcpyHostToDevice, s), "partition: upload");
+    dev_values = staged;
+  }
+  int32_t* ds = nullptr;
+  int32_t* de = nullptr;
+  int64_t P = 0;
+  std::string perr;
+  cudaError_t e = launch_partition_variable(ctx, dtype, dev_values, n, &ds, &de, &P, s, &perr);
+  if (staged) cudaFreeAsync(staged, s);
+  if (e != cudaSuccess) return perr.empty() ? cuda_fail(ctx, e, "partition") : fail(ctx, GLC_ERR_CUDA, perr);
+  *num_partitions = P;
+  glc_status st = GLC_OK;
+  if (P > cap || !starts || !ends) {
+    st = fail(ctx, GLC_ERR_INVALID_ARG, "partition output capacity too small");
+  } else {
+    const cudaMemcpyKind k = (flags & GLC_HOST_OUT) ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
+    e = cudaMemcpyAsync(starts, ds, 4 * P, k, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(ends, de, 4 * P, k, s);
+    if (e != cudaSuccess) st = cuda_fail(ctx, e, "partition: copy out");
+  }
+  cudaFreeAsync(ds, s);
+  cudaFreeAsync(de, s);
+  if (flags & GLC_HOST_OUT) CK(cudaStreamSynchronize(s), "partition: sync");
+  return st;
+}
+
+// ---------------------------------------------------------------------------------------
+// decode / random access
+// ---------------------------------------------------------------------------------------
+static glc_status resolve_source(glc_ctx* ctx, const glc_column* c, glc_source src, int* plain) {
+  if (src == GLC_SRC_AUTO) src = c->d_plain ? GLC_SRC_PREUNPACKED : GLC_SRC_PACKED;
+  if (src == GLC_SRC_PREUNPACKED) {
+    if (!c->d_plain) return fail(ctx, GLC_ERR_UNSUPPORTED, "column has no pre-unpacked residuals");
+    *plain = 1;
+  } else if (src == GLC_SRC_PACKED) {
+    if (!c->d_words && c->n > 0) return fail(ctx, GLC_ERR_UNSUPPORTED, "column has no packed bitstream");
+    *plain = 0;
+  } else {
+    return fail(ctx, GLC_ERR_INVALID_ARG, "unknown source");
+  }
+  return GLC_OK;
+}
+
+glc_status glc_decompress_range(glc_ctx* ctx, const glc_column* col, glc_source source, int64_t first, int64_t count,
+                                void* out, int flags, glc_stream stream) {
+  if (!ctx || !col) return fail(ctx, GLC_ERR_INVALID_ARG, "null argument");
+  if (first < 0 || count < 0 || first + count > col->n) return fail(ctx, GLC_ERR_INVALID_ARG, "range outside the column");
+  if (count == 0) return GLC_OK;
+  if (!out) return fail(ctx, GLC_ERR_INVALID_ARG, "null output");
+  int plain = 0;
+  glc_status st = resolve_source(ctx, col, source, &plain);
+  if (st != GLC_OK) return st;
+  cudaSetDevice(ctx->device);
+  cudaStream_t s = pick(ctx, stream);
+  const size_t es = dtype_size(col->dtype);
+  void* dev_out = out;
+  if (flags & GLC_HOST_OUT) CK(cudaMallocAsync(&dev_out, count * es, s), "decode: output allocation");
+  char* base = (char*)dev_out - first * (int64_t)es;
+  cudaError_t e = launch_decode(ctx, col, plain, 0, first, first + count, base, s);
+  if (e == cudaSuccess && (flags & GLC_HOST_OUT)) e = cudaMemcpyAsync(out, dev_out, count * es, cudaMemcpyDeviceToHost, s);
+  if (flags & GLC_HOST_OUT) cudaFreeAsync(dev_out, s);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "decode");
+  if (flags & GLC_HOST_OUT) return glc_sync(ctx, stream);
+  return GLC_OK;
+}
+
+glc_status glc_decompress_full(glc_ctx* ctx, const glc_column* col, glc_source source, void* out, int flags,
+                               glc_stream stream) {
+  if (!col) return fail(ctx, GLC_ERR_INVALID_ARG, "null column");
+  return glc_decompress_range(ctx, col, source, 0, col->n, out, flags, stream);
+}
+
+glc_status glc_random_access(glc_ctx* ctx, const glc_column* col, glc_source source, const int32_t* positions,
+                             int64_t count, void* out, int flags, int32_t fixed_partition_len, glc_stream stream) {
+  if (!ctx || !col) return fail(ctx, GLC_ERR_INVALID_ARG, "null argument");
+  if (count < 0) return fail(ctx, GLC_ERR_INVALID_ARG, "negative count");
+  if (count == 0) return GLC_OK;
+  if (!positions || !out) return fail(ctx, GLC_ERR_INVALID_ARG, "null positions or output");
+  if (fixed_partition_len < 0) return fail(ctx, GLC_ERR_INVALID_ARG, "negative partition length");
+  if (fixed_partition_len > 0 && col->fixed_len != fixed_partition_len)
+    return fail(ctx, GLC_ERR_INVALID_ARG, "column is not partitioned with that fixed length");
+  int plain = 0;
+  glc_status st = resolve_source(ctx, col, source, &plain);
+  if (st != GLC_OK) return st;
+  cudaSetDevice(ctx->device);
+  cudaStream_t s = pick(ctx, stream);
+  const size_t es = dtype_size(col->dtype);
+  const int32_t* dpos = positions;
+  void* dout = out;
+  void* tpos = nullptr;
+  if (flags & GLC_HOST_IN) {
+    CK(cudaMallocAsync(&tpos, 4 * count, s), "random access: positions");
+    CK(cudaMemcpyAsync(tpos, positions, 4 * count, cudaMemcpyHostToDevice, s), "random access: positions");
+    dpos = (const int32_t*)tpos;
+  }
+  if (flags & GLC_HOST_OUT) CK(cudaMallocAsync(&dout, es * count, s), "random access: output");
+  const int32_t fl = fixed_partition_len > 0 ? fixed_partition_len : col->fixed_len;
+  cudaError_t e = launch_random_access(ctx, col, plain, dpos, count, dout, fl, s);
+  if (e == cudaSuccess && (flags & GLC_HOST_OUT)) e = cudaMemcpyAsync(out, dout, es * count, cudaMemcpyDeviceToHost, s);
+  if (tpos) cudaFreeAsync(tpos, s);
+  if (flags & GLC_HOST_OUT) cudaFreeAsync(dout, s);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "random access");
+  if (flags & (GLC_HOST_OUT | GLC_HOST_IN)) CK(cudaStreamSynchronize(s), "random access: sync");
+  return GLC_OK;
+}
+
+glc_status glc_preunpack(glc_ctx* ctx, glc_column* col, int drop_packed, glc_stream stream) {
+  if (!ctx || !col) return fail(ctx, GLC_ERR_INVALID_ARG, "null argument");
+  if (col->n == 0) return GLC_OK;
+  if (!col->d_plain) {
+    if (!col->d_words) return fail(ctx, GLC_ERR_UNSUPPORTED, "column has no packed bitstream");
+    cudaSetDevice(ctx->device);
+    cudaStream_t s = pick(ctx, stream);
+    CK(cudaMalloc(&col->d_plain, 8 * col->n + 16), "pre-unpack: allocation");  // +16: 16-byte TMA granules
+    CK(cudaMemsetAsync((char*)col->d_plain + 8 * col->n, 0, 16, s), "pre-unpack: padding");
+    CK(launch_decode(ctx, col, 0, 1, 0, col->n, col->d_plain, s), "pre-unpack");
+    CK(cudaStreamSynchronize(s), "pre-unpack: sync");
+  }
+  if (drop_packed && col->d_words) {  // api/G-LeCo.cuh:2283-2287
+    cudaFree(col->d_words);
+    col->d_words = nullptr;
+  }
+  return GLC_OK;
+}
+
+// ---------------------------------------------------------------------------------------
+// blob version 5
+// ---------------------------------------------------------------------------------------
+glc_status glc_blob_size(const glc_column* c, uint64_t* size) {
+  if (!c || !size) return GLC_ERR_INVALID_ARG;
+  BlobHeader h;
+  fill_layout(h, c->P, c->total_bits, dtype_size(c->dtype), c->n);
+  *size = blob_total(h);
+  return GLC_OK;
+}
+
+glc_status glc_serialize(glc_ctx* ctx, const glc_column* c, void* blob, uint64_t cap, int flags, int crc32c,
+                         uint64_t* written, glc_stream stream) {
+  if (!ctx || !c || !blob) return fail(ctx, GLC_ERR_INVALID_ARG, "null argument");
+  if (!c->d_words && c->d_plain) {  // api/G-LeCo.cuh:2005-2011
+    return fail(ctx, GLC_ERR_UNSUPPORTED, "a column whose bitstream was dropped cannot be serialized");
+  }
+  BlobHeader h;
+  fill_layout(h, c->P, c->total_bits, dtype_size(c->dtype), c->n);
+  const uint64_t total = blob_total(h);
+  if (written) *written = total;
+  if (cap < total) return fail(ctx, GLC_ERR_INVALID_ARG, "blob capacity too small");
+  BlobHeader t = h;
+  t.checksum = 0;
+  h.checksum = header_checksum((const uint8_t*)&t, sizeof t, crc32c);
+  cudaSetDevice(ctx->device);
+  cudaStream_t s = pick(ctx, stream);
+  const bool host = (flags & GLC_HOST_OUT) != 0;
+  uint8_t* b = (uint8_t*)blob;
+  const cudaMemcpyKind k = host ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
+  const uint64_t P = c->P;
+  struct Piece { uint64_t off; const void* src; uint64_t bytes; } pieces[8] = {
+      {h.start_off, c->d_start, 4 * P}, {h.end_off, c->d_end, 4 * P},     {h.types_off, c->d_types, 4 * P},
+      {h.params_off, c->d_params, 32 * P}, {h.bits_off, c->d_bits, 4 * P}, {h.offsets_off, c->d_offs, 8 * P},
+      {h.errb_off, c->d_err, 8 * P},     {h.delta_off, c->d_words, h.delta_size}};
+  // zero the gaps (alignment padding and the tail), then the header, then the arrays
+  uint64_t cursor = sizeof(BlobHeader);
+  for (const Piece& pc : pieces) {
+    if (pc.off > cursor) {
+      if (host) std::memset(b + cursor, 0, pc.off - cursor);
+      else CK(cudaMemsetAsync(b + cursor, 0, pc.off - cursor, s), "serialize: padding");
+    }
+    cursor = pc.off + pc.bytes;
+  }
+  if (total > cursor) {
+    if (host) std::memset(b + cursor, 0, total - cursor);
+    else CK(cudaMemsetAsync(b + cursor, 0, total - cursor, s), "serialize: padding");
+  }
+  if (host) std::memcpy(b, &h, sizeof h);
+  else CK(cudaMemcpyAsync(b, &h, sizeof h, cudaMemcpyHostToDevice, s), "serialize: header");
+  for (const Piece& pc : pieces)
+    if (pc.bytes) CK(cudaMemcpyAsync(b + pc.off, pc.src, pc.bytes, k, s), "serialize: arrays");
+  CK(cudaStreamSynchronize(s), "serialize: sync");  // the header lives on this stack frame
+  return GLC_OK;
+}
+
+glc_status glc_deserialize(glc_ctx* ctx, glc_dtype dtype, const void* blob, uint64_t size, int flags, int crc32c,
+                           int pre_unpack, glc_column** out, glc_stream stream) {
+  if (!ctx || !out) return fail(ctx, GLC_ERR_INVALID_ARG, "null argument");
+  *out = nullptr;
+  if (!valid_dtype(dtype)) return fail(ctx, GLC_ERR_INVALID_ARG, "unknown dtype");
+  if (!blob || size < sizeof(BlobHeader)) return fail(ctx, GLC_ERR_BAD_BLOB, "blob shorter than its header");
+  cudaSetDevice(ctx->device);
+  cudaStream_t s = pick(ctx, stream);
+  const bool host = (flags & GLC_HOST_IN) != 0;
+  BlobHeader h;
+  if (host) std::memcpy(&h, blob, sizeof h);
+  else CK(cudaMemcpy(&h, blob, sizeof h, cudaMemcpyDeviceToHost), "deserialize: header");
+  // api/G-LeCo.cuh:1029-1049, plus bounds checks on every array
+  if (h.magic != kMagic || (h.version != 4 && h.version != 5)) return fail(ctx, GLC_ERR_BAD_BLOB, "bad magic or version");
+  if ((int)h.type_size != dtype_size(dtype)) return fail(ctx, GLC_ERR_BAD_BLOB, "blob element size differs from dtype");
+  BlobHeader t = h;
+  t.checksum = 0;
+  if (header_checksum((const uint8_t*)&t, sizeof t, crc32c) != h.checksum)
+    return fail(ctx, GLC_ERR_BAD_BLOB, "header checksum mismatch");
+  uint64_t expected = h.delta_off + h.delta_size;
+  if (h.version == 5) expected = align8(expected);
+  if (h.delta_off > size || h.delta_size > size || expected > size) return fail(ctx, GLC_ERR_BAD_BLOB, "blob is short");
+  const uint64_t P = h.num_partitions;
+  const uint64_t offs[7] = {h.start_off, h.end_off, h.types_off, h.params_off, h.bits_off, h.offsets_off, h.errb_off};
+  const uint64_t lens[7] = {4 * P, 4 * P, 4 * P, 32 * P, 4 * P, 8 * P, 8 * P};
+  for (int k = 0; k < 7; k++)
+    if (offs[k] > size || lens[k] > size - offs[k]) return fail(ctx, GLC_ERR_BAD_BLOB, "array outside the blob");
+  if ((P == 0) != (h.total_values == 0)) return fail(ctx, GLC_ERR_BAD_BLOB, "partition count and length disagree");
+
+  glc_column* c = new (std::nothrow) glc_column();
+  if (!c) return fail(ctx, GLC_ERR_OOM, "host allocation");
+  c->ctx = ctx;
+  c->dtype = dtype;
+  c->n = h.total_values;
+  c->P = (int64_t)P;
+  c->total_bits = (int64_t)h.delta_size * 8;  // bound; refined below
+  auto bail = [&](glc_status st) { cudaStreamSynchronize(s); free_column_arrays(c); delete c; return st; };
+  if (c->n == 0) {
+    set_word_counts(c);
+    c->reported_size = 0;
+    *out = c;
+    return GLC_OK;
+  }
+  cudaError_t e = alloc_meta(c);
+  if (e != cudaSuccess) return bail(cuda_fail(ctx, e, "deserialize: allocation"));
+  set_word_counts(c);
+  if ((e = cudaMalloc(&c->d_words, 4 * c->nwords_alloc)) != cudaSuccess) return bail(cuda_fail(ctx, e, "deserialize: allocation"));
+  const cudaMemcpyKind k = host ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
+  const uint8_t* b = (const uint8_t*)blob;
+  void* dst[7] = {c->d_start, c->d_end, c->d_types, c->d_params, c->d_bits, c->d_offs, c->d_err};
+  for (int j = 0; j < 7; j++)
+    if (lens[j] && (e = cudaMemcpyAsync(dst[j], b + offs[j], lens[j], k, s)) != cudaSuccess)
+      return bail(cuda_fail(ctx, e, "deserialize: arrays"));
+  if ((e = cudaMemsetAsync(c->d_words, 0, 4 * c->nwords_alloc, s)) != cudaSuccess ||
+      (h.delta_size && (e = cudaMemcpyAsync(c->d_words, b + h.delta_off, h.delta_size, k, s)) != cudaSuccess))
+    return bail(cuda_fail(ctx, e, "deserialize: bitstream"));
+  // structure check, fixed-length detection and max width
+  int* d_chk = (int*)(ctx->d_stats + 4);
+  if ((e = cudaMemsetAsync(ctx->d_stats, 0, 8 * sizeof(int64_t), s)) != cudaSuccess ||
+      (e = launch_validate(c, d_chk, s)) != cudaSuccess || (e = launch_max_bits(c, ctx->d_stats + 1, s)) != cudaSuccess ||
+      (e = cudaMemcpyAsync(ctx->h_stats, ctx->d_stats, 8 * sizeof(int64_t), cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
+      (e = cudaStreamSynchronize(s)) != cudaSuccess)
+    return bail(cuda_fail(ctx, e, "deserialize: validation"));
+  const int* chk = (const int*)(ctx->h_stats + 4);
+  if (chk[0]) return bail(fail(ctx, GLC_ERR_BAD_BLOB, "partition arrays are inconsistent"));
+  c->max_bits = (int32_t)ctx->h_stats[1];
+  c->fixed_len = 0;
+  if (!chk[1]) {
+    int32_t s0 = 0, e0 = 0;
+    if (host) {
+      std::memcpy(&s0, b + h.start_off, 4);
+      std::memcpy(&e0, b + h.end_off, 4);
+    } else {
+      cudaMemcpy(&s0, c->d_start, 4, cudaMemcpyDeviceToHost);
+      cudaMemcpy(&e0, c->d_end, 4, cudaMemcpyDeviceToHost);
+    }
+    c->fixed_len = e0 - s0;
+  }
+  // total bits: the end of the last partition's range (api/G-LeCo.cuh:2016-2044)
+  {
+    int32_t ls = 0, le = 0, lb = 0;
+    int64_t lo = 0;
+    const uint64_t L = P - 1;
+    if (host) {
+      std::memcpy(&ls, b + h.start_off + 4 * L, 4);
+      std::memcpy(&le, b + h.end_off + 4 * L, 4);
+      std::memcpy(&lb, b + h.bits_off + 4 * L, 4);
+      std::memcpy(&lo, b + h.offsets_off + 8 * L, 8);
+    } else {
+      cudaMemcpy(&ls, c->d_start + L, 4, cudaMemcpyDeviceToHost);
+      cudaMemcpy(&le, c->d_end + L, 4, cudaMemcpyDeviceToHost);
+      cudaMemcpy(&lb, c->d_bits + L, 4, cudaMemcpyDeviceToHost);
+      cudaMemcpy(&lo, c->d_offs + L, 8, cudaMemcpyDeviceToHost);
+    }
+    c->total_bits = lo + (int64_t)(le - ls) * lb;
+  }
+  if ((e = launch_desc_and_tiles(c, s)) != cudaSuccess) return bail(cuda_fail(ctx, e, "deserialize: tables"));
+  c->reported_size = reported_size(c->P, c->total_bits);
+  if (pre_unpack) {
+    glc_status st = glc_preunpack(ctx, c, 1, stream);
+    if (st != GLC_OK) return bail(st);
+  }
+  if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return bail(cuda_fail(ctx, e, "deserialize: sync"));
+  *out = c;
+  return GLC_OK;
+}
+
+}  // extern "C"

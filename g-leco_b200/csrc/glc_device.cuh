@@ -1,0 +1,222 @@
+// glc_device.cuh -- device-side arithmetic of the G-LeCo format (sm_100a).
+//
+// The format contract (identical to the reference, so reference-made blobs decode here and
+// blobs made here decode with the reference):
+//   prediction  pred = sat_cast<T>(round(fma(theta1, (double)i, theta0)))
+//               decompression/FullDecompressionKernels.cuh:161,177-187; the encoder
+//               compression/CompressionKernels.cuh:318-324 computes the same value because the
+//               GPU double->int conversion saturates (negative -> 0 for unsigned types).
+//   residual    core/MathHelpers.cuh:22-53 calculateDelta (u64: saturating signed difference)
+//   apply       core/MathHelpers.cuh:55-84 applyDelta (wraparound)
+//   bit width   bitlen(max|delta|) + 1, capped at 64 (CompressionKernels.cuh:190-207)
+//   bitstream   field i of partition p at bit offset[p] + i*bits, LSB first in uint32 words,
+//               sign-extended on read; direct-copy fields zero-extended
+//               (core/BitManipulation.cuh:80-200)
+//
+// The model fit is this implementation's own: least squares from EXACT 128-bit integer sums,
+// converted to double with one correctly rounded step, so any summation order gives the
+// same theta (the reference's theta depends on its reduction order).
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace glc {
+
+typedef __int128 i128;
+typedef unsigned __int128 u128;
+
+enum : int { MODEL_CONSTANT = 0, MODEL_LINEAR = 1, MODEL_POLY2 = 2, MODEL_POLY3 = 3, MODEL_DIRECT_COPY = 4 };
+constexpr unsigned FULL_MASK = 0xffffffffu;
+constexpr int kMinPart = 128;        // core/CudaUtils.cuh:20 MIN_PARTITION_SIZE
+constexpr double kModelBytes = 80.0; // compression/CpuPartitioner.cuh:18 sizeof(PartitionInfo)
+
+// 32-byte packed partition descriptor: one sector per lookup in random access.
+// bits_type = delta_bits | (model_type << 8).
+struct __align__(32) PartDesc {
+  double theta0;
+  double theta1;
+  int64_t bit_off;
+  int32_t start;
+  int32_t bits_type;
+};
+
+template <typename T> struct TypeTraits;
+template <> struct TypeTraits<int32_t>  { static constexpr bool is_signed = true;  };
+template <> struct TypeTraits<int64_t>  { static constexpr bool is_signed = true;  };
+template <> struct TypeTraits<uint64_t> { static constexpr bool is_signed = false; };
+template <> struct TypeTraits<uint32_t> { static constexpr bool is_signed = false; };
+
+// ---------------------------------------------------------------------------------------
+// Saturating cast of an integral double (NaN -> 0), the GPU cvt.rzi semantics made explicit.
+// ---------------------------------------------------------------------------------------
+template <typename T> __device__ __forceinline__ T sat_cast(double r);
+template <> __device__ __forceinline__ int32_t sat_cast<int32_t>(double r) {
+  if (r != r) return 0;
+  if (r >= 2147483648.0) return INT32_MAX;
+  if (r <= -2147483648.0) return INT32_MIN;
+  return (int32_t)r;
+}
+template <> __device__ __forceinline__ int64_t sat_cast<int64_t>(double r) {
+  if (r != r) return 0;
+  if (r >= 9223372036854775808.0) return INT64_MAX;
+  if (r <= -9223372036854775808.0) return INT64_MIN;
+  return (int64_t)r;
+}
+template <> __device__ __forceinline__ uint64_t sat_cast<uint64_t>(double r) {
+  if (!(r > 0.0)) return 0ull;
+  if (r >= 18446744073709551616.0) return ~0ull;
+  return (uint64_t)r;
+}
+template <> __device__ __forceinline__ uint32_t sat_cast<uint32_t>(double r) {
+  if (!(r > 0.0)) return 0u;
+  if (r >= 4294967296.0) return 0xffffffffu;
+  return (uint32_t)r;
+}
+
+template <typename T> __device__ __forceinline__ T predict(double theta0, double theta1, int64_t i) {
+  double p = __fma_rn(theta1, __ll2double_rn(i), theta0);
+  return sat_cast<T>(round(p));
+}
+
+template <typename T> __device__ __forceinline__ long long calc_delta(T actual, T pred) {
+  if (TypeTraits<T>::is_signed) {
+    return (long long)((unsigned long long)(long long)actual - (unsigned long long)(long long)pred);
+  } else if (sizeof(T) == 8) {
+    unsigned long long a = (unsigned long long)actual, p = (unsigned long long)pred;
+    if (a >= p) {
+      unsigned long long d = a - p;
+      return d <= 0x7fffffffffffffffull ? (long long)d : (long long)0x7fffffffffffffffull;
+    }
+    unsigned long long d = p - a;
+    return d <= 0x7fffffffffffffffull ? -(long long)d : (long long)0x8000000000000000ull;
+  } else {
+    return (long long)actual - (long long)pred;
+  }
+}
+
+template <typename T> __device__ __forceinline__ T apply_delta(T pred, long long delta) {
+  if (sizeof(T) == 8) return (T)((unsigned long long)pred + (unsigned long long)delta);
+  return (T)((uint32_t)pred + (uint32_t)delta);
+}
+
+// |d| for the bit width; |LLONG_MIN| counts as LLONG_MAX so that residual gets a 64-bit field
+// (the reference's (d < 0) ? -d : d leaves it negative and truncates it,
+// compression/CompressionKernels.cuh:171-174).
+__device__ __forceinline__ long long abs_ref(long long d) {
+  if (d == (long long)0x8000000000000000ull) return 0x7fffffffffffffffll;
+  return d < 0 ? -d : d;
+}
+
+__device__ __forceinline__ int bits_for(long long max_err) {
+  if (max_err <= 0) return 0;
+  int b = 64 - __clzll(max_err);
+  return b + 1 < 64 ? b + 1 : 64;
+}
+
+template <typename T> __device__ __forceinline__ bool overflows_double(T v) {
+  if (TypeTraits<T>::is_signed) return false;
+  return (uint64_t)v > (1ull << 53);
+}
+
+// Field of `bits` bits (1..64), masked.
+__device__ __forceinline__ uint64_t low_bits(uint64_t x, int bits) {
+  return bits >= 64 ? x : (x & ((1ull << bits) - 1ull));
+}
+
+__device__ __forceinline__ long long sign_extend(uint64_t f, int bits) {
+  if (bits <= 0) return 0;
+  if (bits >= 64) return (long long)f;
+  uint64_t sign = 1ull << (bits - 1);
+  return (long long)((f ^ sign) - sign);
+}
+
+// Read `bits` (1..64) bits starting at bit `pos` from a word array (global or shared).
+// Reads up to three consecutive words; callers guarantee those words exist (padding).
+__device__ __forceinline__ uint64_t read_field(const uint32_t* w, int64_t pos, int bits) {
+  int64_t wi = pos >> 5;
+  int sh = (int)(pos & 31);
+  uint64_t lo = (uint64_t)w[wi] | ((uint64_t)w[wi + 1] << 32);
+  uint64_t f = lo >> sh;
+  if (bits + sh > 64) f |= (uint64_t)w[wi + 2] << (64 - sh);
+  return low_bits(f, bits);
+}
+
+// ---------------------------------------------------------------------------------------
+// Exact sums -> least-squares line.
+// ---------------------------------------------------------------------------------------
+__device__ __forceinline__ double pow2_exact(int e) {
+  return __longlong_as_double((long long)(1023 + e) << 52);
+}
+
+// Correctly rounded (nearest-even) conversion of a 128-bit integer.
+__device__ __forceinline__ double i128_to_double(i128 v) {
+  if (v == 0) return 0.0;
+  bool neg = v < 0;
+  u128 u = neg ? (u128)0 - (u128)v : (u128)v;
+  uint64_t hi = (uint64_t)(u >> 64);
+  double r;
+  if (hi == 0) {
+    r = __ull2double_rn((uint64_t)u);
+  } else {
+    int sh = 64 - __clzll((long long)hi);
+    uint64_t m = (uint64_t)(u >> sh);
+    uint64_t mask = (sh == 64) ? ~0ull : ((1ull << sh) - 1ull);
+    if (((uint64_t)u & mask) != 0) m |= 1ull;
+    r = __dmul_rn(__ull2double_rn(m), pow2_exact(sh));
+  }
+  return neg ? -r : r;
+}
+
+// n(n^2-1)/6 exactly, without 128-bit division.
+__device__ __forceinline__ i128 den6_exact(int64_t n) {
+  int64_t a = n - 1, b = n, c = n + 1;
+  if (a % 3 == 0) a /= 3; else if (b % 3 == 0) b /= 3; else c /= 3;
+  if ((a & 1) == 0) a /= 2; else if ((b & 1) == 0) b /= 2; else c /= 2;
+  return (i128)a * (i128)b * (i128)c;
+}
+
+// theta1 = (2 Sxy - (n-1) Sy) / (n(n^2-1)/6);  theta0 = (Sy - theta1 * n(n-1)/2) / n.
+__device__ __forceinline__ void solve_line(int64_t n, i128 sy, i128 sxy, double& theta0, double& theta1) {
+  if (n <= 0) { theta0 = 0.0; theta1 = 0.0; return; }
+  if (n == 1) { theta1 = 0.0; theta0 = i128_to_double(sy); return; }
+  i128 num = (i128)2 * sxy - (i128)(n - 1) * sy;
+  double t1 = __ddiv_rn(i128_to_double(num), i128_to_double(den6_exact(n)));
+  double sx = __ll2double_rn((n * (n - 1)) / 2);
+  double diff = __dsub_rn(i128_to_double(sy), __dmul_rn(t1, sx));
+  theta1 = t1;
+  theta0 = __ddiv_rn(diff, __ll2double_rn(n));
+}
+
+// ---------------------------------------------------------------------------------------
+// Warp reductions.
+// ---------------------------------------------------------------------------------------
+__device__ __forceinline__ i128 shfl_xor_i128(i128 v, int m) {
+  unsigned long long lo = (unsigned long long)v;
+  long long hi = (long long)(v >> 64);
+  lo = __shfl_xor_sync(FULL_MASK, lo, m);
+  hi = __shfl_xor_sync(FULL_MASK, hi, m);
+  return ((i128)hi << 64) | (i128)lo;
+}
+
+__device__ __forceinline__ i128 warp_sum_i128(i128 v) {
+#pragma unroll
+  for (int m = 16; m > 0; m >>= 1) v += shfl_xor_i128(v, m);
+  return v;
+}
+
+__device__ __forceinline__ long long warp_max_ll(long long v) {
+#pragma unroll
+  for (int m = 16; m > 0; m >>= 1) {
+    long long o = __shfl_xor_sync(FULL_MASK, v, m);
+    v = o > v ? o : v;
+  }
+  return v;
+}
+
+// Bounded spin limit for every wait in these kernels (an mbarrier phase); after it the kernel
+// records an error code and returns instead of spinning forever.
+constexpr long long kSpinLimit = 1ll << 26;
+
+enum : int { DEVERR_NONE = 0, DEVERR_TIMEOUT = 1, DEVERR_BOUNDS = 2 };
+
+}  // namespace glc

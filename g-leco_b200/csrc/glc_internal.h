@@ -1,0 +1,106 @@
+// glc_internal.h -- host-side structures and kernel launchers of libglc (not part of the ABI).
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <atomic>
+#include <string>
+#include "glc.h"
+#include "glc_device.cuh"
+
+namespace glc {
+
+// Decode work unit: a fixed run of output values.  4096 values are 16-32 KB of output, the
+// unit each persistent CTA claims from the work counter.
+constexpr int kDecodeTile = 4096;
+constexpr int kDecodeThreads = 256;
+constexpr int kDescCache = 128;  // partitions per tile kept in shared memory
+
+// Per decode tile: bit position of its first value and the partitions it spans.  The table
+// has ntiles + 1 entries; the last one holds total_bits.
+struct TileInfo {
+  int64_t bit_lo;
+  int32_t p_first;
+  int32_t p_last;
+};
+
+// Device scratch owned by a context (grow-only).
+struct Scratch {
+  void* ptr = nullptr;
+  size_t bytes = 0;
+};
+
+}  // namespace glc
+
+namespace glc {
+// Work counters of concurrent decode launches rotate through this many slots.
+constexpr int kCounterSlots = 64;
+constexpr int kFlagError = kCounterSlots;      // device error code (DEVERR_*)
+constexpr int kFlagWords = kCounterSlots + 8;
+}  // namespace glc
+
+struct glc_ctx {
+  int device = 0;
+  int num_sms = 0;
+  cudaStream_t own_stream = nullptr;
+  int* d_flags = nullptr;      // [0, 64) decode work counters, [64] device error code
+  int64_t* d_stats = nullptr;  // small readback area (total bits, max bits, ...)
+  int64_t* h_stats = nullptr;  // pinned mirror of d_stats
+  std::atomic<unsigned> next_slot{0};
+  std::string err;
+};
+
+struct glc_column {
+  glc_ctx* ctx = nullptr;
+  glc_dtype dtype = GLC_I32;
+  int64_t n = 0;
+  int64_t P = 0;
+  int64_t total_bits = 0;
+  int64_t nwords = 0;        // ceil(total_bits / 32)
+  int64_t nwords_alloc = 0;  // nwords rounded up to 4 plus zeroed padding for over-reads
+  int32_t max_bits = 0;
+  int32_t fixed_len = 0;
+  int64_t reported_size = 0;
+  // reference SoA (CompressedData<T>)
+  int32_t* d_start = nullptr;
+  int32_t* d_end = nullptr;
+  int32_t* d_types = nullptr;
+  double* d_params = nullptr;
+  int32_t* d_bits = nullptr;
+  int64_t* d_offs = nullptr;
+  int64_t* d_err = nullptr;
+  uint32_t* d_words = nullptr;
+  int64_t* d_plain = nullptr;
+  // derived lookup tables
+  glc::PartDesc* d_desc = nullptr;
+  glc::TileInfo* d_tiles = nullptr;
+  int64_t ntiles = 0;
+};
+
+namespace glc {
+
+inline int dtype_size(glc_dtype d) { return (d == GLC_I64 || d == GLC_U64) ? 8 : 4; }
+
+// ---- kernel launchers (defined in the .cu files) -------------------------------------
+// fit.cu
+cudaError_t launch_fixed_partitions(int32_t* starts, int32_t* ends, int64_t n, int32_t len, int64_t P, cudaStream_t s);
+size_t fit_scratch_bytes(const int32_t* unused, int64_t n, int64_t P);
+// Fits every partition of c (starts/ends set); d_stats[0] = total bits, d_stats[1] = max bits.
+cudaError_t launch_fit(glc_dtype dt, const void* values, glc_column* c, void* scratch, size_t scratch_bytes,
+                       int64_t* d_stats, cudaStream_t s);
+cudaError_t launch_desc_and_tiles(glc_column* c, cudaStream_t s);
+cudaError_t launch_validate(const glc_column* c, int* d_bad, cudaStream_t s);
+cudaError_t launch_max_bits(const glc_column* c, int64_t* d_out, cudaStream_t s);
+// pack.cu
+cudaError_t launch_pack(glc_dtype dt, const void* values, glc_column* c, cudaStream_t s);
+// decode.cu: values (or residuals when residual_out) of positions [lo, hi) to out_base[lo..hi)
+cudaError_t launch_decode(glc_ctx* ctx, const glc_column* c, int plain_src, int residual_out, int64_t lo,
+                          int64_t hi, void* out_base, cudaStream_t s);
+// random_access.cu
+cudaError_t launch_random_access(glc_ctx* ctx, const glc_column* c, int plain_src, const int32_t* pos,
+                                 int64_t q, void* out, int32_t fixed_len, cudaStream_t s);
+// partition.cu: allocates *d_starts / *d_ends (cudaMallocAsync on s)
+cudaError_t launch_partition_variable(glc_ctx* ctx, glc_dtype dt, const void* values, int64_t n,
+                                      int32_t** d_starts, int32_t** d_ends, int64_t* P, cudaStream_t s,
+                                      std::string* err);
+
+}  // namespace glc

@@ -1,0 +1,457 @@
+// partition.cu -- variable-length partitioning by model cost, on the device.
+//
+// Replaces VariableLengthPartitioner<T>::partition (compression/CpuPartitioner.cuh:342-422),
+// which the reference runs single-threaded on the host (its GPU alternative,
+// GPUVariableLengthPartitionerV6, sizes partitions by a variance heuristic and never merges).
+//
+// Cost of a partition [a, b): 80 + (b - a) * bits / 8 bytes (CpuPartitioner.cuh:128-138), with
+// bits from the exact-sum least-squares fit of [a, b) (glc_device.cuh).
+//
+// Split.  The reference walks from 0: at start s it tries sizes 128..3712 (steps of 128 up to
+// 640, then 256 up to 2176, then 512; CpuPartitioner.cuh:150-175), keeps the first size with
+// the lowest cost per value and jumps there.  Every start on that walk is a multiple of 128,
+// so the best end of EVERY 128-aligned start is computed in parallel (one warp per start; each
+// value is loaded once and scored against all candidate lines that contain it), and the walk
+// is recovered afterwards: the starts are cut into ranges of 1024 blocks, the exit of each
+// possible entry point of a range is computed in parallel, one thread chains the ranges, and
+// each range marks its walk.
+//
+// Merge.  The reference absorbs right neighbours left to right while the merged cost is lower
+// (CpuPartitioner.cuh:198-242).  Here merging runs in rounds: every adjacent pair is scored,
+// and the profitable pairs with (index + round) even merge, so the chosen pairs never overlap;
+// rounds stop when no pair is profitable (at most 64 rounds).  A pair whose two partitions did
+// not change keeps its score from the previous round.
+//
+// Fits use exact 128-bit sums from a prefix over 128-value blocks (every boundary here is a
+// multiple of 128 or n), so each candidate's line costs O(1) and only its max |delta| needs a
+// pass over the values.  The CPU oracle restates this algorithm step for step.
+#include "glc_internal.h"
+#include "glc_scan.cuh"
+
+namespace glc {
+
+constexpr int kNumSizes = 14;
+__constant__ int c_sizes[kNumSizes] = {128, 256, 384, 512, 640, 896, 1152, 1408, 1664, 1920, 2176, 2688, 3200, 3712};
+constexpr int kMaxJumpBlocks = 29;  // 3712 / 128
+constexpr int kRangeBlocks = 1024;
+constexpr int kMaxMergeRounds = 64;
+constexpr int kPairChunk = 4096;
+
+struct SumPair {  // trivially constructible: SumPair() value-initialises to zero
+  i128 y;
+  i128 iy;
+  __device__ __forceinline__ SumPair operator+(const SumPair& o) const {
+    SumPair r;
+    r.y = y + o.y;
+    r.iy = iy + o.iy;
+    return r;
+  }
+};
+
+// ---- block sums -----------------------------------------------------------------------
+template <typename T> __global__ void block_sums_kernel(const T* __restrict__ v, int64_t n, int64_t nb, SumPair* __restrict__ out) {
+  const int64_t j = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (j >= nb) return;
+  i128 sy = 0, siy = 0;
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    const int64_t i = j * kMinPart + k * 32 + lane;
+    if (i < n) {
+      const i128 y = (i128)__ldg(v + i);
+      sy += y;
+      siy += (i128)i * y;
+    }
+  }
+  sy = warp_sum_i128(sy);
+  siy = warp_sum_i128(siy);
+  if (lane == 0) {
+    SumPair s;
+    s.y = sy;
+    s.iy = siy;
+    out[j] = s;
+  }
+}
+
+struct RangeSums {
+  const SumPair* pre;  // nb + 1 entries
+  int64_t n, nb;
+  __device__ __forceinline__ int64_t blk(int64_t pos) const { return pos >= n ? nb : pos / kMinPart; }
+  // exact sums of [a, b): sum y and sum (i - a) * y
+  __device__ __forceinline__ void get(int64_t a, int64_t b, i128& sy, i128& sxy) const {
+    const SumPair pb = pre[blk(b)], pa = pre[blk(a)];
+    sy = pb.y - pa.y;
+    sxy = (pb.iy - pa.iy) - (i128)a * sy;
+  }
+  __device__ __forceinline__ void line(int64_t a, int64_t b, double& t0, double& t1) const {
+    i128 sy, sxy;
+    get(a, b, sy, sxy);
+    solve_line(b - a, sy, sxy, t0, t1);
+  }
+};
+
+__device__ __forceinline__ double part_cost(int64_t len, int bits) {
+  return __dadd_rn(kModelBytes, __ddiv_rn(__dmul_rn(__ll2double_rn(len), (double)bits), 8.0));
+}
+
+// ---- split: best end of every 128-aligned start ------------------------------------------
+template <typename T> __global__ void __launch_bounds__(256)
+split_kernel(const T* __restrict__ v, RangeSums rs, int32_t* __restrict__ nb_next) {
+  __shared__ double s_th[8][kNumSizes][2];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int64_t j = (int64_t)blockIdx.x * 8 + warp;
+  if (j >= rs.nb) return;
+  const int64_t s = j * kMinPart;
+  const int64_t max_size = (rs.n - s < kMinPart * 32) ? rs.n - s : kMinPart * 32;
+  int ncand = 0;
+#pragma unroll
+  for (int k = 0; k < kNumSizes; k++) ncand += (c_sizes[k] <= max_size) ? 1 : 0;
+  if (ncand == 0) {  // fewer than 128 values left: the rest is one partition
+    if (lane == 0) nb_next[j] = (int32_t)rs.nb;
+    return;
+  }
+  if (lane < ncand) {
+    double t0, t1;
+    rs.line(s, s + c_sizes[lane], t0, t1);
+    s_th[warp][lane][0] = t0;
+    s_th[warp][lane][1] = t1;
+  }
+  __syncwarp();
+  long long m[kNumSizes];
+#pragma unroll
+  for (int k = 0; k < kNumSizes; k++) m[k] = 0;
+  const int total = c_sizes[ncand - 1];
+  int band = 0;  // first candidate whose size exceeds the offset (uniform: sizes are multiples of 128)
+  for (int o0 = 0; o0 < total; o0 += 32) {
+    while (c_sizes[band] <= o0) band++;
+    const int o = o0 + lane;
+    const T y = __ldg(v + s + o);
+#pragma unroll
+    for (int k = 0; k < kNumSizes; k++) {
+      if (k < band || k >= ncand) continue;
+      const long long d = abs_ref(calc_delta<T>(y, predict<T>(s_th[warp][k][0], s_th[warp][k][1], o)));
+      m[k] = d > m[k] ? d : m[k];
+    }
+  }
+  double best_cpe = 1.7976931348623157e308;
+  int best = 0;
+#pragma unroll
+  for (int k = 0; k < kNumSizes; k++) {
+    if (k >= ncand) continue;
+    const long long mk = warp_max_ll(m[k]);
+    const double cpe = __ddiv_rn(part_cost(c_sizes[k], bits_for(mk)), (double)c_sizes[k]);
+    if (cpe < best_cpe) { best_cpe = cpe; best = k; }
+  }
+  if (lane == 0) {
+    const int64_t e = s + c_sizes[best];
+    nb_next[j] = (int32_t)(e >= rs.n ? rs.nb : e / kMinPart);
+  }
+}
+
+// ---- walk from 0 ---------------------------------------------------------------------------
+constexpr int32_t kEnd = -1;
+
+__global__ void chain_exit_kernel(const int32_t* __restrict__ nb_next, int64_t nb, int64_t nr, int32_t* __restrict__ exits) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nr * kMaxJumpBlocks) return;
+  const int64_t r = t / kMaxJumpBlocks, x = t % kMaxJumpBlocks;
+  const int64_t lim = (r + 1) * kRangeBlocks;
+  int64_t node = r * kRangeBlocks + x;
+  while (node < lim && node < nb) node = nb_next[node];
+  exits[t] = (node >= nb) ? kEnd : (int32_t)(node - lim);
+}
+
+__global__ void chain_link_kernel(const int32_t* __restrict__ exits, int64_t nr, int32_t* __restrict__ entries) {
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  int32_t e = 0;
+  for (int64_t r = 0; r < nr; r++) {
+    entries[r] = e;
+    if (e != kEnd) e = exits[r * kMaxJumpBlocks + e];
+  }
+}
+
+__global__ void chain_mark_kernel(const int32_t* __restrict__ nb_next, const int32_t* __restrict__ entries, int64_t nb,
+                                  int64_t nr, int64_t* __restrict__ flags) {
+  const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= nr) return;
+  const int32_t e = entries[r];
+  if (e == kEnd) return;
+  const int64_t lim = (r + 1) * kRangeBlocks;
+  int64_t node = r * kRangeBlocks + e;
+  while (node < lim && node < nb) {
+    flags[node] = 1;
+    node = nb_next[node];
+  }
+}
+
+__global__ void chain_compact_kernel(const int64_t* __restrict__ flags, const int64_t* __restrict__ idx,
+                                     const int32_t* __restrict__ nb_next, int64_t nb, int64_t n,
+                                     int32_t* __restrict__ ps, int32_t* __restrict__ pe) {
+  const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= nb || !flags[j]) return;
+  const int64_t k = idx[j];
+  ps[k] = (int32_t)(j * kMinPart);
+  const int64_t e = (int64_t)nb_next[j] * kMinPart;
+  pe[k] = (int32_t)(e > n ? n : e);
+}
+
+// ---- costs of partitions ---------------------------------------------------------------
+struct LineJob {  // one range whose max |delta| is needed
+  int32_t a, b;
+  double t0, t1;
+};
+
+__device__ __forceinline__ int64_t owner_last_le(const int64_t* __restrict__ base, int64_t cnt, int64_t c) {
+  int64_t lo = 0, hi = cnt - 1;
+  while (lo < hi) {
+    int64_t mid = (lo + hi + 1) >> 1;
+    if (base[mid] <= c) lo = mid; else hi = mid - 1;
+  }
+  return lo;
+}
+
+// chunks of each job (0 for jobs that are cached)
+__global__ void job_setup_kernel(const int32_t* __restrict__ ps, const int32_t* __restrict__ pe, int64_t m, int pairs,
+                                 const uint8_t* __restrict__ cached, RangeSums rs, LineJob* __restrict__ jobs,
+                                 int64_t* __restrict__ nch, long long* __restrict__ err) {
+  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t njobs = pairs ? m - 1 : m;
+  if (k >= njobs) return;
+  LineJob jb;
+  jb.a = ps[k];
+  jb.b = pairs ? pe[k + 1] : pe[k];
+  rs.line(jb.a, jb.b, jb.t0, jb.t1);
+  jobs[k] = jb;
+  err[k] = 0;
+  const bool skip = cached && cached[k];
+  nch[k] = skip ? 0 : ((int64_t)jb.b - jb.a + kPairChunk - 1) / kPairChunk;
+}
+
+template <typename T> __global__ void __launch_bounds__(256)
+job_err_kernel(const T* __restrict__ v, const LineJob* __restrict__ jobs, const int64_t* __restrict__ base,
+               int64_t njobs, const int64_t* __restrict__ total_chunks, long long* __restrict__ err) {
+  const int64_t c = blockIdx.x;
+  if (c >= *total_chunks) return;
+  const int64_t k = owner_last_le(base, njobs, c);
+  const LineJob jb = jobs[k];
+  const int64_t off0 = (c - base[k]) * kPairChunk;
+  const int64_t len = (int64_t)jb.b - jb.a;
+  const int64_t off1 = off0 + kPairChunk < len ? off0 + kPairChunk : len;
+  long long mm = 0;
+  for (int64_t o = off0 + threadIdx.x; o < off1; o += 256) {
+    const long long d = abs_ref(calc_delta<T>(__ldg(v + jb.a + o), predict<T>(jb.t0, jb.t1, o)));
+    mm = d > mm ? d : mm;
+  }
+  mm = warp_max_ll(mm);
+  __shared__ long long s_m[8];
+  if ((threadIdx.x & 31) == 0) s_m[threadIdx.x >> 5] = mm;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    long long t = 0;
+    for (int w = 0; w < 8; w++) t = s_m[w] > t ? s_m[w] : t;
+    if (t > 0) atomicMax(err + k, t);
+  }
+}
+
+// Initial part costs.
+__global__ void part_cost_kernel(const LineJob* __restrict__ jobs, const long long* __restrict__ err, int64_t m,
+                                 double* __restrict__ pc) {
+  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= m) return;
+  pc[k] = part_cost((int64_t)jobs[k].b - jobs[k].a, bits_for(err[k]));
+}
+
+// Pair scores: merged cost (fresh or cached) and profitability; any profitable -> *any = 1.
+__global__ void pair_score_kernel(const LineJob* __restrict__ jobs, const long long* __restrict__ err,
+                                  const uint8_t* __restrict__ cached, const double* __restrict__ cached_mc,
+                                  const double* __restrict__ pc, int64_t m, double* __restrict__ mc,
+                                  uint8_t* __restrict__ prof, int* __restrict__ any) {
+  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= m - 1) return;
+  double c;
+  if (cached && cached[k]) c = cached_mc[k];
+  else c = part_cost((int64_t)jobs[k].b - jobs[k].a, bits_for(err[k]));
+  mc[k] = c;
+  const bool p = c < __dadd_rn(pc[k], pc[k + 1]);
+  prof[k] = p ? 1 : 0;
+  if (p) atomicOr(any, 1);
+}
+
+// heads: part k starts a new part unless pair k-1 merges.
+__global__ void merge_heads_kernel(const uint8_t* __restrict__ prof, int64_t m, int round, int64_t* __restrict__ head) {
+  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= m) return;
+  const bool absorbed = k > 0 && prof[k - 1] && (((k - 1) + round) % 2 == 0);
+  head[k] = absorbed ? 0 : 1;
+}
+
+__device__ __forceinline__ bool selected(const uint8_t* prof, int64_t m, int64_t k, int round) {
+  return k >= 0 && k < m - 1 && prof[k] && ((k + round) % 2 == 0);
+}
+
+__global__ void merge_scatter_kernel(const int32_t* __restrict__ ps, const int32_t* __restrict__ pe,
+                                     const double* __restrict__ pc, const double* __restrict__ mc,
+                                     const uint8_t* __restrict__ prof, const int64_t* __restrict__ head,
+                                     const int64_t* __restrict__ idx, int64_t m, int round,
+                                     int32_t* __restrict__ ps2, int32_t* __restrict__ pe2, double* __restrict__ pc2,
+                                     uint8_t* __restrict__ cached2, double* __restrict__ cmc2) {
+  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= m || !head[k]) return;
+  const int64_t d = idx[k];
+  const bool sel = selected(prof, m, k, round);
+  ps2[d] = ps[k];
+  pe2[d] = sel ? pe[k + 1] : pe[k];
+  pc2[d] = sel ? mc[k] : pc[k];
+  // the score of (this part, next part) survives when neither changed
+  const int64_t nxt = sel ? k + 2 : k + 1;  // old index of the next head
+  const bool keep = !sel && nxt < m && !selected(prof, m, nxt, round);
+  cached2[d] = keep ? 1 : 0;
+  cmc2[d] = keep ? mc[k] : 0.0;
+}
+
+static inline size_t al(size_t x) { return (x + 255) & ~(size_t)255; }
+
+template <typename T>
+static cudaError_t partition_typed(glc_ctx* ctx, const T* v, int64_t n, int32_t** out_s, int32_t** out_e, int64_t* outP,
+                                   cudaStream_t s, std::string* err) {
+  cudaError_t e;
+  *out_s = nullptr;
+  *out_e = nullptr;
+  *outP = 0;
+  if (n <= 0) return cudaSuccess;
+  const int64_t nb = (n + kMinPart - 1) / kMinPart;
+  const int64_t nr = (nb + kRangeBlocks - 1) / kRangeBlocks;
+  const int64_t mmax = nb;  // split partitions are >= 128 values except the last
+  size_t bytes = 0;
+  bytes += al(sizeof(SumPair) * (nb + 1));                     // prefix
+  bytes += al(sizeof(SumPair) * (scan_num_tiles(nb) + 1));     // scan tiles (pair)
+  bytes += al(sizeof(int32_t) * nb);                           // nb_next
+  bytes += al(sizeof(int32_t) * nr * kMaxJumpBlocks);          // exits
+  bytes += al(sizeof(int32_t) * nr);                           // entries
+  bytes += al(sizeof(int64_t) * (nb + 1)) * 2;                 // flags, idx
+  bytes += al(sizeof(int64_t) * (scan_num_tiles(nb) + 1));     // scan tiles (i64)
+  bytes += al(sizeof(int32_t) * mmax) * 4;                     // ps, pe, ps2, pe2
+  bytes += al(sizeof(double) * mmax) * 5;                      // pc, pc2, mc, cmc, cmc2
+  bytes += al(sizeof(uint8_t) * mmax) * 3;                     // prof, cached, cached2
+  bytes += al(sizeof(LineJob) * mmax);                         // jobs
+  bytes += al(sizeof(int64_t) * (mmax + 1)) * 2;               // nch, base
+  bytes += al(sizeof(long long) * mmax);                       // err
+  bytes += al(sizeof(int64_t) * 4);                            // device scalars
+  char* buf = nullptr;
+  if ((e = cudaMallocAsync((void**)&buf, bytes, s)) != cudaSuccess) return e;
+  char* sp = buf;
+  auto take = [&](size_t b) { char* r = sp; sp += al(b); return (void*)r; };
+  SumPair* pre = (SumPair*)take(sizeof(SumPair) * (nb + 1));
+  SumPair* ptiles = (SumPair*)take(sizeof(SumPair) * (scan_num_tiles(nb) + 1));
+  int32_t* nb_next = (int32_t*)take(sizeof(int32_t) * nb);
+  int32_t* exits = (int32_t*)take(sizeof(int32_t) * nr * kMaxJumpBlocks);
+  int32_t* entries = (int32_t*)take(sizeof(int32_t) * nr);
+  int64_t* flags = (int64_t*)take(sizeof(int64_t) * (nb + 1));
+  int64_t* idx = (int64_t*)take(sizeof(int64_t) * (nb + 1));
+  int64_t* itiles = (int64_t*)take(sizeof(int64_t) * (scan_num_tiles(nb) + 1));
+  int32_t* ps = (int32_t*)take(sizeof(int32_t) * mmax);
+  int32_t* pe = (int32_t*)take(sizeof(int32_t) * mmax);
+  int32_t* ps2 = (int32_t*)take(sizeof(int32_t) * mmax);
+  int32_t* pe2 = (int32_t*)take(sizeof(int32_t) * mmax);
+  double* pc = (double*)take(sizeof(double) * mmax);
+  double* pc2 = (double*)take(sizeof(double) * mmax);
+  double* mc = (double*)take(sizeof(double) * mmax);
+  double* cmc = (double*)take(sizeof(double) * mmax);
+  double* cmc2 = (double*)take(sizeof(double) * mmax);
+  uint8_t* prof = (uint8_t*)take(mmax);
+  uint8_t* cached = (uint8_t*)take(mmax);
+  uint8_t* cached2 = (uint8_t*)take(mmax);
+  LineJob* jobs = (LineJob*)take(sizeof(LineJob) * mmax);
+  int64_t* nch = (int64_t*)take(sizeof(int64_t) * (mmax + 1));
+  int64_t* base = (int64_t*)take(sizeof(int64_t) * (mmax + 1));
+  long long* perr = (long long*)take(sizeof(long long) * mmax);
+  int64_t* dsc = (int64_t*)take(sizeof(int64_t) * 4);  // [0] total chunks, [1] m, [2] any (int)
+  RangeSums rs{pre, n, nb};
+
+  auto fail = [&](cudaError_t ee) { cudaFreeAsync(buf, s); return ee; };
+  auto grid = [](int64_t x, int b) { return (unsigned)((x + b - 1) / b); };
+
+  block_sums_kernel<T><<<grid(nb * 32, 256), 256, 0, s>>>(v, n, nb, pre);
+  if ((e = exclusive_scan<SumPair>(pre, pre, nb, pre + nb, ptiles, s)) != cudaSuccess) return fail(e);
+  split_kernel<T><<<grid(nb, 8), 256, 0, s>>>(v, rs, nb_next);
+  chain_exit_kernel<<<grid(nr * kMaxJumpBlocks, 128), 128, 0, s>>>(nb_next, nb, nr, exits);
+  chain_link_kernel<<<1, 1, 0, s>>>(exits, nr, entries);
+  if ((e = cudaMemsetAsync(flags, 0, sizeof(int64_t) * (nb + 1), s)) != cudaSuccess) return fail(e);
+  chain_mark_kernel<<<grid(nr, 128), 128, 0, s>>>(nb_next, entries, nb, nr, flags);
+  if ((e = exclusive_scan<int64_t>(flags, idx, nb, dsc + 1, itiles, s)) != cudaSuccess) return fail(e);
+  chain_compact_kernel<<<grid(nb, 256), 256, 0, s>>>(flags, idx, nb_next, nb, n, ps, pe);
+  if ((e = cudaGetLastError()) != cudaSuccess) return fail(e);
+  if ((e = cudaMemcpyAsync(ctx->h_stats, dsc + 1, sizeof(int64_t), cudaMemcpyDeviceToHost, s)) != cudaSuccess) return fail(e);
+  if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return fail(e);
+  int64_t m = ctx->h_stats[0];
+  if (m <= 0 || m > mmax) {
+    if (err) *err = "partitioner produced an invalid split";
+    cudaFreeAsync(buf, s);
+    return cudaErrorUnknown;
+  }
+
+  // costs of the split partitions
+  auto run_jobs = [&](int64_t cnt, int pairs, const uint8_t* cache) -> cudaError_t {
+    job_setup_kernel<<<grid(cnt, 256), 256, 0, s>>>(ps, pe, m, pairs, cache, rs, jobs, nch, perr);
+    cudaError_t ee = exclusive_scan<int64_t>(nch, base, cnt, dsc, itiles, s);
+    if (ee != cudaSuccess) return ee;
+    // each value lies in at most two jobs, so the chunks number at most 2n/4096 + jobs
+    const int64_t cap = 2 * n / kPairChunk + cnt + 1;
+    job_err_kernel<T><<<(unsigned)cap, 256, 0, s>>>(v, jobs, base, cnt, dsc, perr);
+    return cudaGetLastError();
+  };
+  if ((e = run_jobs(m, 0, nullptr)) != cudaSuccess) return fail(e);
+  part_cost_kernel<<<grid(m, 256), 256, 0, s>>>(jobs, perr, m, pc);
+  if ((e = cudaMemsetAsync(cached, 0, mmax, s)) != cudaSuccess) return fail(e);
+
+  for (int round = 0; round < kMaxMergeRounds && m >= 2; round++) {
+    if ((e = run_jobs(m - 1, 1, cached)) != cudaSuccess) return fail(e);
+    if ((e = cudaMemsetAsync(dsc + 2, 0, sizeof(int64_t), s)) != cudaSuccess) return fail(e);
+    pair_score_kernel<<<grid(m - 1, 256), 256, 0, s>>>(jobs, perr, cached, cmc, pc, m, mc, prof, (int*)(dsc + 2));
+    merge_heads_kernel<<<grid(m, 256), 256, 0, s>>>(prof, m, round, flags);
+    if ((e = exclusive_scan<int64_t>(flags, idx, m, dsc + 1, itiles, s)) != cudaSuccess) return fail(e);
+    merge_scatter_kernel<<<grid(m, 256), 256, 0, s>>>(ps, pe, pc, mc, prof, flags, idx, m, round, ps2, pe2, pc2,
+                                                       cached2, cmc2);
+    if ((e = cudaGetLastError()) != cudaSuccess) return fail(e);
+    if ((e = cudaMemcpyAsync(ctx->h_stats, dsc + 1, 2 * sizeof(int64_t), cudaMemcpyDeviceToHost, s)) != cudaSuccess)
+      return fail(e);
+    if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return fail(e);
+    const int64_t m2 = ctx->h_stats[0];
+    const int any = (int)(ctx->h_stats[1] & 0xffffffff);
+    if (!any) break;  // nothing merged: the lists are unchanged
+    std::swap(ps, ps2);
+    std::swap(pe, pe2);
+    std::swap(pc, pc2);
+    std::swap(cached, cached2);
+    std::swap(cmc, cmc2);
+    m = m2;
+  }
+
+  int32_t* rs_out = nullptr;
+  int32_t* re_out = nullptr;
+  if ((e = cudaMallocAsync((void**)&rs_out, sizeof(int32_t) * m, s)) != cudaSuccess) return fail(e);
+  if ((e = cudaMallocAsync((void**)&re_out, sizeof(int32_t) * m, s)) != cudaSuccess) {
+    cudaFreeAsync(rs_out, s);
+    return fail(e);
+  }
+  cudaMemcpyAsync(rs_out, ps, sizeof(int32_t) * m, cudaMemcpyDeviceToDevice, s);
+  cudaMemcpyAsync(re_out, pe, sizeof(int32_t) * m, cudaMemcpyDeviceToDevice, s);
+  cudaFreeAsync(buf, s);
+  *out_s = rs_out;
+  *out_e = re_out;
+  *outP = m;
+  return cudaGetLastError();
+}
+
+cudaError_t launch_partition_variable(glc_ctx* ctx, glc_dtype dt, const void* values, int64_t n, int32_t** d_starts,
+                                      int32_t** d_ends, int64_t* P, cudaStream_t s, std::string* err) {
+  switch (dt) {
+    case GLC_I32: return partition_typed<int32_t>(ctx, (const int32_t*)values, n, d_starts, d_ends, P, s, err);
+    case GLC_I64: return partition_typed<int64_t>(ctx, (const int64_t*)values, n, d_starts, d_ends, P, s, err);
+    case GLC_U64: return partition_typed<uint64_t>(ctx, (const uint64_t*)values, n, d_starts, d_ends, P, s, err);
+    case GLC_U32: return partition_typed<uint32_t>(ctx, (const uint32_t*)values, n, d_starts, d_ends, P, s, err);
+  }
+  return cudaErrorInvalidValue;
+}
+
+}  // namespace glc

@@ -1,0 +1,190 @@
+// random_access.cu -- one lookup per thread slot, branch-free field extraction.
+//
+// Replaces decompressOptimizedKernel (decompression/RandomAccessKernels.cuh:55-169, binary search
+// over start/end for every query), randomAccessPreUnpackedKernel (:338-448),
+// randomAccessFixedPartitionKernel (decompression/FixedPartitionKernels.cuh:50-130) and
+// randomAccessFixedPreUnpackedKernel (:134-222).
+//
+// Per lookup: the position, one 32-byte partition descriptor (theta0, theta1, bit offset,
+// start, bits|type -- a single DRAM sector instead of the reference's four arrays), and the
+// two words that hold the field (or the 8-byte pre-unpacked residual).  Partition lookup is
+// pos / L for fixed partitions; for variable partitions a sample of every k-th start lives in
+// shared memory, a binary search there narrows the range to k partitions, and a short search
+// over the (L2-resident) start array finishes it.  Each thread carries four independent
+// lookups through the load stages so their DRAM latencies overlap.
+// Positions outside [0, n) yield 0, as the reference's variable-partition kernels do; the
+// fixed variants use the same rule here instead of reading past the metadata.
+#include "glc_internal.h"
+
+namespace glc {
+
+constexpr int kRAThreads = 256;
+constexpr int kRAQueries = 4;
+constexpr int kRASample = 4096;
+
+struct RAArgs {
+  const PartDesc* desc;
+  const int32_t* starts;
+  const uint32_t* words;
+  const int64_t* plain;
+  int64_t P, n;
+  const int32_t* pos;
+  int64_t q;
+  void* out;
+  int32_t fixed_len;
+  int32_t fixed_shift;   // >= 0 when fixed_len is a power of two
+  int32_t sample_stride;
+  int32_t nsample;
+};
+
+__device__ __forceinline__ uint64_t read_field_global(const uint32_t* __restrict__ w, int64_t pos, int bits) {
+  const int64_t wi = pos >> 5;
+  const int sh = (int)(pos & 31);
+  const uint64_t lo = (uint64_t)__ldg(w + wi) | ((uint64_t)__ldg(w + wi + 1) << 32);
+  uint64_t f = lo >> sh;
+  if (bits + sh > 64) f |= (uint64_t)__ldg(w + wi + 2) << (64 - sh);
+  return low_bits(f, bits);
+}
+
+__device__ __forceinline__ PartDesc load_desc(const PartDesc* __restrict__ d) {
+  const double2 a = __ldg(reinterpret_cast<const double2*>(d));
+  const longlong2 b = __ldg(reinterpret_cast<const longlong2*>(d) + 1);
+  PartDesc r;
+  r.theta0 = a.x;
+  r.theta1 = a.y;
+  r.bit_off = b.x;
+  r.start = (int32_t)(b.y & 0xffffffffll);
+  r.bits_type = (int32_t)(b.y >> 32);
+  return r;
+}
+
+// MODE 0: fixed, power-of-two length; 1: fixed, any length; 2: variable.
+template <typename T, bool PLAIN, int MODE>
+__global__ void __launch_bounds__(kRAThreads) random_access_kernel(RAArgs a) {
+  __shared__ int32_t s_sample[kRASample];
+  if (MODE == 2) {
+    for (int k = threadIdx.x; k < a.nsample; k += kRAThreads) s_sample[k] = a.starts[(int64_t)k * a.sample_stride];
+    __syncthreads();
+  }
+  T* out = reinterpret_cast<T*>(a.out);
+  const int64_t chunk = (int64_t)kRAThreads * kRAQueries;
+  for (int64_t base = (int64_t)blockIdx.x * chunk; base < a.q; base += (int64_t)gridDim.x * chunk) {
+    int64_t qi[kRAQueries], pos[kRAQueries], p[kRAQueries];
+    bool valid[kRAQueries];
+#pragma unroll
+    for (int k = 0; k < kRAQueries; k++) {
+      qi[k] = base + (int64_t)k * kRAThreads + threadIdx.x;
+      pos[k] = (qi[k] < a.q) ? (int64_t)__ldg(a.pos + qi[k]) : -1;
+      valid[k] = pos[k] >= 0 && pos[k] < a.n;
+      if (!valid[k]) pos[k] = 0;
+    }
+#pragma unroll
+    for (int k = 0; k < kRAQueries; k++) {
+      if (MODE == 0) {
+        p[k] = pos[k] >> a.fixed_shift;
+        p[k] = p[k] < a.P ? p[k] : a.P - 1;
+      } else if (MODE == 1) {
+        p[k] = pos[k] / a.fixed_len;
+        p[k] = p[k] < a.P ? p[k] : a.P - 1;
+      } else {
+        int lo = 0, hi = a.nsample - 1;
+        while (lo < hi) {
+          int mid = (lo + hi + 1) >> 1;
+          if ((int64_t)s_sample[mid] <= pos[k]) lo = mid; else hi = mid - 1;
+        }
+        int64_t plo = (int64_t)lo * a.sample_stride;
+        int64_t phi = plo + a.sample_stride - 1;
+        if (phi > a.P - 1) phi = a.P - 1;
+        while (plo < phi) {
+          int64_t mid = (plo + phi + 1) >> 1;
+          if ((int64_t)__ldg(a.starts + mid) <= pos[k]) plo = mid; else phi = mid - 1;
+        }
+        p[k] = plo;
+      }
+    }
+    PartDesc d[kRAQueries];
+#pragma unroll
+    for (int k = 0; k < kRAQueries; k++) d[k] = load_desc(a.desc + p[k]);
+    long long r[kRAQueries];
+#pragma unroll
+    for (int k = 0; k < kRAQueries; k++) {
+      const int64_t local = pos[k] - d[k].start;
+      const int bits = d[k].bits_type & 0xff;
+      const int type = d[k].bits_type >> 8;
+      if (PLAIN) {
+        r[k] = __ldg(a.plain + pos[k]);
+      } else {
+        const uint64_t f = bits > 0 ? read_field_global(a.words, d[k].bit_off + local * bits, bits) : 0ull;
+        r[k] = (type == MODEL_DIRECT_COPY) ? (long long)f : sign_extend(f, bits);
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < kRAQueries; k++) {
+      if (qi[k] >= a.q) continue;
+      const int type = d[k].bits_type >> 8;
+      T v;
+      if (type == MODEL_DIRECT_COPY) v = (T)r[k];
+      else v = apply_delta<T>(predict<T>(d[k].theta0, d[k].theta1, pos[k] - d[k].start), r[k]);
+      out[qi[k]] = valid[k] ? v : (T)0;
+    }
+  }
+}
+
+template <typename T, bool PLAIN>
+static cudaError_t ra_typed(glc_ctx* ctx, const RAArgs& a, int mode, cudaStream_t s) {
+  void (*k)(RAArgs) = mode == 0 ? random_access_kernel<T, PLAIN, 0>
+                    : mode == 1 ? random_access_kernel<T, PLAIN, 1>
+                                : random_access_kernel<T, PLAIN, 2>;
+  int per_sm = 0;
+  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kRAThreads, 0);
+  if (e != cudaSuccess) return e;
+  if (per_sm < 1) per_sm = 1;
+  const int64_t chunk = (int64_t)kRAThreads * kRAQueries;
+  int64_t grid = (a.q + chunk - 1) / chunk;
+  const int64_t cap = (int64_t)per_sm * ctx->num_sms;
+  if (grid > cap) grid = cap;
+  if (grid < 1) grid = 1;
+  k<<<(unsigned)grid, kRAThreads, 0, s>>>(a);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_random_access(glc_ctx* ctx, const glc_column* c, int plain_src, const int32_t* pos, int64_t q,
+                                 void* out, int32_t fixed_len, cudaStream_t s) {
+  if (q <= 0) return cudaSuccess;
+  RAArgs a;
+  a.desc = c->d_desc;
+  a.starts = c->d_start;
+  a.words = c->d_words;
+  a.plain = c->d_plain;
+  a.P = c->P;
+  a.n = c->n;
+  a.pos = pos;
+  a.q = q;
+  a.out = out;
+  a.fixed_len = fixed_len;
+  a.fixed_shift = -1;
+  int mode = 2;
+  if (c->P <= 0 || c->n <= 0) {
+    // empty column: every position is outside
+    return cudaMemsetAsync(out, 0, (size_t)q * dtype_size(c->dtype), s);
+  }
+  if (fixed_len > 0) {
+    mode = 1;
+    if ((fixed_len & (fixed_len - 1)) == 0) {
+      mode = 0;
+      a.fixed_shift = __builtin_ctz((unsigned)fixed_len);
+    }
+  }
+  a.sample_stride = (int32_t)((c->P + kRASample - 1) / kRASample);
+  if (a.sample_stride < 1) a.sample_stride = 1;
+  a.nsample = (int32_t)((c->P + a.sample_stride - 1) / a.sample_stride);
+  switch (c->dtype) {
+    case GLC_I32: return plain_src ? ra_typed<int32_t, true>(ctx, a, mode, s) : ra_typed<int32_t, false>(ctx, a, mode, s);
+    case GLC_I64: return plain_src ? ra_typed<int64_t, true>(ctx, a, mode, s) : ra_typed<int64_t, false>(ctx, a, mode, s);
+    case GLC_U64: return plain_src ? ra_typed<uint64_t, true>(ctx, a, mode, s) : ra_typed<uint64_t, false>(ctx, a, mode, s);
+    case GLC_U32: return plain_src ? ra_typed<uint32_t, true>(ctx, a, mode, s) : ra_typed<uint32_t, false>(ctx, a, mode, s);
+  }
+  return cudaErrorInvalidValue;
+}
+
+}  // namespace glc

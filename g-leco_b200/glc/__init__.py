@@ -1,0 +1,325 @@
+"""Python binding of libglc (include/glc.h) over ctypes.
+
+``LeCoGPU`` mirrors the reference's class (api/G-LeCo.cuh:39-2304): the same method names,
+argument meaning and error behaviour (a rejected blob gives ``None`` where the reference
+returns ``nullptr``; other failures raise ``GlcError``).  Every call goes through the C ABI to
+the CUDA kernels in libglc.so; there is no host fallback, and importing this module without
+the built library raises.
+
+Lower-level functions (``compress_device``, ``decompress_into`` ...) take raw device pointers
+and a CUDA stream handle so callers can keep data resident in HBM.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from typing import Optional
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libglc.so")
+
+I32, I64, U64, U32 = 0, 1, 2, 3
+FIXED, VARIABLE = 0, 1
+SRC_AUTO, SRC_PACKED, SRC_PREUNPACKED = 0, 1, 2
+HOST_IN, HOST_OUT = 1, 2
+OK, ERR_INVALID_ARG, ERR_BAD_BLOB, ERR_OOM, ERR_CUDA, ERR_TIMEOUT, ERR_BUDGET, ERR_UNSUPPORTED = range(8)
+
+NP_DTYPE = {I32: np.int32, I64: np.int64, U64: np.uint64, U32: np.uint32}
+DTYPE_OF = {np.dtype(np.int32): I32, np.dtype(np.int64): I64, np.dtype(np.uint64): U64, np.dtype(np.uint32): U32}
+TILE_SIZE = 4096  # the reference's default fixed partition length (core/CudaUtils.cuh:18)
+
+EXPORTS = [
+    "glc_create", "glc_destroy", "glc_last_error", "glc_status_string", "glc_sync", "glc_compress",
+    "glc_partition_variable", "glc_column_free", "glc_column_get_info", "glc_decompress_full",
+    "glc_decompress_range", "glc_random_access", "glc_preunpack", "glc_blob_size", "glc_serialize",
+    "glc_deserialize",
+]
+
+
+class GlcError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"glc status {status}: {msg}")
+        self.status = status
+
+
+class ColumnInfo(ctypes.Structure):
+    _fields_ = [
+        ("dtype", ctypes.c_int), ("total_values", ctypes.c_int64), ("num_partitions", ctypes.c_int64),
+        ("total_bits", ctypes.c_int64), ("compressed_size_bytes", ctypes.c_int64),
+        ("fixed_partition_len", ctypes.c_int32), ("has_packed", ctypes.c_int32), ("has_preunpacked", ctypes.c_int32),
+        ("d_start_indices", ctypes.c_void_p), ("d_end_indices", ctypes.c_void_p), ("d_model_types", ctypes.c_void_p),
+        ("d_model_params", ctypes.c_void_p), ("d_delta_bits", ctypes.c_void_p),
+        ("d_delta_array_bit_offsets", ctypes.c_void_p), ("d_error_bounds", ctypes.c_void_p),
+        ("delta_array", ctypes.c_void_p), ("d_plain_deltas", ctypes.c_void_p),
+    ]
+
+
+_lib = None
+
+
+def load() -> ctypes.CDLL:
+    """Load libglc.so; raises if it has not been built (there is no fallback)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"libglc.so is not built ({LIB_PATH}); run __graft_entry__.build()")
+    L = ctypes.CDLL(LIB_PATH)
+    vp, i64, i32, u64, c_int = ctypes.c_void_p, ctypes.c_int64, ctypes.c_int32, ctypes.c_uint64, ctypes.c_int
+    pvp, pi64, pu64 = ctypes.POINTER(vp), ctypes.POINTER(i64), ctypes.POINTER(u64)
+    sig = {
+        "glc_create": ([pvp, c_int], c_int),
+        "glc_destroy": ([vp], c_int),
+        "glc_last_error": ([vp], ctypes.c_char_p),
+        "glc_status_string": ([c_int], ctypes.c_char_p),
+        "glc_sync": ([vp, vp], c_int),
+        "glc_compress": ([vp, c_int, vp, i64, c_int, c_int, i32, pvp, pi64, vp], c_int),
+        "glc_partition_variable": ([vp, c_int, vp, i64, c_int, vp, vp, i64, pi64, vp], c_int),
+        "glc_column_free": ([vp], c_int),
+        "glc_column_get_info": ([vp, ctypes.POINTER(ColumnInfo)], c_int),
+        "glc_decompress_full": ([vp, vp, c_int, vp, c_int, vp], c_int),
+        "glc_decompress_range": ([vp, vp, c_int, i64, i64, vp, c_int, vp], c_int),
+        "glc_random_access": ([vp, vp, c_int, vp, i64, vp, c_int, i32, vp], c_int),
+        "glc_preunpack": ([vp, vp, c_int, vp], c_int),
+        "glc_blob_size": ([vp, pu64], c_int),
+        "glc_serialize": ([vp, vp, vp, u64, c_int, c_int, pu64, vp], c_int),
+        "glc_deserialize": ([vp, c_int, vp, u64, c_int, c_int, c_int, pvp, vp], c_int),
+    }
+    for name, (args, res) in sig.items():
+        f = getattr(L, name)
+        f.argtypes = args
+        f.restype = res
+    _lib = L
+    return L
+
+
+def _ptr(a: np.ndarray) -> ctypes.c_void_p:
+    return ctypes.c_void_p(a.ctypes.data)
+
+
+class Context:
+    """A glc context on one device (the reference's LeCoGPU constructor, api/G-LeCo.cuh:103)."""
+
+    def __init__(self, device: int = -1):
+        self.lib = load()
+        h = ctypes.c_void_p()
+        st = self.lib.glc_create(ctypes.byref(h), device)
+        if st != OK:
+            raise GlcError(st, "glc_create failed (no CUDA device?)")
+        self.handle = h
+
+    def check(self, st: int):
+        if st != OK:
+            raise GlcError(st, self.lib.glc_last_error(self.handle).decode())
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self.lib.glc_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def sync(self, stream: int = 0):
+        self.check(self.lib.glc_sync(self.handle, ctypes.c_void_p(stream)))
+
+
+class Column:
+    """An owned compressed column (CompressedData<T>, api/G-LeCo_Types.cuh:18-42)."""
+
+    def __init__(self, ctx: Context, handle: ctypes.c_void_p):
+        self.ctx = ctx
+        self.handle = handle
+
+    def info(self) -> ColumnInfo:
+        inf = ColumnInfo()
+        self.ctx.check(self.ctx.lib.glc_column_get_info(self.handle, ctypes.byref(inf)))
+        return inf
+
+    @property
+    def dtype(self) -> int:
+        return self.info().dtype
+
+    @property
+    def total_values(self) -> int:
+        return self.info().total_values
+
+    @property
+    def num_partitions(self) -> int:
+        return self.info().num_partitions
+
+    def free(self):
+        if self.handle:
+            self.ctx.lib.glc_column_free(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+# ---- device-pointer level ----------------------------------------------------------------
+def compress_device(ctx: Context, dtype: int, dptr: int, n: int, mode: int, fixed_len: int = TILE_SIZE,
+                    stream: int = 0, host: bool = False) -> Column:
+    h = ctypes.c_void_p()
+    size = ctypes.c_int64()
+    st = ctx.lib.glc_compress(ctx.handle, dtype, ctypes.c_void_p(dptr), n, HOST_IN if host else 0, mode, fixed_len,
+                              ctypes.byref(h), ctypes.byref(size), ctypes.c_void_p(stream))
+    ctx.check(st)
+    return Column(ctx, h)
+
+
+def decompress_into(ctx: Context, col: Column, out_ptr: int, source: int = SRC_AUTO, stream: int = 0,
+                    host_out: bool = False):
+    ctx.check(ctx.lib.glc_decompress_full(ctx.handle, col.handle, source, ctypes.c_void_p(out_ptr),
+                                          HOST_OUT if host_out else 0, ctypes.c_void_p(stream)))
+
+
+def decompress_range_into(ctx: Context, col: Column, first: int, count: int, out_ptr: int, source: int = SRC_AUTO,
+                          stream: int = 0, host_out: bool = False):
+    ctx.check(ctx.lib.glc_decompress_range(ctx.handle, col.handle, source, first, count, ctypes.c_void_p(out_ptr),
+                                           HOST_OUT if host_out else 0, ctypes.c_void_p(stream)))
+
+
+def random_access_into(ctx: Context, col: Column, pos_ptr: int, q: int, out_ptr: int, source: int = SRC_AUTO,
+                       fixed_len: int = 0, stream: int = 0, host_in: bool = False, host_out: bool = False):
+    flags = (HOST_IN if host_in else 0) | (HOST_OUT if host_out else 0)
+    ctx.check(ctx.lib.glc_random_access(ctx.handle, col.handle, source, ctypes.c_void_p(pos_ptr), q,
+                                        ctypes.c_void_p(out_ptr), flags, fixed_len, ctypes.c_void_p(stream)))
+
+
+def preunpack(ctx: Context, col: Column, drop_packed: bool = False, stream: int = 0):
+    ctx.check(ctx.lib.glc_preunpack(ctx.handle, col.handle, 1 if drop_packed else 0, ctypes.c_void_p(stream)))
+
+
+def partition_variable(ctx: Context, values: np.ndarray):
+    """Start/end arrays of the device partitioner for host values."""
+    values = np.ascontiguousarray(values)
+    cap = max(16, len(values) // 128 + 16)
+    s = np.zeros(cap, np.int32)
+    e = np.zeros(cap, np.int32)
+    P = ctypes.c_int64()
+    st = ctx.lib.glc_partition_variable(ctx.handle, DTYPE_OF[values.dtype], _ptr(values), len(values),
+                                        HOST_IN | HOST_OUT, _ptr(s), _ptr(e), cap, ctypes.byref(P), None)
+    ctx.check(st)
+    return s[:P.value].copy(), e[:P.value].copy()
+
+
+def serialize_host(ctx: Context, col: Column, crc32c: bool = False) -> bytes:
+    size = ctypes.c_uint64()
+    ctx.check(ctx.lib.glc_blob_size(col.handle, ctypes.byref(size)))
+    buf = np.zeros(size.value, np.uint8)
+    written = ctypes.c_uint64()
+    ctx.check(ctx.lib.glc_serialize(ctx.handle, col.handle, _ptr(buf), size.value, HOST_OUT, 1 if crc32c else 0,
+                                    ctypes.byref(written), None))
+    return buf.tobytes()
+
+
+def deserialize_host(ctx: Context, dtype: int, blob: bytes, pre_unpack: bool = False, crc32c: bool = False) -> Optional[Column]:
+    b = np.frombuffer(blob, np.uint8)
+    h = ctypes.c_void_p()
+    st = ctx.lib.glc_deserialize(ctx.handle, dtype, _ptr(b) if len(b) else None, len(b), HOST_IN, 1 if crc32c else 0,
+                                 1 if pre_unpack else 0, ctypes.byref(h), None)
+    if st == ERR_BAD_BLOB:
+        return None
+    ctx.check(st)
+    return Column(ctx, h)
+
+
+# ---- the reference's class API -------------------------------------------------------------
+class LeCoGPU:
+    """Drop-in mirror of ``template<typename T> class LeCoGPU`` (api/G-LeCo.cuh:39).
+
+    Host numpy arrays in and out, as the reference's std::vector arguments; every call runs the
+    CUDA kernels of libglc through the C ABI.
+    """
+
+    def __init__(self, dtype=np.int32, device: int = -1):
+        self.np_dtype = np.dtype(dtype)
+        self.code = DTYPE_OF[self.np_dtype]
+        self.ctx = Context(device)
+
+    # api/G-LeCo.cuh:349-614
+    def compress(self, values: np.ndarray, use_variable_partitioning: bool, use_gpu_partitioning: bool = False,
+                 dataset_name: str = "", fixed_partition_size: int = TILE_SIZE):
+        """Returns (column, compressed_size_bytes).  Both partitioning modes run on the GPU here;
+        ``use_gpu_partitioning`` is accepted for signature parity."""
+        v = np.ascontiguousarray(values, self.np_dtype)
+        h = ctypes.c_void_p()
+        size = ctypes.c_int64()
+        st = self.ctx.lib.glc_compress(self.ctx.handle, self.code, _ptr(v) if len(v) else None, len(v), HOST_IN,
+                                       VARIABLE if use_variable_partitioning else FIXED, fixed_partition_size,
+                                       ctypes.byref(h), ctypes.byref(size), None)
+        self.ctx.check(st)
+        return Column(self.ctx, h), size.value
+
+    def _full(self, col: Column, source: int) -> np.ndarray:
+        n = col.total_values
+        out = np.empty(n, self.np_dtype)
+        if n:
+            decompress_into(self.ctx, col, out.ctypes.data, source=source, host_out=True)
+        return out
+
+    # api/G-LeCo.cuh:680-693 and variants
+    def decompressFullFile(self, col: Column) -> np.ndarray:
+        return self._full(col, SRC_AUTO)
+
+    def decompressFullFile_BitPacked(self, col: Column) -> np.ndarray:
+        return self._full(col, SRC_PACKED)
+
+    def decompressFullFile_PreUnpacked(self, col: Column) -> np.ndarray:
+        return self._full(col, SRC_PREUNPACKED)
+
+    decompressFullFile_WorkStealing = decompressFullFile_BitPacked
+    decompressFullFile_WorkStealingAdvanced = decompressFullFile_BitPacked
+    decompressFullFile_OnTheFly_Optimized_V2 = decompressFullFile
+
+    def decompressFullFile_Fix(self, col: Column, partition_size: int) -> np.ndarray:
+        if col.info().fixed_partition_len != partition_size:
+            raise GlcError(ERR_INVALID_ARG, "column is not partitioned with that fixed length")
+        return self._full(col, SRC_AUTO)
+
+    def _ra(self, col: Column, positions, source: int, fixed: int) -> np.ndarray:
+        pos = np.ascontiguousarray(positions, np.int32)
+        out = np.empty(len(pos), self.np_dtype)
+        if len(pos):
+            random_access_into(self.ctx, col, pos.ctypes.data, len(pos), out.ctypes.data, source=source,
+                               fixed_len=fixed, host_in=True, host_out=True)
+        return out
+
+    # api/G-LeCo.cuh:615-678 (random access)
+    def decompress(self, col: Column, positions) -> np.ndarray:
+        return self._ra(col, positions, SRC_AUTO, 0)
+
+    def randomAccessPreUnpacked(self, col: Column, positions) -> np.ndarray:
+        return self._ra(col, positions, SRC_PREUNPACKED, 0)
+
+    def randomAccessFixed(self, col: Column, positions, fixed_partition_size: int) -> np.ndarray:
+        return self._ra(col, positions, SRC_PACKED, fixed_partition_size)
+
+    def randomAccessFixedPreUnpacked(self, col: Column, positions, fixed_partition_size: int) -> np.ndarray:
+        return self._ra(col, positions, SRC_PREUNPACKED, fixed_partition_size)
+
+    # api/G-LeCo.cuh:826, :1999
+    def serialize(self, col: Column, crc32c: bool = False) -> bytes:
+        return serialize_host(self.ctx, col, crc32c)
+
+    serializeGPU = serialize
+
+    # api/G-LeCo.cuh:1019, :2157 -- None where the reference returns nullptr
+    def deserialize(self, blob: bytes, crc32c: bool = False) -> Optional[Column]:
+        return deserialize_host(self.ctx, self.code, blob, False, crc32c)
+
+    def deserializeGPU(self, blob: bytes, preUnpackDeltas: bool = False, crc32c: bool = False) -> Optional[Column]:
+        return deserialize_host(self.ctx, self.code, blob, preUnpackDeltas, crc32c)
+
+    # api/G-LeCo.cuh:793-821
+    def cleanup(self, col: Column):
+        col.free()

@@ -1,0 +1,172 @@
+/* glc.h -- C ABI of the B200-native G-LeCo learned integer-column compression path.
+ *
+ * Every entry point replaces a method of the reference's header-only C++ class
+ * `template<typename T> class LeCoGPU` (api/G-LeCo.cuh:39-2304); the comment above each one
+ * names the reference method (file:line) whose behaviour it keeps.  Plain pointers, sizes and
+ * integer codes only: no C++ or framework types cross this boundary.
+ *
+ * Conventions
+ *  - Every call returns a glc_status; nothing exits the process (the reference's CUDA_CHECK
+ *    calls exit(), core/CudaUtils.cuh:5-13).  glc_last_error() gives a message.
+ *  - Device work is stream-ordered on the `stream` argument (a cudaStream_t; NULL = the
+ *    context's own stream).  Calls that read or write HOST buffers synchronise that stream
+ *    before returning, like the reference's methods; calls on device buffers do not.
+ *  - `flags` bit GLC_HOST_IN / GLC_HOST_OUT say that an input / output pointer is host memory
+ *    (pageable or pinned); otherwise it is device memory of the context's device.
+ *  - A column owns device memory in the reference's SoA layout (CompressedData<T>,
+ *    api/G-LeCo_Types.cuh:18-42) plus derived lookup tables.
+ */
+#ifndef GLC_H_
+#define GLC_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define GLC_API __attribute__((visibility("default")))
+#else
+#define GLC_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  GLC_OK = 0,
+  GLC_ERR_INVALID_ARG = 1, /* bad pointer, size, mode or dtype                       */
+  GLC_ERR_BAD_BLOB = 2,    /* blob rejected: magic, version, type size, checksum, size */
+  GLC_ERR_OOM = 3,         /* device or host allocation failed                        */
+  GLC_ERR_CUDA = 4,        /* a CUDA runtime call failed (message in glc_last_error)  */
+  GLC_ERR_TIMEOUT = 5,     /* a bounded device-side wait gave up                       */
+  GLC_ERR_BUDGET = 6,      /* admission refused: memory budget exceeded                */
+  GLC_ERR_UNSUPPORTED = 7  /* the column lacks what the call needs (e.g. no residuals) */
+} glc_status;
+
+/* Element types: int32 / int64 / uint64 / uint32 (the reference instantiates LeCoGPU for
+ * int, long long, unsigned long long and unsigned int, app/Main.cu:875-987). */
+typedef enum { GLC_I32 = 0, GLC_I64 = 1, GLC_U64 = 2, GLC_U32 = 3 } glc_dtype;
+
+/* Partitioning: fixed length (api/G-LeCo.cuh:401-416) or variable by model cost
+ * (api/G-LeCo.cuh:379-399, compression/CpuPartitioner.cuh). */
+typedef enum { GLC_PART_FIXED = 0, GLC_PART_VARIABLE = 1 } glc_partitioning;
+
+/* Residual source for decoding: the packed bitstream, or the pre-unpacked int64 residual per
+ * value (the reference's "high-throughput" mode, d_plain_deltas). AUTO picks pre-unpacked when
+ * present, like decompressFullFile (api/G-LeCo.cuh:680-693). */
+typedef enum { GLC_SRC_AUTO = 0, GLC_SRC_PACKED = 1, GLC_SRC_PREUNPACKED = 2 } glc_source;
+
+enum { GLC_HOST_IN = 1, GLC_HOST_OUT = 2 };
+
+typedef struct glc_ctx glc_ctx;
+typedef struct glc_column glc_column;
+typedef struct CUstream_st* glc_stream; /* == cudaStream_t */
+
+/* Read-only view of a column's device arrays (the CompressedData<T> fields). */
+typedef struct {
+  glc_dtype dtype;
+  int64_t total_values;           /* CompressedData::total_values                 */
+  int64_t num_partitions;         /* CompressedData::num_partitions               */
+  int64_t total_bits;             /* end of the last partition's bit range        */
+  int64_t compressed_size_bytes;  /* size compress() reports, api/G-LeCo.cuh:589-603 */
+  int32_t fixed_partition_len;    /* > 0 when every partition but the last has this length */
+  int32_t has_packed;             /* delta_array present                           */
+  int32_t has_preunpacked;        /* d_plain_deltas present                        */
+  const int32_t* d_start_indices;
+  const int32_t* d_end_indices;
+  const int32_t* d_model_types;
+  const double* d_model_params;   /* 4 per partition: theta0, theta1, 0, 0 */
+  const int32_t* d_delta_bits;
+  const int64_t* d_delta_array_bit_offsets;
+  const int64_t* d_error_bounds;
+  const uint32_t* delta_array;    /* ceil(total_bits/32) words (+ zero padding)   */
+  const int64_t* d_plain_deltas;  /* total_values residuals, or NULL               */
+} glc_column_info;
+
+/* ---- context ------------------------------------------------------------------------ */
+
+/* Replaces LeCoGPU() (api/G-LeCo.cuh:103-107): binds a device and creates the context's
+ * stream.  device < 0 means the current device. */
+GLC_API glc_status glc_create(glc_ctx** out, int device);
+/* Replaces ~LeCoGPU() (api/G-LeCo.cuh:109-113). */
+GLC_API glc_status glc_destroy(glc_ctx* ctx);
+GLC_API const char* glc_last_error(const glc_ctx* ctx);
+GLC_API const char* glc_status_string(glc_status s);
+/* Synchronise the stream and report device-side error flags (bounded waits that gave up). */
+GLC_API glc_status glc_sync(glc_ctx* ctx, glc_stream stream);
+
+/* ---- compression -------------------------------------------------------------------- */
+
+/* Replaces LeCoGPU::compress (api/G-LeCo.cuh:349-614).  `values` holds n elements of dtype
+ * (host memory when flags & GLC_HOST_IN).  GLC_PART_FIXED uses partitions of
+ * `fixed_partition_len` values (the reference's TILE_SIZE = 4096, core/CudaUtils.cuh:18);
+ * GLC_PART_VARIABLE runs the device split/merge partitioner (the reference runs
+ * VariableLengthPartitioner on the host, compression/CpuPartitioner.cuh:342-422).
+ * *compressed_size_bytes (may be NULL) receives the size the reference reports
+ * (64 B per partition + 120 B header + ceil(total_bits/8)). n == 0 gives an empty column. */
+GLC_API glc_status glc_compress(glc_ctx* ctx, glc_dtype dtype, const void* values, int64_t n, int flags,
+                        glc_partitioning mode, int32_t fixed_partition_len, glc_column** out,
+                        int64_t* compressed_size_bytes, glc_stream stream);
+
+/* Only the partitioner: start/end arrays of the variable partitioning (device or host
+ * buffers of capacity `cap`).  *num_partitions receives P; GLC_ERR_INVALID_ARG when cap < P.
+ * Replaces VariableLengthPartitioner<T>::partition (compression/CpuPartitioner.cuh:342). */
+GLC_API glc_status glc_partition_variable(glc_ctx* ctx, glc_dtype dtype, const void* values, int64_t n,
+                                  int flags, int32_t* starts, int32_t* ends, int64_t cap,
+                                  int64_t* num_partitions, glc_stream stream);
+
+/* Replaces LeCoGPU::cleanup (api/G-LeCo.cuh:793-821). */
+GLC_API glc_status glc_column_free(glc_column* col);
+GLC_API glc_status glc_column_get_info(const glc_column* col, glc_column_info* info);
+
+/* ---- decompression ------------------------------------------------------------------ */
+
+/* Full decode into `out` (total_values elements).  Replaces decompressFullFile
+ * (api/G-LeCo.cuh:680-693) and its variants _BitPacked (:1739), _PreUnpacked (:1790),
+ * _OnTheFly_Optimized_V2 (:1842), _WorkStealing (:166), _WorkStealingAdvanced (:220) and
+ * _Fix (:768): all are one persistent work-stealing kernel here, reading the residuals from
+ * `source`. */
+GLC_API glc_status glc_decompress_full(glc_ctx* ctx, const glc_column* col, glc_source source, void* out,
+                               int flags, glc_stream stream);
+
+/* Decode the values of the position range [first, first + count) (a range decode).  Same
+ * kernel as glc_decompress_full on a sub-range of tiles. */
+GLC_API glc_status glc_decompress_range(glc_ctx* ctx, const glc_column* col, glc_source source, int64_t first,
+                                int64_t count, void* out, int flags, glc_stream stream);
+
+/* Random access: out[k] = value at positions[k] (0 for positions outside the column).
+ * Replaces decompress (random access, api/G-LeCo.cuh:615-678), randomAccessPreUnpacked
+ * (:696-766), randomAccessFixed (:1878-1928) and randomAccessFixedPreUnpacked (:1931-1996).
+ * fixed_partition_len > 0 asserts fixed partitions of that length (O(1) partition lookup, as
+ * the reference's Fixed variants); 0 uses the column's own layout. */
+GLC_API glc_status glc_random_access(glc_ctx* ctx, const glc_column* col, glc_source source,
+                             const int32_t* positions, int64_t count, void* out, int flags,
+                             int32_t fixed_partition_len, glc_stream stream);
+
+/* Build the pre-unpacked int64 residual array (decompression/UnpackKernel.cuh:31-98, called
+ * by deserializeGPU(..., true), api/G-LeCo.cuh:2249-2288).  drop_packed != 0 frees the
+ * bitstream afterwards, as the reference does; such a column can no longer be serialized. */
+GLC_API glc_status glc_preunpack(glc_ctx* ctx, glc_column* col, int drop_packed, glc_stream stream);
+
+/* ---- serialization (blob version 5) --------------------------------------------------- */
+
+/* Exact byte size of the column's blob (api/G-LeCo.cuh:895-960). */
+GLC_API glc_status glc_blob_size(const glc_column* col, uint64_t* size);
+
+/* Replaces serialize / serializeGPU (api/G-LeCo.cuh:826-1016, :1999-2152): writes the blob
+ * into `blob` (capacity `cap`, host memory when flags & GLC_HOST_OUT).  The header checksum is
+ * the rotate-add sum the reference computes without SSE4.2 (api/G-LeCo.cuh:87-100);
+ * crc32c != 0 selects its CRC32C variant. */
+GLC_API glc_status glc_serialize(glc_ctx* ctx, const glc_column* col, void* blob, uint64_t cap, int flags,
+                         int crc32c, uint64_t* written, glc_stream stream);
+
+/* Replaces deserialize / deserializeGPU(blob, preUnpackDeltas) (api/G-LeCo.cuh:1019-1154,
+ * :2157-2302).  Accepts versions 4 and 5; rejects (GLC_ERR_BAD_BLOB) a wrong magic, version,
+ * type size or checksum, a short blob, or any array outside the blob. */
+GLC_API glc_status glc_deserialize(glc_ctx* ctx, glc_dtype dtype, const void* blob, uint64_t size, int flags,
+                           int crc32c, int pre_unpack, glc_column** out, glc_stream stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GLC_H_ */

@@ -1,0 +1,124 @@
+// ref_harness.cu -- drives the reference G-LeCo implementation, compiled from the reference's
+// own headers (include path -I<reference tree>), to pin the oracle.  TEST INFRASTRUCTURE ONLY.
+//
+// Modes (all file I/O is raw little-endian arrays):
+//   partition  <dtype> <values.bin> <out.bin>
+//        VariableLengthPartitioner<T>::partition() (compression/CpuPartitioner.cuh:342).
+//        out.bin = int64 P, then P x {int32 start, int32 end, int32 bits}.
+//   hostdecode <dtype> <blob.bin> <positions.bin> <out.bin> [repeat]
+//        LeCoGPU<T>::createDirectAccessHandle(blob, size, false) + directRandomAccessCPU
+//        (api/G-LeCo.cuh:1157, :1337): the reference's only host-side decoder.  Prints the
+//        seconds per pass (best of `repeat`) on stdout.
+//   golden     <dtype> <values.bin> <outprefix> <fixed|var>
+//        GPU only: LeCoGPU<T>::compress (api/G-LeCo.cuh:349, stock fixed TILE_SIZE=4096 path or
+//        stock CPU-partitioner path) followed by the CPU serialize (api/G-LeCo.cuh:826).  Writes
+//        <outprefix>.blob and prints the reported compressed size.  Only the reference's
+//        compression kernels run on the GPU; none of its decoders does.
+//
+// Without a CUDA device (this harness is also run in CPU-only containers) the CUDA stream
+// calls made by the LeCoGPU constructor/destructor are answered by ref_stubs.cpp when
+// GLC_REF_CPU_ONLY=1, because directRandomAccessCPU uses no device state.
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <chrono>
+#include <vector>
+#include <string>
+#include "api/G-LeCo.cuh"
+
+static std::vector<uint8_t> read_file(const char* path) {
+  std::vector<uint8_t> b;
+  FILE* f = fopen(path, "rb");
+  if (!f) { fprintf(stderr, "cannot open %s\n", path); exit(2); }
+  fseek(f, 0, SEEK_END); long n = ftell(f); fseek(f, 0, SEEK_SET);
+  b.resize((size_t)n);
+  if (n > 0 && fread(b.data(), 1, (size_t)n, f) != (size_t)n) { fprintf(stderr, "short read %s\n", path); exit(2); }
+  fclose(f);
+  return b;
+}
+
+static void write_file(const char* path, const void* p, size_t n) {
+  FILE* f = fopen(path, "wb");
+  if (!f) { fprintf(stderr, "cannot write %s\n", path); exit(2); }
+  if (n > 0) fwrite(p, 1, n, f);
+  fclose(f);
+}
+
+template <typename T> static std::vector<T> as_vec(const std::vector<uint8_t>& b) {
+  std::vector<T> v(b.size() / sizeof(T));
+  if (!v.empty()) memcpy(v.data(), b.data(), v.size() * sizeof(T));
+  return v;
+}
+
+template <typename T> static int run_partition(const char* in, const char* out) {
+  std::vector<T> v = as_vec<T>(read_file(in));
+  VariableLengthPartitioner<T> vp(v, SPLIT_THRESHOLD, MIN_PARTITION_SIZE, "");
+  std::vector<PartitionInfo> parts = vp.partition();
+  std::vector<uint8_t> o(8 + parts.size() * 12);
+  int64_t P = (int64_t)parts.size();
+  memcpy(o.data(), &P, 8);
+  for (size_t i = 0; i < parts.size(); i++) {
+    int32_t rec[3] = {parts[i].start_idx, parts[i].end_idx, parts[i].delta_bits};
+    memcpy(o.data() + 8 + 12 * i, rec, 12);
+  }
+  write_file(out, o.data(), o.size());
+  return 0;
+}
+
+template <typename T> static int run_hostdecode(const char* blobp, const char* posp, const char* out, int repeat) {
+  std::vector<uint8_t> blob = read_file(blobp);
+  std::vector<int> pos = as_vec<int>(read_file(posp));
+  LeCoGPU<T> codec;
+  DirectAccessHandle<T>* h = codec.createDirectAccessHandle(blob.data(), blob.size(), false);
+  if (!h) { fprintf(stderr, "createDirectAccessHandle rejected the blob\n"); return 3; }
+  std::vector<T> res;
+  double best = 1e30;
+  for (int r = 0; r < (repeat > 0 ? repeat : 1); r++) {
+    auto t0 = std::chrono::steady_clock::now();
+    codec.directRandomAccessCPU(h, pos, res, false);
+    auto t1 = std::chrono::steady_clock::now();
+    double s = std::chrono::duration<double>(t1 - t0).count();
+    if (s < best) best = s;
+  }
+  write_file(out, res.data(), res.size() * sizeof(T));
+  printf("%.9f\n", best);
+  h->~DirectAccessHandle<T>();
+  free(h);
+  return 0;
+}
+
+template <typename T> static int run_golden(const char* in, const char* prefix, bool var) {
+  std::vector<T> v = as_vec<T>(read_file(in));
+  LeCoGPU<T> codec;
+  long long size = 0;
+  CompressedData<T>* cd = codec.compress(v, var, &size, false, "");
+  if (!cd) { fprintf(stderr, "compress returned null\n"); return 3; }
+  SerializedData* sd = codec.serialize(cd);
+  if (!sd) { fprintf(stderr, "serialize returned null\n"); return 3; }
+  std::string bp = std::string(prefix) + ".blob";
+  write_file(bp.c_str(), sd->data, sd->size);
+  printf("%lld\n", size);
+  delete sd;
+  codec.cleanup(cd);
+  return 0;
+}
+
+template <typename T> static int dispatch(int argc, char** argv) {
+  std::string mode = argv[1];
+  if (mode == "partition" && argc >= 5) return run_partition<T>(argv[3], argv[4]);
+  if (mode == "hostdecode" && argc >= 6) return run_hostdecode<T>(argv[3], argv[4], argv[5], argc >= 7 ? atoi(argv[6]) : 1);
+  if (mode == "golden" && argc >= 6) return run_golden<T>(argv[3], argv[4], std::string(argv[5]) == "var");
+  fprintf(stderr, "bad arguments\n");
+  return 2;
+}
+
+int main(int argc, char** argv) {
+  if (argc < 3) { fprintf(stderr, "usage: ref_harness <mode> <i32|i64|u64|u32> ...\n"); return 2; }
+  std::string dt = argv[2];
+  if (dt == "i32") return dispatch<int>(argc, argv);
+  if (dt == "i64") return dispatch<long long>(argc, argv);
+  if (dt == "u64") return dispatch<unsigned long long>(argc, argv);
+  if (dt == "u32") return dispatch<unsigned int>(argc, argv);
+  fprintf(stderr, "unknown dtype %s\n", dt.c_str());
+  return 2;
+}

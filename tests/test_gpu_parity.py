@@ -1,0 +1,236 @@
+"""Parity of the CUDA path (through the C ABI) with the CPU oracle, bit for bit.
+
+Every compressed column made on the GPU is serialized and compared byte for byte with the
+oracle's blob for the same input: that covers partition boundaries, theta, bit widths, bit
+offsets, error bounds and every packed word.  Decoders are compared with the input (round trip)
+and with the oracle's decode of the same column.
+"""
+import numpy as np
+import pytest
+
+import glc
+from glc import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+
+def _data(kind: str, n: int, seed: int = 1):
+    rng = np.random.default_rng(seed)
+    i = np.arange(n, dtype=np.int64)
+    if kind == "i32_linear":
+        return (1000 * i + rng.integers(0, 256, n)).astype(np.int32)
+    if kind == "i32_neg":
+        return (-37 * i + rng.integers(-5000, 5000, n)).astype(np.int32)
+    if kind == "i64_walk":
+        return np.cumsum(rng.integers(-1000, 100000, n), dtype=np.int64)
+    if kind == "i64_extreme":
+        v = rng.integers(-(2 ** 62), 2 ** 62, n, dtype=np.int64)
+        v[:: 7] = np.iinfo(np.int64).max
+        v[3:: 11] = np.iinfo(np.int64).min
+        return v
+    if kind == "u64_piecewise":
+        return W.piecewise_linear(n, seed=seed, mean_segment=5000)
+    if kind == "u64_big":  # values above 2^53 in some partitions -> direct copy
+        v = (np.uint64(1) << np.uint64(40)) + i.astype(np.uint64) * np.uint64(3)
+        hi = (np.uint64(1) << np.uint64(60)) + rng.integers(0, 1 << 20, n).astype(np.uint64)
+        sel = (i // 3000) % 3 == 1
+        v[sel] = hi[sel]
+        return v
+    if kind == "u32_noise":
+        return (i * 50 + rng.integers(0, 1 << 12, n)).astype(np.uint32)
+    if kind == "u32_const":
+        return np.full(n, 123456789, np.uint32)
+    if kind == "timestamps":
+        return W.timestamps(n, seed=seed)
+    raise ValueError(kind)
+
+
+KINDS = ["i32_linear", "i32_neg", "i64_walk", "i64_extreme", "u64_piecewise", "u64_big", "u32_noise", "u32_const",
+         "timestamps"]
+
+
+def _codec(values):
+    return glc.LeCoGPU(values.dtype, device=0)
+
+
+def _check_column(codec, col, values, oracle_col, oracle):
+    blob = codec.serialize(col)
+    assert blob == oracle.serialize(oracle_col), "device column differs from the oracle's"
+    out = codec.decompressFullFile(col)
+    assert np.array_equal(out, values)
+    return blob
+
+
+@pytest.mark.parametrize("kind", KINDS)
+@pytest.mark.parametrize("n,L", [(100_003, 1024), (65_536, 4096), (5_000, 128), (777, 1000)])
+def test_fixed_compress_bit_exact(oracle, kind, n, L):
+    v = _data(kind, n)
+    codec = _codec(v)
+    col, size = codec.compress(v, False, fixed_partition_size=L)
+    ocol = oracle.compress(v, "fixed", L)
+    assert size == ocol.reported_size()
+    _check_column(codec, col, v, ocol, oracle)
+
+
+@pytest.mark.parametrize("kind", KINDS)
+@pytest.mark.parametrize("n", [1, 100, 128, 129, 4_000, 50_001, 300_000])
+def test_variable_compress_bit_exact(oracle, kind, n):
+    v = _data(kind, n, seed=n)
+    codec = _codec(v)
+    col, size = codec.compress(v, True)
+    s, e = oracle.partition_variable(v)
+    ocol = oracle.compress(v, starts=s, ends=e)
+    assert col.num_partitions == len(s)
+    assert size == ocol.reported_size()
+    _check_column(codec, col, v, ocol, oracle)
+
+
+def test_partitioner_matches_oracle_large(oracle, glc_ctx):
+    v = W.piecewise_linear(3_000_000, seed=5)
+    ds, de = glc.partition_variable(glc_ctx, v)
+    s, e = oracle.partition_variable(v)
+    assert np.array_equal(ds, s) and np.array_equal(de, e)
+
+
+@pytest.mark.parametrize("kind", ["i32_linear", "i64_walk", "u64_piecewise", "u32_noise", "u64_big"])
+def test_random_access(oracle, kind):
+    n = 200_000
+    v = _data(kind, n)
+    codec = _codec(v)
+    rng = np.random.default_rng(3)
+    pos = np.concatenate([rng.integers(0, n, 50_000), [0, n - 1, 1, n - 2, 4095, 4096, 4097]]).astype(np.int32)
+    for variable in (False, True):
+        col, _ = codec.compress(v, variable, fixed_partition_size=4096)
+        assert np.array_equal(codec.decompress(col, pos), v[pos])
+        if not variable:
+            assert np.array_equal(codec.randomAccessFixed(col, pos, 4096), v[pos])
+        glc.preunpack(codec.ctx, col)
+        assert np.array_equal(codec.randomAccessPreUnpacked(col, pos), v[pos])
+        assert np.array_equal(codec.decompressFullFile_PreUnpacked(col), v)
+        if not variable:
+            assert np.array_equal(codec.randomAccessFixedPreUnpacked(col, pos, 4096), v[pos])
+
+
+def test_random_access_outside_is_zero():
+    v = _data("i64_walk", 10_000)
+    codec = _codec(v)
+    col, _ = codec.compress(v, False, fixed_partition_size=1024)
+    pos = np.array([-1, 10_000, 2 ** 31 - 1, -(2 ** 31), 5], np.int32)
+    out = codec.decompress(col, pos)
+    assert list(out[:4]) == [0, 0, 0, 0] and out[4] == v[5]
+    out = codec.randomAccessFixed(col, pos, 1024)
+    assert list(out[:4]) == [0, 0, 0, 0] and out[4] == v[5]
+
+
+def test_fixed_length_mismatch_is_an_error():
+    v = _data("i32_linear", 10_000)
+    codec = _codec(v)
+    col, _ = codec.compress(v, False, fixed_partition_size=1024)
+    with pytest.raises(glc.GlcError):
+        codec.randomAccessFixed(col, np.arange(10, dtype=np.int32), 4096)
+
+
+@pytest.mark.parametrize("L", [1, 3, 7, 64])
+def test_tiny_partitions(oracle, L):
+    """More partitions per decode tile than the shared-memory descriptor cache holds."""
+    v = _data("i64_walk", 20_000)
+    codec = _codec(v)
+    col, _ = codec.compress(v, False, fixed_partition_size=L)
+    ocol = oracle.compress(v, "fixed", L)
+    _check_column(codec, col, v, ocol, oracle)
+    pos = np.random.default_rng(0).integers(0, len(v), 5000).astype(np.int32)
+    assert np.array_equal(codec.decompress(col, pos), v[pos])
+
+
+@pytest.mark.parametrize("kind", ["i32_linear", "u64_piecewise", "i64_extreme"])
+def test_range_decode(oracle, kind, glc_ctx):
+    n = 123_457
+    v = _data(kind, n)
+    codec = _codec(v)
+    col, _ = codec.compress(v, True)
+    rng = np.random.default_rng(9)
+    cases = [(0, n), (1, 1), (4095, 2), (4096, 4096), (n - 1, 1), (17, 40_000)]
+    cases += [(int(a), int(rng.integers(1, n - a))) for a in rng.integers(0, n - 1, 20)]
+    for first, count in cases:
+        out = np.empty(count, v.dtype)
+        glc.decompress_range_into(codec.ctx, col, first, count, out.ctypes.data, host_out=True)
+        assert np.array_equal(out, v[first:first + count]), (first, count)
+
+
+def test_empty_column():
+    codec = glc.LeCoGPU(np.int64, device=0)
+    col, size = codec.compress(np.zeros(0, np.int64), False)
+    assert size == 0 and col.total_values == 0
+    assert codec.decompressFullFile(col).shape == (0,)
+    assert codec.decompress(col, np.array([0, 1], np.int32)).tolist() == [0, 0]
+
+
+@pytest.mark.parametrize("dtype", [np.int32, np.int64, np.uint64, np.uint32])
+def test_prediction_ties(oracle, dtype):
+    """Predictions landing exactly on .5 round half away from zero in every decoder."""
+    n = 6000
+    i = np.arange(n)
+    rng = np.random.default_rng(2)
+    base = (i + 1) if np.dtype(dtype).kind == "u" else (i - 3000)
+    v = (base + rng.integers(-3, 4, n)).astype(dtype)
+    if np.dtype(dtype).kind == "u":
+        v = np.maximum(v.astype(np.int64), 0).astype(dtype)
+    starts, ends = np.array([0, 3000], np.int32), np.array([3000, n], np.int32)
+    # theta0 = 0.5 / -0.5 with theta1 = 1: every prediction is an exact .5 tie
+    ocol = oracle.column_with_lines(v, starts, ends, [(0.5, 1.0), (-0.5, 1.0)])
+    assert np.array_equal(oracle.decode_full(ocol), v)
+    codec = glc.LeCoGPU(dtype, device=0)
+    col = codec.deserialize(oracle.serialize(ocol))
+    assert col is not None
+    assert np.array_equal(codec.decompressFullFile(col), v)
+    pos = rng.integers(0, n, 3000).astype(np.int32)
+    assert np.array_equal(codec.decompress(col, pos), v[pos])
+    glc.preunpack(codec.ctx, col)
+    assert np.array_equal(codec.decompressFullFile_PreUnpacked(col), v)
+    assert np.array_equal(codec.randomAccessPreUnpacked(col, pos), v[pos])
+
+
+@pytest.mark.parametrize("kind", ["u64_piecewise", "i32_linear", "u64_big"])
+def test_serialize_roundtrip_and_oracle_blobs(oracle, kind):
+    v = _data(kind, 80_000)
+    codec = _codec(v)
+    ocol = oracle.compress(v, "fixed", 2048)
+    blob = oracle.serialize(ocol)
+    col = codec.deserialize(blob)
+    assert np.array_equal(codec.decompressFullFile(col), v)
+    assert codec.serialize(col) == blob
+    col2 = codec.deserializeGPU(blob, True)  # pre-unpacked, bitstream dropped
+    assert np.array_equal(codec.decompressFullFile(col2), v)
+    with pytest.raises(glc.GlcError):
+        codec.serialize(col2)  # api/G-LeCo.cuh:2005-2011
+    crc = oracle.serialize(ocol, crc32c=True)
+    assert codec.deserialize(crc) is None
+    assert np.array_equal(codec.decompressFullFile(codec.deserialize(crc, crc32c=True)), v)
+
+
+def test_bad_blobs_rejected(oracle):
+    v = _data("i32_linear", 10_000)
+    codec = _codec(v)
+    blob = bytearray(oracle.serialize(oracle.compress(v, "fixed", 1024)))
+    assert codec.deserialize(bytes(blob[:100])) is None                     # short
+    for off in (0, 4, 96, 112):                                             # magic, version, type size, reserved
+        b = bytearray(blob)
+        b[off] ^= 0x07
+        assert codec.deserialize(bytes(b)) is None
+    b = bytearray(blob)
+    b[20] ^= 1                                                               # header byte -> checksum
+    assert codec.deserialize(bytes(b)) is None
+    assert codec.deserialize(bytes(blob[:-16])) is None                     # truncated bitstream
+    assert glc.LeCoGPU(np.int64, device=0).deserialize(bytes(blob)) is None  # wrong element type
+
+
+@pytest.mark.parametrize("n", [2_000_000])
+def test_piecewise_scale_roundtrip(oracle, n):
+    """Size-independent properties on a larger piecewise-linear column."""
+    v = W.piecewise_linear(n, seed=11)
+    codec = _codec(v)
+    col, size = codec.compress(v, True)
+    assert np.array_equal(codec.decompressFullFile(col), v)
+    s, e = oracle.ref_partition_cpu(v)
+    ref_size = oracle.compress(v, starts=s, ends=e).reported_size()
+    assert size <= ref_size * 1.01, (size, ref_size)
