@@ -70,55 +70,63 @@ def profiled_traffic_per_value():
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons, sampled every 200 ms while running."""
+    """SM clock and clock-event (throttle) reasons sampled through NVML every 2 ms while the
+    timed region runs (reads only; no GPU setting is changed)."""
 
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASONS = {0x8: "hw_slowdown", 0x40: "hw_thermal_slowdown", 0x20: "sw_thermal_slowdown",
+               0x4: "sw_power_cap", 0x80: "hw_power_brake_slowdown"}
 
-    def __init__(self, device: int):
-        self.device = device
-        self.proc = None
-        self.lines = []
+    def __init__(self, torch_device):
+        self.dev = torch_device
+        self.samples, self.reasons, self.max_mhz = [], set(), None
+        self._stop = threading.Event()
+        self.handle = None
+
+    def _open(self):
+        import pynvml
+        pynvml.nvmlInit()
+        try:
+            import torch
+            uuid = str(torch.cuda.get_device_properties(self.dev).uuid)
+            return pynvml.nvmlDeviceGetHandleByUUID(("GPU-" + uuid) if not uuid.startswith("GPU-") else uuid)
+        except Exception:
+            vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+            idx = int(vis.split(",")[self.dev.index]) if vis and vis.split(",")[0].isdigit() else self.dev.index
+            return pynvml.nvmlDeviceGetHandleByIndex(idx)
 
     def start(self):
         try:
-            self.proc = subprocess.Popen(
-                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self.thread = threading.Thread(target=self._read, daemon=True)
+            import pynvml
+            self.handle = self._open()
+            self.max_mhz = float(pynvml.nvmlDeviceGetMaxClockInfo(self.handle, pynvml.NVML_CLOCK_SM))
+            self.thread = threading.Thread(target=self._loop, daemon=True)
             self.thread.start()
-        except Exception:
-            self.proc = None
+        except Exception as ex:  # reported in the JSON line
+            self.error = str(ex)
+            self.handle = None
 
-    def _read(self):
-        for line in self.proc.stdout:
-            self.lines.append(line.strip())
+    def _loop(self):
+        import pynvml
+        get_reasons = getattr(pynvml, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+            pynvml.nvmlDeviceGetCurrentClocksThrottleReasons
+        while not self._stop.is_set():
+            try:
+                self.samples.append(float(pynvml.nvmlDeviceGetClockInfo(self.handle, pynvml.NVML_CLOCK_SM)))
+                mask = int(get_reasons(self.handle))
+                for bit, name in self.REASONS.items():
+                    if mask & bit:
+                        self.reasons.add(name)
+            except Exception:
+                pass
+            time.sleep(0.002)
 
     def stop(self):
-        if self.proc is None:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
-        self.proc.terminate()
-        try:
-            self.proc.wait(timeout=5)
-        except Exception:
-            self.proc.kill()
-        sm, smax, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
-            parts = [p.strip() for p in ln.split(",")]
-            if len(parts) < 9:
-                continue
-            try:
-                sm.append(float(parts[1]))
-                smax = float(parts[2])
-            except ValueError:
-                continue
-            for name, val in zip(names, parts[5:9]):
-                if val.lower().startswith("active"):
-                    reasons.add(name)
-        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
-                "samples": len(sm)}
+        if self.handle is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "error": getattr(self, "error", "no NVML")}
+        self._stop.set()
+        self.thread.join(timeout=2)
+        return {"sm_mhz": float(np.median(self.samples)) if self.samples else None, "sm_max_mhz": self.max_mhz,
+                "reasons": sorted(self.reasons), "samples": len(self.samples), "source": "NVML, 2 ms"}
 
 
 def make_values(n: int, rank: int) -> np.ndarray:
@@ -155,20 +163,21 @@ def cpu_baseline_decode(values: np.ndarray, blob_maker, threads: int, budget_s: 
             wall = time.perf_counter() - t0
             secs = max(float(p.stdout.read().decode().strip().splitlines()[-1]) for p in procs)
             out = np.concatenate([np.fromfile(os.path.join(td, f"out{k}.bin"), np.uint64) for k in range(len(paths))])
-            ok = bool(np.array_equal(out, sample))
+            mism = int(np.count_nonzero(out != sample))
         else:
             col = oracle.deserialize(blob, "u64")
             t0 = time.perf_counter()
             out = oracle.decode_full(col)
             secs = time.perf_counter() - t0
             wall = secs
-            ok = bool(np.array_equal(out, sample))
+            mism = int(np.count_nonzero(out != sample))
             threads = 1
     gbs = sample_n * 8 / secs / 1e9
     return {"value": round(gbs, 4), "unit": UNIT, "cores": threads, "kind": kind,
             "sample": f"full decode of the first {sample_n:,} values of the workload (all positions, "
                       f"{'directRandomAccessCPU' if kind == 'reference' else 'oracle decode'}), "
-                      f"{threads} process(es); wall {wall:.2f} s; bit-exact={ok}"}
+                      f"{threads} process(es); wall {wall:.2f} s; values differing from the input: {mism} "
+                      f"(the reference's host decoder predicts without fma)"}
 
 
 def run_reference_arm(args):
@@ -204,7 +213,7 @@ def run_reference_arm(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="glc", choices=["glc", "reference"])
     ap.add_argument("--n", type=int, default=DEFAULT_N)
@@ -229,7 +238,8 @@ def main():
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
     dev = torch.device("cuda", local)
-    stream = torch.cuda.current_stream(dev)
+    stream = torch.cuda.Stream(dev)  # every launch and both events on this stream
+    torch.cuda.set_stream(stream)
     sh = stream.cuda_stream
     ctx = glc.Context(local)
 
@@ -253,7 +263,7 @@ def main():
     torch.cuda.synchronize(dev)
     ok = bool(np.array_equal(out.cpu().numpy().view(np.uint64), values))
 
-    clocks = ClockSampler(local)
+    clocks = ClockSampler(dev)
     clocks.start()
     if world > 1:
         dist.barrier()

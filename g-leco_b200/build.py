@@ -49,7 +49,26 @@ def build(verbose_ptxas: bool = False) -> str:
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{r.stderr}")
+    build_dropin()
     return OUT
+
+
+def build_dropin() -> str:
+    """Compile the C++ caller of the drop-in LeCoGPU<T> header (tests/cpp/leco_dropin.cpp)."""
+    src = os.path.join(ROOT, "tests", "cpp", "leco_dropin.cpp")
+    exe = os.path.join(BUILD, "leco_dropin")
+    hdrs = [os.path.join(ROOT, "include", h) for h in ("glc.h", "glc_leco.hpp")]
+    if os.path.exists(exe) and all(os.path.getmtime(exe) >= os.path.getmtime(d) for d in [src, OUT] + hdrs):
+        return exe
+    cuda_inc = os.path.join(os.path.dirname(os.path.dirname(os.path.realpath(
+        subprocess.run(["which", NVCC], capture_output=True, text=True).stdout.strip() or "/usr/local/cuda/bin/nvcc"))),
+        "include")
+    cmd = [os.environ.get("CXX", "g++"), "-std=c++17", "-O2", "-I" + os.path.join(ROOT, "include"), "-I" + cuda_inc,
+           src, "-L" + os.path.dirname(OUT), "-lglc", "-Wl,-rpath,$ORIGIN/../glc", "-o", exe]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"drop-in caller failed to compile:\n{r.stderr}")
+    return exe
 
 
 if __name__ == "__main__":

@@ -115,6 +115,19 @@ void set_word_counts(glc_column* c) {
   c->nwords_alloc = ((c->nwords + 3) & ~3ll) + 8;  // decoders read up to 3 words past a field
 }
 
+// A private pool that keeps freed memory (release threshold = max), so per-call temporaries
+// (host-output staging, scratch) cost no fresh device allocation after the first call.
+cudaError_t create_pool(glc_ctx* ctx) {
+  cudaMemPoolProps props = {};
+  props.allocType = cudaMemAllocationTypePinned;
+  props.location.type = cudaMemLocationTypeDevice;
+  props.location.id = ctx->device;
+  cudaError_t e = cudaMemPoolCreate(&ctx->pool, &props);
+  if (e != cudaSuccess) return e;
+  uint64_t keep = ~0ull;
+  return cudaMemPoolSetAttribute(ctx->pool, cudaMemPoolAttrReleaseThreshold, &keep);
+}
+
 int64_t reported_size(int64_t P, int64_t total_bits) {  // api/G-LeCo.cuh:589-603
   return 64 * P + 120 + (total_bits + 7) / 8;
 }
@@ -152,6 +165,7 @@ glc_status glc_create(glc_ctx** out, int device) {
   ctx->device = device;
   if ((e = cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, device)) != cudaSuccess ||
       (e = cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking)) != cudaSuccess ||
+      (e = create_pool(ctx)) != cudaSuccess ||
       (e = cudaMalloc(&ctx->d_flags, sizeof(int) * kFlagWords)) != cudaSuccess ||
       (e = cudaMemset(ctx->d_flags, 0, sizeof(int) * kFlagWords)) != cudaSuccess ||
       (e = cudaMalloc(&ctx->d_stats, sizeof(int64_t) * 16)) != cudaSuccess ||
@@ -171,6 +185,10 @@ glc_status glc_destroy(glc_ctx* ctx) {
   if (ctx->d_stats) cudaFree(ctx->d_stats);
   if (ctx->h_stats) cudaFreeHost(ctx->h_stats);
   if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
+  if (ctx->pool) {
+    cudaDeviceSynchronize();
+    cudaMemPoolDestroy(ctx->pool);
+  }
   delete ctx;
   return GLC_OK;
 }
@@ -251,7 +269,7 @@ static glc_status compress_impl(glc_ctx* ctx, glc_dtype dtype, const void* dev_v
   }
   const size_t sb = fit_scratch_bytes(nullptr, n, c->P);
   void* scratch = nullptr;
-  CK(cudaMallocAsync(&scratch, sb, s), "compress: scratch allocation");
+  CK(pool_alloc(ctx, &scratch, sb, s), "compress: scratch allocation");
   cudaError_t e = launch_fit(dtype, dev_values, c, scratch, sb, ctx->d_stats, s);
   if (e == cudaSuccess) e = cudaMemcpyAsync(ctx->h_stats, ctx->d_stats, 2 * sizeof(int64_t), cudaMemcpyDeviceToHost, s);
   cudaFreeAsync(scratch, s);
@@ -297,7 +315,7 @@ glc_status glc_compress(glc_ctx* ctx, glc_dtype dtype, const void* values, int64
   void* staged = nullptr;
   if (flags & GLC_HOST_IN) {
     const size_t bytes = (size_t)n * dtype_size(dtype);
-    cudaError_t e = cudaMallocAsync(&staged, bytes, s);
+    cudaError_t e = pool_alloc(ctx, &staged, bytes, s);
     if (e == cudaSuccess) e = cudaMemcpyAsync(staged, values, bytes, cudaMemcpyHostToDevice, s);
     if (e != cudaSuccess) {
       if (staged) cudaFreeAsync(staged, s);
@@ -332,7 +350,7 @@ glc_status glc_partition_variable(glc_ctx* ctx, glc_dtype dtype, const void* val
   void* staged = nullptr;
   if (flags & GLC_HOST_IN) {
     const size_t bytes = (size_t)n * dtype_size(dtype);
-    CK(cudaMallocAsync(&staged, bytes, s), "partition: upload");
+    CK(pool_alloc(ctx, &staged, bytes, s), "partition: upload");
     CK(cudaMemcpyAsync(staged, values, bytes, cudaMemcpyHostToDevice, s), "partition: upload");
     dev_values = staged;
   }
@@ -389,7 +407,7 @@ glc_status glc_decompress_range(glc_ctx* ctx, const glc_column* col, glc_source 
   cudaStream_t s = pick(ctx, stream);
   const size_t es = dtype_size(col->dtype);
   void* dev_out = out;
-  if (flags & GLC_HOST_OUT) CK(cudaMallocAsync(&dev_out, count * es, s), "decode: output allocation");
+  if (flags & GLC_HOST_OUT) CK(pool_alloc(ctx, &dev_out, count * es, s), "decode: output allocation");
   char* base = (char*)dev_out - first * (int64_t)es;
   cudaError_t e = launch_decode(ctx, col, plain, 0, first, first + count, base, s);
   if (e == cudaSuccess && (flags & GLC_HOST_OUT)) e = cudaMemcpyAsync(out, dev_out, count * es, cudaMemcpyDeviceToHost, s);
@@ -424,11 +442,11 @@ glc_status glc_random_access(glc_ctx* ctx, const glc_column* col, glc_source sou
   void* dout = out;
   void* tpos = nullptr;
   if (flags & GLC_HOST_IN) {
-    CK(cudaMallocAsync(&tpos, 4 * count, s), "random access: positions");
+    CK(pool_alloc(ctx, &tpos, 4 * count, s), "random access: positions");
     CK(cudaMemcpyAsync(tpos, positions, 4 * count, cudaMemcpyHostToDevice, s), "random access: positions");
     dpos = (const int32_t*)tpos;
   }
-  if (flags & GLC_HOST_OUT) CK(cudaMallocAsync(&dout, es * count, s), "random access: output");
+  if (flags & GLC_HOST_OUT) CK(pool_alloc(ctx, &dout, es * count, s), "random access: output");
   const int32_t fl = fixed_partition_len > 0 ? fixed_partition_len : col->fixed_len;
   cudaError_t e = launch_random_access(ctx, col, plain, dpos, count, dout, fl, s);
   if (e == cudaSuccess && (flags & GLC_HOST_OUT)) e = cudaMemcpyAsync(out, dout, es * count, cudaMemcpyDeviceToHost, s);

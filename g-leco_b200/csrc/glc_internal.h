@@ -42,6 +42,7 @@ struct glc_ctx {
   int device = 0;
   int num_sms = 0;
   cudaStream_t own_stream = nullptr;
+  cudaMemPool_t pool = nullptr;  // private stream-ordered pool; keeps freed memory for reuse
   int* d_flags = nullptr;      // [0, 64) decode work counters, [64] device error code
   int64_t* d_stats = nullptr;  // small readback area (total bits, max bits, ...)
   int64_t* h_stats = nullptr;  // pinned mirror of d_stats
@@ -79,6 +80,11 @@ struct glc_column {
 namespace glc {
 
 inline int dtype_size(glc_dtype d) { return (d == GLC_I64 || d == GLC_U64) ? 8 : 4; }
+
+// Stream-ordered temporary allocation from the context's pool.
+template <typename P> inline cudaError_t pool_alloc(glc_ctx* ctx, P** p, size_t bytes, cudaStream_t s) {
+  return cudaMallocFromPoolAsync((void**)p, bytes, ctx->pool, s);
+}
 
 // ---- kernel launchers (defined in the .cu files) -------------------------------------
 // fit.cu

@@ -338,7 +338,7 @@ static cudaError_t partition_typed(glc_ctx* ctx, const T* v, int64_t n, int32_t*
   bytes += al(sizeof(long long) * mmax);                       // err
   bytes += al(sizeof(int64_t) * 4);                            // device scalars
   char* buf = nullptr;
-  if ((e = cudaMallocAsync((void**)&buf, bytes, s)) != cudaSuccess) return e;
+  if ((e = pool_alloc(ctx, &buf, bytes, s)) != cudaSuccess) return e;
   char* sp = buf;
   auto take = [&](size_t b) { char* r = sp; sp += al(b); return (void*)r; };
   SumPair* pre = (SumPair*)take(sizeof(SumPair) * (nb + 1));
@@ -429,8 +429,8 @@ static cudaError_t partition_typed(glc_ctx* ctx, const T* v, int64_t n, int32_t*
 
   int32_t* rs_out = nullptr;
   int32_t* re_out = nullptr;
-  if ((e = cudaMallocAsync((void**)&rs_out, sizeof(int32_t) * m, s)) != cudaSuccess) return fail(e);
-  if ((e = cudaMallocAsync((void**)&re_out, sizeof(int32_t) * m, s)) != cudaSuccess) {
+  if ((e = pool_alloc(ctx, &rs_out, sizeof(int32_t) * m, s)) != cudaSuccess) return fail(e);
+  if ((e = pool_alloc(ctx, &re_out, sizeof(int32_t) * m, s)) != cudaSuccess) {
     cudaFreeAsync(rs_out, s);
     return fail(e);
   }

@@ -234,3 +234,16 @@ def test_piecewise_scale_roundtrip(oracle, n):
     s, e = oracle.ref_partition_cpu(v)
     ref_size = oracle.compress(v, starts=s, ends=e).reported_size()
     assert size <= ref_size * 1.01, (size, ref_size)
+
+
+def test_cpp_dropin_caller():
+    """A C++ caller written against the reference's LeCoGPU<T> API runs on include/glc_leco.hpp."""
+    import os
+    import subprocess
+    exe = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "g-leco_b200", "_build",
+                       "leco_dropin")
+    if not os.path.exists(exe):
+        pytest.fail("drop-in caller not built (run __graft_entry__.build())")
+    r = subprocess.run([exe], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert r.stdout.count(": ok") == 4, r.stdout
