@@ -406,12 +406,22 @@ glc_status glc_decompress_range(glc_ctx* ctx, const glc_column* col, glc_source 
   cudaSetDevice(ctx->device);
   cudaStream_t s = pick(ctx, stream);
   const size_t es = dtype_size(col->dtype);
-  void* dev_out = out;
-  if (flags & GLC_HOST_OUT) CK(pool_alloc(ctx, &dev_out, count * es, s), "decode: output allocation");
-  char* base = (char*)dev_out - first * (int64_t)es;
+  // The kernel writes value e at base + e with 16-byte stores, so base must be 16-byte aligned.
+  // Host outputs and misaligned device outputs go through an aligned temporary.
+  const size_t shift = (size_t)(first * (int64_t)es) & 15;
+  const bool staged = (flags & GLC_HOST_OUT) || (((uintptr_t)out - shift) & 15) != 0;
+  void* tmp = nullptr;
+  char* dev_out = (char*)out;
+  if (staged) {
+    CK(pool_alloc(ctx, &tmp, count * es + 16, s), "decode: output allocation");
+    dev_out = (char*)tmp + shift;
+  }
+  char* base = dev_out - first * (int64_t)es;
   cudaError_t e = launch_decode(ctx, col, plain, 0, first, first + count, base, s);
-  if (e == cudaSuccess && (flags & GLC_HOST_OUT)) e = cudaMemcpyAsync(out, dev_out, count * es, cudaMemcpyDeviceToHost, s);
-  if (flags & GLC_HOST_OUT) cudaFreeAsync(dev_out, s);
+  if (e == cudaSuccess && staged)
+    e = cudaMemcpyAsync(out, dev_out, count * es,
+                        (flags & GLC_HOST_OUT) ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice, s);
+  if (tmp) cudaFreeAsync(tmp, s);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "decode");
   if (flags & GLC_HOST_OUT) return glc_sync(ctx, stream);
   return GLC_OK;

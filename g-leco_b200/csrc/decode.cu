@@ -1,4 +1,4 @@
-// decode.cu -- persistent work-stealing full / range decode with TMA-staged input.
+// decode.cu -- persistent work-stealing full / range decode with a TMA producer warp.
 //
 // Replaces the reference's full-decode kernels, which all do the same arithmetic with
 // different work layouts: decompressFullFile_BitPacked / _PreUnpacked (grid-stride, a binary
@@ -8,23 +8,36 @@
 // pre-unpack kernel (decompression/UnpackKernel.cuh:31-98) is the same walk with a residual
 // epilogue, so it is a mode of this kernel too.
 //
-// Work unit: a TILE of 4096 consecutive output values (independent of partition sizes, so
-// every unit writes the same number of bytes).  A table built once per column holds each
-// tile's first bit and first/last partition, so no per-value search is needed.
-// Per CTA (persistent, grid = resident CTAs on all SMs):
-//   thread 0 claims tiles from a global counter one ahead of the CTA, and for each claimed
-//   tile issues a 1-D TMA bulk copy (cp.async.bulk, non-multicast) of the tile's packed words
-//   (or its pre-unpacked residuals) into one of two shared-memory stages, completing on that
-//   stage's mbarrier; while that copy flies, the CTA decodes the previous tile from the other
-//   stage: each thread walks its values with a partition cursor over the tile's descriptors
-//   (cached in shared memory), extracts the field from shared memory, recomputes the FP64
-//   prediction exactly as the reference does and writes 16-byte vector stores.
-// Every mbarrier wait is bounded by wall time; on expiry the kernel records an error code,
-// waits (bounded) for its own copies in flight and returns.
+// Work unit: a TILE of 4096 consecutive output values, independent of partition sizes, so every
+// unit writes the same number of bytes.  A table built once per column gives each tile's first
+// bit and first/last partition; no per-value search is needed.
+//
+// CTA = 1 producer warp + 8 consumer warps, persistent (grid = resident CTAs on all SMs):
+//   producer (one lane): claims the next tile from a global counter (work stealing), waits until
+//     the consumers released the ring stage, then issues 1-D TMA bulk copies (cp.async.bulk,
+//     non-multicast) of the tile's packed words (or pre-unpacked residuals) AND of the tile's
+//     32-byte partition descriptors into that stage, completing on the stage's "full" mbarrier.
+//     Three stages keep up to three tiles in flight per CTA.
+//   consumers: wait on "full", decode the tile from shared memory and write 16-byte vector
+//     stores, then arrive on the stage's "empty" mbarrier.  The common case (a vector whose
+//     values all lie in one partition, fields <= 32 bits) uses 32-bit bit arithmetic relative to
+//     the stage, one funnel shift per field, a two-shift sign extension and the FP64 prediction
+//     fma(theta1, i, theta0) -> round -> saturating convert, exactly as the reference computes it.
+// No CTA-wide barrier runs inside the loop.  A tile whose packed words exceed a stage is decoded
+// straight from global memory (rare: fields averaging more than 32 bits over a tile).
+// Every mbarrier wait is bounded by wall time; on expiry the kernel records an error code and
+// returns after a second bounded wait for its own copies.
+#include <climits>
 #include <type_traits>
 #include "glc_internal.h"
 
 namespace glc {
+
+constexpr int kStages = 3;
+constexpr int kConsumerWarps = 8;
+constexpr int kConsumers = kConsumerWarps * 32;
+constexpr int kPCThreads = kConsumers + 32;
+constexpr int kStageCapWords = 4096 + 16;  // 32 bits per value on average over a tile
 
 struct DecodeArgs {
   const PartDesc* desc;
@@ -41,10 +54,22 @@ struct DecodeArgs {
   int stage_bytes;
 };
 
+struct StageInfo {
+  int64_t tile;
+  int64_t bit_lo;
+  int32_t pf, pl;
+  int32_t big;     // words read from global memory instead of the stage
+  int32_t cached;  // descriptors are in the stage
+};
+
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
 __device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
 
 __device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
@@ -74,7 +99,7 @@ __device__ __forceinline__ uint64_t global_ns() {
   return t;
 }
 
-// Wait for `parity` on `bar`, giving up after ~2 s of wall time.
+// Wait for the phase of parity `parity` on `bar`, giving up after ~2 s of wall time.
 __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity) {
   if (mbar_try_wait(bar, parity)) return true;
   const uint64_t t0 = global_ns();
@@ -85,177 +110,230 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity
   return false;
 }
 
-template <bool PLAIN> __device__ __forceinline__ void issue_tile(const DecodeArgs& a, int64_t t, void* stage, uint64_t* bar) {
-  const void* src;
-  uint32_t bytes;
-  if (PLAIN) {
-    const int64_t e0 = t * kDecodeTile;
-    const int64_t e1 = (e0 + kDecodeTile < a.n) ? e0 + kDecodeTile : a.n;
-    src = a.plain + e0;
-    bytes = (uint32_t)((((e1 - e0) * 8) + 15) & ~15ll);
-  } else {
-    const int64_t bl = a.tiles[t].bit_lo, bh = a.tiles[t + 1].bit_lo;
-    const int64_t w0 = (bl >> 5) & ~3ll;
-    const int64_t w1 = (((bh >> 5) + 3) + 3) & ~3ll;
-    src = a.words + w0;
-    bytes = (uint32_t)((w1 - w0) * 4);
-  }
-  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-  mbar_arrive_expect_tx(bar, bytes);
-  tma_bulk_load(stage, src, bytes, bar);
+__device__ __forceinline__ PartDesc load_desc_g(const PartDesc* d) {
+  const double2 x = __ldg(reinterpret_cast<const double2*>(d));
+  const longlong2 y = __ldg(reinterpret_cast<const longlong2*>(d) + 1);
+  PartDesc r;
+  r.theta0 = x.x;
+  r.theta1 = x.y;
+  r.bit_off = y.x;
+  r.start = (int32_t)(y.y & 0xffffffffll);
+  r.bits_type = (int32_t)(y.y >> 32);
+  return r;
 }
 
+// Field of 0..64 bits at 32-bit bit position `pos` of a word array (shared or global).
+__device__ __forceinline__ uint64_t field_at(const uint32_t* w, uint32_t pos, int bits) {
+  const uint32_t wi = pos >> 5, sh = pos & 31;
+  uint64_t f = (((uint64_t)w[wi + 1] << 32) | w[wi]) >> sh;
+  if (bits + (int)sh > 64) f |= (uint64_t)w[wi + 2] << (64 - sh);
+  return bits >= 64 ? f : (f & ((1ull << bits) - 1ull));
+}
+
+template <typename T> __device__ __forceinline__ T predict_x(double t0, double t1, double x) {
+  return sat_cast<T>(round(__fma_rn(t1, x, t0)));
+}
+
+// Partition cursor of one consumer thread inside a tile.
 struct Cursor {
   double t0, t1;
-  int64_t bit_rel;  // descriptor bit offset minus the stage's first bit
-  int64_t start;
-  int64_t next_start;
-  int bits, type;
-  int idx;
+  uint32_t base;  // bit of value e (relative to the stage) = base + e * bits  (mod 2^32)
+  int start, next, bits, type, idx;
 };
 
-__device__ __forceinline__ void cursor_load(Cursor& c, const PartDesc& d, int64_t next_start, int64_t stage_bit0) {
-  c.t0 = d.theta0;
-  c.t1 = d.theta1;
-  c.bit_rel = d.bit_off - stage_bit0;
-  c.start = d.start;
-  c.bits = d.bits_type & 0xff;
-  c.type = d.bits_type >> 8;
-  c.next_start = next_start;
-}
-
-template <typename T, bool PLAIN, bool RESID, bool VEC>
-__global__ void __launch_bounds__(kDecodeThreads) decode_kernel(DecodeArgs a) {
+template <typename T, bool PLAIN, bool RESID>
+__device__ __forceinline__ void decode_tile(const DecodeArgs& a, const StageInfo& si, const uint8_t* stage,
+                                            const PartDesc* sdesc) {
   typedef typename std::conditional<RESID, int64_t, T>::type OutT;
   constexpr int V = 16 / (int)sizeof(OutT);
-  extern __shared__ __align__(128) uint8_t smem[];
-  __shared__ __align__(8) uint64_t bars[2];
-  __shared__ int64_t s_tile[2];
-  __shared__ PartDesc s_desc[kDescCache];
-
-  uint8_t* stage_ptr[2] = {smem, smem + a.stage_bytes};
-  const int tid = threadIdx.x;
-  if (tid == 0) {
-    mbar_init(&bars[0], 1);
-    mbar_init(&bars[1], 1);
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-  }
-  __syncthreads();
-  if (tid == 0) {
-    const int64_t t = a.t_begin + atomicAdd(a.counter, 1);
-    s_tile[0] = t;
-    if (t < a.t_end) issue_tile<PLAIN>(a, t, stage_ptr[0], &bars[0]);
-  }
-  __syncthreads();
-
-  uint32_t phase[2] = {0u, 0u};
-  int st = 0;
   OutT* out = reinterpret_cast<OutT*>(a.out_base);
-  bool failed = false;
-  while (true) {
-    const int64_t cur = s_tile[st];
-    if (cur >= a.t_end) break;
-    if (tid == 0) {
-      const int64_t nt = a.t_begin + atomicAdd(a.counter, 1);
-      s_tile[st ^ 1] = nt;
-      if (nt < a.t_end) issue_tile<PLAIN>(a, nt, stage_ptr[st ^ 1], &bars[st ^ 1]);
-    }
-    const TileInfo ti = a.tiles[cur];
-    const int64_t pf = ti.p_first, pl = ti.p_last;
-    const int np = (int)(pl - pf + 1);
-    const bool cached = np <= kDescCache;
-    if (cached)
-      for (int k = tid; k < np; k += kDecodeThreads) s_desc[k] = a.desc[pf + k];
-    const bool ok = mbar_wait_bounded(&bars[st], phase[st]);
-    phase[st] ^= 1u;
-    if (__syncthreads_or(!ok)) { failed = true; break; }
+  const int tid = threadIdx.x;
+  const int64_t tile_e0 = si.tile * kDecodeTile;
+  const int E0 = (int)(tile_e0 > a.lo ? tile_e0 : a.lo);
+  const int E1 = (int)((tile_e0 + kDecodeTile < a.hi) ? tile_e0 + kDecodeTile : a.hi);
+  const int Ea = (E0 / V) * V;
+  const int nvec = (E1 - Ea + V - 1) / V;
+  const int64_t w0 = (si.bit_lo >> 5) & ~3ll;
+  const int64_t stage_bit0 = w0 * 32;
+  const uint32_t* src = si.big ? a.words + w0 : reinterpret_cast<const uint32_t*>(stage);
+  const int64_t* sp = reinterpret_cast<const int64_t*>(stage);
+  const int pf = si.pf, np = si.pl - si.pf + 1;
+  const bool cached = si.cached != 0;
 
-    const int64_t tile_e0 = cur * kDecodeTile;
-    const int64_t E0 = tile_e0 > a.lo ? tile_e0 : a.lo;
-    const int64_t E1 = (tile_e0 + kDecodeTile < a.hi) ? tile_e0 + kDecodeTile : a.hi;
-    const int64_t Ea = (E0 / V) * V;
-    const int64_t nvec = (E1 - Ea + V - 1) / V;
-    const int64_t stage_bit0 = ((ti.bit_lo >> 5) & ~3ll) * 32;
-    const uint32_t* sw = reinterpret_cast<const uint32_t*>(stage_ptr[st]);
-    const int64_t* sp = reinterpret_cast<const int64_t*>(stage_ptr[st]);
-
-    Cursor c;
-    c.idx = -1;
-    c.next_start = INT64_MIN;
-    for (int64_t j = tid; j < nvec; j += kDecodeThreads) {
-      const int64_t e = Ea + j * V;
-      OutT vals[V];
-#pragma unroll
-      for (int u = 0; u < V; u++) {
-        const int64_t ee = e + u;
-        vals[u] = OutT(0);
-        if (ee < E0 || ee >= E1) continue;
-        if (c.idx < 0 || ee >= c.next_start) {
-          int k;
-          if (cached) {
-            k = c.idx < 0 ? 0 : c.idx;
-            while (k + 1 < np && (int64_t)s_desc[k + 1].start <= ee) k++;
-            cursor_load(c, s_desc[k], (k + 1 < np) ? (int64_t)s_desc[k + 1].start : INT64_MAX, stage_bit0);
-          } else {
-            int64_t lo = pf, hi = pl;
-            while (lo < hi) {
-              int64_t mid = (lo + hi + 1) >> 1;
-              if ((int64_t)__ldg(a.starts + mid) <= ee) lo = mid; else hi = mid - 1;
-            }
-            k = (int)(lo - pf);
-            cursor_load(c, a.desc[lo], (lo + 1 <= pl) ? (int64_t)__ldg(a.starts + lo + 1) : INT64_MAX, stage_bit0);
-          }
-          c.idx = k;
-        }
-        const int64_t local = ee - c.start;
-        long long resid;
-        if (PLAIN) {
-          resid = sp[ee - tile_e0];
-        } else {
-          uint64_t f = (c.bits > 0) ? read_field(sw, c.bit_rel + local * c.bits, c.bits) : 0ull;
-          resid = (c.type == MODEL_DIRECT_COPY) ? (long long)f : sign_extend(f, c.bits);
-        }
-        if (RESID) {
-          vals[u] = (OutT)resid;
-        } else if (c.type == MODEL_DIRECT_COPY) {
-          vals[u] = (OutT)(T)resid;
-        } else {
-          vals[u] = (OutT)apply_delta<T>(predict<T>(c.t0, c.t1, local), resid);
-        }
+  Cursor c;
+  c.idx = -1;
+  c.next = INT_MIN;
+  c.start = 0;
+  auto load = [&](int k) {
+    const PartDesc d = cached ? sdesc[k] : load_desc_g(a.desc + pf + k);
+    c.t0 = d.theta0;
+    c.t1 = d.theta1;
+    c.bits = d.bits_type & 0xff;
+    c.type = d.bits_type >> 8;
+    c.start = d.start;
+    c.base = (uint32_t)(d.bit_off - stage_bit0) - (uint32_t)d.start * (uint32_t)c.bits;
+    c.next = (k + 1 < np) ? (cached ? sdesc[k + 1].start : __ldg(a.starts + pf + k + 1)) : INT_MAX;
+    c.idx = k;
+  };
+  auto seek = [&](int e) {  // position the cursor on the partition holding value e
+    int k;
+    if (cached) {
+      k = c.idx < 0 ? 0 : c.idx;
+      while (k + 1 < np && sdesc[k + 1].start <= e) k++;
+    } else {
+      int lo = 0, hi = np - 1;
+      while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (__ldg(a.starts + pf + mid) <= e) lo = mid; else hi = mid - 1;
       }
-      if (VEC && e >= E0 && e + V <= E1) {
-        uint4 pk;
-        static_assert(sizeof(vals) == 16, "vector of 16 bytes");
-        memcpy(&pk, vals, 16);
-        *reinterpret_cast<uint4*>(out + e) = pk;
+      k = lo;
+    }
+    load(k);
+  };
+  auto one = [&](int e) -> OutT {  // any value, any width
+    const int local = e - c.start;
+    long long r;
+    if (PLAIN) {
+      r = sp[e - tile_e0];
+    } else {
+      const uint64_t f = c.bits > 0 ? field_at(src, c.base + (uint32_t)e * (uint32_t)c.bits, c.bits) : 0ull;
+      r = (c.type == MODEL_DIRECT_COPY) ? (long long)f : sign_extend(f, c.bits);
+    }
+    if (RESID) return (OutT)r;
+    if (c.type == MODEL_DIRECT_COPY) return (OutT)(T)r;
+    return (OutT)apply_delta<T>(predict_x<T>(c.t0, c.t1, (double)local), r);
+  };
+
+  for (int j = tid; j < nvec; j += kConsumers) {
+    const int e = Ea + j * V;
+    OutT vals[V];
+    bool fast = false;
+    if (e >= E0 && e + V <= E1) {
+      if (c.idx < 0 || e >= c.next) seek(e);
+      fast = e + V - 1 < c.next;
+    }
+    if (fast) {
+      const double x0 = (double)(e - c.start);
+      if (!PLAIN && c.bits <= 32 && c.type != MODEL_DIRECT_COPY) {
+        const uint32_t pos = c.base + (uint32_t)e * (uint32_t)c.bits;
+        const uint32_t shl = (uint32_t)(32 - c.bits) & 31u;
+#pragma unroll
+        for (int u = 0; u < V; u++) {
+          const uint32_t p = pos + (uint32_t)(u * c.bits);
+          const uint32_t wi = p >> 5;
+          const uint32_t f = __funnelshift_r(src[wi], src[wi + 1], p & 31);
+          int32_t r = (int32_t)(f << shl) >> shl;
+          r = c.bits ? r : 0;
+          if (RESID) vals[u] = (OutT)r;
+          else vals[u] = (OutT)apply_delta<T>(predict_x<T>(c.t0, c.t1, x0 + (double)u), (long long)r);
+        }
       } else {
 #pragma unroll
-        for (int u = 0; u < V; u++)
-          if (e + u >= E0 && e + u < E1) out[e + u] = vals[u];
+        for (int u = 0; u < V; u++) vals[u] = one(e + u);
+      }
+      uint4 pk;
+      memcpy(&pk, vals, 16);
+      *reinterpret_cast<uint4*>(out + e) = pk;
+    } else {
+#pragma unroll
+      for (int u = 0; u < V; u++) {
+        const int ee = e + u;
+        if (ee < E0 || ee >= E1) continue;
+        if (c.idx < 0 || ee >= c.next) seek(ee);
+        out[ee] = one(ee);
       }
     }
-    __syncthreads();
-    st ^= 1;
-  }
-  if (failed) {
-    if (tid == 0) {
-      atomicExch(a.err, DEVERR_TIMEOUT);
-      // the copy for the other stage may still be in flight: wait for it (bounded) before exit
-      if (s_tile[st ^ 1] < a.t_end) mbar_wait_bounded(&bars[st ^ 1], phase[st ^ 1]);
-    }
-    __syncthreads();
   }
 }
 
 template <typename T, bool PLAIN, bool RESID>
-static cudaError_t run_decode(glc_ctx* ctx, const DecodeArgs& a0, bool vec, cudaStream_t s) {
-  DecodeArgs a = a0;
-  const size_t smem = 2 * (size_t)a.stage_bytes;
-  void (*kern)(DecodeArgs) = vec ? decode_kernel<T, PLAIN, RESID, true> : decode_kernel<T, PLAIN, RESID, false>;
+__global__ void __launch_bounds__(kPCThreads) decode_kernel(DecodeArgs a) {
+  extern __shared__ __align__(128) uint8_t smem[];
+  __shared__ __align__(128) PartDesc s_desc[kStages][kDescCache];
+  __shared__ __align__(8) uint64_t full[kStages], empty[kStages];
+  __shared__ StageInfo s_info[kStages];
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < kStages; s++) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], kConsumerWarps);
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+
+  if (warp == kConsumerWarps) {  // ---- producer ----
+    if (lane != 0) return;
+    for (int k = 0;; k++) {
+      const int s = k % kStages;
+      if (k >= kStages && !mbar_wait_bounded(&empty[s], (uint32_t)((k / kStages) - 1) & 1u)) {
+        atomicExch(a.err, DEVERR_TIMEOUT);
+        break;
+      }
+      StageInfo si;
+      si.tile = a.t_begin + atomicAdd(a.counter, 1);
+      if (si.tile >= a.t_end) {
+        s_info[s] = si;
+        mbar_arrive(&full[s]);  // no copy: completes the phase, consumers see the end
+        break;
+      }
+      const TileInfo ti = a.tiles[si.tile];
+      si.bit_lo = ti.bit_lo;
+      si.pf = ti.p_first;
+      si.pl = ti.p_last;
+      const int np = si.pl - si.pf + 1;
+      si.cached = np <= kDescCache;
+      const void* src;
+      uint32_t bytes;
+      if (PLAIN) {
+        const int64_t e0 = si.tile * kDecodeTile;
+        const int64_t e1 = (e0 + kDecodeTile < a.n) ? e0 + kDecodeTile : a.n;
+        src = a.plain + e0;
+        bytes = (uint32_t)((((e1 - e0) * 8) + 15) & ~15ll);
+        si.big = 0;
+      } else {
+        const int64_t bh = a.tiles[si.tile + 1].bit_lo;
+        const int64_t w0 = (ti.bit_lo >> 5) & ~3ll;
+        const int64_t w1 = (((bh >> 5) + 3) + 3) & ~3ll;
+        src = a.words + w0;
+        bytes = (uint32_t)((w1 - w0) * 4);
+        si.big = bytes > (uint32_t)a.stage_bytes;
+      }
+      s_info[s] = si;
+      const uint32_t dbytes = si.cached ? (uint32_t)np * (uint32_t)sizeof(PartDesc) : 0u;
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      mbar_arrive_expect_tx(&full[s], (si.big ? 0u : bytes) + dbytes);
+      if (!si.big) tma_bulk_load(smem + (size_t)s * a.stage_bytes, src, bytes, &full[s]);
+      if (dbytes) tma_bulk_load(&s_desc[s][0], a.desc + si.pf, dbytes, &full[s]);
+    }
+    return;
+  }
+
+  // ---- consumers ----
+  for (int k = 0;; k++) {
+    const int s = k % kStages;
+    if (!mbar_wait_bounded(&full[s], (uint32_t)(k / kStages) & 1u)) {
+      if (lane == 0) atomicExch(a.err, DEVERR_TIMEOUT);
+      mbar_wait_bounded(&full[s], (uint32_t)(k / kStages) & 1u);  // copies in flight land first
+      break;
+    }
+    const StageInfo si = s_info[s];
+    if (si.tile >= a.t_end) break;
+    decode_tile<T, PLAIN, RESID>(a, si, smem + (size_t)s * a.stage_bytes, &s_desc[s][0]);
+    __syncwarp();
+    if (lane == 0) mbar_arrive(&empty[s]);
+  }
+}
+
+template <typename T, bool PLAIN, bool RESID>
+static cudaError_t run_decode(glc_ctx* ctx, const DecodeArgs& a, cudaStream_t s) {
+  const size_t smem = (size_t)kStages * a.stage_bytes;
+  void (*kern)(DecodeArgs) = decode_kernel<T, PLAIN, RESID>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   int per_sm = 0;
-  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kDecodeThreads, smem);
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kPCThreads, smem);
   if (e != cudaSuccess) return e;
   if (per_sm < 1) per_sm = 1;
   const int64_t ntile = a.t_end - a.t_begin;
@@ -263,19 +341,20 @@ static cudaError_t run_decode(glc_ctx* ctx, const DecodeArgs& a0, bool vec, cuda
   if (grid > ntile) grid = ntile;
   if (grid < 1) return cudaSuccess;
   if ((e = cudaMemsetAsync(a.counter, 0, sizeof(int), s)) != cudaSuccess) return e;
-  kern<<<(unsigned)grid, kDecodeThreads, smem, s>>>(a);
+  kern<<<(unsigned)grid, kPCThreads, smem, s>>>(a);
   return cudaGetLastError();
 }
 
 template <typename T>
-static cudaError_t decode_typed(glc_ctx* ctx, const DecodeArgs& a, int plain, int resid, bool vec, cudaStream_t s) {
-  if (plain) return resid ? run_decode<T, true, true>(ctx, a, vec, s) : run_decode<T, true, false>(ctx, a, vec, s);
-  return resid ? run_decode<T, false, true>(ctx, a, vec, s) : run_decode<T, false, false>(ctx, a, vec, s);
+static cudaError_t decode_typed(glc_ctx* ctx, const DecodeArgs& a, int plain, int resid, cudaStream_t s) {
+  if (plain) return resid ? run_decode<T, true, true>(ctx, a, s) : run_decode<T, true, false>(ctx, a, s);
+  return resid ? run_decode<T, false, true>(ctx, a, s) : run_decode<T, false, false>(ctx, a, s);
 }
 
 cudaError_t launch_decode(glc_ctx* ctx, const glc_column* c, int plain_src, int residual_out, int64_t lo, int64_t hi,
                           void* out_base, cudaStream_t s) {
   if (hi <= lo || c->n <= 0) return cudaSuccess;
+  if (((uintptr_t)out_base & 15) != 0) return cudaErrorMisalignedAddress;  // 16-byte vector stores
   DecodeArgs a;
   a.desc = c->d_desc;
   a.starts = c->d_start;
@@ -295,14 +374,15 @@ cudaError_t launch_decode(glc_ctx* ctx, const glc_column* c, int plain_src, int 
     a.stage_bytes = kDecodeTile * 8 + 16;
   } else {
     int64_t words = ((int64_t)kDecodeTile * c->max_bits + 31) / 32 + 16;
-    a.stage_bytes = (int)(((words + 3) & ~3ll) * 4);
+    words = (words + 3) & ~3ll;
+    if (words > kStageCapWords) words = kStageCapWords;
+    a.stage_bytes = (int)(words * 4);
   }
-  const bool vec = ((uintptr_t)out_base % 16) == 0;
   switch (c->dtype) {
-    case GLC_I32: return decode_typed<int32_t>(ctx, a, plain_src, residual_out, vec, s);
-    case GLC_I64: return decode_typed<int64_t>(ctx, a, plain_src, residual_out, vec, s);
-    case GLC_U64: return decode_typed<uint64_t>(ctx, a, plain_src, residual_out, vec, s);
-    case GLC_U32: return decode_typed<uint32_t>(ctx, a, plain_src, residual_out, vec, s);
+    case GLC_I32: return decode_typed<int32_t>(ctx, a, plain_src, residual_out, s);
+    case GLC_I64: return decode_typed<int64_t>(ctx, a, plain_src, residual_out, s);
+    case GLC_U64: return decode_typed<uint64_t>(ctx, a, plain_src, residual_out, s);
+    case GLC_U32: return decode_typed<uint32_t>(ctx, a, plain_src, residual_out, s);
   }
   return cudaErrorInvalidValue;
 }

@@ -47,31 +47,16 @@ template <> struct TypeTraits<uint64_t> { static constexpr bool is_signed = fals
 template <> struct TypeTraits<uint32_t> { static constexpr bool is_signed = false; };
 
 // ---------------------------------------------------------------------------------------
-// Saturating cast of an integral double (NaN -> 0), the GPU cvt.rzi semantics made explicit.
+// Saturating cast of an integral double.  The PTX float-to-integer conversion (cvt.rzi) clamps
+// to the destination range by default and maps NaN to 0, which is exactly the reference's
+// static_cast<T>(round(x)) on the GPU and its decoders' clamp of unsigned predictions to
+// [0, max] (decompression/FullDecompressionKernels.cuh:177-186).
 // ---------------------------------------------------------------------------------------
 template <typename T> __device__ __forceinline__ T sat_cast(double r);
-template <> __device__ __forceinline__ int32_t sat_cast<int32_t>(double r) {
-  if (r != r) return 0;
-  if (r >= 2147483648.0) return INT32_MAX;
-  if (r <= -2147483648.0) return INT32_MIN;
-  return (int32_t)r;
-}
-template <> __device__ __forceinline__ int64_t sat_cast<int64_t>(double r) {
-  if (r != r) return 0;
-  if (r >= 9223372036854775808.0) return INT64_MAX;
-  if (r <= -9223372036854775808.0) return INT64_MIN;
-  return (int64_t)r;
-}
-template <> __device__ __forceinline__ uint64_t sat_cast<uint64_t>(double r) {
-  if (!(r > 0.0)) return 0ull;
-  if (r >= 18446744073709551616.0) return ~0ull;
-  return (uint64_t)r;
-}
-template <> __device__ __forceinline__ uint32_t sat_cast<uint32_t>(double r) {
-  if (!(r > 0.0)) return 0u;
-  if (r >= 4294967296.0) return 0xffffffffu;
-  return (uint32_t)r;
-}
+template <> __device__ __forceinline__ int32_t sat_cast<int32_t>(double r) { return __double2int_rz(r); }
+template <> __device__ __forceinline__ int64_t sat_cast<int64_t>(double r) { return __double2ll_rz(r); }
+template <> __device__ __forceinline__ uint64_t sat_cast<uint64_t>(double r) { return __double2ull_rz(r); }
+template <> __device__ __forceinline__ uint32_t sat_cast<uint32_t>(double r) { return __double2uint_rz(r); }
 
 template <typename T> __device__ __forceinline__ T predict(double theta0, double theta1, int64_t i) {
   double p = __fma_rn(theta1, __ll2double_rn(i), theta0);

@@ -247,3 +247,22 @@ def test_cpp_dropin_caller():
     r = subprocess.run([exe], capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stdout + r.stderr
     assert r.stdout.count(": ok") == 4, r.stdout
+
+
+@pytest.mark.parametrize("offset_bytes", [4, 8, 12])
+def test_decode_into_misaligned_device_buffer(offset_bytes):
+    """Device outputs that are not 16-byte aligned are still written exactly."""
+    import torch
+    v = _data("i32_linear", 50_000)
+    codec = _codec(v)
+    col, _ = codec.compress(v, True)
+    buf = torch.zeros(len(v) + 8, dtype=torch.int32, device="cuda:0")
+    ptr = buf.data_ptr() + offset_bytes
+    glc.decompress_into(codec.ctx, col, ptr, glc.SRC_PACKED)
+    glc.decompress_range_into(codec.ctx, col, 3, 1000, ptr, glc.SRC_PACKED)
+    torch.cuda.synchronize()
+    codec.ctx.sync()
+    got = buf.cpu().numpy()[offset_bytes // 4: offset_bytes // 4 + len(v)]
+    want = v.copy()
+    want[:1000] = v[3:1003]
+    assert np.array_equal(got, want)
