@@ -351,6 +351,51 @@ static cudaError_t decode_typed(glc_ctx* ctx, const DecodeArgs& a, int plain, in
   return resid ? run_decode<T, false, true>(ctx, a, s) : run_decode<T, false, false>(ctx, a, s);
 }
 
+// Same kernel with caller-supplied scratch (work counter, error word) and SM count, for the
+// allocation-free entry point (noalloc.cu).  The counter must be zero at launch.
+cudaError_t launch_decode_scratch(const glc_column* c, int64_t lo, int64_t hi, void* out_base, int* counter, int* err,
+                                  int num_sms, cudaStream_t s) {
+  if (hi <= lo || c->n <= 0) return cudaSuccess;
+  if (((uintptr_t)out_base & 15) != 0) return cudaErrorMisalignedAddress;
+  DecodeArgs a;
+  a.desc = c->d_desc;
+  a.starts = c->d_start;
+  a.tiles = c->d_tiles;
+  a.words = c->d_words;
+  a.plain = c->d_plain;
+  a.P = c->P;
+  a.n = c->n;
+  a.lo = lo;
+  a.hi = hi;
+  a.t_begin = lo / kDecodeTile;
+  a.t_end = (hi + kDecodeTile - 1) / kDecodeTile;
+  a.out_base = out_base;
+  a.counter = counter;
+  a.err = err;
+  int64_t words = ((int64_t)kDecodeTile * c->max_bits + 31) / 32 + 16;
+  words = (words + 3) & ~3ll;
+  if (words > kStageCapWords) words = kStageCapWords;
+  a.stage_bytes = (int)(words * 4);
+  void (*kern)(DecodeArgs) = nullptr;
+  switch (c->dtype) {
+    case GLC_I32: kern = decode_kernel<int32_t, false, false>; break;
+    case GLC_I64: kern = decode_kernel<int64_t, false, false>; break;
+    case GLC_U64: kern = decode_kernel<uint64_t, false, false>; break;
+    case GLC_U32: kern = decode_kernel<uint32_t, false, false>; break;
+    default: return cudaErrorInvalidValue;
+  }
+  const size_t smem = (size_t)kStages * a.stage_bytes;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  int per_sm = 0;
+  if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kPCThreads, smem)) != cudaSuccess) return e;
+  if (per_sm < 1) per_sm = 1;
+  int64_t grid = (int64_t)per_sm * num_sms;
+  if (grid > a.t_end - a.t_begin) grid = a.t_end - a.t_begin;
+  kern<<<(unsigned)grid, kPCThreads, smem, s>>>(a);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_decode(glc_ctx* ctx, const glc_column* c, int plain_src, int residual_out, int64_t lo, int64_t hi,
                           void* out_base, cudaStream_t s) {
   if (hi <= lo || c->n <= 0) return cudaSuccess;

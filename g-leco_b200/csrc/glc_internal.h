@@ -101,6 +101,9 @@ cudaError_t launch_pack(glc_dtype dt, const void* values, glc_column* c, cudaStr
 // decode.cu: values (or residuals when residual_out) of positions [lo, hi) to out_base[lo..hi)
 cudaError_t launch_decode(glc_ctx* ctx, const glc_column* c, int plain_src, int residual_out, int64_t lo,
                           int64_t hi, void* out_base, cudaStream_t s);
+// decode.cu: packed-source value decode with caller-supplied scratch; the counter must be zero.
+cudaError_t launch_decode_scratch(const glc_column* c, int64_t lo, int64_t hi, void* out_base, int* counter,
+                                  int* err, int num_sms, cudaStream_t s);
 // random_access.cu
 cudaError_t launch_random_access(glc_ctx* ctx, const glc_column* c, int plain_src, const int32_t* pos,
                                  int64_t q, void* out, int32_t fixed_len, cudaStream_t s);

@@ -34,8 +34,9 @@ EXPORTS = [
     "glc_create", "glc_destroy", "glc_last_error", "glc_status_string", "glc_sync", "glc_compress",
     "glc_partition_variable", "glc_column_free", "glc_column_get_info", "glc_decompress_full",
     "glc_decompress_range", "glc_random_access", "glc_preunpack", "glc_blob_size", "glc_serialize",
-    "glc_deserialize",
+    "glc_deserialize", "glc_decompress_range_noalloc",
 ]
+NOALLOC_MAX_OUTPUT_BYTES = 4 << 20
 
 
 class GlcError(RuntimeError):
@@ -86,6 +87,7 @@ def load() -> ctypes.CDLL:
         "glc_blob_size": ([vp, pu64], c_int),
         "glc_serialize": ([vp, vp, vp, u64, c_int, c_int, pu64, vp], c_int),
         "glc_deserialize": ([vp, c_int, vp, u64, c_int, c_int, c_int, pvp, vp], c_int),
+        "glc_decompress_range_noalloc": ([vp, i64, i64, vp, vp], c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
@@ -186,6 +188,13 @@ def decompress_range_into(ctx: Context, col: Column, first: int, count: int, out
                           stream: int = 0, host_out: bool = False):
     ctx.check(ctx.lib.glc_decompress_range(ctx.handle, col.handle, source, first, count, ctypes.c_void_p(out_ptr),
                                            HOST_OUT if host_out else 0, ctypes.c_void_p(stream)))
+
+
+def decompress_range_noalloc(col: Column, first: int, count: int, out: np.ndarray, stream: int = 0) -> int:
+    """glc_decompress_range_noalloc: values [first, first+count) into the host array ``out``
+    without any allocation; returns the glc status (the caller checks it)."""
+    return col.ctx.lib.glc_decompress_range_noalloc(col.handle, first, count, ctypes.c_void_p(out.ctypes.data),
+                                                    ctypes.c_void_p(stream))
 
 
 def random_access_into(ctx: Context, col: Column, pos_ptr: int, q: int, out_ptr: int, source: int = SRC_AUTO,

@@ -166,6 +166,34 @@ GLC_API glc_status glc_serialize(glc_ctx* ctx, const glc_column* col, void* blob
 GLC_API glc_status glc_deserialize(glc_ctx* ctx, glc_dtype dtype, const void* blob, uint64_t size, int flags,
                            int crc32c, int pre_unpack, glc_column** out, glc_stream stream);
 
+/* ---- allocation-free range decode (no counterpart in the reference) --------------------- */
+
+/* Largest output, in bytes, of one glc_decompress_range_noalloc call:
+ * 1,048,576 int32/uint32 values or 524,288 int64/uint64 values. */
+#define GLC_NOALLOC_MAX_OUTPUT_BYTES (4u << 20)
+
+/* Decode the values of positions [first, first + count) of `col` into host memory `host_out`
+ * without allocating anything: no context is created and no cudaMalloc, cudaFree or pool
+ * allocation happens.  It is meant for callers that cannot allocate device memory while they
+ * run -- request handlers working under a fixed device-memory budget, or code that must not block
+ * on the allocator or trigger its device-wide synchronisation.  glc_decompress_range with
+ * GLC_HOST_OUT gives the same values but takes a device staging buffer on every call.
+ *
+ * The decode kernel's scratch (its work counter and error word) and the device staging of the
+ * values live in one static device array of GLC_NOALLOC_MAX_OUTPUT_BYTES + 272 bytes, which
+ * every GPU that loads this library holds until the process exits.
+ *  - count * element size above GLC_NOALLOC_MAX_OUTPUT_BYTES is rejected (GLC_ERR_INVALID_ARG);
+ *    decode larger ranges in several calls.
+ *  - The first call on a device looks up the array's device address (cudaGetSymbolAddress);
+ *    make that first call before any stream capture.
+ *  - All calls share the array: calls that overlap on the GPU race, so serialise them (one
+ *    stream, or one call at a time).  Each call clears the counter and error word it needs.
+ *  - The column must hold its packed bitstream (GLC_ERR_UNSUPPORTED otherwise).
+ *  - stream NULL = the stream of the context that made the column.  Returns after the values
+ *    are in host_out; GLC_ERR_TIMEOUT if a bounded device-side wait gave up. */
+GLC_API glc_status glc_decompress_range_noalloc(const glc_column* col, int64_t first, int64_t count,
+                                                void* host_out, glc_stream stream);
+
 #ifdef __cplusplus
 }
 #endif
