@@ -210,6 +210,115 @@ def run_reference_arm(args):
     return 0
 
 
+def run_random_access(args):
+    """Random access: 64M int64 timestamps (cumulative exponential gaps, mean 1000), fixed
+    partitions of 4096, 100M positions (half uniform, half Zipf(1.1) over partitions).  One step
+    = one launch answering all positions; value = lookups per second.  Roofline bytes per lookup:
+    4 B position + 8 B value + one 32 B DRAM sector holding the field (44 B)."""
+    import torch
+
+    import glc
+    from glc import workloads as W
+
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.Stream(dev)
+    torch.cuda.set_stream(stream)
+    sh = stream.cuda_stream
+    ctx = glc.Context(local)
+    n = min(args.n, 64 * 1024 * 1024) if args.n != DEFAULT_N else 64 * 1024 * 1024
+    q = 100_000_000 if args.n == DEFAULT_N else max(1, n // 2)
+    L = 4096
+    values = W.timestamps(n, seed=42)
+    pos = W.lookup_positions(n, q, L, seed=42)
+    d_vals = torch.from_numpy(values).to(dev)
+    col = glc.compress_device(ctx, glc.I64, d_vals.data_ptr(), n, glc.FIXED, fixed_len=L, stream=sh)
+    src = glc.SRC_PACKED
+    if args.mode == "preunpacked":
+        glc.preunpack(ctx, col, stream=sh)
+        src = glc.SRC_PREUNPACKED
+    info = col.info()
+    d_pos = torch.from_numpy(pos).to(dev)
+    out = torch.empty(q, dtype=torch.int64, device=dev)
+
+    def step():
+        glc.random_access_into(ctx, col, d_pos.data_ptr(), q, out.data_ptr(), source=src, fixed_len=L, stream=sh)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize(dev)
+    ok = bool(torch.equal(out, d_vals[d_pos.long()]))
+    clocks = ClockSampler(dev)
+    clocks.start()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        step()
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    ms = e0.elapsed_time(e1) / args.steps
+    clk = clocks.stop()
+    lookups_s = q / (ms / 1e3)
+    per_lookup = 4 + 8 + 32
+    peak, peak_kind = measured_peak()
+    achieved = per_lookup * lookups_s / 1e9
+    # end to end: pinned host positions in, pinned host values out, through the C ABI
+    h_pos = torch.from_numpy(pos).pin_memory()
+    h_out = torch.empty(q, dtype=torch.int64).pin_memory()
+
+    def e2e_step():
+        glc.random_access_into(ctx, col, h_pos.data_ptr(), q, h_out.data_ptr(), source=src, fixed_len=L,
+                               stream=sh, host_in=True, host_out=True)
+
+    e2e_step()
+    torch.cuda.synchronize(dev)
+    t0 = time.perf_counter()
+    e0.record(stream)
+    for _ in range(args.e2e_steps):
+        e2e_step()
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    e2e_ms = e0.elapsed_time(e1) / args.e2e_steps
+    e2e_ok = bool(np.array_equal(h_out.numpy(), values[pos]))
+    cpu = None
+    if not args.no_cpu_baseline:
+        import oracle
+        try:
+            blob = glc.serialize_host(ctx, col) if args.mode == "packed" else None
+            if blob is None:
+                raise RuntimeError("pre-unpacked columns have no host decoder in the reference")
+            sample = pos[:2_000_000]
+            with tempfile.TemporaryDirectory() as td:
+                got, secs = oracle.ref_hostdecode(blob, "i64", sample, td)
+            cpu = {"value": round(len(sample) / secs, 1), "unit": "lookups/s", "cores": 1,
+                   "kind": "reference" if oracle.ref_available() else "port",
+                   "sample": f"{len(sample):,} of the positions through directRandomAccessCPU; "
+                             f"mismatches vs input: {int(np.count_nonzero(got != values[sample]))}"}
+        except Exception as ex:
+            cpu = {"value": None, "unit": "lookups/s", "cores": 1, "kind": "reference", "sample": f"skipped: {ex}"}
+    line = {
+        "metric": "random lookups/s", "value": round(lookups_s, 1), "unit": "lookups/s", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 4), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "int64", "data": "synthetic",
+        "config": {"workload": f"timestamps_i64_64M_fixed4096_lookups100M_{args.mode}", "values": n, "lookups": q,
+                   "partitions": info.num_partitions, "bits_per_value": round(info.total_bits / n, 3),
+                   "position_mix": "50% uniform, 50% Zipf(1.1) over partitions", "bit_exact": ok and e2e_ok,
+                   "l2": "positions and outputs larger than L2 (no flush)"},
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                     "frac": round(achieved / peak, 4), "peak_kind": peak_kind, "traffic": None,
+                     "bytes_per_lookup": per_lookup},
+        "e2e": {"value": round(q / (e2e_ms / 1e3), 1), "unit": "lookups/s", "h2d_bytes_per_step": 4 * q,
+                "d2h_bytes_per_step": 8 * q},
+        "gpu_launches": args.steps, "clocks": clk, "cpu_baseline": cpu,
+    }
+    print(json.dumps(line), flush=True)
+    col.free()
+    ctx.close()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -219,11 +328,17 @@ def main():
     ap.add_argument("--n", type=int, default=DEFAULT_N)
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", default="c2_decode", choices=["c2_decode", "c3_random_access"],
+                    help="c2_decode (headline): full decode of the 200M piecewise uint64 column; "
+                         "c3_random_access: 100M lookups into a 64M int64 timestamp column")
+    ap.add_argument("--mode", default="packed", choices=["packed", "preunpacked"], help="c3 residual source")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":
         return run_reference_arm(args)
+    if args.workload == "c3_random_access":
+        return run_random_access(args)
 
     import torch
     import torch.distributed as dist

@@ -17,27 +17,30 @@
 //     the consumers released the ring stage, then issues 1-D TMA bulk copies (cp.async.bulk,
 //     non-multicast) of the tile's packed words (or pre-unpacked residuals) AND of the tile's
 //     32-byte partition descriptors into that stage, completing on the stage's "full" mbarrier.
-//     Three stages keep up to three tiles in flight per CTA.
+//     Two stages keep up to two tiles in flight per CTA (2-4 measured; two leave room for more
+//     resident CTAs).
 //   consumers: wait on "full", decode the tile from shared memory and write 16-byte vector
 //     stores, then arrive on the stage's "empty" mbarrier.  The common case (a vector whose
 //     values all lie in one partition, fields <= 32 bits) uses 32-bit bit arithmetic relative to
 //     the stage, one funnel shift per field, a two-shift sign extension and the FP64 prediction
 //     fma(theta1, i, theta0) -> round -> saturating convert, exactly as the reference computes it.
 // No CTA-wide barrier runs inside the loop.  A tile whose packed words exceed a stage is decoded
-// straight from global memory (rare: fields averaging more than 32 bits over a tile).
+// straight from global memory (rare: fields averaging more than 48 bits over a tile).
 // Every mbarrier wait is bounded by wall time; on expiry the kernel records an error code and
 // returns after a second bounded wait for its own copies.
 #include <climits>
+#include <cstdlib>
 #include <type_traits>
 #include "glc_internal.h"
 
 namespace glc {
 
-constexpr int kStages = 3;
+constexpr int kDefaultStages = 2;  // ring depth; measured best on the 200M uint64 column (2-4 swept)
+constexpr int kTileDescs = 40;  // descriptors staged per tile (a 4096-value tile of >= 128-value partitions spans <= 34)
 constexpr int kConsumerWarps = 8;
 constexpr int kConsumers = kConsumerWarps * 32;
 constexpr int kPCThreads = kConsumers + 32;
-constexpr int kStageCapWords = 4096 + 16;  // 32 bits per value on average over a tile
+constexpr int kStageCapWords = 6144 + 16;  // 48 bits per value on average over a tile (1040-6160 swept)
 
 struct DecodeArgs {
   const PartDesc* desc;
@@ -131,7 +134,7 @@ __device__ __forceinline__ uint64_t field_at(const uint32_t* w, uint32_t pos, in
 }
 
 template <typename T> __device__ __forceinline__ T predict_x(double t0, double t1, double x) {
-  return sat_cast<T>(round(__fma_rn(t1, x, t0)));
+  return predict_from<T>(__fma_rn(t1, x, t0));
 }
 
 // Partition cursor of one consumer thread inside a tile.
@@ -204,52 +207,66 @@ __device__ __forceinline__ void decode_tile(const DecodeArgs& a, const StageInfo
     return (OutT)apply_delta<T>(predict_x<T>(c.t0, c.t1, (double)local), r);
   };
 
-  for (int j = tid; j < nvec; j += kConsumers) {
-    const int e = Ea + j * V;
+  // Fast path for a vector whose values all lie in the cursor's partition: packed fields of at
+  // most 32 bits, 32-bit positions relative to the stage, one funnel shift per field.
+  auto fast_vec = [&](int e) {
     OutT vals[V];
-    bool fast = false;
-    if (e >= E0 && e + V <= E1) {
-      if (c.idx < 0 || e >= c.next) seek(e);
-      fast = e + V - 1 < c.next;
-    }
-    if (fast) {
-      const double x0 = (double)(e - c.start);
-      if (!PLAIN && c.bits <= 32 && c.type != MODEL_DIRECT_COPY) {
-        const uint32_t pos = c.base + (uint32_t)e * (uint32_t)c.bits;
-        const uint32_t shl = (uint32_t)(32 - c.bits) & 31u;
-#pragma unroll
-        for (int u = 0; u < V; u++) {
-          const uint32_t p = pos + (uint32_t)(u * c.bits);
-          const uint32_t wi = p >> 5;
-          const uint32_t f = __funnelshift_r(src[wi], src[wi + 1], p & 31);
-          int32_t r = (int32_t)(f << shl) >> shl;
-          r = c.bits ? r : 0;
-          if (RESID) vals[u] = (OutT)r;
-          else vals[u] = (OutT)apply_delta<T>(predict_x<T>(c.t0, c.t1, x0 + (double)u), (long long)r);
-        }
-      } else {
-#pragma unroll
-        for (int u = 0; u < V; u++) vals[u] = one(e + u);
-      }
-      uint4 pk;
-      memcpy(&pk, vals, 16);
-      *reinterpret_cast<uint4*>(out + e) = pk;
-    } else {
+    const double x0 = (double)(e - c.start);
+    if (!PLAIN && c.bits <= 32 && c.type != MODEL_DIRECT_COPY) {
+      const uint32_t pos = c.base + (uint32_t)e * (uint32_t)c.bits;
+      const uint32_t shl = (uint32_t)(32 - c.bits) & 31u;
+      const int32_t zmask = c.bits ? -1 : 0;
 #pragma unroll
       for (int u = 0; u < V; u++) {
-        const int ee = e + u;
-        if (ee < E0 || ee >= E1) continue;
-        if (c.idx < 0 || ee >= c.next) seek(ee);
-        out[ee] = one(ee);
+        const uint32_t p = pos + (uint32_t)(u * c.bits);
+        const uint32_t wi = p >> 5;
+        const uint32_t f = __funnelshift_r(src[wi], src[wi + 1], p & 31);
+        const int32_t r = ((int32_t)(f << shl) >> shl) & zmask;
+        if (RESID) vals[u] = (OutT)r;
+        else vals[u] = (OutT)apply_delta<T>(predict_x<T>(c.t0, c.t1, u ? x0 + (double)u : x0), (long long)r);
       }
+    } else {
+#pragma unroll
+      for (int u = 0; u < V; u++) vals[u] = one(e + u);
+    }
+    uint4 pk;
+    memcpy(&pk, vals, 16);
+    *reinterpret_cast<uint4*>(out + e) = pk;
+  };
+  auto general_vec = [&](int e) {  // partition boundary inside the vector, or a partial tile
+#pragma unroll
+    for (int u = 0; u < V; u++) {
+      const int ee = e + u;
+      if (ee < E0 || ee >= E1) continue;
+      if (c.idx < 0 || ee >= c.next) seek(ee);
+      out[ee] = one(ee);
+    }
+  };
+
+  if (E0 == tile_e0 && E1 - E0 == kDecodeTile) {  // full tile: every vector is in range
+    constexpr int kIters = kDecodeTile / V / kConsumers;
+#pragma unroll 2
+    for (int it = 0; it < kIters; it++) {
+      const int e = Ea + (it * kConsumers + tid) * V;
+      if (c.idx < 0 || e >= c.next) seek(e);
+      if (e + V - 1 < c.next) fast_vec(e); else general_vec(e);
+    }
+  } else {
+    for (int j = tid; j < nvec; j += kConsumers) {
+      const int e = Ea + j * V;
+      if (e >= E0 && e + V <= E1) {
+        if (c.idx < 0 || e >= c.next) seek(e);
+        if (e + V - 1 < c.next) { fast_vec(e); continue; }
+      }
+      general_vec(e);
     }
   }
 }
 
-template <typename T, bool PLAIN, bool RESID>
+template <typename T, bool PLAIN, bool RESID, int kStages>
 __global__ void __launch_bounds__(kPCThreads) decode_kernel(DecodeArgs a) {
   extern __shared__ __align__(128) uint8_t smem[];
-  __shared__ __align__(128) PartDesc s_desc[kStages][kDescCache];
+  __shared__ __align__(128) PartDesc s_desc[kStages][kTileDescs];
   __shared__ __align__(8) uint64_t full[kStages], empty[kStages];
   __shared__ StageInfo s_info[kStages];
 
@@ -283,7 +300,7 @@ __global__ void __launch_bounds__(kPCThreads) decode_kernel(DecodeArgs a) {
       si.pf = ti.p_first;
       si.pl = ti.p_last;
       const int np = si.pl - si.pf + 1;
-      si.cached = np <= kDescCache;
+      si.cached = np <= kTileDescs;
       const void* src;
       uint32_t bytes;
       if (PLAIN) {
@@ -326,10 +343,10 @@ __global__ void __launch_bounds__(kPCThreads) decode_kernel(DecodeArgs a) {
   }
 }
 
-template <typename T, bool PLAIN, bool RESID>
+template <typename T, bool PLAIN, bool RESID, int kStages>
 static cudaError_t run_decode(glc_ctx* ctx, const DecodeArgs& a, cudaStream_t s) {
   const size_t smem = (size_t)kStages * a.stage_bytes;
-  void (*kern)(DecodeArgs) = decode_kernel<T, PLAIN, RESID>;
+  void (*kern)(DecodeArgs) = decode_kernel<T, PLAIN, RESID, kStages>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   int per_sm = 0;
@@ -345,10 +362,23 @@ static cudaError_t run_decode(glc_ctx* ctx, const DecodeArgs& a, cudaStream_t s)
   return cudaGetLastError();
 }
 
+template <typename T, int kStages>
+static cudaError_t decode_staged(glc_ctx* ctx, const DecodeArgs& a, int plain, int resid, cudaStream_t s) {
+  if (plain) return resid ? run_decode<T, true, true, kStages>(ctx, a, s) : run_decode<T, true, false, kStages>(ctx, a, s);
+  return resid ? run_decode<T, false, true, kStages>(ctx, a, s) : run_decode<T, false, false, kStages>(ctx, a, s);
+}
+
 template <typename T>
-static cudaError_t decode_typed(glc_ctx* ctx, const DecodeArgs& a, int plain, int resid, cudaStream_t s) {
-  if (plain) return resid ? run_decode<T, true, true>(ctx, a, s) : run_decode<T, true, false>(ctx, a, s);
-  return resid ? run_decode<T, false, true>(ctx, a, s) : run_decode<T, false, false>(ctx, a, s);
+static cudaError_t decode_typed(glc_ctx* ctx, const DecodeArgs& a, int plain, int resid, int stages, cudaStream_t s) {
+  if (stages == 2) return decode_staged<T, 2>(ctx, a, plain, resid, s);
+  if (stages == 4) return decode_staged<T, 4>(ctx, a, plain, resid, s);
+  return decode_staged<T, 3>(ctx, a, plain, resid, s);
+}
+
+// Launch shape overrides for tuning sweeps (ring depth, stage capacity in words).
+static int env_int(const char* name, int dflt) {
+  const char* v = getenv(name);
+  return (v && *v) ? atoi(v) : dflt;
 }
 
 // Same kernel with caller-supplied scratch (work counter, error word) and SM count, for the
@@ -378,13 +408,13 @@ cudaError_t launch_decode_scratch(const glc_column* c, int64_t lo, int64_t hi, v
   a.stage_bytes = (int)(words * 4);
   void (*kern)(DecodeArgs) = nullptr;
   switch (c->dtype) {
-    case GLC_I32: kern = decode_kernel<int32_t, false, false>; break;
-    case GLC_I64: kern = decode_kernel<int64_t, false, false>; break;
-    case GLC_U64: kern = decode_kernel<uint64_t, false, false>; break;
-    case GLC_U32: kern = decode_kernel<uint32_t, false, false>; break;
+    case GLC_I32: kern = decode_kernel<int32_t, false, false, kDefaultStages>; break;
+    case GLC_I64: kern = decode_kernel<int64_t, false, false, kDefaultStages>; break;
+    case GLC_U64: kern = decode_kernel<uint64_t, false, false, kDefaultStages>; break;
+    case GLC_U32: kern = decode_kernel<uint32_t, false, false, kDefaultStages>; break;
     default: return cudaErrorInvalidValue;
   }
-  const size_t smem = (size_t)kStages * a.stage_bytes;
+  const size_t smem = (size_t)kDefaultStages * a.stage_bytes;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   int per_sm = 0;
@@ -420,14 +450,16 @@ cudaError_t launch_decode(glc_ctx* ctx, const glc_column* c, int plain_src, int 
   } else {
     int64_t words = ((int64_t)kDecodeTile * c->max_bits + 31) / 32 + 16;
     words = (words + 3) & ~3ll;
-    if (words > kStageCapWords) words = kStageCapWords;
+    const int64_t cap = env_int("GLC_DECODE_CAP_WORDS", kStageCapWords) & ~3;
+    if (words > cap) words = cap < 32 ? 32 : cap;
     a.stage_bytes = (int)(words * 4);
   }
+  const int stages = env_int("GLC_DECODE_STAGES", kDefaultStages);
   switch (c->dtype) {
-    case GLC_I32: return decode_typed<int32_t>(ctx, a, plain_src, residual_out, s);
-    case GLC_I64: return decode_typed<int64_t>(ctx, a, plain_src, residual_out, s);
-    case GLC_U64: return decode_typed<uint64_t>(ctx, a, plain_src, residual_out, s);
-    case GLC_U32: return decode_typed<uint32_t>(ctx, a, plain_src, residual_out, s);
+    case GLC_I32: return decode_typed<int32_t>(ctx, a, plain_src, residual_out, stages, s);
+    case GLC_I64: return decode_typed<int64_t>(ctx, a, plain_src, residual_out, stages, s);
+    case GLC_U64: return decode_typed<uint64_t>(ctx, a, plain_src, residual_out, stages, s);
+    case GLC_U32: return decode_typed<uint32_t>(ctx, a, plain_src, residual_out, stages, s);
   }
   return cudaErrorInvalidValue;
 }

@@ -58,9 +58,23 @@ template <> __device__ __forceinline__ int64_t sat_cast<int64_t>(double r) { ret
 template <> __device__ __forceinline__ uint64_t sat_cast<uint64_t>(double r) { return __double2ull_rz(r); }
 template <> __device__ __forceinline__ uint32_t sat_cast<uint32_t>(double r) { return __double2uint_rz(r); }
 
+// round-half-away-from-zero(x) == trunc(x + copysign(0.5 - 2^-54, x)) for every double x under
+// round-to-nearest-even addition: with k = trunc(|x|) and f = |x| - k, the sum stays below k + 1
+// when f < 0.5 (it falls short of k + 1 by more than half an ulp) and reaches k + 1 when
+// f >= 0.5 (at f = 0.5 in [0.5, 1) it is the tie 1 - 2^-54, which rounds to even, 1.0); values of
+// magnitude >= 2^52 are integers and the addend is below half an ulp.  The truncation is folded
+// into the saturating round-toward-zero conversion, so prediction = one fma, one add, one convert.
+__device__ __forceinline__ double half_away_bias(double x) {
+  return __longlong_as_double((__double_as_longlong(x) & (long long)0x8000000000000000ull) |
+                              0x3FDFFFFFFFFFFFFFll);  // +-(0.5 - 2^-54)
+}
+
+template <typename T> __device__ __forceinline__ T predict_from(double p) {
+  return sat_cast<T>(__dadd_rn(p, half_away_bias(p)));
+}
+
 template <typename T> __device__ __forceinline__ T predict(double theta0, double theta1, int64_t i) {
-  double p = __fma_rn(theta1, __ll2double_rn(i), theta0);
-  return sat_cast<T>(round(p));
+  return predict_from<T>(__fma_rn(theta1, __ll2double_rn(i), theta0));
 }
 
 template <typename T> __device__ __forceinline__ long long calc_delta(T actual, T pred) {

@@ -191,3 +191,18 @@ def test_variable_size_within_one_percent_of_reference_partitioner(oracle, gen):
     ours = oracle.compress(v, "variable").reported_size()
     assert ours <= 1.01 * ref, (ours, ref)
     assert ours >= 0.9 * ref, (ours, ref)
+
+
+def test_half_away_rounding_identity():
+    """The device predicts round-half-away(x) as trunc(x + copysign(0.5 - 2^-54, x)) folded into a
+    truncating conversion; check the identity against exact rounding (x - trunc(x) is exact)."""
+    rng = np.random.default_rng(0)
+    bias = np.nextafter(0.5, 0.0)
+    ties = rng.integers(-(2 ** 53), 2 ** 53, 500_000) / 2.0
+    xs = np.concatenate([rng.standard_normal(500_000) * 10.0 ** rng.integers(-3, 18, 500_000), ties,
+                         np.nextafter(ties, np.inf), np.nextafter(ties, -np.inf),
+                         [0.5, -0.5, 0.49999999999999994, -0.49999999999999994, 2.4999999999999996,
+                          4503599627370495.5, 2.0 ** 53, 2.0 ** 63, -(2.0 ** 63), 0.0, -0.0]])
+    t = np.trunc(xs)
+    exact = np.where(np.abs(xs - t) >= 0.5, t + np.sign(xs), t)
+    assert np.array_equal(np.trunc(xs + np.copysign(bias, xs)), exact)
