@@ -69,64 +69,69 @@ def profiled_traffic_per_value():
     return None
 
 
+_SAMPLER = r"""
+import sys, time, pynvml
+pynvml.nvmlInit()
+uuid, index = sys.argv[1], int(sys.argv[2])
+try:
+    h = pynvml.nvmlDeviceGetHandleByUUID(uuid)
+except Exception:
+    h = pynvml.nvmlDeviceGetHandleByIndex(index)
+get = getattr(pynvml, "nvmlDeviceGetCurrentClocksEventReasons", None) or pynvml.nvmlDeviceGetCurrentClocksThrottleReasons
+print("max", pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM), flush=True)
+while True:
+    print(pynvml.nvmlDeviceGetClockInfo(h, pynvml.NVML_CLOCK_SM), int(get(h)), flush=True)
+    time.sleep(0.002)
+"""
+
+
 class ClockSampler:
-    """SM clock and clock-event (throttle) reasons sampled through NVML every 2 ms while the
-    timed region runs (reads only; no GPU setting is changed)."""
+    """SM clock and clock-event (throttle) reasons of the benchmarked GPU, sampled through NVML
+    every 2 ms by a separate process while the timed region runs (reads only; no GPU setting is
+    changed)."""
 
     REASONS = {0x8: "hw_slowdown", 0x40: "hw_thermal_slowdown", 0x20: "sw_thermal_slowdown",
                0x4: "sw_power_cap", 0x80: "hw_power_brake_slowdown"}
 
     def __init__(self, torch_device):
         self.dev = torch_device
-        self.samples, self.reasons, self.max_mhz = [], set(), None
-        self._stop = threading.Event()
-        self.handle = None
-
-    def _open(self):
-        import pynvml
-        pynvml.nvmlInit()
-        try:
-            import torch
-            uuid = str(torch.cuda.get_device_properties(self.dev).uuid)
-            return pynvml.nvmlDeviceGetHandleByUUID(("GPU-" + uuid) if not uuid.startswith("GPU-") else uuid)
-        except Exception:
-            vis = os.environ.get("CUDA_VISIBLE_DEVICES")
-            idx = int(vis.split(",")[self.dev.index]) if vis and vis.split(",")[0].isdigit() else self.dev.index
-            return pynvml.nvmlDeviceGetHandleByIndex(idx)
+        self.proc = None
 
     def start(self):
+        import torch
         try:
-            import pynvml
-            self.handle = self._open()
-            self.max_mhz = float(pynvml.nvmlDeviceGetMaxClockInfo(self.handle, pynvml.NVML_CLOCK_SM))
-            self.thread = threading.Thread(target=self._loop, daemon=True)
-            self.thread.start()
-        except Exception as ex:  # reported in the JSON line
-            self.error = str(ex)
-            self.handle = None
-
-    def _loop(self):
-        import pynvml
-        get_reasons = getattr(pynvml, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
-            pynvml.nvmlDeviceGetCurrentClocksThrottleReasons
-        while not self._stop.is_set():
-            try:
-                self.samples.append(float(pynvml.nvmlDeviceGetClockInfo(self.handle, pynvml.NVML_CLOCK_SM)))
-                mask = int(get_reasons(self.handle))
-                for bit, name in self.REASONS.items():
-                    if mask & bit:
-                        self.reasons.add(name)
-            except Exception:
-                pass
-            time.sleep(0.002)
+            uuid = str(torch.cuda.get_device_properties(self.dev).uuid)
+            uuid = uuid if uuid.startswith("GPU-") else "GPU-" + uuid
+        except Exception:
+            uuid = ""
+        vis = os.environ.get("CUDA_VISIBLE_DEVICES", "")
+        idx = self.dev.index or 0
+        if vis and vis.split(",")[0].strip().isdigit():
+            idx = int(vis.split(",")[idx])
+        self.proc = subprocess.Popen([sys.executable, "-c", _SAMPLER, uuid, str(idx)], stdout=subprocess.PIPE,
+                                     stderr=subprocess.DEVNULL, text=True)
+        self.max_line = self.proc.stdout.readline()  # the sampler is up before the timed region starts
 
     def stop(self):
-        if self.handle is None:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "error": getattr(self, "error", "no NVML")}
-        self._stop.set()
-        self.thread.join(timeout=2)
-        return {"sm_mhz": float(np.median(self.samples)) if self.samples else None, "sm_max_mhz": self.max_mhz,
-                "reasons": sorted(self.reasons), "samples": len(self.samples), "source": "NVML, 2 ms"}
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "error": "sampler not started"}
+        self.proc.terminate()
+        out, _ = self.proc.communicate(timeout=10)
+        sm, reasons = [], set()
+        for ln in out.splitlines():
+            parts = ln.split()
+            if len(parts) != 2:
+                continue
+            sm.append(float(parts[0]))
+            for bit, name in self.REASONS.items():
+                if int(parts[1]) & bit:
+                    reasons.add(name)
+        try:
+            smax = float(self.max_line.split()[1])
+        except Exception:
+            smax = None
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm), "source": "NVML every 2 ms (separate process)"}
 
 
 def make_values(n: int, rank: int) -> np.ndarray:
@@ -228,7 +233,7 @@ def run_random_access(args):
     sh = stream.cuda_stream
     ctx = glc.Context(local)
     n = min(args.n, 64 * 1024 * 1024) if args.n != DEFAULT_N else 64 * 1024 * 1024
-    q = 100_000_000 if args.n == DEFAULT_N else max(1, n // 2)
+    q = args.queries
     L = 4096
     values = W.timestamps(n, seed=42)
     pos = W.lookup_positions(n, q, L, seed=42)
@@ -332,6 +337,7 @@ def main():
                     help="c2_decode (headline): full decode of the 200M piecewise uint64 column; "
                          "c3_random_access: 100M lookups into a 64M int64 timestamp column")
     ap.add_argument("--mode", default="packed", choices=["packed", "preunpacked"], help="c3 residual source")
+    ap.add_argument("--queries", type=int, default=100_000_000, help="c3 lookups per step")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
