@@ -7,19 +7,19 @@
 //
 // Per lookup: the position, one 32-byte partition descriptor (theta0, theta1, bit offset,
 // start, bits|type -- a single DRAM sector instead of the reference's four arrays), and the
-// two words that hold the field (or the 8-byte pre-unpacked residual).  Partition lookup is
+// words that hold the field (or the 8-byte pre-unpacked residual).  Partition lookup is
 // pos / L for fixed partitions; for variable partitions a sample of every k-th start lives in
 // shared memory, a binary search there narrows the range to k partitions, and a short search
-// over the (L2-resident) start array finishes it.  Each thread carries four independent
+// over the (L2-resident) start array finishes it.  Each thread carries several independent
 // lookups through the load stages so their DRAM latencies overlap.
 // Positions outside [0, n) yield 0, as the reference's variable-partition kernels do; the
 // fixed variants use the same rule here instead of reading past the metadata.
+#include <cstdlib>
 #include "glc_internal.h"
 
 namespace glc {
 
 constexpr int kRAThreads = 256;
-constexpr int kRAQueries = 4;
 constexpr int kRASample = 4096;
 
 struct RAArgs {
@@ -37,12 +37,20 @@ struct RAArgs {
   int32_t nsample;
 };
 
+// The words holding a field come from one aligned 16-byte load (one sector, one request); a
+// second load is needed only when the field continues past that granule.  The word array is
+// 16-byte aligned and padded, so the granule never leaves the allocation.
 __device__ __forceinline__ uint64_t read_field_global(const uint32_t* __restrict__ w, int64_t pos, int bits) {
   const int64_t wi = pos >> 5;
   const int sh = (int)(pos & 31);
-  const uint64_t lo = (uint64_t)__ldg(w + wi) | ((uint64_t)__ldg(w + wi + 1) << 32);
-  uint64_t f = lo >> sh;
-  if (bits + sh > 64) f |= (uint64_t)__ldg(w + wi + 2) << (64 - sh);
+  const int k = (int)(wi & 3);
+  const uint4 g = __ldg(reinterpret_cast<const uint4*>(w + (wi - k)));
+  const uint32_t a = k == 0 ? g.x : k == 1 ? g.y : k == 2 ? g.z : g.w;
+  const int need = (sh + bits + 31) >> 5;  // words the field touches: 1..3
+  uint32_t b = k == 0 ? g.y : k == 1 ? g.z : g.w;
+  if (k == 3 && need > 1) b = __ldg(w + wi + 1);
+  uint64_t f = (((uint64_t)b << 32) | a) >> sh;
+  if (need > 2) f |= (uint64_t)__ldg(w + wi + 2) << (64 - sh);
   return low_bits(f, bits);
 }
 
@@ -59,8 +67,10 @@ __device__ __forceinline__ PartDesc load_desc(const PartDesc* __restrict__ d) {
 }
 
 // MODE 0: fixed, power-of-two length; 1: fixed, any length; 2: variable.
-template <typename T, bool PLAIN, int MODE>
-__global__ void __launch_bounds__(kRAThreads) random_access_kernel(RAArgs a) {
+// QPT lookups per thread are carried through the load stages together; MINB is the residency
+// the register budget is sized for.
+template <typename T, bool PLAIN, int MODE, int kRAQueries, int MINB>
+__global__ void __launch_bounds__(kRAThreads, MINB) random_access_kernel(RAArgs a) {
   __shared__ int32_t s_sample[kRASample];
   if (MODE == 2) {
     for (int k = threadIdx.x; k < a.nsample; k += kRAThreads) s_sample[k] = a.starts[(int64_t)k * a.sample_stride];
@@ -130,22 +140,39 @@ __global__ void __launch_bounds__(kRAThreads) random_access_kernel(RAArgs a) {
   }
 }
 
-template <typename T, bool PLAIN>
-static cudaError_t ra_typed(glc_ctx* ctx, const RAArgs& a, int mode, cudaStream_t s) {
-  void (*k)(RAArgs) = mode == 0 ? random_access_kernel<T, PLAIN, 0>
-                    : mode == 1 ? random_access_kernel<T, PLAIN, 1>
-                                : random_access_kernel<T, PLAIN, 2>;
+template <typename T, bool PLAIN, int QPT, int MINB>
+static cudaError_t ra_shape(glc_ctx* ctx, const RAArgs& a, int mode, cudaStream_t s) {
+  void (*k)(RAArgs) = mode == 0 ? random_access_kernel<T, PLAIN, 0, QPT, MINB>
+                    : mode == 1 ? random_access_kernel<T, PLAIN, 1, QPT, MINB>
+                                : random_access_kernel<T, PLAIN, 2, QPT, MINB>;
   int per_sm = 0;
   cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kRAThreads, 0);
   if (e != cudaSuccess) return e;
   if (per_sm < 1) per_sm = 1;
-  const int64_t chunk = (int64_t)kRAThreads * kRAQueries;
+  const int64_t chunk = (int64_t)kRAThreads * QPT;
   int64_t grid = (a.q + chunk - 1) / chunk;
   const int64_t cap = (int64_t)per_sm * ctx->num_sms;
   if (grid > cap) grid = cap;
   if (grid < 1) grid = 1;
   k<<<(unsigned)grid, kRAThreads, 0, s>>>(a);
   return cudaGetLastError();
+}
+
+// Launch shapes (lookups per thread, CTAs per SM), measured on 100M lookups into a 64M int64
+// column: packed fields -> 2 lookups per thread at 6 CTAs/SM (40 registers, more warps resident);
+// pre-unpacked residuals (every lookup a DRAM sector) -> 8 lookups per thread.  GLC_RA_SHAPE
+// overrides the choice for tuning sweeps.
+template <typename T, bool PLAIN>
+static cudaError_t ra_typed(glc_ctx* ctx, const RAArgs& a, int mode, cudaStream_t s) {
+  const char* v = getenv("GLC_RA_SHAPE");
+  const int shape = (v && *v) ? atoi(v) : (PLAIN ? 3 : 4);
+  switch (shape) {
+    case 1: return ra_shape<T, PLAIN, 4, 5>(ctx, a, mode, s);
+    case 2: return ra_shape<T, PLAIN, 2, 8>(ctx, a, mode, s);
+    case 3: return ra_shape<T, PLAIN, 8, 2>(ctx, a, mode, s);
+    case 4: return ra_shape<T, PLAIN, 2, 6>(ctx, a, mode, s);
+    default: return ra_shape<T, PLAIN, 4, 1>(ctx, a, mode, s);
+  }
 }
 
 cudaError_t launch_random_access(glc_ctx* ctx, const glc_column* c, int plain_src, const int32_t* pos, int64_t q,
