@@ -209,6 +209,7 @@ glc_status glc_sync(glc_ctx* ctx, glc_stream stream) {
 
 glc_status glc_column_free(glc_column* col) {
   if (!col) return GLC_ERR_INVALID_ARG;
+  if (col->view) return fail(col->ctx, GLC_ERR_INVALID_ARG, "a column of a batch is freed with its batch");
   if (col->ctx) cudaSetDevice(col->ctx->device);
   free_column_arrays(col);
   delete col;
@@ -469,6 +470,7 @@ glc_status glc_random_access(glc_ctx* ctx, const glc_column* col, glc_source sou
 
 glc_status glc_preunpack(glc_ctx* ctx, glc_column* col, int drop_packed, glc_stream stream) {
   if (!ctx || !col) return fail(ctx, GLC_ERR_INVALID_ARG, "null argument");
+  if (col->view && drop_packed) return fail(ctx, GLC_ERR_INVALID_ARG, "a batch column keeps its bitstream");
   if (col->n == 0) return GLC_OK;
   if (!col->d_plain) {
     if (!col->d_words) return fail(ctx, GLC_ERR_UNSUPPORTED, "column has no packed bitstream");

@@ -1,0 +1,560 @@
+// batch.cu -- many columns per launch: batched compress and batched decode (device work list).
+//
+// No counterpart in the reference, which compresses and decodes one column per API call
+// (api/G-LeCo.cuh:349, :680).  Thousands of columns of uneven length and mixed int32 / int64 /
+// uint64 / uint32 are handled by a fixed number of launches instead of a launch chain per column:
+//
+// compress (fixed-length partitions; the length is picked per column by compressed size):
+//   1. per candidate length (1024, 2048, 4096): one launch fits every partition of every column
+//      and adds each column's residual bits; the smallest compressed size picks the length
+//      (skipped when the caller fixes the length);
+//   2. one launch writes all partitions, one launch fits them all (a CTA per partition: exact
+//      128-bit sums, line, max |delta|, width), one scan over all widths gives the bit offsets;
+//   3. one launch packs every column's words (a CTA per 8 KB output tile of any column), one
+//      builds all descriptors, one all decode-tile tables.
+//   Each column's arrays are slices of batch-wide allocations; a column compressed here is
+//   identical, byte for byte, to glc_compress of the same values with the same length.
+// decode: one persistent launch (decode.cu batch_decode_kernel) over a work list with one item
+//   per (column, 4096-value tile); optionally captured once in a CUDA graph and replayed.
+#include <algorithm>
+#include <cstring>
+#include <new>
+#include <vector>
+#include "glc_internal.h"
+#include "glc_scan.cuh"
+
+using namespace glc;
+
+struct glc_batch {
+  glc_ctx* ctx = nullptr;
+  std::vector<glc_column*> cols;  // views into `storage` when the batch compressed them
+  bool owns_columns = false;
+  std::vector<void*> storage;     // device allocations owned by the batch
+  BatchColumn* d_cols = nullptr;
+  int max_bits = 0;
+  // decode work list for the last set of outputs
+  std::vector<void*> outs;
+  BatchWork* d_work = nullptr;
+  int64_t nwork = 0;
+  unsigned long long* d_counter = nullptr;
+  int* d_err = nullptr;
+  cudaGraphExec_t graph = nullptr;
+};
+
+namespace {
+
+constexpr int kFitCTA = 256;
+constexpr int kMaxBatchPartLen = 8192;
+const int kCandidates[3] = {1024, 2048, 4096};
+
+glc_status bfail(glc_ctx* ctx, glc_status st, const char* msg) {
+  if (ctx) ctx->err = msg;
+  return st;
+}
+
+glc_status bcuda(glc_ctx* ctx, cudaError_t e, const char* where) {
+  if (ctx) ctx->err = std::string(where) + ": " + cudaGetErrorString(e);
+  return e == cudaErrorMemoryAllocation ? GLC_ERR_OOM : GLC_ERR_CUDA;
+}
+
+#define BCK(call, where)                                  \
+  do {                                                    \
+    cudaError_t e_ = (call);                              \
+    if (e_ != cudaSuccess) return bcuda(ctx, e_, where);  \
+  } while (0)
+
+// Per batch column, on the device.
+struct FitCol {
+  const void* values;
+  int64_t n;
+  int64_t part_base;  // first global partition of the column
+  int32_t len;        // partition length
+  int32_t dtype;
+};
+
+__device__ __forceinline__ int col_of(const int64_t* __restrict__ base, int ncols, int64_t x) {
+  int lo = 0, hi = ncols - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (base[mid] <= x) lo = mid; else hi = mid - 1;
+  }
+  return lo;
+}
+
+template <typename T>
+__device__ void fit_one(const T* __restrict__ v, int64_t len, int& type, double& t0, double& t1, long long& err,
+                        int& bits) {
+  __shared__ i128 s_a[kFitCTA / 32], s_b[kFitCTA / 32];
+  __shared__ long long s_m[kFitCTA / 32];
+  __shared__ int s_o[kFitCTA / 32];
+  __shared__ double s_t0, s_t1;
+  __shared__ int s_over;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  i128 sy = 0, sxy = 0;
+  int ovf = 0;
+  for (int64_t i = threadIdx.x; i < len; i += kFitCTA) {
+    const T x = __ldg(v + i);
+    ovf |= overflows_double<T>(x) ? 1 : 0;
+    sy += (i128)x;
+    sxy += (i128)i * (i128)x;
+  }
+  sy = warp_sum_i128(sy);
+  sxy = warp_sum_i128(sxy);
+  ovf = __any_sync(FULL_MASK, ovf);
+  if (lane == 0) { s_a[warp] = sy; s_b[warp] = sxy; s_o[warp] = ovf; }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    i128 a = 0, b = 0;
+    int o = 0;
+    for (int w = 0; w < kFitCTA / 32; w++) { a += s_a[w]; b += s_b[w]; o |= s_o[w]; }
+    double x0 = 0.0, x1 = 0.0;
+    if (!o) solve_line(len, a, b, x0, x1);
+    s_t0 = x0;
+    s_t1 = x1;
+    s_over = o;
+  }
+  __syncthreads();
+  const double a0 = s_t0, a1 = s_t1;
+  const bool over = s_over != 0;
+  long long m = 0;
+  if (!over)
+    for (int64_t i = threadIdx.x; i < len; i += kFitCTA) {
+      const long long d = abs_ref(calc_delta<T>(__ldg(v + i), predict<T>(a0, a1, i)));
+      m = d > m ? d : m;
+    }
+  m = warp_max_ll(m);
+  if (lane == 0) s_m[warp] = m;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    long long t = 0;
+    for (int w = 0; w < kFitCTA / 32; w++) t = s_m[w] > t ? s_m[w] : t;
+    type = over ? MODEL_DIRECT_COPY : MODEL_LINEAR;
+    t0 = a0;
+    t1 = a1;
+    err = over ? 0 : t;
+    bits = over ? (int)sizeof(T) * 8 : bits_for(t);
+  }
+}
+
+// One CTA per global partition.  size_only: add the column's residual bits into col_bits[c];
+// otherwise write the partition's SoA entries and its width.
+__global__ void __launch_bounds__(kFitCTA)
+batch_fit_kernel(const FitCol* __restrict__ cols, const int64_t* __restrict__ part_base, int ncols, int size_only,
+                 unsigned long long* __restrict__ col_bits, int32_t* __restrict__ starts, int32_t* __restrict__ ends,
+                 int32_t* __restrict__ types, double* __restrict__ params, int32_t* __restrict__ bits,
+                 int64_t* __restrict__ errs, int64_t* __restrict__ widths) {
+  const int64_t p = blockIdx.x;
+  const int c = col_of(part_base, ncols, p);
+  const FitCol fc = cols[c];
+  const int64_t k = p - fc.part_base;
+  const int64_t s = k * fc.len;
+  const int64_t len = (s + fc.len < fc.n ? s + fc.len : fc.n) - s;
+  int type = 0, b = 0;
+  double t0 = 0.0, t1 = 0.0;
+  long long err = 0;
+  switch (fc.dtype) {
+    case GLC_I32: fit_one<int32_t>((const int32_t*)fc.values + s, len, type, t0, t1, err, b); break;
+    case GLC_I64: fit_one<int64_t>((const int64_t*)fc.values + s, len, type, t0, t1, err, b); break;
+    case GLC_U64: fit_one<uint64_t>((const uint64_t*)fc.values + s, len, type, t0, t1, err, b); break;
+    default: fit_one<uint32_t>((const uint32_t*)fc.values + s, len, type, t0, t1, err, b); break;
+  }
+  if (threadIdx.x != 0) return;
+  if (size_only) {
+    atomicAdd(col_bits + c, (unsigned long long)(len * b));
+    return;
+  }
+  starts[p] = (int32_t)s;
+  ends[p] = (int32_t)(s + len);
+  types[p] = type;
+  params[4 * p] = t0;
+  params[4 * p + 1] = t1;
+  params[4 * p + 2] = 0.0;
+  params[4 * p + 3] = 0.0;
+  bits[p] = b;
+  errs[p] = err;
+  widths[p] = len * b;
+}
+
+// Global exclusive bit prefix -> column-local offsets; col_stats[c] = {total bits, max bits}.
+__global__ void batch_local_offsets_kernel(const int64_t* __restrict__ gofs, const int64_t* __restrict__ part_base,
+                                           const int32_t* __restrict__ bits, int ncols, int64_t P,
+                                           const int64_t* __restrict__ grand, int64_t* __restrict__ offs,
+                                           int64_t* __restrict__ col_stats) {
+  const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= P) return;
+  const int c = col_of(part_base, ncols, p);
+  const int64_t base = gofs[part_base[c]];
+  offs[p] = gofs[p] - base;
+  atomicMax((unsigned long long*)(col_stats + 2 * c + 1), (unsigned long long)bits[p]);
+  if (p == part_base[c]) {
+    // the next column's first partition, or the grand total when every later column is empty
+    const int64_t nb = (c + 1 < ncols) ? part_base[c + 1] : P;
+    const int64_t next = nb < P ? gofs[nb] : *grand;
+    col_stats[2 * c] = next - base;
+  }
+}
+
+struct TileCol {
+  const int32_t* starts;
+  const int32_t* bits;
+  const int64_t* offs;
+  glc::TileInfo* tiles;
+  int64_t P, n, ntiles, total_bits;
+};
+
+__device__ __forceinline__ int64_t owner_in(const int32_t* __restrict__ starts, int64_t P, int64_t e) {
+  int64_t lo = 0, hi = P - 1;
+  while (lo < hi) {
+    const int64_t mid = (lo + hi + 1) >> 1;
+    if ((int64_t)starts[mid] <= e) lo = mid; else hi = mid - 1;
+  }
+  return lo;
+}
+
+// One thread per tile-table entry of any column (ntiles + 1 entries per column).
+__global__ void batch_tiles_kernel(const TileCol* __restrict__ cols, const int64_t* __restrict__ entry_base, int ncols,
+                                   int64_t total) {
+  const int64_t x = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (x >= total) return;
+  const int c = col_of(entry_base, ncols, x);
+  const TileCol tc = cols[c];
+  const int64_t t = x - entry_base[c];
+  glc::TileInfo ti;
+  if (t == tc.ntiles) {
+    ti.bit_lo = tc.total_bits;
+    ti.p_first = (int32_t)(tc.P - 1);
+    ti.p_last = (int32_t)(tc.P - 1);
+  } else {
+    const int64_t e0 = t * kDecodeTile;
+    const int64_t e1 = e0 + kDecodeTile < tc.n ? e0 + kDecodeTile : tc.n;
+    const int64_t pf = owner_in(tc.starts, tc.P, e0);
+    ti.bit_lo = tc.offs[pf] + (e0 - tc.starts[pf]) * (int64_t)tc.bits[pf];
+    ti.p_first = (int32_t)pf;
+    ti.p_last = (int32_t)owner_in(tc.starts, tc.P, e1 - 1);
+  }
+  tc.tiles[t] = ti;
+}
+
+__global__ void batch_desc_kernel(const int32_t* __restrict__ starts, const int32_t* __restrict__ types,
+                                  const double* __restrict__ params, const int32_t* __restrict__ bits,
+                                  const int64_t* __restrict__ offs, int64_t P, PartDesc* __restrict__ desc) {
+  const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= P) return;
+  PartDesc d;
+  d.theta0 = params[4 * p];
+  d.theta1 = params[4 * p + 1];
+  d.bit_off = offs[p];
+  d.start = starts[p];
+  d.bits_type = (bits[p] & 0xff) | (types[p] << 8);
+  desc[p] = d;
+}
+
+template <typename V> cudaError_t dalloc(glc_batch* b, V** p, size_t count) {
+  void* q = nullptr;
+  cudaError_t e = cudaMalloc(&q, count * sizeof(V) + 16);
+  if (e == cudaSuccess) b->storage.push_back(q);
+  *p = (V*)q;
+  return e;
+}
+
+void free_batch(glc_batch* b) {
+  if (b->graph) cudaGraphExecDestroy(b->graph);
+  if (b->owns_columns)
+    for (glc_column* c : b->cols) delete c;  // views: their arrays are in storage
+  for (void* q : b->storage) cudaFree(q);
+  if (b->d_cols) cudaFree(b->d_cols);
+  if (b->d_work) cudaFree(b->d_work);
+  if (b->d_counter) cudaFree(b->d_counter);
+  delete b;
+}
+
+glc_status finish_batch(glc_ctx* ctx, glc_batch* b, cudaStream_t s) {
+  std::vector<BatchColumn> h(b->cols.size());
+  b->max_bits = 0;
+  for (size_t i = 0; i < b->cols.size(); i++) {
+    const glc_column* c = b->cols[i];
+    h[i] = BatchColumn{c->d_desc, c->d_start, c->d_tiles, c->d_words, c->n, (int32_t)c->dtype, c->max_bits};
+    b->max_bits = std::max(b->max_bits, c->max_bits);
+  }
+  BCK(cudaMalloc(&b->d_cols, sizeof(BatchColumn) * std::max<size_t>(1, h.size())), "batch: column table");
+  BCK(cudaMemcpyAsync(b->d_cols, h.data(), sizeof(BatchColumn) * h.size(), cudaMemcpyHostToDevice, s), "batch: column table");
+  void* q = nullptr;
+  BCK(cudaMalloc(&q, 64), "batch: counters");
+  BCK(cudaMemsetAsync(q, 0, 64, s), "batch: counters");
+  b->d_counter = (unsigned long long*)q;
+  b->d_err = (int*)((char*)q + 16);
+  BCK(cudaStreamSynchronize(s), "batch: sync");
+  return GLC_OK;
+}
+
+glc_status build_work(glc_ctx* ctx, glc_batch* b, void* const* outs, cudaStream_t s) {
+  const size_t nc = b->cols.size();
+  bool same = b->d_work && b->outs.size() == nc;
+  for (size_t i = 0; same && i < nc; i++) same = b->outs[i] == outs[i];
+  if (same) return GLC_OK;
+  std::vector<BatchWork> w;
+  for (size_t i = 0; i < nc; i++) {
+    const glc_column* c = b->cols[i];
+    if (c->n == 0) continue;
+    if (!outs[i]) return bfail(ctx, GLC_ERR_INVALID_ARG, "null output for a column of the batch");
+    if (((uintptr_t)outs[i] & 15) != 0) return bfail(ctx, GLC_ERR_INVALID_ARG, "batch outputs must be 16-byte aligned");
+    if (!c->d_words) return bfail(ctx, GLC_ERR_UNSUPPORTED, "a column of the batch has no packed bitstream");
+    for (int64_t t = 0; t < c->ntiles; t++) w.push_back(BatchWork{(int32_t)i, (int32_t)t, 0, c->n, outs[i]});
+  }
+  if (b->graph) {
+    cudaGraphExecDestroy(b->graph);
+    b->graph = nullptr;
+  }
+  if (b->d_work) {
+    cudaStreamSynchronize(s);
+    cudaFree(b->d_work);
+    b->d_work = nullptr;
+  }
+  b->nwork = (int64_t)w.size();
+  if (!w.empty()) {
+    BCK(cudaMalloc(&b->d_work, sizeof(BatchWork) * w.size()), "batch: work list");
+    BCK(cudaMemcpyAsync(b->d_work, w.data(), sizeof(BatchWork) * w.size(), cudaMemcpyHostToDevice, s), "batch: work list");
+    BCK(cudaStreamSynchronize(s), "batch: work list");
+  }
+  b->outs.assign(outs, outs + nc);
+  return GLC_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+glc_status glc_batch_create(glc_ctx* ctx, glc_column* const* cols, int32_t ncols, glc_batch** out) {
+  if (!ctx || !out || ncols < 0 || (ncols > 0 && !cols)) return bfail(ctx, GLC_ERR_INVALID_ARG, "bad batch arguments");
+  *out = nullptr;
+  glc_batch* b = new (std::nothrow) glc_batch();
+  if (!b) return GLC_ERR_OOM;
+  b->ctx = ctx;
+  for (int i = 0; i < ncols; i++) {
+    if (!cols[i]) { delete b; return bfail(ctx, GLC_ERR_INVALID_ARG, "null column in batch"); }
+    b->cols.push_back(cols[i]);
+  }
+  cudaSetDevice(ctx->device);
+  glc_status st = finish_batch(ctx, b, ctx->own_stream);
+  if (st != GLC_OK) { free_batch(b); return st; }
+  *out = b;
+  return GLC_OK;
+}
+
+glc_status glc_batch_compress(glc_ctx* ctx, const glc_dtype* dtypes, const void* const* values, const int64_t* ns,
+                              int32_t ncols, int32_t fixed_partition_len, glc_batch** out,
+                              int64_t* compressed_size_bytes, glc_stream stream) {
+  if (!ctx || !out || ncols <= 0 || !dtypes || !values || !ns) return bfail(ctx, GLC_ERR_INVALID_ARG, "bad batch arguments");
+  if (fixed_partition_len < 0 || fixed_partition_len > kMaxBatchPartLen)
+    return bfail(ctx, GLC_ERR_INVALID_ARG, "batch partition length must be in [1, 8192] (0 = chosen per column)");
+  *out = nullptr;
+  for (int i = 0; i < ncols; i++) {
+    if (dtypes[i] < GLC_I32 || dtypes[i] > GLC_U32 || ns[i] < 0 || ns[i] > 0x7fffffffll || (ns[i] > 0 && !values[i]))
+      return bfail(ctx, GLC_ERR_INVALID_ARG, "bad column in batch");
+  }
+  cudaSetDevice(ctx->device);
+  cudaStream_t s = stream ? (cudaStream_t)stream : ctx->own_stream;
+  glc_batch* b = new (std::nothrow) glc_batch();
+  if (!b) return GLC_ERR_OOM;
+  b->ctx = ctx;
+  b->owns_columns = true;
+  auto bail = [&](glc_status st) { cudaStreamSynchronize(s); free_batch(b); return st; };
+  const int nc = ncols;
+
+  // ---- partition length per column ----
+  std::vector<int32_t> len(nc, fixed_partition_len > 0 ? fixed_partition_len : kCandidates[2]);
+  std::vector<int64_t> pb(nc + 1, 0);
+  FitCol* d_fc = nullptr;
+  int64_t* d_pb = nullptr;
+  unsigned long long* d_colbits = nullptr;
+  cudaError_t e;
+  auto upload_layout = [&](const std::vector<int32_t>& L) -> cudaError_t {
+    std::vector<FitCol> fc(nc);
+    pb[0] = 0;
+    for (int i = 0; i < nc; i++) {
+      const int64_t P = ns[i] > 0 ? (ns[i] + L[i] - 1) / L[i] : 0;
+      pb[i + 1] = pb[i] + P;
+      fc[i] = FitCol{values[i], ns[i], pb[i], L[i], (int32_t)dtypes[i]};
+    }
+    cudaError_t ee = cudaMemcpyAsync(d_fc, fc.data(), sizeof(FitCol) * nc, cudaMemcpyHostToDevice, s);
+    if (ee == cudaSuccess) ee = cudaMemcpyAsync(d_pb, pb.data(), sizeof(int64_t) * (nc + 1), cudaMemcpyHostToDevice, s);
+    if (ee == cudaSuccess) ee = cudaStreamSynchronize(s);  // host vectors are reused next
+    return ee;
+  };
+  if ((e = dalloc(b, &d_fc, nc)) != cudaSuccess || (e = dalloc(b, &d_pb, nc + 1)) != cudaSuccess ||
+      (e = dalloc(b, &d_colbits, nc)) != cudaSuccess)
+    return bail(bcuda(ctx, e, "batch compress: allocation"));
+  if (fixed_partition_len == 0) {
+    std::vector<int64_t> best_size(nc, INT64_MAX);
+    std::vector<int32_t> best_len(nc, kCandidates[2]);
+    std::vector<unsigned long long> hbits(nc);
+    for (int cand : kCandidates) {
+      std::vector<int32_t> L(nc, cand);
+      if ((e = upload_layout(L)) != cudaSuccess) return bail(bcuda(ctx, e, "batch compress: layout"));
+      if ((e = cudaMemsetAsync(d_colbits, 0, sizeof(unsigned long long) * nc, s)) != cudaSuccess)
+        return bail(bcuda(ctx, e, "batch compress: sizes"));
+      if (pb[nc] > 0)
+        batch_fit_kernel<<<(unsigned)pb[nc], kFitCTA, 0, s>>>(d_fc, d_pb, nc, 1, d_colbits, nullptr, nullptr, nullptr,
+                                                              nullptr, nullptr, nullptr, nullptr);
+      if ((e = cudaMemcpyAsync(hbits.data(), d_colbits, sizeof(unsigned long long) * nc, cudaMemcpyDeviceToHost, s)) !=
+              cudaSuccess ||
+          (e = cudaStreamSynchronize(s)) != cudaSuccess)
+        return bail(bcuda(ctx, e, "batch compress: sizes"));
+      for (int i = 0; i < nc; i++) {
+        const int64_t P = pb[i + 1] - pb[i];
+        const int64_t size = 64 * P + 120 + (int64_t)(hbits[i] + 7) / 8;  // api/G-LeCo.cuh:589-603
+        if (size < best_size[i]) { best_size[i] = size; best_len[i] = cand; }
+      }
+    }
+    len = best_len;
+  }
+  if ((e = upload_layout(len)) != cudaSuccess) return bail(bcuda(ctx, e, "batch compress: layout"));
+  const int64_t P = pb[nc];
+
+  // ---- batch-wide arrays ----
+  int32_t *starts, *ends, *types, *bits;
+  double* params;
+  int64_t *offs, *errs, *widths, *gofs, *scan_tmp, *grand, *col_stats;
+  PartDesc* desc;
+  if ((e = dalloc(b, &starts, P)) || (e = dalloc(b, &ends, P)) || (e = dalloc(b, &types, P)) ||
+      (e = dalloc(b, &bits, P)) || (e = dalloc(b, &params, 4 * P)) || (e = dalloc(b, &offs, P)) ||
+      (e = dalloc(b, &errs, P)) || (e = dalloc(b, &widths, P)) || (e = dalloc(b, &gofs, P)) ||
+      (e = dalloc(b, &scan_tmp, scan_num_tiles(P) + 1)) || (e = dalloc(b, &grand, 1)) ||
+      (e = dalloc(b, &col_stats, 2 * nc)) || (e = dalloc(b, &desc, P)))
+    return bail(bcuda(ctx, e, "batch compress: allocation"));
+  if (P > 0)
+    batch_fit_kernel<<<(unsigned)P, kFitCTA, 0, s>>>(d_fc, d_pb, nc, 0, nullptr, starts, ends, types, params, bits, errs,
+                                                     widths);
+  if ((e = exclusive_scan<int64_t>(widths, gofs, P, grand, scan_tmp, s)) != cudaSuccess ||
+      (e = cudaMemsetAsync(col_stats, 0, sizeof(int64_t) * 2 * nc, s)) != cudaSuccess)
+    return bail(bcuda(ctx, e, "batch compress: offsets"));
+  if (P > 0)
+    batch_local_offsets_kernel<<<(unsigned)((P + 255) / 256), 256, 0, s>>>(gofs, d_pb, bits, nc, P, grand, offs,
+                                                                            col_stats);
+  std::vector<int64_t> hstats(2 * nc);
+  if ((e = cudaMemcpyAsync(hstats.data(), col_stats, sizeof(int64_t) * 2 * nc, cudaMemcpyDeviceToHost, s)) !=
+          cudaSuccess ||
+      (e = cudaStreamSynchronize(s)) != cudaSuccess)
+    return bail(bcuda(ctx, e, "batch compress: column sizes"));
+
+  // ---- column views, words, packing and tables ----
+  std::vector<int64_t> word_base(nc + 1, 0), tile_base(nc + 1, 0), entry_base(nc + 1, 0);
+  std::vector<glc_column*> cols(nc, nullptr);
+  for (int i = 0; i < nc; i++) {
+    glc_column* c = new (std::nothrow) glc_column();
+    if (!c) return bail(GLC_ERR_OOM);
+    cols[i] = c;
+    b->cols.push_back(c);
+    c->ctx = ctx;
+    c->view = true;
+    c->dtype = dtypes[i];
+    c->n = ns[i];
+    c->P = pb[i + 1] - pb[i];
+    c->total_bits = hstats[2 * i];
+    c->max_bits = (int32_t)hstats[2 * i + 1];
+    c->fixed_len = len[i];
+    c->nwords = (c->total_bits + 31) / 32;
+    c->nwords_alloc = ((c->nwords + 3) & ~3ll) + 8;
+    c->ntiles = (c->n + kDecodeTile - 1) / kDecodeTile;
+    c->reported_size = c->n ? 64 * c->P + 120 + (c->total_bits + 7) / 8 : 0;
+    word_base[i + 1] = word_base[i] + c->nwords_alloc;
+    tile_base[i + 1] = tile_base[i] + pack_tiles(c->nwords_alloc);
+    entry_base[i + 1] = entry_base[i] + (c->n ? c->ntiles + 1 : 0);
+  }
+  uint32_t* words;
+  TileInfo* tiles;
+  PackArgs* d_pack;
+  TileCol* d_tc;
+  int64_t *d_tb, *d_eb;
+  const void** d_vals;
+  int32_t* d_dt;
+  if ((e = dalloc(b, &words, word_base[nc])) || (e = dalloc(b, &tiles, entry_base[nc])) || (e = dalloc(b, &d_pack, nc)) ||
+      (e = dalloc(b, &d_tc, nc)) || (e = dalloc(b, &d_tb, nc + 1)) || (e = dalloc(b, &d_eb, nc + 1)) ||
+      (e = dalloc(b, &d_vals, nc)) || (e = dalloc(b, &d_dt, nc)))
+    return bail(bcuda(ctx, e, "batch compress: allocation"));
+  std::vector<PackArgs> hp(nc);
+  std::vector<TileCol> htc(nc);
+  std::vector<int32_t> hdt(nc);
+  for (int i = 0; i < nc; i++) {
+    glc_column* c = cols[i];
+    const int64_t p0 = pb[i];
+    c->d_start = starts + p0;
+    c->d_end = ends + p0;
+    c->d_types = types + p0;
+    c->d_params = params + 4 * p0;
+    c->d_bits = bits + p0;
+    c->d_offs = offs + p0;
+    c->d_err = errs + p0;
+    c->d_desc = desc + p0;
+    c->d_words = words + word_base[i];
+    c->d_tiles = tiles + entry_base[i];
+    hp[i] = PackArgs{c->d_start, c->d_end, c->d_types, c->d_params, c->d_bits, c->d_offs, c->P, c->d_words,
+                     c->nwords_alloc};
+    htc[i] = TileCol{c->d_start, c->d_bits, c->d_offs, c->d_tiles, c->P, c->n, c->ntiles, c->total_bits};
+    hdt[i] = dtypes[i];
+  }
+  if ((e = cudaMemcpyAsync(d_pack, hp.data(), sizeof(PackArgs) * nc, cudaMemcpyHostToDevice, s)) ||
+      (e = cudaMemcpyAsync(d_tc, htc.data(), sizeof(TileCol) * nc, cudaMemcpyHostToDevice, s)) ||
+      (e = cudaMemcpyAsync(d_tb, tile_base.data(), sizeof(int64_t) * (nc + 1), cudaMemcpyHostToDevice, s)) ||
+      (e = cudaMemcpyAsync(d_eb, entry_base.data(), sizeof(int64_t) * (nc + 1), cudaMemcpyHostToDevice, s)) ||
+      (e = cudaMemcpyAsync(d_vals, values, sizeof(void*) * nc, cudaMemcpyHostToDevice, s)) ||
+      (e = cudaMemcpyAsync(d_dt, hdt.data(), sizeof(int32_t) * nc, cudaMemcpyHostToDevice, s)))
+    return bail(bcuda(ctx, e, "batch compress: tables"));
+  if ((e = launch_batch_pack(d_pack, d_vals, d_dt, d_tb, nc, tile_base[nc], s)) != cudaSuccess)
+    return bail(bcuda(ctx, e, "batch compress: pack"));
+  if (P > 0) batch_desc_kernel<<<(unsigned)((P + 255) / 256), 256, 0, s>>>(starts, types, params, bits, offs, P, desc);
+  if (entry_base[nc] > 0)
+    batch_tiles_kernel<<<(unsigned)((entry_base[nc] + 255) / 256), 256, 0, s>>>(d_tc, d_eb, nc, entry_base[nc]);
+  if ((e = cudaGetLastError()) != cudaSuccess || (e = cudaStreamSynchronize(s)) != cudaSuccess)
+    return bail(bcuda(ctx, e, "batch compress"));
+  int64_t total = 0;
+  for (glc_column* c : cols) total += c->reported_size;
+  if (compressed_size_bytes) *compressed_size_bytes = total;
+  glc_status st = finish_batch(ctx, b, s);
+  if (st != GLC_OK) return bail(st);
+  *out = b;
+  return GLC_OK;
+}
+
+glc_status glc_batch_column(const glc_batch* b, int32_t i, glc_column** col) {
+  if (!b || !col || i < 0 || i >= (int32_t)b->cols.size()) return GLC_ERR_INVALID_ARG;
+  *col = b->cols[i];
+  return GLC_OK;
+}
+
+glc_status glc_batch_decompress(glc_ctx* ctx, glc_batch* b, void* const* outs, int use_graph, glc_stream stream) {
+  if (!ctx || !b || (!outs && !b->cols.empty())) return bfail(ctx, GLC_ERR_INVALID_ARG, "bad batch arguments");
+  cudaSetDevice(ctx->device);
+  cudaStream_t s = stream ? (cudaStream_t)stream : ctx->own_stream;
+  glc_status st = build_work(ctx, b, outs, s);
+  if (st != GLC_OK) return st;
+  if (b->nwork == 0) return GLC_OK;
+  BatchDecodeArgs a{b->d_cols, b->d_work, b->nwork, b->d_counter, b->d_err, batch_stage_bytes(b->max_bits)};
+  if (!use_graph) {
+    BCK(launch_batch_decode(a, ctx->num_sms, s), "batch decode");
+    return GLC_OK;
+  }
+  if (!b->graph) {  // capture the counter reset and the launch once; replay afterwards
+    cudaGraph_t g = nullptr;
+    BCK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "batch decode: capture");
+    cudaError_t e = launch_batch_decode(a, ctx->num_sms, s);
+    cudaError_t e2 = cudaStreamEndCapture(s, &g);
+    if (e != cudaSuccess) { if (g) cudaGraphDestroy(g); return bcuda(ctx, e, "batch decode: capture"); }
+    if (e2 != cudaSuccess) return bcuda(ctx, e2, "batch decode: capture");
+    e = cudaGraphInstantiate(&b->graph, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) { b->graph = nullptr; return bcuda(ctx, e, "batch decode: instantiate"); }
+  }
+  BCK(cudaGraphLaunch(b->graph, s), "batch decode: graph launch");
+  return GLC_OK;
+}
+
+glc_status glc_batch_free(glc_batch* b) {
+  if (!b) return GLC_ERR_INVALID_ARG;
+  cudaSetDevice(b->ctx->device);
+  cudaDeviceSynchronize();
+  free_batch(b);
+  return GLC_OK;
+}
+
+}  // extern "C"

@@ -343,6 +343,130 @@ __global__ void __launch_bounds__(kPCThreads) decode_kernel(DecodeArgs a) {
   }
 }
 
+// ---------------------------------------------------------------------------------------
+// Batched decode: one persistent launch over a device work list spanning many columns of mixed
+// element types.  A work item is one tile of one column, clipped to an element range, with its
+// own output base, so the same launch serves full decodes of thousands of columns and range
+// requests of different sizes.  The producer stages each item exactly like a single-column tile;
+// consumers switch on the item's element type (uniform per tile) and reuse decode_tile.
+// ---------------------------------------------------------------------------------------
+template <int kStages>
+__global__ void __launch_bounds__(kPCThreads) batch_decode_kernel(BatchDecodeArgs b) {
+  extern __shared__ __align__(128) uint8_t smem[];
+  __shared__ __align__(128) PartDesc s_desc[kStages][kTileDescs];
+  __shared__ __align__(8) uint64_t full[kStages], empty[kStages];
+  __shared__ StageInfo s_info[kStages];
+  __shared__ int64_t s_item[kStages];
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < kStages; s++) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], kConsumerWarps);
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+
+  if (warp == kConsumerWarps) {  // ---- producer ----
+    if (lane != 0) return;
+    for (int k = 0;; k++) {
+      const int s = k % kStages;
+      if (k >= kStages && !mbar_wait_bounded(&empty[s], (uint32_t)((k / kStages) - 1) & 1u)) {
+        atomicExch(b.err, DEVERR_TIMEOUT);
+        break;
+      }
+      const int64_t item = (int64_t)atomicAdd(b.counter, 1ull);
+      s_item[s] = item;
+      StageInfo si;
+      if (item >= b.nwork) {
+        si.tile = -1;
+        s_info[s] = si;
+        mbar_arrive(&full[s]);
+        break;
+      }
+      const BatchWork w = b.work[item];
+      const BatchColumn col = b.cols[w.col];
+      const TileInfo ti = col.tiles[w.tile];
+      const int64_t bh = col.tiles[w.tile + 1].bit_lo;
+      si.tile = w.tile;
+      si.bit_lo = ti.bit_lo;
+      si.pf = ti.p_first;
+      si.pl = ti.p_last;
+      const int np = si.pl - si.pf + 1;
+      si.cached = np <= kTileDescs;
+      const int64_t w0 = (ti.bit_lo >> 5) & ~3ll;
+      const int64_t w1 = (((bh >> 5) + 3) + 3) & ~3ll;
+      const uint32_t bytes = (uint32_t)((w1 - w0) * 4);
+      si.big = bytes > (uint32_t)b.stage_bytes;
+      s_info[s] = si;
+      const uint32_t dbytes = si.cached ? (uint32_t)np * (uint32_t)sizeof(PartDesc) : 0u;
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      mbar_arrive_expect_tx(&full[s], (si.big ? 0u : bytes) + dbytes);
+      if (!si.big) tma_bulk_load(smem + (size_t)s * b.stage_bytes, col.words + w0, bytes, &full[s]);
+      if (dbytes) tma_bulk_load(&s_desc[s][0], col.desc + si.pf, dbytes, &full[s]);
+    }
+    return;
+  }
+
+  for (int k = 0;; k++) {  // ---- consumers ----
+    const int s = k % kStages;
+    if (!mbar_wait_bounded(&full[s], (uint32_t)(k / kStages) & 1u)) {
+      if (lane == 0) atomicExch(b.err, DEVERR_TIMEOUT);
+      mbar_wait_bounded(&full[s], (uint32_t)(k / kStages) & 1u);
+      break;
+    }
+    const StageInfo si = s_info[s];
+    if (si.tile < 0) break;
+    const BatchWork w = b.work[s_item[s]];
+    const BatchColumn col = b.cols[w.col];
+    DecodeArgs a;
+    a.desc = col.desc;
+    a.starts = col.starts;
+    a.tiles = col.tiles;
+    a.words = col.words;
+    a.plain = nullptr;
+    a.P = 0;
+    a.n = col.n;
+    a.lo = w.lo;
+    a.hi = w.hi;
+    a.out_base = w.out_base;
+    a.stage_bytes = b.stage_bytes;
+    const uint8_t* stage = smem + (size_t)s * b.stage_bytes;
+    switch (col.dtype) {
+      case GLC_I32: decode_tile<int32_t, false, false>(a, si, stage, &s_desc[s][0]); break;
+      case GLC_I64: decode_tile<int64_t, false, false>(a, si, stage, &s_desc[s][0]); break;
+      case GLC_U64: decode_tile<uint64_t, false, false>(a, si, stage, &s_desc[s][0]); break;
+      default: decode_tile<uint32_t, false, false>(a, si, stage, &s_desc[s][0]); break;
+    }
+    __syncwarp();
+    if (lane == 0) mbar_arrive(&empty[s]);
+  }
+}
+
+cudaError_t launch_batch_decode(const BatchDecodeArgs& b, int num_sms, cudaStream_t s) {
+  if (b.nwork <= 0) return cudaSuccess;
+  void (*kern)(BatchDecodeArgs) = batch_decode_kernel<kDefaultStages>;
+  const size_t smem = (size_t)kDefaultStages * b.stage_bytes;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  int per_sm = 0;
+  if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kPCThreads, smem)) != cudaSuccess) return e;
+  if (per_sm < 1) per_sm = 1;
+  int64_t grid = (int64_t)per_sm * num_sms;
+  if (grid > b.nwork) grid = b.nwork;
+  if ((e = cudaMemsetAsync(b.counter, 0, sizeof(unsigned long long), s)) != cudaSuccess) return e;
+  kern<<<(unsigned)grid, kPCThreads, smem, s>>>(b);
+  return cudaGetLastError();
+}
+
+int batch_stage_bytes(int max_bits) {
+  int64_t words = ((int64_t)kDecodeTile * max_bits + 31) / 32 + 16;
+  words = (words + 3) & ~3ll;
+  if (words > kStageCapWords) words = kStageCapWords;
+  return (int)(words * 4);
+}
+
 template <typename T, bool PLAIN, bool RESID, int kStages>
 static cudaError_t run_decode(glc_ctx* ctx, const DecodeArgs& a, cudaStream_t s) {
   const size_t smem = (size_t)kStages * a.stage_bytes;

@@ -52,6 +52,7 @@ struct glc_ctx {
 
 struct glc_column {
   glc_ctx* ctx = nullptr;
+  bool view = false;         // arrays are slices of a batch's storage (freed with the batch)
   glc_dtype dtype = GLC_I32;
   int64_t n = 0;
   int64_t P = 0;
@@ -96,6 +97,21 @@ cudaError_t launch_fit(glc_dtype dt, const void* values, glc_column* c, void* sc
 cudaError_t launch_desc_and_tiles(glc_column* c, cudaStream_t s);
 cudaError_t launch_validate(const glc_column* c, int* d_bad, cudaStream_t s);
 cudaError_t launch_max_bits(const glc_column* c, int64_t* d_out, cudaStream_t s);
+// pack.cu: one column's arrays for the packer
+struct PackArgs {
+  const int32_t* starts;
+  const int32_t* ends;
+  const int32_t* types;
+  const double* params;
+  const int32_t* bits;
+  const int64_t* offs;
+  int64_t P;
+  uint32_t* words;
+  int64_t nwords_alloc;
+};
+int64_t pack_tiles(int64_t nwords_alloc);
+cudaError_t launch_batch_pack(const PackArgs* cols, const void* const* values, const int32_t* dtypes,
+                              const int64_t* tile_base, int ncols, int64_t total_tiles, cudaStream_t s);
 // pack.cu
 cudaError_t launch_pack(glc_dtype dt, const void* values, glc_column* c, cudaStream_t s);
 // decode.cu: values (or residuals when residual_out) of positions [lo, hi) to out_base[lo..hi)
@@ -104,6 +120,32 @@ cudaError_t launch_decode(glc_ctx* ctx, const glc_column* c, int plain_src, int 
 // decode.cu: packed-source value decode with caller-supplied scratch; the counter must be zero.
 cudaError_t launch_decode_scratch(const glc_column* c, int64_t lo, int64_t hi, void* out_base, int* counter,
                                   int* err, int num_sms, cudaStream_t s);
+// decode.cu: batched decode over a device work list (many columns, mixed element types)
+struct BatchColumn {
+  const PartDesc* desc;
+  const int32_t* starts;
+  const TileInfo* tiles;
+  const uint32_t* words;
+  int64_t n;
+  int32_t dtype;
+  int32_t max_bits;
+};
+struct BatchWork {
+  int32_t col;
+  int32_t tile;    // tile of that column
+  int64_t lo, hi;  // element range of the column decoded by this item (clipped to the tile)
+  void* out_base;  // element e of the column is written to out_base[e] (16-byte aligned)
+};
+struct BatchDecodeArgs {
+  const BatchColumn* cols;
+  const BatchWork* work;
+  int64_t nwork;
+  unsigned long long* counter;  // work-item counter, zeroed per launch
+  int* err;
+  int stage_bytes;
+};
+cudaError_t launch_batch_decode(const BatchDecodeArgs& b, int num_sms, cudaStream_t s);
+int batch_stage_bytes(int max_bits);
 // random_access.cu
 cudaError_t launch_random_access(glc_ctx* ctx, const glc_column* c, int plain_src, const int32_t* pos,
                                  int64_t q, void* out, int32_t fixed_len, cudaStream_t s);

@@ -26,28 +26,17 @@ constexpr int kPackWords = 2048;
 constexpr int kPackThreads = 256;
 constexpr int kPackWarps = kPackThreads / 32;
 
-struct PackArgs {
-  const int32_t* starts;
-  const int32_t* ends;
-  const int32_t* types;
-  const double* params;
-  const int32_t* bits;
-  const int64_t* offs;
-  int64_t P;
-  uint32_t* words;
-  int64_t nwords_alloc;
-};
-
 __device__ __forceinline__ int64_t end_bit(const PackArgs& a, int64_t p) {
   return a.offs[p] + ((int64_t)a.ends[p] - a.starts[p]) * (int64_t)a.bits[p];
 }
 
-template <typename T> __global__ void __launch_bounds__(kPackThreads)
-pack_kernel(const T* __restrict__ v, PackArgs a) {
+// Builds output word tile `tile` (kPackWords words) of one column; every thread of the CTA calls it.
+template <typename T> __device__ __forceinline__ void pack_word_tile(const T* __restrict__ v, const PackArgs& a,
+                                                                    int64_t tile) {
   __shared__ __align__(16) uint32_t s_tile[kPackWords];
   __shared__ int64_t s_plo;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int64_t W0 = (int64_t)blockIdx.x * kPackWords;
+  const int64_t W0 = tile * kPackWords;
   const int64_t W1 = (W0 + kPackWords < a.nwords_alloc) ? W0 + kPackWords : a.nwords_alloc;
   const int tile_words = (int)(W1 - W0);
   const int64_t B0 = W0 * 32, B1 = W1 * 32;
@@ -132,6 +121,10 @@ pack_kernel(const T* __restrict__ v, PackArgs a) {
   for (int k = threadIdx.x; k < tile_words / 4; k += kPackThreads) dst[k] = src[k];
 }
 
+template <typename T> __global__ void __launch_bounds__(kPackThreads) pack_kernel(const T* __restrict__ v, PackArgs a) {
+  pack_word_tile<T>(v, a, blockIdx.x);
+}
+
 cudaError_t launch_pack(glc_dtype dt, const void* values, glc_column* c, cudaStream_t s) {
   if (c->nwords_alloc <= 0) return cudaSuccess;
   PackArgs a{c->d_start, c->d_end, c->d_types, c->d_params, c->d_bits, c->d_offs, c->P, c->d_words, c->nwords_alloc};
@@ -142,6 +135,35 @@ cudaError_t launch_pack(glc_dtype dt, const void* values, glc_column* c, cudaStr
     case GLC_U64: pack_kernel<uint64_t><<<grid, kPackThreads, 0, s>>>((const uint64_t*)values, a); break;
     case GLC_U32: pack_kernel<uint32_t><<<grid, kPackThreads, 0, s>>>((const uint32_t*)values, a); break;
   }
+  return cudaGetLastError();
+}
+
+// Batched pack: one CTA per output word tile of any column of a batch (PackArgs per column).
+__global__ void __launch_bounds__(kPackThreads)
+batch_pack_kernel(const PackArgs* __restrict__ cols, const void* const* __restrict__ values,
+                  const int32_t* __restrict__ dtypes, const int64_t* __restrict__ tile_base, int ncols) {
+  const int64_t t = blockIdx.x;
+  int lo = 0, hi = ncols - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (tile_base[mid] <= t) lo = mid; else hi = mid - 1;
+  }
+  const PackArgs a = cols[lo];
+  const int64_t tile = t - tile_base[lo];
+  switch (dtypes[lo]) {
+    case GLC_I32: pack_word_tile<int32_t>((const int32_t*)values[lo], a, tile); break;
+    case GLC_I64: pack_word_tile<int64_t>((const int64_t*)values[lo], a, tile); break;
+    case GLC_U64: pack_word_tile<uint64_t>((const uint64_t*)values[lo], a, tile); break;
+    default: pack_word_tile<uint32_t>((const uint32_t*)values[lo], a, tile); break;
+  }
+}
+
+int64_t pack_tiles(int64_t nwords_alloc) { return (nwords_alloc + kPackWords - 1) / kPackWords; }
+
+cudaError_t launch_batch_pack(const PackArgs* cols, const void* const* values, const int32_t* dtypes,
+                              const int64_t* tile_base, int ncols, int64_t total_tiles, cudaStream_t s) {
+  if (total_tiles <= 0) return cudaSuccess;
+  batch_pack_kernel<<<(unsigned)total_tiles, kPackThreads, 0, s>>>(cols, values, dtypes, tile_base, ncols);
   return cudaGetLastError();
 }
 

@@ -34,7 +34,8 @@ EXPORTS = [
     "glc_create", "glc_destroy", "glc_last_error", "glc_status_string", "glc_sync", "glc_compress",
     "glc_partition_variable", "glc_column_free", "glc_column_get_info", "glc_decompress_full",
     "glc_decompress_range", "glc_random_access", "glc_preunpack", "glc_blob_size", "glc_serialize",
-    "glc_deserialize", "glc_decompress_range_noalloc",
+    "glc_deserialize", "glc_decompress_range_noalloc", "glc_batch_create", "glc_batch_compress",
+    "glc_batch_column", "glc_batch_decompress", "glc_batch_free",
 ]
 NOALLOC_MAX_OUTPUT_BYTES = 4 << 20
 
@@ -88,6 +89,11 @@ def load() -> ctypes.CDLL:
         "glc_serialize": ([vp, vp, vp, u64, c_int, c_int, pu64, vp], c_int),
         "glc_deserialize": ([vp, c_int, vp, u64, c_int, c_int, c_int, pvp, vp], c_int),
         "glc_decompress_range_noalloc": ([vp, i64, i64, vp, vp], c_int),
+        "glc_batch_create": ([vp, vp, i32, pvp], c_int),
+        "glc_batch_compress": ([vp, vp, vp, vp, i32, i32, pvp, pi64, vp], c_int),
+        "glc_batch_column": ([vp, i32, pvp], c_int),
+        "glc_batch_decompress": ([vp, vp, vp, c_int, vp], c_int),
+        "glc_batch_free": ([vp], c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
@@ -240,6 +246,66 @@ def deserialize_host(ctx: Context, dtype: int, blob: bytes, pre_unpack: bool = F
         return None
     ctx.check(st)
     return Column(ctx, h)
+
+
+class BorrowedColumn(Column):
+    """A column owned by a batch: freed with the batch, never on its own."""
+
+    def free(self):
+        self.handle = None
+
+
+class Batch:
+    """Many columns per launch: batched compress and one-launch decode (glc_batch_*)."""
+
+    def __init__(self, ctx: Context, handle: ctypes.c_void_p, columns):
+        self.ctx = ctx
+        self.handle = handle
+        self.columns = columns
+
+    @classmethod
+    def compress(cls, ctx: Context, dtypes, dptrs, ns, fixed_len: int = 0, stream: int = 0):
+        n = len(dtypes)
+        dt = (ctypes.c_int * n)(*dtypes)
+        vp = (ctypes.c_void_p * n)(*dptrs)
+        nn = (ctypes.c_int64 * n)(*ns)
+        h = ctypes.c_void_p()
+        size = ctypes.c_int64()
+        ctx.check(ctx.lib.glc_batch_compress(ctx.handle, dt, vp, nn, n, fixed_len, ctypes.byref(h), ctypes.byref(size),
+                                             ctypes.c_void_p(stream)))
+        cols = []
+        for i in range(n):
+            c = ctypes.c_void_p()
+            ctx.check(ctx.lib.glc_batch_column(h, i, ctypes.byref(c)))
+            cols.append(BorrowedColumn(ctx, c))
+        b = cls(ctx, h, cols)
+        b.compressed_size = size.value
+        return b
+
+    @classmethod
+    def of(cls, ctx: Context, columns):
+        n = len(columns)
+        arr = (ctypes.c_void_p * n)(*[c.handle.value for c in columns])
+        h = ctypes.c_void_p()
+        ctx.check(ctx.lib.glc_batch_create(ctx.handle, arr, n, ctypes.byref(h)))
+        return cls(ctx, h, list(columns))
+
+    def decompress(self, out_ptrs, use_graph: bool = False, stream: int = 0):
+        n = len(self.columns)
+        arr = (ctypes.c_void_p * n)(*out_ptrs)
+        self.ctx.check(self.ctx.lib.glc_batch_decompress(self.ctx.handle, self.handle, arr, 1 if use_graph else 0,
+                                                         ctypes.c_void_p(stream)))
+
+    def free(self):
+        if self.handle:
+            self.ctx.lib.glc_batch_free(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
 
 
 # ---- the reference's class API -------------------------------------------------------------

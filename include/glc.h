@@ -166,6 +166,33 @@ GLC_API glc_status glc_serialize(glc_ctx* ctx, const glc_column* col, void* blob
 GLC_API glc_status glc_deserialize(glc_ctx* ctx, glc_dtype dtype, const void* blob, uint64_t size, int flags,
                            int crc32c, int pre_unpack, glc_column** out, glc_stream stream);
 
+/* ---- batches: many columns per launch (no counterpart in the reference) ----------------- */
+
+typedef struct glc_batch glc_batch;
+
+/* A batch over existing columns (not owned; they must outlive the batch). */
+GLC_API glc_status glc_batch_create(glc_ctx* ctx, glc_column* const* cols, int32_t ncols, glc_batch** out);
+
+/* Compress ncols device columns (values[i]: ns[i] elements of dtypes[i]) with fixed-length
+ * partitions in a fixed number of launches.  fixed_partition_len = 0 picks, per column, the length
+ * among 1024 / 2048 / 4096 with the smallest compressed size; otherwise 1..8192 for all.  Each
+ * column equals glc_compress of the same values with the same length.  The batch owns the
+ * columns (glc_batch_column); *compressed_size_bytes receives the sum of their reported sizes. */
+GLC_API glc_status glc_batch_compress(glc_ctx* ctx, const glc_dtype* dtypes, const void* const* values,
+                                      const int64_t* ns, int32_t ncols, int32_t fixed_partition_len,
+                                      glc_batch** out, int64_t* compressed_size_bytes, glc_stream stream);
+
+/* Borrowed handle of column i (valid while the batch lives; freed with it). */
+GLC_API glc_status glc_batch_column(const glc_batch* batch, int32_t i, glc_column** col);
+
+/* Decode every column of the batch (outs[i]: 16-byte aligned device buffer for column i) in ONE
+ * persistent launch over a device work list.  use_graph != 0 captures the launch in a CUDA graph
+ * on the first call and replays it while the outputs stay the same. */
+GLC_API glc_status glc_batch_decompress(glc_ctx* ctx, glc_batch* batch, void* const* outs, int use_graph,
+                                        glc_stream stream);
+
+GLC_API glc_status glc_batch_free(glc_batch* batch);
+
 /* ---- allocation-free range decode (no counterpart in the reference) --------------------- */
 
 /* Largest output, in bytes, of one glc_decompress_range_noalloc call:

@@ -1,0 +1,130 @@
+"""Batches of many columns per launch (glc_batch_*), checked against the single-column path.
+
+A column compressed in a batch must serialize to the same bytes as glc_compress of the same
+values with the same fixed partition length (and therefore match the oracle); the one-launch
+batched decode, plain and replayed from a CUDA graph, must return every column exactly.
+"""
+import numpy as np
+import pytest
+import torch
+
+import glc
+
+pytestmark = pytest.mark.gpu
+
+DT = {glc.I32: (np.int32, torch.int32), glc.I64: (np.int64, torch.int64), glc.U64: (np.uint64, torch.int64),
+      glc.U32: (np.uint32, torch.int32)}
+
+
+def _columns(ncols, seed=0, max_len=300_000):
+    rng = np.random.default_rng(seed)
+    cols = []
+    for c in range(ncols):
+        dt = [glc.I32, glc.I64, glc.U64, glc.U32][c % 4]
+        n = int(rng.choice([0, 1, 7, 128, 4095, 4096, 4097, int(rng.integers(1, max_len))]))
+        i = np.arange(n, dtype=np.int64)
+        w = int(rng.integers(0, 21))
+        noise = rng.integers(0, 1 << w, n) if w else np.zeros(n, np.int64)
+        if dt in (glc.I32, glc.U32):
+            slope = int(rng.integers(0, 400))
+            v = (int(rng.integers(0, 1 << 20)) + slope * i + noise) % (1 << 31)
+        else:
+            slope = int(rng.integers(0, 10_000))
+            v = int(rng.integers(0, 1 << 40)) + slope * i + noise
+            if c % 11 == 0 and dt == glc.U64 and n > 5:  # some values above 2^53: direct copy
+                v = v + (1 << 60)
+        cols.append((dt, v.astype(DT[dt][0])))
+    return cols
+
+
+def _to_device(values):
+    return torch.from_numpy(values.view(np.int64) if values.dtype.itemsize == 8 else values.view(np.int32)).cuda()
+
+
+@pytest.mark.parametrize("fixed_len", [0, 1024, 3000])
+def test_batch_compress_matches_single_column(oracle, fixed_len):
+    ctx = glc.Context(0)
+    cols = _columns(40, seed=fixed_len)
+    dev = [_to_device(v) for _, v in cols]
+    batch = glc.Batch.compress(ctx, [d for d, _ in cols], [t.data_ptr() for t in dev], [len(v) for _, v in cols],
+                               fixed_len=fixed_len)
+    total = 0
+    for (dt, v), bc in zip(cols, batch.columns):
+        info = bc.info()
+        assert info.total_values == len(v)
+        L = info.fixed_partition_len
+        if fixed_len:
+            assert L == fixed_len
+        else:
+            assert L in (1024, 2048, 4096)
+        if len(v) == 0:
+            continue
+        total += info.compressed_size_bytes
+        single = glc.compress_device(ctx, dt, v.ctypes.data, len(v), glc.FIXED, fixed_len=L, host=True)
+        blob = glc.serialize_host(ctx, bc)
+        assert blob == glc.serialize_host(ctx, single)
+        assert blob == oracle.serialize(oracle.compress(v, "fixed", L))
+        single.free()
+    assert batch.compressed_size == total
+    batch.free()
+
+
+@pytest.mark.parametrize("use_graph", [False, True])
+def test_batch_decode(use_graph):
+    ctx = glc.Context(0)
+    cols = _columns(60, seed=7)
+    dev = [_to_device(v) for _, v in cols]
+    batch = glc.Batch.compress(ctx, [d for d, _ in cols], [t.data_ptr() for t in dev], [len(v) for _, v in cols])
+    outs = [torch.full((max(len(v), 1) + 4,), -1, dtype=DT[dt][1], device="cuda:0") for dt, v in cols]
+    for rep in range(3):  # replays of the same graph / launch
+        for o in outs:
+            o.fill_(-1)
+        batch.decompress([o.data_ptr() for o in outs], use_graph=use_graph)
+        ctx.sync()
+        torch.cuda.synchronize()
+        for (dt, v), o in zip(cols, outs):
+            got = o.cpu().numpy().view(DT[dt][0])[: len(v)]
+            assert np.array_equal(got, v), (rep, dt, len(v))
+    # new outputs rebuild the work list (and the graph)
+    outs2 = [torch.zeros(max(len(v), 1), dtype=DT[dt][1], device="cuda:0") for dt, v in cols]
+    batch.decompress([o.data_ptr() for o in outs2], use_graph=use_graph)
+    torch.cuda.synchronize()
+    for (dt, v), o in zip(cols, outs2):
+        assert np.array_equal(o.cpu().numpy().view(DT[dt][0])[: len(v)], v)
+    batch.free()
+
+
+def test_batch_over_existing_columns():
+    ctx = glc.Context(0)
+    cols = _columns(12, seed=3)
+    singles = [glc.compress_device(ctx, dt, v.ctypes.data, len(v), glc.VARIABLE, host=True) for dt, v in cols]
+    batch = glc.Batch.of(ctx, singles)
+    outs = [torch.zeros(max(len(v), 1), dtype=DT[dt][1], device="cuda:0") for dt, v in cols]
+    batch.decompress([o.data_ptr() for o in outs], use_graph=True)
+    torch.cuda.synchronize()
+    for (dt, v), o in zip(cols, outs):
+        assert np.array_equal(o.cpu().numpy().view(DT[dt][0])[: len(v)], v)
+    batch.free()
+    for s in singles:
+        s.free()
+
+
+def test_batch_column_random_access_and_range():
+    ctx = glc.Context(0)
+    cols = _columns(8, seed=11)
+    dev = [_to_device(v) for _, v in cols]
+    batch = glc.Batch.compress(ctx, [d for d, _ in cols], [t.data_ptr() for t in dev], [len(v) for _, v in cols])
+    for (dt, v), bc in zip(cols, batch.columns):
+        if len(v) == 0:
+            continue
+        pos = np.random.default_rng(1).integers(0, len(v), 1000).astype(np.int32)
+        out = np.zeros(len(pos), DT[dt][0])
+        glc.random_access_into(ctx, bc, pos.ctypes.data, len(pos), out.ctypes.data, host_in=True, host_out=True)
+        assert np.array_equal(out, v[pos])
+        first = len(v) // 3
+        r = np.zeros(len(v) - first, DT[dt][0])
+        glc.decompress_range_into(ctx, bc, first, len(r), r.ctypes.data, host_out=True)
+        assert np.array_equal(r, v[first:])
+    with pytest.raises(glc.GlcError):
+        ctx.check(ctx.lib.glc_column_free(batch.columns[0].handle))  # owned by the batch
+    batch.free()
