@@ -465,6 +465,326 @@ def run_batch(args):
     return 0
 
 
+def device_piecewise_u64(n: int, seed: int, dev):
+    """The piecewise-linear uint64 distribution of glc.workloads.piecewise_linear, generated on the
+    device: segment lengths ~ Poisson(50,000), slope U{1..10^6}, intercept jump U{0..2^40}, noise
+    U[0, 2^b) with b in {0,4,8,16,24}.  Values stay below 2^63 (returned as int64 bit patterns)."""
+    import torch
+    g = torch.Generator(device=dev)
+    g.manual_seed(seed)
+    S = n // 50_000 * 2 + 64
+    lens = torch.poisson(torch.full((S,), 50_000.0, device=dev), generator=g).clamp_min(1).to(torch.int64)
+    ends = torch.cumsum(lens, 0)
+    S = int(torch.searchsorted(ends, torch.tensor([n], device=dev)).item()) + 1
+    lens = lens[:S].clone()
+    lens[-1] -= int(ends[S - 1].item()) - n
+    starts = torch.cumsum(lens, 0) - lens
+    slope = torch.randint(1, 1_000_001, (S,), device=dev, generator=g, dtype=torch.int64)
+    jump = torch.randint(0, (1 << 40) + 1, (S,), device=dev, generator=g, dtype=torch.int64)
+    bsel = torch.tensor([0, 4, 8, 16, 24], device=dev)[torch.randint(0, 5, (S,), device=dev, generator=g)]
+    span = slope * (lens - 1)
+    base = torch.cumsum(jump, 0) + torch.cumsum(span, 0) - span
+    seg = torch.repeat_interleave(torch.arange(S, device=dev), lens)
+    j = torch.arange(n, device=dev, dtype=torch.int64) - starts[seg]
+    v = base[seg] + slope[seg] * j
+    del j
+    noise = torch.randint(0, 1 << 24, (n,), device=dev, generator=g, dtype=torch.int64)
+    v += noise & ((torch.ones_like(noise) << bsel[seg]) - 1)
+    return v
+
+
+def device_timestamps_i64(n: int, seed: int, dev):
+    """Cumulative sums of exponential gaps (mean 1000) rounded to integers, starting at 0."""
+    import torch
+    g = torch.Generator(device=dev)
+    g.manual_seed(seed)
+    gaps = torch.empty(n, device=dev, dtype=torch.float64).exponential_(1.0 / 1000.0, generator=g)
+    gaps = torch.round(gaps).to(torch.int64)
+    gaps[0] = 0
+    return torch.cumsum(gaps, 0)
+
+
+def device_linear_i32(n: int, seed: int, dev):
+    """intercept + slope * i + noise with slope U[0, 10^4] capped to stay inside int32, noise
+    U[0, 2^w) with w U{0..20} (one column of the batched workload's distribution)."""
+    import torch
+    rng = np.random.default_rng(seed)
+    slope = min(int(rng.integers(0, 10_001)), (2 ** 30) // n)
+    w = int(rng.integers(0, 21))
+    g = torch.Generator(device=dev)
+    g.manual_seed(seed)
+    v = int(rng.integers(0, 1 << 20)) + slope * torch.arange(n, device=dev, dtype=torch.int64)
+    if w:
+        v += torch.randint(0, 1 << w, (n,), device=dev, generator=g, dtype=torch.int64)
+    return v.to(torch.int32)
+
+
+# Serving column sources: (name, dtype code, values, partitioning, fixed length, columns admitted)
+SERVE_SOURCES = [("piecewise_u64_600M_variable", "U64", 600_000_000, "VARIABLE", 0, 32),
+                 ("timestamps_i64_256M_fixed4096", "I64", 256_000_000, "FIXED", 4096, 16),
+                 ("linear_i32_16M_fixed2048", "I32", 16_000_000, "FIXED", 2048, 16)]
+
+
+def _pct(a, q):
+    return float(np.percentile(a, q)) if len(a) else None
+
+
+def run_serving(args):
+    """Serving: 64 resident compressed columns (32 piecewise uint64 of 600M values, 16 int64
+    timestamp columns of 256M, 16 int32 linear+noise columns of 16M; about 40 GB resident under a
+    60 GB admission budget), driven by open-loop Poisson request streams at swept rates.  A request
+    is a lookup of floor(exp(U[0, ln 65,536])) positions (uniform over the column) or a range
+    decode of floor(exp(U[ln 1,024, ln 16M])) values, 50/50; during every rate point new columns
+    are admitted and the least recently used idle ones evicted.  Latency = completion seen by the
+    server minus the request's scheduled arrival.  The comparison is the plain per-call form:
+    one glc_random_access call per lookup request on one stream, back to back."""
+    import ctypes
+
+    import torch
+
+    import glc
+
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.Stream(dev)
+    torch.cuda.set_stream(stream)
+    sh = stream.cuda_stream
+    ctx = glc.Context(local)
+    scale = args.serve_scale
+    gens = {"U64": device_piecewise_u64, "I64": device_timestamps_i64, "I32": device_linear_i32}
+    sources = []
+    t_build = time.perf_counter()
+    for k, (name, dt, n, mode, L, copies) in enumerate(SERVE_SOURCES):
+        n = max(8192, int(n * scale))
+        v = gens[dt](n, 42 + k, dev)
+        code = getattr(glc, dt)
+        col = glc.compress_device(ctx, code, v.data_ptr(), n, getattr(glc, mode), fixed_len=L or 4096, stream=sh)
+        size = ctypes.c_uint64()
+        ctx.check(ctx.lib.glc_blob_size(col.handle, ctypes.byref(size)))
+        blob = torch.empty(int(size.value), dtype=torch.uint8, device=dev)
+        wrote = ctypes.c_uint64()
+        ctx.check(ctx.lib.glc_serialize(ctx.handle, col.handle, ctypes.c_void_p(blob.data_ptr()), size.value, 0, 0,
+                                        ctypes.byref(wrote), ctypes.c_void_p(sh)))
+        pool = torch.randint(0, n, (1 << 24,), device=dev, dtype=torch.int32)
+        # a few known values to check the served results against
+        sources.append(dict(name=name, code=code, n=n, col=col, blob=blob, pool=pool, copies=copies,
+                            esize=4 if dt == "I32" else 8, check=v[:1 << 20].clone(),
+                            bits=col.info().total_bits / n))
+        del v
+    torch.cuda.synchronize(dev)
+    torch.cuda.empty_cache()
+    budget = int(60e9 * scale) if scale < 1 else int(60e9)
+    server = glc.Server(ctx, budget_bytes=budget, slots=args.slots)
+    ids, src_of = [], {}
+    t0 = time.perf_counter()
+    for si, s in enumerate(sources):
+        for _ in range(s["copies"]):
+            cid = server.admit_blob(s["code"], s["blob"].data_ptr(), s["blob"].numel(), stream=sh)
+            ids.append(cid)
+            src_of[cid] = si
+    admit_s = time.perf_counter() - t0
+    st = server.stats()
+    resident_gb = st.resident_bytes / 1e9
+    build_s = time.perf_counter() - t_build
+    lk_arena = torch.empty(1 << 28, dtype=torch.uint8, device=dev)
+    rg_arena = torch.empty(4 << 30, dtype=torch.uint8, device=dev)
+
+    def make_stream(rate, lookup_frac, nreq, seed, resident):
+        rng = np.random.default_rng(seed)
+        req = glc.requests(nreq)
+        hot = rng.choice(np.array(resident), min(48, len(resident)), replace=False)
+        col = hot[rng.integers(0, len(hot), nreq)]
+        is_lk = rng.random(nreq) < lookup_frac
+        si = np.array([src_of[int(c)] for c in col])
+        n_of = np.array([s["n"] for s in sources])[si]
+        es = np.array([s["esize"] for s in sources])[si]
+        cnt_l = np.clip(np.floor(np.exp(rng.uniform(0, np.log(65536), nreq))), 1, 65536).astype(np.int64)
+        cnt_r = np.floor(np.exp(rng.uniform(np.log(1024), np.log(16 << 20), nreq))).astype(np.int64)
+        cnt_r = np.minimum(cnt_r, n_of)
+        cnt = np.where(is_lk, cnt_l, cnt_r)
+        first = np.where(is_lk, 0, (rng.random(nreq) * (n_of - cnt + 1)).astype(np.int64))
+        pool_base = np.array([s["pool"].data_ptr() for s in sources], np.uint64)[si]
+        pool_off = (rng.random(nreq) * ((1 << 24) - cnt_l)).astype(np.uint64) * np.uint64(4)
+        # outputs: consecutive slices of two arenas (wrapping); ranges placed so that
+        # out - first * esize is 16-byte aligned (decoded in place)
+        nbytes = cnt * es
+        lk_off = np.cumsum(np.where(is_lk, (nbytes + 15) // 16 * 16, 0)) % ((1 << 28) - (1 << 20))
+        rg_need = np.where(is_lk, 0, (nbytes + 31) // 16 * 16)
+        rg_off = (np.cumsum(rg_need) % ((4 << 30) - (256 << 20))) // 16 * 16 + ((first * es) % 16)
+        out = np.where(is_lk, np.uint64(lk_arena.data_ptr()) + lk_off.astype(np.uint64),
+                       np.uint64(rg_arena.data_ptr()) + rg_off.astype(np.uint64))
+        req["kind"] = np.where(is_lk, glc.REQ_LOOKUP, glc.REQ_RANGE)
+        req["column"] = col
+        req["first"] = first
+        req["count"] = cnt
+        req["positions"] = np.where(is_lk, pool_base + pool_off, 0)
+        req["out"] = out
+        req["tag"] = np.arange(nreq)
+        gaps = rng.exponential(1e9 / rate, nreq)
+        start = server.now_ns() + 50_000_000 + nreq * 300
+        req["not_before_ns"] = start + np.cumsum(gaps).astype(np.int64)
+        return req, si, es
+
+    def run_point(rate, lookup_frac, seed, admit_during):
+        nonlocal ids
+        nreq = int(np.clip(rate * args.serve_seconds, 4000, 500_000))
+        req, si, es = make_stream(rate, lookup_frac, nreq, seed, ids)
+        before = server.stats()
+        server.submit(req)
+        admitted, refused, adm_t = 0, 0, 0.0
+        if admit_during:  # new columns arrive while the stream runs; LRU idle columns make room
+            time.sleep(max(0.0, (int(req["not_before_ns"][0]) - server.now_ns()) / 1e9))
+            for k in range(admit_during):
+                s = sources[0]  # the largest columns
+                ta = time.perf_counter()
+                try:
+                    cid = server.admit_blob(s["code"], s["blob"].data_ptr(), s["blob"].numel(), stream=sh)
+                    src_of[cid] = 0
+                    admitted += 1
+                except glc.GlcError as ex:
+                    if ex.status != glc.ERR_BUDGET:
+                        raise
+                    refused += 1
+                adm_t += time.perf_counter() - ta
+        server.drain(600_000)
+        after = server.stats()
+        ids = server.columns()
+        recs = []
+        while True:
+            r = server.poll()
+            if len(r) == 0:
+                break
+            recs.append(r)
+        recs = np.concatenate(recs)
+        assert len(recs) == nreq and np.all(recs["status"] == glc.OK), "served request failed"
+        order = np.argsort(recs["tag"])
+        recs = recs[order]
+        lat_us = (recs["done_ns"] - recs["arrival_ns"]) / 1e3
+        is_lk = req["kind"] == glc.REQ_LOOKUP
+        span_s = (recs["done_ns"].max() - recs["arrival_ns"].min()) / 1e9
+        lookups = int(req["count"][is_lk].sum())
+        rvals = req["count"][~is_lk]
+        rbytes = float((rvals * es[~is_lk]).sum())
+        return {"rate_req_s": rate, "requests": nreq, "lookup_share": lookup_frac,
+                "lookup_p50_us": round(_pct(lat_us[is_lk], 50), 1) if is_lk.any() else None,
+                "lookup_p99_us": round(_pct(lat_us[is_lk], 99), 1) if is_lk.any() else None,
+                "range_p50_us": round(_pct(lat_us[~is_lk], 50), 1) if (~is_lk).any() else None,
+                "range_p99_us": round(_pct(lat_us[~is_lk], 99), 1) if (~is_lk).any() else None,
+                "lookups_per_s": round(lookups / span_s, 1), "range_gb_s": round(rbytes / span_s / 1e9, 2),
+                "launches": after.launches - before.launches,
+                "requests_per_launch": round(nreq / max(1, after.launches - before.launches), 2),
+                "span_s": round(span_s, 4), "admitted_during": admitted, "refused_during": refused,
+                "admit_s": round(adm_t, 3), "evictions": after.evictions - before.evictions}
+
+    # bit-exactness of served results: one lookup and one range request per source, checked
+    chk_ok = True
+    for si, s in enumerate(sources):
+        cid = [c for c in ids if src_of[c] == si][0]
+        pos = torch.randint(0, s["check"].numel(), (4096,), device=dev, dtype=torch.int32)
+        lo = torch.zeros(4096, dtype=s["check"].dtype, device=dev)
+        ro = torch.zeros(s["check"].numel(), dtype=s["check"].dtype, device=dev)
+        r = glc.requests(2)
+        r[0] = (glc.REQ_LOOKUP, cid, 0, 4096, pos.data_ptr(), lo.data_ptr(), 0, 0)
+        r[1] = (glc.REQ_RANGE, cid, 0, s["check"].numel(), 0, ro.data_ptr(), 1, 0)
+        server.submit(r)
+        server.drain(60_000)
+        server.poll()
+        torch.cuda.synchronize(dev)
+        chk_ok &= bool(torch.equal(lo, s["check"][pos.long()])) and bool(torch.equal(ro, s["check"]))
+
+    rates = [float(x) for x in args.rates.split(",")]
+    ra_rates = [float(x) for x in args.ra_rates.split(",")] if args.ra_rates else []
+    clocks = ClockSampler(dev)
+    clocks.start()
+    sweep = []
+    for k, rate in enumerate(rates):
+        sweep.append(run_point(rate, 0.5, 100 + k, admit_during=4))
+    ra_sweep = []
+    for k, rate in enumerate(ra_rates):
+        ra_sweep.append(run_point(rate, 1.0, 200 + k, admit_during=0))
+    clk = clocks.stop()
+
+    # the plain per-call form: the same kind of stream, one libglc call per request from a C++ loop
+    pc_lib = ctypes.CDLL(os.path.join(ROOT, "g-leco_b200", "_build", "libglc_percall.so"))
+    src_handles = (ctypes.c_void_p * len(sources))(*[s["col"].handle.value for s in sources])
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+
+    def per_call(lookup_frac, nreq, seed):
+        req, si, es = make_stream(1e6, lookup_frac, nreq, seed, ids)
+        arrs = [np.ascontiguousarray(req["kind"]), si.astype(np.int32), np.ascontiguousarray(req["first"]),
+                np.ascontiguousarray(req["count"]), np.ascontiguousarray(req["positions"]),
+                np.ascontiguousarray(req["out"])]
+
+        def go(k):
+            rc = pc_lib.percall_run(ctx.handle, src_handles, ctypes.c_int32(k),
+                                    *[ctypes.c_void_p(a.ctypes.data) for a in arrs], ctypes.c_void_p(sh))
+            if rc != 0:
+                raise RuntimeError(f"per-call loop failed with status {rc}")
+        go(min(200, nreq))
+        torch.cuda.synchronize(dev)
+        e0.record(stream)
+        go(nreq)
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        secs = e0.elapsed_time(e1) / 1e3
+        is_lk = req["kind"] == glc.REQ_LOOKUP
+        return {"requests": nreq, "lookup_share": lookup_frac, "seconds": round(secs, 4),
+                "requests_per_s": round(nreq / secs, 1),
+                "lookups_per_s": round(float(req["count"][is_lk].sum()) / secs, 1),
+                "range_gb_s": round(float((req["count"][~is_lk] * es[~is_lk]).sum()) / secs / 1e9, 2)}
+
+    pc_lookups = per_call(1.0, 20_000, 7)
+    pc_mix = per_call(0.5, 4_000, 8)
+    per_call_lps = pc_lookups["lookups_per_s"]
+
+    def ok_point(p):
+        return p["lookup_p99_us"] is not None and p["lookup_p99_us"] <= 1000.0
+    good = [p for p in sweep + ra_sweep if ok_point(p)]
+    best = max(good, key=lambda p: p["lookups_per_s"]) if good else None
+    value = best["lookups_per_s"] if best else 0.0
+    peak, peak_kind = measured_peak()
+    if best:
+        bpv = {i: sources[i]["bits"] / 8 for i in range(len(sources))}
+        alg = best["lookups_per_s"] * 44 + best["range_gb_s"] * 1e9 * (1 + float(np.mean(list(bpv.values()))) / 8)
+    else:
+        alg = 0.0
+    st = server.stats()
+    line = {
+        "metric": "served lookups/s at lookup p99 <= 1 ms", "value": round(value, 1), "unit": "lookups/s",
+        "n_gpus": 1, "steps": len(sweep) + len(ra_sweep), "warmup": args.warmup,
+        "ms_per_step": round(1e3 * (best["span_s"] if best else 0.0), 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "mixed int32/int64/uint64", "data": "synthetic",
+        "config": {"workload": "serving_64_columns_poisson", "columns": len(ids), "resident_gb": round(resident_gb, 2),
+                   "budget_gb": round(budget / 1e9, 1), "slots": args.slots,
+                   "sources": [f"{s['copies']} x {s['name']}" for s in sources],
+                   "lookup_sizes": "floor(exp(U[0, ln 65536])) positions, uniform over the column",
+                   "range_sizes": "floor(exp(U[ln 1024, ln 16M])) values",
+                   "mix": "50/50 lookup/range (sweep); lookups only (ra_sweep)",
+                   "admission_s": round(admit_s, 2), "build_s": round(build_s, 1), "bit_exact": chk_ok,
+                   "best_point": best, "sweep": sweep, "ra_sweep": ra_sweep,
+                   "per_call_lookups_per_s": round(per_call_lps, 1),
+                   "per_call": {"form": "one glc_random_access / glc_decompress_range call per request from a "
+                                        "C++ loop, one stream, back to back (device time)",
+                                "lookups_only": pc_lookups, "mix_50_50": pc_mix},
+                   "served_over_per_call": round(value / per_call_lps, 2) if per_call_lps else None,
+                   "evictions_total": st.evictions, "admissions_refused_total": st.admissions_refused,
+                   "l2": "columns, positions and outputs far larger than L2"},
+        "roofline": {"bound": "hbm", "achieved": round(alg / 1e9, 1), "peak": peak, "unit": "GB/s",
+                     "frac": round(alg / 1e9 / peak, 4), "peak_kind": peak_kind, "traffic": None,
+                     "basis": "whole served stream at the best point: 44 B per lookup + range bytes written "
+                              "and read, over the stream's span"},
+        "e2e": None, "gpu_launches": int(st.launches), "clocks": clk, "cpu_baseline": None,
+    }
+    print(json.dumps(line), flush=True)
+    server.close()
+    for s in sources:
+        s["col"].free()
+    ctx.close()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -475,11 +795,17 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--columns", type=int, default=4096, help="c4 batch: number of columns")
-    ap.add_argument("--workload", default="c2_decode", choices=["c2_decode", "c3_random_access", "c4_batch"],
+    ap.add_argument("--workload", default="c2_decode",
+                    choices=["c2_decode", "c3_random_access", "c4_batch", "c5_serving"],
                     help="c2_decode (headline): full decode of the 200M piecewise uint64 column; "
                          "c3_random_access: 100M lookups into a 64M int64 timestamp column")
     ap.add_argument("--mode", default="packed", choices=["packed", "preunpacked"], help="c3 residual source")
     ap.add_argument("--queries", type=int, default=100_000_000, help="c3 lookups per step")
+    ap.add_argument("--rates", default="10000,30000,100000,300000,1000000", help="c5: request rates (req/s)")
+    ap.add_argument("--ra-rates", default="1000000,2000000,4000000", help="c5: lookup-only request rates")
+    ap.add_argument("--serve-seconds", type=float, default=0.5, help="c5: scheduled duration per rate")
+    ap.add_argument("--serve-scale", type=float, default=1.0, help="c5: column length scale (1 = full size)")
+    ap.add_argument("--slots", type=int, default=4, help="c5: shared launches in flight")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -489,6 +815,8 @@ def main():
         return run_random_access(args)
     if args.workload == "c4_batch":
         return run_batch(args)
+    if args.workload == "c5_serving":
+        return run_serving(args)
 
     import torch
     import torch.distributed as dist

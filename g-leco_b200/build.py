@@ -50,7 +50,25 @@ def build(verbose_ptxas: bool = False) -> str:
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{r.stderr}")
     build_dropin()
+    build_percall()
     return OUT
+
+
+def build_percall() -> str:
+    """Compile the per-call request loop the serving benchmark compares against
+    (g-leco_b200/percall/percall.cpp -> _build/libglc_percall.so, linked to libglc)."""
+    src = os.path.join(HERE, "percall", "percall.cpp")
+    so = os.path.join(BUILD, "libglc_percall.so")
+    hdr = os.path.join(ROOT, "include", "glc.h")
+    if os.path.exists(so) and all(os.path.getmtime(so) >= os.path.getmtime(d) for d in (src, OUT, hdr)):
+        return so
+    cmd = [os.environ.get("CXX", "g++"), "-std=c++17", "-O2", "-shared", "-fPIC", "-fvisibility=hidden",
+           "-I" + os.path.join(ROOT, "include"), src, "-L" + os.path.dirname(OUT), "-lglc",
+           "-Wl,-rpath,$ORIGIN/../glc", "-o", so]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"per-call loop failed to compile:\n{r.stderr}")
+    return so
 
 
 def build_dropin() -> str:

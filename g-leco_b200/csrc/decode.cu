@@ -444,7 +444,7 @@ __global__ void __launch_bounds__(kPCThreads) batch_decode_kernel(BatchDecodeArg
   }
 }
 
-cudaError_t launch_batch_decode(const BatchDecodeArgs& b, int num_sms, cudaStream_t s) {
+static cudaError_t batch_decode_go(const BatchDecodeArgs& b, int num_sms, bool zero, cudaStream_t s) {
   if (b.nwork <= 0) return cudaSuccess;
   void (*kern)(BatchDecodeArgs) = batch_decode_kernel<kDefaultStages>;
   const size_t smem = (size_t)kDefaultStages * b.stage_bytes;
@@ -455,9 +455,17 @@ cudaError_t launch_batch_decode(const BatchDecodeArgs& b, int num_sms, cudaStrea
   if (per_sm < 1) per_sm = 1;
   int64_t grid = (int64_t)per_sm * num_sms;
   if (grid > b.nwork) grid = b.nwork;
-  if ((e = cudaMemsetAsync(b.counter, 0, sizeof(unsigned long long), s)) != cudaSuccess) return e;
+  if (zero && (e = cudaMemsetAsync(b.counter, 0, sizeof(unsigned long long), s)) != cudaSuccess) return e;
   kern<<<(unsigned)grid, kPCThreads, smem, s>>>(b);
   return cudaGetLastError();
+}
+
+cudaError_t launch_batch_decode(const BatchDecodeArgs& b, int num_sms, cudaStream_t s) {
+  return batch_decode_go(b, num_sms, true, s);
+}
+
+cudaError_t launch_batch_decode_zeroed(const BatchDecodeArgs& b, int num_sms, cudaStream_t s) {
+  return batch_decode_go(b, num_sms, false, s);
 }
 
 int batch_stage_bytes(int max_bits) {

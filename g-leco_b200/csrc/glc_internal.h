@@ -145,10 +145,30 @@ struct BatchDecodeArgs {
   int stage_bytes;
 };
 cudaError_t launch_batch_decode(const BatchDecodeArgs& b, int num_sms, cudaStream_t s);
+// Same launch without zeroing the work counter first (the caller's stream has zeroed it).
+cudaError_t launch_batch_decode_zeroed(const BatchDecodeArgs& b, int num_sms, cudaStream_t s);
 int batch_stage_bytes(int max_bits);
 // random_access.cu
 cudaError_t launch_random_access(glc_ctx* ctx, const glc_column* c, int plain_src, const int32_t* pos,
                                  int64_t q, void* out, int32_t fixed_len, cudaStream_t s);
+// random_access.cu: lookups of many requests into many columns (serving)
+struct RAColumn {
+  const PartDesc* desc;
+  const int32_t* starts;
+  const uint32_t* words;
+  int64_t P, n;
+  int32_t fixed_len;  // > 0: partition = pos / fixed_len
+  int32_t dtype;
+};
+struct RARequest {
+  int64_t base;         // first lookup of the request in the launch
+  int32_t col;          // index into the launch's column table
+  int32_t pad;
+  const int32_t* pos;   // the request's positions
+  uint8_t* out;         // value k goes to out + k * element size
+};
+cudaError_t launch_multi_lookup(const RAColumn* cols, const RARequest* reqs, int nreq, int64_t total, int num_sms,
+                                cudaStream_t s);
 // partition.cu: allocates *d_starts / *d_ends (cudaMallocAsync on s)
 cudaError_t launch_partition_variable(glc_ctx* ctx, glc_dtype dt, const void* values, int64_t n,
                                       int32_t** d_starts, int32_t** d_ends, int64_t* P, cudaStream_t s,

@@ -214,4 +214,67 @@ cudaError_t launch_random_access(glc_ctx* ctx, const glc_column* c, int plain_sr
   return cudaErrorInvalidValue;
 }
 
+// ---------------------------------------------------------------------------------------
+// Lookups of many requests into many columns in one launch (the serving path).  Lookup i
+// belongs to the request whose [base, base + count) holds i; the request names the column and
+// where its values go (device or staging memory, byte offset).
+// ---------------------------------------------------------------------------------------
+template <typename T>
+__device__ __forceinline__ void lookup_one(const RAColumn& c, int64_t pos, uint8_t* out) {
+  T v = (T)0;
+  if (pos >= 0 && pos < c.n) {
+    int64_t p;
+    if (c.fixed_len > 0) {
+      p = pos / c.fixed_len;
+      p = p < c.P ? p : c.P - 1;
+    } else {
+      int64_t lo = 0, hi = c.P - 1;
+      while (lo < hi) {
+        const int64_t mid = (lo + hi + 1) >> 1;
+        if ((int64_t)__ldg(c.starts + mid) <= pos) lo = mid; else hi = mid - 1;
+      }
+      p = lo;
+    }
+    const PartDesc d = load_desc(c.desc + p);
+    const int bits = d.bits_type & 0xff, type = d.bits_type >> 8;
+    const int64_t local = pos - d.start;
+    const uint64_t f = bits > 0 ? read_field_global(c.words, d.bit_off + local * bits, bits) : 0ull;
+    if (type == MODEL_DIRECT_COPY) v = (T)f;
+    else v = apply_delta<T>(predict<T>(d.theta0, d.theta1, local), sign_extend(f, bits));
+  }
+  *reinterpret_cast<T*>(out) = v;
+}
+
+__global__ void __launch_bounds__(256)
+multi_lookup_kernel(const RAColumn* __restrict__ cols, const RARequest* __restrict__ reqs, int nreq,
+                    int64_t total) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
+    int lo = 0, hi = nreq - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (reqs[mid].base <= i) lo = mid; else hi = mid - 1;
+    }
+    const RARequest r = reqs[lo];
+    const RAColumn c = cols[r.col];
+    const int64_t k = i - r.base;
+    const int64_t pos = __ldg(r.pos + k);
+    switch (c.dtype) {
+      case GLC_I32: lookup_one<int32_t>(c, pos, r.out + 4 * k); break;
+      case GLC_U32: lookup_one<uint32_t>(c, pos, r.out + 4 * k); break;
+      case GLC_I64: lookup_one<int64_t>(c, pos, r.out + 8 * k); break;
+      default: lookup_one<uint64_t>(c, pos, r.out + 8 * k); break;
+    }
+  }
+}
+
+cudaError_t launch_multi_lookup(const RAColumn* cols, const RARequest* reqs, int nreq, int64_t total, int num_sms,
+                                cudaStream_t s) {
+  if (total <= 0) return cudaSuccess;
+  int64_t grid = (total + 255) / 256;
+  const int64_t cap = (int64_t)num_sms * 8;
+  if (grid > cap) grid = cap;
+  multi_lookup_kernel<<<(unsigned)grid, 256, 0, s>>>(cols, reqs, nreq, total);
+  return cudaGetLastError();
+}
+
 }  // namespace glc

@@ -35,8 +35,11 @@ EXPORTS = [
     "glc_partition_variable", "glc_column_free", "glc_column_get_info", "glc_decompress_full",
     "glc_decompress_range", "glc_random_access", "glc_preunpack", "glc_blob_size", "glc_serialize",
     "glc_deserialize", "glc_decompress_range_noalloc", "glc_batch_create", "glc_batch_compress",
-    "glc_batch_column", "glc_batch_decompress", "glc_batch_free",
+    "glc_batch_column", "glc_batch_decompress", "glc_batch_free", "glc_server_create", "glc_server_destroy",
+    "glc_server_admit", "glc_server_admit_blob", "glc_server_evict", "glc_server_submit", "glc_server_poll",
+    "glc_server_drain", "glc_server_get_stats", "glc_server_now_ns", "glc_server_columns",
 ]
+REQ_LOOKUP, REQ_RANGE = 0, 1
 NOALLOC_MAX_OUTPUT_BYTES = 4 << 20
 
 
@@ -57,6 +60,37 @@ class ColumnInfo(ctypes.Structure):
         ("delta_array", ctypes.c_void_p), ("d_plain_deltas", ctypes.c_void_p),
     ]
 
+
+class ServerConfig(ctypes.Structure):
+    _fields_ = [("budget_bytes", ctypes.c_uint64), ("slots", ctypes.c_int32), ("max_requests", ctypes.c_int32),
+                ("max_lookups", ctypes.c_int64), ("max_range_values", ctypes.c_int64)]
+
+
+class Request(ctypes.Structure):
+    _fields_ = [("kind", ctypes.c_int32), ("column", ctypes.c_int32), ("first", ctypes.c_int64),
+                ("count", ctypes.c_int64), ("positions", ctypes.c_void_p), ("out", ctypes.c_void_p),
+                ("tag", ctypes.c_int64), ("not_before_ns", ctypes.c_int64)]
+
+
+class Completion(ctypes.Structure):
+    _fields_ = [("tag", ctypes.c_int64), ("status", ctypes.c_int32), ("launches", ctypes.c_int32),
+                ("arrival_ns", ctypes.c_int64), ("done_ns", ctypes.c_int64)]
+
+
+class ServerStats(ctypes.Structure):
+    _fields_ = [("resident_bytes", ctypes.c_uint64), ("resident_columns", ctypes.c_int32),
+                ("in_flight", ctypes.c_int32), ("launches", ctypes.c_int64), ("submitted", ctypes.c_int64),
+                ("completed", ctypes.c_int64), ("lookups", ctypes.c_int64), ("range_values", ctypes.c_int64),
+                ("evictions", ctypes.c_int64), ("admissions_refused", ctypes.c_int64)]
+
+
+# numpy mirrors of the structures, for building many requests at once
+REQUEST_DTYPE = np.dtype([("kind", np.int32), ("column", np.int32), ("first", np.int64), ("count", np.int64),
+                          ("positions", np.uint64), ("out", np.uint64), ("tag", np.int64),
+                          ("not_before_ns", np.int64)])
+COMPLETION_DTYPE = np.dtype([("tag", np.int64), ("status", np.int32), ("launches", np.int32),
+                             ("arrival_ns", np.int64), ("done_ns", np.int64)])
+assert REQUEST_DTYPE.itemsize == ctypes.sizeof(Request) and COMPLETION_DTYPE.itemsize == ctypes.sizeof(Completion)
 
 _lib = None
 
@@ -94,6 +128,17 @@ def load() -> ctypes.CDLL:
         "glc_batch_column": ([vp, i32, pvp], c_int),
         "glc_batch_decompress": ([vp, vp, vp, c_int, vp], c_int),
         "glc_batch_free": ([vp], c_int),
+        "glc_server_create": ([vp, ctypes.POINTER(ServerConfig), pvp], c_int),
+        "glc_server_destroy": ([vp], c_int),
+        "glc_server_admit": ([vp, vp, ctypes.POINTER(i32)], c_int),
+        "glc_server_admit_blob": ([vp, c_int, vp, u64, c_int, ctypes.POINTER(i32), vp], c_int),
+        "glc_server_evict": ([vp, i32], c_int),
+        "glc_server_submit": ([vp, vp, i32], c_int),
+        "glc_server_poll": ([vp, vp, i32, ctypes.POINTER(i32)], c_int),
+        "glc_server_drain": ([vp, i64], c_int),
+        "glc_server_get_stats": ([vp, ctypes.POINTER(ServerStats)], c_int),
+        "glc_server_now_ns": ([], i64),
+        "glc_server_columns": ([vp, vp, i32, ctypes.POINTER(i32)], c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
@@ -306,6 +351,83 @@ class Batch:
             self.free()
         except Exception:
             pass
+
+
+class Server:
+    """Resident columns and continuously batched requests (glc_server_*)."""
+
+    def __init__(self, ctx: Context, budget_bytes: int, slots: int = 0, max_requests: int = 0, max_lookups: int = 0,
+                 max_range_values: int = 0):
+        self.ctx = ctx
+        cfg = ServerConfig(budget_bytes, slots, max_requests, max_lookups, max_range_values)
+        h = ctypes.c_void_p()
+        ctx.check(ctx.lib.glc_server_create(ctx.handle, ctypes.byref(cfg), ctypes.byref(h)))
+        self.handle = h
+
+    def admit(self, column: "Column") -> int:
+        """Make a column resident; the server owns it afterwards."""
+        i = ctypes.c_int32()
+        self.ctx.check(self.ctx.lib.glc_server_admit(self.handle, column.handle, ctypes.byref(i)))
+        column.handle = None
+        return i.value
+
+    def admit_blob(self, dtype: int, blob_ptr: int, size: int, host: bool = False, stream: int = 0) -> int:
+        i = ctypes.c_int32()
+        self.ctx.check(self.ctx.lib.glc_server_admit_blob(self.handle, dtype, ctypes.c_void_p(blob_ptr), size,
+                                                          HOST_IN if host else 0, ctypes.byref(i),
+                                                          ctypes.c_void_p(stream)))
+        return i.value
+
+    def evict(self, column_id: int):
+        self.ctx.check(self.ctx.lib.glc_server_evict(self.handle, column_id))
+
+    def submit(self, requests: np.ndarray):
+        """requests: a REQUEST_DTYPE array."""
+        r = np.ascontiguousarray(requests, REQUEST_DTYPE)
+        self.ctx.check(self.ctx.lib.glc_server_submit(self.handle, ctypes.c_void_p(r.ctypes.data), len(r)))
+
+    def poll(self, max_records: int = 1 << 16) -> np.ndarray:
+        out = np.zeros(max_records, COMPLETION_DTYPE)
+        got = ctypes.c_int32()
+        self.ctx.check(self.ctx.lib.glc_server_poll(self.handle, ctypes.c_void_p(out.ctypes.data), max_records,
+                                                    ctypes.byref(got)))
+        return out[: got.value]
+
+    def drain(self, timeout_ms: int = -1):
+        self.ctx.check(self.ctx.lib.glc_server_drain(self.handle, timeout_ms))
+
+    def stats(self) -> ServerStats:
+        s = ServerStats()
+        self.ctx.check(self.ctx.lib.glc_server_get_stats(self.handle, ctypes.byref(s)))
+        return s
+
+    def now_ns(self) -> int:
+        return self.ctx.lib.glc_server_now_ns()
+
+    def columns(self) -> list:
+        """Ids of the columns that accept requests."""
+        n = 1 << 16
+        ids = np.zeros(n, np.int32)
+        got = ctypes.c_int32()
+        self.ctx.check(self.ctx.lib.glc_server_columns(self.handle, ctypes.c_void_p(ids.ctypes.data), n,
+                                                       ctypes.byref(got)))
+        return ids[: got.value].tolist()
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self.ctx.lib.glc_server_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def requests(n: int) -> np.ndarray:
+    """An empty array of n requests (REQUEST_DTYPE)."""
+    return np.zeros(n, REQUEST_DTYPE)
 
 
 # ---- the reference's class API -------------------------------------------------------------

@@ -221,6 +221,103 @@ GLC_API glc_status glc_batch_free(glc_batch* batch);
 GLC_API glc_status glc_decompress_range_noalloc(const glc_column* col, int64_t first, int64_t count,
                                                 void* host_out, glc_stream stream);
 
+/* ---- serving: resident columns and continuously batched requests (no counterpart in the
+ * reference, whose every call is a blocking host round trip) ------------------------------ */
+
+typedef struct glc_server glc_server;
+
+typedef enum { GLC_REQ_LOOKUP = 0, GLC_REQ_RANGE = 1 } glc_request_kind;
+
+/* One request against a resident column.  Inputs and outputs are device memory of the server's
+ * device and must stay valid until the request's completion is reported.
+ *  LOOKUP: out[k] = value at positions[k] for k < count (0 outside the column), as
+ *          glc_random_access.
+ *  RANGE:  out[k] = value at first + k for k < count, as glc_decompress_range; [first,
+ *          first + count) must lie inside the column.  When (out - first * element size) is
+ *          16-byte aligned the values are written in place, otherwise through the server's
+ *          staging and one device copy per piece. */
+typedef struct glc_request {
+  int32_t kind;              /* glc_request_kind */
+  int32_t column;            /* id from glc_server_admit */
+  int64_t first;             /* RANGE: first position */
+  int64_t count;             /* LOOKUP: positions; RANGE: values (>= 1) */
+  const int32_t* positions;  /* LOOKUP: device array of count positions */
+  void* out;                 /* device output of count values */
+  int64_t tag;               /* caller's identifier, returned in the completion */
+  int64_t not_before_ns;     /* arrival time on glc_server_now_ns()'s clock; the request is not
+                                scheduled earlier and its latency counts from then.  0 = now. */
+} glc_request;
+
+typedef struct glc_completion {
+  int64_t tag;
+  int32_t status;      /* GLC_OK, or GLC_ERR_TIMEOUT / GLC_ERR_CUDA from its launches */
+  int32_t launches;    /* shared launches that carried a piece of the request */
+  int64_t arrival_ns;  /* max(not_before_ns, submission time) */
+  int64_t done_ns;     /* when the server saw the request's last launch complete */
+} glc_completion;
+
+typedef struct glc_server_config {
+  uint64_t budget_bytes;     /* device bytes the resident columns may hold (> 0) */
+  int32_t slots;             /* shared launches in flight at once (0 = 4, at most 16) */
+  int32_t max_requests;      /* lookup requests per launch (0 = 4096) */
+  int64_t max_lookups;       /* positions per launch (0 = 4,194,304); one larger request runs alone */
+  int64_t max_range_values;  /* range values per launch (0 = 4,194,304); longer ranges are split
+                                into pieces so that they cannot hold back small requests */
+} glc_server_config;
+
+typedef struct glc_server_stats {
+  uint64_t resident_bytes;   /* device bytes of admitted columns not yet freed */
+  int32_t resident_columns;
+  int32_t in_flight;         /* launches on the GPU now */
+  int64_t launches, submitted, completed, lookups, range_values, evictions, admissions_refused;
+} glc_server_stats;
+
+/* A server on ctx's device: a worker thread takes submitted requests once they have arrived and
+ * packs every request that is waiting into the next free launch slot (one lookup launch over all
+ * of the slot's lookup requests and one persistent decode launch over all of its range pieces,
+ * whatever their columns and element types), while up to `slots` launches run on the GPU. */
+GLC_API glc_status glc_server_create(glc_ctx* ctx, const glc_server_config* config, glc_server** out);
+
+/* Waits for every submitted request, stops the worker and frees every resident column. */
+GLC_API glc_status glc_server_destroy(glc_server* server);
+
+/* Make `col` resident and give it an id; the server takes ownership on success.  When the budget
+ * would be exceeded, idle columns are evicted least recently used first; if that cannot make room
+ * the call fails with GLC_ERR_BUDGET, evicts nothing and the caller keeps the column.  The column
+ * must hold its packed bitstream (GLC_ERR_UNSUPPORTED otherwise), and its device data must be
+ * complete: synchronise the stream that produced it first (calls with host buffers, and
+ * glc_server_admit_blob, return with their stream synchronised). */
+GLC_API glc_status glc_server_admit(glc_server* server, glc_column* col, int32_t* id);
+
+/* Deserialize a blob (as glc_deserialize, host or device memory) and admit the column. */
+GLC_API glc_status glc_server_admit_blob(glc_server* server, glc_dtype dtype, const void* blob, uint64_t size,
+                                         int flags, int32_t* id, glc_stream stream);
+
+/* Remove a column: no new requests are accepted for it and its memory is freed once its
+ * submitted requests have completed. */
+GLC_API glc_status glc_server_evict(glc_server* server, int32_t id);
+
+/* Queue requests (thread-safe).  Every request is checked first; if one is invalid (unknown or
+ * evicted column, count < 1, range outside the column, null pointer) none is queued and the call
+ * returns GLC_ERR_INVALID_ARG. */
+GLC_API glc_status glc_server_submit(glc_server* server, const glc_request* requests, int32_t count);
+
+/* Take up to `max` completion records (in completion order); *got receives how many. */
+GLC_API glc_status glc_server_poll(glc_server* server, glc_completion* out, int32_t max, int32_t* got);
+
+/* Wait until every submitted request has completed; GLC_ERR_TIMEOUT after timeout_ms (< 0 = no
+ * limit). */
+GLC_API glc_status glc_server_drain(glc_server* server, int64_t timeout_ms);
+
+GLC_API glc_status glc_server_get_stats(glc_server* server, glc_server_stats* stats);
+
+/* Ids of the columns that accept requests (admitted, not evicted), ascending; *got receives how
+ * many were written (at most max). */
+GLC_API glc_status glc_server_columns(glc_server* server, int32_t* ids, int32_t max, int32_t* got);
+
+/* The server's clock (CLOCK_MONOTONIC, nanoseconds). */
+GLC_API int64_t glc_server_now_ns(void);
+
 #ifdef __cplusplus
 }
 #endif

@@ -48,3 +48,13 @@ def test_no_device_is_an_error_not_a_fallback():
         pytest.skip("a CUDA device is present")
     with pytest.raises(glc.GlcError):
         glc.Context(0)
+
+
+def test_server_entry_points_reject_null_arguments():
+    lib = glc.load()
+    assert lib.glc_server_create(None, None, None) == glc.ERR_INVALID_ARG
+    assert lib.glc_server_submit(None, None, 1) == glc.ERR_INVALID_ARG
+    assert lib.glc_server_destroy(None) == glc.ERR_INVALID_ARG
+    assert lib.glc_server_drain(None, 0) == glc.ERR_INVALID_ARG
+    t0 = lib.glc_server_now_ns()
+    assert lib.glc_server_now_ns() >= t0 > 0
