@@ -80,11 +80,23 @@ cudaStream_t pick(glc_ctx* ctx, glc_stream s) { return s ? (cudaStream_t)s : ctx
 
 bool valid_dtype(int d) { return d >= GLC_I32 && d <= GLC_U32; }
 
+// Column arrays come from cudaMalloc, or from a stream-ordered pool when c->pool is set (the
+// columns a server deserializes: their allocation and release never synchronise the device).
+template <typename P> cudaError_t col_alloc(glc_column* c, P** p, size_t bytes, cudaStream_t s) {
+  if (c->pool) return cudaMallocFromPoolAsync((void**)p, bytes, c->pool, s);
+  return cudaMalloc((void**)p, bytes);
+}
+
+void col_release(glc_column* c, void* p) {
+  if (!p) return;
+  if (c->pool) cudaFreeAsync(p, c->ctx->own_stream);
+  else cudaFree(p);
+}
+
 void free_column_arrays(glc_column* c) {
   void* ptrs[] = {c->d_start, c->d_end, c->d_types, c->d_params, c->d_bits, c->d_offs, c->d_err,
                   c->d_words, c->d_plain, c->d_desc, c->d_tiles};
-  for (void* p : ptrs)
-    if (p) cudaFree(p);
+  for (void* p : ptrs) col_release(c, p);
   c->d_start = c->d_end = c->d_types = c->d_bits = nullptr;
   c->d_params = nullptr;
   c->d_offs = c->d_err = c->d_plain = nullptr;
@@ -94,19 +106,19 @@ void free_column_arrays(glc_column* c) {
 }
 
 // Metadata arrays for P partitions and the decode tile table.
-cudaError_t alloc_meta(glc_column* c) {
+cudaError_t alloc_meta(glc_column* c, cudaStream_t s) {
   const int64_t P = c->P > 0 ? c->P : 1;
   cudaError_t e;
-  if ((e = cudaMalloc(&c->d_start, 4 * P)) != cudaSuccess) return e;
-  if ((e = cudaMalloc(&c->d_end, 4 * P)) != cudaSuccess) return e;
-  if ((e = cudaMalloc(&c->d_types, 4 * P)) != cudaSuccess) return e;
-  if ((e = cudaMalloc(&c->d_params, 32 * P)) != cudaSuccess) return e;
-  if ((e = cudaMalloc(&c->d_bits, 4 * P)) != cudaSuccess) return e;
-  if ((e = cudaMalloc(&c->d_offs, 8 * P)) != cudaSuccess) return e;
-  if ((e = cudaMalloc(&c->d_err, 8 * P)) != cudaSuccess) return e;
-  if ((e = cudaMalloc(&c->d_desc, sizeof(PartDesc) * P)) != cudaSuccess) return e;
+  if ((e = col_alloc(c, &c->d_start, 4 * P, s)) != cudaSuccess) return e;
+  if ((e = col_alloc(c, &c->d_end, 4 * P, s)) != cudaSuccess) return e;
+  if ((e = col_alloc(c, &c->d_types, 4 * P, s)) != cudaSuccess) return e;
+  if ((e = col_alloc(c, &c->d_params, 32 * P, s)) != cudaSuccess) return e;
+  if ((e = col_alloc(c, &c->d_bits, 4 * P, s)) != cudaSuccess) return e;
+  if ((e = col_alloc(c, &c->d_offs, 8 * P, s)) != cudaSuccess) return e;
+  if ((e = col_alloc(c, &c->d_err, 8 * P, s)) != cudaSuccess) return e;
+  if ((e = col_alloc(c, &c->d_desc, sizeof(PartDesc) * P, s)) != cudaSuccess) return e;
   c->ntiles = (c->n + kDecodeTile - 1) / kDecodeTile;
-  if ((e = cudaMalloc(&c->d_tiles, sizeof(TileInfo) * (c->ntiles + 1))) != cudaSuccess) return e;
+  if ((e = col_alloc(c, &c->d_tiles, sizeof(TileInfo) * (c->ntiles + 1), s)) != cudaSuccess) return e;
   return cudaSuccess;
 }
 
@@ -259,7 +271,7 @@ static glc_status compress_impl(glc_ctx* ctx, glc_dtype dtype, const void* dev_v
     c->P = P;
     c->fixed_len = 0;
   }
-  CK(alloc_meta(c), "compress: metadata allocation");
+  CK(alloc_meta(c, s), "compress: metadata allocation");
   if (mode == GLC_PART_FIXED) {
     CK(launch_fixed_partitions(c->d_start, c->d_end, n, fixed_len, c->P, s), "compress: fixed partitions");
   } else {
@@ -476,13 +488,13 @@ glc_status glc_preunpack(glc_ctx* ctx, glc_column* col, int drop_packed, glc_str
     if (!col->d_words) return fail(ctx, GLC_ERR_UNSUPPORTED, "column has no packed bitstream");
     cudaSetDevice(ctx->device);
     cudaStream_t s = pick(ctx, stream);
-    CK(cudaMalloc(&col->d_plain, 8 * col->n + 16), "pre-unpack: allocation");  // +16: 16-byte TMA granules
+    CK(col_alloc(col, &col->d_plain, 8 * col->n + 16, s), "pre-unpack: allocation");  // +16: 16-byte TMA granules
     CK(cudaMemsetAsync((char*)col->d_plain + 8 * col->n, 0, 16, s), "pre-unpack: padding");
     CK(launch_decode(ctx, col, 0, 1, 0, col->n, col->d_plain, s), "pre-unpack");
     CK(cudaStreamSynchronize(s), "pre-unpack: sync");
   }
   if (drop_packed && col->d_words) {  // api/G-LeCo.cuh:2283-2287
-    cudaFree(col->d_words);
+    col_release(col, col->d_words);
     col->d_words = nullptr;
   }
   return GLC_OK;
@@ -546,6 +558,14 @@ glc_status glc_serialize(glc_ctx* ctx, const glc_column* c, void* blob, uint64_t
 
 glc_status glc_deserialize(glc_ctx* ctx, glc_dtype dtype, const void* blob, uint64_t size, int flags, int crc32c,
                            int pre_unpack, glc_column** out, glc_stream stream) {
+  return glc::deserialize_column(ctx, dtype, blob, size, flags, crc32c, pre_unpack, out, stream, nullptr);
+}
+
+}  // extern "C"
+
+glc_status glc::deserialize_column(glc_ctx* ctx, glc_dtype dtype, const void* blob, uint64_t size, int flags,
+                                   int crc32c, int pre_unpack, glc_column** out, glc_stream stream,
+                                   cudaMemPool_t pool) {
   if (!ctx || !out) return fail(ctx, GLC_ERR_INVALID_ARG, "null argument");
   *out = nullptr;
   if (!valid_dtype(dtype)) return fail(ctx, GLC_ERR_INVALID_ARG, "unknown dtype");
@@ -576,6 +596,7 @@ glc_status glc_deserialize(glc_ctx* ctx, glc_dtype dtype, const void* blob, uint
   glc_column* c = new (std::nothrow) glc_column();
   if (!c) return fail(ctx, GLC_ERR_OOM, "host allocation");
   c->ctx = ctx;
+  c->pool = pool;
   c->dtype = dtype;
   c->n = h.total_values;
   c->P = (int64_t)P;
@@ -587,10 +608,11 @@ glc_status glc_deserialize(glc_ctx* ctx, glc_dtype dtype, const void* blob, uint
     *out = c;
     return GLC_OK;
   }
-  cudaError_t e = alloc_meta(c);
+  cudaError_t e = alloc_meta(c, s);
   if (e != cudaSuccess) return bail(cuda_fail(ctx, e, "deserialize: allocation"));
   set_word_counts(c);
-  if ((e = cudaMalloc(&c->d_words, 4 * c->nwords_alloc)) != cudaSuccess) return bail(cuda_fail(ctx, e, "deserialize: allocation"));
+  if ((e = col_alloc(c, &c->d_words, 4 * c->nwords_alloc, s)) != cudaSuccess)
+    return bail(cuda_fail(ctx, e, "deserialize: allocation"));
   const cudaMemcpyKind k = host ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
   const uint8_t* b = (const uint8_t*)blob;
   void* dst[7] = {c->d_start, c->d_end, c->d_types, c->d_params, c->d_bits, c->d_offs, c->d_err};
@@ -650,5 +672,3 @@ glc_status glc_deserialize(glc_ctx* ctx, glc_dtype dtype, const void* blob, uint
   *out = c;
   return GLC_OK;
 }
-
-}  // extern "C"

@@ -28,6 +28,7 @@
 // straight from global memory (rare: fields averaging more than 48 bits over a tile).
 // Every mbarrier wait is bounded by wall time; on expiry the kernel records an error code and
 // returns after a second bounded wait for its own copies.
+#include <atomic>
 #include <climits>
 #include <cstdlib>
 #include <type_traits>
@@ -373,7 +374,7 @@ __global__ void __launch_bounds__(kPCThreads) batch_decode_kernel(BatchDecodeArg
     for (int k = 0;; k++) {
       const int s = k % kStages;
       if (k >= kStages && !mbar_wait_bounded(&empty[s], (uint32_t)((k / kStages) - 1) & 1u)) {
-        atomicExch(b.err, DEVERR_TIMEOUT);
+        *(volatile int*)b.err = DEVERR_TIMEOUT;  // may be mapped host memory
         break;
       }
       const int64_t item = (int64_t)atomicAdd(b.counter, 1ull);
@@ -412,7 +413,7 @@ __global__ void __launch_bounds__(kPCThreads) batch_decode_kernel(BatchDecodeArg
   for (int k = 0;; k++) {  // ---- consumers ----
     const int s = k % kStages;
     if (!mbar_wait_bounded(&full[s], (uint32_t)(k / kStages) & 1u)) {
-      if (lane == 0) atomicExch(b.err, DEVERR_TIMEOUT);
+      if (lane == 0) *(volatile int*)b.err = DEVERR_TIMEOUT;  // may be mapped host memory
       mbar_wait_bounded(&full[s], (uint32_t)(k / kStages) & 1u);
       break;
     }
@@ -444,15 +445,37 @@ __global__ void __launch_bounds__(kPCThreads) batch_decode_kernel(BatchDecodeArg
   }
 }
 
+// Launch configuration of the batched decode, per device: the shared-memory attribute is raised
+// once to the largest stage ring, and the resident CTAs per SM are kept per stage size (these
+// queries cost microseconds, and the serving loop launches tens of thousands of times a second).
+constexpr int kMaxDevices = 16;
+static std::atomic<int> g_batch_attr[kMaxDevices];
+static std::atomic<int> g_batch_per_sm[kMaxDevices][kStageCapWords / 4 + 1];
+
 static cudaError_t batch_decode_go(const BatchDecodeArgs& b, int num_sms, bool zero, cudaStream_t s) {
   if (b.nwork <= 0) return cudaSuccess;
   void (*kern)(BatchDecodeArgs) = batch_decode_kernel<kDefaultStages>;
   const size_t smem = (size_t)kDefaultStages * b.stage_bytes;
-  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return e;
+  const bool cached = dev >= 0 && dev < kMaxDevices && b.stage_bytes % 16 == 0 && b.stage_bytes <= kStageCapWords * 4;
   int per_sm = 0;
-  if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kPCThreads, smem)) != cudaSuccess) return e;
-  if (per_sm < 1) per_sm = 1;
+  if (cached) {
+    if (!g_batch_attr[dev].load(std::memory_order_acquire)) {
+      e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, kDefaultStages * kStageCapWords * 4);
+      if (e != cudaSuccess) return e;
+      g_batch_attr[dev].store(1, std::memory_order_release);
+    }
+    per_sm = g_batch_per_sm[dev][b.stage_bytes / 16].load(std::memory_order_relaxed);
+  } else if ((e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) != cudaSuccess) {
+    return e;
+  }
+  if (per_sm == 0) {
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kPCThreads, smem)) != cudaSuccess) return e;
+    if (per_sm < 1) per_sm = 1;
+    if (cached) g_batch_per_sm[dev][b.stage_bytes / 16].store(per_sm, std::memory_order_relaxed);
+  }
   int64_t grid = (int64_t)per_sm * num_sms;
   if (grid > b.nwork) grid = b.nwork;
   if (zero && (e = cudaMemsetAsync(b.counter, 0, sizeof(unsigned long long), s)) != cudaSuccess) return e;

@@ -52,6 +52,7 @@ struct glc_ctx {
 
 struct glc_column {
   glc_ctx* ctx = nullptr;
+  cudaMemPool_t pool = nullptr;  // arrays from this stream-ordered pool (else cudaMalloc)
   bool view = false;         // arrays are slices of a batch's storage (freed with the batch)
   glc_dtype dtype = GLC_I32;
   int64_t n = 0;
@@ -151,6 +152,9 @@ int batch_stage_bytes(int max_bits);
 // random_access.cu
 cudaError_t launch_random_access(glc_ctx* ctx, const glc_column* c, int plain_src, const int32_t* pos,
                                  int64_t q, void* out, int32_t fixed_len, cudaStream_t s);
+// api.cu: glc_deserialize with the column's arrays allocated from `pool` (nullptr: cudaMalloc)
+glc_status deserialize_column(glc_ctx* ctx, glc_dtype dtype, const void* blob, uint64_t size, int flags, int crc32c,
+                              int pre_unpack, glc_column** out, glc_stream stream, cudaMemPool_t pool);
 // random_access.cu: lookups of many requests into many columns (serving)
 struct RAColumn {
   const PartDesc* desc;

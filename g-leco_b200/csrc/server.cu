@@ -88,7 +88,8 @@ struct Slot {
   uint8_t* h_meta = nullptr;      // pinned staging of the launch's tables
   uint8_t* d_meta = nullptr;
   uint8_t* d_stage = nullptr;     // range pieces whose output is not 16-byte aligned
-  int* h_err = nullptr;           // pinned copy of the launch's device error word
+  int* h_err = nullptr;           // mapped host word: the launch's device error code
+  int* d_err = nullptr;           // its device address
   bool busy = false;
   bool lookups_pending = false;   // lreqs not yet reported
   std::vector<Req*> lreqs;        // lookup requests of the launch
@@ -100,6 +101,7 @@ struct Slot {
 struct glc_server {
   glc_ctx* ctx = nullptr;
   glc_server_config cfg{};
+  cudaMemPool_t pool = nullptr;  // arrays of the columns admitted from blobs
   int64_t max_work = 0;
   size_t meta_cap = 0, stage_cap = 0;
 
@@ -271,7 +273,7 @@ void launch_slot(glc_server* S, Slot& sl, std::deque<Req*>& ready_l, std::deque<
     if (hi == end) ready_r.pop_front();
   }
 
-  // One host-to-device copy of all tables: [counter u64, error int, pad][lookup columns]
+  // One host-to-device copy of all tables: [decode work counter u64, pad][lookup columns]
   // [decode columns][lookup requests][work items].
   const size_t o_ra = 16;
   const size_t o_bc = align16(o_ra + sizeof(RAColumn) * S->w_ra.size());
@@ -300,13 +302,12 @@ void launch_slot(glc_server* S, Slot& sl, std::deque<Req*>& ready_l, std::deque<
     a.work = (const BatchWork*)(sl.d_meta + o_work);
     a.nwork = (int64_t)S->w_work.size();
     a.counter = (unsigned long long*)sl.d_meta;
-    a.err = (int*)(sl.d_meta + 8);
+    a.err = sl.d_err;
     a.stage_bytes = batch_stage_bytes(max_bits);
     e = launch_batch_decode_zeroed(a, S->ctx->num_sms, sl.stream);
   }
   for (size_t i = 0; e == cudaSuccess && i < S->w_copy.size(); i++)
     e = cudaMemcpyAsync(S->w_copy[i].dst, S->w_copy[i].src, S->w_copy[i].bytes, cudaMemcpyDeviceToDevice, sl.stream);
-  if (e == cudaSuccess) e = cudaMemcpyAsync(sl.h_err, sl.d_meta + 8, sizeof(int), cudaMemcpyDeviceToHost, sl.stream);
   if (e != cudaSuccess) {
     for (Req* r : sl.lreqs) r->status = GLC_ERR_CUDA;
     for (Req* r : sl.rreqs) r->status = GLC_ERR_CUDA;
@@ -433,6 +434,7 @@ void destroy_slots(glc_server* S) {
     if (sl.lk_done) cudaEventDestroy(sl.lk_done);
     if (sl.stream) cudaStreamDestroy(sl.stream);
     if (sl.h_meta) cudaFreeHost(sl.h_meta);
+    if (sl.h_err) cudaFreeHost(sl.h_err);
     if (sl.d_meta) cudaFree(sl.d_meta);
     if (sl.d_stage) cudaFree(sl.d_stage);
     sl = Slot();
@@ -453,9 +455,9 @@ glc_status glc_server_create(glc_ctx* ctx, const glc_server_config* config, glc_
   if (c.slots == 0) c.slots = 4;
   if (c.max_requests == 0) c.max_requests = 4096;
   if (c.max_lookups == 0) c.max_lookups = 1ll << 22;
-  if (c.max_range_values == 0) c.max_range_values = 1ll << 22;
+  if (c.max_range_values == 0) c.max_range_values = 1ll << 24;
   if (c.slots < 1 || c.slots > kMaxSlots || c.max_requests < 1 || c.max_requests > (1 << 20) || c.max_lookups < 1 ||
-      c.max_range_values < 1 || c.max_range_values > (1ll << 30))
+      c.max_range_values < 1 || c.max_range_values > (1ll << 30) || (c.flags & ~GLC_SERVER_RESERVE) != 0)
     return sfail(ctx, GLC_ERR_INVALID_ARG, "server: configuration out of range");
   glc_server* S = new (std::nothrow) glc_server();
   if (!S) return GLC_ERR_OOM;
@@ -473,13 +475,31 @@ glc_status glc_server_create(glc_ctx* ctx, const glc_server_config* config, glc_
     if ((e = cudaStreamCreateWithFlags(&sl.stream, cudaStreamNonBlocking)) != cudaSuccess) break;
     if ((e = cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming)) != cudaSuccess) break;
     if ((e = cudaEventCreateWithFlags(&sl.lk_done, cudaEventDisableTiming)) != cudaSuccess) break;
-    if ((e = cudaHostAlloc((void**)&sl.h_meta, S->meta_cap + 64, cudaHostAllocDefault)) != cudaSuccess) break;
-    sl.h_err = (int*)(sl.h_meta + S->meta_cap);
+    if ((e = cudaHostAlloc((void**)&sl.h_meta, S->meta_cap, cudaHostAllocDefault)) != cudaSuccess) break;
+    // the decode kernel stores its error code straight into this mapped host word
+    if ((e = cudaHostAlloc((void**)&sl.h_err, 64, cudaHostAllocMapped)) != cudaSuccess) break;
+    if ((e = cudaHostGetDevicePointer((void**)&sl.d_err, sl.h_err, 0)) != cudaSuccess) break;
     if ((e = cudaMalloc((void**)&sl.d_meta, S->meta_cap)) != cudaSuccess) break;
     e = cudaMalloc((void**)&sl.d_stage, S->stage_cap);
   }
+  if (e == cudaSuccess) {
+    cudaMemPoolProps props = {};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = ctx->device;
+    uint64_t keep = ~0ull;
+    e = cudaMemPoolCreate(&S->pool, &props);
+    if (e == cudaSuccess) e = cudaMemPoolSetAttribute(S->pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    if (e == cudaSuccess && (c.flags & GLC_SERVER_RESERVE)) {  // grow the pool once; freed memory stays
+      void* p = nullptr;
+      e = cudaMallocFromPoolAsync(&p, c.budget_bytes, S->pool, ctx->own_stream);
+      if (e == cudaSuccess) e = cudaFreeAsync(p, ctx->own_stream);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->own_stream);
+    }
+  }
   if (e != cudaSuccess) {
     destroy_slots(S);
+    if (S->pool) cudaMemPoolDestroy(S->pool);
     delete S;
     return scuda(ctx, e, "server: slot resources");
   }
@@ -516,7 +536,9 @@ glc_status glc_server_destroy(glc_server* S) {
   free_pending(S);
   for (SrvColumn& c : S->cols)
     if (c.col) glc_column_free(c.col);
+  cudaStreamSynchronize(S->ctx->own_stream);  // pooled arrays are released on the context's stream
   destroy_slots(S);
+  cudaMemPoolDestroy(S->pool);
   delete S;
   return GLC_OK;
 }
@@ -580,7 +602,7 @@ glc_status glc_server_admit_blob(glc_server* S, glc_dtype dtype, const void* blo
                                  int32_t* id, glc_stream stream) {
   if (!S || !id) return GLC_ERR_INVALID_ARG;
   glc_column* col = nullptr;
-  glc_status st = glc_deserialize(S->ctx, dtype, blob, size, flags, 0, 0, &col, stream);
+  glc_status st = deserialize_column(S->ctx, dtype, blob, size, flags, 0, 0, &col, stream, S->pool);
   if (st != GLC_OK) return st;
   st = glc_server_admit(S, col, id);
   if (st != GLC_OK) glc_column_free(col);

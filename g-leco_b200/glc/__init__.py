@@ -40,6 +40,7 @@ EXPORTS = [
     "glc_server_drain", "glc_server_get_stats", "glc_server_now_ns", "glc_server_columns",
 ]
 REQ_LOOKUP, REQ_RANGE = 0, 1
+SERVER_RESERVE = 1
 NOALLOC_MAX_OUTPUT_BYTES = 4 << 20
 
 
@@ -63,7 +64,8 @@ class ColumnInfo(ctypes.Structure):
 
 class ServerConfig(ctypes.Structure):
     _fields_ = [("budget_bytes", ctypes.c_uint64), ("slots", ctypes.c_int32), ("max_requests", ctypes.c_int32),
-                ("max_lookups", ctypes.c_int64), ("max_range_values", ctypes.c_int64)]
+                ("max_lookups", ctypes.c_int64), ("max_range_values", ctypes.c_int64), ("flags", ctypes.c_int32),
+                ("reserved", ctypes.c_int32)]
 
 
 class Request(ctypes.Structure):
@@ -357,9 +359,10 @@ class Server:
     """Resident columns and continuously batched requests (glc_server_*)."""
 
     def __init__(self, ctx: Context, budget_bytes: int, slots: int = 0, max_requests: int = 0, max_lookups: int = 0,
-                 max_range_values: int = 0):
+                 max_range_values: int = 0, reserve: bool = False):
         self.ctx = ctx
-        cfg = ServerConfig(budget_bytes, slots, max_requests, max_lookups, max_range_values)
+        cfg = ServerConfig(budget_bytes, slots, max_requests, max_lookups, max_range_values,
+                           SERVER_RESERVE if reserve else 0, 0)
         h = ctypes.c_void_p()
         ctx.check(ctx.lib.glc_server_create(ctx.handle, ctypes.byref(cfg), ctypes.byref(h)))
         self.handle = h

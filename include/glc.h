@@ -261,9 +261,14 @@ typedef struct glc_server_config {
   int32_t slots;             /* shared launches in flight at once (0 = 4, at most 16) */
   int32_t max_requests;      /* lookup requests per launch (0 = 4096) */
   int64_t max_lookups;       /* positions per launch (0 = 4,194,304); one larger request runs alone */
-  int64_t max_range_values;  /* range values per launch (0 = 4,194,304); longer ranges are split
+  int64_t max_range_values;  /* range values per launch (0 = 16,777,216); longer ranges are split
                                 into pieces so that they cannot hold back small requests */
+  int32_t flags;             /* GLC_SERVER_RESERVE: reserve budget_bytes of device memory for
+                                glc_server_admit_blob at creation */
+  int32_t reserved;          /* 0 */
 } glc_server_config;
+
+enum { GLC_SERVER_RESERVE = 1 };
 
 typedef struct glc_server_stats {
   uint64_t resident_bytes;   /* device bytes of admitted columns not yet freed */
@@ -289,7 +294,10 @@ GLC_API glc_status glc_server_destroy(glc_server* server);
  * glc_server_admit_blob, return with their stream synchronised). */
 GLC_API glc_status glc_server_admit(glc_server* server, glc_column* col, int32_t* id);
 
-/* Deserialize a blob (as glc_deserialize, host or device memory) and admit the column. */
+/* Deserialize a blob (as glc_deserialize, host or device memory) and admit the column.  Its arrays
+ * come from the server's stream-ordered pool, so neither this admission nor the column's later
+ * eviction calls cudaMalloc or cudaFree, which would stall the launches in flight; with
+ * GLC_SERVER_RESERVE the pool holds budget_bytes from creation on. */
 GLC_API glc_status glc_server_admit_blob(glc_server* server, glc_dtype dtype, const void* blob, uint64_t size,
                                          int flags, int32_t* id, glc_stream stream);
 

@@ -262,9 +262,10 @@ def test_invalid_requests_queue_nothing():
     server.close()
 
 
-def test_admit_blob_from_device_memory(oracle):
+@pytest.mark.parametrize("reserve", [False, True])
+def test_admit_blob_from_device_memory(oracle, reserve):
     ctx = glc.Context(0)
-    server = glc.Server(ctx, budget_bytes=1 << 32)
+    server = glc.Server(ctx, budget_bytes=1 << 30, reserve=reserve)
     v = _values(glc.U64, 300_000, 5)
     blob = oracle.serialize(oracle.compress(v, "fixed", 2048))
     dblob = torch.from_numpy(np.frombuffer(blob, np.uint8).copy()).cuda()
@@ -275,4 +276,14 @@ def test_admit_blob_from_device_memory(oracle):
     server.submit(r)
     server.drain(10_000)
     assert np.array_equal(out.cpu().numpy().view(np.uint64), v)
+    # blob columns live in the server's pool: evicting and re-admitting reuses it
+    server.evict(cid)
+    host_blob = np.frombuffer(blob, np.uint8).copy()
+    cid2 = server.admit_blob(glc.U64, host_blob.ctypes.data, len(blob), host=True)
+    out.zero_()
+    r[0]["column"] = cid2
+    server.submit(r)
+    server.drain(10_000)
+    assert np.array_equal(out.cpu().numpy().view(np.uint64), v)
+    assert server.columns() == [cid2]
     server.close()
