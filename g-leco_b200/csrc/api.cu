@@ -185,6 +185,9 @@ glc_status glc_create(glc_ctx** out, int device) {
     glc_destroy(ctx);
     return e == cudaErrorMemoryAllocation ? GLC_ERR_OOM : GLC_ERR_CUDA;
   }
+  tune_defaults(ctx);
+  const char* cache = getenv("GLC_TUNE_CACHE");  // results of an earlier glc_autotune, if they fit
+  if (cache && *cache) tune_load(ctx, cache);
   *out = ctx;
   return GLC_OK;
 }

@@ -145,7 +145,7 @@ struct Cursor {
   int start, next, bits, type, idx;
 };
 
-template <typename T, bool PLAIN, bool RESID>
+template <typename T, bool PLAIN, bool RESID, int kUnroll = 2>
 __device__ __forceinline__ void decode_tile(const DecodeArgs& a, const StageInfo& si, const uint8_t* stage,
                                             const PartDesc* sdesc) {
   typedef typename std::conditional<RESID, int64_t, T>::type OutT;
@@ -246,7 +246,7 @@ __device__ __forceinline__ void decode_tile(const DecodeArgs& a, const StageInfo
 
   if (E0 == tile_e0 && E1 - E0 == kDecodeTile) {  // full tile: every vector is in range
     constexpr int kIters = kDecodeTile / V / kConsumers;
-#pragma unroll 2
+#pragma unroll kUnroll
     for (int it = 0; it < kIters; it++) {
       const int e = Ea + (it * kConsumers + tid) * V;
       if (c.idx < 0 || e >= c.next) seek(e);
@@ -264,7 +264,7 @@ __device__ __forceinline__ void decode_tile(const DecodeArgs& a, const StageInfo
   }
 }
 
-template <typename T, bool PLAIN, bool RESID, int kStages>
+template <typename T, bool PLAIN, bool RESID, int kStages, int kUnroll>
 __global__ void __launch_bounds__(kPCThreads) decode_kernel(DecodeArgs a) {
   extern __shared__ __align__(128) uint8_t smem[];
   __shared__ __align__(128) PartDesc s_desc[kStages][kTileDescs];
@@ -338,7 +338,7 @@ __global__ void __launch_bounds__(kPCThreads) decode_kernel(DecodeArgs a) {
     }
     const StageInfo si = s_info[s];
     if (si.tile >= a.t_end) break;
-    decode_tile<T, PLAIN, RESID>(a, si, smem + (size_t)s * a.stage_bytes, &s_desc[s][0]);
+    decode_tile<T, PLAIN, RESID, kUnroll>(a, si, smem + (size_t)s * a.stage_bytes, &s_desc[s][0]);
     __syncwarp();
     if (lane == 0) mbar_arrive(&empty[s]);
   }
@@ -498,10 +498,10 @@ int batch_stage_bytes(int max_bits) {
   return (int)(words * 4);
 }
 
-template <typename T, bool PLAIN, bool RESID, int kStages>
+template <typename T, bool PLAIN, bool RESID, int kStages, int kUnroll>
 static cudaError_t run_decode(glc_ctx* ctx, const DecodeArgs& a, cudaStream_t s) {
   const size_t smem = (size_t)kStages * a.stage_bytes;
-  void (*kern)(DecodeArgs) = decode_kernel<T, PLAIN, RESID, kStages>;
+  void (*kern)(DecodeArgs) = decode_kernel<T, PLAIN, RESID, kStages, kUnroll>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   int per_sm = 0;
@@ -517,17 +517,23 @@ static cudaError_t run_decode(glc_ctx* ctx, const DecodeArgs& a, cudaStream_t s)
   return cudaGetLastError();
 }
 
+// The unroll depth is a tuning choice of the packed value decode (the path every full and range
+// decode takes); the residual and pre-unpacked variants keep depth 2.
 template <typename T, int kStages>
-static cudaError_t decode_staged(glc_ctx* ctx, const DecodeArgs& a, int plain, int resid, cudaStream_t s) {
-  if (plain) return resid ? run_decode<T, true, true, kStages>(ctx, a, s) : run_decode<T, true, false, kStages>(ctx, a, s);
-  return resid ? run_decode<T, false, true, kStages>(ctx, a, s) : run_decode<T, false, false, kStages>(ctx, a, s);
+static cudaError_t decode_staged(glc_ctx* ctx, const DecodeArgs& a, int plain, int resid, int unroll, cudaStream_t s) {
+  if (plain) return resid ? run_decode<T, true, true, kStages, 2>(ctx, a, s) : run_decode<T, true, false, kStages, 2>(ctx, a, s);
+  if (resid) return run_decode<T, false, true, kStages, 2>(ctx, a, s);
+  if (unroll == 1) return run_decode<T, false, false, kStages, 1>(ctx, a, s);
+  if (unroll == 4) return run_decode<T, false, false, kStages, 4>(ctx, a, s);
+  return run_decode<T, false, false, kStages, 2>(ctx, a, s);
 }
 
 template <typename T>
-static cudaError_t decode_typed(glc_ctx* ctx, const DecodeArgs& a, int plain, int resid, int stages, cudaStream_t s) {
-  if (stages == 2) return decode_staged<T, 2>(ctx, a, plain, resid, s);
-  if (stages == 4) return decode_staged<T, 4>(ctx, a, plain, resid, s);
-  return decode_staged<T, 3>(ctx, a, plain, resid, s);
+static cudaError_t decode_typed(glc_ctx* ctx, const DecodeArgs& a, int plain, int resid, int stages, int unroll,
+                                cudaStream_t s) {
+  if (stages == 2) return decode_staged<T, 2>(ctx, a, plain, resid, unroll, s);
+  if (stages == 4) return decode_staged<T, 4>(ctx, a, plain, resid, unroll, s);
+  return decode_staged<T, 3>(ctx, a, plain, resid, unroll, s);
 }
 
 // Launch shape overrides for tuning sweeps (ring depth, stage capacity in words).
@@ -563,10 +569,10 @@ cudaError_t launch_decode_scratch(const glc_column* c, int64_t lo, int64_t hi, v
   a.stage_bytes = (int)(words * 4);
   void (*kern)(DecodeArgs) = nullptr;
   switch (c->dtype) {
-    case GLC_I32: kern = decode_kernel<int32_t, false, false, kDefaultStages>; break;
-    case GLC_I64: kern = decode_kernel<int64_t, false, false, kDefaultStages>; break;
-    case GLC_U64: kern = decode_kernel<uint64_t, false, false, kDefaultStages>; break;
-    case GLC_U32: kern = decode_kernel<uint32_t, false, false, kDefaultStages>; break;
+    case GLC_I32: kern = decode_kernel<int32_t, false, false, kDefaultStages, 2>; break;
+    case GLC_I64: kern = decode_kernel<int64_t, false, false, kDefaultStages, 2>; break;
+    case GLC_U64: kern = decode_kernel<uint64_t, false, false, kDefaultStages, 2>; break;
+    case GLC_U32: kern = decode_kernel<uint32_t, false, false, kDefaultStages, 2>; break;
     default: return cudaErrorInvalidValue;
   }
   const size_t smem = (size_t)kDefaultStages * a.stage_bytes;
@@ -581,8 +587,8 @@ cudaError_t launch_decode_scratch(const glc_column* c, int64_t lo, int64_t hi, v
   return cudaGetLastError();
 }
 
-cudaError_t launch_decode(glc_ctx* ctx, const glc_column* c, int plain_src, int residual_out, int64_t lo, int64_t hi,
-                          void* out_base, cudaStream_t s) {
+cudaError_t launch_decode_shape(glc_ctx* ctx, const glc_column* c, int plain_src, int residual_out, int64_t lo,
+                                int64_t hi, void* out_base, int stages, int unroll, cudaStream_t s) {
   if (hi <= lo || c->n <= 0) return cudaSuccess;
   if (((uintptr_t)out_base & 15) != 0) return cudaErrorMisalignedAddress;  // 16-byte vector stores
   DecodeArgs a;
@@ -609,14 +615,23 @@ cudaError_t launch_decode(glc_ctx* ctx, const glc_column* c, int plain_src, int 
     if (words > cap) words = cap < 32 ? 32 : cap;
     a.stage_bytes = (int)(words * 4);
   }
-  const int stages = env_int("GLC_DECODE_STAGES", kDefaultStages);
   switch (c->dtype) {
-    case GLC_I32: return decode_typed<int32_t>(ctx, a, plain_src, residual_out, stages, s);
-    case GLC_I64: return decode_typed<int64_t>(ctx, a, plain_src, residual_out, stages, s);
-    case GLC_U64: return decode_typed<uint64_t>(ctx, a, plain_src, residual_out, stages, s);
-    case GLC_U32: return decode_typed<uint32_t>(ctx, a, plain_src, residual_out, stages, s);
+    case GLC_I32: return decode_typed<int32_t>(ctx, a, plain_src, residual_out, stages, unroll, s);
+    case GLC_I64: return decode_typed<int64_t>(ctx, a, plain_src, residual_out, stages, unroll, s);
+    case GLC_U64: return decode_typed<uint64_t>(ctx, a, plain_src, residual_out, stages, unroll, s);
+    case GLC_U32: return decode_typed<uint32_t>(ctx, a, plain_src, residual_out, stages, unroll, s);
   }
   return cudaErrorInvalidValue;
+}
+
+// Ring depth and unroll depth from the context's tuning table for the column's element type and
+// widest field (GLC_DECODE_STAGES / GLC_DECODE_UNROLL override both, for sweeps).
+cudaError_t launch_decode(glc_ctx* ctx, const glc_column* c, int plain_src, int residual_out, int64_t lo, int64_t hi,
+                          void* out_base, cudaStream_t s) {
+  const TuneEntry& t = tune_entry(ctx, c->dtype, c->max_bits, plain_src);
+  const int stages = env_int("GLC_DECODE_STAGES", t.decode_stages);
+  const int unroll = env_int("GLC_DECODE_UNROLL", t.decode_unroll);
+  return launch_decode_shape(ctx, c, plain_src, residual_out, lo, hi, out_base, stages, unroll, s);
 }
 
 }  // namespace glc

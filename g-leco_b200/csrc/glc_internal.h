@@ -38,6 +38,23 @@ constexpr int kFlagError = kCounterSlots;      // device error code (DEVERR_*)
 constexpr int kFlagWords = kCounterSlots + 8;
 }  // namespace glc
 
+namespace glc {
+// Launch choices per (element type, widest-field bucket, residual source), filled with measured
+// defaults and replaced by glc_autotune.
+constexpr int kTuneBuckets = 6;  // widest field <= 8, 16, 24, 32, 48, 64 bits
+struct TuneEntry {
+  int32_t decode_stages;  // TMA ring depth of the decode kernel (2, 3, 4)
+  int32_t decode_unroll;  // unroll depth of its full-tile loop (1, 2, 4)
+  int32_t ra_shape;       // random-access launch shape (0..4)
+  int32_t measured;       // 1 when set by a measurement
+  float decode_gbs;       // decoded GB/s of the chosen decode shape (when measured)
+  float ra_glookups;      // G lookups/s of the chosen random-access shape (when measured)
+};
+inline int tune_bucket(int bits) {
+  return bits <= 8 ? 0 : bits <= 16 ? 1 : bits <= 24 ? 2 : bits <= 32 ? 3 : bits <= 48 ? 4 : 5;
+}
+}  // namespace glc
+
 struct glc_ctx {
   int device = 0;
   int num_sms = 0;
@@ -48,6 +65,7 @@ struct glc_ctx {
   int64_t* h_stats = nullptr;  // pinned mirror of d_stats
   std::atomic<unsigned> next_slot{0};
   std::string err;
+  glc::TuneEntry tune[4][glc::kTuneBuckets][2];  // [dtype][bucket][pre-unpacked source]
 };
 
 struct glc_column {
@@ -82,6 +100,12 @@ struct glc_column {
 namespace glc {
 
 inline int dtype_size(glc_dtype d) { return (d == GLC_I64 || d == GLC_U64) ? 8 : 4; }
+
+inline const TuneEntry& tune_entry(const glc_ctx* ctx, glc_dtype d, int bits, int plain) {
+  return ctx->tune[(int)d & 3][tune_bucket(bits)][plain ? 1 : 0];
+}
+void tune_defaults(glc_ctx* ctx);                  // tune.cu
+bool tune_load(glc_ctx* ctx, const char* path);   // tune.cu: true when the file fits this device
 
 // Stream-ordered temporary allocation from the context's pool.
 template <typename P> inline cudaError_t pool_alloc(glc_ctx* ctx, P** p, size_t bytes, cudaStream_t s) {
@@ -118,6 +142,9 @@ cudaError_t launch_pack(glc_dtype dt, const void* values, glc_column* c, cudaStr
 // decode.cu: values (or residuals when residual_out) of positions [lo, hi) to out_base[lo..hi)
 cudaError_t launch_decode(glc_ctx* ctx, const glc_column* c, int plain_src, int residual_out, int64_t lo,
                           int64_t hi, void* out_base, cudaStream_t s);
+// decode.cu: the same with an explicit ring depth and unroll depth (the tuner's candidates)
+cudaError_t launch_decode_shape(glc_ctx* ctx, const glc_column* c, int plain_src, int residual_out, int64_t lo,
+                                int64_t hi, void* out_base, int stages, int unroll, cudaStream_t s);
 // decode.cu: packed-source value decode with caller-supplied scratch; the counter must be zero.
 cudaError_t launch_decode_scratch(const glc_column* c, int64_t lo, int64_t hi, void* out_base, int* counter,
                                   int* err, int num_sms, cudaStream_t s);
@@ -152,6 +179,8 @@ int batch_stage_bytes(int max_bits);
 // random_access.cu
 cudaError_t launch_random_access(glc_ctx* ctx, const glc_column* c, int plain_src, const int32_t* pos,
                                  int64_t q, void* out, int32_t fixed_len, cudaStream_t s);
+cudaError_t launch_random_access_shape(glc_ctx* ctx, const glc_column* c, int plain_src, const int32_t* pos, int64_t q,
+                                       void* out, int32_t fixed_len, int shape, cudaStream_t s);
 // api.cu: glc_deserialize with the column's arrays allocated from `pool` (nullptr: cudaMalloc)
 glc_status deserialize_column(glc_ctx* ctx, glc_dtype dtype, const void* blob, uint64_t size, int flags, int crc32c,
                               int pre_unpack, glc_column** out, glc_stream stream, cudaMemPool_t pool);

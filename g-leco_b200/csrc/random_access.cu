@@ -158,14 +158,13 @@ static cudaError_t ra_shape(glc_ctx* ctx, const RAArgs& a, int mode, cudaStream_
   return cudaGetLastError();
 }
 
-// Launch shapes (lookups per thread, CTAs per SM), measured on 100M lookups into a 64M int64
-// column: packed fields -> 2 lookups per thread at 6 CTAs/SM (40 registers, more warps resident);
-// pre-unpacked residuals (every lookup a DRAM sector) -> 8 lookups per thread.  GLC_RA_SHAPE
-// overrides the choice for tuning sweeps.
+// Launch shapes (lookups per thread, CTAs per SM): 0 = (4, 1), 1 = (4, 5), 2 = (2, 8), 3 = (8, 2),
+// 4 = (2, 6).  The untuned defaults were measured on 100M lookups into a 64M int64 column: packed
+// fields -> shape 4 (40 registers, more warps resident); pre-unpacked residuals (every lookup a
+// DRAM sector) -> shape 3.  The context's tuning table picks per element type and field width;
+// GLC_RA_SHAPE overrides it for sweeps.
 template <typename T, bool PLAIN>
-static cudaError_t ra_typed(glc_ctx* ctx, const RAArgs& a, int mode, cudaStream_t s) {
-  const char* v = getenv("GLC_RA_SHAPE");
-  const int shape = (v && *v) ? atoi(v) : (PLAIN ? 3 : 4);
+static cudaError_t ra_typed(glc_ctx* ctx, const RAArgs& a, int mode, int shape, cudaStream_t s) {
   switch (shape) {
     case 1: return ra_shape<T, PLAIN, 4, 5>(ctx, a, mode, s);
     case 2: return ra_shape<T, PLAIN, 2, 8>(ctx, a, mode, s);
@@ -177,6 +176,13 @@ static cudaError_t ra_typed(glc_ctx* ctx, const RAArgs& a, int mode, cudaStream_
 
 cudaError_t launch_random_access(glc_ctx* ctx, const glc_column* c, int plain_src, const int32_t* pos, int64_t q,
                                  void* out, int32_t fixed_len, cudaStream_t s) {
+  const char* v = getenv("GLC_RA_SHAPE");
+  const int shape = (v && *v) ? atoi(v) : tune_entry(ctx, c->dtype, c->max_bits, plain_src).ra_shape;
+  return launch_random_access_shape(ctx, c, plain_src, pos, q, out, fixed_len, shape, s);
+}
+
+cudaError_t launch_random_access_shape(glc_ctx* ctx, const glc_column* c, int plain_src, const int32_t* pos, int64_t q,
+                                       void* out, int32_t fixed_len, int shape, cudaStream_t s) {
   if (q <= 0) return cudaSuccess;
   RAArgs a;
   a.desc = c->d_desc;
@@ -206,10 +212,10 @@ cudaError_t launch_random_access(glc_ctx* ctx, const glc_column* c, int plain_sr
   if (a.sample_stride < 1) a.sample_stride = 1;
   a.nsample = (int32_t)((c->P + a.sample_stride - 1) / a.sample_stride);
   switch (c->dtype) {
-    case GLC_I32: return plain_src ? ra_typed<int32_t, true>(ctx, a, mode, s) : ra_typed<int32_t, false>(ctx, a, mode, s);
-    case GLC_I64: return plain_src ? ra_typed<int64_t, true>(ctx, a, mode, s) : ra_typed<int64_t, false>(ctx, a, mode, s);
-    case GLC_U64: return plain_src ? ra_typed<uint64_t, true>(ctx, a, mode, s) : ra_typed<uint64_t, false>(ctx, a, mode, s);
-    case GLC_U32: return plain_src ? ra_typed<uint32_t, true>(ctx, a, mode, s) : ra_typed<uint32_t, false>(ctx, a, mode, s);
+    case GLC_I32: return plain_src ? ra_typed<int32_t, true>(ctx, a, mode, shape, s) : ra_typed<int32_t, false>(ctx, a, mode, shape, s);
+    case GLC_I64: return plain_src ? ra_typed<int64_t, true>(ctx, a, mode, shape, s) : ra_typed<int64_t, false>(ctx, a, mode, shape, s);
+    case GLC_U64: return plain_src ? ra_typed<uint64_t, true>(ctx, a, mode, shape, s) : ra_typed<uint64_t, false>(ctx, a, mode, shape, s);
+    case GLC_U32: return plain_src ? ra_typed<uint32_t, true>(ctx, a, mode, shape, s) : ra_typed<uint32_t, false>(ctx, a, mode, shape, s);
   }
   return cudaErrorInvalidValue;
 }

@@ -1,0 +1,243 @@
+// tune.cu -- measured choice of launch shapes per element type and field width.
+//
+// The reference fixes its launch shapes at compile time (core/CudaUtils.cuh:16-21).  Here each
+// context holds a table, indexed by element type, widest-field bucket (<= 8, 16, 24, 32, 48, 64
+// bits) and residual source (packed / pre-unpacked), of
+//   - the decode kernel's TMA ring depth (2, 3, 4) and the unroll depth of its full-tile loop
+//     (1, 2, 4): the values each CTA keeps in flight per tile;
+//   - the random-access launch shape (lookups per thread x CTAs per SM, five candidates).
+// glc_autotune times every candidate on a synthetic fixed-partitioned column whose fields have the
+// bucket's width (48M values, larger than L2) and keeps the fastest; the table can be written to
+// and read from a text file keyed by the device (name, SM count, compute capability).
+#include <cstdio>
+#include <cstring>
+#include <string>
+
+#include "glc_internal.h"
+
+using namespace glc;
+
+namespace {
+
+constexpr int kTuneVersion = 1;
+constexpr int64_t kTuneValues = 48ll << 20;
+constexpr int64_t kTuneLookups = 16ll << 20;
+constexpr int kNoiseBits[kTuneBuckets] = {5, 13, 21, 29, 45, 59};  // fields of 6..60 bits
+
+__device__ __forceinline__ uint64_t mix64(uint64_t x) {  // splitmix64 finaliser
+  x ^= x >> 30;
+  x *= 0xbf58476d1ce4e5b9ull;
+  x ^= x >> 27;
+  x *= 0x94d049bb133111ebull;
+  return x ^ (x >> 31);
+}
+
+// v[i] = base + slope * i + noise, noise uniform over `noise_bits` bits.
+template <typename T>
+__global__ void fill_line_noise(T* v, int64_t n, int noise_bits, uint64_t seed) {
+  const bool wide = sizeof(T) == 8;
+  const uint64_t base = wide ? (1ull << 40) : 1000ull, slope = wide ? 1000ull : 3ull;
+  const uint64_t mask = (1ull << noise_bits) - 1;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    v[i] = (T)(base + slope * (uint64_t)i + (mix64((uint64_t)i ^ seed) & mask));
+}
+
+__global__ void fill_positions(int32_t* pos, int64_t q, int64_t n, uint64_t seed) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < q; i += (int64_t)gridDim.x * blockDim.x)
+    pos[i] = (int32_t)(mix64((uint64_t)i * 0x9e3779b97f4a7c15ull + seed) % (uint64_t)n);
+}
+
+std::string device_key(const glc_ctx* ctx) {
+  cudaDeviceProp p;
+  if (cudaGetDeviceProperties(&p, ctx->device) != cudaSuccess) return "unknown";
+  std::string name = p.name;
+  for (char& ch : name)
+    if (ch == ' ') ch = '_';
+  char buf[256];
+  snprintf(buf, sizeof buf, "glc-tune %d %d %d.%d %s", kTuneVersion, p.multiProcessorCount, p.major, p.minor,
+           name.c_str());
+  return buf;
+}
+
+bool tune_save(const glc_ctx* ctx, const char* path) {
+  FILE* f = fopen(path, "w");
+  if (!f) return false;
+  fprintf(f, "%s\n", device_key(ctx).c_str());
+  for (int d = 0; d < 4; d++)
+    for (int b = 0; b < kTuneBuckets; b++)
+      for (int p = 0; p < 2; p++) {
+        const TuneEntry& t = ctx->tune[d][b][p];
+        fprintf(f, "%d %d %d %d %d %d %.3f %.4f\n", d, b, p, t.decode_stages, t.decode_unroll, t.ra_shape,
+                t.decode_gbs, t.ra_glookups);
+      }
+  return fclose(f) == 0;
+}
+
+// Mean device time of `reps` launches after two warm-up launches, in milliseconds (< 0: failure).
+template <typename F>
+float time_launches(F launch, cudaStream_t s, cudaEvent_t e0, cudaEvent_t e1, int reps = 5) {
+  for (int i = 0; i < 2; i++)
+    if (launch() != cudaSuccess) return -1.f;
+  if (cudaEventRecord(e0, s) != cudaSuccess) return -1.f;
+  for (int i = 0; i < reps; i++)
+    if (launch() != cudaSuccess) return -1.f;
+  if (cudaEventRecord(e1, s) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess) return -1.f;
+  float ms = 0.f;
+  if (cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess) return -1.f;
+  return ms / reps;
+}
+
+glc_status tfail(glc_ctx* ctx, glc_status st, const std::string& msg) {
+  ctx->err = msg;
+  return st;
+}
+
+}  // namespace
+
+void glc::tune_defaults(glc_ctx* ctx) {
+  for (int d = 0; d < 4; d++)
+    for (int b = 0; b < kTuneBuckets; b++)
+      for (int p = 0; p < 2; p++) {
+        TuneEntry& t = ctx->tune[d][b][p];
+        t.decode_stages = 2;
+        t.decode_unroll = 2;
+        t.ra_shape = p ? 3 : 4;
+        t.measured = 0;
+        t.decode_gbs = 0.f;
+        t.ra_glookups = 0.f;
+      }
+}
+
+bool glc::tune_load(glc_ctx* ctx, const char* path) {
+  FILE* f = fopen(path, "r");
+  if (!f) return false;
+  char line[512];
+  bool ok = fgets(line, sizeof line, f) != nullptr;
+  if (ok) {
+    line[strcspn(line, "\n")] = 0;
+    ok = device_key(ctx) == line;
+  }
+  TuneEntry tab[4][kTuneBuckets][2];
+  int seen = 0;
+  while (ok && fgets(line, sizeof line, f)) {
+    int d, b, p, st, un, ra;
+    float gbs, gl;
+    if (sscanf(line, "%d %d %d %d %d %d %f %f", &d, &b, &p, &st, &un, &ra, &gbs, &gl) != 8) { ok = false; break; }
+    if (d < 0 || d > 3 || b < 0 || b >= kTuneBuckets || p < 0 || p > 1 || st < 2 || st > 4 ||
+        (un != 1 && un != 2 && un != 4) || ra < 0 || ra > 4) { ok = false; break; }
+    tab[d][b][p] = TuneEntry{st, un, ra, 1, gbs, gl};
+    seen++;
+  }
+  fclose(f);
+  if (!ok || seen != 4 * kTuneBuckets * 2) return false;
+  std::memcpy(ctx->tune, tab, sizeof tab);
+  return true;
+}
+
+extern "C" {
+
+glc_status glc_tune_get(const glc_ctx* ctx, glc_dtype dtype, int32_t field_bits, int32_t preunpacked,
+                        glc_tune_entry* out) {
+  if (!ctx || !out || (int)dtype < 0 || (int)dtype > 3 || field_bits < 0 || field_bits > 64) return GLC_ERR_INVALID_ARG;
+  const TuneEntry& t = tune_entry(ctx, dtype, field_bits, preunpacked);
+  *out = glc_tune_entry{t.decode_stages, t.decode_unroll, t.ra_shape, t.measured, t.decode_gbs, t.ra_glookups};
+  return GLC_OK;
+}
+
+glc_status glc_tune_set(glc_ctx* ctx, glc_dtype dtype, int32_t field_bits, int32_t preunpacked,
+                        const glc_tune_entry* e) {
+  if (!ctx || !e || (int)dtype < 0 || (int)dtype > 3 || field_bits < 0 || field_bits > 64) return GLC_ERR_INVALID_ARG;
+  if (e->decode_stages < 2 || e->decode_stages > 4 || (e->decode_unroll != 1 && e->decode_unroll != 2 &&
+      e->decode_unroll != 4) || e->ra_shape < 0 || e->ra_shape > 4)
+    return tfail(ctx, GLC_ERR_INVALID_ARG, "tune entry out of range");
+  ctx->tune[(int)dtype][tune_bucket(field_bits)][preunpacked ? 1 : 0] =
+      TuneEntry{e->decode_stages, e->decode_unroll, e->ra_shape, e->measured, e->decode_gbs, e->ra_glookups};
+  return GLC_OK;
+}
+
+glc_status glc_autotune(glc_ctx* ctx, const char* cache_path, int32_t flags) {
+  if (!ctx || (flags & ~GLC_TUNE_FORCE) != 0) return GLC_ERR_INVALID_ARG;
+  if (cache_path && !(flags & GLC_TUNE_FORCE) && tune_load(ctx, cache_path)) return GLC_OK;
+  cudaSetDevice(ctx->device);
+  cudaStream_t s = ctx->own_stream;
+  void* vals = nullptr;
+  void* out = nullptr;
+  int32_t* pos = nullptr;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  TuneEntry tab[4][kTuneBuckets][2];
+  std::memcpy(tab, ctx->tune, sizeof tab);
+  glc_status st = GLC_OK;
+  cudaError_t e;
+  if ((e = cudaMalloc(&vals, 8 * kTuneValues)) != cudaSuccess || (e = cudaMalloc(&out, 8 * kTuneValues + 16)) != cudaSuccess ||
+      (e = cudaMalloc((void**)&pos, 4 * kTuneLookups)) != cudaSuccess || (e = cudaEventCreate(&e0)) != cudaSuccess ||
+      (e = cudaEventCreate(&e1)) != cudaSuccess) {
+    st = tfail(ctx, GLC_ERR_OOM, std::string("autotune: ") + cudaGetErrorString(e));
+  }
+  if (st == GLC_OK) fill_positions<<<ctx->num_sms * 8, 256, 0, s>>>(pos, kTuneLookups, kTuneValues, 7);
+  for (int d = 0; d < 4 && st == GLC_OK; d++) {
+    const glc_dtype dt = (glc_dtype)d;
+    const int nb = dtype_size(dt) == 8 ? kTuneBuckets : 4;  // 32-bit fields at most for 4-byte types
+    for (int b = 0; b < nb && st == GLC_OK; b++) {
+      const int grid = ctx->num_sms * 8;
+      switch (dt) {
+        case GLC_I32: fill_line_noise<<<grid, 256, 0, s>>>((int32_t*)vals, kTuneValues, kNoiseBits[b], 11 + b); break;
+        case GLC_U32: fill_line_noise<<<grid, 256, 0, s>>>((uint32_t*)vals, kTuneValues, kNoiseBits[b], 11 + b); break;
+        case GLC_I64: fill_line_noise<<<grid, 256, 0, s>>>((int64_t*)vals, kTuneValues, kNoiseBits[b], 11 + b); break;
+        default: fill_line_noise<<<grid, 256, 0, s>>>((uint64_t*)vals, kTuneValues, kNoiseBits[b], 11 + b); break;
+      }
+      glc_column* col = nullptr;
+      st = glc_compress(ctx, dt, vals, kTuneValues, 0, GLC_PART_FIXED, 4096, &col, nullptr, s);
+      if (st != GLC_OK) break;
+      const int bucket = tune_bucket(col->max_bits);
+      for (int plain = 0; plain < 2 && st == GLC_OK; plain++) {
+        if (plain && (st = glc_preunpack(ctx, col, 0, s)) != GLC_OK) break;
+        TuneEntry best = tab[d][bucket][plain];
+        float best_ms = 1e30f;
+        for (int stages = 2; stages <= 4; stages++)
+          for (int unroll : {1, 2, 4}) {
+            if (plain && unroll != 2) continue;  // the pre-unpacked decode has no unroll choice
+            const float ms = time_launches([&] {
+              return launch_decode_shape(ctx, col, plain, 0, 0, kTuneValues, out, stages, unroll, s);
+            }, s, e0, e1);
+            if (ms < 0.f) { st = tfail(ctx, GLC_ERR_CUDA, "autotune: decode launch failed"); break; }
+            if (ms < best_ms) {
+              best_ms = ms;
+              best.decode_stages = stages;
+              best.decode_unroll = unroll;
+              best.decode_gbs = (float)(dtype_size(dt) * (double)kTuneValues / (ms * 1e6));
+            }
+          }
+        float best_ra = 1e30f;
+        for (int shape = 0; shape < 5 && st == GLC_OK; shape++) {
+          const float ms = time_launches([&] {
+            return launch_random_access_shape(ctx, col, plain, pos, kTuneLookups, out, col->fixed_len, shape, s);
+          }, s, e0, e1);
+          if (ms < 0.f) { st = tfail(ctx, GLC_ERR_CUDA, "autotune: random-access launch failed"); break; }
+          if (ms < best_ra) {
+            best_ra = ms;
+            best.ra_shape = shape;
+            best.ra_glookups = (float)(kTuneLookups / (ms * 1e6));
+          }
+        }
+        best.measured = 1;
+        tab[d][bucket][plain] = best;
+      }
+      glc_column_free(col);
+      if (st == GLC_OK) st = glc_sync(ctx, s);  // a device-side wait that gave up fails the tuning
+    }
+    if (st == GLC_OK && nb < kTuneBuckets)  // wider buckets of 4-byte types reuse the 32-bit choice
+      for (int b = nb; b < kTuneBuckets; b++)
+        for (int p = 0; p < 2; p++) tab[d][b][p] = tab[d][nb - 1][p];
+  }
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  cudaFree(vals);
+  cudaFree(out);
+  cudaFree(pos);
+  if (st != GLC_OK) return st;
+  std::memcpy(ctx->tune, tab, sizeof tab);
+  if (cache_path && !tune_save(ctx, cache_path)) return tfail(ctx, GLC_ERR_INVALID_ARG, "autotune: cannot write the cache file");
+  return GLC_OK;
+}
+
+}  // extern "C"

@@ -38,6 +38,7 @@ EXPORTS = [
     "glc_batch_column", "glc_batch_decompress", "glc_batch_free", "glc_server_create", "glc_server_destroy",
     "glc_server_admit", "glc_server_admit_blob", "glc_server_evict", "glc_server_submit", "glc_server_poll",
     "glc_server_drain", "glc_server_get_stats", "glc_server_now_ns", "glc_server_columns",
+    "glc_autotune", "glc_tune_get", "glc_tune_set",
 ]
 REQ_LOOKUP, REQ_RANGE = 0, 1
 SERVER_RESERVE = 1
@@ -60,6 +61,17 @@ class ColumnInfo(ctypes.Structure):
         ("d_delta_array_bit_offsets", ctypes.c_void_p), ("d_error_bounds", ctypes.c_void_p),
         ("delta_array", ctypes.c_void_p), ("d_plain_deltas", ctypes.c_void_p),
     ]
+
+
+class TuneEntry(ctypes.Structure):
+    _fields_ = [("decode_stages", ctypes.c_int32), ("decode_unroll", ctypes.c_int32), ("ra_shape", ctypes.c_int32),
+                ("measured", ctypes.c_int32), ("decode_gbs", ctypes.c_float), ("ra_glookups", ctypes.c_float)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+TUNE_FORCE = 1
 
 
 class ServerConfig(ctypes.Structure):
@@ -141,6 +153,9 @@ def load() -> ctypes.CDLL:
         "glc_server_get_stats": ([vp, ctypes.POINTER(ServerStats)], c_int),
         "glc_server_now_ns": ([], i64),
         "glc_server_columns": ([vp, vp, i32, ctypes.POINTER(i32)], c_int),
+        "glc_autotune": ([vp, ctypes.c_char_p, i32], c_int),
+        "glc_tune_get": ([vp, c_int, i32, i32, ctypes.POINTER(TuneEntry)], c_int),
+        "glc_tune_set": ([vp, c_int, i32, i32, ctypes.POINTER(TuneEntry)], c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
@@ -182,6 +197,23 @@ class Context:
 
     def sync(self, stream: int = 0):
         self.check(self.lib.glc_sync(self.handle, ctypes.c_void_p(stream)))
+
+
+def autotune(ctx: "Context", cache_path: Optional[str] = None, force: bool = False):
+    """Measure and keep the fastest launch shapes per element type and field width (glc_autotune)."""
+    ctx.check(ctx.lib.glc_autotune(ctx.handle, cache_path.encode() if cache_path else None,
+                                   TUNE_FORCE if force else 0))
+
+
+def tune_get(ctx: "Context", dtype: int, field_bits: int, preunpacked: bool = False) -> TuneEntry:
+    e = TuneEntry()
+    ctx.check(ctx.lib.glc_tune_get(ctx.handle, dtype, field_bits, 1 if preunpacked else 0, ctypes.byref(e)))
+    return e
+
+
+def tune_set(ctx: "Context", dtype: int, field_bits: int, preunpacked: bool, stages: int, unroll: int, ra_shape: int):
+    e = TuneEntry(stages, unroll, ra_shape, 0, 0.0, 0.0)
+    ctx.check(ctx.lib.glc_tune_set(ctx.handle, dtype, field_bits, 1 if preunpacked else 0, ctypes.byref(e)))
 
 
 class Column:

@@ -221,6 +221,36 @@ GLC_API glc_status glc_batch_free(glc_batch* batch);
 GLC_API glc_status glc_decompress_range_noalloc(const glc_column* col, int64_t first, int64_t count,
                                                 void* host_out, glc_stream stream);
 
+/* ---- launch-shape tuning (no counterpart in the reference, whose launch shapes are
+ * compile-time constants, core/CudaUtils.cuh:16-21) ---------------------------------------- */
+
+typedef struct glc_tune_entry {
+  int32_t decode_stages;  /* TMA ring depth of the decode kernel: 2, 3 or 4 */
+  int32_t decode_unroll;  /* unroll depth of the decode's full-tile loop: 1, 2 or 4 */
+  int32_t ra_shape;       /* random-access shape 0..4: (lookups per thread, CTAs per SM) =
+                             (4,1), (4,5), (2,8), (8,2), (2,6) */
+  int32_t measured;       /* 1 when chosen by glc_autotune, 0 for the built-in default */
+  float decode_gbs;       /* decoded GB/s of the chosen shape on the tuning column */
+  float ra_glookups;      /* G lookups/s of the chosen random-access shape */
+} glc_tune_entry;
+
+enum { GLC_TUNE_FORCE = 1 };
+
+/* Time every candidate decode shape (ring depth x unroll depth) and random-access shape on this
+ * context's device, per element type, widest-field bucket (<= 8, 16, 24, 32, 48, 64 bits) and
+ * residual source (packed, pre-unpacked), each on a synthetic fixed-partitioned column of 48M
+ * values with fields of that width, and keep the fastest in the context (about 2 s).  With
+ * cache_path, results already stored there for this device (name, SM count, compute capability)
+ * are loaded instead (unless GLC_TUNE_FORCE), and new results are written there.  A context also
+ * loads the file named by the GLC_TUNE_CACHE environment variable when it is created. */
+GLC_API glc_status glc_autotune(glc_ctx* ctx, const char* cache_path, int32_t flags);
+
+/* The shapes used for columns of `dtype` whose widest field has `field_bits` bits. */
+GLC_API glc_status glc_tune_get(const glc_ctx* ctx, glc_dtype dtype, int32_t field_bits, int32_t preunpacked,
+                                glc_tune_entry* out);
+GLC_API glc_status glc_tune_set(glc_ctx* ctx, glc_dtype dtype, int32_t field_bits, int32_t preunpacked,
+                                const glc_tune_entry* entry);
+
 /* ---- serving: resident columns and continuously batched requests (no counterpart in the
  * reference, whose every call is a blocking host round trip) ------------------------------ */
 

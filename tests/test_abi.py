@@ -58,3 +58,10 @@ def test_server_entry_points_reject_null_arguments():
     assert lib.glc_server_drain(None, 0) == glc.ERR_INVALID_ARG
     t0 = lib.glc_server_now_ns()
     assert lib.glc_server_now_ns() >= t0 > 0
+
+
+def test_tuning_entry_points_reject_null_arguments():
+    lib = glc.load()
+    assert lib.glc_autotune(None, None, 0) == glc.ERR_INVALID_ARG
+    assert lib.glc_tune_get(None, 0, 8, 0, None) == glc.ERR_INVALID_ARG
+    assert lib.glc_tune_set(None, 0, 8, 0, None) == glc.ERR_INVALID_ARG

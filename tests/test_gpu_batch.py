@@ -79,6 +79,7 @@ def test_batch_decode(use_graph):
     for rep in range(3):  # replays of the same graph / launch
         for o in outs:
             o.fill_(-1)
+        torch.cuda.synchronize()  # the library runs on its own stream
         batch.decompress([o.data_ptr() for o in outs], use_graph=use_graph)
         ctx.sync()
         torch.cuda.synchronize()
@@ -87,6 +88,7 @@ def test_batch_decode(use_graph):
             assert np.array_equal(got, v), (rep, dt, len(v))
     # new outputs rebuild the work list (and the graph)
     outs2 = [torch.zeros(max(len(v), 1), dtype=DT[dt][1], device="cuda:0") for dt, v in cols]
+    torch.cuda.synchronize()
     batch.decompress([o.data_ptr() for o in outs2], use_graph=use_graph)
     torch.cuda.synchronize()
     for (dt, v), o in zip(cols, outs2):
@@ -100,6 +102,7 @@ def test_batch_over_existing_columns():
     singles = [glc.compress_device(ctx, dt, v.ctypes.data, len(v), glc.VARIABLE, host=True) for dt, v in cols]
     batch = glc.Batch.of(ctx, singles)
     outs = [torch.zeros(max(len(v), 1), dtype=DT[dt][1], device="cuda:0") for dt, v in cols]
+    torch.cuda.synchronize()
     batch.decompress([o.data_ptr() for o in outs], use_graph=True)
     torch.cuda.synchronize()
     for (dt, v), o in zip(cols, outs):
@@ -119,10 +122,12 @@ def test_batch_column_random_access_and_range():
             continue
         pos = np.random.default_rng(1).integers(0, len(v), 1000).astype(np.int32)
         out = np.zeros(len(pos), DT[dt][0])
+        torch.cuda.synchronize()
         glc.random_access_into(ctx, bc, pos.ctypes.data, len(pos), out.ctypes.data, host_in=True, host_out=True)
         assert np.array_equal(out, v[pos])
         first = len(v) // 3
         r = np.zeros(len(v) - first, DT[dt][0])
+        torch.cuda.synchronize()
         glc.decompress_range_into(ctx, bc, first, len(r), r.ctypes.data, host_out=True)
         assert np.array_equal(r, v[first:])
     with pytest.raises(glc.GlcError):

@@ -257,6 +257,7 @@ def test_decode_into_misaligned_device_buffer(offset_bytes):
     codec = _codec(v)
     col, _ = codec.compress(v, True)
     buf = torch.zeros(len(v) + 8, dtype=torch.int32, device="cuda:0")
+    torch.cuda.synchronize()  # the library runs on its own stream
     ptr = buf.data_ptr() + offset_bytes
     glc.decompress_into(codec.ctx, col, ptr, glc.SRC_PACKED)
     glc.decompress_range_into(codec.ctx, col, 3, 1000, ptr, glc.SRC_PACKED)

@@ -70,6 +70,7 @@ def _device_buffers(reqs):
         else:
             r["dout"] = torch.full((r["count"] + 8,), -7, dtype=th_t, device="cuda:0")
             r["optr"] = r["dout"].data_ptr() + r["skew"] * np.dtype(np_t).itemsize
+    torch.cuda.synchronize()  # the server's streams do not wait for torch's
 
 
 def _as_array(reqs, not_before=None):
@@ -118,6 +119,7 @@ def test_each_result_same_alone_and_in_the_mix():
     _device_buffers(reqs)
 
     for r in reqs:  # alone: one request in flight at a time
+        torch.cuda.synchronize()
         server.submit(_as_array([r]))
         server.drain(60_000)
     alone = _results(reqs)
@@ -129,9 +131,11 @@ def test_each_result_same_alone_and_in_the_mix():
     alone_launches = server.stats().launches
     for r in reqs:
         r["dout"].fill_(-7)
+    torch.cuda.synchronize()
     t0 = server.now_ns()
     rng = np.random.default_rng(9)
     arrivals = t0 + np.sort(rng.integers(0, 30_000_000, len(reqs)))  # spread over 30 ms
+    torch.cuda.synchronize()
     server.submit(_as_array(reqs, arrivals))
     server.drain(60_000)
     mixed = _results(reqs)
@@ -158,6 +162,7 @@ def test_everything_submitted_at_once_shares_launches():
     cols = _columns(ctx, server, SPECS[:4])
     reqs = _mixed_requests(cols, 400, seed=6, big=50_000)
     _device_buffers(reqs)
+    torch.cuda.synchronize()
     server.submit(_as_array(reqs))
     server.drain(60_000)
     for r, g in zip(reqs, _results(reqs)):
@@ -186,6 +191,7 @@ def test_admission_budget_and_lru_eviction():
     out = torch.zeros(10, dtype=torch.int64, device="cuda:0")
     r = glc.requests(1)
     r[0] = (glc.REQ_LOOKUP, ids[0], 0, 10, pos.data_ptr(), out.data_ptr(), 0, 0)
+    torch.cuda.synchronize()
     server.submit(r)
     server.drain(10_000)
     ids.append(server.admit(glc.compress_device(ctx, glc.I64, v.ctypes.data, len(v), glc.FIXED, host=True)))
@@ -193,6 +199,7 @@ def test_admission_budget_and_lru_eviction():
     assert st.resident_columns == 2 and st.evictions == 1 and st.resident_bytes <= int(2.5 * one)
     with pytest.raises(glc.GlcError) as e:  # evicted column: the request is refused on the host
         r[0]["column"] = ids[1]
+        torch.cuda.synchronize()
         server.submit(r)
     assert e.value.status == glc.ERR_INVALID_ARG
 
@@ -202,6 +209,7 @@ def test_admission_budget_and_lru_eviction():
     r2[0] = (glc.REQ_LOOKUP, ids[0], 0, 10, pos.data_ptr(), out.data_ptr(), 1, far)
     out2 = torch.zeros(10, dtype=torch.int64, device="cuda:0")
     r2[1] = (glc.REQ_LOOKUP, ids[2], 0, 10, pos.data_ptr(), out2.data_ptr(), 2, far)
+    torch.cuda.synchronize()
     server.submit(r2)
     extra = glc.compress_device(ctx, glc.I64, v.ctypes.data, len(v), glc.FIXED, host=True)
     with pytest.raises(glc.GlcError) as e:
@@ -225,11 +233,13 @@ def test_evict_waits_for_submitted_requests():
     out = torch.zeros(len(v), dtype=torch.int32, device="cuda:0")
     r = glc.requests(1)
     r[0] = (glc.REQ_RANGE, cid, 0, len(v), 0, out.data_ptr(), 0, server.now_ns() + 100_000_000)
+    torch.cuda.synchronize()
     server.submit(r)
     before = server.stats().resident_bytes
     server.evict(cid)
     assert server.stats().resident_bytes == before  # still pinned by the waiting request
     with pytest.raises(glc.GlcError):
+        torch.cuda.synchronize()
         server.submit(r)
     server.drain(10_000)
     assert np.array_equal(out.cpu().numpy().view(np.uint32), v)
@@ -248,14 +258,18 @@ def test_invalid_requests_queue_nothing():
     r[0] = (glc.REQ_RANGE, cid, 0, 100, 0, out.data_ptr(), 0, 0)
     r[1] = (glc.REQ_RANGE, cid, 9_950, 100, 0, out.data_ptr(), 1, 0)  # past the end
     with pytest.raises(glc.GlcError):
+        torch.cuda.synchronize()
         server.submit(r)
     r[1] = (glc.REQ_LOOKUP, cid, 0, 0, 0, out.data_ptr(), 1, 0)  # count 0
     with pytest.raises(glc.GlcError):
+        torch.cuda.synchronize()
         server.submit(r)
     r[1] = (glc.REQ_RANGE, cid + 7, 0, 10, 0, out.data_ptr(), 1, 0)  # unknown column
     with pytest.raises(glc.GlcError):
+        torch.cuda.synchronize()
         server.submit(r)
     assert server.stats().submitted == 0
+    torch.cuda.synchronize()
     server.submit(r[:1])
     server.drain(10_000)
     assert np.array_equal(out.cpu().numpy(), v[:100])
@@ -273,6 +287,7 @@ def test_admit_blob_from_device_memory(oracle, reserve):
     out = torch.zeros(len(v), dtype=torch.int64, device="cuda:0")
     r = glc.requests(1)
     r[0] = (glc.REQ_RANGE, cid, 0, len(v), 0, out.data_ptr(), 0, 0)
+    torch.cuda.synchronize()
     server.submit(r)
     server.drain(10_000)
     assert np.array_equal(out.cpu().numpy().view(np.uint64), v)
@@ -281,7 +296,9 @@ def test_admit_blob_from_device_memory(oracle, reserve):
     host_blob = np.frombuffer(blob, np.uint8).copy()
     cid2 = server.admit_blob(glc.U64, host_blob.ctypes.data, len(blob), host=True)
     out.zero_()
+    torch.cuda.synchronize()
     r[0]["column"] = cid2
+    torch.cuda.synchronize()
     server.submit(r)
     server.drain(10_000)
     assert np.array_equal(out.cpu().numpy().view(np.uint64), v)
