@@ -266,6 +266,12 @@ static glc_status compress_impl(glc_ctx* ctx, glc_dtype dtype, const void* dev_v
   if (mode == GLC_PART_FIXED) {
     c->P = (n + fixed_len - 1) / fixed_len;
     c->fixed_len = fixed_len;
+  } else if (mode == GLC_PART_VARIABLE_V6) {
+    int64_t P = 0;
+    cudaError_t e = launch_partition_v6(ctx, dtype, dev_values, n, kV6Base, &tmp_s, &tmp_e, &P, s);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "GPU partitioner (V6)");
+    c->P = P;
+    c->fixed_len = 0;
   } else {
     std::string perr;
     int64_t P = 0;
@@ -309,7 +315,8 @@ glc_status glc_compress(glc_ctx* ctx, glc_dtype dtype, const void* values, int64
   if (!valid_dtype(dtype)) return fail(ctx, GLC_ERR_INVALID_ARG, "unknown dtype");
   if (n < 0 || n > 0x7fffffffll) return fail(ctx, GLC_ERR_INVALID_ARG, "n must be in [0, 2^31)");
   if (n > 0 && !values) return fail(ctx, GLC_ERR_INVALID_ARG, "null values");
-  if (mode != GLC_PART_FIXED && mode != GLC_PART_VARIABLE) return fail(ctx, GLC_ERR_INVALID_ARG, "unknown partitioning");
+  if (mode != GLC_PART_FIXED && mode != GLC_PART_VARIABLE && mode != GLC_PART_VARIABLE_V6)
+    return fail(ctx, GLC_ERR_INVALID_ARG, "unknown partitioning");
   if (mode == GLC_PART_FIXED && fixed_partition_len <= 0)
     return fail(ctx, GLC_ERR_INVALID_ARG, "fixed partition length must be positive");
   cudaSetDevice(ctx->device);
@@ -353,15 +360,18 @@ glc_status glc_compress(glc_ctx* ctx, glc_dtype dtype, const void* values, int64
   return GLC_OK;
 }
 
-glc_status glc_partition_variable(glc_ctx* ctx, glc_dtype dtype, const void* values, int64_t n, int flags,
-                                  int32_t* starts, int32_t* ends, int64_t cap, int64_t* num_partitions,
-                                  glc_stream stream) {
+// Partition boundaries only: the split/merge partitioner (v6_base == 0) or the reference's GPU
+// partitioner with that base size.
+static glc_status partition_only(glc_ctx* ctx, glc_dtype dtype, const void* values, int64_t n, int flags,
+                                 int32_t v6_base, int32_t* starts, int32_t* ends, int64_t cap,
+                                 int64_t* num_partitions, glc_stream stream) {
   if (!ctx || !num_partitions) return fail(ctx, GLC_ERR_INVALID_ARG, "null argument");
   if (!valid_dtype(dtype) || n < 0 || n > 0x7fffffffll) return fail(ctx, GLC_ERR_INVALID_ARG, "bad dtype or n");
   cudaSetDevice(ctx->device);
   cudaStream_t s = pick(ctx, stream);
   *num_partitions = 0;
   if (n == 0) return GLC_OK;
+  if (n > 0 && !values) return fail(ctx, GLC_ERR_INVALID_ARG, "null values");
   const void* dev_values = values;
   void* staged = nullptr;
   if (flags & GLC_HOST_IN) {
@@ -374,7 +384,8 @@ glc_status glc_partition_variable(glc_ctx* ctx, glc_dtype dtype, const void* val
   int32_t* de = nullptr;
   int64_t P = 0;
   std::string perr;
-  cudaError_t e = launch_partition_variable(ctx, dtype, dev_values, n, &ds, &de, &P, s, &perr);
+  cudaError_t e = v6_base > 0 ? launch_partition_v6(ctx, dtype, dev_values, n, v6_base, &ds, &de, &P, s)
+                              : launch_partition_variable(ctx, dtype, dev_values, n, &ds, &de, &P, s, &perr);
   if (staged) cudaFreeAsync(staged, s);
   if (e != cudaSuccess) return perr.empty() ? cuda_fail(ctx, e, "partition") : fail(ctx, GLC_ERR_CUDA, perr);
   *num_partitions = P;
@@ -391,6 +402,20 @@ glc_status glc_partition_variable(glc_ctx* ctx, glc_dtype dtype, const void* val
   cudaFreeAsync(de, s);
   if (flags & GLC_HOST_OUT) CK(cudaStreamSynchronize(s), "partition: sync");
   return st;
+}
+
+glc_status glc_partition_variable(glc_ctx* ctx, glc_dtype dtype, const void* values, int64_t n, int flags,
+                                  int32_t* starts, int32_t* ends, int64_t cap, int64_t* num_partitions,
+                                  glc_stream stream) {
+  return partition_only(ctx, dtype, values, n, flags, 0, starts, ends, cap, num_partitions, stream);
+}
+
+glc_status glc_partition_v6(glc_ctx* ctx, glc_dtype dtype, const void* values, int64_t n, int flags,
+                            int32_t base_size, int32_t* starts, int32_t* ends, int64_t cap, int64_t* num_partitions,
+                            glc_stream stream) {
+  if (ctx && (base_size < 2 || base_size > (1 << 26) || (base_size & 1)))
+    return fail(ctx, GLC_ERR_INVALID_ARG, "base size must be even and in [2, 2^26]");
+  return partition_only(ctx, dtype, values, n, flags, base_size, starts, ends, cap, num_partitions, stream);
 }
 
 // ---------------------------------------------------------------------------------------

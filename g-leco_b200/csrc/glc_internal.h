@@ -206,5 +206,9 @@ cudaError_t launch_multi_lookup(const RAColumn* cols, const RARequest* reqs, int
 cudaError_t launch_partition_variable(glc_ctx* ctx, glc_dtype dt, const void* values, int64_t n,
                                       int32_t** d_starts, int32_t** d_ends, int64_t* P, cudaStream_t s,
                                       std::string* err);
+// partition_v6.cu: the reference's GPU partitioner boundaries (pool-allocated starts/ends)
+constexpr int32_t kV6Base = 2048;  // base size compress passes (api/G-LeCo.cuh:384-387)
+cudaError_t launch_partition_v6(glc_ctx* ctx, glc_dtype dt, const void* values, int64_t n, int32_t base,
+                                int32_t** d_starts, int32_t** d_ends, int64_t* P, cudaStream_t s);
 
 }  // namespace glc

@@ -21,7 +21,7 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libglc.so")
 
 I32, I64, U64, U32 = 0, 1, 2, 3
-FIXED, VARIABLE = 0, 1
+FIXED, VARIABLE, VARIABLE_V6 = 0, 1, 2
 SRC_AUTO, SRC_PACKED, SRC_PREUNPACKED = 0, 1, 2
 HOST_IN, HOST_OUT = 1, 2
 OK, ERR_INVALID_ARG, ERR_BAD_BLOB, ERR_OOM, ERR_CUDA, ERR_TIMEOUT, ERR_BUDGET, ERR_UNSUPPORTED = range(8)
@@ -32,7 +32,7 @@ TILE_SIZE = 4096  # the reference's default fixed partition length (core/CudaUti
 
 EXPORTS = [
     "glc_create", "glc_destroy", "glc_last_error", "glc_status_string", "glc_sync", "glc_compress",
-    "glc_partition_variable", "glc_column_free", "glc_column_get_info", "glc_decompress_full",
+    "glc_partition_variable", "glc_partition_v6", "glc_column_free", "glc_column_get_info", "glc_decompress_full",
     "glc_decompress_range", "glc_random_access", "glc_preunpack", "glc_blob_size", "glc_serialize",
     "glc_deserialize", "glc_decompress_range_noalloc", "glc_batch_create", "glc_batch_compress",
     "glc_batch_column", "glc_batch_decompress", "glc_batch_free", "glc_server_create", "glc_server_destroy",
@@ -127,6 +127,7 @@ def load() -> ctypes.CDLL:
         "glc_sync": ([vp, vp], c_int),
         "glc_compress": ([vp, c_int, vp, i64, c_int, c_int, i32, pvp, pi64, vp], c_int),
         "glc_partition_variable": ([vp, c_int, vp, i64, c_int, vp, vp, i64, pi64, vp], c_int),
+        "glc_partition_v6": ([vp, c_int, vp, i64, c_int, i32, vp, vp, i64, pi64, vp], c_int),
         "glc_column_free": ([vp], c_int),
         "glc_column_get_info": ([vp, ctypes.POINTER(ColumnInfo)], c_int),
         "glc_decompress_full": ([vp, vp, c_int, vp, c_int, vp], c_int),
@@ -291,6 +292,18 @@ def random_access_into(ctx: Context, col: Column, pos_ptr: int, q: int, out_ptr:
 
 def preunpack(ctx: Context, col: Column, drop_packed: bool = False, stream: int = 0):
     ctx.check(ctx.lib.glc_preunpack(ctx.handle, col.handle, 1 if drop_packed else 0, ctypes.c_void_p(stream)))
+
+
+def partition_v6(ctx: Context, values: np.ndarray, base: int = 2048):
+    """The reference's GPU partitioner boundaries on the device (glc_partition_v6)."""
+    v = np.ascontiguousarray(values)
+    cap = len(v) // max(1, base // 2) + 64
+    s = np.zeros(cap, np.int32)
+    e = np.zeros(cap, np.int32)
+    P = ctypes.c_int64()
+    ctx.check(ctx.lib.glc_partition_v6(ctx.handle, DTYPE_OF[v.dtype], _ptr(v), len(v), HOST_IN | HOST_OUT, base,
+                                       _ptr(s), _ptr(e), cap, ctypes.byref(P), None))
+    return s[:P.value].copy(), e[:P.value].copy()
 
 
 def partition_variable(ctx: Context, values: np.ndarray):
@@ -481,14 +494,14 @@ class LeCoGPU:
     # api/G-LeCo.cuh:349-614
     def compress(self, values: np.ndarray, use_variable_partitioning: bool, use_gpu_partitioning: bool = False,
                  dataset_name: str = "", fixed_partition_size: int = TILE_SIZE):
-        """Returns (column, compressed_size_bytes).  Both partitioning modes run on the GPU here;
-        ``use_gpu_partitioning`` is accepted for signature parity."""
+        """Returns (column, compressed_size_bytes).  Every partitioning runs on the GPU here;
+        ``use_gpu_partitioning`` selects the reference's GPU partitioner's boundaries."""
         v = np.ascontiguousarray(values, self.np_dtype)
         h = ctypes.c_void_p()
         size = ctypes.c_int64()
+        mode = (VARIABLE_V6 if use_gpu_partitioning else VARIABLE) if use_variable_partitioning else FIXED
         st = self.ctx.lib.glc_compress(self.ctx.handle, self.code, _ptr(v) if len(v) else None, len(v), HOST_IN,
-                                       VARIABLE if use_variable_partitioning else FIXED, fixed_partition_size,
-                                       ctypes.byref(h), ctypes.byref(size), None)
+                                       mode, fixed_partition_size, ctypes.byref(h), ctypes.byref(size), None)
         self.ctx.check(st)
         return Column(self.ctx, h), size.value
 

@@ -47,9 +47,12 @@ typedef enum {
  * int, long long, unsigned long long and unsigned int, app/Main.cu:875-987). */
 typedef enum { GLC_I32 = 0, GLC_I64 = 1, GLC_U64 = 2, GLC_U32 = 3 } glc_dtype;
 
-/* Partitioning: fixed length (api/G-LeCo.cuh:401-416) or variable by model cost
- * (api/G-LeCo.cuh:379-399, compression/CpuPartitioner.cuh). */
-typedef enum { GLC_PART_FIXED = 0, GLC_PART_VARIABLE = 1 } glc_partitioning;
+/* Partitioning: fixed length (api/G-LeCo.cuh:401-416); variable by model cost
+ * (api/G-LeCo.cuh:390-398, compression/CpuPartitioner.cuh: the reference's default variable
+ * mode); or the reference's GPU partitioner, compress(..., use_gpu_partitioning = true)
+ * (api/G-LeCo.cuh:382-389, compression/GpuPartitioner.cuh:34-214): blocks of 16,384 values get
+ * partitions of 8192 / 4096 / 2048 / 1024 values by the quartile of a per-block variance. */
+typedef enum { GLC_PART_FIXED = 0, GLC_PART_VARIABLE = 1, GLC_PART_VARIABLE_V6 = 2 } glc_partitioning;
 
 /* Residual source for decoding: the packed bitstream, or the pre-unpacked int64 residual per
  * value (the reference's "high-throughput" mode, d_plain_deltas). AUTO picks pre-unpacked when
@@ -114,6 +117,15 @@ GLC_API glc_status glc_compress(glc_ctx* ctx, glc_dtype dtype, const void* value
 GLC_API glc_status glc_partition_variable(glc_ctx* ctx, glc_dtype dtype, const void* values, int64_t n,
                                   int flags, int32_t* starts, int32_t* ends, int64_t cap,
                                   int64_t* num_partitions, glc_stream stream);
+
+/* Only the reference's GPU partitioner (GPUVariableLengthPartitionerV6<T>::partition,
+ * compression/GpuPartitioner.cuh:34-214) with its base size (compress uses 2048; even, 2..2^26):
+ * the same boundaries, without the reference's per-partition fit (compress refits them).  Where the
+ * reference would write more partitions than n / (base / 2) (n <= 8 * base and not a multiple of
+ * base / 2) it leaves the last ones unwritten; here every partition is written. */
+GLC_API glc_status glc_partition_v6(glc_ctx* ctx, glc_dtype dtype, const void* values, int64_t n, int flags,
+                                    int32_t base_size, int32_t* starts, int32_t* ends, int64_t cap,
+                                    int64_t* num_partitions, glc_stream stream);
 
 /* Replaces LeCoGPU::cleanup (api/G-LeCo.cuh:793-821). */
 GLC_API glc_status glc_column_free(glc_column* col);

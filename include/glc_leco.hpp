@@ -155,19 +155,21 @@ class LeCoGPU {
   LeCoGPU(const LeCoGPU&) = delete;
   LeCoGPU& operator=(const LeCoGPU&) = delete;
 
-  // api/G-LeCo.cuh:349-614.  Both partitioning modes run on the GPU; use_gpu_partitioning and
-  // dataset_name are accepted for signature parity (no side file is written).
+  // api/G-LeCo.cuh:349-614.  Every partitioning runs on the GPU: variable partitioning uses the
+  // split/merge partitioner (the reference's CPU partitioner's model), or, with
+  // use_gpu_partitioning, the reference's GPU partitioner's boundaries (GLC_PART_VARIABLE_V6).
+  // dataset_name is accepted for signature parity (no side file is written).
   CompressedData<T>* compress(const std::vector<T>& host_data_vec, bool use_variable_partitioning,
                               long long* compressed_size_bytes_result, bool use_gpu_partitioning = false,
                               const std::string& dataset_name = "") {
-    (void)use_gpu_partitioning;
     (void)dataset_name;
     if (!ctx_) return nullptr;
     glc_column* col = nullptr;
     int64_t size = 0;
+    const glc_partitioning mode = !use_variable_partitioning ? GLC_PART_FIXED
+                                  : (use_gpu_partitioning ? GLC_PART_VARIABLE_V6 : GLC_PART_VARIABLE);
     glc_status s = glc_compress(ctx_, kCode, host_data_vec.data(), (int64_t)host_data_vec.size(), GLC_HOST_IN,
-                                use_variable_partitioning ? GLC_PART_VARIABLE : GLC_PART_FIXED, kTileSize, &col,
-                                &size, nullptr);
+                                mode, kTileSize, &col, &size, nullptr);
     if (!ok(s, "compress")) {
       if (compressed_size_bytes_result) *compressed_size_bytes_result = 0;
       return nullptr;

@@ -56,6 +56,10 @@ def _declare(L):
     L.orc_checksum.argtypes = [c_vp, c_u64, c_int]
     L.orc_partition_fixed.restype = c_i64
     L.orc_partition_fixed.argtypes = [c_i64, c_i32, c_vp, c_vp, c_i64]
+    for name in ("orc_partition_v6", "orc_v6_variances"):
+        f = getattr(L, name)
+        f.restype = c_i64
+        f.argtypes = [c_int, c_vp, c_i64, c_i32, c_vp] + ([c_vp, c_i64] if name == "orc_partition_v6" else [c_i64])
     for name in ("orc_partition_variable", "orc_ref_partition_cpu"):
         f = getattr(L, name)
         f.restype = c_i64
@@ -152,6 +156,29 @@ def partition_variable(values: np.ndarray):
 def ref_partition_cpu(values: np.ndarray):
     """The reference's VariableLengthPartitioner (compression/CpuPartitioner.cuh), restated."""
     return _partition_call(lib().orc_ref_partition_cpu, values)
+
+
+def partition_v6(values: np.ndarray, base: int = 2048):
+    """The reference's GPU partitioner boundaries (GPUVariableLengthPartitionerV6, restated)."""
+    values = np.ascontiguousarray(values)
+    code, _ = DTYPES[dtype_code(values)]
+    cap = len(values) // max(1, base // 2) + 64
+    s = np.zeros(cap, np.int32)
+    e = np.zeros(cap, np.int32)
+    got = lib().orc_partition_v6(code, _p(values), len(values), base, _p(s), _p(e), cap)
+    assert got >= 0
+    return s[:got].copy(), e[:got].copy()
+
+
+def v6_variances(values: np.ndarray, base: int = 2048) -> np.ndarray:
+    """The per-block values the V6 thresholds come from."""
+    values = np.ascontiguousarray(values)
+    code, _ = DTYPES[dtype_code(values)]
+    cap = len(values) // (8 * base) + 2
+    out = np.zeros(cap, np.float32)
+    got = lib().orc_v6_variances(code, _p(values), len(values), base, _p(out), cap)
+    assert got >= 0
+    return out[:got].copy()
 
 
 def split_best_end(values: np.ndarray, start: int) -> int:
@@ -352,6 +379,19 @@ def ref_partition(values: np.ndarray, workdir: str):
     P = int(raw[:8].view(np.int64)[0])
     rec = raw[8:].view(np.int32).reshape(P, 3)
     return rec[:, 0].copy(), rec[:, 1].copy(), rec[:, 2].copy()
+
+
+def ref_partition_v6(values: np.ndarray, workdir: str):
+    """The reference's own GPUVariableLengthPartitionerV6 (base 2048, as compress uses it), run
+    from the compiled reference on a GPU: (starts, ends)."""
+    vin = os.path.join(workdir, "ref_values.bin")
+    vout = os.path.join(workdir, "ref_parts_v6.bin")
+    np.ascontiguousarray(values).tofile(vin)
+    _ref_run(["v6", dtype_code(values), vin, vout], cpu_only=False)
+    raw = np.fromfile(vout, np.uint8)
+    P = int(raw[:8].view(np.int64)[0])
+    rec = raw[8:].view(np.int32).reshape(P, 3)
+    return rec[:, 0].copy(), rec[:, 1].copy()
 
 
 def ref_hostdecode(blob: bytes, dtype: str, positions: np.ndarray, workdir: str, repeat: int = 1):

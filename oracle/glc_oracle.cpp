@@ -519,6 +519,86 @@ uint64_t align8(uint64_t x) { return (x + 7) & ~7ULL; }
 }  // namespace
 
 // =======================================================================================
+// (4) The reference's GPU partitioner (use_gpu_partitioning = true):
+//     GPUVariableLengthPartitionerV6<T>::partition, compression/GpuPartitioner.cuh:34-214, with
+//     analyzeDataVarianceFast and createPartitionsFast, compression/PartitioningKernels.cuh:647-727.
+//     Only its boundaries matter: compress refits every partition (api/G-LeCo.cuh:512-530).
+// =======================================================================================
+
+// PartitioningKernels.cuh:647-692: 128 threads per variance block; thread t Kahan-sums v and v^2
+// over positions start + t + 128k (v*v - c contracted to one fma by the reference's compiler);
+// each warp reduces with __shfl_down over 16, 8, 4, 2, 1 (MathHelpers.cuh:91-95), and lane 0 adds
+// float(S2/n - (S1/n)^2) (again one fma) into the block's value.  The reference adds the four
+// warp values with float atomics in completion order; this restatement adds them in warp order.
+template <typename T>
+static float v6_block_variance(const T* v, int64_t start, int64_t end) {
+  double s1[128], s2[128];
+  for (int t = 0; t < 128; t++) {
+    double a = 0.0, b = 0.0, c1 = 0.0, c2 = 0.0;
+    for (int64_t i = start + t; i < end; i += 128) {
+      const double x = (double)v[i];
+      const double y1 = x - c1;
+      const double t1 = a + y1;
+      c1 = (t1 - a) - y1;
+      a = t1;
+      const double y2 = std::fma(x, x, -c2);
+      const double t2 = b + y2;
+      c2 = (t2 - b) - y2;
+      b = t2;
+    }
+    s1[t] = a;
+    s2[t] = b;
+  }
+  const double dn = (double)(end - start);
+  float acc = 0.0f;
+  for (int w = 0; w < 4; w++) {
+    double a[32], b[32];
+    for (int l = 0; l < 32; l++) { a[l] = s1[32 * w + l]; b[l] = s2[32 * w + l]; }
+    for (int off = 16; off > 0; off >>= 1)  // lanes whose source is past the warp keep their value
+      for (int l = 0; l < 32; l++) {
+        const double ya = l + off < 32 ? a[l + off] : a[l];
+        const double yb = l + off < 32 ? b[l + off] : b[l];
+        // lane l reads lane l + off's value from before this step: walk lanes upwards
+        a[l] = a[l] + ya;
+        b[l] = b[l] + yb;
+      }
+    const double m = a[0] / dn;
+    acc = acc + (float)std::fma(-m, m, b[0] / dn);
+  }
+  return acc;
+}
+
+// GpuPartitioner.cuh:44-84 and PartitioningKernels.cuh:695-727: the thresholds are the values of
+// rank nb/4, nb/2, 3nb/4 of the sorted block values.  thrust::sort sorts the value array IN PLACE
+// (GpuPartitioner.cuh:60-61) before createPartitionsFast reads it, so block i is sized by the i-th
+// smallest value, not by its own: 4*base, 2*base, base or base/2 by the first threshold that value
+// is below (with distinct values: the first quarter of the blocks by position get 4*base, and so
+// on).  The last partition of a block ends at the block's end.
+template <typename T>
+static void v6_partition(const T* v, int64_t n, int64_t base, std::vector<int32_t>& starts,
+                         std::vector<int32_t>& ends, std::vector<float>* variances) {
+  starts.clear();
+  ends.clear();
+  if (n <= 0) return;
+  const int64_t blen = 8 * base, nb = (n + blen - 1) / blen;
+  std::vector<float> var((size_t)nb);
+  for (int64_t b = 0; b < nb; b++) var[b] = v6_block_variance(v, b * blen, std::min(n, (b + 1) * blen));
+  std::vector<float> sorted = var;
+  std::sort(sorted.begin(), sorted.end());
+  const float t0 = sorted[nb / 4], t1 = sorted[nb / 2], t2 = sorted[3 * nb / 4];
+  for (int64_t b = 0; b < nb; b++) {
+    const float x = sorted[b];
+    const int64_t size = x < t0 ? 4 * base : (x < t1 ? 2 * base : (x < t2 ? base : base / 2));
+    const int64_t bs = b * blen, be = std::min(n, bs + blen);
+    for (int64_t j = bs; j < be; j += size) {
+      starts.push_back((int32_t)j);
+      ends.push_back((int32_t)std::min(j + size, be));
+    }
+  }
+  if (variances) *variances = var;
+}
+
+// =======================================================================================
 // extern "C" surface used by tests/ through ctypes.
 // =======================================================================================
 #define DISPATCH(dtype, CALL)                                   \
@@ -562,6 +642,26 @@ int64_t orc_partition_variable(int dtype, const void* values, int64_t n, int32_t
   if ((int64_t)s.size() > cap) return -(int64_t)s.size();
   for (size_t i = 0; i < s.size(); i++) { starts[i] = s[i]; ends[i] = e[i]; }
   return (int64_t)s.size();
+}
+
+// The reference's GPU partitioner boundaries (restated).  Returns P, or -P if cap is short.
+int64_t orc_partition_v6(int dtype, const void* values, int64_t n, int32_t base, int32_t* starts, int32_t* ends,
+                         int64_t cap) {
+  std::vector<int32_t> s, e;
+  DISPATCH(dtype, { v6_partition<T>((const T*)values, n, base, s, e, nullptr); });
+  if ((int64_t)s.size() > cap) return -(int64_t)s.size();
+  for (size_t i = 0; i < s.size(); i++) { starts[i] = s[i]; ends[i] = e[i]; }
+  return (int64_t)s.size();
+}
+
+// The per-block values the V6 thresholds are taken from.  Returns the block count.
+int64_t orc_v6_variances(int dtype, const void* values, int64_t n, int32_t base, float* out, int64_t cap) {
+  std::vector<int32_t> s, e;
+  std::vector<float> var;
+  DISPATCH(dtype, { v6_partition<T>((const T*)values, n, base, s, e, &var); });
+  if ((int64_t)var.size() > cap) return -(int64_t)var.size();
+  for (size_t i = 0; i < var.size(); i++) out[i] = var[i];
+  return (int64_t)var.size();
 }
 
 // Best split end of one 128-aligned start (one entry of the device's split table).

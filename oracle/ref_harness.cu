@@ -9,11 +9,16 @@
 //        LeCoGPU<T>::createDirectAccessHandle(blob, size, false) + directRandomAccessCPU
 //        (api/G-LeCo.cuh:1157, :1337): the reference's only host-side decoder.  Prints the
 //        seconds per pass (best of `repeat`) on stdout.
-//   golden     <dtype> <values.bin> <outprefix> <fixed|var>
-//        GPU only: LeCoGPU<T>::compress (api/G-LeCo.cuh:349, stock fixed TILE_SIZE=4096 path or
-//        stock CPU-partitioner path) followed by the CPU serialize (api/G-LeCo.cuh:826).  Writes
-//        <outprefix>.blob and prints the reported compressed size.  Only the reference's
-//        compression kernels run on the GPU; none of its decoders does.
+//   golden     <dtype> <values.bin> <outprefix> <fixed|var|v6>
+//        GPU only: LeCoGPU<T>::compress (api/G-LeCo.cuh:349, stock fixed TILE_SIZE=4096 path,
+//        stock CPU-partitioner path, or the GPU-partitioner path use_gpu_partitioning = true)
+//        followed by the CPU serialize (api/G-LeCo.cuh:826).  Writes <outprefix>.blob and prints
+//        the reported compressed size.  Only the reference's compression kernels run on the GPU;
+//        none of its decoders does.
+//   v6         <dtype> <values.bin> <out.bin>
+//        GPU only: GPUVariableLengthPartitionerV6<T>(values, 2048).partition()
+//        (compression/GpuPartitioner.cuh:34-214, base size as compress passes it).  out.bin as for
+//        `partition`.
 //
 // Without a CUDA device (this harness is also run in CPU-only containers) the CUDA stream
 // calls made by the LeCoGPU constructor/destructor are answered by ref_stubs.cpp when
@@ -87,11 +92,26 @@ template <typename T> static int run_hostdecode(const char* blobp, const char* p
   return 0;
 }
 
-template <typename T> static int run_golden(const char* in, const char* prefix, bool var) {
+template <typename T> static int run_v6(const char* in, const char* out) {
+  std::vector<T> v = as_vec<T>(read_file(in));
+  GPUVariableLengthPartitionerV6<T> vp(v, 2048, 0);
+  std::vector<PartitionInfo> parts = vp.partition();
+  std::vector<uint8_t> o(8 + parts.size() * 12);
+  int64_t P = (int64_t)parts.size();
+  memcpy(o.data(), &P, 8);
+  for (size_t i = 0; i < parts.size(); i++) {
+    int32_t rec[3] = {parts[i].start_idx, parts[i].end_idx, parts[i].delta_bits};
+    memcpy(o.data() + 8 + 12 * i, rec, 12);
+  }
+  write_file(out, o.data(), o.size());
+  return 0;
+}
+
+template <typename T> static int run_golden(const char* in, const char* prefix, bool var, bool gpu_part) {
   std::vector<T> v = as_vec<T>(read_file(in));
   LeCoGPU<T> codec;
   long long size = 0;
-  CompressedData<T>* cd = codec.compress(v, var, &size, false, "");
+  CompressedData<T>* cd = codec.compress(v, var, &size, gpu_part, "");
   if (!cd) { fprintf(stderr, "compress returned null\n"); return 3; }
   SerializedData* sd = codec.serialize(cd);
   if (!sd) { fprintf(stderr, "serialize returned null\n"); return 3; }
@@ -107,7 +127,11 @@ template <typename T> static int dispatch(int argc, char** argv) {
   std::string mode = argv[1];
   if (mode == "partition" && argc >= 5) return run_partition<T>(argv[3], argv[4]);
   if (mode == "hostdecode" && argc >= 6) return run_hostdecode<T>(argv[3], argv[4], argv[5], argc >= 7 ? atoi(argv[6]) : 1);
-  if (mode == "golden" && argc >= 6) return run_golden<T>(argv[3], argv[4], std::string(argv[5]) == "var");
+  if (mode == "golden" && argc >= 6) {
+    const std::string how = argv[5];
+    return run_golden<T>(argv[3], argv[4], how != "fixed", how == "v6");
+  }
+  if (mode == "v6" && argc >= 5) return run_v6<T>(argv[3], argv[4]);
   fprintf(stderr, "bad arguments\n");
   return 2;
 }

@@ -3,7 +3,8 @@
 Runs on a machine with a CUDA GPU and the reference harness built (``make -C oracle ref``,
 which compiles the reference's own headers into oracle/_ref/ref_harness).  For each seeded
 input below it runs the reference's stock ``LeCoGPU<T>::compress`` (fixed TILE_SIZE = 4096
-partitions, or its CPU VariableLengthPartitioner) followed by its CPU ``serialize``
+partitions, its CPU VariableLengthPartitioner, or its GPU partitioner V6 with
+``use_gpu_partitioning = true``) followed by its CPU ``serialize``
 (api/G-LeCo.cuh:349, :826), and stores
 
     tests/golden/<name>.values.npy   the input
@@ -12,7 +13,9 @@ partitions, or its CPU VariableLengthPartitioner) followed by its CPU ``serializ
 
 Only the reference's compression kernels run on the GPU; none of its decoders does.
 
-    python tests/golden/make_golden.py [outdir]
+    python tests/golden/make_golden.py [outdir] [--missing]
+
+``--missing`` generates only the cases that have no blob yet and keeps the others.
 """
 from __future__ import annotations
 
@@ -45,15 +48,27 @@ def cases():
     out.append(("i32_short_fixed", "i32", (7 * i[:1000] - 3000 + rng.integers(0, 16, 1000)).astype(np.int32), "fixed"))
     out.append(("i64_one_fixed", "i64", np.array([-123456789012], np.int64), "fixed"))
     out.append(("i64_ts_var", "i64", W.timestamps(25_000, seed=3), "var"))
+    # the GPU partitioner: sizes of 16,384-value blocks by quartile of a per-block variance
+    out.append(("u64_piecewise_v6", "u64", W.piecewise_linear(120_000, seed=11, mean_segment=9_000), "v6"))
+    out.append(("i64_ts_v6", "i64", W.timestamps(98_304, seed=12), "v6"))
+    amp = np.repeat(np.array([1 << 4, 1 << 12, 1 << 8, 1 << 20, 1 << 2, 1 << 16]), 16_384)
+    noisy = (i[:len(amp)] * 11 + rng.integers(0, 1 << 30, len(amp)) % amp).astype(np.uint32)
+    out.append(("u32_blocks_v6", "u32", noisy, "v6"))
     return out
 
 
-def main(outdir: str = HERE) -> None:
+def main(outdir: str = HERE, missing_only: bool = False) -> None:
     if not os.path.exists(HARNESS):
         raise SystemExit("reference harness not built: make -C oracle ref")
     os.makedirs(outdir, exist_ok=True)
     manifest = {}
+    mpath = os.path.join(outdir, "manifest.json")
+    if missing_only and os.path.exists(mpath):
+        with open(mpath) as f:
+            manifest = json.load(f)
     for name, dt, values, mode in cases():
+        if missing_only and name in manifest and os.path.exists(os.path.join(outdir, f"{name}.blob")):
+            continue
         vpath = os.path.join(outdir, f"{name}.values.npy")
         np.save(vpath, values)
         raw = os.path.join(outdir, f"{name}.values.bin")
@@ -71,4 +86,5 @@ def main(outdir: str = HERE) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else HERE)
+    args = [a for a in sys.argv[1:] if not a.startswith("--")]
+    main(args[0] if args else HERE, "--missing" in sys.argv)

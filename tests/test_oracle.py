@@ -206,3 +206,33 @@ def test_half_away_rounding_identity():
     t = np.trunc(xs)
     exact = np.where(np.abs(xs - t) >= 0.5, t + np.sign(xs), t)
     assert np.array_equal(np.trunc(xs + np.copysign(bias, xs)), exact)
+
+
+def test_v6_partitions_follow_sorted_ranks(oracle):
+    """The reference's GPU partitioner sizes block i by the i-th SMALLEST block value (it sorts the
+    value array in place before the partition kernel reads it): with distinct values the blocks
+    get 8192, 4096, 2048, 1024 by position quartile, whatever their own variance; ties (constant
+    data) push every block into the 1024 class."""
+    rng = np.random.default_rng(4)
+    amps = [1 << 20, 1 << 4, 1 << 12, 1 << 8]  # block k's noise amplitude: values all distinct
+    v = np.concatenate([rng.integers(0, a, 16_384) for a in amps]).astype(np.int64)
+    var = oracle.v6_variances(v, 2048)
+    assert len(var) == 4 and len(set(var.tolist())) == 4
+    s, e = oracle.partition_v6(v, 2048)
+    assert s[0] == 0 and e[-1] == len(v) and np.array_equal(s[1:], e[:-1])
+    for b, size in enumerate((8192, 4096, 2048, 1024)):
+        inside = (s >= 16_384 * b) & (s < 16_384 * (b + 1))
+        assert np.all(e[inside] - s[inside] == size), b
+    s, e = oracle.partition_v6(np.full(4 * 16_384, 77, np.int64), 2048)
+    assert np.all(e - s == 1024)
+
+
+@pytest.mark.parametrize("n", [1, 1000, 16_384, 16_385, 50_000, 300_001])
+def test_v6_partitions_cover_the_column(oracle, n):
+    v = W.piecewise_linear(n, seed=n % 97, mean_segment=5_000)
+    s, e = oracle.partition_v6(v, 2048)
+    assert s[0] == 0 and e[-1] == n and np.array_equal(s[1:], e[:-1])
+    sizes = e - s
+    assert np.all(np.isin(sizes[:-1], [1024, 2048, 4096, 8192]) | ((e[:-1] % 16_384) == 0))
+    col = oracle.compress(v, starts=s, ends=e)
+    assert np.array_equal(oracle.decode_full(col), v)

@@ -89,6 +89,8 @@ def test_golden_reference_blobs(oracle, name, meta):
     # (3) same partitions as the oracle's restatement of the reference's partitioning
     if meta["mode"] == "fixed":
         s, e = oracle.partition_fixed(len(values), 4096)
+    elif meta["mode"] == "v6":  # the reference's GPU partitioner (compress, use_gpu_partitioning)
+        s, e = oracle.partition_v6(values, 2048)
     else:
         s, e = oracle.ref_partition_cpu(values)
     assert np.array_equal(col.starts, s) and np.array_equal(col.ends, e)
