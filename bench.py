@@ -45,6 +45,16 @@ UNIT = "GB/s"
 WORKLOAD = "piecewise_u64_200M_variable"
 DEFAULT_N = 200_000_000
 PROFILE_NOTE = os.path.join(ROOT, "profiles", "decode_piecewise_u64_200M.md")
+# launch shapes measured once per device by glc_autotune (built files, not committed)
+TUNE_CACHE = os.path.join(ROOT, "g-leco_b200", "_build", "tune_cache.txt")
+
+
+def tuned_context(glc, device: int):
+    """A context whose launch shapes come from the autotuner (measured on first use, ~1 s)."""
+    ctx = glc.Context(device)
+    os.makedirs(os.path.dirname(TUNE_CACHE), exist_ok=True)
+    glc.autotune(ctx, TUNE_CACHE)
+    return ctx
 
 
 def measured_peak():
@@ -231,7 +241,7 @@ def run_random_access(args):
     stream = torch.cuda.Stream(dev)
     torch.cuda.set_stream(stream)
     sh = stream.cuda_stream
-    ctx = glc.Context(local)
+    ctx = tuned_context(glc, local)
     n = min(args.n, 64 * 1024 * 1024) if args.n != DEFAULT_N else 64 * 1024 * 1024
     q = args.queries
     L = 4096
@@ -357,7 +367,7 @@ def run_batch(args):
     stream = torch.cuda.Stream(dev)
     torch.cuda.set_stream(stream)
     sh = stream.cuda_stream
-    ctx = glc.Context(local)
+    ctx = tuned_context(glc, local)
     code = {0: glc.I32, 1: glc.I64, 2: glc.U64}
     specs = batch_columns(args.columns, 2.5e9 if args.n == DEFAULT_N else float(args.n))
     gen = torch.Generator(device=dev)
@@ -550,7 +560,7 @@ def run_serving(args):
     stream = torch.cuda.Stream(dev)
     torch.cuda.set_stream(stream)
     sh = stream.cuda_stream
-    ctx = glc.Context(local)
+    ctx = tuned_context(glc, local)
     scale = args.serve_scale
     gens = {"U64": device_piecewise_u64, "I64": device_timestamps_i64, "I32": device_linear_i32}
     sources = []
@@ -835,7 +845,7 @@ def main():
     stream = torch.cuda.Stream(dev)  # every launch and both events on this stream
     torch.cuda.set_stream(stream)
     sh = stream.cuda_stream
-    ctx = glc.Context(local)
+    ctx = tuned_context(glc, local)
 
     n = args.n
     values = make_values(n, rank)
@@ -934,6 +944,7 @@ def main():
             "warmup": args.warmup, "ms_per_step": round(ms_per_step, 4), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
             "config": {"workload": WORKLOAD, "values": n, "partitions": info.num_partitions,
+                       "tuned_shape": glc.tune_get(ctx, glc.U64, info.max_delta_bits).as_dict(),
                        "bits_per_value": round(info.total_bits / n, 3),
                        "compressed_bytes": info.compressed_size_bytes,
                        "compression_ratio": round(decoded_bytes / info.compressed_size_bytes, 3),

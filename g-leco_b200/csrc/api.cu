@@ -250,6 +250,7 @@ glc_status glc_column_get_info(const glc_column* c, glc_column_info* info) {
   info->d_error_bounds = c->d_err;
   info->delta_array = c->d_words;
   info->d_plain_deltas = c->d_plain;
+  info->max_delta_bits = c->max_bits;
   return GLC_OK;
 }
 

@@ -37,6 +37,7 @@ struct glc_batch {
   BatchWork* d_work = nullptr;
   int64_t nwork = 0;
   unsigned long long* d_counter = nullptr;
+  int64_t group_begin[5] = {0, 0, 0, 0, 0};  // work items grouped by element type
   int* d_err = nullptr;
   cudaGraphExec_t graph = nullptr;
 };
@@ -281,8 +282,8 @@ glc_status finish_batch(glc_ctx* ctx, glc_batch* b, cudaStream_t s) {
   void* q = nullptr;
   BCK(cudaMalloc(&q, 64), "batch: counters");
   BCK(cudaMemsetAsync(q, 0, 64, s), "batch: counters");
-  b->d_counter = (unsigned long long*)q;
-  b->d_err = (int*)((char*)q + 16);
+  b->d_counter = (unsigned long long*)q;  // 4 counters, one per element type
+  b->d_err = (int*)((char*)q + 32);
   BCK(cudaStreamSynchronize(s), "batch: sync");
   return GLC_OK;
 }
@@ -301,6 +302,9 @@ glc_status build_work(glc_ctx* ctx, glc_batch* b, void* const* outs, cudaStream_
     if (!c->d_words) return bfail(ctx, GLC_ERR_UNSUPPORTED, "a column of the batch has no packed bitstream");
     for (int64_t t = 0; t < c->ntiles; t++) w.push_back(BatchWork{(int32_t)i, (int32_t)t, 0, c->n, outs[i]});
   }
+  std::vector<int32_t> col_dtype(nc);
+  for (size_t i = 0; i < nc; i++) col_dtype[i] = (int32_t)b->cols[i]->dtype;
+  group_work_by_type(w, col_dtype, b->group_begin);
   if (b->graph) {
     cudaGraphExecDestroy(b->graph);
     b->graph = nullptr;
@@ -529,7 +533,14 @@ glc_status glc_batch_decompress(glc_ctx* ctx, glc_batch* b, void* const* outs, i
   glc_status st = build_work(ctx, b, outs, s);
   if (st != GLC_OK) return st;
   if (b->nwork == 0) return GLC_OK;
-  BatchDecodeArgs a{b->d_cols, b->d_work, b->nwork, b->d_counter, b->d_err, batch_stage_bytes(b->max_bits)};
+  BatchDecodeArgs a;
+  a.cols = b->d_cols;
+  a.work = b->d_work;
+  a.nwork = b->nwork;
+  for (int d = 0; d < 5; d++) a.group_begin[d] = b->group_begin[d];
+  a.counter = b->d_counter;
+  a.err = b->d_err;
+  a.stage_bytes = batch_stage_bytes(b->max_bits);
   if (!use_graph) {
     BCK(launch_batch_decode(a, ctx->num_sms, s), "batch decode");
     return GLC_OK;

@@ -29,6 +29,7 @@
 // Every mbarrier wait is bounded by wall time; on expiry the kernel records an error code and
 // returns after a second bounded wait for its own copies.
 #include <atomic>
+#include <vector>
 #include <climits>
 #include <cstdlib>
 #include <type_traits>
@@ -351,24 +352,17 @@ __global__ void __launch_bounds__(kPCThreads) decode_kernel(DecodeArgs a) {
 // requests of different sizes.  The producer stages each item exactly like a single-column tile;
 // consumers switch on the item's element type (uniform per tile) and reuse decode_tile.
 // ---------------------------------------------------------------------------------------
-template <int kStages>
-__global__ void __launch_bounds__(kPCThreads) batch_decode_kernel(BatchDecodeArgs b) {
-  extern __shared__ __align__(128) uint8_t smem[];
-  __shared__ __align__(128) PartDesc s_desc[kStages][kTileDescs];
-  __shared__ __align__(8) uint64_t full[kStages], empty[kStages];
-  __shared__ StageInfo s_info[kStages];
-  __shared__ int64_t s_item[kStages];
-
+// The work list is grouped by element type ([int32 items][int64][uint64][uint32]) and so is the
+// grid: a CTA decodes items of one type for its whole life, from its group's own counter, so the
+// hot loop is one type's (a per-item type switch doubles the registers and thrashes the
+// instruction cache).  Groups follow one another in block order: as the CTAs of one type run
+// out of items and exit, CTAs of the next type take their place.
+template <typename T, int kStages>
+__device__ __forceinline__ void batch_body(const BatchDecodeArgs& b, int g, uint8_t* smem,
+                                           PartDesc (*s_desc)[kTileDescs], uint64_t* full, uint64_t* empty,
+                                           StageInfo* s_info, int64_t* s_item) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  if (threadIdx.x == 0) {
-    for (int s = 0; s < kStages; s++) {
-      mbar_init(&full[s], 1);
-      mbar_init(&empty[s], kConsumerWarps);
-    }
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-  }
-  __syncthreads();
-
+  const int64_t first = b.group_begin[g], last = b.group_begin[g + 1];
   if (warp == kConsumerWarps) {  // ---- producer ----
     if (lane != 0) return;
     for (int k = 0;; k++) {
@@ -377,10 +371,10 @@ __global__ void __launch_bounds__(kPCThreads) batch_decode_kernel(BatchDecodeArg
         *(volatile int*)b.err = DEVERR_TIMEOUT;  // may be mapped host memory
         break;
       }
-      const int64_t item = (int64_t)atomicAdd(b.counter, 1ull);
+      const int64_t item = first + (int64_t)atomicAdd(b.counter + g, 1ull);
       s_item[s] = item;
       StageInfo si;
-      if (item >= b.nwork) {
+      if (item >= last) {
         si.tile = -1;
         s_info[s] = si;
         mbar_arrive(&full[s]);
@@ -413,7 +407,7 @@ __global__ void __launch_bounds__(kPCThreads) batch_decode_kernel(BatchDecodeArg
   for (int k = 0;; k++) {  // ---- consumers ----
     const int s = k % kStages;
     if (!mbar_wait_bounded(&full[s], (uint32_t)(k / kStages) & 1u)) {
-      if (lane == 0) *(volatile int*)b.err = DEVERR_TIMEOUT;  // may be mapped host memory
+      if (lane == 0) *(volatile int*)b.err = DEVERR_TIMEOUT;
       mbar_wait_bounded(&full[s], (uint32_t)(k / kStages) & 1u);
       break;
     }
@@ -433,16 +427,52 @@ __global__ void __launch_bounds__(kPCThreads) batch_decode_kernel(BatchDecodeArg
     a.hi = w.hi;
     a.out_base = w.out_base;
     a.stage_bytes = b.stage_bytes;
-    const uint8_t* stage = smem + (size_t)s * b.stage_bytes;
-    switch (col.dtype) {
-      case GLC_I32: decode_tile<int32_t, false, false>(a, si, stage, &s_desc[s][0]); break;
-      case GLC_I64: decode_tile<int64_t, false, false>(a, si, stage, &s_desc[s][0]); break;
-      case GLC_U64: decode_tile<uint64_t, false, false>(a, si, stage, &s_desc[s][0]); break;
-      default: decode_tile<uint32_t, false, false>(a, si, stage, &s_desc[s][0]); break;
-    }
+    decode_tile<T, false, false>(a, si, smem + (size_t)s * b.stage_bytes, &s_desc[s][0]);
     __syncwarp();
     if (lane == 0) mbar_arrive(&empty[s]);
   }
+}
+
+template <int kStages>
+__global__ void __launch_bounds__(kPCThreads) batch_decode_kernel(BatchDecodeArgs b) {
+  extern __shared__ __align__(128) uint8_t smem[];
+  __shared__ __align__(128) PartDesc s_desc[kStages][kTileDescs];
+  __shared__ __align__(8) uint64_t full[kStages], empty[kStages];
+  __shared__ StageInfo s_info[kStages];
+  __shared__ int64_t s_item[kStages];
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < kStages; s++) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], kConsumerWarps);
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  int g = 0;
+  while (g < 3 && (int)blockIdx.x >= b.grid_begin[g + 1]) g++;
+  switch (g) {  // the group's element type: GLC_I32, GLC_I64, GLC_U64, GLC_U32
+    case 0: batch_body<int32_t, kStages>(b, g, smem, s_desc, full, empty, s_info, s_item); break;
+    case 1: batch_body<int64_t, kStages>(b, g, smem, s_desc, full, empty, s_info, s_item); break;
+    case 2: batch_body<uint64_t, kStages>(b, g, smem, s_desc, full, empty, s_info, s_item); break;
+    default: batch_body<uint32_t, kStages>(b, g, smem, s_desc, full, empty, s_info, s_item); break;
+  }
+}
+
+// Stable grouping of a work list by element type; group_begin[d] .. group_begin[d + 1] are the
+// items of type d afterwards.
+void group_work_by_type(std::vector<BatchWork>& w, const std::vector<int32_t>& col_dtype, int64_t group_begin[5]) {
+  int64_t cnt[4] = {0, 0, 0, 0};
+  for (const BatchWork& x : w) cnt[col_dtype[x.col] & 3]++;
+  group_begin[0] = 0;
+  for (int d = 0; d < 4; d++) group_begin[d + 1] = group_begin[d] + cnt[d];
+  bool sorted = true;
+  for (size_t i = 1; i < w.size() && sorted; i++) sorted = (col_dtype[w[i - 1].col] & 3) <= (col_dtype[w[i].col] & 3);
+  if (sorted) return;
+  std::vector<BatchWork> out(w.size());
+  int64_t pos[4] = {group_begin[0], group_begin[1], group_begin[2], group_begin[3]};
+  for (const BatchWork& x : w) out[(size_t)pos[col_dtype[x.col] & 3]++] = x;
+  w.swap(out);
 }
 
 // Launch configuration of the batched decode, per device: the shared-memory attribute is raised
@@ -476,10 +506,16 @@ static cudaError_t batch_decode_go(const BatchDecodeArgs& b, int num_sms, bool z
     if (per_sm < 1) per_sm = 1;
     if (cached) g_batch_per_sm[dev][b.stage_bytes / 16].store(per_sm, std::memory_order_relaxed);
   }
-  int64_t grid = (int64_t)per_sm * num_sms;
-  if (grid > b.nwork) grid = b.nwork;
-  if (zero && (e = cudaMemsetAsync(b.counter, 0, sizeof(unsigned long long), s)) != cudaSuccess) return e;
-  kern<<<(unsigned)grid, kPCThreads, smem, s>>>(b);
+  BatchDecodeArgs a = b;
+  a.grid_begin[0] = 0;
+  for (int d = 0; d < 4; d++) {
+    const int64_t items = b.group_begin[d + 1] - b.group_begin[d];
+    const int64_t g = items < (int64_t)per_sm * num_sms ? items : (int64_t)per_sm * num_sms;
+    a.grid_begin[d + 1] = a.grid_begin[d] + (int32_t)g;
+  }
+  if (a.grid_begin[4] <= 0) return cudaSuccess;
+  if (zero && (e = cudaMemsetAsync(b.counter, 0, 4 * sizeof(unsigned long long), s)) != cudaSuccess) return e;
+  kern<<<(unsigned)a.grid_begin[4], kPCThreads, smem, s>>>(a);
   return cudaGetLastError();
 }
 

@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 #include <cstdint>
 #include <atomic>
+#include <vector>
 #include <string>
 #include "glc.h"
 #include "glc_device.cuh"
@@ -168,10 +169,14 @@ struct BatchDecodeArgs {
   const BatchColumn* cols;
   const BatchWork* work;
   int64_t nwork;
-  unsigned long long* counter;  // work-item counter, zeroed per launch
+  int64_t group_begin[5];       // items of element type d: [group_begin[d], group_begin[d + 1])
+  int32_t grid_begin[5];        // CTAs of element type d (set by the launcher)
+  unsigned long long* counter;  // 4 work-item counters (one per type), zeroed per launch
   int* err;
   int stage_bytes;
 };
+// decode.cu: stable grouping of a work list by element type (col_dtype[c] = type of column c)
+void group_work_by_type(std::vector<BatchWork>& w, const std::vector<int32_t>& col_dtype, int64_t group_begin[5]);
 cudaError_t launch_batch_decode(const BatchDecodeArgs& b, int num_sms, cudaStream_t s);
 // Same launch without zeroing the work counter first (the caller's stream has zeroed it).
 cudaError_t launch_batch_decode_zeroed(const BatchDecodeArgs& b, int num_sms, cudaStream_t s);

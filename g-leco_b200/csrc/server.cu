@@ -128,6 +128,7 @@ struct glc_server {
   std::vector<RARequest> w_req;
   std::vector<BatchWork> w_work;
   std::vector<Copy> w_copy;
+  std::vector<int32_t> w_dtype;
   std::vector<int32_t> w_colmap;    // column id -> local index + 1 (valid when w_epoch matches)
   std::vector<uint64_t> w_epoch;
   uint64_t launch_no = 0;
@@ -273,14 +274,22 @@ void launch_slot(glc_server* S, Slot& sl, std::deque<Req*>& ready_l, std::deque<
     if (hi == end) ready_r.pop_front();
   }
 
-  // One host-to-device copy of all tables: [decode work counter u64, pad][lookup columns]
+  // Range pieces grouped by element type (the decode runs one type per CTA).
+  int64_t group_begin[5] = {0, 0, 0, 0, 0};
+  if (!S->w_work.empty()) {
+    S->w_dtype.resize(S->w_bc.size());
+    for (size_t i = 0; i < S->w_bc.size(); i++) S->w_dtype[i] = S->w_bc[i].dtype;
+    group_work_by_type(S->w_work, S->w_dtype, group_begin);
+  }
+
+  // One host-to-device copy of all tables: [4 decode work counters u64][lookup columns]
   // [decode columns][lookup requests][work items].
-  const size_t o_ra = 16;
+  const size_t o_ra = 32;
   const size_t o_bc = align16(o_ra + sizeof(RAColumn) * S->w_ra.size());
   const size_t o_req = align16(o_bc + sizeof(BatchColumn) * S->w_bc.size());
   const size_t o_work = align16(o_req + sizeof(RARequest) * S->w_req.size());
   const size_t total = align16(o_work + sizeof(BatchWork) * S->w_work.size());
-  std::memset(sl.h_meta, 0, 16);
+  std::memset(sl.h_meta, 0, 32);
   std::memcpy(sl.h_meta + o_ra, S->w_ra.data(), sizeof(RAColumn) * S->w_ra.size());
   std::memcpy(sl.h_meta + o_bc, S->w_bc.data(), sizeof(BatchColumn) * S->w_bc.size());
   std::memcpy(sl.h_meta + o_req, S->w_req.data(), sizeof(RARequest) * S->w_req.size());
@@ -301,6 +310,7 @@ void launch_slot(glc_server* S, Slot& sl, std::deque<Req*>& ready_l, std::deque<
     a.cols = (const BatchColumn*)(sl.d_meta + o_bc);
     a.work = (const BatchWork*)(sl.d_meta + o_work);
     a.nwork = (int64_t)S->w_work.size();
+    for (int d = 0; d < 5; d++) a.group_begin[d] = group_begin[d];
     a.counter = (unsigned long long*)sl.d_meta;
     a.err = sl.d_err;
     a.stage_bytes = batch_stage_bytes(max_bits);
@@ -465,7 +475,7 @@ glc_status glc_server_create(glc_ctx* ctx, const glc_server_config* config, glc_
   S->cfg = c;
   // Work items: every full tile of the launch's range values plus two partial tiles per piece.
   S->max_work = c.max_range_values / kDecodeTile + 2ll * c.max_requests + 2;
-  S->meta_cap = align16(16 + (sizeof(RAColumn) + sizeof(BatchColumn)) * kMaxColsPerLaunch + 64 +
+  S->meta_cap = align16(32 + (sizeof(RAColumn) + sizeof(BatchColumn)) * kMaxColsPerLaunch + 64 +
                         sizeof(RARequest) * (size_t)c.max_requests + sizeof(BatchWork) * (size_t)S->max_work);
   S->stage_cap = (size_t)c.max_range_values * 8 + 16 * (size_t)c.max_requests + 256;
   cudaSetDevice(ctx->device);

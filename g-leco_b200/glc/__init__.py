@@ -59,7 +59,7 @@ class ColumnInfo(ctypes.Structure):
         ("d_start_indices", ctypes.c_void_p), ("d_end_indices", ctypes.c_void_p), ("d_model_types", ctypes.c_void_p),
         ("d_model_params", ctypes.c_void_p), ("d_delta_bits", ctypes.c_void_p),
         ("d_delta_array_bit_offsets", ctypes.c_void_p), ("d_error_bounds", ctypes.c_void_p),
-        ("delta_array", ctypes.c_void_p), ("d_plain_deltas", ctypes.c_void_p),
+        ("delta_array", ctypes.c_void_p), ("d_plain_deltas", ctypes.c_void_p), ("max_delta_bits", ctypes.c_int32),
     ]
 
 

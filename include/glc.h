@@ -84,6 +84,7 @@ typedef struct {
   const int64_t* d_error_bounds;
   const uint32_t* delta_array;    /* ceil(total_bits/32) words (+ zero padding)   */
   const int64_t* d_plain_deltas;  /* total_values residuals, or NULL               */
+  int32_t max_delta_bits;         /* widest residual field (selects the tuned launch shapes) */
 } glc_column_info;
 
 /* ---- context ------------------------------------------------------------------------ */

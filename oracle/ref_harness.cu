@@ -18,7 +18,7 @@
 //   v6         <dtype> <values.bin> <out.bin>
 //        GPU only: GPUVariableLengthPartitionerV6<T>(values, 2048).partition()
 //        (compression/GpuPartitioner.cuh:34-214, base size as compress passes it).  out.bin as for
-//        `partition`.
+//        `partition`; prints the seconds partition() took (the upload excluded).
 //
 // Without a CUDA device (this harness is also run in CPU-only containers) the CUDA stream
 // calls made by the LeCoGPU constructor/destructor are answered by ref_stubs.cpp when
@@ -95,7 +95,11 @@ template <typename T> static int run_hostdecode(const char* blobp, const char* p
 template <typename T> static int run_v6(const char* in, const char* out) {
   std::vector<T> v = as_vec<T>(read_file(in));
   GPUVariableLengthPartitionerV6<T> vp(v, 2048, 0);
+  cudaDeviceSynchronize();  // the constructor's upload is not part of partition()
+  auto t0 = std::chrono::steady_clock::now();
   std::vector<PartitionInfo> parts = vp.partition();
+  auto t1 = std::chrono::steady_clock::now();
+  printf("%.9f\n", std::chrono::duration<double>(t1 - t0).count());
   std::vector<uint8_t> o(8 + parts.size() * 12);
   int64_t P = (int64_t)parts.size();
   memcpy(o.data(), &P, 8);
