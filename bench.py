@@ -12,8 +12,9 @@ both larger than L2 (126 MB), so no L2 flush is needed between steps.
 
 ``value`` = decoded bytes (8 B x values, the reference's decode GB/s definition, app/Main.cu)
 / device time, inputs resident in HBM.  ``e2e`` = the same through the public C ABI with host
-buffers: every step deserializes the host (pinned) blob onto the device and decodes into pinned
-host memory.  ``roofline`` = algorithmic bytes (compressed bytes read + decoded bytes written)
+buffers: every step decodes the host (pinned) blob into pinned host memory with
+glc_decode_blob_to_host, which checks the blob, uploads its bitstream, decodes and downloads the
+values in chunks overlapped on three streams.  ``roofline`` = algorithmic bytes (compressed bytes read + decoded bytes written)
 per decode launch / its CUDA-event duration, against the measured HBM copy bandwidth.
 
 With N > 1 (torchrun, one process per GPU) every rank decodes its own column (columns are
@@ -904,13 +905,9 @@ def main():
     lib = ctx.lib
     import ctypes
 
-    def e2e_step():
-        h = ctypes.c_void_p()
-        ctx.check(lib.glc_deserialize(ctx.handle, glc.U64, ctypes.c_void_p(h_blob.data_ptr()), len(blob), glc.HOST_IN,
-                                      0, 0, ctypes.byref(h), ctypes.c_void_p(sh)))
-        c2 = glc.Column(ctx, h)
-        glc.decompress_into(ctx, c2, h_out.data_ptr(), glc.SRC_PACKED, stream=sh, host_out=True)
-        c2.free()
+    def e2e_step():  # glc_decode_blob_to_host: upload, decode and download overlapped in chunks
+        ctx.check(lib.glc_decode_blob_to_host(ctx.handle, glc.U64, ctypes.c_void_p(h_blob.data_ptr()), len(blob), 0,
+                                              ctypes.c_void_p(h_out.data_ptr()), None, ctypes.c_void_p(sh)))
 
     e2e_step()
     if world > 1:

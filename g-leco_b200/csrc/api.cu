@@ -200,6 +200,8 @@ glc_status glc_destroy(glc_ctx* ctx) {
   if (ctx->d_stats) cudaFree(ctx->d_stats);
   if (ctx->h_stats) cudaFreeHost(ctx->h_stats);
   if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
+  for (cudaStream_t a : ctx->aux_stream)
+    if (a) cudaStreamDestroy(a);
   if (ctx->pool) {
     cudaDeviceSynchronize();
     cudaMemPoolDestroy(ctx->pool);
@@ -587,14 +589,14 @@ glc_status glc_serialize(glc_ctx* ctx, const glc_column* c, void* blob, uint64_t
 
 glc_status glc_deserialize(glc_ctx* ctx, glc_dtype dtype, const void* blob, uint64_t size, int flags, int crc32c,
                            int pre_unpack, glc_column** out, glc_stream stream) {
-  return glc::deserialize_column(ctx, dtype, blob, size, flags, crc32c, pre_unpack, out, stream, nullptr);
+  return glc::deserialize_column(ctx, dtype, blob, size, flags, crc32c, pre_unpack, out, stream, nullptr, false);
 }
 
 }  // extern "C"
 
 glc_status glc::deserialize_column(glc_ctx* ctx, glc_dtype dtype, const void* blob, uint64_t size, int flags,
                                    int crc32c, int pre_unpack, glc_column** out, glc_stream stream,
-                                   cudaMemPool_t pool) {
+                                   cudaMemPool_t pool, bool defer_words) {
   if (!ctx || !out) return fail(ctx, GLC_ERR_INVALID_ARG, "null argument");
   *out = nullptr;
   if (!valid_dtype(dtype)) return fail(ctx, GLC_ERR_INVALID_ARG, "unknown dtype");
@@ -649,7 +651,8 @@ glc_status glc::deserialize_column(glc_ctx* ctx, glc_dtype dtype, const void* bl
     if (lens[j] && (e = cudaMemcpyAsync(dst[j], b + offs[j], lens[j], k, s)) != cudaSuccess)
       return bail(cuda_fail(ctx, e, "deserialize: arrays"));
   if ((e = cudaMemsetAsync(c->d_words, 0, 4 * c->nwords_alloc, s)) != cudaSuccess ||
-      (h.delta_size && (e = cudaMemcpyAsync(c->d_words, b + h.delta_off, h.delta_size, k, s)) != cudaSuccess))
+      (h.delta_size && !defer_words &&
+       (e = cudaMemcpyAsync(c->d_words, b + h.delta_off, h.delta_size, k, s)) != cudaSuccess))
     return bail(cuda_fail(ctx, e, "deserialize: bitstream"));
   // structure check, fixed-length detection and max width
   int* d_chk = (int*)(ctx->d_stats + 4);
@@ -700,4 +703,109 @@ glc_status glc::deserialize_column(glc_ctx* ctx, glc_dtype dtype, const void* bl
   if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return bail(cuda_fail(ctx, e, "deserialize: sync"));
   *out = c;
   return GLC_OK;
+}
+
+// ---------------------------------------------------------------------------------------
+// streaming decode of a host blob into host memory
+// ---------------------------------------------------------------------------------------
+namespace {
+
+template <typename V> V load_at(const uint8_t* p, int64_t i) {  // the blob may sit at any address
+  V v;
+  std::memcpy(&v, p + i * (int64_t)sizeof(V), sizeof(V));
+  return v;
+}
+
+// Bit position of value e in a blob's column: offset of its partition + (e - start) * bits.
+int64_t blob_bit_of(const uint8_t* starts, const uint8_t* bits, const uint8_t* offs, int64_t P, int64_t e) {
+  int64_t lo = 0, hi = P - 1;
+  while (lo < hi) {
+    const int64_t mid = (lo + hi + 1) >> 1;
+    if (load_at<int32_t>(starts, mid) <= e) lo = mid; else hi = mid - 1;
+  }
+  return load_at<int64_t>(offs, lo) + (e - load_at<int32_t>(starts, lo)) * (int64_t)load_at<int32_t>(bits, lo);
+}
+
+}  // namespace
+
+extern "C" glc_status glc_decode_blob_to_host(glc_ctx* ctx, glc_dtype dtype, const void* blob, uint64_t size,
+                                              int crc32c, void* out, glc_column** col_out, glc_stream stream) {
+  if (!ctx || !blob || (!out && !col_out)) return fail(ctx, GLC_ERR_INVALID_ARG, "null argument");
+  if (col_out) *col_out = nullptr;
+  cudaSetDevice(ctx->device);
+  cudaStream_t up = pick(ctx, stream);
+  // metadata, checks and lookup tables; the bitstream follows in chunks below
+  glc_column* c = nullptr;
+  glc_status st = deserialize_column(ctx, dtype, blob, size, GLC_HOST_IN, crc32c, 0, &c, stream,
+                                     col_out ? nullptr : ctx->pool, true);
+  if (st != GLC_OK) return st;
+  BlobHeader h;
+  std::memcpy(&h, blob, sizeof h);
+  const uint8_t* b = (const uint8_t*)blob;
+  auto finish = [&](glc_status r) {
+    cudaStreamSynchronize(up);
+    if (ctx->aux_stream[0]) cudaStreamSynchronize(ctx->aux_stream[0]);
+    if (ctx->aux_stream[1]) cudaStreamSynchronize(ctx->aux_stream[1]);
+    if (r == GLC_OK && col_out) *col_out = c;
+    else glc_column_free(c);
+    return r;
+  };
+  if (c->n == 0) return finish(GLC_OK);
+  for (int i = 0; i < 2; i++)
+    if (!ctx->aux_stream[i] && cudaStreamCreateWithFlags(&ctx->aux_stream[i], cudaStreamNonBlocking) != cudaSuccess)
+      return finish(fail(ctx, GLC_ERR_CUDA, "streaming decode: stream"));
+  cudaStream_t dec = ctx->aux_stream[1], down = ctx->aux_stream[0];
+  const int64_t es = dtype_size(dtype);
+  // chunks of whole decode tiles, about 64 MB of values each, through a ring of 3 staging slots
+  const int64_t chunk = std::max<int64_t>(1, (64ll << 20) / (kDecodeTile * es)) * kDecodeTile;
+  const int64_t nchunks = (c->n + chunk - 1) / chunk;
+  constexpr int kSlots = 3;
+  const size_t slot_bytes = (size_t)(chunk * es);
+  uint8_t* ring = nullptr;
+  std::vector<cudaEvent_t> ev_up(nchunks), ev_dec(nchunks), ev_down(nchunks);
+  for (auto* v : {&ev_up, &ev_dec, &ev_down})
+    for (auto& x : *v) x = nullptr;
+  cudaError_t e = pool_alloc(ctx, &ring, slot_bytes * kSlots, up);
+  const uint8_t* hs = b + h.start_off;
+  const uint8_t* hb = b + h.bits_off;
+  const uint8_t* ho = b + h.offsets_off;
+  uint64_t uploaded = 0;  // bytes of the bitstream already queued
+  for (int64_t k = 0; k < nchunks && e == cudaSuccess; k++) {
+    const int64_t lo = k * chunk, hi = std::min(c->n, lo + chunk);
+    // words the decode of [lo, hi) reads: through the last value's field plus the read-ahead
+    const int64_t bit_hi = hi >= c->n ? c->total_bits : blob_bit_of(hs, hb, ho, c->P, hi);
+    const uint64_t need = std::min<uint64_t>(h.delta_size, (uint64_t)((((bit_hi + 31) >> 5) + 8) * 4));
+    for (auto* v : {&ev_up, &ev_dec, &ev_down})
+      if (e == cudaSuccess) e = cudaEventCreateWithFlags(&(*v)[k], cudaEventDisableTiming);
+    if (e == cudaSuccess && need > uploaded) {
+      e = cudaMemcpyAsync((uint8_t*)c->d_words + uploaded, b + h.delta_off + uploaded, need - uploaded,
+                          cudaMemcpyHostToDevice, up);
+      uploaded = need;
+    }
+    if (e == cudaSuccess) e = cudaEventRecord(ev_up[k], up);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(dec, ev_up[k], 0);
+    if (e == cudaSuccess && k >= kSlots) e = cudaStreamWaitEvent(dec, ev_down[k - kSlots], 0);  // slot free
+    uint8_t* slot = ring + (size_t)(k % kSlots) * slot_bytes;
+    if (e == cudaSuccess) e = launch_decode(ctx, c, 0, 0, lo, hi, slot - lo * es, dec);
+    if (e == cudaSuccess) e = cudaEventRecord(ev_dec[k], dec);
+    if (e == cudaSuccess && out) {
+      e = cudaStreamWaitEvent(down, ev_dec[k], 0);
+      if (e == cudaSuccess)
+        e = cudaMemcpyAsync((uint8_t*)out + lo * es, slot, (size_t)((hi - lo) * es), cudaMemcpyDeviceToHost, down);
+    }
+    if (e == cudaSuccess) e = cudaEventRecord(ev_down[k], down);
+  }
+  if (e == cudaSuccess && uploaded < h.delta_size)  // the rest of the bitstream (kept for later calls)
+    e = cudaMemcpyAsync((uint8_t*)c->d_words + uploaded, b + h.delta_off + uploaded, h.delta_size - uploaded,
+                        cudaMemcpyHostToDevice, up);
+  if (e == cudaSuccess && nchunks > 0) e = cudaStreamWaitEvent(up, ev_down[nchunks - 1], 0);
+  if (ring) cudaFreeAsync(ring, up);  // after the last download
+  cudaStreamSynchronize(up);
+  cudaStreamSynchronize(dec);
+  cudaStreamSynchronize(down);
+  for (auto* v : {&ev_up, &ev_dec, &ev_down})
+    for (auto& x : *v)
+      if (x) cudaEventDestroy(x);
+  if (e != cudaSuccess) return finish(cuda_fail(ctx, e, "streaming decode"));
+  return finish(glc_sync(ctx, stream));
 }

@@ -60,6 +60,7 @@ struct glc_ctx {
   int device = 0;
   int num_sms = 0;
   cudaStream_t own_stream = nullptr;
+  cudaStream_t aux_stream[2] = {nullptr, nullptr};  // streaming decode: download, upload (lazy)
   cudaMemPool_t pool = nullptr;  // private stream-ordered pool; keeps freed memory for reuse
   int* d_flags = nullptr;      // [0, 64) decode work counters, [64] device error code
   int64_t* d_stats = nullptr;  // small readback area (total bits, max bits, ...)
@@ -186,9 +187,11 @@ cudaError_t launch_random_access(glc_ctx* ctx, const glc_column* c, int plain_sr
                                  int64_t q, void* out, int32_t fixed_len, cudaStream_t s);
 cudaError_t launch_random_access_shape(glc_ctx* ctx, const glc_column* c, int plain_src, const int32_t* pos, int64_t q,
                                        void* out, int32_t fixed_len, int shape, cudaStream_t s);
-// api.cu: glc_deserialize with the column's arrays allocated from `pool` (nullptr: cudaMalloc)
+// api.cu: glc_deserialize with the column's arrays allocated from `pool` (nullptr: cudaMalloc);
+// defer_words leaves the bitstream zeroed (the caller uploads it).
 glc_status deserialize_column(glc_ctx* ctx, glc_dtype dtype, const void* blob, uint64_t size, int flags, int crc32c,
-                              int pre_unpack, glc_column** out, glc_stream stream, cudaMemPool_t pool);
+                              int pre_unpack, glc_column** out, glc_stream stream, cudaMemPool_t pool,
+                              bool defer_words = false);
 // random_access.cu: lookups of many requests into many columns (serving)
 struct RAColumn {
   const PartDesc* desc;

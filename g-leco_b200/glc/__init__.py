@@ -34,7 +34,7 @@ EXPORTS = [
     "glc_create", "glc_destroy", "glc_last_error", "glc_status_string", "glc_sync", "glc_compress",
     "glc_partition_variable", "glc_partition_v6", "glc_column_free", "glc_column_get_info", "glc_decompress_full",
     "glc_decompress_range", "glc_random_access", "glc_preunpack", "glc_blob_size", "glc_serialize",
-    "glc_deserialize", "glc_decompress_range_noalloc", "glc_batch_create", "glc_batch_compress",
+    "glc_deserialize", "glc_decode_blob_to_host", "glc_decompress_range_noalloc", "glc_batch_create", "glc_batch_compress",
     "glc_batch_column", "glc_batch_decompress", "glc_batch_free", "glc_server_create", "glc_server_destroy",
     "glc_server_admit", "glc_server_admit_blob", "glc_server_evict", "glc_server_submit", "glc_server_poll",
     "glc_server_drain", "glc_server_get_stats", "glc_server_now_ns", "glc_server_columns",
@@ -138,6 +138,7 @@ def load() -> ctypes.CDLL:
         "glc_serialize": ([vp, vp, vp, u64, c_int, c_int, pu64, vp], c_int),
         "glc_deserialize": ([vp, c_int, vp, u64, c_int, c_int, c_int, pvp, vp], c_int),
         "glc_decompress_range_noalloc": ([vp, i64, i64, vp, vp], c_int),
+        "glc_decode_blob_to_host": ([vp, c_int, vp, u64, c_int, vp, pvp, vp], c_int),
         "glc_batch_create": ([vp, vp, i32, pvp], c_int),
         "glc_batch_compress": ([vp, vp, vp, vp, i32, i32, pvp, pi64, vp], c_int),
         "glc_batch_column": ([vp, i32, pvp], c_int),
@@ -327,6 +328,16 @@ def serialize_host(ctx: Context, col: Column, crc32c: bool = False) -> bytes:
     ctx.check(ctx.lib.glc_serialize(ctx.handle, col.handle, _ptr(buf), size.value, HOST_OUT, 1 if crc32c else 0,
                                     ctypes.byref(written), None))
     return buf.tobytes()
+
+
+def decode_blob_to_host(ctx: Context, dtype: int, blob_ptr: int, size: int, out_ptr: int, keep: bool = False,
+                        stream: int = 0) -> Optional[Column]:
+    """Streaming host blob -> host values (glc_decode_blob_to_host); with keep, the column."""
+    h = ctypes.c_void_p()
+    ctx.check(ctx.lib.glc_decode_blob_to_host(ctx.handle, dtype, ctypes.c_void_p(blob_ptr), size, 0,
+                                              ctypes.c_void_p(out_ptr) if out_ptr else None,
+                                              ctypes.byref(h) if keep else None, ctypes.c_void_p(stream)))
+    return Column(ctx, h) if keep else None
 
 
 def deserialize_host(ctx: Context, dtype: int, blob: bytes, pre_unpack: bool = False, crc32c: bool = False) -> Optional[Column]:

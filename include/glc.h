@@ -179,6 +179,17 @@ GLC_API glc_status glc_serialize(glc_ctx* ctx, const glc_column* col, void* blob
 GLC_API glc_status glc_deserialize(glc_ctx* ctx, glc_dtype dtype, const void* blob, uint64_t size, int flags,
                            int crc32c, int pre_unpack, glc_column** out, glc_stream stream);
 
+/* Decode a serialized column held in HOST memory straight into host memory `out` (total_values
+ * elements), streaming: the bitstream is uploaded, decoded and the values downloaded in chunks of
+ * about 64 MB on three streams, so upload, decode and download overlap (PCIe carries both
+ * directions at once) and the call takes about the download time.  The same checks as
+ * glc_deserialize; the values equal glc_deserialize + glc_decompress_full(..., GLC_HOST_OUT),
+ * which is the reference's deserializeGPU + decompressFullFile (api/G-LeCo.cuh:2157, :680).
+ * col_out (may be NULL) receives the deserialized column, which then stays on the device;
+ * out may be NULL when col_out is not.  Pinned `out` gives the full PCIe rate. */
+GLC_API glc_status glc_decode_blob_to_host(glc_ctx* ctx, glc_dtype dtype, const void* blob, uint64_t size,
+                                           int crc32c, void* out, glc_column** col_out, glc_stream stream);
+
 /* ---- batches: many columns per launch (no counterpart in the reference) ----------------- */
 
 typedef struct glc_batch glc_batch;

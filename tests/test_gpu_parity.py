@@ -267,3 +267,38 @@ def test_decode_into_misaligned_device_buffer(offset_bytes):
     want = v.copy()
     want[:1000] = v[3:1003]
     assert np.array_equal(got, want)
+
+
+@pytest.mark.parametrize("kind,n", [("u64_piecewise", 0), ("u64_piecewise", 1), ("i32_linear", 70_001),
+                                    ("u64_piecewise", 20_000_000), ("i32_linear", 40_000_000),
+                                    ("u64_big", 300_000)])
+def test_streaming_blob_decode_to_host(oracle, kind, n):
+    """glc_decode_blob_to_host: host blob in, host values out, chunks overlapped on three streams;
+    the same values as deserialize + full decode, and the kept column works afterwards."""
+    import torch
+    v = _data(kind, n) if n else np.zeros(0, _data(kind, 10).dtype)
+    dt = glc.DTYPE_OF[v.dtype]
+    codec = _codec(v) if n else glc.LeCoGPU(v.dtype)
+    if n:
+        col, _ = codec.compress(v, True)
+        blob = glc.serialize_host(codec.ctx, col)
+        col.free()
+    else:
+        blob = oracle.serialize(oracle.compress(v, "fixed", 4096))
+    hb = torch.from_numpy(np.frombuffer(blob, np.uint8).copy()).pin_memory()
+    out = torch.empty(max(n, 1) * v.dtype.itemsize, dtype=torch.uint8).pin_memory()
+    out.fill_(0xAB)
+    glc.decode_blob_to_host(codec.ctx, dt, hb.data_ptr(), len(blob), out.data_ptr())
+    assert np.array_equal(out.numpy()[: n * v.dtype.itemsize].view(v.dtype), v)
+    kept = glc.decode_blob_to_host(codec.ctx, dt, hb.data_ptr(), len(blob), 0, keep=True)
+    if n:
+        pos = np.random.default_rng(2).integers(0, n, 10_000).astype(np.int32)
+        got = np.zeros(len(pos), v.dtype)
+        glc.random_access_into(codec.ctx, kept, pos.ctypes.data, len(pos), got.ctypes.data, host_in=True,
+                               host_out=True)
+        assert np.array_equal(got, v[pos])
+    kept.free()
+    bad = np.frombuffer(blob, np.uint8).copy()  # kept alive across the call
+    bad[8] ^= 1
+    with pytest.raises(glc.GlcError):
+        glc.decode_blob_to_host(codec.ctx, dt, bad.ctypes.data, len(bad), out.data_ptr())
