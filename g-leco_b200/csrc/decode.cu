@@ -624,7 +624,7 @@ cudaError_t launch_decode_scratch(const glc_column* c, int64_t lo, int64_t hi, v
 }
 
 cudaError_t launch_decode_shape(glc_ctx* ctx, const glc_column* c, int plain_src, int residual_out, int64_t lo,
-                                int64_t hi, void* out_base, int stages, int unroll, cudaStream_t s) {
+                                int64_t hi, void* out_base, int stages, int unroll, int cap_words, cudaStream_t s) {
   if (hi <= lo || c->n <= 0) return cudaSuccess;
   if (((uintptr_t)out_base & 15) != 0) return cudaErrorMisalignedAddress;  // 16-byte vector stores
   DecodeArgs a;
@@ -647,7 +647,8 @@ cudaError_t launch_decode_shape(glc_ctx* ctx, const glc_column* c, int plain_src
   } else {
     int64_t words = ((int64_t)kDecodeTile * c->max_bits + 31) / 32 + 16;
     words = (words + 3) & ~3ll;
-    const int64_t cap = env_int("GLC_DECODE_CAP_WORDS", kStageCapWords) & ~3;
+    int64_t cap = (cap_words > 0 ? cap_words : kStageCapWords) & ~3;
+    if (cap > kStageCapWordsMax) cap = kStageCapWordsMax;
     if (words > cap) words = cap < 32 ? 32 : cap;
     a.stage_bytes = (int)(words * 4);
   }
@@ -660,14 +661,15 @@ cudaError_t launch_decode_shape(glc_ctx* ctx, const glc_column* c, int plain_src
   return cudaErrorInvalidValue;
 }
 
-// Ring depth and unroll depth from the context's tuning table for the column's element type and
-// widest field (GLC_DECODE_STAGES / GLC_DECODE_UNROLL override both, for sweeps).
+// Ring depth, unroll depth and stage capacity from the context's tuning table for the column's
+// element type and widest field (GLC_DECODE_STAGES / _UNROLL / _CAP_WORDS override them, for sweeps).
 cudaError_t launch_decode(glc_ctx* ctx, const glc_column* c, int plain_src, int residual_out, int64_t lo, int64_t hi,
                           void* out_base, cudaStream_t s) {
   const TuneEntry& t = tune_entry(ctx, c->dtype, c->max_bits, plain_src);
   const int stages = env_int("GLC_DECODE_STAGES", t.decode_stages);
   const int unroll = env_int("GLC_DECODE_UNROLL", t.decode_unroll);
-  return launch_decode_shape(ctx, c, plain_src, residual_out, lo, hi, out_base, stages, unroll, s);
+  const int cap = env_int("GLC_DECODE_CAP_WORDS", t.decode_cap_words);
+  return launch_decode_shape(ctx, c, plain_src, residual_out, lo, hi, out_base, stages, unroll, cap, s);
 }
 
 }  // namespace glc

@@ -4,7 +4,9 @@
 // context holds a table, indexed by element type, widest-field bucket (<= 8, 16, 24, 32, 48, 64
 // bits) and residual source (packed / pre-unpacked), of
 //   - the decode kernel's TMA ring depth (2, 3, 4) and the unroll depth of its full-tile loop
-//     (1, 2, 4): the values each CTA keeps in flight per tile;
+//     (1, 2, 4): the values each CTA keeps in flight per tile; for fields wider than 32 bits also
+//     the largest tile staged in shared memory (6160 words, or a whole tile of 64-bit fields at
+//     the cost of fewer CTAs per SM; larger tiles are read from global memory);
 //   - the random-access launch shape (lookups per thread x CTAs per SM, five candidates).
 // glc_autotune times every candidate on a synthetic fixed-partitioned column whose fields have the
 // bucket's width (48M values, larger than L2) and keeps the fastest; the table can be written to
@@ -19,7 +21,7 @@ using namespace glc;
 
 namespace {
 
-constexpr int kTuneVersion = 1;
+constexpr int kTuneVersion = 2;
 constexpr int64_t kTuneValues = 48ll << 20;
 constexpr int64_t kTuneLookups = 16ll << 20;
 constexpr int kNoiseBits[kTuneBuckets] = {5, 13, 21, 29, 45, 59};  // fields of 6..60 bits
@@ -67,8 +69,8 @@ bool tune_save(const glc_ctx* ctx, const char* path) {
     for (int b = 0; b < kTuneBuckets; b++)
       for (int p = 0; p < 2; p++) {
         const TuneEntry& t = ctx->tune[d][b][p];
-        fprintf(f, "%d %d %d %d %d %d %.3f %.4f\n", d, b, p, t.decode_stages, t.decode_unroll, t.ra_shape,
-                t.decode_gbs, t.ra_glookups);
+        fprintf(f, "%d %d %d %d %d %d %d %.3f %.4f\n", d, b, p, t.decode_stages, t.decode_unroll, t.ra_shape,
+                t.decode_cap_words, t.decode_gbs, t.ra_glookups);
       }
   return fclose(f) == 0;
 }
@@ -103,6 +105,8 @@ void glc::tune_defaults(glc_ctx* ctx) {
         t.decode_unroll = 2;
         t.ra_shape = p ? 3 : 4;
         t.measured = 0;
+        t.decode_cap_words = 0;
+        t.reserved = 0;
         t.decode_gbs = 0.f;
         t.ra_glookups = 0.f;
       }
@@ -120,12 +124,12 @@ bool glc::tune_load(glc_ctx* ctx, const char* path) {
   TuneEntry tab[4][kTuneBuckets][2];
   int seen = 0;
   while (ok && fgets(line, sizeof line, f)) {
-    int d, b, p, st, un, ra;
+    int d, b, p, st, un, ra, cap;
     float gbs, gl;
-    if (sscanf(line, "%d %d %d %d %d %d %f %f", &d, &b, &p, &st, &un, &ra, &gbs, &gl) != 8) { ok = false; break; }
+    if (sscanf(line, "%d %d %d %d %d %d %d %f %f", &d, &b, &p, &st, &un, &ra, &cap, &gbs, &gl) != 9) { ok = false; break; }
     if (d < 0 || d > 3 || b < 0 || b >= kTuneBuckets || p < 0 || p > 1 || st < 2 || st > 4 ||
-        (un != 1 && un != 2 && un != 4) || ra < 0 || ra > 4) { ok = false; break; }
-    tab[d][b][p] = TuneEntry{st, un, ra, 1, gbs, gl};
+        (un != 1 && un != 2 && un != 4) || ra < 0 || ra > 4 || cap < 0 || cap > kStageCapWordsMax) { ok = false; break; }
+    tab[d][b][p] = TuneEntry{st, un, ra, 1, cap, 0, gbs, gl};
     seen++;
   }
   fclose(f);
@@ -140,7 +144,8 @@ glc_status glc_tune_get(const glc_ctx* ctx, glc_dtype dtype, int32_t field_bits,
                         glc_tune_entry* out) {
   if (!ctx || !out || (int)dtype < 0 || (int)dtype > 3 || field_bits < 0 || field_bits > 64) return GLC_ERR_INVALID_ARG;
   const TuneEntry& t = tune_entry(ctx, dtype, field_bits, preunpacked);
-  *out = glc_tune_entry{t.decode_stages, t.decode_unroll, t.ra_shape, t.measured, t.decode_gbs, t.ra_glookups};
+  *out = glc_tune_entry{t.decode_stages, t.decode_unroll, t.ra_shape, t.measured, t.decode_cap_words, 0,
+                        t.decode_gbs, t.ra_glookups};
   return GLC_OK;
 }
 
@@ -148,10 +153,12 @@ glc_status glc_tune_set(glc_ctx* ctx, glc_dtype dtype, int32_t field_bits, int32
                         const glc_tune_entry* e) {
   if (!ctx || !e || (int)dtype < 0 || (int)dtype > 3 || field_bits < 0 || field_bits > 64) return GLC_ERR_INVALID_ARG;
   if (e->decode_stages < 2 || e->decode_stages > 4 || (e->decode_unroll != 1 && e->decode_unroll != 2 &&
-      e->decode_unroll != 4) || e->ra_shape < 0 || e->ra_shape > 4)
+      e->decode_unroll != 4) || e->ra_shape < 0 || e->ra_shape > 4 || e->decode_cap_words < 0 ||
+      e->decode_cap_words > kStageCapWordsMax)
     return tfail(ctx, GLC_ERR_INVALID_ARG, "tune entry out of range");
   ctx->tune[(int)dtype][tune_bucket(field_bits)][preunpacked ? 1 : 0] =
-      TuneEntry{e->decode_stages, e->decode_unroll, e->ra_shape, e->measured, e->decode_gbs, e->ra_glookups};
+      TuneEntry{e->decode_stages, e->decode_unroll, e->ra_shape, e->measured, e->decode_cap_words, 0, e->decode_gbs,
+                e->ra_glookups};
   return GLC_OK;
 }
 
@@ -193,20 +200,24 @@ glc_status glc_autotune(glc_ctx* ctx, const char* cache_path, int32_t flags) {
         if (plain && (st = glc_preunpack(ctx, col, 0, s)) != GLC_OK) break;
         TuneEntry best = tab[d][bucket][plain];
         float best_ms = 1e30f;
-        for (int stages = 2; stages <= 4; stages++)
-          for (int unroll : {1, 2, 4}) {
-            if (plain && unroll != 2) continue;  // the pre-unpacked decode has no unroll choice
-            const float ms = time_launches([&] {
-              return launch_decode_shape(ctx, col, plain, 0, 0, kTuneValues, out, stages, unroll, s);
-            }, s, e0, e1);
-            if (ms < 0.f) { st = tfail(ctx, GLC_ERR_CUDA, "autotune: decode launch failed"); break; }
-            if (ms < best_ms) {
-              best_ms = ms;
-              best.decode_stages = stages;
-              best.decode_unroll = unroll;
-              best.decode_gbs = (float)(dtype_size(dt) * (double)kTuneValues / (ms * 1e6));
+        for (int cap : {0, kStageCapWordsMax}) {
+          if (cap && (plain || col->max_bits <= 32)) continue;  // only tiles of wide fields exceed the default
+          for (int stages = 2; stages <= 4; stages++)
+            for (int unroll : {1, 2, 4}) {
+              if (plain && unroll != 2) continue;  // the pre-unpacked decode has no unroll choice
+              const float ms = time_launches([&] {
+                return launch_decode_shape(ctx, col, plain, 0, 0, kTuneValues, out, stages, unroll, cap, s);
+              }, s, e0, e1);
+              if (ms < 0.f) { st = tfail(ctx, GLC_ERR_CUDA, "autotune: decode launch failed"); break; }
+              if (ms < best_ms) {
+                best_ms = ms;
+                best.decode_stages = stages;
+                best.decode_unroll = unroll;
+                best.decode_cap_words = cap;
+                best.decode_gbs = (float)(dtype_size(dt) * (double)kTuneValues / (ms * 1e6));
+              }
             }
-          }
+        }
         float best_ra = 1e30f;
         for (int shape = 0; shape < 5 && st == GLC_OK; shape++) {
           const float ms = time_launches([&] {

@@ -254,6 +254,9 @@ typedef struct glc_tune_entry {
   int32_t ra_shape;       /* random-access shape 0..4: (lookups per thread, CTAs per SM) =
                              (4,1), (4,5), (2,8), (8,2), (2,6) */
   int32_t measured;       /* 1 when chosen by glc_autotune, 0 for the built-in default */
+  int32_t decode_cap_words; /* largest tile staged in shared memory, in 32-bit words: 0 = 6160
+                             (48-bit fields), up to 8208 (a whole tile of 64-bit fields) */
+  int32_t reserved;       /* 0 */
   float decode_gbs;       /* decoded GB/s of the chosen shape on the tuning column */
   float ra_glookups;      /* G lookups/s of the chosen random-access shape */
 } glc_tune_entry;

@@ -87,7 +87,7 @@ def test_autotune_measures_and_caches(tmp_path):
     # a file written for another device is ignored by a new context
     with open(path) as f:
         lines = f.read().splitlines()
-    lines[0] = lines[0].replace("glc-tune 1", "glc-tune 1 other")
+    lines[0] = lines[0] + "_other_device"
     other = str(tmp_path / "other.txt")
     with open(other, "w") as f:
         f.write("\n".join(lines) + "\n")
@@ -97,3 +97,29 @@ def test_autotune_measures_and_caches(tmp_path):
     finally:
         del os.environ["GLC_TUNE_CACHE"]
     assert glc.tune_get(ctx3, glc.U64, 25).measured == 0
+
+
+@pytest.mark.parametrize("dt", [glc.I64, glc.U64])
+def test_wide_fields_with_a_whole_tile_staged(dt):
+    """Columns with fields wider than 48 bits (and direct-copy partitions) decode the same whether
+    their tiles are staged in shared memory (capacity 8208 words) or read from global memory."""
+    ctx = glc.Context(0)
+    rng = np.random.default_rng(9)
+    n = 200_003
+    i = np.arange(n, dtype=np.int64)
+    v = ((1 << 40) + 1000 * i + rng.integers(0, 1 << 59, n)).astype(np.int64)
+    if dt == glc.U64:
+        v = v.astype(np.uint64)
+        v[50_000:60_000] += np.uint64(1 << 62)  # above 2^53: direct copy
+    col = glc.compress_device(ctx, dt, v.ctypes.data, n, glc.FIXED, host=True)
+    out = torch.zeros(n, dtype=torch.int64, device="cuda:0")
+    for cap in (0, 8208):
+        for stages in (2, 3, 4):
+            for b in (8, 16, 24, 32, 48, 64):
+                glc.tune_set(ctx, dt, b, False, stages, 2, 4, cap)
+            out.fill_(0)
+            torch.cuda.synchronize()
+            glc.decompress_into(ctx, col, out.data_ptr(), source=glc.SRC_PACKED)
+            ctx.sync()
+            assert np.array_equal(out.cpu().numpy().view(v.dtype), v), (cap, stages)
+    col.free()
