@@ -555,9 +555,18 @@ def run_serving(args):
 
     import glc
 
+    from glc.sharding import gather_objects, merge_serving_points
+
     local = int(os.environ.get("LOCAL_RANK", "0"))
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
+    if world > 1:  # whole columns per GPU: every rank serves its own columns; no data-path collective
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     stream = torch.cuda.Stream(dev)
     torch.cuda.set_stream(stream)
     sh = stream.cuda_stream
@@ -568,7 +577,7 @@ def run_serving(args):
     t_build = time.perf_counter()
     for k, (name, dt, n, mode, L, copies) in enumerate(SERVE_SOURCES):
         n = max(8192, int(n * scale))
-        v = gens[dt](n, 42 + k, dev)
+        v = gens[dt](n, 42 + k + 1000 * rank, dev)
         code = getattr(glc, dt)
         col = glc.compress_device(ctx, code, v.data_ptr(), n, getattr(glc, mode), fixed_len=L or 4096, stream=sh)
         size = ctypes.c_uint64()
@@ -640,7 +649,9 @@ def run_serving(args):
     def run_point(rate, lookup_frac, seed, admit_during):
         nonlocal ids
         nreq = int(np.clip(rate * args.serve_seconds, 4000, 500_000))
-        req, si, es = make_stream(rate, lookup_frac, nreq, seed, ids)
+        req, si, es = make_stream(rate, lookup_frac, nreq, seed + 7919 * rank, ids)
+        if world > 1:
+            torch.distributed.barrier()  # all ranks serve the rate point at the same time
         before = server.stats()
         server.submit(req)
         admitted, refused, adm_t = 0, 0, 0.0
@@ -748,7 +759,14 @@ def run_serving(args):
 
     pc_lookups = per_call(1.0, 20_000, 7)
     pc_mix = per_call(0.5, 4_000, 8)
-    per_call_lps = pc_lookups["lookups_per_s"]
+    # merge the ranks' measurements: throughputs add up, percentiles take the worst rank
+    all_pc = gather_objects((pc_lookups["lookups_per_s"], pc_mix["requests_per_s"]))
+    if world > 1:
+        sweep = merge_serving_points(gather_objects(sweep))
+        ra_sweep = merge_serving_points(gather_objects(ra_sweep))
+        resident_gb = sum(gather_objects(resident_gb))
+        chk_ok = all(gather_objects(chk_ok))
+    per_call_lps = sum(x[0] for x in all_pc)
 
     def ok_point(p):
         return p["lookup_p99_us"] is not None and p["lookup_p99_us"] <= 1000.0
@@ -762,12 +780,26 @@ def run_serving(args):
     else:
         alg = 0.0
     st = server.stats()
+    st_all = gather_objects((int(st.evictions), int(st.admissions_refused), int(st.launches)))
+    if rank != 0:
+        server.close()
+        for s in sources:
+            s["col"].free()
+        ctx.close()
+        if world > 1:
+            torch.distributed.barrier()
+            torch.distributed.destroy_process_group()
+        return 0
     line = {
         "metric": "served lookups/s at lookup p99 <= 1 ms", "value": round(value, 1), "unit": "lookups/s",
-        "n_gpus": 1, "steps": len(sweep) + len(ra_sweep), "warmup": args.warmup,
+        "n_gpus": world, "steps": len(sweep) + len(ra_sweep), "warmup": args.warmup,
         "ms_per_step": round(1e3 * (best["span_s"] if best else 0.0), 3), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "mixed int32/int64/uint64", "data": "synthetic",
-        "config": {"workload": "serving_64_columns_poisson", "columns": len(ids), "resident_gb": round(resident_gb, 2),
+        "config": {"workload": "serving_64_columns_poisson", "columns": len(ids) * world,
+                   "sharding": "whole columns per GPU: every rank its own server and columns (weak scaling); "
+                               "rate points are per GPU, merged by summing throughput and taking the worst "
+                               "rank's percentiles" if world > 1 else "one GPU",
+                   "resident_gb": round(resident_gb, 2),
                    "budget_gb": round(budget / 1e9, 1), "slots": args.slots,
                    "sources": [f"{s['copies']} x {s['name']}" for s in sources],
                    "lookup_sizes": "floor(exp(U[0, ln 65536])) positions, uniform over the column",
@@ -780,19 +812,23 @@ def run_serving(args):
                                         "C++ loop, one stream, back to back (device time)",
                                 "lookups_only": pc_lookups, "mix_50_50": pc_mix},
                    "served_over_per_call": round(value / per_call_lps, 2) if per_call_lps else None,
-                   "evictions_total": st.evictions, "admissions_refused_total": st.admissions_refused,
+                   "evictions_total": sum(x[0] for x in st_all),
+                   "admissions_refused_total": sum(x[1] for x in st_all),
                    "l2": "columns, positions and outputs far larger than L2"},
         "roofline": {"bound": "hbm", "achieved": round(alg / 1e9, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(alg / 1e9 / peak, 4), "peak_kind": peak_kind, "traffic": None,
                      "basis": "whole served stream at the best point: 44 B per lookup + range bytes written "
                               "and read, over the stream's span"},
-        "e2e": None, "gpu_launches": int(st.launches), "clocks": clk, "cpu_baseline": None,
+        "e2e": None, "gpu_launches": sum(x[2] for x in st_all), "clocks": clk, "cpu_baseline": None,
     }
     print(json.dumps(line), flush=True)
     server.close()
     for s in sources:
         s["col"].free()
     ctx.close()
+    if world > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
     return 0
 
 
