@@ -14,6 +14,8 @@
 // lookups through the load stages so their DRAM latencies overlap.
 // Positions outside [0, n) yield 0, as the reference's variable-partition kernels do; the
 // fixed variants use the same rule here instead of reading past the metadata.
+// Cache hints: positions are read and values written exactly once, so they go through L2 as
+// streaming (evict-first) accesses and leave L2 to the partition descriptors and hot fields.
 #include <cstdlib>
 #include "glc_internal.h"
 
@@ -71,7 +73,7 @@ __device__ __forceinline__ PartDesc load_desc(const PartDesc* __restrict__ d) {
 // the register budget is sized for.
 template <typename T, bool PLAIN, int MODE, int kRAQueries, int MINB>
 __global__ void __launch_bounds__(kRAThreads, MINB) random_access_kernel(RAArgs a) {
-  __shared__ int32_t s_sample[kRASample];
+  __shared__ int32_t s_sample[MODE == 2 ? kRASample : 1];  // fixed modes leave L1 to descriptors
   if (MODE == 2) {
     for (int k = threadIdx.x; k < a.nsample; k += kRAThreads) s_sample[k] = a.starts[(int64_t)k * a.sample_stride];
     __syncthreads();
@@ -84,7 +86,7 @@ __global__ void __launch_bounds__(kRAThreads, MINB) random_access_kernel(RAArgs 
 #pragma unroll
     for (int k = 0; k < kRAQueries; k++) {
       qi[k] = base + (int64_t)k * kRAThreads + threadIdx.x;
-      pos[k] = (qi[k] < a.q) ? (int64_t)__ldg(a.pos + qi[k]) : -1;
+      pos[k] = (qi[k] < a.q) ? (int64_t)__ldcs(a.pos + qi[k]) : -1;
       valid[k] = pos[k] >= 0 && pos[k] < a.n;
       if (!valid[k]) pos[k] = 0;
     }
@@ -135,7 +137,7 @@ __global__ void __launch_bounds__(kRAThreads, MINB) random_access_kernel(RAArgs 
       T v;
       if (type == MODEL_DIRECT_COPY) v = (T)r[k];
       else v = apply_delta<T>(predict<T>(d[k].theta0, d[k].theta1, pos[k] - d[k].start), r[k]);
-      out[qi[k]] = valid[k] ? v : (T)0;
+      __stcs(out + qi[k], valid[k] ? v : (T)0);
     }
   }
 }
@@ -146,7 +148,16 @@ static cudaError_t ra_shape(glc_ctx* ctx, const RAArgs& a, int mode, cudaStream_
                     : mode == 1 ? random_access_kernel<T, PLAIN, 1, QPT, MINB>
                                 : random_access_kernel<T, PLAIN, 2, QPT, MINB>;
   int per_sm = 0;
-  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kRAThreads, 0);
+  cudaError_t e;
+  if (mode != 2) {  // no shared memory in the fixed modes: prefer the largest L1 for descriptors
+    static bool carveout_set = false;
+    if (!carveout_set) {
+      cudaFuncSetAttribute(random_access_kernel<T, PLAIN, 0, QPT, MINB>, cudaFuncAttributePreferredSharedMemoryCarveout, 0);
+      cudaFuncSetAttribute(random_access_kernel<T, PLAIN, 1, QPT, MINB>, cudaFuncAttributePreferredSharedMemoryCarveout, 0);
+      carveout_set = true;
+    }
+  }
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kRAThreads, 0);
   if (e != cudaSuccess) return e;
   if (per_sm < 1) per_sm = 1;
   const int64_t chunk = (int64_t)kRAThreads * QPT;
