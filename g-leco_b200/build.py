@@ -75,7 +75,7 @@ def build_dropin() -> str:
     """Compile the C++ caller of the drop-in LeCoGPU<T> header (tests/cpp/leco_dropin.cpp)."""
     src = os.path.join(ROOT, "tests", "cpp", "leco_dropin.cpp")
     exe = os.path.join(BUILD, "leco_dropin")
-    hdrs = [os.path.join(ROOT, "include", h) for h in ("glc.h", "glc_leco.hpp")]
+    hdrs = [os.path.join(ROOT, "include", h) for h in ("glc.h", "glc_leco.hpp", "glc_io.hpp")]
     if os.path.exists(exe) and all(os.path.getmtime(exe) >= os.path.getmtime(d) for d in [src, OUT] + hdrs):
         return exe
     cuda_inc = os.path.join(os.path.dirname(os.path.dirname(os.path.realpath(

@@ -4,6 +4,10 @@
 #include <random>
 #include <vector>
 
+#include <cstdio>
+#include <string>
+
+#include "glc_io.hpp"
 #include "glc_leco.hpp"
 
 template <typename T>
@@ -13,9 +17,9 @@ static int run(const char* name, const std::vector<T>& data) {
   std::mt19937_64 rng(7);
   std::vector<int> pos(10000);
   for (auto& p : pos) p = (int)(rng() % data.size());
-  for (int var = 0; var < 2; var++) {
+  for (int var = 0; var < 3; var++) {  // fixed, variable (CPU-partitioner model), variable (GPU partitioner)
     long long size = 0;
-    CompressedData<T>* cd = codec.compress(data, var == 1, &size);
+    CompressedData<T>* cd = codec.compress(data, var >= 1, &size, var == 2);
     if (!cd || size <= 0) { printf("%s: compress failed\n", name); return 1; }
     std::vector<T> out;
     codec.decompressFullFile(cd, out);
@@ -52,6 +56,43 @@ static int run(const char* name, const std::vector<T>& data) {
   return bad ? 1 : 0;
 }
 
+// The reference driver loads columns with read_binary_file / read_text_file (app/Main.cu:875-987).
+template <typename T>
+static int file_round_trip(const char* name, const std::vector<T>& data) {
+  const std::string path = std::string("/tmp/glc_dropin_") + name + ".bin";
+  FILE* f = fopen(path.c_str(), "wb");
+  if (!f) return 1;
+  fwrite(data.data(), sizeof(T), data.size(), f);
+  fclose(f);
+  std::vector<T> loaded;
+  if (!read_binary_file(path, loaded) || loaded != data) { printf("%s: read_binary_file failed\n", name); return 1; }
+  LeCoGPU<T> codec;
+  long long size = 0;
+  CompressedData<T>* cd = codec.compress(loaded, true, &size);
+  SerializedData* sd = codec.serialize(cd);
+  const std::string blob = path + ".leco";
+  int bad = !codec.saveToFile(sd->data, sd->size, blob);
+  size_t bytes = 0;
+  uint8_t* back = codec.loadFromFile(blob, bytes);
+  bad += !back || bytes != sd->size;
+  if (back) {
+    SerializedData in;  // takes ownership of the loaded buffer
+    in.data = back;
+    in.size = bytes;
+    CompressedData<T>* cd2 = codec.deserialize(&in);
+    std::vector<T> out;
+    if (cd2) codec.decompressFullFile(cd2, out);
+    bad += !cd2 || out != data;
+    if (cd2) codec.cleanup(cd2);
+  }
+  delete sd;
+  codec.cleanup(cd);
+  remove(path.c_str());
+  remove(blob.c_str());
+  printf("%s file round trip: %s\n", name, bad ? "MISMATCH" : "ok");
+  return bad ? 1 : 0;
+}
+
 int main() {
   std::mt19937_64 rng(42);
   const int n = 1 << 20;
@@ -65,5 +106,6 @@ int main() {
   std::vector<unsigned int> d(n);
   for (int i = 0; i < n; i++) d[i] = 13u * i + (unsigned)(rng() % 100);
   int r = run("int", a) | run("long long", b) | run("unsigned long long", c) | run("unsigned int", d);
+  r |= file_round_trip("int", a) | file_round_trip("ull", c);
   return r;
 }
