@@ -251,14 +251,15 @@ __device__ __forceinline__ void decode_tile(const DecodeArgs& a, const StageInfo
     for (int it = 0; it < kIters; it++) {
       const int e = Ea + (it * kConsumers + tid) * V;
       if (c.idx < 0 || e >= c.next) seek(e);
-      if (e + V - 1 < c.next) fast_vec(e); else general_vec(e);
+      if (e <= c.next - V) fast_vec(e); else general_vec(e);  // e + V - 1 < next, without overflow
     }
   } else {
     for (int j = tid; j < nvec; j += kConsumers) {
       const int e = Ea + j * V;
-      if (e >= E0 && e + V <= E1) {
+      // e + V <= E1 and e + V - 1 < next, written so that they cannot overflow at n = 2^31 - 1
+      if (e >= E0 && e <= E1 - V) {
         if (c.idx < 0 || e >= c.next) seek(e);
-        if (e + V - 1 < c.next) { fast_vec(e); continue; }
+        if (e <= c.next - V) { fast_vec(e); continue; }
       }
       general_vec(e);
     }

@@ -110,3 +110,45 @@ def test_batch_4096_columns_full_size():
         assert glc.serialize_host(ctx, bc) == glc.serialize_host(ctx, single)
         single.free()
     batch.free()
+
+
+@pytest.mark.parametrize("dt,mode", [(glc.I32, glc.FIXED), (glc.I32, glc.VARIABLE), (glc.U64, glc.FIXED)])
+def test_longest_column(dt, mode):
+    """n = 2^31 - 1 values, the longest column int32 positions address: decode, a range at the end
+    and lookups of the last positions.  The outputs carry 64 sentinel elements past their end,
+    so a write past n would show instead of landing outside the allocation."""
+    n = 2 ** 31 - 1
+    ctx = _ctx()
+    s = torch.cuda.current_stream().cuda_stream
+    g = torch.Generator(device="cuda:0")
+    g.manual_seed(5)
+    tdt = torch.int32 if dt == glc.I32 else torch.int64
+    v = torch.randint(0, 1 << 12, (n,), device="cuda:0", generator=g, dtype=torch.int64)
+    v += torch.arange(n, device="cuda:0", dtype=torch.int64) >> 4
+    v = v.to(tdt)
+    torch.cuda.synchronize()
+    col = glc.compress_device(ctx, dt, v.data_ptr(), n, mode, fixed_len=4096, stream=s)
+    assert col.info().total_values == n
+    pad = 64
+    out = torch.full((n + pad,), -5, dtype=tdt, device="cuda:0")
+    torch.cuda.synchronize()
+    glc.decompress_into(ctx, col, out.data_ptr(), glc.SRC_PACKED, stream=s)
+    ctx.sync()
+    torch.cuda.synchronize()
+    assert torch.equal(out[:n], v)
+    assert bool((out[n:] == -5).all()), "write past the end of the output"
+    del out
+    r = torch.full((1000 + pad,), -5, dtype=tdt, device="cuda:0")
+    torch.cuda.synchronize()
+    glc.decompress_range_into(ctx, col, n - 1000, 1000, r.data_ptr(), glc.SRC_PACKED, stream=s)
+    ctx.sync()
+    torch.cuda.synchronize()
+    assert torch.equal(r[:1000], v[n - 1000:]) and bool((r[1000:] == -5).all())
+    pos = torch.arange(n - 5000, n, dtype=torch.int32, device="cuda:0")
+    q = torch.empty(5000, dtype=tdt, device="cuda:0")
+    torch.cuda.synchronize()
+    glc.random_access_into(ctx, col, pos.data_ptr(), 5000, q.data_ptr(), stream=s)
+    ctx.sync()
+    torch.cuda.synchronize()
+    assert torch.equal(q, v[n - 5000:])
+    col.free()
