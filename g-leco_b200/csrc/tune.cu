@@ -11,6 +11,8 @@
 // glc_autotune times every candidate on a synthetic fixed-partitioned column whose fields have the
 // bucket's width (48M values, larger than L2) and keeps the fastest; the table can be written to
 // and read from a text file keyed by the device (name, SM count, compute capability).
+#include <unistd.h>
+
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -61,8 +63,11 @@ std::string device_key(const glc_ctx* ctx) {
   return buf;
 }
 
+// Written to a private temporary file and renamed over `path`, so processes tuning at the same
+// time (one per GPU) never read a half-written table.
 bool tune_save(const glc_ctx* ctx, const char* path) {
-  FILE* f = fopen(path, "w");
+  const std::string tmp = std::string(path) + ".tmp." + std::to_string((long long)getpid());
+  FILE* f = fopen(tmp.c_str(), "w");
   if (!f) return false;
   fprintf(f, "%s\n", device_key(ctx).c_str());
   for (int d = 0; d < 4; d++)
@@ -72,7 +77,15 @@ bool tune_save(const glc_ctx* ctx, const char* path) {
         fprintf(f, "%d %d %d %d %d %d %d %.3f %.4f\n", d, b, p, t.decode_stages, t.decode_unroll, t.ra_shape,
                 t.decode_cap_words, t.decode_gbs, t.ra_glookups);
       }
-  return fclose(f) == 0;
+  if (fclose(f) != 0) {
+    remove(tmp.c_str());
+    return false;
+  }
+  if (rename(tmp.c_str(), path) != 0) {
+    remove(tmp.c_str());
+    return false;
+  }
+  return true;
 }
 
 // Mean device time of `reps` launches after two warm-up launches, in milliseconds (< 0: failure).
