@@ -849,7 +849,7 @@ def main():
     ap.add_argument("--mode", default="packed", choices=["packed", "preunpacked"], help="c3 residual source")
     ap.add_argument("--queries", type=int, default=100_000_000, help="c3 lookups per step")
     ap.add_argument("--rates", default="10000,30000,100000,300000,1000000", help="c5: request rates (req/s)")
-    ap.add_argument("--ra-rates", default="1000000,2000000,4000000", help="c5: lookup-only request rates")
+    ap.add_argument("--ra-rates", default="1000000,2000000,4000000,8000000", help="c5: lookup-only request rates")
     ap.add_argument("--serve-seconds", type=float, default=0.5, help="c5: scheduled duration per rate")
     ap.add_argument("--serve-scale", type=float, default=1.0, help="c5: column length scale (1 = full size)")
     ap.add_argument("--slots", type=int, default=4, help="c5: shared launches in flight")

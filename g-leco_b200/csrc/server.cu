@@ -17,6 +17,7 @@
 #include <algorithm>
 #include <atomic>
 #include <chrono>
+#include <climits>
 #include <condition_variable>
 #include <cstring>
 #include <deque>
@@ -333,11 +334,20 @@ void launch_slot(glc_server* S, Slot& sl, std::deque<Req*>& ready_l, std::deque<
 
 void worker_main(glc_server* S) {
   cudaSetDevice(S->ctx->device);
+  // Requests not yet arrived: a FIFO for the usual case of submissions in arrival order, and a
+  // heap for the ones that arrive earlier than a request already queued.
   auto later = [](const Req* a, const Req* b) { return a->arrival > b->arrival; };
-  std::priority_queue<Req*, std::vector<Req*>, decltype(later)> future(later);
+  std::priority_queue<Req*, std::vector<Req*>, decltype(later)> future_heap(later);
+  std::deque<Req*> future_fifo;
   std::deque<Req*> ready_l, ready_r;
   std::vector<Req*> fresh;
   const int nslots = S->cfg.slots;
+  auto next_arrival = [&]() -> int64_t {
+    int64_t t = INT64_MAX;
+    if (!future_fifo.empty()) t = future_fifo.front()->arrival;
+    if (!future_heap.empty() && future_heap.top()->arrival < t) t = future_heap.top()->arrival;
+    return t;
+  };
   for (;;) {
     bool any_busy = false;
     for (int i = 0; i < nslots; i++) {
@@ -360,13 +370,26 @@ void worker_main(glc_server* S) {
         fresh.swap(S->incoming);
         S->n_incoming.store(0, std::memory_order_relaxed);
       }
-      for (Req* r : fresh) future.push(r);
+      for (Req* r : fresh) {
+        if (future_fifo.empty() || r->arrival >= future_fifo.back()->arrival) future_fifo.push_back(r);
+        else future_heap.push(r);
+      }
       fresh.clear();
     }
     const int64_t t = now_ns();
-    while (!future.empty() && future.top()->arrival <= t) {
-      Req* r = future.top();
-      future.pop();
+    for (;;) {  // move every arrived request to its ready queue, in arrival order
+      Req* r = nullptr;
+      const bool f = !future_fifo.empty() && future_fifo.front()->arrival <= t;
+      const bool h = !future_heap.empty() && future_heap.top()->arrival <= t;
+      if (f && (!h || future_fifo.front()->arrival <= future_heap.top()->arrival)) {
+        r = future_fifo.front();
+        future_fifo.pop_front();
+      } else if (h) {
+        r = future_heap.top();
+        future_heap.pop();
+      } else {
+        break;
+      }
       (r->r.kind == GLC_REQ_LOOKUP ? ready_l : ready_r).push_back(r);
     }
     if (!ready_l.empty() || !ready_r.empty()) {
@@ -383,17 +406,18 @@ void worker_main(glc_server* S) {
       continue;
     }
     // Nothing on the GPU and nothing ready: wait for a submission, the next arrival or stop.
-    if (!future.empty() && future.top()->arrival - t < 200000) {
+    const int64_t na = next_arrival();
+    if (na != INT64_MAX && na - t < 200000) {
       std::this_thread::yield();  // arrival within 200 us: keep polling for punctual scheduling
       continue;
     }
     std::unique_lock<std::mutex> lk(S->mu);
-    if (S->stop && S->incoming.empty() && future.empty()) break;
+    if (S->stop && S->incoming.empty() && na == INT64_MAX) break;
     if (!S->incoming.empty()) continue;
-    if (future.empty()) {
+    if (na == INT64_MAX) {
       S->wake.wait(lk, [&] { return S->stop || !S->incoming.empty(); });
     } else {
-      const auto until = std::chrono::steady_clock::time_point(std::chrono::nanoseconds(future.top()->arrival - 100000));
+      const auto until = std::chrono::steady_clock::time_point(std::chrono::nanoseconds(na - 100000));
       S->wake.wait_until(lk, until, [&] { return S->stop || !S->incoming.empty(); });
     }
   }

@@ -304,3 +304,30 @@ def test_admit_blob_from_device_memory(oracle, reserve):
     assert np.array_equal(out.cpu().numpy().view(np.uint64), v)
     assert server.columns() == [cid2]
     server.close()
+
+
+def test_arrivals_out_of_submission_order():
+    """Requests submitted out of arrival order are scheduled by arrival time (not before it) and
+    all complete with the right values."""
+    ctx = glc.Context(0)
+    server = glc.Server(ctx, budget_bytes=1 << 32, slots=2)
+    cols = _columns(ctx, server, SPECS[:3])
+    reqs = _mixed_requests(cols, 120, seed=21, big=30_000)
+    _device_buffers(reqs)
+    t0 = server.now_ns() + 5_000_000
+    rng = np.random.default_rng(3)
+    arrivals = t0 + rng.permutation(len(reqs)) * 100_000  # 0.1 ms apart, shuffled against submission
+    torch.cuda.synchronize()
+    for lo in range(0, len(reqs), 17):  # several submissions, each out of order
+        part = reqs[lo:lo + 17]
+        server.submit(_as_array(part, arrivals[lo:lo + 17]))
+    server.drain(60_000)
+    recs = server.poll()
+    assert len(recs) == len(reqs) and np.all(recs["status"] == glc.OK)
+    for r, g in zip(reqs, _results(reqs)):
+        assert np.array_equal(g, r["want"])
+    by_tag = {int(c["tag"]): c for c in recs}
+    for r in reqs:
+        assert by_tag[r["tag"]]["arrival_ns"] == arrivals[r["tag"]]
+        assert by_tag[r["tag"]]["done_ns"] > arrivals[r["tag"]]
+    server.close()
