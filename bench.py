@@ -595,7 +595,8 @@ def run_serving(args):
     torch.cuda.synchronize(dev)
     torch.cuda.empty_cache()
     budget = int(60e9 * scale) if scale < 1 else int(60e9)
-    server = glc.Server(ctx, budget_bytes=budget, slots=args.slots, reserve=True)
+    server = glc.Server(ctx, budget_bytes=budget, slots=args.slots, max_range_values=args.max_range_values,
+                        reserve=True)
     ids, src_of = [], {}
     t0 = time.perf_counter()
     for si, s in enumerate(sources):
@@ -853,6 +854,7 @@ def main():
     ap.add_argument("--serve-seconds", type=float, default=0.5, help="c5: scheduled duration per rate")
     ap.add_argument("--serve-scale", type=float, default=1.0, help="c5: column length scale (1 = full size)")
     ap.add_argument("--slots", type=int, default=4, help="c5: shared launches in flight")
+    ap.add_argument("--max-range-values", type=int, default=0, help="c5: range values per launch (0 = server default)")
     ap.add_argument("--admit-during", type=int, default=8, help="c5: columns admitted during each rate point")
     args = ap.parse_args()
     if args.warmup < 3:
