@@ -217,7 +217,10 @@ def run_reference_arm(args):
             results.append(r)
     val = float(np.median([r["value"] for r in results]))
     line = {"impl": "reference", "metric": METRIC, "value": val, "unit": UNIT, "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+            "steps": args.steps, "warmup": args.warmup,
+            # the whole workload (n values) at the rate measured on the sample
+            "ms_per_step": round(n * 8 / (val * 1e9) * 1e3, 3) if val else None,
+            "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "u64", "data": "synthetic",
             "config": {"workload": WORKLOAD, "values": n, "sample_values": len(values)},
             "cpu_baseline": {**results[-1], "value": val},
