@@ -144,6 +144,7 @@ struct Cursor {
   double t0, t1;
   uint32_t base;  // bit of value e (relative to the stage) = base + e * bits  (mod 2^32)
   int start, next, bits, type, idx;
+  bool nonneg;    // theta0 >= 0 and theta1 >= 0: predictions at x >= 0 are never negative
 };
 
 template <typename T, bool PLAIN, bool RESID, int kUnroll = 2>
@@ -173,6 +174,7 @@ __device__ __forceinline__ void decode_tile(const DecodeArgs& a, const StageInfo
     const PartDesc d = cached ? sdesc[k] : load_desc_g(a.desc + pf + k);
     c.t0 = d.theta0;
     c.t1 = d.theta1;
+    c.nonneg = d.theta0 >= 0.0 && d.theta1 >= 0.0;
     c.bits = d.bits_type & 0xff;
     c.type = d.bits_type >> 8;
     c.start = d.start;
@@ -215,17 +217,36 @@ __device__ __forceinline__ void decode_tile(const DecodeArgs& a, const StageInfo
     OutT vals[V];
     const double x0 = (double)(e - c.start);
     if (!PLAIN && c.bits <= 32 && c.type != MODEL_DIRECT_COPY) {
-      const uint32_t pos = c.base + (uint32_t)e * (uint32_t)c.bits;
-      const uint32_t shl = (uint32_t)(32 - c.bits) & 31u;
-      const int32_t zmask = c.bits ? -1 : 0;
+      // fields of the vector, sign-extended (zero-width fields read nothing)
+      int32_t rr[V];
+      if (c.bits == 0) {
 #pragma unroll
-      for (int u = 0; u < V; u++) {
-        const uint32_t p = pos + (uint32_t)(u * c.bits);
-        const uint32_t wi = p >> 5;
-        const uint32_t f = __funnelshift_r(src[wi], src[wi + 1], p & 31);
-        const int32_t r = ((int32_t)(f << shl) >> shl) & zmask;
-        if (RESID) vals[u] = (OutT)r;
-        else vals[u] = (OutT)apply_delta<T>(predict_x<T>(c.t0, c.t1, u ? x0 + (double)u : x0), (long long)r);
+        for (int u = 0; u < V; u++) rr[u] = 0;
+      } else {
+        const uint32_t pos = c.base + (uint32_t)e * (uint32_t)c.bits;
+        const uint32_t shl = (uint32_t)(32 - c.bits) & 31u;
+#pragma unroll
+        for (int u = 0; u < V; u++) {
+          const uint32_t p = pos + (uint32_t)(u * c.bits);
+          const uint32_t wi = p >> 5;
+          const uint32_t f = __funnelshift_r(src[wi], src[wi + 1], p & 31);
+          rr[u] = (int32_t)(f << shl) >> shl;
+        }
+      }
+      if (RESID) {
+#pragma unroll
+        for (int u = 0; u < V; u++) vals[u] = (OutT)rr[u];
+      } else if (c.nonneg) {  // theta0, theta1 >= 0: every prediction is >= 0, one rounding bias
+        const double bias = __longlong_as_double(0x3FDFFFFFFFFFFFFFll);
+#pragma unroll
+        for (int u = 0; u < V; u++) {
+          const double pr = __fma_rn(c.t1, u ? x0 + (double)u : x0, c.t0);
+          vals[u] = (OutT)apply_delta<T>(sat_cast<T>(__dadd_rn(pr, bias)), (long long)rr[u]);
+        }
+      } else {
+#pragma unroll
+        for (int u = 0; u < V; u++)
+          vals[u] = (OutT)apply_delta<T>(predict_x<T>(c.t0, c.t1, u ? x0 + (double)u : x0), (long long)rr[u]);
       }
     } else {
 #pragma unroll
