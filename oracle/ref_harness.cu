@@ -15,6 +15,17 @@
 //        followed by the CPU serialize (api/G-LeCo.cuh:826).  Writes <outprefix>.blob and prints
 //        the reported compressed size.  Only the reference's compression kernels run on the GPU;
 //        none of its decoders does.
+//   gpudecode  <dtype> <blob.bin> <values.bin> <repeat>
+//        GPU only: deserializeGPU (api/G-LeCo.cuh:2157) of a blob, then the reference's own
+//        full decoders decompressFullFile_BitPacked (:1739), _OnTheFly_Optimized_V2 (:1842) and
+//        _WorkStealingAdvanced (:220), each `repeat` times; prints one line per decoder with the
+//        best API-call seconds (output allocation, kernel, device-to-host copy, free) and the
+//        values that differ from values.bin.  decompressFullFile_WorkStealing (:166) is not run:
+//        its work counter is a fresh cudaMalloc that the kernel resets from one thread while the
+//        other blocks may already read it, so an arbitrary start value can index outside the
+//        partition arrays.  The decoders read the word after a field, one past the bitstream at
+//        its end; the run is refused when the bitstream ends exactly at a 2 MB boundary, where
+//        that word would fall outside the allocation's pages.
 //   v6         <dtype> <values.bin> <out.bin>
 //        GPU only: GPUVariableLengthPartitionerV6<T>(values, 2048).partition()
 //        (compression/GpuPartitioner.cuh:34-214, base size as compress passes it).  out.bin as for
@@ -26,6 +37,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <algorithm>
 #include <chrono>
 #include <vector>
 #include <string>
@@ -111,6 +123,47 @@ template <typename T> static int run_v6(const char* in, const char* out) {
   return 0;
 }
 
+template <typename T> static int run_gpudecode(const char* blobp, const char* valp, int repeat) {
+  std::vector<uint8_t> blob = read_file(blobp);
+  std::vector<T> want = as_vec<T>(read_file(valp));
+  if (blob.size() < sizeof(SerializedHeader)) { fprintf(stderr, "short blob\n"); return 3; }
+  SerializedHeader hdr;
+  memcpy(&hdr, blob.data(), sizeof hdr);
+  const uint64_t dbytes = ((hdr.delta_array_size_bytes + 3) / 4) * 4;
+  if (dbytes == 0 || dbytes % (2u << 20) == 0) {
+    fprintf(stderr, "bitstream ends at a 2 MB boundary: not run\n");
+    return 4;
+  }
+  LeCoGPU<T> codec;
+  SerializedData sd;
+  sd.data = new uint8_t[blob.size()];
+  memcpy(sd.data, blob.data(), blob.size());
+  sd.size = blob.size();
+  CompressedData<T>* cd = codec.deserializeGPU(&sd, false);
+  if (!cd) { fprintf(stderr, "deserializeGPU rejected the blob\n"); return 3; }
+  typedef void (LeCoGPU<T>::*Dec)(CompressedData<T>*, std::vector<T>&);
+  const struct { const char* name; Dec f; } decs[] = {
+      {"decompressFullFile_BitPacked", &LeCoGPU<T>::decompressFullFile_BitPacked},
+      {"decompressFullFile_OnTheFly_Optimized_V2", &LeCoGPU<T>::decompressFullFile_OnTheFly_Optimized_V2},
+      {"decompressFullFile_WorkStealingAdvanced", &LeCoGPU<T>::decompressFullFile_WorkStealingAdvanced}};
+  for (const auto& d : decs) {
+    std::vector<T> out;
+    double best = 1e30;
+    for (int r = 0; r < (repeat > 0 ? repeat : 1); r++) {
+      cudaDeviceSynchronize();
+      auto t0 = std::chrono::steady_clock::now();
+      (codec.*(d.f))(cd, out);
+      auto t1 = std::chrono::steady_clock::now();
+      best = std::min(best, std::chrono::duration<double>(t1 - t0).count());
+    }
+    size_t bad = out.size() == want.size() ? 0 : want.size();
+    for (size_t i = 0; i < out.size() && i < want.size(); i++) bad += out[i] != want[i];
+    printf("%s %.9f %zu\n", d.name, best, bad);
+  }
+  codec.cleanup(cd);
+  return 0;
+}
+
 template <typename T> static int run_golden(const char* in, const char* prefix, bool var, bool gpu_part) {
   std::vector<T> v = as_vec<T>(read_file(in));
   LeCoGPU<T> codec;
@@ -136,6 +189,7 @@ template <typename T> static int dispatch(int argc, char** argv) {
     return run_golden<T>(argv[3], argv[4], how != "fixed", how == "v6");
   }
   if (mode == "v6" && argc >= 5) return run_v6<T>(argv[3], argv[4]);
+  if (mode == "gpudecode" && argc >= 6) return run_gpudecode<T>(argv[3], argv[4], atoi(argv[5]));
   fprintf(stderr, "bad arguments\n");
   return 2;
 }
