@@ -26,6 +26,12 @@
 //        partition arrays.  The decoders read the word after a field, one past the bitstream at
 //        its end; the run is refused when the bitstream ends exactly at a 2 MB boundary, where
 //        that word would fall outside the allocation's pages.
+//   gpura      <dtype> <blob.bin> <positions.bin> <values.bin> <partition_len> <repeat>
+//        GPU only: deserializeGPU of a fixed-partition blob, then the reference's own
+//        randomAccessFixed (:1878, partition = pos / len) and decompress (:615, binary search over
+//        the partitions), each `repeat` times over the int32 positions; prints one line per method
+//        with the best API-call seconds and the lookups that differ from values[pos].  The same
+//        2 MB-boundary rule as gpudecode applies.
 //   v6         <dtype> <values.bin> <out.bin>
 //        GPU only: GPUVariableLengthPartitionerV6<T>(values, 2048).partition()
 //        (compression/GpuPartitioner.cuh:34-214, base size as compress passes it).  out.bin as for
@@ -164,6 +170,47 @@ template <typename T> static int run_gpudecode(const char* blobp, const char* va
   return 0;
 }
 
+template <typename T> static int run_gpura(const char* blobp, const char* posp, const char* valp, int plen,
+                                           int repeat) {
+  std::vector<uint8_t> blob = read_file(blobp);
+  std::vector<int> pos = as_vec<int>(read_file(posp));
+  std::vector<T> vals = as_vec<T>(read_file(valp));
+  if (blob.size() < sizeof(SerializedHeader)) { fprintf(stderr, "short blob\n"); return 3; }
+  SerializedHeader hdr;
+  memcpy(&hdr, blob.data(), sizeof hdr);
+  const uint64_t dbytes = ((hdr.delta_array_size_bytes + 3) / 4) * 4;
+  if (dbytes == 0 || dbytes % (2u << 20) == 0) {
+    fprintf(stderr, "bitstream ends at a 2 MB boundary: not run\n");
+    return 4;
+  }
+  for (int p : pos)
+    if (p < 0 || (size_t)p >= vals.size()) { fprintf(stderr, "position outside the column\n"); return 3; }
+  LeCoGPU<T> codec;
+  SerializedData sd;
+  sd.data = new uint8_t[blob.size()];
+  memcpy(sd.data, blob.data(), blob.size());
+  sd.size = blob.size();
+  CompressedData<T>* cd = codec.deserializeGPU(&sd, false);
+  if (!cd) { fprintf(stderr, "deserializeGPU rejected the blob\n"); return 3; }
+  for (int m = 0; m < 2; m++) {
+    std::vector<T> out;
+    double best = 1e30;
+    for (int r = 0; r < (repeat > 0 ? repeat : 1); r++) {
+      cudaDeviceSynchronize();
+      auto t0 = std::chrono::steady_clock::now();
+      if (m == 0) codec.randomAccessFixed(cd, pos, out, plen);
+      else codec.decompress(cd, pos, out);
+      auto t1 = std::chrono::steady_clock::now();
+      best = std::min(best, std::chrono::duration<double>(t1 - t0).count());
+    }
+    size_t bad = out.size() == pos.size() ? 0 : pos.size();
+    for (size_t i = 0; i < out.size() && i < pos.size(); i++) bad += out[i] != vals[pos[i]];
+    printf("%s %.9f %zu\n", m == 0 ? "randomAccessFixed" : "decompress", best, bad);
+  }
+  codec.cleanup(cd);
+  return 0;
+}
+
 template <typename T> static int run_golden(const char* in, const char* prefix, bool var, bool gpu_part) {
   std::vector<T> v = as_vec<T>(read_file(in));
   LeCoGPU<T> codec;
@@ -190,6 +237,7 @@ template <typename T> static int dispatch(int argc, char** argv) {
   }
   if (mode == "v6" && argc >= 5) return run_v6<T>(argv[3], argv[4]);
   if (mode == "gpudecode" && argc >= 6) return run_gpudecode<T>(argv[3], argv[4], atoi(argv[5]));
+  if (mode == "gpura" && argc >= 8) return run_gpura<T>(argv[3], argv[4], argv[5], atoi(argv[6]), atoi(argv[7]));
   fprintf(stderr, "bad arguments\n");
   return 2;
 }
