@@ -32,6 +32,11 @@
 //        the partitions), each `repeat` times over the int32 positions; prints one line per method
 //        with the best API-call seconds and the lookups that differ from values[pos].  The same
 //        2 MB-boundary rule as gpudecode applies.
+//   gpucompress <dtype> <values.bin> <fixed|v6> <repeat>
+//        GPU only: the reference's own LeCoGPU<T>::compress (api/G-LeCo.cuh:349) with fixed
+//        partitions of TILE_SIZE or with its GPU partitioner (use_gpu_partitioning = true), each
+//        `repeat` times; prints the best API-call seconds (host values in, the upload included)
+//        and the reported compressed size.
 //   v6         <dtype> <values.bin> <out.bin>
 //        GPU only: GPUVariableLengthPartitionerV6<T>(values, 2048).partition()
 //        (compression/GpuPartitioner.cuh:34-214, base size as compress passes it).  out.bin as for
@@ -211,6 +216,25 @@ template <typename T> static int run_gpura(const char* blobp, const char* posp, 
   return 0;
 }
 
+template <typename T> static int run_gpucompress(const char* in, bool v6, int repeat) {
+  std::vector<T> v = as_vec<T>(read_file(in));
+  LeCoGPU<T> codec;
+  double best = 1e30;
+  long long size = 0;
+  for (int r = 0; r < (repeat > 0 ? repeat : 1); r++) {
+    cudaDeviceSynchronize();
+    auto t0 = std::chrono::steady_clock::now();
+    CompressedData<T>* cd = codec.compress(v, v6, &size, v6, "");
+    cudaDeviceSynchronize();
+    auto t1 = std::chrono::steady_clock::now();
+    if (!cd) { fprintf(stderr, "compress returned null\n"); return 3; }
+    best = std::min(best, std::chrono::duration<double>(t1 - t0).count());
+    codec.cleanup(cd);
+  }
+  printf("compress_%s %.9f %lld\n", v6 ? "v6" : "fixed", best, size);
+  return 0;
+}
+
 template <typename T> static int run_golden(const char* in, const char* prefix, bool var, bool gpu_part) {
   std::vector<T> v = as_vec<T>(read_file(in));
   LeCoGPU<T> codec;
@@ -236,6 +260,7 @@ template <typename T> static int dispatch(int argc, char** argv) {
     return run_golden<T>(argv[3], argv[4], how != "fixed", how == "v6");
   }
   if (mode == "v6" && argc >= 5) return run_v6<T>(argv[3], argv[4]);
+  if (mode == "gpucompress" && argc >= 6) return run_gpucompress<T>(argv[3], std::string(argv[4]) == "v6", atoi(argv[5]));
   if (mode == "gpudecode" && argc >= 6) return run_gpudecode<T>(argv[3], argv[4], atoi(argv[5]));
   if (mode == "gpura" && argc >= 8) return run_gpura<T>(argv[3], argv[4], argv[5], atoi(argv[6]), atoi(argv[7]));
   fprintf(stderr, "bad arguments\n");
