@@ -199,6 +199,7 @@ glc_status glc_destroy(glc_ctx* ctx) {
   if (ctx->d_flags) cudaFree(ctx->d_flags);
   if (ctx->d_stats) cudaFree(ctx->d_stats);
   if (ctx->h_stats) cudaFreeHost(ctx->h_stats);
+  stager_free(ctx);
   if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
   for (cudaStream_t a : ctx->aux_stream)
     if (a) cudaStreamDestroy(a);
@@ -342,7 +343,7 @@ glc_status glc_compress(glc_ctx* ctx, glc_dtype dtype, const void* values, int64
   if (flags & GLC_HOST_IN) {
     const size_t bytes = (size_t)n * dtype_size(dtype);
     cudaError_t e = pool_alloc(ctx, &staged, bytes, s);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(staged, values, bytes, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = host_upload(ctx, staged, values, bytes, s);
     if (e != cudaSuccess) {
       if (staged) cudaFreeAsync(staged, s);
       delete c;
@@ -380,7 +381,7 @@ static glc_status partition_only(glc_ctx* ctx, glc_dtype dtype, const void* valu
   if (flags & GLC_HOST_IN) {
     const size_t bytes = (size_t)n * dtype_size(dtype);
     CK(pool_alloc(ctx, &staged, bytes, s), "partition: upload");
-    CK(cudaMemcpyAsync(staged, values, bytes, cudaMemcpyHostToDevice, s), "partition: upload");
+    CK(host_upload(ctx, staged, values, bytes, s), "partition: upload");
     dev_values = staged;
   }
   int32_t* ds = nullptr;
@@ -463,8 +464,8 @@ glc_status glc_decompress_range(glc_ctx* ctx, const glc_column* col, glc_source 
   char* base = dev_out - first * (int64_t)es;
   cudaError_t e = launch_decode(ctx, col, plain, 0, first, first + count, base, s);
   if (e == cudaSuccess && staged)
-    e = cudaMemcpyAsync(out, dev_out, count * es,
-                        (flags & GLC_HOST_OUT) ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice, s);
+    e = (flags & GLC_HOST_OUT) ? host_download(ctx, out, dev_out, count * es, s)
+                               : cudaMemcpyAsync(out, dev_out, count * es, cudaMemcpyDeviceToDevice, s);
   if (tmp) cudaFreeAsync(tmp, s);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "decode");
   if (flags & GLC_HOST_OUT) return glc_sync(ctx, stream);
@@ -497,13 +498,13 @@ glc_status glc_random_access(glc_ctx* ctx, const glc_column* col, glc_source sou
   void* tpos = nullptr;
   if (flags & GLC_HOST_IN) {
     CK(pool_alloc(ctx, &tpos, 4 * count, s), "random access: positions");
-    CK(cudaMemcpyAsync(tpos, positions, 4 * count, cudaMemcpyHostToDevice, s), "random access: positions");
+    CK(host_upload(ctx, tpos, positions, 4 * count, s), "random access: positions");
     dpos = (const int32_t*)tpos;
   }
   if (flags & GLC_HOST_OUT) CK(pool_alloc(ctx, &dout, es * count, s), "random access: output");
   const int32_t fl = fixed_partition_len > 0 ? fixed_partition_len : col->fixed_len;
   cudaError_t e = launch_random_access(ctx, col, plain, dpos, count, dout, fl, s);
-  if (e == cudaSuccess && (flags & GLC_HOST_OUT)) e = cudaMemcpyAsync(out, dout, es * count, cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess && (flags & GLC_HOST_OUT)) e = host_download(ctx, out, dout, es * count, s);
   if (tpos) cudaFreeAsync(tpos, s);
   if (flags & GLC_HOST_OUT) cudaFreeAsync(dout, s);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "random access");
@@ -582,7 +583,9 @@ glc_status glc_serialize(glc_ctx* ctx, const glc_column* c, void* blob, uint64_t
   if (host) std::memcpy(b, &h, sizeof h);
   else CK(cudaMemcpyAsync(b, &h, sizeof h, cudaMemcpyHostToDevice, s), "serialize: header");
   for (const Piece& pc : pieces)
-    if (pc.bytes) CK(cudaMemcpyAsync(b + pc.off, pc.src, pc.bytes, k, s), "serialize: arrays");
+    if (pc.bytes)
+      CK(host ? host_download(ctx, b + pc.off, pc.src, pc.bytes, s) : cudaMemcpyAsync(b + pc.off, pc.src, pc.bytes, k, s),
+         "serialize: arrays");
   CK(cudaStreamSynchronize(s), "serialize: sync");  // the header lives on this stack frame
   return GLC_OK;
 }
@@ -647,12 +650,14 @@ glc_status glc::deserialize_column(glc_ctx* ctx, glc_dtype dtype, const void* bl
   const cudaMemcpyKind k = host ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
   const uint8_t* b = (const uint8_t*)blob;
   void* dst[7] = {c->d_start, c->d_end, c->d_types, c->d_params, c->d_bits, c->d_offs, c->d_err};
+  auto copy_in = [&](void* d, const void* src, size_t len) {
+    return host ? host_upload(ctx, d, src, len, s) : cudaMemcpyAsync(d, src, len, k, s);
+  };
   for (int j = 0; j < 7; j++)
-    if (lens[j] && (e = cudaMemcpyAsync(dst[j], b + offs[j], lens[j], k, s)) != cudaSuccess)
+    if (lens[j] && (e = copy_in(dst[j], b + offs[j], lens[j])) != cudaSuccess)
       return bail(cuda_fail(ctx, e, "deserialize: arrays"));
   if ((e = cudaMemsetAsync(c->d_words, 0, 4 * c->nwords_alloc, s)) != cudaSuccess ||
-      (h.delta_size && !defer_words &&
-       (e = cudaMemcpyAsync(c->d_words, b + h.delta_off, h.delta_size, k, s)) != cudaSuccess))
+      (h.delta_size && !defer_words && (e = copy_in(c->d_words, b + h.delta_off, h.delta_size)) != cudaSuccess))
     return bail(cuda_fail(ctx, e, "deserialize: bitstream"));
   // structure check, fixed-length detection and max width
   int* d_chk = (int*)(ctx->d_stats + 4);

@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 #include <cstdint>
 #include <atomic>
+#include <mutex>
 #include <vector>
 #include <string>
 #include "glc.h"
@@ -40,6 +41,7 @@ constexpr int kFlagWords = kCounterSlots + 8;
 }  // namespace glc
 
 namespace glc {
+struct HostStager;  // hostxfer.cu: pinned chunks and copy threads for pageable host transfers
 // Launch choices per (element type, widest-field bucket, residual source), filled with measured
 // defaults and replaced by glc_autotune.
 constexpr int kTuneBuckets = 6;  // widest field <= 8, 16, 24, 32, 48, 64 bits
@@ -70,6 +72,8 @@ struct glc_ctx {
   std::atomic<unsigned> next_slot{0};
   std::string err;
   glc::TuneEntry tune[4][glc::kTuneBuckets][2];  // [dtype][bucket][pre-unpacked source]
+  std::mutex stage_mu;                     // creates `stager` once
+  glc::HostStager* stager = nullptr;       // created by the first large pageable transfer
 };
 
 struct glc_column {
@@ -108,6 +112,11 @@ inline int dtype_size(glc_dtype d) { return (d == GLC_I64 || d == GLC_U64) ? 8 :
 inline const TuneEntry& tune_entry(const glc_ctx* ctx, glc_dtype d, int bits, int plain) {
   return ctx->tune[(int)d & 3][tune_bucket(bits)][plain ? 1 : 0];
 }
+// hostxfer.cu: host <-> device copies in stream order; pageable buffers of 4 MB and more go
+// through the context's pinned chunks (a download returns once `dst` holds the data)
+cudaError_t host_upload(glc_ctx* ctx, void* dst, const void* src, size_t bytes, cudaStream_t s);
+cudaError_t host_download(glc_ctx* ctx, void* dst, const void* src, size_t bytes, cudaStream_t s);
+void stager_free(glc_ctx* ctx);
 void tune_defaults(glc_ctx* ctx);                  // tune.cu
 bool tune_load(glc_ctx* ctx, const char* path);   // tune.cu: true when the file fits this device
 

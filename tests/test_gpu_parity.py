@@ -302,3 +302,26 @@ def test_streaming_blob_decode_to_host(oracle, kind, n):
     bad[8] ^= 1
     with pytest.raises(glc.GlcError):
         glc.decode_blob_to_host(codec.ctx, dt, bad.ctypes.data, len(bad), out.data_ptr())
+
+
+@pytest.mark.parametrize("n", [524_288, 4_194_305, 12_500_001])
+def test_large_pageable_host_buffers(n):
+    """Host (pageable) buffers of several MB go through the context's pinned chunks: compress from
+    host memory, decode into host memory (also at an odd offset), random access with host positions
+    and outputs, and a host blob round trip all return the input."""
+    v = _data("u64_piecewise", n)
+    codec = _codec(v)
+    col, _ = codec.compress(v, True)
+    assert np.array_equal(codec.decompressFullFile(col), v)
+    buf = np.zeros(n + 1, np.uint64)
+    glc.decompress_range_into(codec.ctx, col, 0, n, buf[1:].ctypes.data, glc.SRC_PACKED, host_out=True)
+    assert np.array_equal(buf[1:], v) and buf[0] == 0
+    pos = np.random.default_rng(3).integers(0, n, 2 * n).astype(np.int32)
+    out = np.zeros(len(pos), np.uint64)
+    glc.random_access_into(codec.ctx, col, pos.ctypes.data, len(pos), out.ctypes.data, host_in=True, host_out=True)
+    assert np.array_equal(out, v[pos])
+    blob = glc.serialize_host(codec.ctx, col)
+    back = glc.deserialize_host(codec.ctx, glc.U64, blob)
+    assert np.array_equal(codec.decompressFullFile(back), v)
+    back.free()
+    col.free()
