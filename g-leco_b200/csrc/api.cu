@@ -351,7 +351,11 @@ glc_status glc_compress(glc_ctx* ctx, glc_dtype dtype, const void* values, int64
     }
     dev_values = staged;
   }
-  glc_status st = compress_impl(ctx, dtype, dev_values, n, mode, fixed_partition_len, c, s);
+  glc_status st;
+  {
+    std::lock_guard<std::mutex> lk(ctx->stats_mu);  // the fit's totals come back through h_stats
+    st = compress_impl(ctx, dtype, dev_values, n, mode, fixed_partition_len, c, s);
+  }
   if (staged) cudaFreeAsync(staged, s);
   if (st != GLC_OK) {
     cudaStreamSynchronize(s);
@@ -388,6 +392,7 @@ static glc_status partition_only(glc_ctx* ctx, glc_dtype dtype, const void* valu
   int32_t* de = nullptr;
   int64_t P = 0;
   std::string perr;
+  std::unique_lock<std::mutex> stats_lock(ctx->stats_mu);  // partition counts come back through h_stats
   cudaError_t e = v6_base > 0 ? launch_partition_v6(ctx, dtype, dev_values, n, v6_base, &ds, &de, &P, s)
                               : launch_partition_variable(ctx, dtype, dev_values, n, &ds, &de, &P, s, &perr);
   if (staged) cudaFreeAsync(staged, s);
@@ -601,6 +606,7 @@ glc_status glc::deserialize_column(glc_ctx* ctx, glc_dtype dtype, const void* bl
                                    int crc32c, int pre_unpack, glc_column** out, glc_stream stream,
                                    cudaMemPool_t pool, bool defer_words) {
   if (!ctx || !out) return fail(ctx, GLC_ERR_INVALID_ARG, "null argument");
+  std::lock_guard<std::mutex> stats_lock(ctx->stats_mu);  // the checks come back through h_stats
   *out = nullptr;
   if (!valid_dtype(dtype)) return fail(ctx, GLC_ERR_INVALID_ARG, "unknown dtype");
   if (!blob || size < sizeof(BlobHeader)) return fail(ctx, GLC_ERR_BAD_BLOB, "blob shorter than its header");

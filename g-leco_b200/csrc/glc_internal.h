@@ -72,6 +72,7 @@ struct glc_ctx {
   std::atomic<unsigned> next_slot{0};
   std::string err;
   glc::TuneEntry tune[4][glc::kTuneBuckets][2];  // [dtype][bucket][pre-unpacked source]
+  std::mutex stats_mu;                     // held by calls that read results back through h_stats
   std::mutex stage_mu;                     // creates `stager` once
   glc::HostStager* stager = nullptr;       // created by the first large pageable transfer
 };

@@ -15,6 +15,10 @@
  *    (pageable or pinned); otherwise it is device memory of the context's device.
  *  - A column owns device memory in the reference's SoA layout (CompressedData<T>,
  *    api/G-LeCo_Types.cuh:18-42) plus derived lookup tables.
+ *  - A context may be shared by several host threads (the reference's instances may not,
+ *    api/G-LeCo.cuh:46-85, :103-107): calls that read results back to the host (compress,
+ *    partition, deserialize) take the context's lock, and pageable host buffers of 4 MB or more
+ *    share its two pinned 32 MB chunks one transfer at a time.
  */
 #ifndef GLC_H_
 #define GLC_H_

@@ -325,3 +325,31 @@ def test_large_pageable_host_buffers(n):
     assert np.array_equal(codec.decompressFullFile(back), v)
     back.free()
     col.free()
+
+
+def test_host_transfers_from_two_threads_on_one_context():
+    """Two host threads share one context: their pageable transfers go through the same pinned
+    chunks (one transfer at a time) and every result is still exact."""
+    import threading
+    ctx = glc.Context(0)
+    cols = [_data("u64_piecewise", 9_000_001, seed=s) for s in (1, 2)]
+    errors = []
+
+    def work(v):
+        try:
+            for _ in range(3):
+                col = glc.compress_device(ctx, glc.U64, v.ctypes.data, len(v), glc.VARIABLE, host=True)
+                out = np.zeros(len(v), np.uint64)
+                glc.decompress_into(ctx, col, out.ctypes.data, glc.SRC_PACKED, host_out=True)
+                if not np.array_equal(out, v):
+                    errors.append("mismatch")
+                col.free()
+        except Exception as ex:  # reported below
+            errors.append(repr(ex))
+
+    ts = [threading.Thread(target=work, args=(v,)) for v in cols]
+    for t in ts:
+        t.start()
+    for t in ts:
+        t.join(300)
+    assert not errors, errors
