@@ -389,19 +389,29 @@ def run_batch(args):
     ns = [n for _, n, *_ in specs]
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
-    # batched compress (partition length picked per column) vs a per-column compress loop
-    torch.cuda.synchronize(dev)
-    e0.record(stream)
-    batch = glc.Batch.compress(ctx, dtypes, [c.data_ptr() for c in cols], ns, fixed_len=0, stream=sh)
-    e1.record(stream)
-    torch.cuda.synchronize(dev)
-    batch_compress_ms = e0.elapsed_time(e1)
-    e0.record(stream)
-    singles = [glc.compress_device(ctx, d, c.data_ptr(), n, glc.FIXED, fixed_len=4096, stream=sh)
-               for d, c, n in zip(dtypes, cols, ns)]
-    e1.record(stream)
-    torch.cuda.synchronize(dev)
-    loop_compress_ms = e0.elapsed_time(e1)
+    # batched compress (partition length picked per column) vs a per-column compress loop; best of
+    # 3 calls each (the first call also grows the context's memory pool)
+    batch_compress_ms, loop_compress_ms, batch, singles = 1e30, 1e30, None, None
+    for rep in range(3):
+        if batch is not None:
+            batch.free()
+        torch.cuda.synchronize(dev)
+        e0.record(stream)
+        batch = glc.Batch.compress(ctx, dtypes, [c.data_ptr() for c in cols], ns, fixed_len=0, stream=sh)
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        batch_compress_ms = min(batch_compress_ms, e0.elapsed_time(e1))
+    for rep in range(3):
+        if singles is not None:
+            for sgl in singles:
+                sgl.free()
+        torch.cuda.synchronize(dev)
+        e0.record(stream)
+        singles = [glc.compress_device(ctx, d, c.data_ptr(), n, glc.FIXED, fixed_len=4096, stream=sh)
+                   for d, c, n in zip(dtypes, cols, ns)]
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        loop_compress_ms = min(loop_compress_ms, e0.elapsed_time(e1))
     comp_bytes = batch.compressed_size
     # outputs: one buffer, 16-byte aligned slices
     offs, o = [], 0
@@ -462,6 +472,7 @@ def run_batch(args):
                    "per_column_loop_ms": round(loop_ms, 3), "per_column_loop_gbs": round(raw_bytes / loop_ms / 1e6, 2),
                    "speedup_vs_per_column_loop": round(loop_ms / ms, 2),
                    "batch_compress_ms": round(batch_compress_ms, 2), "per_column_compress_loop_ms": round(loop_compress_ms, 2),
+                   "compress_timing": "best of 3 calls each (CUDA events on the calling stream)",
                    "partition_lengths": {str(L): sum(1 for c in batch.columns if c.info().fixed_partition_len == L)
                                          for L in (1024, 2048, 4096)},
                    "graph": "one persistent launch captured in a CUDA graph and replayed", "bit_exact": ok},

@@ -38,6 +38,7 @@ struct glc_batch {
   int64_t nwork = 0;
   unsigned long long* d_counter = nullptr;
   int64_t group_begin[5] = {0, 0, 0, 0, 0};  // work items grouped by element type
+  cudaStream_t alloc_stream = nullptr;        // stream of the pool allocations in `storage`
   int* d_err = nullptr;
   cudaGraphExec_t graph = nullptr;
 };
@@ -176,6 +177,142 @@ batch_fit_kernel(const FitCol* __restrict__ cols, const int64_t* __restrict__ pa
   widths[p] = len * b;
 }
 
+// Choice of the partition length, one read of the values: one CTA per 4096-value chunk of a
+// column fits the chunk (length 4096), its two halves (2048) and its four quarters (1024) from
+// exact per-quarter sums, then measures all seven lines in one residual pass.  Partitions of each
+// candidate length start at multiples of that length, so the halves and quarters are exactly the
+// 2048- and 1024-value partitions, and the bits equal those of three separate fits.
+// col_bits[3 c + k] receives the column's residual bits for length 1024 << k.
+template <typename T>
+__device__ void choose_chunk(const T* __restrict__ v, int64_t len, unsigned long long* __restrict__ col_bits) {
+  constexpr int W = kFitCTA / 32;
+  __shared__ i128 s_y[W][4], s_xy[W][4];
+  __shared__ int s_ov[W];
+  __shared__ double s_t0[7], s_t1[7];
+  __shared__ int s_over;
+  __shared__ long long s_m[W][7];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  i128 y[4], xy[4];
+  int ov = 0;
+#pragma unroll
+  for (int q = 0; q < 4; q++) {
+    y[q] = 0;
+    xy[q] = 0;
+#pragma unroll
+    for (int k = 0; k < 1024 / kFitCTA; k++) {
+      const int64_t i = q * 1024 + k * kFitCTA + threadIdx.x;
+      if (i < len) {
+        const T x = __ldg(v + i);
+        if (overflows_double<T>(x)) ov |= 1 << q;
+        y[q] += (i128)x;
+        xy[q] += (i128)i * (i128)x;  // chunk-relative position; lines subtract their start below
+      }
+    }
+  }
+#pragma unroll
+  for (int q = 0; q < 4; q++) {
+    y[q] = warp_sum_i128(y[q]);
+    xy[q] = warp_sum_i128(xy[q]);
+  }
+  ov = __reduce_or_sync(FULL_MASK, ov);
+  if (lane == 0) {
+#pragma unroll
+    for (int q = 0; q < 4; q++) { s_y[warp][q] = y[q]; s_xy[warp][q] = xy[q]; }
+    s_ov[warp] = ov;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    i128 Y[4] = {0, 0, 0, 0}, XY[4] = {0, 0, 0, 0};
+    int o = 0;
+    for (int w = 0; w < W; w++) {
+      for (int q = 0; q < 4; q++) { Y[q] += s_y[w][q]; XY[q] += s_xy[w][q]; }
+      o |= s_ov[w];
+    }
+    // lines: 0 = the chunk, 1-2 = halves, 3-6 = quarters: [q0, q1) in quarters
+    const int q0s[7] = {0, 0, 2, 0, 1, 2, 3}, q1s[7] = {4, 2, 4, 1, 2, 3, 4};
+    int over = 0;
+    for (int l = 0; l < 7; l++) {
+      const int64_t a = q0s[l] * 1024, b = q1s[l] * 1024 < len ? q1s[l] * 1024 : len;
+      double t0 = 0.0, t1 = 0.0;
+      int lo = 0;
+      for (int q = q0s[l]; q < q1s[l]; q++) lo |= (o >> q) & 1;
+      if (b > a && !lo) {
+        i128 sy = 0, sxy = 0;
+        for (int q = q0s[l]; q < q1s[l]; q++) { sy += Y[q]; sxy += XY[q]; }
+        solve_line(b - a, sy, sxy - (i128)a * sy, t0, t1);
+      }
+      if (lo) over |= 1 << l;
+      s_t0[l] = t0;
+      s_t1[l] = t1;
+    }
+    s_over = over;
+  }
+  __syncthreads();
+  const int over = s_over;
+  long long m[7] = {0, 0, 0, 0, 0, 0, 0};
+#pragma unroll
+  for (int q = 0; q < 4; q++) {
+    const int lh = 1 + (q >> 1), lq = 3 + q;
+#pragma unroll
+    for (int k = 0; k < 1024 / kFitCTA; k++) {
+      const int64_t i = q * 1024 + k * kFitCTA + threadIdx.x;
+      if (i < len) {
+        const T x = __ldg(v + i);
+        if (!(over & 1)) {
+          const long long d = abs_ref(calc_delta<T>(x, predict<T>(s_t0[0], s_t1[0], i)));
+          m[0] = d > m[0] ? d : m[0];
+        }
+        if (!((over >> lh) & 1)) {
+          const long long d = abs_ref(calc_delta<T>(x, predict<T>(s_t0[lh], s_t1[lh], i - (q >> 1) * 2048)));
+          m[lh] = d > m[lh] ? d : m[lh];
+        }
+        if (!((over >> lq) & 1)) {
+          const long long d = abs_ref(calc_delta<T>(x, predict<T>(s_t0[lq], s_t1[lq], i - q * 1024)));
+          m[lq] = d > m[lq] ? d : m[lq];
+        }
+      }
+    }
+  }
+#pragma unroll
+  for (int l = 0; l < 7; l++) {
+    const long long t = warp_max_ll(m[l]);
+    if (lane == 0) s_m[warp][l] = t;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned long long add[3] = {0, 0, 0};
+    for (int l = 0; l < 7; l++) {
+      const int q0 = l == 0 ? 0 : (l < 3 ? (l - 1) * 2 : l - 3);
+      const int q1 = l == 0 ? 4 : (l < 3 ? q0 + 2 : q0 + 1);
+      const int64_t a = q0 * 1024, b = q1 * 1024 < len ? q1 * 1024 : len;
+      if (b <= a) continue;
+      long long t = 0;
+      for (int w = 0; w < W; w++) t = s_m[w][l] > t ? s_m[w][l] : t;
+      const int bits = ((over >> l) & 1) ? (int)sizeof(T) * 8 : bits_for(t);
+      add[l == 0 ? 2 : (l < 3 ? 1 : 0)] += (unsigned long long)((b - a) * bits);
+    }
+    for (int k = 0; k < 3; k++)
+      if (add[k]) atomicAdd(col_bits + k, add[k]);
+  }
+}
+
+// One CTA per 4096-value chunk of any column (cols[] laid out with length 4096).
+__global__ void __launch_bounds__(kFitCTA)
+batch_choose_kernel(const FitCol* __restrict__ cols, const int64_t* __restrict__ part_base, int ncols,
+                    unsigned long long* __restrict__ col_bits) {
+  const int64_t p = blockIdx.x;
+  const int c = col_of(part_base, ncols, p);
+  const FitCol fc = cols[c];
+  const int64_t s = (p - fc.part_base) * 4096;
+  const int64_t len = (s + 4096 < fc.n ? s + 4096 : fc.n) - s;
+  switch (fc.dtype) {
+    case GLC_I32: choose_chunk<int32_t>((const int32_t*)fc.values + s, len, col_bits + 3 * c); break;
+    case GLC_I64: choose_chunk<int64_t>((const int64_t*)fc.values + s, len, col_bits + 3 * c); break;
+    case GLC_U64: choose_chunk<uint64_t>((const uint64_t*)fc.values + s, len, col_bits + 3 * c); break;
+    default: choose_chunk<uint32_t>((const uint32_t*)fc.values + s, len, col_bits + 3 * c); break;
+  }
+}
+
 // Global exclusive bit prefix -> column-local offsets; col_stats[c] = {total bits, max bits}.
 __global__ void batch_local_offsets_kernel(const int64_t* __restrict__ gofs, const int64_t* __restrict__ part_base,
                                            const int32_t* __restrict__ bits, int ncols, int64_t P,
@@ -250,9 +387,11 @@ __global__ void batch_desc_kernel(const int32_t* __restrict__ starts, const int3
   desc[p] = d;
 }
 
+// The batch's arrays come from the context's stream-ordered pool (no device-wide synchronisation
+// per allocation); they are returned to it when the batch is freed.
 template <typename V> cudaError_t dalloc(glc_batch* b, V** p, size_t count) {
   void* q = nullptr;
-  cudaError_t e = cudaMalloc(&q, count * sizeof(V) + 16);
+  cudaError_t e = cudaMallocFromPoolAsync(&q, count * sizeof(V) + 16, b->ctx->pool, b->alloc_stream);
   if (e == cudaSuccess) b->storage.push_back(q);
   *p = (V*)q;
   return e;
@@ -262,7 +401,8 @@ void free_batch(glc_batch* b) {
   if (b->graph) cudaGraphExecDestroy(b->graph);
   if (b->owns_columns)
     for (glc_column* c : b->cols) delete c;  // views: their arrays are in storage
-  for (void* q : b->storage) cudaFree(q);
+  for (void* q : b->storage) cudaFreeAsync(q, b->ctx->own_stream);
+  if (!b->storage.empty()) cudaStreamSynchronize(b->ctx->own_stream);
   if (b->d_cols) cudaFree(b->d_cols);
   if (b->d_work) cudaFree(b->d_work);
   if (b->d_counter) cudaFree(b->d_counter);
@@ -362,6 +502,7 @@ glc_status glc_batch_compress(glc_ctx* ctx, const glc_dtype* dtypes, const void*
   if (!b) return GLC_ERR_OOM;
   b->ctx = ctx;
   b->owns_columns = true;
+  b->alloc_stream = s;
   auto bail = [&](glc_status st) { cudaStreamSynchronize(s); free_batch(b); return st; };
   const int nc = ncols;
 
@@ -386,31 +527,29 @@ glc_status glc_batch_compress(glc_ctx* ctx, const glc_dtype* dtypes, const void*
     return ee;
   };
   if ((e = dalloc(b, &d_fc, nc)) != cudaSuccess || (e = dalloc(b, &d_pb, nc + 1)) != cudaSuccess ||
-      (e = dalloc(b, &d_colbits, nc)) != cudaSuccess)
+      (e = dalloc(b, &d_colbits, 3 * (size_t)nc)) != cudaSuccess)
     return bail(bcuda(ctx, e, "batch compress: allocation"));
-  if (fixed_partition_len == 0) {
-    std::vector<int64_t> best_size(nc, INT64_MAX);
-    std::vector<int32_t> best_len(nc, kCandidates[2]);
-    std::vector<unsigned long long> hbits(nc);
-    for (int cand : kCandidates) {
-      std::vector<int32_t> L(nc, cand);
-      if ((e = upload_layout(L)) != cudaSuccess) return bail(bcuda(ctx, e, "batch compress: layout"));
-      if ((e = cudaMemsetAsync(d_colbits, 0, sizeof(unsigned long long) * nc, s)) != cudaSuccess)
-        return bail(bcuda(ctx, e, "batch compress: sizes"));
-      if (pb[nc] > 0)
-        batch_fit_kernel<<<(unsigned)pb[nc], kFitCTA, 0, s>>>(d_fc, d_pb, nc, 1, d_colbits, nullptr, nullptr, nullptr,
-                                                              nullptr, nullptr, nullptr, nullptr);
-      if ((e = cudaMemcpyAsync(hbits.data(), d_colbits, sizeof(unsigned long long) * nc, cudaMemcpyDeviceToHost, s)) !=
-              cudaSuccess ||
-          (e = cudaStreamSynchronize(s)) != cudaSuccess)
-        return bail(bcuda(ctx, e, "batch compress: sizes"));
-      for (int i = 0; i < nc; i++) {
-        const int64_t P = pb[i + 1] - pb[i];
-        const int64_t size = 64 * P + 120 + (int64_t)(hbits[i] + 7) / 8;  // api/G-LeCo.cuh:589-603
-        if (size < best_size[i]) { best_size[i] = size; best_len[i] = cand; }
+  if (fixed_partition_len == 0) {  // one pass measures all three candidate lengths
+    std::vector<int32_t> L(nc, 4096);
+    std::vector<unsigned long long> hbits(3 * (size_t)nc);
+    if ((e = upload_layout(L)) != cudaSuccess) return bail(bcuda(ctx, e, "batch compress: layout"));
+    if ((e = cudaMemsetAsync(d_colbits, 0, sizeof(unsigned long long) * 3 * nc, s)) != cudaSuccess)
+      return bail(bcuda(ctx, e, "batch compress: sizes"));
+    if (pb[nc] > 0) batch_choose_kernel<<<(unsigned)pb[nc], kFitCTA, 0, s>>>(d_fc, d_pb, nc, d_colbits);
+    if ((e = cudaGetLastError()) != cudaSuccess ||
+        (e = cudaMemcpyAsync(hbits.data(), d_colbits, sizeof(unsigned long long) * 3 * nc, cudaMemcpyDeviceToHost,
+                             s)) != cudaSuccess ||
+        (e = cudaStreamSynchronize(s)) != cudaSuccess)
+      return bail(bcuda(ctx, e, "batch compress: sizes"));
+    for (int i = 0; i < nc; i++) {
+      int64_t best = INT64_MAX;
+      for (int k = 0; k < 3; k++) {
+        const int64_t cand = kCandidates[k];
+        const int64_t P = ns[i] > 0 ? (ns[i] + cand - 1) / cand : 0;
+        const int64_t size = 64 * P + 120 + (int64_t)(hbits[3 * i + k] + 7) / 8;  // api/G-LeCo.cuh:589-603
+        if (size < best) { best = size; len[i] = (int32_t)cand; }
       }
     }
-    len = best_len;
   }
   if ((e = upload_layout(len)) != cudaSuccess) return bail(bcuda(ctx, e, "batch compress: layout"));
   const int64_t P = pb[nc];

@@ -60,6 +60,13 @@ def test_batch_compress_matches_single_column(oracle, fixed_len):
         if len(v) == 0:
             continue
         total += info.compressed_size_bytes
+        if not fixed_len:  # the chosen length is the first of 1024 / 2048 / 4096 with the smallest size
+            sizes = []
+            for cand in (1024, 2048, 4096):
+                sc = glc.compress_device(ctx, dt, v.ctypes.data, len(v), glc.FIXED, fixed_len=cand, host=True)
+                sizes.append(sc.info().compressed_size_bytes)
+                sc.free()
+            assert L == (1024, 2048, 4096)[int(np.argmin(sizes))], (L, sizes)
         single = glc.compress_device(ctx, dt, v.ctypes.data, len(v), glc.FIXED, fixed_len=L, host=True)
         blob = glc.serialize_host(ctx, bc)
         assert blob == glc.serialize_host(ctx, single)
