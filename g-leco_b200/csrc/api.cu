@@ -229,6 +229,7 @@ glc_status glc_column_free(glc_column* col) {
   if (!col) return GLC_ERR_INVALID_ARG;
   if (col->view) return fail(col->ctx, GLC_ERR_INVALID_ARG, "a column of a batch is freed with its batch");
   if (col->ctx) cudaSetDevice(col->ctx->device);
+  if (col->sync_free) cudaDeviceSynchronize();  // work on any stream may still read the arrays
   free_column_arrays(col);
   delete col;
   return GLC_OK;
@@ -265,6 +266,10 @@ static glc_status compress_impl(glc_ctx* ctx, glc_dtype dtype, const void* dev_v
   c->ctx = ctx;
   c->dtype = dtype;
   c->n = n;
+  // The column's arrays come from the context's pool (no cudaMalloc per array per call); freeing
+  // the column synchronises the device first, so a free behaves as cudaFree does.
+  c->pool = ctx->pool;
+  c->sync_free = true;
   int32_t* tmp_s = nullptr;
   int32_t* tmp_e = nullptr;
   if (mode == GLC_PART_FIXED) {
@@ -297,16 +302,18 @@ static glc_status compress_impl(glc_ctx* ctx, glc_dtype dtype, const void* dev_v
   void* scratch = nullptr;
   CK(pool_alloc(ctx, &scratch, sb, s), "compress: scratch allocation");
   cudaError_t e = launch_fit(dtype, dev_values, c, scratch, sb, ctx->d_stats, s);
-  if (e == cudaSuccess) e = cudaMemcpyAsync(ctx->h_stats, ctx->d_stats, 2 * sizeof(int64_t), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(ctx->h_stats, ctx->d_stats, 4 * sizeof(int64_t), cudaMemcpyDeviceToHost, s);
   cudaFreeAsync(scratch, s);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "compress: fit");
+  if (ctx->h_stats[2] != DEVERR_NONE) return fail(ctx, GLC_ERR_TIMEOUT, "compress: a device-side wait of the fit gave up");
   c->total_bits = ctx->h_stats[0];
   c->max_bits = (int32_t)ctx->h_stats[1];
   set_word_counts(c);
-  CK(cudaMalloc(&c->d_words, 4 * c->nwords_alloc), "compress: word allocation");
-  CK(launch_pack(dtype, dev_values, c, s), "compress: pack");
+  CK(col_alloc(c, &c->d_words, 4 * c->nwords_alloc, s), "compress: word allocation");
+  const int64_t parts_per_tile = ctx->h_stats[3];
   CK(launch_desc_and_tiles(c, s), "compress: tables");
+  CK(launch_pack(dtype, dev_values, c, parts_per_tile, ctx->d_flags + kFlagError, s), "compress: pack");
   c->reported_size = reported_size(c->P, c->total_bits);
   return GLC_OK;
 }
@@ -323,6 +330,8 @@ glc_status glc_compress(glc_ctx* ctx, glc_dtype dtype, const void* values, int64
     return fail(ctx, GLC_ERR_INVALID_ARG, "unknown partitioning");
   if (mode == GLC_PART_FIXED && fixed_partition_len <= 0)
     return fail(ctx, GLC_ERR_INVALID_ARG, "fixed partition length must be positive");
+  if (!(flags & GLC_HOST_IN) && ((uintptr_t)values % dtype_size(dtype)) != 0)
+    return fail(ctx, GLC_ERR_INVALID_ARG, "device values must be aligned to the element size");
   cudaSetDevice(ctx->device);
   cudaStream_t s = pick(ctx, stream);
   glc_column* c = new (std::nothrow) glc_column();
@@ -531,6 +540,7 @@ glc_status glc_preunpack(glc_ctx* ctx, glc_column* col, int drop_packed, glc_str
     CK(cudaStreamSynchronize(s), "pre-unpack: sync");
   }
   if (drop_packed && col->d_words) {  // api/G-LeCo.cuh:2283-2287
+    if (col->sync_free) cudaDeviceSynchronize();  // work on any stream may still read the bitstream
     col_release(col, col->d_words);
     col->d_words = nullptr;
   }

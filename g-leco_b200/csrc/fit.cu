@@ -10,8 +10,10 @@
 // (64-bit atomicMax per partition), and a thread per partition sets the bit width.  The
 // bit offsets are an exclusive scan of len * bits.  All passes read the values once or twice
 // with coalesced loads; nothing here is a contraction, so the bound is HBM bandwidth.
+#include <type_traits>
 #include "glc_internal.h"
 #include "glc_scan.cuh"
+#include "glc_tma.cuh"
 
 namespace glc {
 
@@ -40,14 +42,13 @@ __global__ void chunk_count_kernel(const int32_t* __restrict__ starts, const int
   nch[p] = len > 0 ? (len + kFitChunk - 1) / kFitChunk : 0;
 }
 
-// Partition owning chunk c: the last p with base[p] <= c.
-__device__ __forceinline__ int64_t chunk_owner(const int64_t* __restrict__ base, int64_t P, int64_t c) {
-  int64_t lo = 0, hi = P - 1;
-  while (lo < hi) {
-    int64_t mid = (lo + hi + 1) >> 1;
-    if (base[mid] <= c) lo = mid; else hi = mid - 1;
-  }
-  return lo;
+// owner[c] = the partition of chunk c (one thread per partition writes its chunks), so a fit CTA
+// finds its partition with one load instead of a dependent binary search.
+__global__ void chunk_owner_kernel(const int64_t* __restrict__ base, const int64_t* __restrict__ nch, int64_t P,
+                                   int32_t* __restrict__ owner) {
+  int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= P) return;
+  for (int64_t c = base[p], e = base[p] + nch[p]; c < e; c++) owner[c] = (int32_t)p;
 }
 
 struct FitChunkArgs {
@@ -55,31 +56,19 @@ struct FitChunkArgs {
   const int32_t* ends;
   const int64_t* chunk_base;
   const int64_t* num_chunks;  // device scalar: total chunks
+  const int32_t* owner;       // chunk -> partition
   int64_t P;
   i128* sy;
   i128* sxy;
   int* ovf;
 };
 
-template <typename T> __global__ void __launch_bounds__(kFitThreads)
-fit_sums_kernel(const T* __restrict__ v, FitChunkArgs a) {
-  const int64_t c = blockIdx.x;
-  if (c >= *a.num_chunks) return;
-  const int64_t p = chunk_owner(a.chunk_base, a.P, c);
-  const int64_t k = c - a.chunk_base[p];
-  const int64_t start = a.starts[p];
-  const int64_t len = (int64_t)a.ends[p] - start;
-  const int64_t i0 = k * kFitChunk;
-  const int64_t i1 = (i0 + kFitChunk < len) ? i0 + kFitChunk : len;
-  i128 sy = 0, sxy = 0;
-  int ovf = 0;
-  for (int64_t i = i0 + threadIdx.x; i < i1; i += kFitThreads) {
-    T x = __ldg(v + start + i);
-    ovf |= overflows_double<T>(x) ? 1 : 0;
-    i128 y = (i128)x;
-    sy += y;
-    sxy += (i128)i * y;
-  }
+// Barrier of the kFitThreads compute threads only (named barrier 1; a producer warp may run beside
+// them in the same CTA).
+__device__ __forceinline__ void fit_sync() { asm volatile("bar.sync 1, %0;" ::"n"(kFitThreads) : "memory"); }
+
+// Sum over the kFitThreads compute threads of two 128-bit values and an OR; valid in thread 0.
+__device__ __forceinline__ void block_sums(i128& sy, i128& sxy, int& ovf) {
   sy = warp_sum_i128(sy);
   sxy = warp_sum_i128(sxy);
   ovf = __any_sync(FULL_MASK, ovf);
@@ -87,23 +76,252 @@ fit_sums_kernel(const T* __restrict__ v, FitChunkArgs a) {
   __shared__ int s_ovf[kFitThreads / 32];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   if (lane == 0) { s_sy[warp] = sy; s_sxy[warp] = sxy; s_ovf[warp] = ovf; }
-  __syncthreads();
+  fit_sync();
   if (threadIdx.x == 0) {
-    i128 ty = 0, txy = 0;
-    int to = 0;
-    for (int w = 0; w < kFitThreads / 32; w++) { ty += s_sy[w]; txy += s_sxy[w]; to |= s_ovf[w]; }
-    a.sy[c] = ty;
-    a.sxy[c] = txy;
-    a.ovf[c] = to;
+    for (int w = 1; w < kFitThreads / 32; w++) { sy += s_sy[w]; sxy += s_sxy[w]; ovf |= s_ovf[w]; }
   }
 }
 
+// Max over the kFitThreads compute threads; valid in thread 0.
+__device__ __forceinline__ long long block_max(long long m) {
+  m = warp_max_ll(m);
+  __shared__ long long s_m[kFitThreads / 32];
+  if ((threadIdx.x & 31) == 0) s_m[threadIdx.x >> 5] = m;
+  fit_sync();
+  if (threadIdx.x == 0)
+    for (int w = 1; w < kFitThreads / 32; w++) m = s_m[w] > m ? s_m[w] : m;
+  return m;
+}
+
+// Persistent fit passes over a dense list of chunks (chunk j -> partition owner[j], chunk index
+// j - base[owner[j]] within it).  CTA = 8 compute warps + 1 producer warp.  The producer (one
+// lane) looks up each chunk's partition and stages its values in shared memory with one bulk
+// copy (source rounded down and length up to 16 bytes: the extra bytes lie in the same 16-byte
+// blocks as the chunk, never in another page), kFitStages chunks ahead, on full/empty mbarriers;
+// the compute warps work from shared memory while the next copies land.  Their ring wait is
+// done by thread 0 (bounded) and broadcast, so a timeout takes them out of the loop together.
+//   PASS 0 (every chunk): overflow flag and exact sums; a partition of at most one chunk is
+//     fitted completely -- line, max |delta| -- from the staged values (one HBM read).
+//   PASS 1 (chunks of partitions longer than one chunk): max |delta| against the line that
+//     fit_solve_kernel derived from the chunk sums, one atomicMax per chunk.
+constexpr int kFitStages = 2;
+
+struct FitStreamArgs {
+  const int32_t* starts;
+  const int32_t* ends;
+  const int64_t* count;   // device scalar: chunks in the list
+  const int32_t* owner;   // list entry -> partition
+  const int64_t* base;    // partition -> its first list entry
+  int64_t P;
+  i128* sy;               // PASS 0: sums of chunks of long partitions, by chunk number
+  i128* sxy;
+  int* ovf;
+  const int64_t* chunk_base;  // partition -> its first chunk number (PASS 0 list == chunk numbers)
+  int32_t* types;
+  double* params;
+  int64_t* err;
+  unsigned long long* status;  // DEVERR_* on a timed-out wait
+};
+
+struct FitStage {
+  int64_t j;       // list entry, -1 = no more work
+  int64_t p, i0;   // partition, first value of the chunk within it
+  int64_t len;     // partition length
+  double t0, t1;   // PASS 1: the partition's line
+  int32_t cnt;     // values in the chunk
+  int32_t head;    // byte offset of the first value in the stage
+  int32_t skip;    // PASS 1: direct-copy partition, nothing to measure
+};
+
+template <typename T> __host__ __device__ constexpr int fit_stage_bytes() { return kFitChunk * (int)sizeof(T) + 32; }
+
+// max over this thread's values x[jj] (jj = tid, tid + 256, ...) of abs_ref(calc_delta(x, pred))
+// with pred = predict(t0, t1, i0 + jj): the index advances as an exact double (no conversion per
+// value), and the saturating |delta| is formed once from the extreme differences.
+template <typename T>
+__device__ __forceinline__ long long chunk_max_abs_delta(const T* x, int cnt, double t0, double t1, int64_t i0) {
+  double xd = (double)(i0 + (int64_t)threadIdx.x);
+  if (TypeTraits<T>::is_signed || sizeof(T) == 4) {
+    // calc_delta is the plain (wrapping for 64-bit) signed difference
+    long long dmax = 0, dmin = 0;
+#pragma unroll 4
+    for (int jj = threadIdx.x; jj < cnt; jj += kFitThreads, xd += (double)kFitThreads) {
+      const long long d = calc_delta<T>(x[jj], predict_from<T>(__fma_rn(t1, xd, t0)));
+      dmax = d > dmax ? d : dmax;
+      dmin = d < dmin ? d : dmin;
+    }
+    const long long a1 = abs_ref(dmax), a2 = abs_ref(dmin);
+    return a1 > a2 ? a1 : a2;
+  } else {
+    // unsigned 64-bit: |a - p| saturated at 2^63 - 1 (calc_delta's saturation, then abs_ref)
+    uint64_t um = 0;
+#pragma unroll 4
+    for (int jj = threadIdx.x; jj < cnt; jj += kFitThreads, xd += (double)kFitThreads) {
+      const uint64_t a = (uint64_t)x[jj], p = (uint64_t)predict_from<T>(__fma_rn(t1, xd, t0));
+      const uint64_t d = a >= p ? a - p : p - a;
+      um = d > um ? d : um;
+    }
+    return um > 0x7fffffffffffffffull ? 0x7fffffffffffffffll : (long long)um;
+  }
+}
+
+constexpr int kFitCTA = kFitThreads + 32;  // compute warps + producer warp
+
+template <typename T, int PASS>
+__device__ __forceinline__ FitStage fit_stage_for(const T* __restrict__ v, const FitStreamArgs& a, int64_t j) {
+  FitStage m;
+  m.j = j;
+  m.p = a.owner[j];
+  const int64_t start = a.starts[m.p];
+  m.len = (int64_t)a.ends[m.p] - start;
+  m.i0 = (j - a.base[m.p]) * kFitChunk;
+  m.cnt = (int)((m.len - m.i0) < kFitChunk ? (m.len - m.i0) : kFitChunk);
+  m.skip = 0;
+  m.t0 = m.t1 = 0.0;
+  if (PASS == 1) {
+    m.skip = a.types[m.p] == MODEL_DIRECT_COPY;
+    m.t0 = a.params[4 * m.p];
+    m.t1 = a.params[4 * m.p + 1];
+  }
+  const uintptr_t addr = reinterpret_cast<uintptr_t>(v + start + m.i0);
+  m.head = (int)(addr & 15);
+  return m;
+}
+
+template <typename T, int PASS> __global__ void __launch_bounds__(kFitCTA)
+fit_stream_kernel(const T* __restrict__ v, FitStreamArgs a) {
+  extern __shared__ __align__(128) uint8_t smem[];
+  __shared__ __align__(8) uint64_t full[kFitStages], empty[kFitStages];
+  __shared__ FitStage s_meta[kFitStages];
+  __shared__ int s_ok, s_direct;
+  __shared__ double s_t[2];
+  if (threadIdx.x == 0) {
+    for (int st = 0; st < kFitStages; st++) {
+      mbar_init(&full[st], 1);
+      mbar_init(&empty[st], 1);
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+
+  if (threadIdx.x >= kFitThreads) {  // ---- producer ----
+    if (threadIdx.x != kFitThreads) return;
+    const int64_t total = *a.count;
+    int64_t j = blockIdx.x;
+    for (int k = 0;; k++, j += gridDim.x) {
+      const int st = k % kFitStages;
+      if (k >= kFitStages && !mbar_wait_bounded(&empty[st], (uint32_t)((k / kFitStages) - 1) & 1u)) {
+        atomicExch(a.status, (unsigned long long)DEVERR_TIMEOUT);
+        s_meta[st].j = -1;  // the compute warps stop at this stage (or time out on it)
+        mbar_arrive(&full[st]);
+        return;
+      }
+      if (j >= total) {
+        s_meta[st].j = -1;
+        mbar_arrive(&full[st]);  // no copy: completes the phase, the compute warps see the end
+        return;
+      }
+      const FitStage m = fit_stage_for<T, PASS>(v, a, j);
+      s_meta[st] = m;
+      if (m.skip) {
+        mbar_arrive(&full[st]);
+      } else {
+        const uint32_t bytes = (uint32_t)((m.head + (int64_t)m.cnt * (int64_t)sizeof(T) + 15) & ~15ll);
+        const void* src = reinterpret_cast<const uint8_t*>(v + a.starts[m.p] + m.i0) - m.head;
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        mbar_arrive_expect_tx(&full[st], bytes);
+        tma_bulk_load(smem + (size_t)st * fit_stage_bytes<T>(), src, bytes, &full[st]);
+      }
+    }
+  }
+
+  // ---- compute warps ----
+  for (int k = 0;; k++) {
+    const int st = k % kFitStages;
+    const uint32_t par = (uint32_t)(k / kFitStages) & 1u;
+    if (threadIdx.x == 0) {
+      s_ok = mbar_wait_bounded(&full[st], par);
+      if (!s_ok) {
+        atomicExch(a.status, (unsigned long long)DEVERR_TIMEOUT);
+        mbar_wait_bounded(&full[st], par);  // a copy in flight lands before the CTA exits
+      }
+    }
+    fit_sync();
+    if (!s_ok) return;
+    mbar_try_wait(&full[st], par);  // the phase is complete: orders this thread's reads after the copy
+    const FitStage m = s_meta[st];
+    if (m.j < 0) return;
+    const T* x = reinterpret_cast<const T*>(smem + (size_t)st * fit_stage_bytes<T>() + m.head);
+    if (PASS == 0) {
+      // Exact sums from 64-bit partials: y = yh * 2^32 + yl, so sum(y) and sum(jj * y) (jj < 4096,
+      // the index within the chunk) split into four sums that cannot overflow 64 bits over the
+      // 16 values of a thread; sum((i0 + jj) * y) = sum(jj * y) + i0 * sum(y) is added once.
+      typedef typename std::conditional<TypeTraits<T>::is_signed, int64_t, uint64_t>::type Acc;
+      Acc s_lo = 0, s_hi = 0, x_lo = 0, x_hi = 0;
+      int ovf = 0;
+#pragma unroll 4
+      for (int jj = threadIdx.x; jj < m.cnt; jj += kFitThreads) {
+        const T xv = x[jj];
+        ovf |= overflows_double<T>(xv) ? 1 : 0;
+        if (sizeof(T) == 8) {
+          const uint32_t yl = (uint32_t)(uint64_t)xv;
+          const Acc yh = TypeTraits<T>::is_signed ? (Acc)(int32_t)((int64_t)xv >> 32) : (Acc)(uint32_t)((uint64_t)xv >> 32);
+          s_lo += (Acc)yl;
+          s_hi += yh;
+          x_lo += (Acc)((uint64_t)(uint32_t)jj * yl);
+          x_hi += (Acc)jj * yh;
+        } else {
+          s_lo += (Acc)xv;
+          x_lo += (Acc)jj * (Acc)xv;
+        }
+      }
+      i128 sy = (i128)s_lo + (i128)s_hi * ((i128)1 << 32);
+      i128 sxy = (i128)x_lo + (i128)x_hi * ((i128)1 << 32);
+      block_sums(sy, sxy, ovf);
+      if (threadIdx.x == 0) sxy += (i128)m.i0 * sy;
+      if (m.len > kFitChunk) {  // a chunk of a longer partition: its sums, by chunk number
+        if (threadIdx.x == 0) { a.sy[m.j] = sy; a.sxy[m.j] = sxy; a.ovf[m.j] = ovf; }
+      } else {
+        if (threadIdx.x == 0) {
+          double t0 = 0.0, t1 = 0.0;
+          if (ovf) {
+            a.types[m.p] = MODEL_DIRECT_COPY;  // CompressionKernels.cuh:95-105
+          } else {
+            solve_line(m.len, sy, sxy, t0, t1);
+            a.types[m.p] = MODEL_LINEAR;
+          }
+          a.params[4 * m.p] = t0;
+          a.params[4 * m.p + 1] = t1;
+          a.params[4 * m.p + 2] = 0.0;
+          a.params[4 * m.p + 3] = 0.0;
+          s_t[0] = t0;
+          s_t[1] = t1;
+          s_direct = ovf;
+        }
+        fit_sync();
+        long long mx = 0;
+        if (!s_direct) mx = chunk_max_abs_delta<T>(x, m.cnt, s_t[0], s_t[1], 0);
+        mx = block_max(mx);
+        if (threadIdx.x == 0) a.err[m.p] = mx;
+      }
+    } else if (!m.skip) {
+      long long mx = chunk_max_abs_delta<T>(x, m.cnt, m.t0, m.t1, m.i0);
+      mx = block_max(mx);
+      if (threadIdx.x == 0 && mx > 0) atomicMax((long long*)a.err + m.p, mx);
+    }
+    fit_sync();  // every compute thread is done with stage st (and with s_t / s_direct)
+    if (threadIdx.x == 0) mbar_arrive(&empty[st]);
+  }
+}
+
+// Line of every partition longer than one chunk, from its chunks' sums.
 template <typename T> __global__ void fit_solve_kernel(FitChunkArgs a, const int64_t* __restrict__ nch,
                                                       int32_t* __restrict__ types, double* __restrict__ params,
                                                       int64_t* __restrict__ err) {
   int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= a.P) return;
   const int64_t len = (int64_t)a.ends[p] - a.starts[p];
+  if (len > 0 && len <= kFitChunk) return;  // fitted by PASS 0 of fit_stream_kernel
   const int64_t c0 = a.chunk_base[p], c1 = c0 + nch[p];
   i128 sy = 0, sxy = 0;
   int ovf = 0;
@@ -122,60 +340,72 @@ template <typename T> __global__ void fit_solve_kernel(FitChunkArgs a, const int
   err[p] = 0;
 }
 
-template <typename T> __global__ void __launch_bounds__(kFitThreads)
-fit_maxerr_kernel(const T* __restrict__ v, FitChunkArgs a, const int32_t* __restrict__ types,
-                  const double* __restrict__ params, long long* __restrict__ err) {
-  const int64_t c = blockIdx.x;
-  if (c >= *a.num_chunks) return;
-  const int64_t p = chunk_owner(a.chunk_base, a.P, c);
-  if (types[p] == MODEL_DIRECT_COPY) return;
-  const int64_t k = c - a.chunk_base[p];
-  const int64_t start = a.starts[p];
-  const int64_t len = (int64_t)a.ends[p] - start;
-  const int64_t i0 = k * kFitChunk;
-  const int64_t i1 = (i0 + kFitChunk < len) ? i0 + kFitChunk : len;
-  const double t0 = params[4 * p], t1 = params[4 * p + 1];
-  long long m = 0;
-  for (int64_t i = i0 + threadIdx.x; i < i1; i += kFitThreads) {
-    long long d = abs_ref(calc_delta<T>(__ldg(v + start + i), predict<T>(t0, t1, i)));
-    m = d > m ? d : m;
-  }
-  m = warp_max_ll(m);
-  __shared__ long long s_m[kFitThreads / 32];
-  if ((threadIdx.x & 31) == 0) s_m[threadIdx.x >> 5] = m;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    long long t = 0;
-    for (int w = 0; w < kFitThreads / 32; w++) t = s_m[w] > t ? s_m[w] : t;
-    if (t > 0) atomicMax(err + p, t);
-  }
-}
-
-// bits and len*bits; stats[1] = max bits.
+// bits and len*bits; stats[1] = max bits; stats[3] = max over all partitions but the last of
+// ceil(4096 / len) (bounds the partitions a 4096-value tile can span); one atomic per warp each.
 template <typename T> __global__ void fit_bits_kernel(const int32_t* __restrict__ starts, const int32_t* __restrict__ ends,
                                                      const int32_t* __restrict__ types, const int64_t* __restrict__ err,
                                                      int32_t* __restrict__ bits, int64_t* __restrict__ widths, int64_t P,
-                                                     unsigned long long* __restrict__ max_bits) {
-  int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= P) return;
-  int b = (types[p] == MODEL_DIRECT_COPY) ? (int)sizeof(T) * 8 : bits_for(err[p]);
-  bits[p] = b;
-  widths[p] = ((int64_t)ends[p] - starts[p]) * b;
-  atomicMax(max_bits, (unsigned long long)b);
+                                                     unsigned long long* __restrict__ max_bits,
+                                                     unsigned long long* __restrict__ per_tile) {
+  const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  int b = 0;
+  unsigned k = 0;
+  if (p < P) {
+    b = (types[p] == MODEL_DIRECT_COPY) ? (int)sizeof(T) * 8 : bits_for(err[p]);
+    bits[p] = b;
+    const int64_t len = (int64_t)ends[p] - starts[p];
+    widths[p] = len * b;
+    if (p < P - 1 && len > 0) k = (unsigned)((kDecodeTile + len - 1) / len);
+  }
+  b = (int)__reduce_max_sync(FULL_MASK, (unsigned)b);
+  k = __reduce_max_sync(FULL_MASK, k);
+  if ((threadIdx.x & 31) == 0) {
+    if (b > 0) atomicMax(max_bits, (unsigned long long)b);
+    if (k > 0) atomicMax(per_tile, (unsigned long long)k);
+  }
 }
 
 static inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 
+// nm[p] = chunks of p when p is longer than one chunk (their maximum error takes a second pass).
+__global__ void multi_count_kernel(const int32_t* __restrict__ starts, const int32_t* __restrict__ ends,
+                                   const int64_t* __restrict__ nch, int64_t P, int64_t* __restrict__ nm) {
+  int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= P) return;
+  nm[p] = ((int64_t)ends[p] - starts[p]) > kFitChunk ? nch[p] : 0;
+}
+
 size_t fit_scratch_bytes(const int32_t*, int64_t n, int64_t P) {
   int64_t ncmax = n / kFitChunk + P + 1;
   size_t b = 0;
-  b += align_up(sizeof(int64_t) * (P + 1), 256) * 2;                  // nch, chunk_base
+  b += align_up(sizeof(int64_t) * (P + 1), 256) * 4;                  // nch, chunk_base, nm, mbase
   b += align_up(sizeof(int64_t) * (scan_num_tiles(P) + 1), 256);      // scan tiles
-  b += align_up(sizeof(int64_t) * 2, 256);                            // num chunks
+  b += align_up(sizeof(int64_t) * 2, 256) * 2;                        // chunk count, long-partition chunk count
   b += align_up(sizeof(i128) * ncmax, 256) * 2;                       // sy, sxy
   b += align_up(sizeof(int) * ncmax, 256);                            // ovf
+  b += align_up(sizeof(int32_t) * ncmax, 256) * 2;                    // owner, owner of the long-partition list
   b += align_up(sizeof(int64_t) * (P + 1), 256);                      // widths
   return b;
+}
+
+template <typename T, int PASS>
+static cudaError_t launch_fit_stream(const T* v, const FitStreamArgs& a, int num_sms, cudaStream_t s) {
+  const int smem = kFitStages * fit_stage_bytes<T>();
+  static bool attr_set = false;  // per instantiation
+  cudaError_t e;
+  if (!attr_set) {
+    if ((e = cudaFuncSetAttribute(fit_stream_kernel<T, PASS>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) !=
+        cudaSuccess)
+      return e;
+    attr_set = true;
+  }
+  int per_sm = 0;
+  if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fit_stream_kernel<T, PASS>, kFitCTA, smem)) !=
+      cudaSuccess)
+    return e;
+  if (per_sm < 1) per_sm = 1;
+  fit_stream_kernel<T, PASS><<<(unsigned)(per_sm * num_sms), kFitCTA, smem, s>>>(v, a);
+  return cudaGetLastError();
 }
 
 template <typename T>
@@ -186,24 +416,43 @@ static cudaError_t fit_typed(const T* v, glc_column* c, void* scratch, int64_t* 
   auto take = [&](size_t bytes) { void* r = sp; sp += align_up(bytes, 256); return r; };
   int64_t* nch = (int64_t*)take(sizeof(int64_t) * (P + 1));
   int64_t* base = (int64_t*)take(sizeof(int64_t) * (P + 1));
+  int64_t* nm = (int64_t*)take(sizeof(int64_t) * (P + 1));
+  int64_t* mbase = (int64_t*)take(sizeof(int64_t) * (P + 1));
   int64_t* tiles = (int64_t*)take(sizeof(int64_t) * (scan_num_tiles(P) + 1));
   int64_t* nchunks = (int64_t*)take(sizeof(int64_t) * 2);
+  int64_t* nmulti = (int64_t*)take(sizeof(int64_t) * 2);
   i128* sy = (i128*)take(sizeof(i128) * ncmax);
   i128* sxy = (i128*)take(sizeof(i128) * ncmax);
   int* ovf = (int*)take(sizeof(int) * ncmax);
+  int32_t* owner = (int32_t*)take(sizeof(int32_t) * ncmax);
+  int32_t* owner_m = (int32_t*)take(sizeof(int32_t) * ncmax);
   int64_t* widths = (int64_t*)take(sizeof(int64_t) * (P + 1));
   const unsigned pg = (unsigned)((P + 255) / 256);
+  const int num_sms = c->ctx->num_sms;
+  cudaError_t e;
+  // stats: [0] total bits, [1] max bits, [2] device status of the fit passes, [3] the bound on
+  // partitions per 4096-value tile (without the last partition)
+  if ((e = cudaMemsetAsync(d_stats, 0, 4 * sizeof(int64_t), s)) != cudaSuccess) return e;
 
   chunk_count_kernel<<<pg, 256, 0, s>>>(c->d_start, c->d_end, P, nch);
-  cudaError_t e = exclusive_scan<int64_t>(nch, base, P, nchunks, tiles, s);
-  if (e != cudaSuccess) return e;
-  FitChunkArgs a{c->d_start, c->d_end, base, nchunks, P, sy, sxy, ovf};
-  fit_sums_kernel<T><<<(unsigned)ncmax, kFitThreads, 0, s>>>(v, a);
-  fit_solve_kernel<T><<<pg, 256, 0, s>>>(a, nch, c->d_types, c->d_params, c->d_err);
-  fit_maxerr_kernel<T><<<(unsigned)ncmax, kFitThreads, 0, s>>>(v, a, c->d_types, c->d_params, (long long*)c->d_err);
-  if ((e = cudaMemsetAsync(d_stats, 0, 2 * sizeof(int64_t), s)) != cudaSuccess) return e;
+  if ((e = exclusive_scan<int64_t>(nch, base, P, nchunks, tiles, s)) != cudaSuccess) return e;
+  chunk_owner_kernel<<<pg, 256, 0, s>>>(base, nch, P, owner);
+  multi_count_kernel<<<pg, 256, 0, s>>>(c->d_start, c->d_end, nch, P, nm);
+  if ((e = exclusive_scan<int64_t>(nm, mbase, P, nmulti, tiles, s)) != cudaSuccess) return e;
+  chunk_owner_kernel<<<pg, 256, 0, s>>>(mbase, nm, P, owner_m);
+
+  FitStreamArgs a{c->d_start, c->d_end, nchunks, owner, base, P, sy, sxy, ovf, base,
+                  c->d_types, c->d_params, c->d_err, (unsigned long long*)(d_stats + 2)};
+  if ((e = launch_fit_stream<T, 0>(v, a, num_sms, s)) != cudaSuccess) return e;
+  FitChunkArgs fa{c->d_start, c->d_end, base, nchunks, owner, P, sy, sxy, ovf};
+  fit_solve_kernel<T><<<pg, 256, 0, s>>>(fa, nch, c->d_types, c->d_params, c->d_err);
+  FitStreamArgs am = a;
+  am.count = nmulti;
+  am.owner = owner_m;
+  am.base = mbase;
+  if ((e = launch_fit_stream<T, 1>(v, am, num_sms, s)) != cudaSuccess) return e;
   fit_bits_kernel<T><<<pg, 256, 0, s>>>(c->d_start, c->d_end, c->d_types, c->d_err, c->d_bits, widths, P,
-                                         (unsigned long long*)(d_stats + 1));
+                                         (unsigned long long*)(d_stats + 1), (unsigned long long*)(d_stats + 3));
   // bit offsets = exclusive scan of len*bits; stats[0] = total bits
   e = exclusive_scan<int64_t>(widths, c->d_offs, P, d_stats, tiles, s);
   if (e != cudaSuccess) return e;

@@ -80,6 +80,7 @@ struct glc_ctx {
 struct glc_column {
   glc_ctx* ctx = nullptr;
   cudaMemPool_t pool = nullptr;  // arrays from this stream-ordered pool (else cudaMalloc)
+  bool sync_free = false;    // glc_column_free synchronises the device first (as cudaFree would)
   bool view = false;         // arrays are slices of a batch's storage (freed with the batch)
   glc_dtype dtype = GLC_I32;
   int64_t n = 0;
@@ -151,8 +152,11 @@ struct PackArgs {
 int64_t pack_tiles(int64_t nwords_alloc);
 cudaError_t launch_batch_pack(const PackArgs* cols, const void* const* values, const int32_t* dtypes,
                               const int64_t* tile_base, int ncols, int64_t total_tiles, cudaStream_t s);
-// pack.cu
-cudaError_t launch_pack(glc_dtype dt, const void* values, glc_column* c, cudaStream_t s);
+// pack.cu: packs c's values; the column's descriptor and tile tables must be built.
+// parts_per_tile bounds the partitions a 4096-value tile spans (the fit's stats[3]); a device
+// wait that gives up is reported in *status (the context's error word, read by glc_sync).
+cudaError_t launch_pack(glc_dtype dt, const void* values, glc_column* c, int64_t parts_per_tile, int* status,
+                        cudaStream_t s);
 // decode.cu: values (or residuals when residual_out) of positions [lo, hi) to out_base[lo..hi)
 cudaError_t launch_decode(glc_ctx* ctx, const glc_column* c, int plain_src, int residual_out, int64_t lo,
                           int64_t hi, void* out_base, cudaStream_t s);

@@ -80,64 +80,89 @@ __global__ void __launch_bounds__(kRAThreads, MINB) random_access_kernel(RAArgs 
   }
   T* out = reinterpret_cast<T*>(a.out);
   const int64_t chunk = (int64_t)kRAThreads * kRAQueries;
-  for (int64_t base = (int64_t)blockIdx.x * chunk; base < a.q; base += (int64_t)gridDim.x * chunk) {
-    int64_t qi[kRAQueries], pos[kRAQueries], p[kRAQueries];
-    bool valid[kRAQueries];
+  const int64_t stride = (int64_t)gridDim.x * chunk;
+  // The positions of the next chunk are loaded while this chunk's lookups are in flight, so the
+  // streaming read of the positions overlaps the random reads instead of preceding them.
+  int32_t next_pos[kRAQueries];
+#pragma unroll
+  for (int k = 0; k < kRAQueries; k++) {
+    const int64_t qn = (int64_t)blockIdx.x * chunk + (int64_t)k * kRAThreads + threadIdx.x;
+    next_pos[k] = (qn < a.q) ? __ldcs(a.pos + qn) : -1;
+  }
+  const int32_t last_p = (int32_t)(a.P - 1);
+  for (int64_t base = (int64_t)blockIdx.x * chunk; base < a.q; base += stride) {
+    // 32-bit positions and partition numbers (positions are int32 by the API), one bit of
+    // `valid` per lookup: fewer registers per lookup, more lookups resident per SM.
+    int32_t pos[kRAQueries], p[kRAQueries];
+    uint32_t valid = 0;
 #pragma unroll
     for (int k = 0; k < kRAQueries; k++) {
-      qi[k] = base + (int64_t)k * kRAThreads + threadIdx.x;
-      pos[k] = (qi[k] < a.q) ? (int64_t)__ldcs(a.pos + qi[k]) : -1;
-      valid[k] = pos[k] >= 0 && pos[k] < a.n;
-      if (!valid[k]) pos[k] = 0;
+      const int64_t qi = base + (int64_t)k * kRAThreads + threadIdx.x;
+      pos[k] = next_pos[k];
+      if (qi < a.q && pos[k] >= 0 && pos[k] < a.n) valid |= 1u << k; else pos[k] = 0;
+    }
+#pragma unroll
+    for (int k = 0; k < kRAQueries; k++) {
+      const int64_t qn = base + stride + (int64_t)k * kRAThreads + threadIdx.x;
+      next_pos[k] = (qn < a.q) ? __ldcs(a.pos + qn) : -1;
+    }
+    long long r[kRAQueries];
+    if (PLAIN) {  // the residual depends on the position only: issue it before the descriptor
+#pragma unroll
+      for (int k = 0; k < kRAQueries; k++) r[k] = __ldg(a.plain + pos[k]);
     }
 #pragma unroll
     for (int k = 0; k < kRAQueries; k++) {
       if (MODE == 0) {
         p[k] = pos[k] >> a.fixed_shift;
-        p[k] = p[k] < a.P ? p[k] : a.P - 1;
+        p[k] = p[k] < last_p ? p[k] : last_p;
       } else if (MODE == 1) {
         p[k] = pos[k] / a.fixed_len;
-        p[k] = p[k] < a.P ? p[k] : a.P - 1;
+        p[k] = p[k] < last_p ? p[k] : last_p;
       } else {
         int lo = 0, hi = a.nsample - 1;
         while (lo < hi) {
-          int mid = (lo + hi + 1) >> 1;
-          if ((int64_t)s_sample[mid] <= pos[k]) lo = mid; else hi = mid - 1;
+          const int mid = (lo + hi + 1) >> 1;
+          if (s_sample[mid] <= pos[k]) lo = mid; else hi = mid - 1;
         }
-        int64_t plo = (int64_t)lo * a.sample_stride;
-        int64_t phi = plo + a.sample_stride - 1;
-        if (phi > a.P - 1) phi = a.P - 1;
+        int32_t plo = lo * a.sample_stride;
+        int32_t phi = plo + a.sample_stride - 1;
+        if (phi > last_p) phi = last_p;
         while (plo < phi) {
-          int64_t mid = (plo + phi + 1) >> 1;
-          if ((int64_t)__ldg(a.starts + mid) <= pos[k]) plo = mid; else phi = mid - 1;
+          const int32_t mid = (plo + phi + 1) >> 1;
+          if (__ldg(a.starts + mid) <= pos[k]) plo = mid; else phi = mid - 1;
         }
         p[k] = plo;
       }
     }
-    PartDesc d[kRAQueries];
+    double2 th[kRAQueries];  // theta0, theta1
+    int2 sb[kRAQueries];     // start, bits | type << 8
+    if (PLAIN) {  // the bit offset is not needed: read the 24 bytes that are
 #pragma unroll
-    for (int k = 0; k < kRAQueries; k++) d[k] = load_desc(a.desc + p[k]);
-    long long r[kRAQueries];
+      for (int k = 0; k < kRAQueries; k++) {
+        th[k] = __ldg(reinterpret_cast<const double2*>(a.desc + p[k]));
+        sb[k] = __ldg(reinterpret_cast<const int2*>(a.desc + p[k]) + 3);
+      }
+    } else {
 #pragma unroll
-    for (int k = 0; k < kRAQueries; k++) {
-      const int64_t local = pos[k] - d[k].start;
-      const int bits = d[k].bits_type & 0xff;
-      const int type = d[k].bits_type >> 8;
-      if (PLAIN) {
-        r[k] = __ldg(a.plain + pos[k]);
-      } else {
-        const uint64_t f = bits > 0 ? read_field_global(a.words, d[k].bit_off + local * bits, bits) : 0ull;
-        r[k] = (type == MODEL_DIRECT_COPY) ? (long long)f : sign_extend(f, bits);
+      for (int k = 0; k < kRAQueries; k++) {
+        const PartDesc d = load_desc(a.desc + p[k]);
+        th[k] = make_double2(d.theta0, d.theta1);
+        sb[k] = make_int2(d.start, d.bits_type);
+        const int bits = d.bits_type & 0xff;
+        const int64_t local = pos[k] - d.start;
+        const uint64_t f = bits > 0 ? read_field_global(a.words, d.bit_off + local * bits, bits) : 0ull;
+        r[k] = ((d.bits_type >> 8) == MODEL_DIRECT_COPY) ? (long long)f : sign_extend(f, bits);
       }
     }
 #pragma unroll
     for (int k = 0; k < kRAQueries; k++) {
-      if (qi[k] >= a.q) continue;
-      const int type = d[k].bits_type >> 8;
+      const int64_t qi = base + (int64_t)k * kRAThreads + threadIdx.x;
+      if (qi >= a.q) continue;
       T v;
-      if (type == MODEL_DIRECT_COPY) v = (T)r[k];
-      else v = apply_delta<T>(predict<T>(d[k].theta0, d[k].theta1, pos[k] - d[k].start), r[k]);
-      __stcs(out + qi[k], valid[k] ? v : (T)0);
+      if ((sb[k].y >> 8) == MODEL_DIRECT_COPY) v = (T)r[k];
+      else v = apply_delta<T>(predict<T>(th[k].x, th[k].y, (int64_t)(pos[k] - sb[k].x)), r[k]);
+      __stcs(out + qi, ((valid >> k) & 1u) ? v : (T)0);
     }
   }
 }
