@@ -338,6 +338,107 @@ def run_random_access(args):
     return 0
 
 
+COMPRESS_LAUNCHES = {"fixed": 22, "v6": 29}  # kernels per compress call (ncu launch list of one call)
+
+
+def run_compress(args):
+    """Compress: the 200M piecewise uint64 column of the decode workload, from device memory, with
+    fixed partitions of 4096 (--partitioning fixed), the reference's GPU partitioner (v6) or the
+    split/merge partitioner (variable).  One step = one glc_compress call (partition, fit, offsets,
+    pack) timed alone with CUDA events; the column is freed between steps outside the timed region.
+    value = input GB/s.  Roofline bytes: the input read once + the compressed bytes written."""
+    import torch
+
+    import glc
+
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.Stream(dev)
+    torch.cuda.set_stream(stream)
+    sh = stream.cuda_stream
+    ctx = tuned_context(glc, local)
+    n = args.n
+    values = make_values(n, 0)
+    d_in = torch.from_numpy(values.view(np.int64)).to(dev)
+    mode = {"fixed": glc.FIXED, "v6": glc.VARIABLE_V6, "variable": glc.VARIABLE}[args.partitioning]
+
+    def step():
+        return glc.compress_device(ctx, glc.U64, d_in.data_ptr(), n, mode, fixed_len=4096, stream=sh)
+
+    for _ in range(args.warmup):
+        step().free()
+    torch.cuda.synchronize(dev)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    clocks = ClockSampler(dev)
+    clocks.start()
+    times = []
+    col = None
+    for _ in range(args.steps):
+        if col is not None:
+            col.free()
+        e0.record(stream)
+        col = step()
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        times.append(e0.elapsed_time(e1))
+    clk = clocks.stop()
+    ms = sum(times) / len(times)
+    info = col.info()
+    comp = info.compressed_size_bytes
+    out = torch.empty(n, dtype=torch.int64, device=dev)
+    glc.decompress_into(ctx, col, out.data_ptr(), glc.SRC_PACKED, stream=sh)
+    torch.cuda.synchronize(dev)
+    ok = bool(torch.equal(out, d_in))
+    del out
+    col.free()
+    in_bytes = 8 * n
+    peak, peak_kind = measured_peak()
+    achieved = (in_bytes + comp) / (ms / 1e3) / 1e9
+    # end to end: pinned host values in (uploaded inside the call), the compressed size read back
+    h_in = torch.from_numpy(values.view(np.int64)).pin_memory()
+    e2e = []
+    for k in range(args.e2e_steps + 1):
+        e0.record(stream)
+        c = glc.compress_device(ctx, glc.U64, h_in.data_ptr(), n, mode, fixed_len=4096, stream=sh, host=True)
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        if k:
+            e2e.append(e0.elapsed_time(e1))
+        c.free()
+    e2e_ms = sum(e2e) / len(e2e)
+    cpu = None
+    if not args.no_cpu_baseline and args.partitioning == "fixed":
+        import oracle
+        sample = np.ascontiguousarray(values[:4_000_000])
+        t0 = time.perf_counter()
+        oc = oracle.compress(sample, "fixed", 4096)
+        secs = time.perf_counter() - t0
+        cpu = {"value": round(8 * len(sample) / secs / 1e9, 3), "unit": "GB/s", "cores": 1, "kind": "port",
+               "sample": f"{len(sample):,} values through the oracle's compress (fixed 4096); "
+                         f"size {oc.reported_size()} B"}
+    line = {
+        "metric": "compress GB/s (input)", "value": round(in_bytes / (ms / 1e3) / 1e9, 2), "unit": "GB/s",
+        "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 4),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "uint64", "data": "synthetic",
+        "config": {"workload": f"piecewise_u64_{n // 1_000_000}M_compress_{args.partitioning}", "values": n,
+                   "partitions": info.num_partitions, "compressed_bytes": comp,
+                   "compression_ratio": round(in_bytes / comp, 3), "best_ms": round(min(times), 4),
+                   "round_trip_exact": ok, "l2": "input larger than L2 (no flush)"},
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                     "frac": round(achieved / peak, 4), "peak_kind": peak_kind, "traffic": None,
+                     "algorithmic_bytes": in_bytes + comp},
+        "e2e": {"value": round(in_bytes / (e2e_ms / 1e3) / 1e9, 2), "unit": "GB/s", "h2d_bytes_per_step": in_bytes,
+                "d2h_bytes_per_step": 8},
+        "gpu_launches": COMPRESS_LAUNCHES[args.partitioning] * args.steps if args.partitioning in COMPRESS_LAUNCHES else None,
+        "clocks": clk, "cpu_baseline": cpu,
+    }
+    print(json.dumps(line), flush=True)
+    ctx.close()
+    return 0
+
+
 def batch_columns(ncols: int, total_bytes: float, seed: int = 42):
     """Column specs of the batched workload: log-normal lengths (median 256K before scaling,
     sigma 1.0, clipped to [1K, 16M]) scaled so the raw total is about total_bytes; dtype uniform
@@ -858,10 +959,12 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--columns", type=int, default=4096, help="c4 batch: number of columns")
     ap.add_argument("--workload", default="c2_decode",
-                    choices=["c2_decode", "c3_random_access", "c4_batch", "c5_serving"],
+                    choices=["c2_decode", "c3_random_access", "c4_batch", "c5_serving", "compress"],
                     help="c2_decode (headline): full decode of the 200M piecewise uint64 column; "
                          "c3_random_access: 100M lookups into a 64M int64 timestamp column")
     ap.add_argument("--mode", default="packed", choices=["packed", "preunpacked"], help="c3 residual source")
+    ap.add_argument("--partitioning", default="fixed", choices=["fixed", "v6", "variable"],
+                    help="compress: fixed partitions of 4096, the reference's GPU partitioner, or split/merge")
     ap.add_argument("--queries", type=int, default=100_000_000, help="c3 lookups per step")
     ap.add_argument("--rates", default="10000,30000,100000,300000,1000000", help="c5: request rates (req/s)")
     ap.add_argument("--ra-rates", default="1000000,2000000,4000000,8000000", help="c5: lookup-only request rates")
@@ -881,6 +984,8 @@ def main():
         return run_batch(args)
     if args.workload == "c5_serving":
         return run_serving(args)
+    if args.workload == "compress":
+        return run_compress(args)
 
     import torch
     import torch.distributed as dist
