@@ -580,8 +580,8 @@ glc_status glc_batch_compress(glc_ctx* ctx, const glc_dtype* dtypes, const void*
       (e = cudaStreamSynchronize(s)) != cudaSuccess)
     return bail(bcuda(ctx, e, "batch compress: column sizes"));
 
-  // ---- column views, words, packing and tables ----
-  std::vector<int64_t> word_base(nc + 1, 0), tile_base(nc + 1, 0), entry_base(nc + 1, 0);
+  // ---- column views, words, tables and packing ----
+  std::vector<int64_t> word_base(nc + 1, 0), entry_base(nc + 1, 0);
   std::vector<glc_column*> cols(nc, nullptr);
   for (int i = 0; i < nc; i++) {
     glc_column* c = new (std::nothrow) glc_column();
@@ -601,23 +601,16 @@ glc_status glc_batch_compress(glc_ctx* ctx, const glc_dtype* dtypes, const void*
     c->ntiles = (c->n + kDecodeTile - 1) / kDecodeTile;
     c->reported_size = c->n ? 64 * c->P + 120 + (c->total_bits + 7) / 8 : 0;
     word_base[i + 1] = word_base[i] + c->nwords_alloc;
-    tile_base[i + 1] = tile_base[i] + pack_tiles(c->nwords_alloc);
     entry_base[i + 1] = entry_base[i] + (c->n ? c->ntiles + 1 : 0);
   }
   uint32_t* words;
   TileInfo* tiles;
-  PackArgs* d_pack;
   TileCol* d_tc;
-  int64_t *d_tb, *d_eb;
-  const void** d_vals;
-  int32_t* d_dt;
-  if ((e = dalloc(b, &words, word_base[nc])) || (e = dalloc(b, &tiles, entry_base[nc])) || (e = dalloc(b, &d_pack, nc)) ||
-      (e = dalloc(b, &d_tc, nc)) || (e = dalloc(b, &d_tb, nc + 1)) || (e = dalloc(b, &d_eb, nc + 1)) ||
-      (e = dalloc(b, &d_vals, nc)) || (e = dalloc(b, &d_dt, nc)))
+  int64_t* d_eb;
+  if ((e = dalloc(b, &words, word_base[nc])) || (e = dalloc(b, &tiles, entry_base[nc])) || (e = dalloc(b, &d_tc, nc)) ||
+      (e = dalloc(b, &d_eb, nc + 1)))
     return bail(bcuda(ctx, e, "batch compress: allocation"));
-  std::vector<PackArgs> hp(nc);
   std::vector<TileCol> htc(nc);
-  std::vector<int32_t> hdt(nc);
   for (int i = 0; i < nc; i++) {
     glc_column* c = cols[i];
     const int64_t p0 = pb[i];
@@ -631,23 +624,55 @@ glc_status glc_batch_compress(glc_ctx* ctx, const glc_dtype* dtypes, const void*
     c->d_desc = desc + p0;
     c->d_words = words + word_base[i];
     c->d_tiles = tiles + entry_base[i];
-    hp[i] = PackArgs{c->d_start, c->d_end, c->d_types, c->d_params, c->d_bits, c->d_offs, c->P, c->d_words,
-                     c->nwords_alloc};
     htc[i] = TileCol{c->d_start, c->d_bits, c->d_offs, c->d_tiles, c->P, c->n, c->ntiles, c->total_bits};
-    hdt[i] = dtypes[i];
   }
-  if ((e = cudaMemcpyAsync(d_pack, hp.data(), sizeof(PackArgs) * nc, cudaMemcpyHostToDevice, s)) ||
-      (e = cudaMemcpyAsync(d_tc, htc.data(), sizeof(TileCol) * nc, cudaMemcpyHostToDevice, s)) ||
-      (e = cudaMemcpyAsync(d_tb, tile_base.data(), sizeof(int64_t) * (nc + 1), cudaMemcpyHostToDevice, s)) ||
+  // Work items of the value-tile pack, grouped by element type: one launch per type, each with its
+  // own columns, item bases (first tile of each column) and item -> column table.
+  struct PackGroup {
+    glc_dtype dt;
+    int64_t c0, ncols, ib0, own0, nitems;
+  };
+  std::vector<PackTileCol> hptc;
+  std::vector<int64_t> hib;
+  std::vector<PackGroup> groups;
+  int64_t total_items = 0;
+  for (glc_dtype dt : {GLC_I32, GLC_I64, GLC_U64, GLC_U32}) {
+    PackGroup g{dt, (int64_t)hptc.size(), 0, (int64_t)hib.size(), total_items, 0};
+    hib.push_back(0);
+    for (int i = 0; i < nc; i++) {
+      glc_column* c = cols[i];
+      if (dtypes[i] != dt || c->n == 0) continue;
+      hptc.push_back(PackTileCol{values[i], c->d_desc, c->d_tiles, c->n, c->ntiles, c->d_words});
+      g.nitems += c->ntiles;
+      hib.push_back(g.nitems);
+    }
+    g.ncols = (int64_t)hptc.size() - g.c0;
+    total_items += g.nitems;
+    groups.push_back(g);
+  }
+  PackTileCol* d_ptc;
+  int64_t* d_ib;
+  int32_t* d_owner;
+  if ((e = dalloc(b, &d_ptc, hptc.size() + 1)) || (e = dalloc(b, &d_ib, hib.size())) ||
+      (e = dalloc(b, &d_owner, total_items + 1)))
+    return bail(bcuda(ctx, e, "batch compress: allocation"));
+  if ((e = cudaMemcpyAsync(d_tc, htc.data(), sizeof(TileCol) * nc, cudaMemcpyHostToDevice, s)) ||
       (e = cudaMemcpyAsync(d_eb, entry_base.data(), sizeof(int64_t) * (nc + 1), cudaMemcpyHostToDevice, s)) ||
-      (e = cudaMemcpyAsync(d_vals, values, sizeof(void*) * nc, cudaMemcpyHostToDevice, s)) ||
-      (e = cudaMemcpyAsync(d_dt, hdt.data(), sizeof(int32_t) * nc, cudaMemcpyHostToDevice, s)))
+      (e = cudaMemcpyAsync(d_ptc, hptc.data(), sizeof(PackTileCol) * hptc.size(), cudaMemcpyHostToDevice, s)) ||
+      (e = cudaMemcpyAsync(d_ib, hib.data(), sizeof(int64_t) * hib.size(), cudaMemcpyHostToDevice, s)) ||
+      (e = cudaMemsetAsync(words, 0, sizeof(uint32_t) * word_base[nc], s)))
     return bail(bcuda(ctx, e, "batch compress: tables"));
-  if ((e = launch_batch_pack(d_pack, d_vals, d_dt, d_tb, nc, tile_base[nc], s)) != cudaSuccess)
-    return bail(bcuda(ctx, e, "batch compress: pack"));
+  // descriptor and tile tables first: the packer reads them
   if (P > 0) batch_desc_kernel<<<(unsigned)((P + 255) / 256), 256, 0, s>>>(starts, types, params, bits, offs, P, desc);
   if (entry_base[nc] > 0)
     batch_tiles_kernel<<<(unsigned)((entry_base[nc] + 255) / 256), 256, 0, s>>>(d_tc, d_eb, nc, entry_base[nc]);
+  for (const PackGroup& g : groups) {
+    if (g.nitems == 0) continue;
+    if ((e = launch_pack_item_owner(d_ib + g.ib0, (int)g.ncols, d_owner + g.own0, s)) != cudaSuccess ||
+        (e = launch_batch_pack_tiles(g.dt, d_ptc + g.c0, d_owner + g.own0, d_ib + g.ib0, g.nitems,
+                                     ctx->d_flags + kFlagError, ctx->num_sms, s)) != cudaSuccess)
+      return bail(bcuda(ctx, e, "batch compress: pack"));
+  }
   if ((e = cudaGetLastError()) != cudaSuccess || (e = cudaStreamSynchronize(s)) != cudaSuccess)
     return bail(bcuda(ctx, e, "batch compress"));
   int64_t total = 0;

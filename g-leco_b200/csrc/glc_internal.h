@@ -149,9 +149,18 @@ struct PackArgs {
   uint32_t* words;
   int64_t nwords_alloc;
 };
-int64_t pack_tiles(int64_t nwords_alloc);
-cudaError_t launch_batch_pack(const PackArgs* cols, const void* const* values, const int32_t* dtypes,
-                              const int64_t* tile_base, int ncols, int64_t total_tiles, cudaStream_t s);
+// pack.cu: one column of a value-tile pack (its decode tile table and descriptors built)
+struct PackTileCol {
+  const void* v;
+  const PartDesc* desc;
+  const TileInfo* tiles;
+  int64_t n, ntiles;
+  uint32_t* words;
+};
+constexpr int kPackTilePartsMax = 40;  // partitions a 4096-value tile may span in the value-tile pack
+cudaError_t launch_batch_pack_tiles(glc_dtype dt, const PackTileCol* cols, const int32_t* owner,
+                                    const int64_t* item_base, int64_t nitems, int* status, int num_sms, cudaStream_t s);
+cudaError_t launch_pack_item_owner(const int64_t* item_base, int ncols, int32_t* owner, cudaStream_t s);
 // pack.cu: packs c's values; the column's descriptor and tile tables must be built.
 // parts_per_tile bounds the partitions a 4096-value tile spans (the fit's stats[3]); a device
 // wait that gives up is reported in *status (the context's error word, read by glc_sync).

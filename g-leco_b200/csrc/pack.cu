@@ -140,16 +140,17 @@ template <typename T> __global__ void __launch_bounds__(kPackThreads) pack_kerne
 // pack_edge_zero_kernel cleared first (the two kinds never meet: a word wholly inside one tile's
 // range has no bits from another tile).  Needs at most kPackTileParts partitions per tile.
 // ---------------------------------------------------------------------------------------
-constexpr int kPackTileParts = 40;
+constexpr int kPackTileParts = kPackTilePartsMax;
 constexpr int kPackCompute = 256;
 constexpr int kPackCTA = kPackCompute + 32;
 constexpr int kPackStages = 2;
 
 struct PackTileArgs {
-  const PartDesc* desc;
-  const TileInfo* tiles;
-  int64_t n, ntiles;
-  uint32_t* words;
+  PackTileCol col;           // single column (BATCH = false)
+  const PackTileCol* cols;   // batch: the columns of one element type
+  const int32_t* owner;      // batch: work item -> column
+  const int64_t* item_base;  // batch: column -> its first work item (its tiles follow)
+  int64_t nitems;            // batch: work items (tiles of all the columns)
   int* status;  // DEVERR_* (the context's device error word)
 };
 
@@ -157,6 +158,7 @@ struct PackStage {
   int64_t tile;    // -1 = no more work
   int64_t e0;      // first value of the tile
   int64_t bit_lo, bit_hi;
+  uint32_t* words; // the tile's column's word array
   int32_t cnt;     // values in the tile
   int32_t head;    // byte offset of the first value in the stage
   int32_t pf, np;  // partitions of the tile
@@ -191,8 +193,8 @@ __global__ void pack_edge_zero_kernel(const TileInfo* __restrict__ tiles, int64_
   if (w < nwords_alloc) words[w] = 0u;
 }
 
-template <typename T> __global__ void __launch_bounds__(kPackCTA)
-pack_tile_kernel(const T* __restrict__ v, PackTileArgs a) {
+template <typename T, bool BATCH> __global__ void __launch_bounds__(kPackCTA)
+pack_tile_kernel(PackTileArgs a) {
   extern __shared__ __align__(128) uint8_t smem[];  // [stages][values | descriptors] (+ fields for 4-byte types)
   __shared__ __align__(8) uint64_t full[kPackStages], empty[kPackStages];
   __shared__ PackStage s_meta[kPackStages];
@@ -213,8 +215,9 @@ pack_tile_kernel(const T* __restrict__ v, PackTileArgs a) {
 
   if (threadIdx.x >= kPackCompute) {  // ---- producer ----
     if (threadIdx.x != kPackCompute) return;
-    int64_t t = blockIdx.x;
-    for (int k = 0;; k++, t += gridDim.x) {
+    const int64_t nitems = BATCH ? a.nitems : a.col.ntiles;
+    int64_t item = blockIdx.x;
+    for (int k = 0;; k++, item += gridDim.x) {
       const int st = k % kPackStages;
       if (k >= kPackStages && !mbar_wait_bounded(&empty[st], (uint32_t)((k / kPackStages) - 1) & 1u)) {
         atomicExch(a.status, DEVERR_TIMEOUT);
@@ -222,21 +225,31 @@ pack_tile_kernel(const T* __restrict__ v, PackTileArgs a) {
         mbar_arrive(&full[st]);
         return;
       }
-      if (t >= a.ntiles) {
+      if (item >= nitems) {
         s_meta[st].tile = -1;
         mbar_arrive(&full[st]);  // no copy: completes the phase, the compute warps see the end
         return;
       }
-      const TileInfo ti = a.tiles[t];
+      PackTileCol c;
+      int64_t t = item;
+      if (BATCH) {
+        const int32_t ci = a.owner[item];
+        c = a.cols[ci];
+        t = item - a.item_base[ci];
+      } else {
+        c = a.col;
+      }
+      const TileInfo ti = c.tiles[t];
       PackStage m;
       m.tile = t;
       m.e0 = t * kDecodeTile;
-      m.cnt = (int)((a.n - m.e0) < kDecodeTile ? (a.n - m.e0) : kDecodeTile);
+      m.cnt = (int)((c.n - m.e0) < kDecodeTile ? (c.n - m.e0) : kDecodeTile);
       m.bit_lo = ti.bit_lo;
-      m.bit_hi = a.tiles[t + 1].bit_lo;
+      m.bit_hi = c.tiles[t + 1].bit_lo;
+      m.words = c.words;
       m.pf = ti.p_first;
       m.np = ti.p_last - ti.p_first + 1;
-      const uintptr_t addr = reinterpret_cast<uintptr_t>(v + m.e0);
+      const uintptr_t addr = reinterpret_cast<uintptr_t>(reinterpret_cast<const T*>(c.v) + m.e0);
       m.head = (int)(addr & 15);
       s_meta[st] = m;
       const uint32_t vbytes = (uint32_t)((m.head + (int64_t)m.cnt * (int64_t)sizeof(T) + 15) & ~15ll);
@@ -245,7 +258,7 @@ pack_tile_kernel(const T* __restrict__ v, PackTileArgs a) {
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       mbar_arrive_expect_tx(&full[st], vbytes + dbytes);
       tma_bulk_load(stage, reinterpret_cast<const uint8_t*>(addr - m.head), vbytes, &full[st]);
-      if (dbytes) tma_bulk_load(stage + kDecodeTile * sizeof(T) + 32, a.desc + m.pf, dbytes, &full[st]);
+      if (dbytes) tma_bulk_load(stage + kDecodeTile * sizeof(T) + 32, c.desc + m.pf, dbytes, &full[st]);
     }
   }
 
@@ -349,8 +362,8 @@ pack_tile_kernel(const T* __restrict__ v, PackTileArgs a) {
           uint32_t word = sh >= 0 ? (f32[NS * j] << sh) : (f32[NS * j] >> -sh);
           for (fb += qb, sh += qb, j++; fb < wend; fb += qb, sh += qb, j++) word |= f32[NS * j] << sh;
           const bool partial = (w == 0 && sh0 != 0) || (w == nw - 1 && last_partial);
-          if (partial) atomicOr(a.words + W0 + w, word);
-          else a.words[W0 + w] = word;
+          if (partial) atomicOr(m.words + W0 + w, word);
+          else m.words[W0 + w] = word;
         }
       } else {
       int qi = 0;
@@ -385,8 +398,8 @@ pack_tile_kernel(const T* __restrict__ v, PackTileArgs a) {
           pos = qend;
         }
         const bool partial = (w == 0 && sh0 != 0) || (w == nw - 1 && last_partial);
-        if (partial) atomicOr(a.words + W0 + w, word);
-        else a.words[W0 + w] = word;
+        if (partial) atomicOr(m.words + W0 + w, word);
+        else m.words[W0 + w] = word;
       }
       }
     }
@@ -395,28 +408,71 @@ pack_tile_kernel(const T* __restrict__ v, PackTileArgs a) {
   }
 }
 
-template <typename T>
-static cudaError_t launch_pack_tiles(const T* v, glc_column* c, int* status, cudaStream_t s) {
+template <typename T, bool BATCH>
+static cudaError_t launch_pack_tile_kernel(const PackTileArgs& a, int64_t nitems, int num_sms, cudaStream_t s) {
   const int smem = kPackStages * pack_stage_bytes<T>() + (sizeof(T) == 4 ? kDecodeTile * 8 : 0);
   static bool attr_set = false;  // per instantiation
   cudaError_t e;
   if (!attr_set) {
-    if ((e = cudaFuncSetAttribute(pack_tile_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) != cudaSuccess)
+    if ((e = cudaFuncSetAttribute(pack_tile_kernel<T, BATCH>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) !=
+        cudaSuccess)
       return e;
     attr_set = true;
   }
   int per_sm = 0;
-  if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pack_tile_kernel<T>, kPackCTA, smem)) != cudaSuccess)
+  if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pack_tile_kernel<T, BATCH>, kPackCTA, smem)) !=
+      cudaSuccess)
     return e;
   if (per_sm < 1) per_sm = 1;
+  int64_t grid = (int64_t)per_sm * num_sms;
+  if (grid > nitems) grid = nitems;
+  if (grid < 1) grid = 1;
+  pack_tile_kernel<T, BATCH><<<(unsigned)grid, kPackCTA, smem, s>>>(a);
+  return cudaGetLastError();
+}
+
+template <typename T>
+static cudaError_t launch_pack_tiles(const T* v, glc_column* c, int* status, cudaStream_t s) {
   const int64_t zthreads = (c->ntiles + 1) > (c->nwords_alloc - c->nwords) ? c->ntiles + 1 : c->nwords_alloc - c->nwords;
   pack_edge_zero_kernel<<<(unsigned)((zthreads + 255) / 256), 256, 0, s>>>(c->d_tiles, c->ntiles, c->nwords,
                                                                           c->nwords_alloc, c->d_words);
-  PackTileArgs a{c->d_desc, c->d_tiles, c->n, c->ntiles, c->d_words, status};
-  int64_t grid = (int64_t)per_sm * c->ctx->num_sms;
-  if (grid > c->ntiles) grid = c->ntiles;
-  if (grid < 1) grid = 1;
-  pack_tile_kernel<T><<<(unsigned)grid, kPackCTA, smem, s>>>(v, a);
+  PackTileArgs a{};
+  a.col = PackTileCol{v, c->d_desc, c->d_tiles, c->n, c->ntiles, c->d_words};
+  a.status = status;
+  return launch_pack_tile_kernel<T, false>(a, c->ntiles, c->ctx->num_sms, s);
+}
+
+// Batched value-tile pack over the columns of one element type: cols[i] (device), item_base[i] =
+// its first work item, owner[item] = its column, nitems = all their tiles.  The word arrays must be
+// zero (interior words are stored, the edge words merged with atomicOr).
+cudaError_t launch_batch_pack_tiles(glc_dtype dt, const PackTileCol* cols, const int32_t* owner,
+                                    const int64_t* item_base, int64_t nitems, int* status, int num_sms, cudaStream_t s) {
+  if (nitems <= 0) return cudaSuccess;
+  PackTileArgs a{};
+  a.cols = cols;
+  a.owner = owner;
+  a.item_base = item_base;
+  a.nitems = nitems;
+  a.status = status;
+  switch (dt) {
+    case GLC_I32: return launch_pack_tile_kernel<int32_t, true>(a, nitems, num_sms, s);
+    case GLC_I64: return launch_pack_tile_kernel<int64_t, true>(a, nitems, num_sms, s);
+    case GLC_U64: return launch_pack_tile_kernel<uint64_t, true>(a, nitems, num_sms, s);
+    case GLC_U32: return launch_pack_tile_kernel<uint32_t, true>(a, nitems, num_sms, s);
+  }
+  return cudaErrorInvalidValue;
+}
+
+// owner[item] = i for the items of column i (one thread per column).
+__global__ void pack_item_owner_kernel(const int64_t* __restrict__ item_base, int ncols, int32_t* __restrict__ owner) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= ncols) return;
+  for (int64_t k = item_base[i]; k < item_base[i + 1]; k++) owner[k] = i;
+}
+
+cudaError_t launch_pack_item_owner(const int64_t* item_base, int ncols, int32_t* owner, cudaStream_t s) {
+  if (ncols <= 0) return cudaSuccess;
+  pack_item_owner_kernel<<<(unsigned)((ncols + 255) / 256), 256, 0, s>>>(item_base, ncols, owner);
   return cudaGetLastError();
 }
 
@@ -441,36 +497,6 @@ cudaError_t launch_pack(glc_dtype dt, const void* values, glc_column* c, int64_t
     case GLC_U64: pack_kernel<uint64_t><<<grid, kPackThreads, 0, s>>>((const uint64_t*)values, a); break;
     case GLC_U32: pack_kernel<uint32_t><<<grid, kPackThreads, 0, s>>>((const uint32_t*)values, a); break;
   }
-  return cudaGetLastError();
-}
-
-// Batched pack: one CTA per output word tile of any column of a batch (PackArgs per column).
-__global__ void __launch_bounds__(kPackThreads)
-batch_pack_kernel(const PackArgs* __restrict__ cols, const void* const* __restrict__ values,
-                  const int32_t* __restrict__ dtypes, const int64_t* __restrict__ tile_base, int ncols) {
-  const int64_t t = blockIdx.x;
-  int lo = 0, hi = ncols - 1;
-  while (lo < hi) {
-    const int mid = (lo + hi + 1) >> 1;
-    if (tile_base[mid] <= t) lo = mid; else hi = mid - 1;
-  }
-  const PackArgs a = cols[lo];
-  const int64_t tile = t - tile_base[lo];
-  __shared__ __align__(16) PackSmem sm;
-  switch (dtypes[lo]) {
-    case GLC_I32: pack_word_tile<int32_t>((const int32_t*)values[lo], a, tile, sm); break;
-    case GLC_I64: pack_word_tile<int64_t>((const int64_t*)values[lo], a, tile, sm); break;
-    case GLC_U64: pack_word_tile<uint64_t>((const uint64_t*)values[lo], a, tile, sm); break;
-    default: pack_word_tile<uint32_t>((const uint32_t*)values[lo], a, tile, sm); break;
-  }
-}
-
-int64_t pack_tiles(int64_t nwords_alloc) { return (nwords_alloc + kPackWords - 1) / kPackWords; }
-
-cudaError_t launch_batch_pack(const PackArgs* cols, const void* const* values, const int32_t* dtypes,
-                              const int64_t* tile_base, int ncols, int64_t total_tiles, cudaStream_t s) {
-  if (total_tiles <= 0) return cudaSuccess;
-  batch_pack_kernel<<<(unsigned)total_tiles, kPackThreads, 0, s>>>(cols, values, dtypes, tile_base, ncols);
   return cudaGetLastError();
 }
 
