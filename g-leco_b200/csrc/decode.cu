@@ -104,7 +104,10 @@ template <typename T, bool PLAIN, bool RESID, int kUnroll = 2>
 __device__ __forceinline__ void decode_tile(const DecodeArgs& a, const StageInfo& si, const uint8_t* stage,
                                             const PartDesc* sdesc) {
   typedef typename std::conditional<RESID, int64_t, T>::type OutT;
-  constexpr int V = 16 / (int)sizeof(OutT);
+  // values per thread-vector: 32 bytes for 4-byte outputs (two 16-byte stores; the per-vector
+  // cursor and address work is then shared by 8 values), 16 bytes for 8-byte outputs
+  constexpr int kVecBytes = sizeof(OutT) == 4 ? 32 : 16;
+  constexpr int V = kVecBytes / (int)sizeof(OutT);
   OutT* out = reinterpret_cast<OutT*>(a.out_base);
   const int tid = threadIdx.x;
   const int64_t tile_e0 = si.tile * kDecodeTile;
@@ -205,9 +208,12 @@ __device__ __forceinline__ void decode_tile(const DecodeArgs& a, const StageInfo
 #pragma unroll
       for (int u = 0; u < V; u++) vals[u] = one(e + u);
     }
-    uint4 pk;
-    memcpy(&pk, vals, 16);
-    *reinterpret_cast<uint4*>(out + e) = pk;
+#pragma unroll
+    for (int h = 0; h < kVecBytes / 16; h++) {
+      uint4 pk;
+      memcpy(&pk, reinterpret_cast<const uint8_t*>(vals) + 16 * h, 16);
+      *reinterpret_cast<uint4*>(reinterpret_cast<uint8_t*>(out + e) + 16 * h) = pk;
+    }
   };
   auto general_vec = [&](int e) {  // partition boundary inside the vector, or a partial tile
 #pragma unroll
@@ -335,7 +341,7 @@ __global__ void __launch_bounds__(kPCThreads) decode_kernel(DecodeArgs a) {
 template <typename T, int kStages>
 __device__ __forceinline__ void batch_body(const BatchDecodeArgs& b, int g, uint8_t* smem,
                                            PartDesc (*s_desc)[kTileDescs], uint64_t* full, uint64_t* empty,
-                                           StageInfo* s_info, int64_t* s_item) {
+                                           StageInfo* s_info, BatchWork* s_work, BatchColumn* s_col) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int64_t first = b.group_begin[g], last = b.group_begin[g + 1];
   if (warp == kConsumerWarps) {  // ---- producer ----
@@ -347,7 +353,6 @@ __device__ __forceinline__ void batch_body(const BatchDecodeArgs& b, int g, uint
         break;
       }
       const int64_t item = first + (int64_t)atomicAdd(b.counter + g, 1ull);
-      s_item[s] = item;
       StageInfo si;
       if (item >= last) {
         si.tile = -1;
@@ -357,6 +362,8 @@ __device__ __forceinline__ void batch_body(const BatchDecodeArgs& b, int g, uint
       }
       const BatchWork w = b.work[item];
       const BatchColumn col = b.cols[w.col];
+      s_work[s] = w;  // the consumers read the item and its column from the stage, not from global memory
+      s_col[s] = col;
       const TileInfo ti = col.tiles[w.tile];
       const int64_t bh = col.tiles[w.tile + 1].bit_lo;
       si.tile = w.tile;
@@ -388,8 +395,8 @@ __device__ __forceinline__ void batch_body(const BatchDecodeArgs& b, int g, uint
     }
     const StageInfo si = s_info[s];
     if (si.tile < 0) break;
-    const BatchWork w = b.work[s_item[s]];
-    const BatchColumn col = b.cols[w.col];
+    const BatchWork w = s_work[s];
+    const BatchColumn col = s_col[s];
     DecodeArgs a;
     a.desc = col.desc;
     a.starts = col.starts;
@@ -414,7 +421,8 @@ __global__ void __launch_bounds__(kPCThreads) batch_decode_kernel(BatchDecodeArg
   __shared__ __align__(128) PartDesc s_desc[kStages][kTileDescs];
   __shared__ __align__(8) uint64_t full[kStages], empty[kStages];
   __shared__ StageInfo s_info[kStages];
-  __shared__ int64_t s_item[kStages];
+  __shared__ BatchWork s_work[kStages];
+  __shared__ BatchColumn s_col[kStages];
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < kStages; s++) {
@@ -427,10 +435,10 @@ __global__ void __launch_bounds__(kPCThreads) batch_decode_kernel(BatchDecodeArg
   int g = 0;
   while (g < 3 && (int)blockIdx.x >= b.grid_begin[g + 1]) g++;
   switch (g) {  // the group's element type: GLC_I32, GLC_I64, GLC_U64, GLC_U32
-    case 0: batch_body<int32_t, kStages>(b, g, smem, s_desc, full, empty, s_info, s_item); break;
-    case 1: batch_body<int64_t, kStages>(b, g, smem, s_desc, full, empty, s_info, s_item); break;
-    case 2: batch_body<uint64_t, kStages>(b, g, smem, s_desc, full, empty, s_info, s_item); break;
-    default: batch_body<uint32_t, kStages>(b, g, smem, s_desc, full, empty, s_info, s_item); break;
+    case 0: batch_body<int32_t, kStages>(b, g, smem, s_desc, full, empty, s_info, s_work, s_col); break;
+    case 1: batch_body<int64_t, kStages>(b, g, smem, s_desc, full, empty, s_info, s_work, s_col); break;
+    case 2: batch_body<uint64_t, kStages>(b, g, smem, s_desc, full, empty, s_info, s_work, s_col); break;
+    default: batch_body<uint32_t, kStages>(b, g, smem, s_desc, full, empty, s_info, s_work, s_col); break;
   }
 }
 

@@ -42,6 +42,16 @@ def _data(kind: str, n: int, seed: int = 1):
         return np.full(n, 123456789, np.uint32)
     if kind == "timestamps":
         return W.timestamps(n, seed=seed)
+    if kind == "i32_extreme":  # residuals near +-2^32: 33-bit fields in a 4-byte type
+        v = rng.integers(-(2 ** 31), 2 ** 31, n, dtype=np.int64).astype(np.int32)
+        v[:: 5] = np.iinfo(np.int32).max
+        v[2:: 5] = np.iinfo(np.int32).min
+        return v
+    if kind == "u32_extreme":
+        v = rng.integers(0, 2 ** 32, n, dtype=np.int64).astype(np.uint32)
+        v[:: 3] = np.iinfo(np.uint32).max
+        v[1:: 3] = 0
+        return v
     raise ValueError(kind)
 
 
@@ -128,6 +138,36 @@ def test_fixed_length_mismatch_is_an_error():
     col, _ = codec.compress(v, False, fixed_partition_size=1024)
     with pytest.raises(glc.GlcError):
         codec.randomAccessFixed(col, np.arange(10, dtype=np.int32), 4096)
+
+
+@pytest.mark.parametrize("kind", ["i32_extreme", "u32_extreme", "i64_extreme"])
+@pytest.mark.parametrize("L", [100, 108, 1000, 4096])
+def test_widest_fields_each_packer(oracle, kind, L):
+    """Fields as wide as the type allows (33 bits for 4-byte types, 64 for 8-byte ones), with
+    partitions short enough for the output-word packer (100) and long enough for the value-tile
+    packer (108 and up)."""
+    v = _data(kind, 20_001, seed=L)
+    codec = _codec(v)
+    col, size = codec.compress(v, False, fixed_partition_size=L)
+    ocol = oracle.compress(v, "fixed", L)
+    assert size == ocol.reported_size()
+    _check_column(codec, col, v, ocol, oracle)
+
+
+@pytest.mark.parametrize("mode", ["fixed", "variable"])
+@pytest.mark.parametrize("skip", [1, 2, 3])
+def test_compress_from_unaligned_device_values(oracle, glc_ctx, mode, skip):
+    """Device input that starts 8, 16 or 24 bytes into a buffer (not 16-byte aligned in two cases):
+    the staged bulk copies start on the enclosing 16-byte boundary and skip the head."""
+    import torch
+    v = _data("u64_piecewise", 30_000 + skip, seed=skip)
+    d = torch.from_numpy(v.view(np.int64)).cuda()
+    sub = v[skip:]
+    col = glc.compress_device(glc_ctx, glc.U64, d.data_ptr() + 8 * skip, len(sub),
+                              glc.FIXED if mode == "fixed" else glc.VARIABLE, fixed_len=1024)
+    ocol = oracle.compress(sub, mode, 1024)
+    assert glc.serialize_host(glc_ctx, col) == oracle.serialize(ocol)
+    col.free()
 
 
 @pytest.mark.parametrize("L", [1, 3, 7, 64])
