@@ -97,7 +97,7 @@ __device__ __forceinline__ double part_cost(int64_t len, int bits) {
 // ---- split: best end of every 128-aligned start ------------------------------------------
 template <typename T> __global__ void __launch_bounds__(256)
 split_kernel(const T* __restrict__ v, RangeSums rs, int32_t* __restrict__ nb_next) {
-  __shared__ double s_th[8][kNumSizes][2];
+  __shared__ __align__(16) double s_th[8][kNumSizes][2];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int64_t j = (int64_t)blockIdx.x * 8 + warp;
   if (j >= rs.nb) return;
@@ -110,27 +110,72 @@ split_kernel(const T* __restrict__ v, RangeSums rs, int32_t* __restrict__ nb_nex
     if (lane == 0) nb_next[j] = (int32_t)rs.nb;
     return;
   }
+  // Fast path: when every value of the start's reach and every candidate's prediction (checked
+  // at both ends of the candidate: fma(theta1, o, theta0) is monotone in o) lie well inside
+  // (-2^51, 2^51) and inside T's range, the saturating conversion, the saturating or wrapping
+  // difference and abs_ref all reduce to plain arithmetic: pred = trunc(x + bias) with one
+  // conversion, delta = y - pred with one 64-bit subtraction.  Same results; any start that
+  // leaves those bounds is measured by the exact loop below.
+  constexpr double kSafe = 2251799813685248.0;  // 2^51
+  const double lo_ok = TypeTraits<T>::is_signed ? (sizeof(T) == 4 ? -2147483647.0 : -kSafe) : -0.25;
+  const double hi_ok = sizeof(T) == 4 ? (TypeTraits<T>::is_signed ? 2147483646.0 : 4294967294.0) : kSafe;
+  bool cand_ok = true;
   if (lane < ncand) {
     double t0, t1;
     rs.line(s, s + c_sizes[lane], t0, t1);
     s_th[warp][lane][0] = t0;
     s_th[warp][lane][1] = t1;
+    const double xa = t0, xb = __fma_rn(t1, (double)(c_sizes[lane] - 1), t0);
+    cand_ok = xa >= lo_ok && xa <= hi_ok && xb >= lo_ok && xb <= hi_ok;
   }
   __syncwarp();
   long long m[kNumSizes];
 #pragma unroll
   for (int k = 0; k < kNumSizes; k++) m[k] = 0;
   const int total = c_sizes[ncand - 1];
-  int band = 0;  // first candidate whose size exceeds the offset (uniform: sizes are multiples of 128)
-  for (int o0 = 0; o0 < total; o0 += 32) {
-    while (c_sizes[band] <= o0) band++;
-    const int o = o0 + lane;
-    const T y = __ldg(v + s + o);
+  bool fast = __all_sync(FULL_MASK, cand_ok);
+  if (fast) {
+    // every quantity below is an integer of magnitude < 2^53, so FP64 holds it exactly: the
+    // prediction trunc(x + bias), the residual y - pred, and the running max of |residual|
+    double md[kNumSizes];
 #pragma unroll
-    for (int k = 0; k < kNumSizes; k++) {
-      if (k < band || k >= ncand) continue;
-      const long long d = abs_ref(calc_delta<T>(y, predict<T>(s_th[warp][k][0], s_th[warp][k][1], o)));
-      m[k] = d > m[k] ? d : m[k];
+    for (int k = 0; k < kNumSizes; k++) md[k] = 0.0;
+    bool vals_ok = true;
+    int band = 0;  // first candidate whose size exceeds the offset (uniform: sizes are multiples of 128)
+    double od = (double)lane;
+    for (int o0 = 0; o0 < total; o0 += 32, od += 32.0) {
+      while (c_sizes[band] <= o0) band++;
+      const T y = __ldg(v + s + o0 + lane);
+      const long long yv = (long long)y;
+      vals_ok &= TypeTraits<T>::is_signed ? (yv > -(1ll << 51) && yv < (1ll << 51)) : ((uint64_t)y < (1ull << 51));
+      const double yd = (double)yv;  // exact when vals_ok (a start where it is not is measured again below)
+#pragma unroll
+      for (int k = 0; k < kNumSizes; k++) {
+        if (k < band || k >= ncand) continue;
+        const double2 th = *reinterpret_cast<const double2*>(&s_th[warp][k][0]);
+        const double x = __fma_rn(th.y, od, th.x);
+        const double pred = trunc(__dadd_rn(x, half_away_bias(x)));
+        md[k] = fmax(md[k], fabs(__dsub_rn(yd, pred)));
+      }
+    }
+    fast = __all_sync(FULL_MASK, vals_ok);
+    if (fast) {
+#pragma unroll
+      for (int k = 0; k < kNumSizes; k++) m[k] = (long long)md[k];
+    }
+  }
+  if (!fast) {
+    int band = 0;
+    for (int o0 = 0; o0 < total; o0 += 32) {
+      while (c_sizes[band] <= o0) band++;
+      const int o = o0 + lane;
+      const T y = __ldg(v + s + o);
+#pragma unroll
+      for (int k = 0; k < kNumSizes; k++) {
+        if (k < band || k >= ncand) continue;
+        const long long d = abs_ref(calc_delta<T>(y, predict<T>(s_th[warp][k][0], s_th[warp][k][1], o)));
+        m[k] = d > m[k] ? d : m[k];
+      }
     }
   }
   double best_cpe = 1.7976931348623157e308;
