@@ -32,6 +32,11 @@ namespace glc {
 
 constexpr int kNumSizes = 14;
 __constant__ int c_sizes[kNumSizes] = {128, 256, 384, 512, 640, 896, 1152, 1408, 1664, 1920, 2176, 2688, 3200, 3712};
+__host__ __device__ constexpr int split_size(int k) {
+  return k < 5 ? 128 * (k + 1) : k < 11 ? 640 + 256 * (k - 4) : 2176 + 512 * (k - 10);
+}
+static_assert(split_size(0) == 128 && split_size(4) == 640 && split_size(5) == 896 && split_size(10) == 2176 &&
+              split_size(11) == 2688 && split_size(13) == 3712, "candidate sizes");
 constexpr int kMaxJumpBlocks = 29;  // 3712 / 128
 constexpr int kRangeBlocks = 1024;
 constexpr int kMaxMergeRounds = 64;
@@ -95,6 +100,35 @@ __device__ __forceinline__ double part_cost(int64_t len, int bits) {
 }
 
 // ---- split: best end of every 128-aligned start ------------------------------------------
+// Offsets [size(B-1), size(B)) lie in candidates B..13 only: one loop per band with the candidate
+// range known at compile time, no per-candidate test.  Used when all 14 candidates exist and every
+// prediction is >= -0.25 (so round-half-away is trunc(x + 0.5 - 2^-54) with a constant addend)
+// and the values are below 2^51: all quantities are exact integers in FP64.
+template <int B, typename T>
+__device__ __forceinline__ void split_bands(const T* __restrict__ v, int64_t s, int lane, const double (*th)[2],
+                                            double (&md)[kNumSizes], bool& vals_ok) {
+  if constexpr (B < kNumSizes) {
+    constexpr int lo = B == 0 ? 0 : split_size(B - 1), hi = split_size(B);
+    constexpr double kBias = 0x1.fffffffffffffp-2;  // 0.5 - 2^-54
+    double od = (double)(lo + lane);
+#pragma unroll 2
+    for (int o0 = lo; o0 < hi; o0 += 32, od += 32.0) {
+      const T y = __ldg(v + s + o0 + lane);
+      vals_ok &= TypeTraits<T>::is_signed ? ((long long)y > -(1ll << 51) && (long long)y < (1ll << 51))
+                                          : ((uint64_t)y < (1ull << 51));
+      const double yd = (double)(long long)y;
+#pragma unroll
+      for (int k = B; k < kNumSizes; k++) {
+        const double2 t = *reinterpret_cast<const double2*>(th[k]);  // broadcast shared-memory load
+        const double pred = trunc(__dadd_rn(__fma_rn(t.y, od, t.x), kBias));
+        md[k] = fmax(md[k], fabs(__dsub_rn(yd, pred)));
+      }
+    }
+    split_bands<B + 1, T>(v, s, lane, th, md, vals_ok);
+  }
+}
+
+
 template <typename T> __global__ void __launch_bounds__(256)
 split_kernel(const T* __restrict__ v, RangeSums rs, int32_t* __restrict__ nb_next) {
   __shared__ __align__(16) double s_th[8][kNumSizes][2];
@@ -119,7 +153,7 @@ split_kernel(const T* __restrict__ v, RangeSums rs, int32_t* __restrict__ nb_nex
   constexpr double kSafe = 2251799813685248.0;  // 2^51
   const double lo_ok = TypeTraits<T>::is_signed ? (sizeof(T) == 4 ? -2147483647.0 : -kSafe) : -0.25;
   const double hi_ok = sizeof(T) == 4 ? (TypeTraits<T>::is_signed ? 2147483646.0 : 4294967294.0) : kSafe;
-  bool cand_ok = true;
+  bool cand_ok = true, cand_nonneg = true;
   if (lane < ncand) {
     double t0, t1;
     rs.line(s, s + c_sizes[lane], t0, t1);
@@ -127,6 +161,7 @@ split_kernel(const T* __restrict__ v, RangeSums rs, int32_t* __restrict__ nb_nex
     s_th[warp][lane][1] = t1;
     const double xa = t0, xb = __fma_rn(t1, (double)(c_sizes[lane] - 1), t0);
     cand_ok = xa >= lo_ok && xa <= hi_ok && xb >= lo_ok && xb <= hi_ok;
+    cand_nonneg = xa >= -0.25 && xb >= -0.25;
   }
   __syncwarp();
   long long m[kNumSizes];
@@ -134,7 +169,20 @@ split_kernel(const T* __restrict__ v, RangeSums rs, int32_t* __restrict__ nb_nex
   for (int k = 0; k < kNumSizes; k++) m[k] = 0;
   const int total = c_sizes[ncand - 1];
   bool fast = __all_sync(FULL_MASK, cand_ok);
-  if (fast) {
+  bool banded = false;
+  if (fast && ncand == kNumSizes && __all_sync(FULL_MASK, cand_nonneg)) {
+    double md[kNumSizes];
+#pragma unroll
+    for (int k = 0; k < kNumSizes; k++) md[k] = 0.0;
+    bool vals_ok = true;
+    split_bands<0, T>(v, s, lane, s_th[warp], md, vals_ok);
+    if (__all_sync(FULL_MASK, vals_ok)) {
+#pragma unroll
+      for (int k = 0; k < kNumSizes; k++) m[k] = (long long)md[k];
+      banded = true;
+    }
+  }
+  if (fast && !banded) {
     // every quantity below is an integer of magnitude < 2^53, so FP64 holds it exactly: the
     // prediction trunc(x + bias), the residual y - pred, and the running max of |residual|
     double md[kNumSizes];
@@ -164,7 +212,7 @@ split_kernel(const T* __restrict__ v, RangeSums rs, int32_t* __restrict__ nb_nex
       for (int k = 0; k < kNumSizes; k++) m[k] = (long long)md[k];
     }
   }
-  if (!fast) {
+  if (!fast && !banded) {
     int band = 0;
     for (int o0 = 0; o0 < total; o0 += 32) {
       while (c_sizes[band] <= o0) band++;
