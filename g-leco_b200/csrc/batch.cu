@@ -92,14 +92,14 @@ __device__ void fit_one(const T* __restrict__ v, int64_t len, int& type, double&
   __shared__ double s_t0, s_t1;
   __shared__ int s_over;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  i128 sy = 0, sxy = 0;
+  HalfSums<T> hs;  // exact 64-bit partials (len <= 8192: at most 32 values per thread)
   int ovf = 0;
   for (int64_t i = threadIdx.x; i < len; i += kFitCTA) {
     const T x = __ldg(v + i);
     ovf |= overflows_double<T>(x) ? 1 : 0;
-    sy += (i128)x;
-    sxy += (i128)i * (i128)x;
+    hs.add(x, (int)i);
   }
+  i128 sy = hs.sy(), sxy = hs.sxy();
   sy = warp_sum_i128(sy);
   sxy = warp_sum_i128(sxy);
   ovf = __any_sync(FULL_MASK, ovf);
@@ -119,7 +119,18 @@ __device__ void fit_one(const T* __restrict__ v, int64_t len, int& type, double&
   const double a0 = s_t0, a1 = s_t1;
   const bool over = s_over != 0;
   long long m = 0;
-  if (!over)
+  bool exact = !over;
+  if (!over && len > 0 && line_fp64_safe<T>(a0, a1, 0, len - 1)) {  // exact in FP64 (glc_device.cuh)
+    double md = 0.0, id = (double)threadIdx.x;
+    bool ok = true;
+    for (int64_t i = threadIdx.x; i < len; i += kFitCTA, id += (double)kFitCTA) {
+      const T y = __ldg(v + i);
+      ok &= value_fp64_safe<T>(y);
+      md = fmax(md, abs_resid_fp64((double)(long long)y, __fma_rn(a1, id, a0)));
+    }
+    if (ok) { m = (long long)md; exact = false; }
+  }
+  if (exact)
     for (int64_t i = threadIdx.x; i < len; i += kFitCTA) {
       const long long d = abs_ref(calc_delta<T>(__ldg(v + i), predict<T>(a0, a1, i)));
       m = d > m ? d : m;
@@ -196,18 +207,18 @@ __device__ void choose_chunk(const T* __restrict__ v, int64_t len, unsigned long
   int ov = 0;
 #pragma unroll
   for (int q = 0; q < 4; q++) {
-    y[q] = 0;
-    xy[q] = 0;
+    HalfSums<T> hs;  // exact 64-bit partials of the quarter
 #pragma unroll
     for (int k = 0; k < 1024 / kFitCTA; k++) {
       const int64_t i = q * 1024 + k * kFitCTA + threadIdx.x;
       if (i < len) {
         const T x = __ldg(v + i);
         if (overflows_double<T>(x)) ov |= 1 << q;
-        y[q] += (i128)x;
-        xy[q] += (i128)i * (i128)x;  // chunk-relative position; lines subtract their start below
+        hs.add(x, (int)i);  // chunk-relative position; lines subtract their start below
       }
     }
+    y[q] = hs.sy();
+    xy[q] = hs.sxy();
   }
 #pragma unroll
   for (int q = 0; q < 4; q++) {
@@ -249,7 +260,19 @@ __device__ void choose_chunk(const T* __restrict__ v, int64_t len, unsigned long
   }
   __syncthreads();
   const int over = s_over;
+  // lines whose predictions stay inside the FP64-exact bounds over their values (glc_device.cuh)
+  int safe = 0;
+#pragma unroll
+  for (int l = 0; l < 7; l++) {
+    const int q0 = l == 0 ? 0 : (l < 3 ? (l - 1) * 2 : l - 3);
+    const int q1 = l == 0 ? 4 : (l < 3 ? q0 + 2 : q0 + 1);
+    const int64_t a = q0 * 1024, b = q1 * 1024 < len ? q1 * 1024 : len;
+    if (b > a && !((over >> l) & 1) && line_fp64_safe<T>(s_t0[l], s_t1[l], 0, b - a - 1)) safe |= 1 << l;
+  }
   long long m[7] = {0, 0, 0, 0, 0, 0, 0};
+  double md[7] = {0, 0, 0, 0, 0, 0, 0};
+  bool ok = true;
+  const double tid_d = (double)threadIdx.x;
 #pragma unroll
   for (int q = 0; q < 4; q++) {
     const int lh = 1 + (q >> 1), lq = 3 + q;
@@ -258,18 +281,40 @@ __device__ void choose_chunk(const T* __restrict__ v, int64_t len, unsigned long
       const int64_t i = q * 1024 + k * kFitCTA + threadIdx.x;
       if (i < len) {
         const T x = __ldg(v + i);
-        if (!(over & 1)) {
-          const long long d = abs_ref(calc_delta<T>(x, predict<T>(s_t0[0], s_t1[0], i)));
-          m[0] = d > m[0] ? d : m[0];
+        ok &= value_fp64_safe<T>(x);
+        const double id = tid_d + (double)(q * 1024 + k * kFitCTA);
+        const double yd = (double)(long long)x;
+        const int ls[3] = {0, lh, lq};
+        const int base[3] = {0, (q >> 1) * 2048, q * 1024};
+#pragma unroll
+        for (int t = 0; t < 3; t++) {
+          const int l = ls[t];
+          if ((over >> l) & 1) continue;
+          if ((safe >> l) & 1) {
+            md[l] = fmax(md[l], abs_resid_fp64(yd, __fma_rn(s_t1[l], id - (double)base[t], s_t0[l])));
+          } else {
+            const long long d = abs_ref(calc_delta<T>(x, predict<T>(s_t0[l], s_t1[l], i - base[t])));
+            m[l] = d > m[l] ? d : m[l];
+          }
         }
-        if (!((over >> lh) & 1)) {
-          const long long d = abs_ref(calc_delta<T>(x, predict<T>(s_t0[lh], s_t1[lh], i - (q >> 1) * 2048)));
-          m[lh] = d > m[lh] ? d : m[lh];
-        }
-        if (!((over >> lq) & 1)) {
-          const long long d = abs_ref(calc_delta<T>(x, predict<T>(s_t0[lq], s_t1[lq], i - q * 1024)));
-          m[lq] = d > m[lq] ? d : m[lq];
-        }
+      }
+    }
+  }
+  if (ok) {
+#pragma unroll
+    for (int l = 0; l < 7; l++)
+      if ((safe >> l) & 1) m[l] = (long long)md[l];
+  } else {  // this thread holds a value beyond 2^51: its FP64-measured lines again, exactly
+    for (int i = threadIdx.x; i < len; i += kFitCTA) {
+      const T x = __ldg(v + i);
+      const int q = i >> 10;
+      const int ls[3] = {0, 1 + (q >> 1), 3 + q};
+      const int base[3] = {0, (q >> 1) * 2048, q * 1024};
+      for (int t = 0; t < 3; t++) {
+        const int l = ls[t];
+        if (!((safe >> l) & 1)) continue;
+        const long long d = abs_ref(calc_delta<T>(x, predict<T>(s_t0[l], s_t1[l], i - base[t])));
+        m[l] = d > m[l] ? d : m[l];
       }
     }
   }

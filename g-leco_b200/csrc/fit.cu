@@ -140,6 +140,18 @@ template <typename T> __host__ __device__ constexpr int fit_stage_bytes() { retu
 // value), and the saturating |delta| is formed once from the extreme differences.
 template <typename T>
 __device__ __forceinline__ long long chunk_max_abs_delta(const T* x, int cnt, double t0, double t1, int64_t i0) {
+  if (cnt > 0 && line_fp64_safe<T>(t0, t1, i0, i0 + cnt - 1)) {
+    // exact in FP64 (values checked as they are read; a thread with a larger value redoes its own)
+    double md = 0.0, xd = (double)(i0 + (int64_t)threadIdx.x);
+    bool ok = true;
+#pragma unroll 4
+    for (int jj = threadIdx.x; jj < cnt; jj += kFitThreads, xd += (double)kFitThreads) {
+      const T y = x[jj];
+      ok &= value_fp64_safe<T>(y);
+      md = fmax(md, abs_resid_fp64((double)(long long)y, __fma_rn(t1, xd, t0)));
+    }
+    if (ok) return (long long)md;
+  }
   double xd = (double)(i0 + (int64_t)threadIdx.x);
   if (TypeTraits<T>::is_signed || sizeof(T) == 4) {
     // calc_delta is the plain (wrapping for 64-bit) signed difference

@@ -18,6 +18,7 @@
 // same theta (the reference's theta depends on its reduction order).
 #pragma once
 #include <cstdint>
+#include <type_traits>
 #include <cuda_runtime.h>
 
 namespace glc {
@@ -76,6 +77,52 @@ template <typename T> __device__ __forceinline__ T predict_from(double p) {
 template <typename T> __device__ __forceinline__ T predict(double theta0, double theta1, int64_t i) {
   return predict_from<T>(__fma_rn(theta1, __ll2double_rn(i), theta0));
 }
+
+// ---- exact residual magnitudes in FP64 -------------------------------------------------
+// For a value with |y| < 2^51 and a prediction argument x inside pred_fp64_safe's bounds, the
+// prediction round_half_away(x) = trunc(x + copysign(0.5 - 2^-54, x)) is an FP64 integer that
+// the saturating conversion leaves unchanged, y - pred is below 2^52 in magnitude (no
+// saturation, no wraparound), and every step is exact: abs_resid_fp64 equals
+// abs_ref(calc_delta<T>(y, predict<T>(...))).  fma(theta1, i, theta0) is monotone in i, so a
+// line is safe over [i0, i1] when its two ends are.
+template <typename T> __device__ __forceinline__ bool value_fp64_safe(T y) {
+  return TypeTraits<T>::is_signed ? ((long long)y > -(1ll << 51) && (long long)y < (1ll << 51))
+                                  : ((uint64_t)y < (1ull << 51));
+}
+template <typename T> __device__ __forceinline__ bool pred_fp64_safe(double x) {
+  constexpr double kSafe = 2251799813685248.0;  // 2^51
+  const double lo = TypeTraits<T>::is_signed ? (sizeof(T) == 4 ? -2147483647.0 : -kSafe) : -0.25;
+  const double hi = sizeof(T) == 4 ? (TypeTraits<T>::is_signed ? 2147483646.0 : 4294967294.0) : kSafe;
+  return x >= lo && x <= hi;
+}
+template <typename T> __device__ __forceinline__ bool line_fp64_safe(double t0, double t1, int64_t i0, int64_t i1) {
+  return pred_fp64_safe<T>(__fma_rn(t1, (double)i0, t0)) && pred_fp64_safe<T>(__fma_rn(t1, (double)i1, t0));
+}
+__device__ __forceinline__ double abs_resid_fp64(double yd, double x) {
+  return fabs(__dsub_rn(yd, trunc(__dadd_rn(x, half_away_bias(x)))));
+}
+
+// Exact sums of y and j * y over the values a thread adds (j < 2^14, at most 2^10 values per
+// thread) from 64-bit partials of the 32-bit halves of y; sum(y) and sum(j * y) as 128-bit.
+template <typename T> struct HalfSums {
+  typedef typename std::conditional<TypeTraits<T>::is_signed, int64_t, uint64_t>::type Acc;
+  Acc s_lo = 0, s_hi = 0, x_lo = 0, x_hi = 0;
+  __device__ __forceinline__ void add(T y, int j) {
+    if (sizeof(T) == 8) {
+      const uint32_t yl = (uint32_t)(uint64_t)y;
+      const Acc yh = TypeTraits<T>::is_signed ? (Acc)(int32_t)((int64_t)y >> 32) : (Acc)(uint32_t)((uint64_t)y >> 32);
+      s_lo += (Acc)yl;
+      s_hi += yh;
+      x_lo += (Acc)((uint64_t)(uint32_t)j * yl);
+      x_hi += (Acc)j * yh;
+    } else {
+      s_lo += (Acc)y;
+      x_lo += (Acc)j * (Acc)y;
+    }
+  }
+  __device__ __forceinline__ i128 sy() const { return (i128)s_lo + (i128)s_hi * ((i128)1 << 32); }
+  __device__ __forceinline__ i128 sxy() const { return (i128)x_lo + (i128)x_hi * ((i128)1 << 32); }
+};
 
 template <typename T> __device__ __forceinline__ long long calc_delta(T actual, T pred) {
   if (TypeTraits<T>::is_signed) {

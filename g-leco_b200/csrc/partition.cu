@@ -331,10 +331,22 @@ job_err_kernel(const T* __restrict__ v, const LineJob* __restrict__ jobs, const 
   const int64_t len = (int64_t)jb.b - jb.a;
   const int64_t off1 = off0 + kPairChunk < len ? off0 + kPairChunk : len;
   long long mm = 0;
-  for (int64_t o = off0 + threadIdx.x; o < off1; o += 256) {
-    const long long d = abs_ref(calc_delta<T>(__ldg(v + jb.a + o), predict<T>(jb.t0, jb.t1, o)));
-    mm = d > mm ? d : mm;
+  bool exact = true;
+  if (off1 > off0 && line_fp64_safe<T>(jb.t0, jb.t1, off0, off1 - 1)) {  // exact in FP64 (glc_device.cuh)
+    double md = 0.0, od = (double)(off0 + threadIdx.x);
+    bool ok = true;
+    for (int64_t o = off0 + threadIdx.x; o < off1; o += 256, od += 256.0) {
+      const T y = __ldg(v + jb.a + o);
+      ok &= value_fp64_safe<T>(y);
+      md = fmax(md, abs_resid_fp64((double)(long long)y, __fma_rn(jb.t1, od, jb.t0)));
+    }
+    if (ok) { mm = (long long)md; exact = false; }
   }
+  if (exact)
+    for (int64_t o = off0 + threadIdx.x; o < off1; o += 256) {
+      const long long d = abs_ref(calc_delta<T>(__ldg(v + jb.a + o), predict<T>(jb.t0, jb.t1, o)));
+      mm = d > mm ? d : mm;
+    }
   mm = warp_max_ll(mm);
   __shared__ long long s_m[8];
   if ((threadIdx.x & 31) == 0) s_m[threadIdx.x >> 5] = mm;
