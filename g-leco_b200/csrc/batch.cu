@@ -200,7 +200,7 @@ __device__ void choose_chunk(const T* __restrict__ v, int64_t len, unsigned long
   __shared__ i128 s_y[W][4], s_xy[W][4];
   __shared__ int s_ov[W];
   __shared__ double s_t0[7], s_t1[7];
-  __shared__ int s_over;
+  __shared__ int s_over, s_lover[7];
   __shared__ long long s_m[W][7];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   i128 y[4], xy[4];
@@ -232,30 +232,30 @@ __device__ void choose_chunk(const T* __restrict__ v, int64_t len, unsigned long
     s_ov[warp] = ov;
   }
   __syncthreads();
-  if (threadIdx.x == 0) {
-    i128 Y[4] = {0, 0, 0, 0}, XY[4] = {0, 0, 0, 0};
+  if (threadIdx.x < 7) {  // one thread per line: 0 = the chunk, 1-2 = halves, 3-6 = quarters
+    const int l = threadIdx.x;
+    const int q0 = l == 0 ? 0 : (l < 3 ? (l - 1) * 2 : l - 3);
+    const int q1 = l == 0 ? 4 : (l < 3 ? q0 + 2 : q0 + 1);
     int o = 0;
-    for (int w = 0; w < W; w++) {
-      for (int q = 0; q < 4; q++) { Y[q] += s_y[w][q]; XY[q] += s_xy[w][q]; }
-      o |= s_ov[w];
+    for (int w = 0; w < W; w++) o |= s_ov[w];
+    int lo = 0;
+    for (int q = q0; q < q1; q++) lo |= (o >> q) & 1;
+    const int64_t a = q0 * 1024, b = q1 * 1024 < len ? q1 * 1024 : len;
+    double t0 = 0.0, t1 = 0.0;
+    if (b > a && !lo) {
+      i128 sy = 0, sxy = 0;
+      for (int w = 0; w < W; w++)
+        for (int q = q0; q < q1; q++) { sy += s_y[w][q]; sxy += s_xy[w][q]; }
+      solve_line(b - a, sy, sxy - (i128)a * sy, t0, t1);
     }
-    // lines: 0 = the chunk, 1-2 = halves, 3-6 = quarters: [q0, q1) in quarters
-    const int q0s[7] = {0, 0, 2, 0, 1, 2, 3}, q1s[7] = {4, 2, 4, 1, 2, 3, 4};
+    s_t0[l] = t0;
+    s_t1[l] = t1;
+    s_lover[l] = lo;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
     int over = 0;
-    for (int l = 0; l < 7; l++) {
-      const int64_t a = q0s[l] * 1024, b = q1s[l] * 1024 < len ? q1s[l] * 1024 : len;
-      double t0 = 0.0, t1 = 0.0;
-      int lo = 0;
-      for (int q = q0s[l]; q < q1s[l]; q++) lo |= (o >> q) & 1;
-      if (b > a && !lo) {
-        i128 sy = 0, sxy = 0;
-        for (int q = q0s[l]; q < q1s[l]; q++) { sy += Y[q]; sxy += XY[q]; }
-        solve_line(b - a, sy, sxy - (i128)a * sy, t0, t1);
-      }
-      if (lo) over |= 1 << l;
-      s_t0[l] = t0;
-      s_t1[l] = t1;
-    }
+    for (int l = 0; l < 7; l++) over |= s_lover[l] << l;
     s_over = over;
   }
   __syncthreads();
