@@ -458,6 +458,33 @@ void group_work_by_type(std::vector<BatchWork>& w, const std::vector<int32_t>& c
   w.swap(out);
 }
 
+// Range pieces -> per-tile work items, on the device: item t (in the pieces' order, grouped by
+// element type) is tile (t - tile_base[p]) of piece p, the last piece with tile_base[p] <= t.  A
+// piece is one BatchWork whose `tile` is its first tile; the host builds one per range piece
+// instead of one per tile.
+__global__ void expand_pieces_kernel(const BatchWork* __restrict__ pieces, const int64_t* __restrict__ tile_base,
+                                     int npieces, int64_t ntiles, BatchWork* __restrict__ work) {
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < ntiles; t += (int64_t)gridDim.x * blockDim.x) {
+    int lo = 0, hi = npieces - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (tile_base[mid] <= t) lo = mid; else hi = mid - 1;
+    }
+    BatchWork w = pieces[lo];
+    w.tile += (int32_t)(t - tile_base[lo]);
+    work[t] = w;
+  }
+}
+
+cudaError_t launch_expand_pieces(const BatchWork* pieces, const int64_t* tile_base, int npieces, int64_t ntiles,
+                                 BatchWork* work, int num_sms, cudaStream_t s) {
+  if (ntiles <= 0 || npieces <= 0) return cudaSuccess;
+  int64_t grid = (ntiles + 255) / 256;
+  if (grid > 4ll * num_sms) grid = 4ll * num_sms;
+  expand_pieces_kernel<<<(unsigned)grid, 256, 0, s>>>(pieces, tile_base, npieces, ntiles, work);
+  return cudaGetLastError();
+}
+
 // Launch configuration of the batched decode, per device: the shared-memory attribute is raised
 // once to the largest stage ring, and the resident CTAs per SM are kept per stage size (these
 // queries cost microseconds, and the serving loop launches tens of thousands of times a second).

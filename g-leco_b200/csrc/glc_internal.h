@@ -192,6 +192,10 @@ struct BatchWork {
   int64_t lo, hi;  // element range of the column decoded by this item (clipped to the tile)
   void* out_base;  // element e of the column is written to out_base[e] (16-byte aligned)
 };
+// decode.cu: range pieces (one BatchWork each, `tile` = its first tile) -> per-tile work items;
+// tile_base[p] = tiles of the pieces before p (npieces + 1 entries)
+cudaError_t launch_expand_pieces(const BatchWork* pieces, const int64_t* tile_base, int npieces, int64_t ntiles,
+                                 BatchWork* work, int num_sms, cudaStream_t s);
 struct BatchDecodeArgs {
   const BatchColumn* cols;
   const BatchWork* work;

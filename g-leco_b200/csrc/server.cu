@@ -127,7 +127,8 @@ struct glc_server {
   std::vector<RAColumn> w_ra;
   std::vector<BatchColumn> w_bc;
   std::vector<RARequest> w_req;
-  std::vector<BatchWork> w_work;
+  std::vector<BatchWork> w_work;  // range pieces of the launch being built
+  std::vector<int64_t> w_tb;       // tiles before each piece
   std::vector<Copy> w_copy;
   std::vector<int32_t> w_dtype;
   std::vector<int32_t> w_colmap;    // column id -> local index + 1 (valid when w_epoch matches)
@@ -263,8 +264,7 @@ void launch_slot(glc_server* S, Slot& sl, std::deque<Req*>& ready_l, std::deque<
                                (size_t)((hi - lo) * es)});
       stage_off += (size_t)((hi - lo) * es);
     }
-    for (int64_t t = lo / kDecodeTile; t * kDecodeTile < hi; t++)
-      S->w_work.push_back(BatchWork{li, (int32_t)t, lo, hi, (void*)base});
+    S->w_work.push_back(BatchWork{li, (int32_t)(lo / kDecodeTile), lo, hi, (void*)base});  // one per piece
     max_bits = std::max(max_bits, (int)r->bc.max_bits);
     budget -= hi - lo;
     r->next = hi;
@@ -275,26 +275,39 @@ void launch_slot(glc_server* S, Slot& sl, std::deque<Req*>& ready_l, std::deque<
     if (hi == end) ready_r.pop_front();
   }
 
-  // Range pieces grouped by element type (the decode runs one type per CTA).
+  // Range pieces grouped by element type (the decode runs one type per CTA); their tiles become
+  // the decode's work items on the device (expand_pieces_kernel), group order kept.
   int64_t group_begin[5] = {0, 0, 0, 0, 0};
-  if (!S->w_work.empty()) {
+  npieces = (int)S->w_work.size();  // pieces after the loop (equal to its count)
+  S->w_tb.assign((size_t)npieces + 1, 0);
+  if (npieces > 0) {
     S->w_dtype.resize(S->w_bc.size());
     for (size_t i = 0; i < S->w_bc.size(); i++) S->w_dtype[i] = S->w_bc[i].dtype;
     group_work_by_type(S->w_work, S->w_dtype, group_begin);
+    for (int p = 0; p < npieces; p++) {
+      const BatchWork& w = S->w_work[p];
+      S->w_tb[p + 1] = S->w_tb[p] + (w.hi + kDecodeTile - 1) / kDecodeTile - w.lo / kDecodeTile;
+    }
+    for (int d = 0; d < 5; d++) group_begin[d] = S->w_tb[group_begin[d]];  // in tiles
   }
+  const int64_t ntiles = S->w_tb[npieces];
 
   // One host-to-device copy of all tables: [4 decode work counters u64][lookup columns]
-  // [decode columns][lookup requests][work items].
+  // [decode columns][lookup requests][range pieces][piece tile bases]; the per-tile work items
+  // follow on the device only.
   const size_t o_ra = 32;
   const size_t o_bc = align16(o_ra + sizeof(RAColumn) * S->w_ra.size());
   const size_t o_req = align16(o_bc + sizeof(BatchColumn) * S->w_bc.size());
-  const size_t o_work = align16(o_req + sizeof(RARequest) * S->w_req.size());
-  const size_t total = align16(o_work + sizeof(BatchWork) * S->w_work.size());
+  const size_t o_piece = align16(o_req + sizeof(RARequest) * S->w_req.size());
+  const size_t o_tb = align16(o_piece + sizeof(BatchWork) * (size_t)npieces);
+  const size_t o_work = align16(o_tb + sizeof(int64_t) * ((size_t)npieces + 1));
+  const size_t total = o_work;
   std::memset(sl.h_meta, 0, 32);
   std::memcpy(sl.h_meta + o_ra, S->w_ra.data(), sizeof(RAColumn) * S->w_ra.size());
   std::memcpy(sl.h_meta + o_bc, S->w_bc.data(), sizeof(BatchColumn) * S->w_bc.size());
   std::memcpy(sl.h_meta + o_req, S->w_req.data(), sizeof(RARequest) * S->w_req.size());
-  std::memcpy(sl.h_meta + o_work, S->w_work.data(), sizeof(BatchWork) * S->w_work.size());
+  std::memcpy(sl.h_meta + o_piece, S->w_work.data(), sizeof(BatchWork) * (size_t)npieces);
+  std::memcpy(sl.h_meta + o_tb, S->w_tb.data(), sizeof(int64_t) * ((size_t)npieces + 1));
   *sl.h_err = 0;
 
   cudaError_t e = cudaMemcpyAsync(sl.d_meta, sl.h_meta, total, cudaMemcpyHostToDevice, sl.stream);
@@ -302,15 +315,18 @@ void launch_slot(glc_server* S, Slot& sl, std::deque<Req*>& ready_l, std::deque<
     e = launch_multi_lookup((const RAColumn*)(sl.d_meta + o_ra), (const RARequest*)(sl.d_meta + o_req),
                             (int)S->w_req.size(), nl, S->ctx->num_sms, sl.stream);
   sl.lookups_pending = false;
-  if (e == cudaSuccess && nl > 0 && !S->w_work.empty()) {  // lookups need not wait for the decode
+  if (e == cudaSuccess && nl > 0 && npieces > 0) {  // lookups need not wait for the decode
     e = cudaEventRecord(sl.lk_done, sl.stream);
     sl.lookups_pending = e == cudaSuccess;
   }
-  if (e == cudaSuccess && !S->w_work.empty()) {
+  if (e == cudaSuccess && npieces > 0)
+    e = launch_expand_pieces((const BatchWork*)(sl.d_meta + o_piece), (const int64_t*)(sl.d_meta + o_tb), npieces,
+                             ntiles, (BatchWork*)(sl.d_meta + o_work), S->ctx->num_sms, sl.stream);
+  if (e == cudaSuccess && npieces > 0) {
     BatchDecodeArgs a;
     a.cols = (const BatchColumn*)(sl.d_meta + o_bc);
     a.work = (const BatchWork*)(sl.d_meta + o_work);
-    a.nwork = (int64_t)S->w_work.size();
+    a.nwork = ntiles;
     for (int d = 0; d < 5; d++) a.group_begin[d] = group_begin[d];
     a.counter = (unsigned long long*)sl.d_meta;
     a.err = sl.d_err;
@@ -500,7 +516,8 @@ glc_status glc_server_create(glc_ctx* ctx, const glc_server_config* config, glc_
   // Work items: every full tile of the launch's range values plus two partial tiles per piece.
   S->max_work = c.max_range_values / kDecodeTile + 2ll * c.max_requests + 2;
   S->meta_cap = align16(32 + (sizeof(RAColumn) + sizeof(BatchColumn)) * kMaxColsPerLaunch + 64 +
-                        sizeof(RARequest) * (size_t)c.max_requests + sizeof(BatchWork) * (size_t)S->max_work);
+                        sizeof(RARequest) * (size_t)c.max_requests + sizeof(BatchWork) * (size_t)c.max_requests +
+                        sizeof(int64_t) * ((size_t)c.max_requests + 1) + 48 + sizeof(BatchWork) * (size_t)S->max_work);
   S->stage_cap = (size_t)c.max_range_values * 8 + 16 * (size_t)c.max_requests + 256;
   cudaSetDevice(ctx->device);
   cudaError_t e = cudaSuccess;
