@@ -111,7 +111,10 @@ GLC_API glc_status glc_sync(glc_ctx* ctx, glc_stream stream);
  * GLC_PART_VARIABLE runs the device split/merge partitioner (the reference runs
  * VariableLengthPartitioner on the host, compression/CpuPartitioner.cuh:342-422).
  * *compressed_size_bytes (may be NULL) receives the size the reference reports
- * (64 B per partition + 120 B header + ceil(total_bits/8)). n == 0 gives an empty column. */
+ * (64 B per partition + 120 B header + ceil(total_bits/8)). n == 0 gives an empty column.
+ * Device `values` must be aligned to the element size (GLC_ERR_INVALID_ARG otherwise).  The
+ * column's arrays come from the context's memory pool; glc_column_free synchronises the device
+ * before releasing them, as the reference's cleanup() (cudaFree) does. */
 GLC_API glc_status glc_compress(glc_ctx* ctx, glc_dtype dtype, const void* values, int64_t n, int flags,
                         glc_partitioning mode, int32_t fixed_partition_len, glc_column** out,
                         int64_t* compressed_size_bytes, glc_stream stream);
@@ -132,7 +135,9 @@ GLC_API glc_status glc_partition_v6(glc_ctx* ctx, glc_dtype dtype, const void* v
                                     int32_t base_size, int32_t* starts, int32_t* ends, int64_t cap,
                                     int64_t* num_partitions, glc_stream stream);
 
-/* Replaces LeCoGPU::cleanup (api/G-LeCo.cuh:793-821). */
+/* Replaces LeCoGPU::cleanup (api/G-LeCo.cuh:793-821).  Like its cudaFree calls, it waits for all
+ * work on the device before the column's memory is released (compressed and deserialized columns),
+ * so a decode still running on any stream finishes first.  Free columns before glc_destroy. */
 GLC_API glc_status glc_column_free(glc_column* col);
 GLC_API glc_status glc_column_get_info(const glc_column* col, glc_column_info* info);
 
