@@ -403,13 +403,14 @@ size_t fit_scratch_bytes(const int32_t*, int64_t n, int64_t P) {
 template <typename T, int PASS>
 static cudaError_t launch_fit_stream(const T* v, const FitStreamArgs& a, int num_sms, cudaStream_t s) {
   const int smem = kFitStages * fit_stage_bytes<T>();
-  static bool attr_set = false;  // per instantiation
+  static PerDeviceFlag attr_set;  // per instantiation and device
+  const int dev = current_device();
   cudaError_t e;
-  if (!attr_set) {
+  if (!attr_set.test(dev)) {
     if ((e = cudaFuncSetAttribute(fit_stream_kernel<T, PASS>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) !=
         cudaSuccess)
       return e;
-    attr_set = true;
+    attr_set.set(dev);
   }
   int per_sm = 0;
   if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fit_stream_kernel<T, PASS>, kFitCTA, smem)) !=

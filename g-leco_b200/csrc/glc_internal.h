@@ -122,6 +122,20 @@ void stager_free(glc_ctx* ctx);
 void tune_defaults(glc_ctx* ctx);                  // tune.cu
 bool tune_load(glc_ctx* ctx, const char* path);   // tune.cu: true when the file fits this device
 
+// One bit per device: a per-device launch step (a kernel attribute, which belongs to the
+// device's copy of the kernel) has been done.  Safe for concurrent host threads.
+struct PerDeviceFlag {
+  std::atomic<unsigned long long> bits{0};
+  bool test(int dev) const { return dev >= 0 && dev < 64 && ((bits.load(std::memory_order_acquire) >> dev) & 1ull); }
+  void set(int dev) {
+    if (dev >= 0 && dev < 64) bits.fetch_or(1ull << dev, std::memory_order_release);
+  }
+};
+inline int current_device() {
+  int d = 0;
+  return cudaGetDevice(&d) == cudaSuccess ? d : -1;
+}
+
 // Stream-ordered temporary allocation from the context's pool.
 template <typename P> inline cudaError_t pool_alloc(glc_ctx* ctx, P** p, size_t bytes, cudaStream_t s) {
   return cudaMallocFromPoolAsync((void**)p, bytes, ctx->pool, s);

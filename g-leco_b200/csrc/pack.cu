@@ -411,13 +411,14 @@ pack_tile_kernel(PackTileArgs a) {
 template <typename T, bool BATCH>
 static cudaError_t launch_pack_tile_kernel(const PackTileArgs& a, int64_t nitems, int num_sms, cudaStream_t s) {
   const int smem = kPackStages * pack_stage_bytes<T>() + (sizeof(T) == 4 ? kDecodeTile * 8 : 0);
-  static bool attr_set = false;  // per instantiation
+  static PerDeviceFlag attr_set;  // per instantiation and device
+  const int dev = current_device();
   cudaError_t e;
-  if (!attr_set) {
+  if (!attr_set.test(dev)) {
     if ((e = cudaFuncSetAttribute(pack_tile_kernel<T, BATCH>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) !=
         cudaSuccess)
       return e;
-    attr_set = true;
+    attr_set.set(dev);
   }
   int per_sm = 0;
   if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pack_tile_kernel<T, BATCH>, kPackCTA, smem)) !=

@@ -175,11 +175,12 @@ static cudaError_t ra_shape(glc_ctx* ctx, const RAArgs& a, int mode, cudaStream_
   int per_sm = 0;
   cudaError_t e;
   if (mode != 2) {  // no shared memory in the fixed modes: prefer the largest L1 for descriptors
-    static bool carveout_set = false;
-    if (!carveout_set) {
+    static PerDeviceFlag carveout_set;  // per instantiation and device
+    const int dev = current_device();
+    if (!carveout_set.test(dev)) {
       cudaFuncSetAttribute(random_access_kernel<T, PLAIN, 0, QPT, MINB>, cudaFuncAttributePreferredSharedMemoryCarveout, 0);
       cudaFuncSetAttribute(random_access_kernel<T, PLAIN, 1, QPT, MINB>, cudaFuncAttributePreferredSharedMemoryCarveout, 0);
-      carveout_set = true;
+      carveout_set.set(dev);
     }
   }
   e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kRAThreads, 0);
