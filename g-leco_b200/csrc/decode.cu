@@ -181,12 +181,34 @@ __device__ __forceinline__ void decode_tile(const DecodeArgs& a, const StageInfo
       } else {
         const uint32_t pos = c.base + (uint32_t)e * (uint32_t)c.bits;
         const uint32_t shl = (uint32_t)(32 - c.bits) & 31u;
+        const int b = c.bits;
+        if (V % 4 == 0 && b <= 8) {
+          // the 32-bit window at field u holds fields u .. u+3 whole (4b <= 32): one window per 4
 #pragma unroll
-        for (int u = 0; u < V; u++) {
-          const uint32_t p = pos + (uint32_t)(u * c.bits);
-          const uint32_t wi = p >> 5;
-          const uint32_t f = __funnelshift_r(src[wi], src[wi + 1], p & 31);
-          rr[u] = (int32_t)(f << shl) >> shl;
+          for (int g = 0; g < V; g += 4) {
+            const uint32_t p = pos + (uint32_t)(g * b);
+            const uint32_t wi = p >> 5;
+            const uint32_t f = __funnelshift_r(src[wi], src[wi + 1], p & 31);
+#pragma unroll
+            for (int h = 0; h < 4; h++) rr[g + h] = (int32_t)(f << (uint32_t)(32 - (h + 1) * b)) >> shl;
+          }
+        } else if (V % 2 == 0 && b <= 16) {  // two fields per window (2b <= 32)
+#pragma unroll
+          for (int g = 0; g < V; g += 2) {
+            const uint32_t p = pos + (uint32_t)(g * b);
+            const uint32_t wi = p >> 5;
+            const uint32_t f = __funnelshift_r(src[wi], src[wi + 1], p & 31);
+            rr[g] = (int32_t)(f << shl) >> shl;
+            rr[g + 1] = (int32_t)(f << (uint32_t)(32 - 2 * b)) >> shl;
+          }
+        } else {
+#pragma unroll
+          for (int u = 0; u < V; u++) {
+            const uint32_t p = pos + (uint32_t)(u * c.bits);
+            const uint32_t wi = p >> 5;
+            const uint32_t f = __funnelshift_r(src[wi], src[wi + 1], p & 31);
+            rr[u] = (int32_t)(f << shl) >> shl;
+          }
         }
       }
       if (RESID) {
