@@ -338,6 +338,69 @@ def run_random_access(args):
     return 0
 
 
+def run_decode_i32(args):
+    """Full decode of an int32 column: n values 1000 + 3 i + U[0, 2^w) (w = --noise-bits), fixed
+    partitions of 4096, generated and compressed on the device.  One step = one full decode;
+    value = decoded GB/s.  Roofline bytes: compressed bytes read + 4 B per value written."""
+    import torch
+
+    import glc
+
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.Stream(dev)
+    torch.cuda.set_stream(stream)
+    sh = stream.cuda_stream
+    ctx = tuned_context(glc, local)
+    n = args.n if args.n != DEFAULT_N else 100_000_000
+    w = args.noise_bits
+    i = torch.arange(n, device=dev, dtype=torch.int64)
+    g = torch.Generator(device=dev)
+    g.manual_seed(1)
+    v = (1000 + 3 * i + torch.randint(0, 1 << w, (n,), device=dev, generator=g)).to(torch.int32)
+    del i
+    col = glc.compress_device(ctx, glc.I32, v.data_ptr(), n, glc.FIXED, fixed_len=4096, stream=sh)
+    info = col.info()
+    out = torch.empty_like(v)
+
+    def step():
+        glc.decompress_into(ctx, col, out.data_ptr(), glc.SRC_PACKED, stream=sh)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize(dev)
+    ok = bool(torch.equal(out, v))
+    clocks = ClockSampler(dev)
+    clocks.start()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        step()
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    clk = clocks.stop()
+    ms = e0.elapsed_time(e1) / args.steps
+    peak, peak_kind = measured_peak()
+    algo = info.compressed_size_bytes + 4 * n
+    line = {
+        "metric": "decoded GB/s", "value": round(4 * n / (ms / 1e3) / 1e9, 2), "unit": "GB/s", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 4), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
+        "config": {"workload": f"linear_i32_{n // 1_000_000}M_noise{w}_fixed4096", "values": n,
+                   "bits_per_value": round(info.total_bits / n, 3), "values_per_s": round(n / (ms / 1e3), 1),
+                   "bit_exact": ok, "l2": "output larger than L2 (no flush)"},
+        "roofline": {"bound": "hbm", "achieved": round(algo / (ms / 1e3) / 1e9, 1), "peak": peak, "unit": "GB/s",
+                     "frac": round(algo / (ms / 1e3) / 1e9 / peak, 4), "peak_kind": peak_kind, "traffic": None},
+        "e2e": None, "gpu_launches": args.steps, "clocks": clk, "cpu_baseline": None,
+    }
+    print(json.dumps(line), flush=True)
+    col.free()
+    ctx.close()
+    return 0
+
+
 COMPRESS_LAUNCHES = {"fixed": 22, "v6": 29}  # kernels per compress call (ncu launch list of one call)
 
 
@@ -959,10 +1022,11 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--columns", type=int, default=4096, help="c4 batch: number of columns")
     ap.add_argument("--workload", default="c2_decode",
-                    choices=["c2_decode", "c3_random_access", "c4_batch", "c5_serving", "compress"],
+                    choices=["c2_decode", "c3_random_access", "c4_batch", "c5_serving", "compress", "decode_i32"],
                     help="c2_decode (headline): full decode of the 200M piecewise uint64 column; "
                          "c3_random_access: 100M lookups into a 64M int64 timestamp column")
     ap.add_argument("--mode", default="packed", choices=["packed", "preunpacked"], help="c3 residual source")
+    ap.add_argument("--noise-bits", type=int, default=6, help="decode_i32: noise bits of the int32 column")
     ap.add_argument("--partitioning", default="fixed", choices=["fixed", "v6", "variable"],
                     help="compress: fixed partitions of 4096, the reference's GPU partitioner, or split/merge")
     ap.add_argument("--queries", type=int, default=100_000_000, help="c3 lookups per step")
@@ -986,6 +1050,8 @@ def main():
         return run_serving(args)
     if args.workload == "compress":
         return run_compress(args)
+    if args.workload == "decode_i32":
+        return run_decode_i32(args)
 
     import torch
     import torch.distributed as dist
