@@ -387,6 +387,35 @@ __global__ void multi_count_kernel(const int32_t* __restrict__ starts, const int
   nm[p] = ((int64_t)ends[p] - starts[p]) > kFitChunk ? nch[p] : 0;
 }
 
+// Fixed partitions of length L (the last one n - (P - 1) L): the chunk tables in closed form, in
+// one launch -- chunks per partition, each partition's first chunk, chunk -> partition, and the
+// chunk counts of the two fit passes.  Partitions longer than one chunk are all the full ones
+// (when L > 4096) and perhaps the last, so the second pass's list is a prefix of the first's
+// and shares its tables.
+__global__ void fixed_chunk_setup_kernel(int64_t n, int64_t L, int64_t P, int64_t* __restrict__ nch,
+                                         int64_t* __restrict__ base, int32_t* __restrict__ owner,
+                                         int64_t* __restrict__ nchunks, int64_t* __restrict__ nmulti) {
+  const int64_t nch_full = (L + kFitChunk - 1) / kFitChunk;
+  const int64_t len_last = n - (P - 1) * L;
+  const int64_t nch_last = (len_last + kFitChunk - 1) / kFitChunk;
+  const int64_t total = (P - 1) * nch_full + nch_last;
+  const int64_t span = P > total ? P : total;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < span; i += (int64_t)gridDim.x * blockDim.x) {
+    if (i < P) {
+      nch[i] = i < P - 1 ? nch_full : nch_last;
+      base[i] = i * nch_full;
+    }
+    if (i < total) {
+      const int64_t o = i / nch_full;
+      owner[i] = (int32_t)(o < P - 1 ? o : P - 1);
+    }
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    *nchunks = total;
+    *nmulti = (L > kFitChunk ? (P - 1) * nch_full : 0) + (len_last > kFitChunk ? nch_last : 0);
+  }
+}
+
 size_t fit_scratch_bytes(const int32_t*, int64_t n, int64_t P) {
   int64_t ncmax = n / kFitChunk + P + 1;
   size_t b = 0;
@@ -447,12 +476,21 @@ static cudaError_t fit_typed(const T* v, glc_column* c, void* scratch, int64_t* 
   // partitions per 4096-value tile (without the last partition)
   if ((e = cudaMemsetAsync(d_stats, 0, 4 * sizeof(int64_t), s)) != cudaSuccess) return e;
 
-  chunk_count_kernel<<<pg, 256, 0, s>>>(c->d_start, c->d_end, P, nch);
-  if ((e = exclusive_scan<int64_t>(nch, base, P, nchunks, tiles, s)) != cudaSuccess) return e;
-  chunk_owner_kernel<<<pg, 256, 0, s>>>(base, nch, P, owner);
-  multi_count_kernel<<<pg, 256, 0, s>>>(c->d_start, c->d_end, nch, P, nm);
-  if ((e = exclusive_scan<int64_t>(nm, mbase, P, nmulti, tiles, s)) != cudaSuccess) return e;
-  chunk_owner_kernel<<<pg, 256, 0, s>>>(mbase, nm, P, owner_m);
+  if (c->fixed_len > 0) {  // fixed partitions: closed-form tables, one launch
+    const int64_t span = n / kFitChunk + P + 1;
+    int64_t grid = (span + 255) / 256;
+    if (grid > 4ll * num_sms) grid = 4ll * num_sms;
+    fixed_chunk_setup_kernel<<<(unsigned)grid, 256, 0, s>>>(n, c->fixed_len, P, nch, base, owner, nchunks, nmulti);
+    owner_m = owner;  // the second pass's chunks are a prefix of the first's
+    mbase = base;
+  } else {
+    chunk_count_kernel<<<pg, 256, 0, s>>>(c->d_start, c->d_end, P, nch);
+    if ((e = exclusive_scan<int64_t>(nch, base, P, nchunks, tiles, s)) != cudaSuccess) return e;
+    chunk_owner_kernel<<<pg, 256, 0, s>>>(base, nch, P, owner);
+    multi_count_kernel<<<pg, 256, 0, s>>>(c->d_start, c->d_end, nch, P, nm);
+    if ((e = exclusive_scan<int64_t>(nm, mbase, P, nmulti, tiles, s)) != cudaSuccess) return e;
+    chunk_owner_kernel<<<pg, 256, 0, s>>>(mbase, nm, P, owner_m);
+  }
 
   FitStreamArgs a{c->d_start, c->d_end, nchunks, owner, base, P, sy, sxy, ovf, base,
                   c->d_types, c->d_params, c->d_err, (unsigned long long*)(d_stats + 2)};

@@ -72,7 +72,8 @@ def _check_column(codec, col, values, oracle_col, oracle):
 
 
 @pytest.mark.parametrize("kind", KINDS)
-@pytest.mark.parametrize("n,L", [(100_003, 1024), (65_536, 4096), (5_000, 128), (777, 1000)])
+@pytest.mark.parametrize("n,L", [(100_003, 1024), (65_536, 4096), (5_000, 128), (777, 1000), (20_000, 6000),
+                                 (50_001, 10_000)])
 def test_fixed_compress_bit_exact(oracle, kind, n, L):
     v = _data(kind, n)
     codec = _codec(v)
