@@ -401,7 +401,7 @@ def run_decode_i32(args):
     return 0
 
 
-COMPRESS_LAUNCHES = {"fixed": 13, "v6": 29}  # kernels per compress call (ncu launch list of one call)
+COMPRESS_LAUNCHES = {"fixed": 13, "v6": 29}  # kernels launched by one compress call
 
 
 def run_compress(args):
