@@ -109,16 +109,21 @@ glc_status tfail(glc_ctx* ctx, glc_status st, const std::string& msg) {
 
 }  // namespace
 
+// Built-in shapes for contexts that never tune: the choices glc_autotune made on a B200 (148 SMs),
+// rounded to one rule per element size -- 4-byte outputs: ring depth 3, unroll 2; 8-byte outputs:
+// depth 2, unroll 4 on packed fields (2 on pre-unpacked residuals), a whole tile staged for 64-bit
+// fields; random access: shape 4 up to 32-bit fields, 0 at 48, 3 at 64, 3 for pre-unpacked.
 void glc::tune_defaults(glc_ctx* ctx) {
   for (int d = 0; d < 4; d++)
     for (int b = 0; b < kTuneBuckets; b++)
       for (int p = 0; p < 2; p++) {
         TuneEntry& t = ctx->tune[d][b][p];
-        t.decode_stages = 2;
-        t.decode_unroll = 2;
-        t.ra_shape = p ? 3 : 4;
+        const bool wide_type = d == GLC_I64 || d == GLC_U64;
+        t.decode_stages = wide_type ? 2 : 3;
+        t.decode_unroll = (wide_type && !p) ? 4 : 2;
+        t.ra_shape = p ? 3 : (b <= 3 ? 4 : (b == 4 ? 0 : 3));
         t.measured = 0;
-        t.decode_cap_words = 0;
+        t.decode_cap_words = (wide_type && !p && b == kTuneBuckets - 1) ? kStageCapWordsMax : 0;
         t.reserved = 0;
         t.decode_gbs = 0.f;
         t.ra_glookups = 0.f;
