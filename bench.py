@@ -45,7 +45,7 @@ METRIC = "decode GB/s"
 UNIT = "GB/s"
 WORKLOAD = "piecewise_u64_200M_variable"
 DEFAULT_N = 200_000_000
-PROFILE_NOTE = os.path.join(ROOT, "profiles", "decode_piecewise_u64_200M.md")
+TRAFFIC_JSON = os.path.join(ROOT, "profiles", "decode_piecewise_u64_200M.traffic.json")
 # launch shapes measured once per device by glc_autotune (built files, not committed)
 TUNE_CACHE = os.path.join(ROOT, "g-leco_b200", "_build", "tune_cache.txt")
 
@@ -68,16 +68,16 @@ def measured_peak():
         return 6650.0, "fallback"
 
 
-def profiled_traffic_per_value():
-    """DRAM bytes per decoded value from the committed ncu summary (one capture), or None."""
+def profiled_traffic(n: int):
+    """DRAM bytes (read + write) of one decode launch over n values, from the ncu capture that the
+    profiling step writes as JSON beside its summary (one launch of the full-size workload),
+    scaled by the values decoded; None when there is no capture."""
     try:
-        with open(PROFILE_NOTE) as f:
-            for line in f:
-                if line.startswith("traffic_bytes_per_value:"):
-                    return float(line.split(":", 1)[1].strip())
-    except OSError:
-        pass
-    return None
+        with open(TRAFFIC_JSON) as f:
+            t = json.load(f)
+        return round((t["dram_bytes_read"] + t["dram_bytes_write"]) * n / t["values"])
+    except (OSError, KeyError, ValueError):
+        return None
 
 
 _SAMPLER = r"""
@@ -150,81 +150,119 @@ def make_values(n: int, rank: int) -> np.ndarray:
     return W.piecewise_linear(n, seed=42 + rank)
 
 
-def cpu_baseline_decode(values: np.ndarray, blob_maker, threads: int, budget_s: float = 20.0):
-    """Time the reference's host decoder on a bounded prefix sample; returns a dict."""
+REF_CACHE = os.path.join(ROOT, "g-leco_b200", "_build", "reference_arm")
+
+
+def host_threads() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def cpu_baseline_decode(blob: bytes, values: np.ndarray, threads: int, passes: int = 3):
+    """The reference's host decoder (directRandomAccessCPU, compiled from the reference's sources)
+    over EVERY position of ``blob`` on ``threads`` host threads; returns a cpu_baseline dict.
+    Without the compiled reference, the oracle's decode (one thread) stands in ("port")."""
     import oracle
-    sample_n = min(len(values), 16_000_000)
-    sample = np.ascontiguousarray(values[:sample_n])
-    blob = blob_maker(sample)
-    pos = np.arange(sample_n, dtype=np.int32)
-    kind = "reference" if oracle.ref_available() else "port"
-    with tempfile.TemporaryDirectory() as td:
-        if kind == "reference":
-            chunks = np.array_split(pos, threads)
-            paths = []
-            for k, ch in enumerate(chunks):
-                pp = os.path.join(td, f"pos{k}.bin")
-                ch.tofile(pp)
-                paths.append(pp)
-            bp = os.path.join(td, "blob.bin")
+    n = len(values)
+    if oracle.ref_available():
+        with tempfile.TemporaryDirectory() as td:
+            bp, vp, mp = (os.path.join(td, f) for f in ("blob.bin", "values.bin", "mism.bin"))
             with open(bp, "wb") as f:
                 f.write(blob)
-            env = dict(os.environ, GLC_REF_CPU_ONLY="1")
-            t0 = time.perf_counter()
-            procs = [subprocess.Popen([oracle.REF_HARNESS, "hostdecode", "u64", bp, paths[k],
-                                       os.path.join(td, f"out{k}.bin"), "1"], stdout=subprocess.PIPE,
-                                      stderr=subprocess.PIPE, env=env) for k in range(len(paths))]
-            for p in procs:
-                p.wait()
-            wall = time.perf_counter() - t0
-            secs = max(float(p.stdout.read().decode().strip().splitlines()[-1]) for p in procs)
-            out = np.concatenate([np.fromfile(os.path.join(td, f"out{k}.bin"), np.uint64) for k in range(len(paths))])
-            mism = int(np.count_nonzero(out != sample))
-        else:
-            col = oracle.deserialize(blob, "u64")
-            t0 = time.perf_counter()
-            out = oracle.decode_full(col)
-            secs = time.perf_counter() - t0
-            wall = secs
-            mism = int(np.count_nonzero(out != sample))
-            threads = 1
-    gbs = sample_n * 8 / secs / 1e9
-    return {"value": round(gbs, 4), "unit": UNIT, "cores": threads, "kind": kind,
-            "sample": f"full decode of the first {sample_n:,} values of the workload (all positions, "
-                      f"{'directRandomAccessCPU' if kind == 'reference' else 'oracle decode'}), "
-                      f"{threads} process(es); wall {wall:.2f} s; values differing from the input: {mism} "
-                      f"(the reference's host decoder predicts without fma)"}
+            values.tofile(vp)
+            secs, mism = oracle.ref_hostdecode_all(bp, vp, "u64", threads, passes, mp)
+            where = np.fromfile(mp, np.int64).astype(np.int32)
+        col = oracle.deserialize(blob, "u64")
+        # every value the reference's host decoder gets wrong is one where its prediction without
+        # fma rounds differently from the format's fma prediction (the oracle restates both)
+        explained = bool(np.all(oracle.decode_variant(col, where, oracle.PRED_HOST)
+                                != oracle.decode_variant(col, where, oracle.PRED_CONTRACT)))
+        best = min(secs)
+        kind, how = "reference", "directRandomAccessCPU (the reference's host decoder, compiled from its sources)"
+    else:
+        col = oracle.deserialize(blob, "u64")
+        t0 = time.perf_counter()
+        out = oracle.decode_full(col)
+        best = time.perf_counter() - t0
+        mism, explained, threads, passes = int(np.count_nonzero(out != values)), True, 1, 1
+        kind, how = "port", "the oracle's decode (the reference harness is not built)"
+    return {"value": round(n * 8 / best / 1e9, 4), "unit": UNIT, "cores": threads, "kind": kind,
+            "sample": f"full decode of all {n:,} values of the workload's blob by {how} on {threads} host "
+                      f"thread(s), best of {passes} passes ({best:.3f} s); values differing from the input: "
+                      f"{mism}, all at positions where that decoder's prediction without fma rounds "
+                      f"differently: {explained}"}
+
+
+def reference_blob(n: int, seed: int):
+    """The workload column compressed by the reference's own stock compress with its CPU
+    partitioner (use_variable_partitioning = true, api/G-LeCo.cuh:349-614) and serialize (:826),
+    run from the compiled reference on this host's GPU; cached under _build/.  Returns
+    (values, blob path, values path, reported compressed size, how)."""
+    import oracle
+    os.makedirs(REF_CACHE, exist_ok=True)
+    stem = os.path.join(REF_CACHE, f"piecewise_u64_{n}_seed{seed}")
+    meta_p, vp, bp = stem + ".json", stem + ".values.bin", stem + ".blob"
+    values = make_values(n, seed - 42)
+    if os.path.exists(meta_p) and os.path.exists(bp) and os.path.exists(vp):
+        with open(meta_p) as f:
+            meta = json.load(f)
+        return values, bp, vp, meta["size"], meta["how"]
+    values.tofile(vp)
+    t0 = time.perf_counter()
+    try:
+        size = oracle.ref_compress_blob(vp, "u64", "var", stem)
+        how = (f"the reference's own compress (CPU partitioner) + serialize, "
+               f"{time.perf_counter() - t0:.1f} s")
+    except Exception as ex:  # no GPU or no harness: the oracle's restatement of the same path
+        s, e = oracle.ref_partition_cpu(values)
+        col = oracle.compress(values, starts=s, ends=e)
+        with open(bp, "wb") as f:
+            f.write(oracle.serialize(col))
+        size = col.reported_size()
+        how = f"the oracle's restatement of the reference's CPU partitioner and fit ({str(ex)[:80]})"
+    with open(meta_p, "w") as f:
+        json.dump({"size": size, "how": how}, f)
+    return values, bp, vp, size, how
 
 
 def run_reference_arm(args):
+    """The reference's own CPU path on this host: its host decoder directRandomAccessCPU
+    (api/G-LeCo.cuh:1337-1672), the only decoder it runs on host cores, over every position of
+    the same 200M-value column, on all host threads; one step = one pass over the column."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
     import oracle
-    n = min(args.n, 200_000_000)
-    threads = os.cpu_count() or 1
-    values = make_values(min(n, 16_000_000), 0)
-    # blob of the sample: the reference's own CPU partitioner (restated) and the format's fit
-    def make_blob(sample):
-        s, e = oracle.ref_partition_cpu(sample)
-        return oracle.serialize(oracle.compress(sample, starts=s, ends=e))
-    blob = make_blob(values)
-    maker = lambda sample: blob  # noqa: E731
-    results = []
-    for step in range(args.warmup + args.steps):
-        r = cpu_baseline_decode(values, maker, threads)
-        if step >= args.warmup:
-            results.append(r)
-    val = float(np.median([r["value"] for r in results]))
-    line = {"impl": "reference", "metric": METRIC, "value": val, "unit": UNIT, "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup,
-            # the whole workload (n values) at the rate measured on the sample
-            "ms_per_step": round(n * 8 / (val * 1e9) * 1e3, 3) if val else None,
-            "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "u64", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "values": n, "sample_values": len(values)},
-            "cpu_baseline": {**results[-1], "value": val},
-            "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    n = args.n
+    threads = host_threads()
+    values, bp, vp, ref_size, how = reference_blob(n, 42)
+    if oracle.ref_available():
+        secs, mism = oracle.ref_hostdecode_all(bp, vp, "u64", threads, args.warmup + args.steps)
+        kind = "reference"
+    else:  # the oracle port, one thread
+        with open(bp, "rb") as f:
+            col = oracle.deserialize(f.read(), "u64")
+        secs = []
+        for _ in range(args.warmup + args.steps):
+            t0 = time.perf_counter()
+            out = oracle.decode_full(col)
+            secs.append(time.perf_counter() - t0)
+        mism, threads, kind = int(np.count_nonzero(out != values)), 1, "port"
+    timed = secs[args.warmup:]
+    step_s = float(np.mean(timed))
+    val = n * 8 / step_s / 1e9
+    line = {"impl": "reference", "metric": METRIC, "value": round(val, 4), "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(step_s * 1e3, 3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "values": n, "ref_compressed_bytes": ref_size, "blob": how,
+                       "l2": "host decode; column larger than the host caches"},
+            "cpu_baseline": {"value": round(val, 4), "unit": UNIT, "cores": threads, "kind": kind,
+                             "sample": f"every step decodes all {n:,} values (directRandomAccessCPU over every "
+                                       f"position, {threads} host threads, wall clock per pass); values "
+                                       f"differing from the input: {mism}"},
+            "e2e": {"value": round(val, 4), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
 
@@ -397,6 +435,119 @@ def run_decode_i32(args):
     }
     print(json.dumps(line), flush=True)
     col.free()
+    ctx.close()
+    return 0
+
+
+def run_c1(args):
+    """The plain small workload: 1,048,576 int32 v[i] = 1000 i + U{0..255} (seed 42), fixed
+    partitions of 1024.  One step = compress from device memory + full decode + 10,000 uniform
+    lookups, each step's column freed outside the timed region; value = raw input GB/s of the step
+    (4 MiB / step time).  Roofline bytes: input read + compressed written (compress), compressed read +
+    4 B per value written (decode), 4 + 4 + 32 B per lookup.  cpu_baseline: the reference's host code
+    for the same step -- its CPU partitioner (one thread, as the reference runs it), then
+    directRandomAccessCPU over all values and over the 10,000 positions (the reference has no host
+    fit or pack)."""
+    import torch
+
+    import glc
+    from glc import workloads as W
+
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.Stream(dev)
+    torch.cuda.set_stream(stream)
+    sh = stream.cuda_stream
+    ctx = tuned_context(glc, local)
+    n, L, q = 1 << 20, 1024, 10_000
+    values = W.plain_small(n, seed=42)
+    pos = np.random.default_rng(42).integers(0, n, q).astype(np.int32)
+    d_in = torch.from_numpy(values).to(dev)
+    d_pos = torch.from_numpy(pos).to(dev)
+    out = torch.empty(n, dtype=torch.int32, device=dev)
+    look = torch.empty(q, dtype=torch.int32, device=dev)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+
+    def step():
+        ev[0].record(stream)
+        col = glc.compress_device(ctx, glc.I32, d_in.data_ptr(), n, glc.FIXED, fixed_len=L, stream=sh)
+        ev[1].record(stream)
+        glc.decompress_into(ctx, col, out.data_ptr(), glc.SRC_PACKED, stream=sh)
+        ev[2].record(stream)
+        glc.random_access_into(ctx, col, d_pos.data_ptr(), q, look.data_ptr(), source=glc.SRC_PACKED, fixed_len=L,
+                               stream=sh)
+        ev[3].record(stream)
+        torch.cuda.synchronize(dev)
+        t = [ev[0].elapsed_time(ev[1]), ev[1].elapsed_time(ev[2]), ev[2].elapsed_time(ev[3])]
+        return col, t
+
+    for _ in range(args.warmup):
+        step()[0].free()
+    ok = bool(torch.equal(out, d_in)) and bool(torch.equal(look, d_in[d_pos.long()]))
+    clocks = ClockSampler(dev)
+    clocks.start()
+    parts = []
+    for _ in range(args.steps):
+        col, t = step()
+        parts.append(t)
+        info = col.info()
+        col.free()
+    clk = clocks.stop()
+    parts = np.array(parts)
+    ms = float(parts.sum(axis=1).mean())
+    comp = info.compressed_size_bytes
+    algo = (4 * n + comp) + (comp + 4 * n) + 40 * q
+    peak, peak_kind = measured_peak()
+    # end to end through the reference-facing API: host values in, host values out
+    codec = glc.LeCoGPU(np.int32, device=local)
+    e2e = []
+    for k in range(args.e2e_steps + 1):
+        t0 = time.perf_counter()
+        c, _ = codec.compress(values, False, fixed_partition_size=L)
+        full = codec.decompressFullFile(c)
+        got = codec.randomAccessFixed(c, pos, L)
+        e2e.append(time.perf_counter() - t0)
+        c.free()
+    e2e_ok = bool(np.array_equal(full, values)) and bool(np.array_equal(got, values[pos]))
+    e2e_s = float(np.mean(e2e[1:]))
+    cpu = None
+    if not args.no_cpu_baseline:
+        import oracle
+        try:
+            with tempfile.TemporaryDirectory() as td:
+                t0 = time.perf_counter()
+                oracle.ref_partition(values, td)
+                part_s = time.perf_counter() - t0
+                blob = glc.serialize_host(ctx, glc.compress_device(ctx, glc.I32, values.ctypes.data, n, glc.FIXED,
+                                                                   fixed_len=L, host=True))
+                _, full_s = oracle.ref_hostdecode(blob, "i32", np.arange(n, dtype=np.int32), td, repeat=3)
+                _, ra_s = oracle.ref_hostdecode(blob, "i32", pos, td, repeat=3)
+            tot = part_s + full_s + ra_s
+            cpu = {"value": round(4 * n / tot / 1e9, 4), "unit": "GB/s", "cores": 1, "kind": "reference",
+                   "sample": f"the whole step on the reference's host code, one thread: CPU partitioner "
+                             f"{part_s * 1e3:.1f} ms (process run), directRandomAccessCPU over all values "
+                             f"{full_s * 1e3:.1f} ms and over the 10,000 positions {ra_s * 1e3:.2f} ms; the "
+                             f"reference has no host fit or pack"}
+        except Exception as ex:
+            cpu = {"value": None, "unit": "GB/s", "cores": 1, "kind": "reference", "sample": f"failed: {ex}"}
+    line = {
+        "metric": "C1 round trip GB/s (input)", "value": round(4 * n / (ms / 1e3) / 1e9, 3), "unit": "GB/s",
+        "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 4),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
+        "config": {"workload": "plain_i32_1M_fixed1024_compress_decode_10k_lookups", "values": n, "lookups": q,
+                   "partitions": info.num_partitions, "compressed_bytes": comp,
+                   "compress_ms": round(float(parts[:, 0].mean()), 4), "decode_ms": round(float(parts[:, 1].mean()), 4),
+                   "lookups_ms": round(float(parts[:, 2].mean()), 4), "bit_exact": ok and e2e_ok,
+                   "l2": "4 MiB column: L2-resident; the step is launch-latency bound"},
+        "roofline": {"bound": "hbm", "achieved": round(algo / (ms / 1e3) / 1e9, 1), "peak": peak, "unit": "GB/s",
+                     "frac": round(algo / (ms / 1e3) / 1e9 / peak, 4), "peak_kind": peak_kind, "traffic": None,
+                     "algorithmic_bytes": algo},
+        "e2e": {"value": round(4 * n / e2e_s / 1e9, 3), "unit": "GB/s", "h2d_bytes_per_step": 4 * n + 4 * q,
+                "d2h_bytes_per_step": 4 * n + 4 * q + 8},
+        "gpu_launches": (COMPRESS_LAUNCHES["fixed"] + 2) * args.steps, "clocks": clk, "cpu_baseline": cpu,
+    }
+    print(json.dumps(line), flush=True)
     ctx.close()
     return 0
 
@@ -1022,7 +1173,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--columns", type=int, default=4096, help="c4 batch: number of columns")
     ap.add_argument("--workload", default="c2_decode",
-                    choices=["c2_decode", "c3_random_access", "c4_batch", "c5_serving", "compress", "decode_i32"],
+                    choices=["c1_plain", "c2_decode", "c3_random_access", "c4_batch", "c5_serving", "compress",
+                             "decode_i32"],
                     help="c2_decode (headline): full decode of the 200M piecewise uint64 column; "
                          "c3_random_access: 100M lookups into a 64M int64 timestamp column")
     ap.add_argument("--mode", default="packed", choices=["packed", "preunpacked"], help="c3 residual source")
@@ -1042,6 +1194,8 @@ def main():
         args.warmup = 3
     if args.impl == "reference":
         return run_reference_arm(args)
+    if args.workload == "c1_plain":
+        return run_c1(args)
     if args.workload == "c3_random_access":
         return run_random_access(args)
     if args.workload == "c4_batch":
@@ -1119,7 +1273,7 @@ def main():
     algo_bytes = info.compressed_size_bytes + decoded_bytes
     achieved = algo_bytes / (ms / args.steps / 1e3) / 1e9
     peak, peak_kind = measured_peak()
-    tpv = profiled_traffic_per_value()
+    traffic = profiled_traffic(n)
 
     # end to end through the C ABI with host buffers: host blob -> device -> decode -> host
     blob = glc.serialize_host(ctx, col)
@@ -1152,11 +1306,9 @@ def main():
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
-            threads = 1
-            cpu = cpu_baseline_decode(values, lambda s: glc.serialize_host(
-                ctx, glc.compress_device(ctx, glc.U64, s.ctypes.data, len(s), glc.VARIABLE, host=True)), threads)
+            cpu = cpu_baseline_decode(blob, values, host_threads())
         except Exception as ex:  # reported, never fatal
-            cpu = {"value": None, "unit": UNIT, "cores": 1, "kind": "reference", "sample": f"failed: {ex}"}
+            cpu = {"value": None, "unit": UNIT, "cores": host_threads(), "kind": "reference", "sample": f"failed: {ex}"}
 
     if rank == 0:
         line = {
@@ -1172,7 +1324,7 @@ def main():
                        "compress_s": round(compress_s, 3), "bit_exact": ok and e2e_ok},
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 4), "peak_kind": peak_kind,
-                         "traffic": (round(tpv * n) if tpv else None),
+                         "traffic": traffic, "traffic_source": os.path.relpath(TRAFFIC_JSON, ROOT),
                          "algorithmic_bytes": algo_bytes},
             "e2e": {"value": round(e2e_value, 3), "unit": UNIT, "h2d_bytes_per_step": len(blob),
                     "d2h_bytes_per_step": decoded_bytes},

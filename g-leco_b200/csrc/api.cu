@@ -173,7 +173,8 @@ glc_status glc_create(glc_ctx** out, int device) {
   if (device < 0) {
     if ((e = cudaGetDevice(&device)) != cudaSuccess) { delete ctx; return GLC_ERR_CUDA; }
   }
-  if ((e = cudaSetDevice(device)) != cudaSuccess) { delete ctx; return GLC_ERR_CUDA; }
+  glc::DeviceScope device_scope(device);
+  if (!device_scope.ok()) { delete ctx; return GLC_ERR_CUDA; }
   ctx->device = device;
   if ((e = cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, device)) != cudaSuccess ||
       (e = cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking)) != cudaSuccess ||
@@ -194,7 +195,7 @@ glc_status glc_create(glc_ctx** out, int device) {
 
 glc_status glc_destroy(glc_ctx* ctx) {
   if (!ctx) return GLC_ERR_INVALID_ARG;
-  cudaSetDevice(ctx->device);
+  glc::DeviceScope device_scope(ctx->device);
   if (ctx->own_stream) cudaStreamSynchronize(ctx->own_stream);
   if (ctx->d_flags) cudaFree(ctx->d_flags);
   if (ctx->d_stats) cudaFree(ctx->d_stats);
@@ -213,7 +214,7 @@ glc_status glc_destroy(glc_ctx* ctx) {
 
 glc_status glc_sync(glc_ctx* ctx, glc_stream stream) {
   if (!ctx) return GLC_ERR_INVALID_ARG;
-  cudaSetDevice(ctx->device);
+  glc::DeviceScope device_scope(ctx->device);
   cudaStream_t s = pick(ctx, stream);
   CK(cudaStreamSynchronize(s), "sync");
   int code = 0;
@@ -228,7 +229,7 @@ glc_status glc_sync(glc_ctx* ctx, glc_stream stream) {
 glc_status glc_column_free(glc_column* col) {
   if (!col) return GLC_ERR_INVALID_ARG;
   if (col->view) return fail(col->ctx, GLC_ERR_INVALID_ARG, "a column of a batch is freed with its batch");
-  if (col->ctx) cudaSetDevice(col->ctx->device);
+  glc::DeviceScope device_scope(col->ctx ? col->ctx->device : -1);
   if (col->sync_free) cudaDeviceSynchronize();  // work on any stream may still read the arrays
   free_column_arrays(col);
   delete col;
@@ -290,6 +291,39 @@ static glc_status compress_impl(glc_ctx* ctx, glc_dtype dtype, const void* dev_v
     c->fixed_len = 0;
   }
   CK(alloc_meta(c, s), "compress: metadata allocation");
+  if (mode == GLC_PART_FIXED && fixed_compress_supported(n, fixed_len)) {
+    // one pass over the values: fit, widths, offsets, tables and words in one kernel; the words go
+    // to a worst-case buffer and the used ones into the column's exact-size array
+    uint32_t* wtmp = nullptr;
+    void* scratch = nullptr;
+    CK(pool_alloc(ctx, &wtmp, 4 * (size_t)fixed_compress_worst_words(dtype, n), s), "compress: word buffer");
+    cudaError_t e = pool_alloc(ctx, &scratch, fixed_compress_scratch_bytes(n), s);
+    if (e == cudaSuccess)
+      e = launch_fixed_compress(dtype, dev_values, c, fixed_len, wtmp, scratch, (unsigned long long*)ctx->d_stats, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(ctx->h_stats, ctx->d_stats, 3 * sizeof(int64_t), cudaMemcpyDeviceToHost, s);
+    if (scratch) cudaFreeAsync(scratch, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) {
+      cudaFreeAsync(wtmp, s);
+      return cuda_fail(ctx, e, "compress: one-pass fixed compression");
+    }
+    if (ctx->h_stats[2] != DEVERR_NONE) {
+      cudaFreeAsync(wtmp, s);
+      return fail(ctx, GLC_ERR_TIMEOUT, "compress: a device-side wait gave up");
+    }
+    c->total_bits = ctx->h_stats[0];
+    c->max_bits = (int32_t)ctx->h_stats[1];
+    set_word_counts(c);
+    e = col_alloc(c, &c->d_words, 4 * c->nwords_alloc, s);
+    if (e == cudaSuccess && c->nwords > 0)
+      e = cudaMemcpyAsync(c->d_words, wtmp, 4 * (size_t)c->nwords, cudaMemcpyDeviceToDevice, s);
+    if (e == cudaSuccess)
+      e = cudaMemsetAsync(c->d_words + c->nwords, 0, 4 * (size_t)(c->nwords_alloc - c->nwords), s);
+    cudaFreeAsync(wtmp, s);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "compress: words");
+    c->reported_size = reported_size(c->P, c->total_bits);
+    return GLC_OK;
+  }
   if (mode == GLC_PART_FIXED) {
     CK(launch_fixed_partitions(c->d_start, c->d_end, n, fixed_len, c->P, s), "compress: fixed partitions");
   } else {
@@ -332,7 +366,7 @@ glc_status glc_compress(glc_ctx* ctx, glc_dtype dtype, const void* values, int64
     return fail(ctx, GLC_ERR_INVALID_ARG, "fixed partition length must be positive");
   if (!(flags & GLC_HOST_IN) && ((uintptr_t)values % dtype_size(dtype)) != 0)
     return fail(ctx, GLC_ERR_INVALID_ARG, "device values must be aligned to the element size");
-  cudaSetDevice(ctx->device);
+  glc::DeviceScope device_scope(ctx->device);
   cudaStream_t s = pick(ctx, stream);
   glc_column* c = new (std::nothrow) glc_column();
   if (!c) return fail(ctx, GLC_ERR_OOM, "host allocation");
@@ -384,7 +418,7 @@ static glc_status partition_only(glc_ctx* ctx, glc_dtype dtype, const void* valu
                                  int64_t* num_partitions, glc_stream stream) {
   if (!ctx || !num_partitions) return fail(ctx, GLC_ERR_INVALID_ARG, "null argument");
   if (!valid_dtype(dtype) || n < 0 || n > 0x7fffffffll) return fail(ctx, GLC_ERR_INVALID_ARG, "bad dtype or n");
-  cudaSetDevice(ctx->device);
+  glc::DeviceScope device_scope(ctx->device);
   cudaStream_t s = pick(ctx, stream);
   *num_partitions = 0;
   if (n == 0) return GLC_OK;
@@ -456,13 +490,14 @@ static glc_status resolve_source(glc_ctx* ctx, const glc_column* c, glc_source s
 glc_status glc_decompress_range(glc_ctx* ctx, const glc_column* col, glc_source source, int64_t first, int64_t count,
                                 void* out, int flags, glc_stream stream) {
   if (!ctx || !col) return fail(ctx, GLC_ERR_INVALID_ARG, "null argument");
-  if (first < 0 || count < 0 || first + count > col->n) return fail(ctx, GLC_ERR_INVALID_ARG, "range outside the column");
+  if (first < 0 || count < 0 || first > col->n || count > col->n - first)  // no signed overflow for any count
+    return fail(ctx, GLC_ERR_INVALID_ARG, "range outside the column");
   if (count == 0) return GLC_OK;
   if (!out) return fail(ctx, GLC_ERR_INVALID_ARG, "null output");
   int plain = 0;
   glc_status st = resolve_source(ctx, col, source, &plain);
   if (st != GLC_OK) return st;
-  cudaSetDevice(ctx->device);
+  glc::DeviceScope device_scope(ctx->device);
   cudaStream_t s = pick(ctx, stream);
   const size_t es = dtype_size(col->dtype);
   // The kernel writes value e at base + e with 16-byte stores, so base must be 16-byte aligned.
@@ -504,7 +539,7 @@ glc_status glc_random_access(glc_ctx* ctx, const glc_column* col, glc_source sou
   int plain = 0;
   glc_status st = resolve_source(ctx, col, source, &plain);
   if (st != GLC_OK) return st;
-  cudaSetDevice(ctx->device);
+  glc::DeviceScope device_scope(ctx->device);
   cudaStream_t s = pick(ctx, stream);
   const size_t es = dtype_size(col->dtype);
   const int32_t* dpos = positions;
@@ -532,7 +567,7 @@ glc_status glc_preunpack(glc_ctx* ctx, glc_column* col, int drop_packed, glc_str
   if (col->n == 0) return GLC_OK;
   if (!col->d_plain) {
     if (!col->d_words) return fail(ctx, GLC_ERR_UNSUPPORTED, "column has no packed bitstream");
-    cudaSetDevice(ctx->device);
+    glc::DeviceScope device_scope(ctx->device);
     cudaStream_t s = pick(ctx, stream);
     CK(col_alloc(col, &col->d_plain, 8 * col->n + 16, s), "pre-unpack: allocation");  // +16: 16-byte TMA granules
     CK(cudaMemsetAsync((char*)col->d_plain + 8 * col->n, 0, 16, s), "pre-unpack: padding");
@@ -572,7 +607,7 @@ glc_status glc_serialize(glc_ctx* ctx, const glc_column* c, void* blob, uint64_t
   BlobHeader t = h;
   t.checksum = 0;
   h.checksum = header_checksum((const uint8_t*)&t, sizeof t, crc32c);
-  cudaSetDevice(ctx->device);
+  glc::DeviceScope device_scope(ctx->device);
   cudaStream_t s = pick(ctx, stream);
   const bool host = (flags & GLC_HOST_OUT) != 0;
   uint8_t* b = (uint8_t*)blob;
@@ -620,7 +655,7 @@ glc_status glc::deserialize_column(glc_ctx* ctx, glc_dtype dtype, const void* bl
   *out = nullptr;
   if (!valid_dtype(dtype)) return fail(ctx, GLC_ERR_INVALID_ARG, "unknown dtype");
   if (!blob || size < sizeof(BlobHeader)) return fail(ctx, GLC_ERR_BAD_BLOB, "blob shorter than its header");
-  cudaSetDevice(ctx->device);
+  glc::DeviceScope device_scope(ctx->device);
   cudaStream_t s = pick(ctx, stream);
   const bool host = (flags & GLC_HOST_IN) != 0;
   BlobHeader h;
@@ -753,7 +788,7 @@ extern "C" glc_status glc_decode_blob_to_host(glc_ctx* ctx, glc_dtype dtype, con
                                               int crc32c, void* out, glc_column** col_out, glc_stream stream) {
   if (!ctx || !blob || (!out && !col_out)) return fail(ctx, GLC_ERR_INVALID_ARG, "null argument");
   if (col_out) *col_out = nullptr;
-  cudaSetDevice(ctx->device);
+  glc::DeviceScope device_scope(ctx->device);
   cudaStream_t up = pick(ctx, stream);
   // metadata, checks and lookup tables; the bitstream follows in chunks below
   glc_column* c = nullptr;

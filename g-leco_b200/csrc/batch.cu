@@ -523,7 +523,7 @@ glc_status glc_batch_create(glc_ctx* ctx, glc_column* const* cols, int32_t ncols
     if (!cols[i]) { delete b; return bfail(ctx, GLC_ERR_INVALID_ARG, "null column in batch"); }
     b->cols.push_back(cols[i]);
   }
-  cudaSetDevice(ctx->device);
+  glc::DeviceScope device_scope(ctx->device);
   glc_status st = finish_batch(ctx, b, ctx->own_stream);
   if (st != GLC_OK) { free_batch(b); return st; }
   *out = b;
@@ -541,7 +541,7 @@ glc_status glc_batch_compress(glc_ctx* ctx, const glc_dtype* dtypes, const void*
     if (dtypes[i] < GLC_I32 || dtypes[i] > GLC_U32 || ns[i] < 0 || ns[i] > 0x7fffffffll || (ns[i] > 0 && !values[i]))
       return bfail(ctx, GLC_ERR_INVALID_ARG, "bad column in batch");
   }
-  cudaSetDevice(ctx->device);
+  glc::DeviceScope device_scope(ctx->device);
   cudaStream_t s = stream ? (cudaStream_t)stream : ctx->own_stream;
   glc_batch* b = new (std::nothrow) glc_batch();
   if (!b) return GLC_ERR_OOM;
@@ -737,7 +737,7 @@ glc_status glc_batch_column(const glc_batch* b, int32_t i, glc_column** col) {
 
 glc_status glc_batch_decompress(glc_ctx* ctx, glc_batch* b, void* const* outs, int use_graph, glc_stream stream) {
   if (!ctx || !b || (!outs && !b->cols.empty())) return bfail(ctx, GLC_ERR_INVALID_ARG, "bad batch arguments");
-  cudaSetDevice(ctx->device);
+  glc::DeviceScope device_scope(ctx->device);
   cudaStream_t s = stream ? (cudaStream_t)stream : ctx->own_stream;
   glc_status st = build_work(ctx, b, outs, s);
   if (st != GLC_OK) return st;
@@ -771,7 +771,7 @@ glc_status glc_batch_decompress(glc_ctx* ctx, glc_batch* b, void* const* outs, i
 
 glc_status glc_batch_free(glc_batch* b) {
   if (!b) return GLC_ERR_INVALID_ARG;
-  cudaSetDevice(b->ctx->device);
+  glc::DeviceScope device_scope(b->ctx->device);
   cudaDeviceSynchronize();
   free_batch(b);
   return GLC_OK;

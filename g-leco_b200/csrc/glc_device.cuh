@@ -59,7 +59,9 @@ template <> __device__ __forceinline__ int64_t sat_cast<int64_t>(double r) { ret
 template <> __device__ __forceinline__ uint64_t sat_cast<uint64_t>(double r) { return __double2ull_rz(r); }
 template <> __device__ __forceinline__ uint32_t sat_cast<uint32_t>(double r) { return __double2uint_rz(r); }
 
-// round-half-away-from-zero(x) == trunc(x + copysign(0.5 - 2^-54, x)) for every double x under
+// Rounding half away from zero by adding the predecessor of 0.5 and truncating: the method of the
+// fix of Java's Math.round (OpenJDK bug 6430675, floor(x + 0.49999999999999994)), applied here to
+// both signs.  round-half-away-from-zero(x) == trunc(x + copysign(0.5 - 2^-54, x)) for every double x under
 // round-to-nearest-even addition: with k = trunc(|x|) and f = |x| - k, the sum stays below k + 1
 // when f < 0.5 (it falls short of k + 1 by more than half an ulp) and reaches k + 1 when
 // f >= 0.5 (at f = 0.5 in [0.5, 1) it is the tie 1 - 2^-54, which rounds to even, 1.0); values of

@@ -136,6 +136,30 @@ inline int current_device() {
   return cudaGetDevice(&d) == cudaSuccess ? d : -1;
 }
 
+// Makes `dev` the calling thread's current device for the scope and gives the caller's device
+// back at its end, so that no entry point leaves the thread's device switched.  dev < 0: no change.
+class DeviceScope {
+ public:
+  explicit DeviceScope(int dev) {
+    if (dev < 0) return;
+    int cur = -1;
+    if (cudaGetDevice(&cur) != cudaSuccess) cur = -1;
+    if (cur == dev) return;
+    ok_ = cudaSetDevice(dev) == cudaSuccess;
+    if (ok_ && cur >= 0) prev_ = cur;
+  }
+  ~DeviceScope() {
+    if (prev_ >= 0) cudaSetDevice(prev_);
+  }
+  bool ok() const { return ok_; }
+  DeviceScope(const DeviceScope&) = delete;
+  DeviceScope& operator=(const DeviceScope&) = delete;
+
+ private:
+  int prev_ = -1;
+  bool ok_ = true;
+};
+
 // Stream-ordered temporary allocation from the context's pool.
 template <typename P> inline cudaError_t pool_alloc(glc_ctx* ctx, P** p, size_t bytes, cudaStream_t s) {
   return cudaMallocFromPoolAsync((void**)p, bytes, ctx->pool, s);
@@ -149,6 +173,12 @@ size_t fit_scratch_bytes(const int32_t* unused, int64_t n, int64_t P);
 cudaError_t launch_fit(glc_dtype dt, const void* values, glc_column* c, void* scratch, size_t scratch_bytes,
                        int64_t* d_stats, cudaStream_t s);
 cudaError_t launch_desc_and_tiles(glc_column* c, cudaStream_t s);
+// compress_fixed.cu: one-pass compression of fixed partitions of L values, L a divisor of 4096 and >= 256
+bool fixed_compress_supported(int64_t n, int32_t L);
+int64_t fixed_compress_worst_words(glc_dtype dt, int64_t n);
+size_t fixed_compress_scratch_bytes(int64_t n);
+cudaError_t launch_fixed_compress(glc_dtype dt, const void* values, glc_column* c, int32_t L, uint32_t* words,
+                                  void* scratch, unsigned long long* stats, cudaStream_t s);
 cudaError_t launch_validate(const glc_column* c, int* d_bad, cudaStream_t s);
 cudaError_t launch_max_bits(const glc_column* c, int64_t* d_out, cudaStream_t s);
 // pack.cu: one column's arrays for the packer

@@ -56,15 +56,17 @@ cudaError_t scratch_for_device(int dev, unsigned char** ptr, int* num_sms) {
 extern "C" glc_status glc_decompress_range_noalloc(const glc_column* col, int64_t first, int64_t count,
                                                      void* host_out, glc_stream stream) {
   if (!col) return GLC_ERR_INVALID_ARG;
-  if (first < 0 || count < 0 || first + count > col->n) return GLC_ERR_INVALID_ARG;
+  const size_t es = (size_t)glc::dtype_size(col->dtype);
+  // the size limit first: then count * es cannot overflow, nor can the range test below
+  if (count < 0 || (uint64_t)count > (uint64_t)GLC_NOALLOC_MAX_OUTPUT_BYTES / es) return GLC_ERR_INVALID_ARG;
+  if (first < 0 || first > col->n || count > col->n - first) return GLC_ERR_INVALID_ARG;
   if (count == 0) return GLC_OK;
   if (!host_out) return GLC_ERR_INVALID_ARG;
-  const size_t es = (size_t)glc::dtype_size(col->dtype);
-  if ((size_t)count * es > (size_t)GLC_NOALLOC_MAX_OUTPUT_BYTES) return GLC_ERR_INVALID_ARG;  // larger than the array
   if (!col->d_words) return GLC_ERR_UNSUPPORTED;
   int dev = col->ctx ? col->ctx->device : 0;
   if (dev < 0 || dev >= kMaxDevices) return GLC_ERR_INVALID_ARG;
-  if (cudaSetDevice(dev) != cudaSuccess) return GLC_ERR_CUDA;
+  glc::DeviceScope device_scope(dev);  // the caller's current device is given back on return
+  if (!device_scope.ok()) return GLC_ERR_CUDA;
   cudaStream_t s = stream ? (cudaStream_t)stream : (col->ctx ? col->ctx->own_stream : nullptr);
   unsigned char* scratch = nullptr;
   int num_sms = 0;

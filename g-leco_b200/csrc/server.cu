@@ -519,7 +519,7 @@ glc_status glc_server_create(glc_ctx* ctx, const glc_server_config* config, glc_
                         sizeof(RARequest) * (size_t)c.max_requests + sizeof(BatchWork) * (size_t)c.max_requests +
                         sizeof(int64_t) * ((size_t)c.max_requests + 1) + 48 + sizeof(BatchWork) * (size_t)S->max_work);
   S->stage_cap = (size_t)c.max_range_values * 8 + 16 * (size_t)c.max_requests + 256;
-  cudaSetDevice(ctx->device);
+  glc::DeviceScope device_scope(ctx->device);
   cudaError_t e = cudaSuccess;
   for (int i = 0; i < c.slots && e == cudaSuccess; i++) {
     Slot& sl = S->slots[i];
@@ -581,7 +581,7 @@ glc_status glc_server_destroy(glc_server* S) {
   }
   S->wake.notify_all();
   if (S->worker.joinable()) S->worker.join();
-  cudaSetDevice(S->ctx->device);
+  glc::DeviceScope device_scope(S->ctx->device);
   for (int i = 0; i < kMaxSlots; i++)
     if (S->slots[i].stream) cudaStreamSynchronize(S->slots[i].stream);
   free_pending(S);
@@ -699,7 +699,8 @@ glc_status glc_server_submit(glc_server* S, const glc_request* reqs, int32_t cou
       const uintptr_t es = col_ok ? (uintptr_t)dtype_size(S->cols[q.column].col->dtype) : 1;
       if (ok) ok = ((uintptr_t)q.out % es) == 0;
       if (ok && q.kind == GLC_REQ_LOOKUP) ok = q.positions != nullptr && ((uintptr_t)q.positions & 3) == 0;
-      if (ok && q.kind == GLC_REQ_RANGE) ok = q.first >= 0 && q.first + q.count <= S->cols[q.column].col->n;
+      if (ok && q.kind == GLC_REQ_RANGE)
+        ok = q.first >= 0 && q.first <= S->cols[q.column].col->n && q.count <= S->cols[q.column].col->n - q.first;
       if (!ok) return sfail(S->ctx, GLC_ERR_INVALID_ARG, "server submit: invalid request (nothing queued)");
     }
     for (int32_t i = 0; i < count; i++) {

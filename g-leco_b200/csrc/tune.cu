@@ -183,7 +183,7 @@ glc_status glc_tune_set(glc_ctx* ctx, glc_dtype dtype, int32_t field_bits, int32
 glc_status glc_autotune(glc_ctx* ctx, const char* cache_path, int32_t flags) {
   if (!ctx || (flags & ~GLC_TUNE_FORCE) != 0) return GLC_ERR_INVALID_ARG;
   if (cache_path && !(flags & GLC_TUNE_FORCE) && tune_load(ctx, cache_path)) return GLC_OK;
-  cudaSetDevice(ctx->device);
+  glc::DeviceScope device_scope(ctx->device);
   cudaStream_t s = ctx->own_stream;
   void* vals = nullptr;
   void* out = nullptr;

@@ -281,7 +281,15 @@ def decompress_range_into(ctx: Context, col: Column, first: int, count: int, out
 
 def decompress_range_noalloc(col: Column, first: int, count: int, out: np.ndarray, stream: int = 0) -> int:
     """glc_decompress_range_noalloc: values [first, first+count) into the host array ``out``
-    without any allocation; returns the glc status (the caller checks it)."""
+    without any allocation; returns the glc status (the caller checks it).  ``out`` must be a
+    C-contiguous array of the column's element size holding at least ``count`` elements
+    (ValueError otherwise: the C call would write past a shorter buffer)."""
+    if not isinstance(out, np.ndarray) or not out.flags.c_contiguous:
+        raise ValueError("out must be a C-contiguous numpy array")
+    if out.itemsize != np.dtype(NP_DTYPE[col.dtype]).itemsize:
+        raise ValueError("out's element size differs from the column's")
+    if count > 0 and out.size < count:
+        raise ValueError("out holds fewer than count elements")
     return col.ctx.lib.glc_decompress_range_noalloc(col.handle, first, count, ctypes.c_void_p(out.ctypes.data),
                                                     ctypes.c_void_p(stream))
 

@@ -84,6 +84,9 @@ def _declare(L):
     L.orc_decode_full.argtypes = [c_int, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_i64, c_vp, c_i64, c_i64, c_vp]
     L.orc_random_access.restype = c_int
     L.orc_random_access.argtypes = [c_int, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_i64, c_vp, c_i64, c_vp, c_i64, c_vp]
+    L.orc_decode_variant.restype = c_int
+    L.orc_decode_variant.argtypes = [c_int, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_i64, c_vp, c_i64, c_vp, c_i64, c_int,
+                                     c_vp]
     L.orc_unpack_deltas.restype = c_int
     L.orc_unpack_deltas.argtypes = [c_int, c_vp, c_vp, c_vp, c_vp, c_vp, c_i64, c_vp, c_i64, c_i64, c_vp]
     L.orc_decode_preunpacked.restype = c_int
@@ -280,6 +283,24 @@ def random_access(col: Column, positions: np.ndarray) -> np.ndarray:
     return out
 
 
+# prediction variants of the reference's decoders (glc_oracle.cpp PredVariant)
+PRED_CONTRACT = 0          # fma, round half away: every full decoder and packed random access
+PRED_HOST = 1              # directRandomAccessCPU (api/G-LeCo.cuh:1470-1646): no fma
+PRED_FIXED_PREUNPACKED = 2  # randomAccessFixedPreUnpackedKernel (FixedPartitionKernels.cuh:185-206): ties to even
+
+
+def decode_variant(col: Column, positions: np.ndarray, variant: int) -> np.ndarray:
+    """Values that the reference decoder named by ``variant`` returns at ``positions``."""
+    code, npdt = DTYPES[col.dtype]
+    pos = np.ascontiguousarray(positions, np.int32)
+    out = np.zeros(len(pos), npdt)
+    w = _words_padded(col)
+    lib().orc_decode_variant(code, _p(col.starts), _p(col.ends), _p(col.types), _p(col.params), _p(col.bits),
+                             _p(col.offsets), col.num_partitions, _p(w), len(col.words), _p(pos), len(pos), variant,
+                             _p(out))
+    return out
+
+
 def unpack_deltas(col: Column) -> np.ndarray:
     """decompression/UnpackKernel.cuh:31-98."""
     code, _ = DTYPES[col.dtype]
@@ -404,3 +425,60 @@ def ref_hostdecode(blob: bytes, dtype: str, positions: np.ndarray, workdir: str,
     np.ascontiguousarray(positions, np.int32).tofile(ppath)
     secs = float(_ref_run(["hostdecode", dtype, bpath, ppath, opath, repeat]).strip().splitlines()[-1])
     return np.fromfile(opath, DTYPES[dtype][1]), secs
+
+
+def ref_compress_blob(values_path: str, dtype: str, how: str, blob_prefix: str) -> int:
+    """The reference's own stock LeCoGPU<T>::compress (fixed TILE_SIZE, its CPU partitioner
+    ("var") or its GPU partitioner ("v6"), api/G-LeCo.cuh:349) + serialize (:826) of the raw
+    values in ``values_path``, run from the compiled reference on a GPU.  Writes
+    ``blob_prefix + ".blob"`` and returns the compressed size the reference reports."""
+    return int(_ref_run(["golden", dtype, values_path, blob_prefix, how], cpu_only=False).strip().splitlines()[-1])
+
+
+def ref_hostdecode_all(blob_path: str, values_path: str, dtype: str, threads: int, passes: int,
+                       mism_path: str = None):
+    """The reference's directRandomAccessCPU over every position of a blob, split across
+    ``threads`` host threads; returns (seconds of each pass, values differing from the input)."""
+    args = ["hostdecode_all", dtype, blob_path, values_path, threads, passes] + ([mism_path] if mism_path else [])
+    lines = _ref_run(args).strip().splitlines()
+    secs = [float(ln.split()[1]) for ln in lines if ln.startswith("pass ")]
+    return secs, int(lines[-1].split()[1])
+
+
+def ref_gpudecode(blob: bytes, values: np.ndarray, dtype: str, workdir: str, repeat: int = 1) -> dict:
+    """The reference's own full decoders (deserializeGPU + _BitPacked, _OnTheFly_Optimized_V2,
+    _WorkStealingAdvanced, and deserializeGPU(blob, true) + _PreUnpacked; api/G-LeCo.cuh:1739,
+    :1842, :220, :1790) on a GPU: {decoder: (best API seconds, values differing from ``values``)}."""
+    bp = os.path.join(workdir, "gd_blob.bin")
+    vp = os.path.join(workdir, "gd_values.bin")
+    with open(bp, "wb") as f:
+        f.write(blob)
+    np.ascontiguousarray(values).tofile(vp)
+    res = {}
+    for ln in _ref_run(["gpudecode", dtype, bp, vp, repeat], cpu_only=False).strip().splitlines():
+        parts = ln.split()
+        if len(parts) == 3 and parts[0].startswith("decompressFullFile"):
+            res[parts[0]] = (float(parts[1]), int(parts[2]))
+    return res
+
+
+def ref_gpura(blob: bytes, values: np.ndarray, positions: np.ndarray, dtype: str, partition_len: int, workdir: str,
+              repeat: int = 1) -> dict:
+    """The reference's own random access on a GPU (randomAccessFixed when partition_len > 0,
+    decompress, and on a pre-unpacked deserialization randomAccessPreUnpacked and, when
+    partition_len > 0, randomAccessFixedPreUnpacked; api/G-LeCo.cuh:1878, :615, :696, :1931):
+    {method: output array}."""
+    bp = os.path.join(workdir, "ra_blob.bin")
+    pp = os.path.join(workdir, "ra_pos.bin")
+    vp = os.path.join(workdir, "ra_values.bin")
+    prefix = os.path.join(workdir, "ra_out")
+    with open(bp, "wb") as f:
+        f.write(blob)
+    np.ascontiguousarray(positions, np.int32).tofile(pp)
+    np.ascontiguousarray(values).tofile(vp)
+    out = {}
+    for ln in _ref_run(["gpura", dtype, bp, pp, vp, partition_len, repeat, prefix], cpu_only=False).strip().splitlines():
+        parts = ln.split()
+        if len(parts) == 3 and not parts[0][0].isdigit():
+            out[parts[0]] = np.fromfile(f"{prefix}.{parts[0]}.bin", DTYPES[dtype][1])
+    return out

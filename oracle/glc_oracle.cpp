@@ -275,6 +275,44 @@ template <typename T> T decode_one(const int32_t* starts, const int32_t* types, 
   return apply_delta<T>(pred, d);
 }
 
+// Prediction variants of the reference's decoders that depart from the format's contract
+// (fma, round half away from zero).  They exist only to predict, value for value, what those
+// decoders return on a blob, so that a test can compare the reference's output exactly.
+enum PredVariant {
+  PV_FMA_HALF_AWAY = 0,  // every full decoder and packed random access (the contract, predict<T>)
+  // directRandomAccessCPU (api/G-LeCo.cuh:1470-1646): theta0 + theta1 * i as two separately
+  // rounded operations (x86-64 host code, no fma unit assumed), clamps for 4-byte types and
+  // unsigned types below zero, then static_cast<T>(std::round(p)).
+  PV_SUM_HALF_AWAY = 1,
+  // randomAccessFixedPreUnpackedKernel (decompression/FixedPartitionKernels.cuh:185-206):
+  // __fma_rn, then __double2int_rn / __double2uint_rn after clamping (4-byte types) or
+  // __double2ll_rn (8-byte types): round half to EVEN, saturating.
+  PV_FMA_HALF_EVEN = 2,
+};
+
+template <typename T> T predict_variant(double theta0, double theta1, int64_t i, int variant) {
+  if (variant == PV_FMA_HALF_AWAY) return predict<T>(theta0, theta1, i);
+  if (variant == PV_SUM_HALF_AWAY) {
+    double p = theta0 + theta1 * (double)i;  // -ffp-contract=off: two roundings
+    if (!TypeInfo<T>::is_signed) {
+      if (p < 0) p = 0;
+      else if (sizeof(T) == 4 && p > 4294967295.0) p = 4294967295.0;
+    } else if (sizeof(T) == 4) {
+      if (p > 2147483647.0) p = 2147483647.0;
+      else if (p < -2147483648.0) p = -2147483648.0;
+    }
+    // out-of-range 8-byte casts are undefined in C++; in-range values are exact either way
+    return sat_cast<T>(std::round(p));
+  }
+  double p = std::fma(theta1, (double)i, theta0);
+  double r = std::nearbyint(p);  // default rounding mode: nearest, ties to even
+  if (sizeof(T) == 4) {
+    if (!TypeInfo<T>::is_signed) return (T)sat_cast<uint32_t>(std::nearbyint(std::fmax(0.0, std::fmin(p, 4294967295.0))));
+    return (T)sat_cast<int32_t>(std::nearbyint(std::fmax(-2147483648.0, std::fmin(p, 2147483647.0))));
+  }
+  return (T)sat_cast<int64_t>(r);  // __double2ll_rn saturates to the int64 range, then static_cast<T>
+}
+
 // Partition of a position by binary search over [start, end) (RandomAccessKernels.cuh:55-169).
 int find_partition(const int32_t* starts, const int32_t* ends, int P, int64_t pos) {
   int lo = 0, hi = P - 1;
@@ -769,6 +807,30 @@ int orc_random_access(int dtype, const int32_t* starts, const int32_t* ends, con
     for (int64_t k = 0; k < q; k++) {
       int p = find_partition(starts, ends, (int)P, pos[k]);
       o[k] = (p < 0) ? (T)0 : decode_one<T>(starts, types, params, bits, offs, words, nwords, p, pos[k]);
+    }
+  });
+  return 0;
+}
+
+// What one of the reference's decoders returns at each position (see PredVariant): the same
+// residual field and direct-copy rule as decode_one, with that decoder's prediction.  0 for
+// positions outside the column.
+int orc_decode_variant(int dtype, const int32_t* starts, const int32_t* ends, const int32_t* types,
+                       const double* params, const int32_t* bits, const int64_t* offs, int64_t P,
+                       const uint32_t* words, int64_t nwords, const int32_t* pos, int64_t q, int variant, void* out) {
+  DISPATCH(dtype, {
+    T* o = (T*)out;
+    for (int64_t k = 0; k < q; k++) {
+      int p = find_partition(starts, ends, (int)P, pos[k]);
+      if (p < 0) { o[k] = (T)0; continue; }
+      int64_t local = (int64_t)pos[k] - starts[p];
+      int b = bits[p];
+      if (types[p] == M_DIRECT) {
+        o[k] = b <= 0 ? (T)0 : (T)get_bits(words, nwords, offs[p] + local * b, b);
+        continue;
+      }
+      long long d = b > 0 ? sign_extend(get_bits(words, nwords, offs[p] + local * b, b), b) : 0;
+      o[k] = apply_delta<T>(predict_variant<T>(params[4 * (int64_t)p], params[4 * (int64_t)p + 1], local, variant), d);
     }
   });
   return 0;

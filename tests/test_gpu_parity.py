@@ -47,6 +47,20 @@ def _data(kind: str, n: int, seed: int = 1):
         v[:: 5] = np.iinfo(np.int32).max
         v[2:: 5] = np.iinfo(np.int32).min
         return v
+    if kind == "i64_runs":  # runs of whole constant tiles between noisy ones: tiles without bits,
+        # and tile boundaries in the middle of a word (odd widths)
+        v = np.zeros(n, np.int64)
+        pos = 0
+        while pos < n:
+            run = int(rng.integers(1, 4)) * 4096 + int(rng.integers(0, 3)) * 1024
+            if rng.random() < 0.5:
+                v[pos:pos + run] = rng.integers(-10 ** 12, 10 ** 12)
+            else:
+                w = int(rng.choice([1, 3, 5, 7, 13]))
+                seg = v[pos:pos + run]
+                v[pos:pos + run] = 12345 * np.arange(len(seg)) + rng.integers(0, 1 << w, len(seg))
+            pos += run
+        return v
     if kind == "u32_extreme":
         v = rng.integers(0, 2 ** 32, n, dtype=np.int64).astype(np.uint32)
         v[:: 3] = np.iinfo(np.uint32).max
@@ -56,7 +70,7 @@ def _data(kind: str, n: int, seed: int = 1):
 
 
 KINDS = ["i32_linear", "i32_neg", "i64_walk", "i64_extreme", "u64_piecewise", "u64_big", "u32_noise", "u32_const",
-         "timestamps"]
+         "timestamps", "i64_runs"]
 
 
 def _codec(values):
@@ -73,7 +87,10 @@ def _check_column(codec, col, values, oracle_col, oracle):
 
 @pytest.mark.parametrize("kind", KINDS)
 @pytest.mark.parametrize("n,L", [(100_003, 1024), (65_536, 4096), (5_000, 128), (777, 1000), (20_000, 6000),
-                                 (50_001, 10_000)])
+                                 (50_001, 10_000),
+                                 # lengths that divide the 4096-value tile (>= 256): the one-pass kernel
+                                 (1, 4096), (255, 256), (4_097, 256), (300_001, 512), (123_457, 2048),
+                                 (4096 * 37 + 5, 4096), (1 << 20, 1024)])
 def test_fixed_compress_bit_exact(oracle, kind, n, L):
     v = _data(kind, n)
     codec = _codec(v)
@@ -275,6 +292,27 @@ def test_piecewise_scale_roundtrip(oracle, n):
     s, e = oracle.ref_partition_cpu(v)
     ref_size = oracle.compress(v, starts=s, ends=e).reported_size()
     assert size <= ref_size * 1.01, (size, ref_size)
+
+
+def test_c1_plain_config(oracle):
+    """The plain small workload at its stated size: 1,048,576 int32 v[i] = 1000 i + U{0..255}
+    (seed 42), fixed partitions of 1024: the device blob equals the oracle's byte for byte, the
+    full decode and 10,000 uniform lookups (fixed-length and binary-search paths) are exact, and
+    the variable partitioning stays within 1% of the size of the reference partitioner's layout."""
+    v = W.plain_small(1 << 20, seed=42)
+    codec = _codec(v)
+    col, size = codec.compress(v, False, fixed_partition_size=1024)
+    ocol = oracle.compress(v, "fixed", 1024)
+    assert size == ocol.reported_size() and col.info().num_partitions == 1024
+    assert codec.serialize(col) == oracle.serialize(ocol)
+    assert np.array_equal(codec.decompressFullFile(col), v)
+    pos = np.random.default_rng(42).integers(0, len(v), 10_000).astype(np.int32)
+    assert np.array_equal(codec.randomAccessFixed(col, pos, 1024), v[pos])
+    assert np.array_equal(codec.decompress(col, pos), v[pos])
+    vcol, vsize = codec.compress(v, True)
+    assert np.array_equal(codec.decompressFullFile(vcol), v)
+    s, e = oracle.ref_partition_cpu(v)
+    assert vsize <= 1.01 * oracle.compress(v, starts=s, ends=e).reported_size()
 
 
 def test_cpp_dropin_caller():
