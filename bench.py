@@ -91,15 +91,17 @@ except Exception:
 get = getattr(pynvml, "nvmlDeviceGetCurrentClocksEventReasons", None) or pynvml.nvmlDeviceGetCurrentClocksThrottleReasons
 print("max", pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM), flush=True)
 while True:
-    print(pynvml.nvmlDeviceGetClockInfo(h, pynvml.NVML_CLOCK_SM), int(get(h)), flush=True)
-    time.sleep(0.002)
+    print(time.monotonic_ns(), pynvml.nvmlDeviceGetClockInfo(h, pynvml.NVML_CLOCK_SM), int(get(h)), flush=True)
+    time.sleep(0.0002)
 """
 
 
 class ClockSampler:
     """SM clock and clock-event (throttle) reasons of the benchmarked GPU, sampled through NVML
-    every 2 ms by a separate process while the timed region runs (reads only; no GPU setting is
-    changed)."""
+    about every 0.3 ms by a separate process (reads only; no GPU setting is changed).  begin() and
+    end() mark the timed region on the host's monotonic clock (both sides synchronised with the
+    device); the summary keeps the samples inside it, or the nearest one on each side when the
+    region is shorter than the sampling interval."""
 
     REASONS = {0x8: "hw_slowdown", 0x40: "hw_thermal_slowdown", 0x20: "sw_thermal_slowdown",
                0x4: "sw_power_cap", 0x80: "hw_power_brake_slowdown"}
@@ -107,6 +109,7 @@ class ClockSampler:
     def __init__(self, torch_device):
         self.dev = torch_device
         self.proc = None
+        self.t_begin = self.t_end = None
 
     def start(self):
         import torch
@@ -121,28 +124,50 @@ class ClockSampler:
             idx = int(vis.split(",")[idx])
         self.proc = subprocess.Popen([sys.executable, "-c", _SAMPLER, uuid, str(idx)], stdout=subprocess.PIPE,
                                      stderr=subprocess.DEVNULL, text=True)
-        self.max_line = self.proc.stdout.readline()  # the sampler is up before the timed region starts
+        self.max_line = self.proc.stdout.readline()
+        self.first_line = self.proc.stdout.readline()  # sampling runs before the timed region starts
+
+    def begin(self):
+        self.t_begin = time.monotonic_ns()
+
+    def end(self):
+        self.t_end = time.monotonic_ns()
 
     def stop(self):
         if self.proc is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "error": "sampler not started"}
+        if self.t_end is not None:
+            time.sleep(0.002)  # a sample after the region
         self.proc.terminate()
         out, _ = self.proc.communicate(timeout=10)
-        sm, reasons = [], set()
-        for ln in out.splitlines():
+        rows = []
+        for ln in [self.first_line] + out.splitlines():
             parts = ln.split()
-            if len(parts) != 2:
-                continue
-            sm.append(float(parts[0]))
+            if len(parts) == 3:
+                rows.append((int(parts[0]), float(parts[1]), int(parts[2])))
+        picked = rows
+        if self.t_begin is not None and self.t_end is not None and rows:
+            inside = [r for r in rows if self.t_begin <= r[0] <= self.t_end]
+            if inside:
+                picked = inside
+            else:  # the region is shorter than the interval: the nearest sample on each side
+                before = [r for r in rows if r[0] < self.t_begin][-1:]
+                after = [r for r in rows if r[0] > self.t_end][:1]
+                picked = before + after
+        reasons = set()
+        for _, _, bits in picked:
             for bit, name in self.REASONS.items():
-                if int(parts[1]) & bit:
+                if bits & bit:
                     reasons.add(name)
         try:
             smax = float(self.max_line.split()[1])
         except Exception:
             smax = None
-        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
-                "samples": len(sm), "source": "NVML every 2 ms (separate process)"}
+        inside_n = sum(1 for r in rows if self.t_begin is not None and self.t_end is not None
+                       and self.t_begin <= r[0] <= self.t_end)
+        return {"sm_mhz": float(np.median([r[1] for r in picked])) if picked else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(picked), "samples_in_region": inside_n,
+                "source": "NVML every ~0.3 ms (separate process)"}
 
 
 def make_values(n: int, rank: int) -> np.ndarray:
@@ -1252,11 +1277,13 @@ def main():
     torch.cuda.synchronize(dev)
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
+    clocks.begin()
     ev0.record(stream)
     for _ in range(args.steps):
         step()
     ev1.record(stream)
     torch.cuda.synchronize(dev)
+    clocks.end()
     ms = ev0.elapsed_time(ev1)
     if world > 1:
         dist.barrier()

@@ -94,9 +94,15 @@ void col_release(glc_column* c, void* p) {
 }
 
 void free_column_arrays(glc_column* c) {
-  void* ptrs[] = {c->d_start, c->d_end, c->d_types, c->d_params, c->d_bits, c->d_offs, c->d_err,
-                  c->d_words, c->d_plain, c->d_desc, c->d_tiles};
-  for (void* p : ptrs) col_release(c, p);
+  if (c->blob_view) {  // the SoA arrays and the bitstream lie in the blob (owned or borrowed)
+    void* ptrs[] = {c->d_plain, c->d_desc, c->d_tiles, c->owned};
+    for (void* p : ptrs) col_release(c, p);
+    c->owned = nullptr;
+  } else {
+    void* ptrs[] = {c->d_start, c->d_end, c->d_types, c->d_params, c->d_bits, c->d_offs, c->d_err,
+                    c->d_words, c->d_plain, c->d_desc, c->d_tiles};
+    for (void* p : ptrs) col_release(c, p);
+  }
   c->d_start = c->d_end = c->d_types = c->d_bits = nullptr;
   c->d_params = nullptr;
   c->d_offs = c->d_err = c->d_plain = nullptr;
@@ -187,6 +193,8 @@ glc_status glc_create(glc_ctx** out, int device) {
     return e == cudaErrorMemoryAllocation ? GLC_ERR_OOM : GLC_ERR_CUDA;
   }
   tune_defaults(ctx);
+  const char* expire = getenv("GLC_TEST_EXPIRE_FIRST_WAIT");  // test hook: see glc_ctx::expire_next_wait
+  if (expire && expire[0] == '1') ctx->expire_next_wait.store(1);
   const char* cache = getenv("GLC_TUNE_CACHE");  // results of an earlier glc_autotune, if they fit
   if (cache && *cache) tune_load(ctx, cache);
   *out = ctx;
@@ -253,7 +261,7 @@ glc_status glc_column_get_info(const glc_column* c, glc_column_info* info) {
   info->d_delta_bits = c->d_bits;
   info->d_delta_array_bit_offsets = c->d_offs;
   info->d_error_bounds = c->d_err;
-  info->delta_array = c->d_words;
+  info->delta_array = words_begin(c);
   info->d_plain_deltas = c->d_plain;
   info->max_delta_bits = c->max_bits;
   return GLC_OK;
@@ -534,7 +542,10 @@ glc_status glc_random_access(glc_ctx* ctx, const glc_column* col, glc_source sou
   if (count == 0) return GLC_OK;
   if (!positions || !out) return fail(ctx, GLC_ERR_INVALID_ARG, "null positions or output");
   if (fixed_partition_len < 0) return fail(ctx, GLC_ERR_INVALID_ARG, "negative partition length");
-  if (fixed_partition_len > 0 && col->fixed_len != fixed_partition_len)
+  // a layout of fixed length L: every partition but the last has L values.  A single partition of
+  // at most L values is one (the reference's TILE_SIZE layout of a short column).
+  const bool single = col->P == 1 && col->n <= fixed_partition_len;
+  if (fixed_partition_len > 0 && col->fixed_len != fixed_partition_len && !single)
     return fail(ctx, GLC_ERR_INVALID_ARG, "column is not partitioned with that fixed length");
   int plain = 0;
   glc_status st = resolve_source(ctx, col, source, &plain);
@@ -551,7 +562,7 @@ glc_status glc_random_access(glc_ctx* ctx, const glc_column* col, glc_source sou
     dpos = (const int32_t*)tpos;
   }
   if (flags & GLC_HOST_OUT) CK(pool_alloc(ctx, &dout, es * count, s), "random access: output");
-  const int32_t fl = fixed_partition_len > 0 ? fixed_partition_len : col->fixed_len;
+  const int32_t fl = fixed_partition_len > 0 && !single ? fixed_partition_len : col->fixed_len;
   cudaError_t e = launch_random_access(ctx, col, plain, dpos, count, dout, fl, s);
   if (e == cudaSuccess && (flags & GLC_HOST_OUT)) e = host_download(ctx, out, dout, es * count, s);
   if (tpos) cudaFreeAsync(tpos, s);
@@ -564,6 +575,7 @@ glc_status glc_random_access(glc_ctx* ctx, const glc_column* col, glc_source sou
 glc_status glc_preunpack(glc_ctx* ctx, glc_column* col, int drop_packed, glc_stream stream) {
   if (!ctx || !col) return fail(ctx, GLC_ERR_INVALID_ARG, "null argument");
   if (col->view && drop_packed) return fail(ctx, GLC_ERR_INVALID_ARG, "a batch column keeps its bitstream");
+  if (col->blob_view && drop_packed) return fail(ctx, GLC_ERR_INVALID_ARG, "an attached blob keeps its bitstream");
   if (col->n == 0) return GLC_OK;
   if (!col->d_plain) {
     if (!col->d_words) return fail(ctx, GLC_ERR_UNSUPPORTED, "column has no packed bitstream");
@@ -616,7 +628,7 @@ glc_status glc_serialize(glc_ctx* ctx, const glc_column* c, void* blob, uint64_t
   struct Piece { uint64_t off; const void* src; uint64_t bytes; } pieces[8] = {
       {h.start_off, c->d_start, 4 * P}, {h.end_off, c->d_end, 4 * P},     {h.types_off, c->d_types, 4 * P},
       {h.params_off, c->d_params, 32 * P}, {h.bits_off, c->d_bits, 4 * P}, {h.offsets_off, c->d_offs, 8 * P},
-      {h.errb_off, c->d_err, 8 * P},     {h.delta_off, c->d_words, h.delta_size}};
+      {h.errb_off, c->d_err, 8 * P},     {h.delta_off, words_begin(c), h.delta_size}};
   // zero the gaps (alignment padding and the tail), then the header, then the arrays
   uint64_t cursor = sizeof(BlobHeader);
   for (const Piece& pc : pieces) {
@@ -647,21 +659,15 @@ glc_status glc_deserialize(glc_ctx* ctx, glc_dtype dtype, const void* blob, uint
 
 }  // extern "C"
 
-glc_status glc::deserialize_column(glc_ctx* ctx, glc_dtype dtype, const void* blob, uint64_t size, int flags,
-                                   int crc32c, int pre_unpack, glc_column** out, glc_stream stream,
-                                   cudaMemPool_t pool, bool defer_words) {
-  if (!ctx || !out) return fail(ctx, GLC_ERR_INVALID_ARG, "null argument");
-  std::lock_guard<std::mutex> stats_lock(ctx->stats_mu);  // the checks come back through h_stats
-  *out = nullptr;
-  if (!valid_dtype(dtype)) return fail(ctx, GLC_ERR_INVALID_ARG, "unknown dtype");
-  if (!blob || size < sizeof(BlobHeader)) return fail(ctx, GLC_ERR_BAD_BLOB, "blob shorter than its header");
-  glc::DeviceScope device_scope(ctx->device);
-  cudaStream_t s = pick(ctx, stream);
-  const bool host = (flags & GLC_HOST_IN) != 0;
-  BlobHeader h;
+namespace {
+
+// Reads and checks a blob's header (api/G-LeCo.cuh:1029-1049: magic, version, element size,
+// checksum, size), plus bounds checks on every array and on the partition count.
+glc_status read_blob_header(glc_ctx* ctx, glc_dtype dtype, const void* blob, uint64_t size, bool host, int crc32c,
+                            BlobHeader* out) {
+  BlobHeader& h = *out;
   if (host) std::memcpy(&h, blob, sizeof h);
-  else CK(cudaMemcpy(&h, blob, sizeof h, cudaMemcpyDeviceToHost), "deserialize: header");
-  // api/G-LeCo.cuh:1029-1049, plus bounds checks on every array
+  else CK(cudaMemcpy(&h, blob, sizeof h, cudaMemcpyDeviceToHost), "blob: header");
   if (h.magic != kMagic || (h.version != 4 && h.version != 5)) return fail(ctx, GLC_ERR_BAD_BLOB, "bad magic or version");
   if ((int)h.type_size != dtype_size(dtype)) return fail(ctx, GLC_ERR_BAD_BLOB, "blob element size differs from dtype");
   BlobHeader t = h;
@@ -677,6 +683,28 @@ glc_status glc::deserialize_column(glc_ctx* ctx, glc_dtype dtype, const void* bl
   for (int k = 0; k < 7; k++)
     if (offs[k] > size || lens[k] > size - offs[k]) return fail(ctx, GLC_ERR_BAD_BLOB, "array outside the blob");
   if ((P == 0) != (h.total_values == 0)) return fail(ctx, GLC_ERR_BAD_BLOB, "partition count and length disagree");
+  return GLC_OK;
+}
+
+}  // namespace
+
+glc_status glc::deserialize_column(glc_ctx* ctx, glc_dtype dtype, const void* blob, uint64_t size, int flags,
+                                   int crc32c, int pre_unpack, glc_column** out, glc_stream stream,
+                                   cudaMemPool_t pool, bool defer_words) {
+  if (!ctx || !out) return fail(ctx, GLC_ERR_INVALID_ARG, "null argument");
+  std::lock_guard<std::mutex> stats_lock(ctx->stats_mu);  // the checks come back through h_stats
+  *out = nullptr;
+  if (!valid_dtype(dtype)) return fail(ctx, GLC_ERR_INVALID_ARG, "unknown dtype");
+  if (!blob || size < sizeof(BlobHeader)) return fail(ctx, GLC_ERR_BAD_BLOB, "blob shorter than its header");
+  glc::DeviceScope device_scope(ctx->device);
+  cudaStream_t s = pick(ctx, stream);
+  const bool host = (flags & GLC_HOST_IN) != 0;
+  BlobHeader h;
+  glc_status hst = read_blob_header(ctx, dtype, blob, size, host, crc32c, &h);
+  if (hst != GLC_OK) return hst;
+  const uint64_t P = h.num_partitions;
+  const uint64_t offs[7] = {h.start_off, h.end_off, h.types_off, h.params_off, h.bits_off, h.offsets_off, h.errb_off};
+  const uint64_t lens[7] = {4 * P, 4 * P, 4 * P, 32 * P, 4 * P, 8 * P, 8 * P};
 
   glc_column* c = new (std::nothrow) glc_column();
   if (!c) return fail(ctx, GLC_ERR_OOM, "host allocation");
@@ -759,6 +787,158 @@ glc_status glc::deserialize_column(glc_ctx* ctx, glc_dtype dtype, const void* bl
   if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return bail(cuda_fail(ctx, e, "deserialize: sync"));
   *out = c;
   return GLC_OK;
+}
+
+// ---------------------------------------------------------------------------------------
+// a column attached to a blob: the blob's arrays read where they lie
+// ---------------------------------------------------------------------------------------
+namespace {
+
+// End of the device allocation holding p (the driver's cuMemGetAddressRange, fetched through the
+// runtime so the library links no driver stub); 0 when it cannot be told.
+uintptr_t allocation_end(const void* p) {
+  typedef int (*AddrRange)(unsigned long long*, size_t*, unsigned long long);
+  static AddrRange fn = [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuMemGetAddressRange", &f, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      f = nullptr;
+    return (AddrRange)f;
+  }();
+  if (!fn) return 0;
+  unsigned long long base = 0;
+  size_t bytes = 0;
+  if (fn(&base, &bytes, (unsigned long long)(uintptr_t)p) != 0) return 0;
+  return (uintptr_t)(base + bytes);
+}
+
+constexpr uint64_t kAttachSlack = 64;  // readable bytes the decoders may touch past the bitstream
+
+}  // namespace
+
+glc_status glc::attach_column(glc_ctx* ctx, glc_dtype dtype, const void* blob, uint64_t size, int flags, int crc32c,
+                              glc_column** out, glc_stream stream, cudaMemPool_t pool, bool own_copy) {
+  if (!ctx || !out) return fail(ctx, GLC_ERR_INVALID_ARG, "null argument");
+  std::lock_guard<std::mutex> stats_lock(ctx->stats_mu);  // the checks come back through h_stats
+  *out = nullptr;
+  if (!valid_dtype(dtype)) return fail(ctx, GLC_ERR_INVALID_ARG, "unknown dtype");
+  if (!blob || size < sizeof(BlobHeader)) return fail(ctx, GLC_ERR_BAD_BLOB, "blob shorter than its header");
+  glc::DeviceScope device_scope(ctx->device);
+  cudaStream_t s = pick(ctx, stream);
+  const bool host = (flags & GLC_HOST_IN) != 0;
+  if (!host && ((uintptr_t)blob & 7) != 0) return fail(ctx, GLC_ERR_INVALID_ARG, "device blob must be 8-byte aligned");
+  BlobHeader h;
+  glc_status hst = read_blob_header(ctx, dtype, blob, size, host, crc32c, &h);
+  if (hst != GLC_OK) return hst;
+  glc_column* c = new (std::nothrow) glc_column();
+  if (!c) return fail(ctx, GLC_ERR_OOM, "host allocation");
+  c->ctx = ctx;
+  c->pool = pool;
+  c->sync_free = pool == nullptr || pool == ctx->pool;  // as the reference's cudaFree in cleanup()
+  c->dtype = dtype;
+  c->blob_view = true;
+  c->n = h.total_values;
+  c->P = (int64_t)h.num_partitions;
+  auto bail = [&](glc_status st) { cudaStreamSynchronize(s); free_column_arrays(c); delete c; return st; };
+  cudaError_t e;
+  // where the blob lies on the device: borrowed in place, or a copy placed so that its bitstream
+  // starts on a 16-byte boundary, with zeroed slack after it for the decoders' read-ahead
+  const uint8_t* b = (const uint8_t*)blob;
+  if (host || own_copy) {
+    const uint64_t lead = (16 - (h.delta_off & 15)) & 15;
+    c->owned_bytes = lead + size + kAttachSlack;
+    if ((e = col_alloc(c, (uint8_t**)&c->owned, c->owned_bytes, s)) != cudaSuccess)
+      return bail(cuda_fail(ctx, e, "attach: allocation"));
+    uint8_t* d = (uint8_t*)c->owned + lead;
+    e = host ? host_upload(ctx, d, blob, size, s) : cudaMemcpyAsync(d, blob, size, cudaMemcpyDeviceToDevice, s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(d + size, 0, kAttachSlack, s);
+    if (e != cudaSuccess) return bail(cuda_fail(ctx, e, "attach: copy of the blob"));
+    b = d;
+  }
+  c->d_start = (int32_t*)(b + h.start_off);
+  c->d_end = (int32_t*)(b + h.end_off);
+  c->d_types = (int32_t*)(b + h.types_off);
+  c->d_params = (double*)(b + h.params_off);
+  c->d_bits = (int32_t*)(b + h.bits_off);
+  c->d_offs = (int64_t*)(b + h.offsets_off);
+  c->d_err = (int64_t*)(b + h.errb_off);
+  if (c->n == 0) {
+    c->d_words = nullptr;
+    set_word_counts(c);
+    c->reported_size = 0;
+    if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return bail(cuda_fail(ctx, e, "attach: sync"));
+    *out = c;
+    return GLC_OK;
+  }
+  // total bits: the end of the last partition's range (api/G-LeCo.cuh:2016-2044)
+  {
+    struct { int32_t ls, le, lb, pad; int64_t lo; } last;
+    const uint64_t L = h.num_partitions - 1;
+    e = cudaMemcpyAsync(&last.ls, b + h.start_off + 4 * L, 4, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&last.le, b + h.end_off + 4 * L, 4, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&last.lb, b + h.bits_off + 4 * L, 4, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&last.lo, b + h.offsets_off + 8 * L, 8, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return bail(cuda_fail(ctx, e, "attach: last partition"));
+    c->total_bits = last.lo + (int64_t)(last.le - last.ls) * last.lb;
+  }
+  set_word_counts(c);
+  if ((uint64_t)((c->total_bits + 7) / 8) > h.delta_size && c->total_bits >= 0)
+    return bail(fail(ctx, GLC_ERR_BAD_BLOB, "partition arrays are inconsistent"));
+  // the kernels read the bitstream from a 16-byte aligned base in aligned 16-byte pieces, and up
+  // to a few words past its last field
+  const uintptr_t first = (uintptr_t)(b + h.delta_off);
+  const uintptr_t base = first & ~(uintptr_t)15;
+  const int shift = (int)((first - base) / 4);
+  const uint64_t need = (uint64_t)((((c->total_bits + 32 * shift) >> 5) + 8) & ~3ll) * 4;  // bytes from base
+  const bool in_place = host || own_copy || (allocation_end(b) >= base + need);
+  if (in_place) {
+    c->d_words = (uint32_t*)base;
+    c->word_shift = shift;
+  } else {  // a borrowed blob without room after its bitstream: its bitstream alone is copied
+    c->owned_bytes = 4 * (uint64_t)c->nwords_alloc;
+    if ((e = col_alloc(c, (uint32_t**)&c->owned, c->owned_bytes, s)) != cudaSuccess ||
+        (e = cudaMemsetAsync(c->owned, 0, c->owned_bytes, s)) != cudaSuccess ||
+        (h.delta_size && (e = cudaMemcpyAsync(c->owned, b + h.delta_off, h.delta_size, cudaMemcpyDeviceToDevice, s)) !=
+                             cudaSuccess))
+      return bail(cuda_fail(ctx, e, "attach: bitstream copy"));
+    c->d_words = (uint32_t*)c->owned;
+    c->word_shift = 0;
+  }
+  const int64_t P = c->P;
+  c->ntiles = (c->n + kDecodeTile - 1) / kDecodeTile;
+  if ((e = col_alloc(c, &c->d_desc, sizeof(PartDesc) * P, s)) != cudaSuccess ||
+      (e = col_alloc(c, &c->d_tiles, sizeof(TileInfo) * (c->ntiles + 1), s)) != cudaSuccess)
+    return bail(cuda_fail(ctx, e, "attach: tables"));
+  // structure check, fixed-length detection and max width (as deserialize)
+  int* d_chk = (int*)(ctx->d_stats + 4);
+  if ((e = cudaMemsetAsync(ctx->d_stats, 0, 8 * sizeof(int64_t), s)) != cudaSuccess ||
+      (e = launch_validate(c, d_chk, s)) != cudaSuccess || (e = launch_max_bits(c, ctx->d_stats + 1, s)) != cudaSuccess ||
+      (e = cudaMemcpyAsync(ctx->h_stats, ctx->d_stats, 8 * sizeof(int64_t), cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
+      (e = cudaStreamSynchronize(s)) != cudaSuccess)
+    return bail(cuda_fail(ctx, e, "attach: validation"));
+  const int* chk = (const int*)(ctx->h_stats + 4);
+  if (chk[0]) return bail(fail(ctx, GLC_ERR_BAD_BLOB, "partition arrays are inconsistent"));
+  c->max_bits = (int32_t)ctx->h_stats[1];
+  c->fixed_len = 0;
+  if (!chk[1]) {
+    int32_t se[2] = {0, 0};
+    if ((e = cudaMemcpy(&se[0], c->d_start, 4, cudaMemcpyDeviceToHost)) != cudaSuccess ||
+        (e = cudaMemcpy(&se[1], c->d_end, 4, cudaMemcpyDeviceToHost)) != cudaSuccess)
+      return bail(cuda_fail(ctx, e, "attach: layout"));
+    c->fixed_len = se[1] - se[0];
+  }
+  if ((e = launch_desc_and_tiles(c, s)) != cudaSuccess || (e = cudaStreamSynchronize(s)) != cudaSuccess)
+    return bail(cuda_fail(ctx, e, "attach: tables"));
+  c->reported_size = reported_size(c->P, c->total_bits);
+  *out = c;
+  return GLC_OK;
+}
+
+extern "C" glc_status glc_attach_blob(glc_ctx* ctx, glc_dtype dtype, const void* blob, uint64_t size, int flags,
+                                      int crc32c, glc_column** out, glc_stream stream) {
+  return glc::attach_column(ctx, dtype, blob, size, flags, crc32c, out, stream, ctx ? ctx->pool : nullptr, false);
 }
 
 // ---------------------------------------------------------------------------------------

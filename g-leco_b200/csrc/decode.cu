@@ -58,6 +58,9 @@ struct DecodeArgs {
   int* counter;
   int* err;
   int stage_bytes;
+  // >= 0: the consumers' FIRST wait for a stage gives up after this many non-blocking tests
+  // (0: at once) -- a test hook that makes a bounded wait run out on a healthy copy; -1: normal
+  int first_wait_tests;
 };
 
 struct StageInfo {
@@ -335,7 +338,9 @@ __global__ void __launch_bounds__(kPCThreads) decode_kernel(DecodeArgs a) {
   // ---- consumers ----
   for (int k = 0;; k++) {
     const int s = k % kStages;
-    if (!mbar_wait_bounded(&full[s], (uint32_t)(k / kStages) & 1u)) {
+    const bool got = (k == 0 && a.first_wait_tests >= 0) ? mbar_test_n(&full[s], 0u, a.first_wait_tests)
+                                                          : mbar_wait_bounded(&full[s], (uint32_t)(k / kStages) & 1u);
+    if (!got) {
       if (lane == 0) atomicExch(a.err, DEVERR_TIMEOUT);
       mbar_wait_bounded(&full[s], (uint32_t)(k / kStages) & 1u);  // copies in flight land first
       break;
@@ -431,6 +436,7 @@ __device__ __forceinline__ void batch_body(const BatchDecodeArgs& b, int g, uint
     a.hi = w.hi;
     a.out_base = w.out_base;
     a.stage_bytes = b.stage_bytes;
+    a.first_wait_tests = -1;
     decode_tile<T, false, false>(a, si, smem + (size_t)s * b.stage_bytes, &s_desc[s][0]);
     __syncwarp();
     if (lane == 0) mbar_arrive(&empty[s]);
@@ -645,6 +651,7 @@ cudaError_t launch_decode_scratch(const glc_column* c, int64_t lo, int64_t hi, v
   a.out_base = out_base;
   a.counter = counter;
   a.err = err;
+  a.first_wait_tests = -1;
   int64_t words = ((int64_t)kDecodeTile * c->max_bits + 31) / 32 + 16;
   words = (words + 3) & ~3ll;
   if (words > kStageCapWords) words = kStageCapWords;
@@ -688,6 +695,7 @@ cudaError_t launch_decode_shape(glc_ctx* ctx, const glc_column* c, int plain_src
   a.out_base = out_base;
   a.counter = ctx->d_flags + (ctx->next_slot.fetch_add(1u) % kCounterSlots);
   a.err = ctx->d_flags + kFlagError;
+  a.first_wait_tests = ctx->expire_next_wait.exchange(0) ? 0 : -1;  // test hook, one launch
   if (plain_src) {
     a.stage_bytes = kDecodeTile * 8 + 16;
   } else {

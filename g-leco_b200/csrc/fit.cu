@@ -524,15 +524,17 @@ cudaError_t launch_fit(glc_dtype dt, const void* values, glc_column* c, void* sc
 // ---------------------------------------------------------------------------------------
 // Derived tables: 32-byte partition descriptors and the decode tile table.
 // ---------------------------------------------------------------------------------------
+// bit_shift: bits between the kernels' word base and the bitstream's first bit (attached blobs)
 __global__ void build_desc_kernel(const int32_t* __restrict__ starts, const int32_t* __restrict__ types,
                                   const double* __restrict__ params, const int32_t* __restrict__ bits,
-                                  const int64_t* __restrict__ offs, int64_t P, PartDesc* __restrict__ desc) {
+                                  const int64_t* __restrict__ offs, int64_t P, int64_t bit_shift,
+                                  PartDesc* __restrict__ desc) {
   int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= P) return;
   PartDesc d;
   d.theta0 = params[4 * p];
   d.theta1 = params[4 * p + 1];
-  d.bit_off = offs[p];
+  d.bit_off = offs[p] + bit_shift;
   d.start = starts[p];
   d.bits_type = (bits[p] & 0xff) | (types[p] << 8);
   desc[p] = d;
@@ -550,12 +552,12 @@ __device__ __forceinline__ int64_t owner_of(const int32_t* __restrict__ starts, 
 
 __global__ void build_tiles_kernel(const int32_t* __restrict__ starts, const int32_t* __restrict__ bits,
                                    const int64_t* __restrict__ offs, int64_t P, int64_t n, int64_t ntiles,
-                                   int64_t total_bits, TileInfo* __restrict__ tiles) {
+                                   int64_t total_bits, int64_t bit_shift, TileInfo* __restrict__ tiles) {
   int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t > ntiles) return;
   TileInfo ti;
   if (t == ntiles) {
-    ti.bit_lo = total_bits;
+    ti.bit_lo = total_bits + bit_shift;
     ti.p_first = (int32_t)(P - 1);
     ti.p_last = (int32_t)(P - 1);
   } else {
@@ -563,7 +565,7 @@ __global__ void build_tiles_kernel(const int32_t* __restrict__ starts, const int
     int64_t e1 = e0 + kDecodeTile < n ? e0 + kDecodeTile : n;
     int64_t pf = owner_of(starts, P, e0);
     int64_t pl = owner_of(starts, P, e1 - 1);
-    ti.bit_lo = offs[pf] + (e0 - starts[pf]) * (int64_t)bits[pf];
+    ti.bit_lo = offs[pf] + (e0 - starts[pf]) * (int64_t)bits[pf] + bit_shift;
     ti.p_first = (int32_t)pf;
     ti.p_last = (int32_t)pl;
   }
@@ -594,10 +596,11 @@ __global__ void validate_kernel(const int32_t* __restrict__ starts, const int32_
 
 cudaError_t launch_desc_and_tiles(glc_column* c, cudaStream_t s) {
   if (c->P > 0) {
+    const int64_t shift = 32 * (int64_t)c->word_shift;
     build_desc_kernel<<<(unsigned)((c->P + 255) / 256), 256, 0, s>>>(c->d_start, c->d_types, c->d_params, c->d_bits,
-                                                                       c->d_offs, c->P, c->d_desc);
-    build_tiles_kernel<<<(unsigned)((c->ntiles + 1 + 255) / 256), 256, 0, s>>>(c->d_start, c->d_bits, c->d_offs, c->P,
-                                                                                 c->n, c->ntiles, c->total_bits, c->d_tiles);
+                                                                       c->d_offs, c->P, shift, c->d_desc);
+    build_tiles_kernel<<<(unsigned)((c->ntiles + 1 + 255) / 256), 256, 0, s>>>(
+        c->d_start, c->d_bits, c->d_offs, c->P, c->n, c->ntiles, c->total_bits, shift, c->d_tiles);
   }
   return cudaGetLastError();
 }

@@ -70,6 +70,9 @@ struct glc_ctx {
   int64_t* d_stats = nullptr;  // small readback area (total bits, max bits, ...)
   int64_t* h_stats = nullptr;  // pinned mirror of d_stats
   std::atomic<unsigned> next_slot{0};
+  // test hook (GLC_TEST_EXPIRE_FIRST_WAIT=1 at glc_create): the next decode launch's consumers give
+  // up their first wait at once, so that launch reports GLC_ERR_TIMEOUT on a healthy copy
+  std::atomic<int> expire_next_wait{0};
   std::string err;
   glc::TuneEntry tune[4][glc::kTuneBuckets][2];  // [dtype][bucket][pre-unpacked source]
   std::mutex stats_mu;                     // held by calls that read results back through h_stats
@@ -105,11 +108,23 @@ struct glc_column {
   glc::PartDesc* d_desc = nullptr;
   glc::TileInfo* d_tiles = nullptr;
   int64_t ntiles = 0;
+  // A column attached to a blob (glc_attach_blob) reads the blob's arrays where they lie: the SoA
+  // pointers point into the blob and are not freed with the column.  d_words is then the 16-byte
+  // aligned address at or below the blob's bitstream, which starts word_shift words above it; the
+  // descriptors and the tile table carry bit positions relative to d_words.  `owned` is device
+  // memory the column holds (a copy of the blob, or of its bitstream), freed with it.
+  bool blob_view = false;
+  int32_t word_shift = 0;
+  void* owned = nullptr;
+  uint64_t owned_bytes = 0;
 };
 
 namespace glc {
 
 inline int dtype_size(glc_dtype d) { return (d == GLC_I64 || d == GLC_U64) ? 8 : 4; }
+
+// The first word of a column's bitstream (d_words is a kernel base below it for attached blobs).
+inline const uint32_t* words_begin(const glc_column* c) { return c->d_words ? c->d_words + c->word_shift : nullptr; }
 
 inline const TuneEntry& tune_entry(const glc_ctx* ctx, glc_dtype d, int bits, int plain) {
   return ctx->tune[(int)d & 3][tune_bucket(bits)][plain ? 1 : 0];
@@ -266,6 +281,10 @@ cudaError_t launch_random_access_shape(glc_ctx* ctx, const glc_column* c, int pl
 glc_status deserialize_column(glc_ctx* ctx, glc_dtype dtype, const void* blob, uint64_t size, int flags, int crc32c,
                               int pre_unpack, glc_column** out, glc_stream stream, cudaMemPool_t pool,
                               bool defer_words = false);
+// api.cu: glc_attach_blob; with own_copy the blob is first copied into memory the column owns
+// (from `pool`, or cudaMalloc when pool is null), whether it lies in host or device memory.
+glc_status attach_column(glc_ctx* ctx, glc_dtype dtype, const void* blob, uint64_t size, int flags, int crc32c,
+                         glc_column** out, glc_stream stream, cudaMemPool_t pool, bool own_copy);
 // random_access.cu: lookups of many requests into many columns (serving)
 struct RAColumn {
   const PartDesc* desc;

@@ -43,6 +43,9 @@ int64_t now_ns() {
 // bitstream and the optional pre-unpacked residuals.
 uint64_t column_device_bytes(const glc_column* c) {
   const uint64_t P = (uint64_t)c->P;
+  if (c->blob_view)  // an attached blob: the blob (or its bitstream) it holds and its derived tables
+    return c->owned_bytes + P * sizeof(PartDesc) + sizeof(TileInfo) * (uint64_t)(c->ntiles + 1) +
+           (c->d_plain ? 8ull * (uint64_t)c->n + 16 : 0);
   uint64_t b = P * (4 + 4 + 4 + 32 + 4 + 8 + 8) + P * sizeof(PartDesc) + sizeof(TileInfo) * (uint64_t)(c->ntiles + 1);
   if (c->d_words) b += 4ull * (uint64_t)c->nwords_alloc;
   if (c->d_plain) b += 8ull * (uint64_t)c->n + 16;
@@ -653,7 +656,8 @@ glc_status glc_server_admit_blob(glc_server* S, glc_dtype dtype, const void* blo
                                  int32_t* id, glc_stream stream) {
   if (!S || !id) return GLC_ERR_INVALID_ARG;
   glc_column* col = nullptr;
-  glc_status st = deserialize_column(S->ctx, dtype, blob, size, flags, 0, 0, &col, stream, S->pool);
+  // the blob itself stays resident (copied once into the server's pool) and is read in place
+  glc_status st = attach_column(S->ctx, dtype, blob, size, flags, 0, &col, stream, S->pool, true);
   if (st != GLC_OK) return st;
   st = glc_server_admit(S, col, id);
   if (st != GLC_OK) glc_column_free(col);

@@ -34,7 +34,8 @@ EXPORTS = [
     "glc_create", "glc_destroy", "glc_last_error", "glc_status_string", "glc_sync", "glc_compress",
     "glc_partition_variable", "glc_partition_v6", "glc_column_free", "glc_column_get_info", "glc_decompress_full",
     "glc_decompress_range", "glc_random_access", "glc_preunpack", "glc_blob_size", "glc_serialize",
-    "glc_deserialize", "glc_decode_blob_to_host", "glc_decompress_range_noalloc", "glc_batch_create", "glc_batch_compress",
+    "glc_deserialize", "glc_attach_blob", "glc_decode_blob_to_host", "glc_decompress_range_noalloc",
+    "glc_batch_create", "glc_batch_compress",
     "glc_batch_column", "glc_batch_decompress", "glc_batch_free", "glc_server_create", "glc_server_destroy",
     "glc_server_admit", "glc_server_admit_blob", "glc_server_evict", "glc_server_submit", "glc_server_poll",
     "glc_server_drain", "glc_server_get_stats", "glc_server_now_ns", "glc_server_columns",
@@ -139,6 +140,7 @@ def load() -> ctypes.CDLL:
         "glc_serialize": ([vp, vp, vp, u64, c_int, c_int, pu64, vp], c_int),
         "glc_deserialize": ([vp, c_int, vp, u64, c_int, c_int, c_int, pvp, vp], c_int),
         "glc_decompress_range_noalloc": ([vp, i64, i64, vp, vp], c_int),
+        "glc_attach_blob": ([vp, c_int, vp, u64, c_int, c_int, pvp, vp], c_int),
         "glc_decode_blob_to_host": ([vp, c_int, vp, u64, c_int, vp, pvp, vp], c_int),
         "glc_batch_create": ([vp, vp, i32, pvp], c_int),
         "glc_batch_compress": ([vp, vp, vp, vp, i32, i32, pvp, pi64, vp], c_int),
@@ -361,6 +363,29 @@ def deserialize_host(ctx: Context, dtype: int, blob: bytes, pre_unpack: bool = F
     return Column(ctx, h)
 
 
+def attach_blob(ctx: Context, dtype: int, blob_ptr: int, size: int, host: bool = False, crc32c: bool = False,
+                stream: int = 0) -> Optional[Column]:
+    """glc_attach_blob: a column that reads a serialized blob in place (a host blob is copied to the
+    device once; a device blob is borrowed and must outlive the column).  None for a rejected blob."""
+    h = ctypes.c_void_p()
+    st = ctx.lib.glc_attach_blob(ctx.handle, dtype, ctypes.c_void_p(blob_ptr), size, HOST_IN if host else 0,
+                                 1 if crc32c else 0, ctypes.byref(h), ctypes.c_void_p(stream))
+    if st == ERR_BAD_BLOB:
+        return None
+    ctx.check(st)
+    return Column(ctx, h)
+
+
+class DirectAccessHandle:
+    """The reference's DirectAccessHandle<T> (api/G-LeCo_Types.cuh:75-107): the host blob it was
+    made from, and the device column that reads the blob's copy in place."""
+
+    def __init__(self, blob: bytes, column: Column):
+        self.data_blob_host = blob
+        self.data_blob_size = len(blob)
+        self.column = column
+
+
 class BorrowedColumn(Column):
     """A column owned by a batch: freed with the batch, never on its own."""
 
@@ -548,7 +573,9 @@ class LeCoGPU:
     decompressFullFile_OnTheFly_Optimized_V2 = decompressFullFile
 
     def decompressFullFile_Fix(self, col: Column, partition_size: int) -> np.ndarray:
-        if col.info().fixed_partition_len != partition_size:
+        inf = col.info()
+        if inf.fixed_partition_len != partition_size and not (inf.num_partitions == 1 and
+                                                              inf.total_values <= partition_size):
             raise GlcError(ERR_INVALID_ARG, "column is not partitioned with that fixed length")
         return self._full(col, SRC_AUTO)
 
@@ -589,3 +616,22 @@ class LeCoGPU:
     # api/G-LeCo.cuh:793-821
     def cleanup(self, col: Column):
         col.free()
+
+    # api/G-LeCo.cuh:1157-1255 -- None where the reference returns nullptr
+    def createDirectAccessHandle(self, blob: bytes, copy_to_device: bool = True) -> Optional[DirectAccessHandle]:
+        b = np.frombuffer(blob, np.uint8)
+        if len(b) == 0:
+            return None
+        col = attach_blob(self.ctx, self.code, b.ctypes.data, len(b), host=True)
+        return DirectAccessHandle(blob, col) if col is not None else None
+
+    # api/G-LeCo.cuh:1257-1334: the lookups read the device copy of the blob in place
+    def directRandomAccessGPU(self, handle: DirectAccessHandle, positions) -> np.ndarray:
+        return self._ra(handle.column, positions, SRC_PACKED, 0)
+
+    # api/G-LeCo.cuh:1337-1672: this library has no host decoder; the same values come from the device
+    directRandomAccessCPU = directRandomAccessGPU
+
+    # api/G-LeCo.cuh:1674-1681
+    def destroyDirectAccessHandle(self, handle: DirectAccessHandle):
+        handle.column.free()

@@ -199,6 +199,22 @@ GLC_API glc_status glc_deserialize(glc_ctx* ctx, glc_dtype dtype, const void* bl
 GLC_API glc_status glc_decode_blob_to_host(glc_ctx* ctx, glc_dtype dtype, const void* blob, uint64_t size,
                                            int crc32c, void* out, glc_column** col_out, glc_stream stream);
 
+/* Replaces createDirectAccessHandle(blob, size, copy_to_device) (api/G-LeCo.cuh:1157-1255),
+ * whose handle directRandomAccessGPU reads in place (:1257-1334,
+ * decompression/RandomAccessKernels.cuh:173-333): a column that reads a serialized blob where it
+ * lies, with no deserialize.  Only the partition descriptors and the decode tile table (48 bytes
+ * per partition and per 4096 values) are built; random access, range and full decode, the batch
+ * and the server read the blob's own arrays and bitstream.  Same checks as glc_deserialize.
+ *  - GLC_HOST_IN: the host blob is copied once into device memory the column owns (the
+ *    reference's copy_to_device = true).
+ *  - otherwise `blob` is device memory of the context's device, 8-byte aligned, BORROWED: it must
+ *    stay valid and unchanged until glc_column_free.  When the allocation holding it ends less
+ *    than 64 bytes after the bitstream (the decoders read ahead in 16-byte pieces), only the
+ *    bitstream is copied into memory the column owns.
+ * The column cannot drop its bitstream (glc_preunpack with drop_packed). */
+GLC_API glc_status glc_attach_blob(glc_ctx* ctx, glc_dtype dtype, const void* blob, uint64_t size, int flags,
+                                   int crc32c, glc_column** out, glc_stream stream);
+
 /* ---- batches: many columns per launch (no counterpart in the reference) ----------------- */
 
 typedef struct glc_batch glc_batch;
@@ -360,10 +376,11 @@ GLC_API glc_status glc_server_destroy(glc_server* server);
  * glc_server_admit_blob, return with their stream synchronised). */
 GLC_API glc_status glc_server_admit(glc_server* server, glc_column* col, int32_t* id);
 
-/* Deserialize a blob (as glc_deserialize, host or device memory) and admit the column.  Its arrays
- * come from the server's stream-ordered pool, so neither this admission nor the column's later
- * eviction calls cudaMalloc or cudaFree, which would stall the launches in flight; with
- * GLC_SERVER_RESERVE the pool holds budget_bytes from creation on. */
+/* Admit a serialized column (host or device memory; the same checks as glc_deserialize).  The blob
+ * itself is copied once into the server's stream-ordered pool and read in place there, as
+ * glc_attach_blob reads it (no deserialize; the caller may free its blob afterwards), so neither
+ * this admission nor the column's later eviction calls cudaMalloc or cudaFree, which would stall
+ * the launches in flight; with GLC_SERVER_RESERVE the pool holds budget_bytes from creation on. */
 GLC_API glc_status glc_server_admit_blob(glc_server* server, glc_dtype dtype, const void* blob, uint64_t size,
                                          int flags, int32_t* id, glc_stream stream);
 

@@ -198,7 +198,8 @@ class LeCoGPU {
   void decompressFullFile_Fix(CompressedData<T>* cd, std::vector<T>& out, int partition_size) {
     glc_column_info info;
     if (!cd || !cd->glc_col || glc_column_get_info(cd->glc_col, &info) != GLC_OK ||
-        info.fixed_partition_len != partition_size) {
+        (info.fixed_partition_len != partition_size &&
+         !(info.num_partitions == 1 && info.total_values <= partition_size))) {  // one short partition
       out.clear();
       return;
     }
@@ -258,10 +259,11 @@ class LeCoGPU {
 
   // api/G-LeCo.cuh:1157-1255
   DirectAccessHandle<T>* createDirectAccessHandle(const uint8_t* blob, size_t blob_size, bool copy_to_device_flag = true) {
-    (void)copy_to_device_flag;
+    (void)copy_to_device_flag;  // the lookups run on the device, so the blob is always copied there
     if (!ctx_ || !blob) return nullptr;
     glc_column* col = nullptr;
-    if (glc_deserialize(ctx_, kCode, blob, blob_size, GLC_HOST_IN, 0, 0, &col, nullptr) != GLC_OK) return nullptr;
+    // the device copy of the blob is read in place (no deserialize), as directRandomAccessGPU does
+    if (glc_attach_blob(ctx_, kCode, blob, blob_size, GLC_HOST_IN, 0, &col, nullptr) != GLC_OK) return nullptr;
     DirectAccessHandle<T>* h = new DirectAccessHandle<T>();
     h->data_blob_host = blob;
     h->data_blob_size = blob_size;
