@@ -305,7 +305,7 @@ static glc_status compress_impl(glc_ctx* ctx, glc_dtype dtype, const void* dev_v
     uint32_t* wtmp = nullptr;
     void* scratch = nullptr;
     CK(pool_alloc(ctx, &wtmp, 4 * (size_t)fixed_compress_worst_words(dtype, n), s), "compress: word buffer");
-    cudaError_t e = pool_alloc(ctx, &scratch, fixed_compress_scratch_bytes(n), s);
+    cudaError_t e = pool_alloc(ctx, &scratch, fixed_compress_scratch_bytes((n + kDecodeTile - 1) / kDecodeTile), s);
     if (e == cudaSuccess)
       e = launch_fixed_compress(dtype, dev_values, c, fixed_len, wtmp, scratch, (unsigned long long*)ctx->d_stats, s);
     if (e == cudaSuccess) e = cudaMemcpyAsync(ctx->h_stats, ctx->d_stats, 3 * sizeof(int64_t), cudaMemcpyDeviceToHost, s);
@@ -317,7 +317,8 @@ static glc_status compress_impl(glc_ctx* ctx, glc_dtype dtype, const void* dev_v
     }
     if (ctx->h_stats[2] != DEVERR_NONE) {
       cudaFreeAsync(wtmp, s);
-      return fail(ctx, GLC_ERR_TIMEOUT, "compress: a device-side wait gave up");
+      return ctx->h_stats[2] == DEVERR_TIMEOUT ? fail(ctx, GLC_ERR_TIMEOUT, "compress: a device-side wait gave up")
+                                               : fail(ctx, GLC_ERR_CUDA, "compress: words beyond their array");
     }
     c->total_bits = ctx->h_stats[0];
     c->max_bits = (int32_t)ctx->h_stats[1];

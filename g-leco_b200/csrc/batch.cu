@@ -509,6 +509,133 @@ glc_status build_work(glc_ctx* ctx, glc_batch* b, void* const* outs, cudaStream_
   return GLC_OK;
 }
 
+// One-pass batched compress (compress_fixed.cu): every column's partition length divides the
+// 4096-value tile, and its exact bit count is known from the choice pass (the same exact-sum fit,
+// so the same widths), so every array is allocated at its exact size before one launch per element
+// type fits, offsets, packs and tabulates all of that type's columns.  The values are read twice
+// in all: once by the choice, once by this launch.
+glc_status compress_one_pass(glc_ctx* ctx, glc_batch* b, const glc_dtype* dtypes, const void* const* values,
+                             const int64_t* ns, int nc, const std::vector<int32_t>& len,
+                             const std::vector<unsigned long long>& hbits, cudaStream_t s, int64_t* total_size) {
+  std::vector<int64_t> pb(nc + 1, 0), wb(nc + 1, 0), eb(nc + 1, 0);
+  std::vector<glc_column*> cols(nc, nullptr);
+  for (int i = 0; i < nc; i++) {
+    glc_column* c = new (std::nothrow) glc_column();
+    if (!c) return GLC_ERR_OOM;
+    cols[i] = c;
+    b->cols.push_back(c);
+    c->ctx = ctx;
+    c->view = true;
+    c->dtype = dtypes[i];
+    c->n = ns[i];
+    c->fixed_len = len[i];
+    c->P = c->n > 0 ? (c->n + len[i] - 1) / len[i] : 0;
+    const int k = len[i] == 1024 ? 0 : (len[i] == 2048 ? 1 : 2);
+    c->total_bits = c->n > 0 ? (int64_t)hbits[3 * (size_t)i + k] : 0;
+    c->nwords = (c->total_bits + 31) / 32;
+    c->nwords_alloc = ((c->nwords + 3) & ~3ll) + 8;
+    c->ntiles = (c->n + kDecodeTile - 1) / kDecodeTile;
+    c->reported_size = c->n ? 64 * c->P + 120 + (c->total_bits + 7) / 8 : 0;  // api/G-LeCo.cuh:589-603
+    pb[i + 1] = pb[i] + c->P;
+    wb[i + 1] = wb[i] + c->nwords_alloc;
+    eb[i + 1] = eb[i] + (c->n ? c->ntiles + 1 : 0);
+  }
+  const int64_t P = pb[nc];
+  int32_t *starts, *ends, *types, *bits;
+  double* params;
+  int64_t *offs, *errs;
+  PartDesc* desc;
+  uint32_t* words;
+  TileInfo* tiles;
+  unsigned long long* stats;  // 2 per column, then the status word
+  cudaError_t e;
+  if ((e = dalloc(b, &starts, P)) || (e = dalloc(b, &ends, P)) || (e = dalloc(b, &types, P)) ||
+      (e = dalloc(b, &bits, P)) || (e = dalloc(b, &params, 4 * P)) || (e = dalloc(b, &offs, P)) ||
+      (e = dalloc(b, &errs, P)) || (e = dalloc(b, &desc, P)) || (e = dalloc(b, &words, wb[nc])) ||
+      (e = dalloc(b, &tiles, eb[nc])) || (e = dalloc(b, &stats, 2 * (size_t)nc + 1)))
+    return bcuda(ctx, e, "batch compress: allocation");
+  BCK(cudaMemsetAsync(stats, 0, sizeof(unsigned long long) * (2 * (size_t)nc + 1), s), "batch compress: stats");
+  std::vector<CfColumn> hc(nc);
+  for (int i = 0; i < nc; i++) {
+    glc_column* c = cols[i];
+    const int64_t p0 = pb[i];
+    c->d_start = starts + p0;
+    c->d_end = ends + p0;
+    c->d_types = types + p0;
+    c->d_params = params + 4 * p0;
+    c->d_bits = bits + p0;
+    c->d_offs = offs + p0;
+    c->d_err = errs + p0;
+    c->d_desc = desc + p0;
+    c->d_words = words + wb[i];
+    c->d_tiles = tiles + eb[i];
+    CfColumn& f = hc[i];
+    f = CfColumn{};
+    f.values = values[i];
+    f.n = c->n;
+    f.L = len[i];
+    f.parts_per_tile = kDecodeTile / len[i];
+    f.P = c->P;
+    f.ntiles = c->ntiles;
+    f.nwords_alloc = c->nwords_alloc;
+    f.words_cap = c->nwords_alloc;
+    f.starts = c->d_start;
+    f.ends = c->d_end;
+    f.types = c->d_types;
+    f.params = c->d_params;
+    f.bits = c->d_bits;
+    f.offs = c->d_offs;
+    f.err = c->d_err;
+    f.desc = c->d_desc;
+    f.tiles = c->d_tiles;
+    f.words = c->d_words;
+    f.stats = stats + 2 * i;
+  }
+  // one launch per element type over the tiles of that type's columns, in column order
+  for (glc_dtype dt : {GLC_I32, GLC_I64, GLC_U64, GLC_U32}) {
+    std::vector<CfColumn> g;
+    std::vector<int64_t> ib(1, 0);
+    for (int i = 0; i < nc; i++) {
+      if (dtypes[i] != dt || ns[i] == 0) continue;
+      CfColumn f = hc[i];
+      f.item_base = ib.back();
+      g.push_back(f);
+      ib.push_back(ib.back() + f.ntiles);
+    }
+    if (g.empty()) continue;
+    const int64_t nitems = ib.back();
+    CfColumn* d_g;
+    int64_t* d_ib;
+    int32_t* d_owner;
+    uint8_t* scratch;
+    if ((e = dalloc(b, &d_g, g.size())) || (e = dalloc(b, &d_ib, ib.size())) || (e = dalloc(b, &d_owner, nitems)) ||
+        (e = dalloc(b, &scratch, fixed_compress_scratch_bytes(nitems))))
+      return bcuda(ctx, e, "batch compress: allocation");
+    BCK(cudaMemcpyAsync(d_g, g.data(), sizeof(CfColumn) * g.size(), cudaMemcpyHostToDevice, s), "batch compress: columns");
+    BCK(cudaMemcpyAsync(d_ib, ib.data(), sizeof(int64_t) * ib.size(), cudaMemcpyHostToDevice, s), "batch compress: columns");
+    BCK(launch_pack_item_owner(d_ib, (int)g.size(), d_owner, s), "batch compress: work list");
+    BCK(launch_fixed_compress_batch(dt, d_g, d_owner, nitems, scratch, stats + 2 * (size_t)nc, ctx->num_sms, s),
+        "batch compress: one-pass compress");
+    BCK(cudaStreamSynchronize(s), "batch compress: sync");  // the host vectors above are reused next
+  }
+  std::vector<unsigned long long> hs(2 * (size_t)nc + 1);
+  BCK(cudaMemcpyAsync(hs.data(), stats, sizeof(unsigned long long) * hs.size(), cudaMemcpyDeviceToHost, s),
+      "batch compress: stats");
+  BCK(cudaStreamSynchronize(s), "batch compress: sync");
+  if (hs[2 * (size_t)nc] == DEVERR_TIMEOUT) return bfail(ctx, GLC_ERR_TIMEOUT, "batch compress: a device-side wait gave up");
+  if (hs[2 * (size_t)nc] != DEVERR_NONE) return bfail(ctx, GLC_ERR_CUDA, "batch compress: words beyond their array");
+  int64_t total = 0;
+  for (int i = 0; i < nc; i++) {
+    glc_column* c = cols[i];
+    if (c->n > 0 && (int64_t)hs[2 * (size_t)i] != c->total_bits)
+      return bfail(ctx, GLC_ERR_CUDA, "batch compress: the pass and the length choice disagree on a column's bits");
+    c->max_bits = (int32_t)hs[2 * (size_t)i + 1];
+    total += c->reported_size;
+  }
+  if (total_size) *total_size = total;
+  return GLC_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -574,9 +701,13 @@ glc_status glc_batch_compress(glc_ctx* ctx, const glc_dtype* dtypes, const void*
   if ((e = dalloc(b, &d_fc, nc)) != cudaSuccess || (e = dalloc(b, &d_pb, nc + 1)) != cudaSuccess ||
       (e = dalloc(b, &d_colbits, 3 * (size_t)nc)) != cudaSuccess)
     return bail(bcuda(ctx, e, "batch compress: allocation"));
-  if (fixed_partition_len == 0) {  // one pass measures all three candidate lengths
+  // lengths 1024 / 2048 / 4096: the choice pass measures the exact bits of all three, and the
+  // one-pass kernel compresses every column at its chosen length
+  const bool one_pass = fixed_partition_len == 0 || fixed_partition_len == 1024 || fixed_partition_len == 2048 ||
+                        fixed_partition_len == 4096;
+  std::vector<unsigned long long> hbits(3 * (size_t)nc);
+  if (one_pass) {  // one pass measures all three candidate lengths
     std::vector<int32_t> L(nc, 4096);
-    std::vector<unsigned long long> hbits(3 * (size_t)nc);
     if ((e = upload_layout(L)) != cudaSuccess) return bail(bcuda(ctx, e, "batch compress: layout"));
     if ((e = cudaMemsetAsync(d_colbits, 0, sizeof(unsigned long long) * 3 * nc, s)) != cudaSuccess)
       return bail(bcuda(ctx, e, "batch compress: sizes"));
@@ -586,7 +717,7 @@ glc_status glc_batch_compress(glc_ctx* ctx, const glc_dtype* dtypes, const void*
                              s)) != cudaSuccess ||
         (e = cudaStreamSynchronize(s)) != cudaSuccess)
       return bail(bcuda(ctx, e, "batch compress: sizes"));
-    for (int i = 0; i < nc; i++) {
+    for (int i = 0; i < nc && fixed_partition_len == 0; i++) {
       int64_t best = INT64_MAX;
       for (int k = 0; k < 3; k++) {
         const int64_t cand = kCandidates[k];
@@ -595,6 +726,13 @@ glc_status glc_batch_compress(glc_ctx* ctx, const glc_dtype* dtypes, const void*
         if (size < best) { best = size; len[i] = (int32_t)cand; }
       }
     }
+    int64_t total = 0;
+    glc_status st = compress_one_pass(ctx, b, dtypes, values, ns, nc, len, hbits, s, &total);
+    if (st == GLC_OK) st = finish_batch(ctx, b, s);
+    if (st != GLC_OK) return bail(st);
+    if (compressed_size_bytes) *compressed_size_bytes = total;
+    *out = b;
+    return GLC_OK;
   }
   if ((e = upload_layout(len)) != cudaSuccess) return bail(bcuda(ctx, e, "batch compress: layout"));
   const int64_t P = pb[nc];

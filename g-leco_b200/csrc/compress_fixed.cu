@@ -53,27 +53,17 @@ template <typename T> __host__ __device__ constexpr int cf_smem_bytes() {
 // posted; the low 62 bits hold the count.  Zero at launch.
 constexpr unsigned long long kLbAgg = 1ull << 62, kLbInc = 2ull << 62, kLbVal = (1ull << 62) - 1;
 
+// A launch: work item i = one 4096-value tile of column owner[i] (every column of one element
+// type, tiles in order), or of `single` when cols is null.
 struct FixedCompressArgs {
-  const void* values;
-  int64_t n;
-  int32_t L;
-  int32_t parts_per_tile;  // 4096 / L
-  int64_t P, ntiles;
-  int32_t* starts;
-  int32_t* ends;
-  int32_t* types;
-  double* params;
-  int32_t* bits;
-  int64_t* offs;
-  int64_t* err;
-  PartDesc* desc;
-  TileInfo* tiles;
-  uint32_t* words;            // worst-case size: the tile's interior words
-  uint32_t* edge_head;        // per tile: its bits of a first word it shares with an earlier tile
-  uint32_t* edge_tail;        // per tile: its bits of a last word it shares with a later tile
-  unsigned long long* state;  // per tile look-back status
-  unsigned long long* stats;  // [0] total bits (written by the last tile), [1] max bit width,
-                              // [2] DEVERR_* when a bounded wait gave up
+  const CfColumn* cols;
+  const int32_t* owner;
+  CfColumn single;
+  int64_t nitems;
+  uint32_t* edge_head;        // per item: its bits of a first word it shares with an earlier tile
+  uint32_t* edge_tail;        // per item: its bits of a last word it shares with a later tile
+  unsigned long long* state;  // per item look-back status, zero at launch
+  unsigned long long* status; // DEVERR_* when a bounded wait gave up
 };
 
 __device__ __forceinline__ void cf_sync() { asm volatile("bar.sync 1, %0;" ::"n"(kCfThreads) : "memory"); }
@@ -86,6 +76,7 @@ __device__ __forceinline__ unsigned long long ld_volatile_u64(const unsigned lon
 
 // Sum of the bits of all tiles before t (thread 0 of the compute warps).  Posts t's own count
 // first, so later tiles can look past t before t knows its prefix.  false when a wait gave up.
+// `state` is the column's first item's status; t the tile within the column.
 __device__ __forceinline__ bool cf_look_back(unsigned long long* state, int64_t t, unsigned long long agg,
                                              unsigned long long* prefix) {
   if (t == 0) {
@@ -114,8 +105,9 @@ template <typename T> __global__ void __launch_bounds__(kCfCTA)
 fixed_compress_kernel(FixedCompressArgs a) {
   extern __shared__ __align__(128) uint8_t smem[];
   __shared__ __align__(8) uint64_t full[kCfStages], empty[kCfStages];
-  __shared__ int64_t s_stile[kCfStages];
+  __shared__ int64_t s_stile[kCfStages];   // work item staged in each stage (-1: the end)
   __shared__ int s_shead[kCfStages];
+  __shared__ int s_scol[kCfStages];
   typedef typename HalfSums<T>::Acc Acc;
   __shared__ Acc s_acc[kCfMaxSegs][4];
   __shared__ int s_ovf[kCfMaxSegs];
@@ -136,30 +128,32 @@ fixed_compress_kernel(FixedCompressArgs a) {
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   __syncthreads();
-  const T* __restrict__ v = reinterpret_cast<const T*>(a.values);
 
   if (threadIdx.x >= kCfThreads) {  // ---- producer ----
     if (threadIdx.x != kCfThreads) return;
-    int64_t t = blockIdx.x;
-    for (int k = 0;; k++, t += gridDim.x) {
+    int64_t item = blockIdx.x;
+    for (int k = 0;; k++, item += gridDim.x) {
       const int st = k % kCfStages;
       if (k >= kCfStages && !mbar_wait_bounded(&empty[st], (uint32_t)((k / kCfStages) - 1) & 1u)) {
-        atomicExch(a.stats + 2, (unsigned long long)DEVERR_TIMEOUT);
+        atomicExch(a.status, (unsigned long long)DEVERR_TIMEOUT);
         s_stile[st] = -1;  // the compute warps stop at this stage (or time out on it)
         mbar_arrive(&full[st]);
         return;
       }
-      if (t >= a.ntiles) {
+      if (item >= a.nitems) {
         s_stile[st] = -1;
         mbar_arrive(&full[st]);  // no copy: completes the phase, the compute warps see the end
         return;
       }
-      const int64_t e0 = t * kDecodeTile;
-      const int cnt = (int)((a.n - e0) < kDecodeTile ? (a.n - e0) : kDecodeTile);
-      const uintptr_t addr = reinterpret_cast<uintptr_t>(v + e0);
+      const int c = a.owner ? a.owner[item] : 0;
+      const CfColumn& col = a.cols ? a.cols[c] : a.single;
+      const int64_t e0 = (item - col.item_base) * kDecodeTile;
+      const int cnt = (int)((col.n - e0) < kDecodeTile ? (col.n - e0) : kDecodeTile);
+      const uintptr_t addr = reinterpret_cast<uintptr_t>(reinterpret_cast<const T*>(col.values) + e0);
       const int head = (int)(addr & 15);
-      s_stile[st] = t;
+      s_stile[st] = item;
       s_shead[st] = head;
+      s_scol[st] = c;
       // the copy covers the 16-byte blocks that hold the tile's values, never another page
       const uint32_t bytes = (uint32_t)((head + (int64_t)cnt * (int64_t)sizeof(T) + 15) & ~15ll);
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -171,35 +165,37 @@ fixed_compress_kernel(FixedCompressArgs a) {
 
   // ---- compute warps ----
   const int tid = threadIdx.x;
-  const int L = a.L;
-  const int g = L >> 4;                     // threads per partition (16 values each)
-  const int W = g < 32 ? g : 32;            // lanes of one reduction segment
-  const int seg = tid / W;                  // reduction segment of this thread
-  const int segs_per_part = g / W;
-  const int p_me = tid / g;                 // this thread's partition within the tile
-  const int r_me = tid - p_me * g;          // and its first value there
   for (int k = 0;; k++) {
     const int st = k % kCfStages;
     const uint32_t par = (uint32_t)(k / kCfStages) & 1u;
     if (tid == 0) {
       s_ok = mbar_wait_bounded(&full[st], par);
       if (!s_ok) {
-        atomicExch(a.stats + 2, (unsigned long long)DEVERR_TIMEOUT);
+        atomicExch(a.status, (unsigned long long)DEVERR_TIMEOUT);
         mbar_wait_bounded(&full[st], par);  // a copy in flight lands before the CTA exits
       }
     }
     cf_sync();
     if (!s_ok) return;
     mbar_try_wait(&full[st], par);  // the phase is complete: orders this thread's reads after the copy
-    const int64_t t = s_stile[st];
-    if (t < 0) return;
+    const int64_t item = s_stile[st];
+    if (item < 0) return;
+    const CfColumn& col = a.cols ? a.cols[s_scol[st]] : a.single;
+    const int64_t t = item - col.item_base;  // the tile within its column
+    const int L = col.L;
+    const int g = L >> 4;                     // threads per partition (16 values each)
+    const int W = g < 32 ? g : 32;            // lanes of one reduction segment
+    const int seg = tid / W;                  // reduction segment of this thread
+    const int segs_per_part = g / W;
+    const int p_me = tid / g;                 // this thread's partition within the tile
+    const int r_me = tid - p_me * g;          // and its first value there
     uint8_t* stage = smem + (size_t)st * cf_stage_bytes<T>();
     T* x = reinterpret_cast<T*>(stage + s_shead[st]);
     // residuals: over the values for 8-byte types, in their own array for 4-byte types
     int64_t* res = sizeof(T) == 8 ? reinterpret_cast<int64_t*>(x)
                                   : reinterpret_cast<int64_t*>(smem + (size_t)kCfStages * cf_stage_bytes<T>());
     const int64_t e0 = t * kDecodeTile;
-    const int cnt = (int)((a.n - e0) < kDecodeTile ? (a.n - e0) : kDecodeTile);
+    const int cnt = (int)((col.n - e0) < kDecodeTile ? (col.n - e0) : kDecodeTile);
     const int np = (cnt + L - 1) / L;  // partitions in this tile (the last may be short)
     const int my_len = p_me < np ? ((cnt - p_me * L) < L ? (cnt - p_me * L) : L) : 0;
     const T* xp = x + p_me * L;
@@ -329,47 +325,48 @@ fixed_compress_kernel(FixedCompressArgs a) {
       }
       s_bl[np] = acc;
       unsigned long long prefix = 0;
-      if (!cf_look_back(a.state, t, (unsigned long long)acc, &prefix)) atomicExch(a.stats + 2, (unsigned long long)DEVERR_TIMEOUT);
+      if (!cf_look_back(a.state + col.item_base, t, (unsigned long long)acc, &prefix))
+        atomicExch(a.status, (unsigned long long)DEVERR_TIMEOUT);
       s_bit0 = prefix;
       TileInfo ti;
       ti.bit_lo = (int64_t)prefix;
-      ti.p_first = (int32_t)(t * a.parts_per_tile);
-      ti.p_last = (int32_t)(t * a.parts_per_tile + np - 1);
-      a.tiles[t] = ti;
-      if (t == a.ntiles - 1) {
+      ti.p_first = (int32_t)(t * col.parts_per_tile);
+      ti.p_last = (int32_t)(t * col.parts_per_tile + np - 1);
+      col.tiles[t] = ti;
+      if (t == col.ntiles - 1) {
         TileInfo te;
         te.bit_lo = (int64_t)(prefix + acc);
-        te.p_first = te.p_last = (int32_t)(a.P - 1);
-        a.tiles[a.ntiles] = te;
-        a.stats[0] = prefix + acc;
+        te.p_first = te.p_last = (int32_t)(col.P - 1);
+        col.tiles[col.ntiles] = te;
+        col.stats[0] = prefix + acc;
       }
-      if (bmax > 0) atomicMax(a.stats + 1, (unsigned long long)bmax);
+      if (bmax > 0) atomicMax(col.stats + 1, (unsigned long long)bmax);
     }
     cf_sync();
     const unsigned long long bit0 = s_bit0;
     if (tid < np) {  // the partitions' metadata and descriptors
       const int p = tid;
-      const int64_t gp = t * a.parts_per_tile + p;
+      const int64_t gp = t * col.parts_per_tile + p;
       const int32_t start = (int32_t)(e0 + (int64_t)p * L);
       const int type = s_direct[p] ? MODEL_DIRECT_COPY : MODEL_LINEAR;
       const int64_t off = (int64_t)bit0 + s_bl[p];
-      a.starts[gp] = start;
-      a.ends[gp] = start + s_len[p];
-      a.types[gp] = type;
-      a.params[4 * gp] = s_t0[p];
-      a.params[4 * gp + 1] = s_t1[p];
-      a.params[4 * gp + 2] = 0.0;
-      a.params[4 * gp + 3] = 0.0;
-      a.bits[gp] = s_b[p];
-      a.offs[gp] = off;
-      a.err[gp] = s_err[p];
+      col.starts[gp] = start;
+      col.ends[gp] = start + s_len[p];
+      col.types[gp] = type;
+      col.params[4 * gp] = s_t0[p];
+      col.params[4 * gp + 1] = s_t1[p];
+      col.params[4 * gp + 2] = 0.0;
+      col.params[4 * gp + 3] = 0.0;
+      col.bits[gp] = s_b[p];
+      col.offs[gp] = off;
+      col.err[gp] = s_err[p];
       PartDesc d;
       d.theta0 = s_t0[p];
       d.theta1 = s_t1[p];
       d.bit_off = off;
       d.start = start;
       d.bits_type = (s_b[p] & 0xff) | (type << 8);
-      a.desc[gp] = d;
+      col.desc[gp] = d;
     }
 
     // ---- C: words.  Word w covers tile-relative bits [32 w - sh0, 32 w - sh0 + 32). ----
@@ -380,9 +377,12 @@ fixed_compress_kernel(FixedCompressArgs a) {
       const bool first_partial = sh0 != 0;
       const bool last_partial = ((bit0 + (unsigned long long)tb) & 31) != 0;
       const uint32_t* f32 = reinterpret_cast<const uint32_t*>(res);  // low half of residual j at 2 j
-      uint32_t* out = a.words + (bit0 >> 5);
+      uint32_t* out = col.words + (bit0 >> 5);
+      // never past the word array (the caller sized it; a disagreement is reported, not written)
+      const bool fits = (int64_t)((bit0 + (unsigned long long)tb + 31) >> 5) <= col.words_cap;
+      if (!fits && tid == 0) atomicExch(a.status, (unsigned long long)DEVERR_BOUNDS);
       int qi = 0;
-      for (int w = tid; w < nw; w += kCfThreads) {
+      for (int w = fits ? tid : nw; w < nw; w += kCfThreads) {
         const int wb = 32 * w - sh0;
         int pos = wb > 0 ? wb : 0;
         const int wend = wb + 32 < tb ? wb + 32 : tb;
@@ -410,8 +410,8 @@ fixed_compress_kernel(FixedCompressArgs a) {
           }
           pos = qend;
         }
-        if (w == 0 && first_partial) a.edge_head[t] = word;
-        else if (w == nw - 1 && last_partial) a.edge_tail[t] = word;
+        if (w == 0 && first_partial) a.edge_head[item] = word;
+        else if (w == nw - 1 && last_partial) a.edge_tail[item] = word;
         else out[w] = word;
       }
     }
@@ -422,25 +422,30 @@ fixed_compress_kernel(FixedCompressArgs a) {
 
 // The words shared by neighbouring tiles.  Word W holding a tile's last bit, when that tile also
 // holds W's first bit, is written here by that tile's thread: its own bits (edge_tail) OR the
-// first bits of every later tile that starts inside W (edge_head; tiles without bits are skipped).
-__global__ void fixed_edges_kernel(const TileInfo* __restrict__ tiles, int64_t ntiles,
-                                   const uint32_t* __restrict__ edge_head, const uint32_t* __restrict__ edge_tail,
-                                   uint32_t* __restrict__ words) {
-  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= ntiles) return;
+// first bits of every later tile of the column that starts inside W (edge_head; tiles without
+// bits are skipped).  The column's last tile also zeroes the padding words after its bitstream.
+__global__ void fixed_edges_kernel(FixedCompressArgs a) {
+  const int64_t item = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (item >= a.nitems) return;
+  const CfColumn& col = a.cols ? a.cols[a.owner ? a.owner[item] : 0] : a.single;
+  const int64_t t = item - col.item_base;
+  const TileInfo* tiles = col.tiles;
   const int64_t b0 = tiles[t].bit_lo, b1 = tiles[t + 1].bit_lo;
+  if (t == col.ntiles - 1 && col.nwords_alloc > 0)
+    for (int64_t w = (b1 + 31) >> 5; w < col.nwords_alloc && w < col.words_cap; w++) col.words[w] = 0u;
   if (b1 == b0 || (b1 & 31) == 0) return;     // no bits, or a complete last word (already written)
   const int64_t wi = b1 >> 5;
+  if (wi >= col.words_cap) return;            // reported by the compress kernel
   if (b0 > (wi << 5)) return;                 // the tile starts inside W: an earlier tile owns it
-  uint32_t word = edge_tail[t];
-  for (int64_t u = t + 1; u < ntiles; u++) {
+  uint32_t word = a.edge_tail[item];
+  for (int64_t u = t + 1; u < col.ntiles; u++) {
     const int64_t c0 = tiles[u].bit_lo, c1 = tiles[u + 1].bit_lo;
     if (c1 == c0) continue;
     if ((c0 >> 5) != wi) break;
-    word |= edge_head[u];
+    word |= a.edge_head[col.item_base + u];
     if (c1 > ((wi + 1) << 5) || (c1 & 31) == 0) break;  // u goes past W
   }
-  words[wi] = word;
+  col.words[wi] = word;
 }
 
 template <typename T> static cudaError_t launch_fixed_compress_t(const FixedCompressArgs& a, int num_sms, cudaStream_t s) {
@@ -461,13 +466,22 @@ template <typename T> static cudaError_t launch_fixed_compress_t(const FixedComp
   if (per_sm < 1) per_sm = 1;
   // every CTA resident at once: a tile's look-back waits only on tiles that resident CTAs own
   int64_t grid = (int64_t)per_sm * num_sms;
-  if (grid > a.ntiles) grid = a.ntiles;
+  if (grid > a.nitems) grid = a.nitems;
   if (grid < 1) grid = 1;
   fixed_compress_kernel<T><<<(unsigned)grid, kCfCTA, smem, s>>>(a);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
-  fixed_edges_kernel<<<(unsigned)((a.ntiles + 255) / 256), 256, 0, s>>>(a.tiles, a.ntiles, a.edge_head, a.edge_tail,
-                                                                        a.words);
+  fixed_edges_kernel<<<(unsigned)((a.nitems + 255) / 256), 256, 0, s>>>(a);
   return cudaGetLastError();
+}
+
+static cudaError_t launch_fixed_compress_dt(glc_dtype dt, const FixedCompressArgs& a, int num_sms, cudaStream_t s) {
+  switch (dt) {
+    case GLC_I32: return launch_fixed_compress_t<int32_t>(a, num_sms, s);
+    case GLC_I64: return launch_fixed_compress_t<int64_t>(a, num_sms, s);
+    case GLC_U64: return launch_fixed_compress_t<uint64_t>(a, num_sms, s);
+    case GLC_U32: return launch_fixed_compress_t<uint32_t>(a, num_sms, s);
+  }
+  return cudaErrorInvalidValue;
 }
 
 bool fixed_compress_supported(int64_t n, int32_t L) {
@@ -479,50 +493,68 @@ int64_t fixed_compress_worst_words(glc_dtype dt, int64_t n) {
   return (n * per_value + 31) / 32 + 8;
 }
 
-size_t fixed_compress_scratch_bytes(int64_t n) {
-  const int64_t nt = (n + kDecodeTile - 1) / kDecodeTile;
-  return (size_t)nt * 8 + (size_t)nt * 4 * 2 + 64;
-}
+size_t fixed_compress_scratch_bytes(int64_t nitems) { return (size_t)nitems * 16 + 64; }
 
-// Compresses values (n of dt, fixed partitions of L) into c's metadata arrays and tables (allocated
-// by the caller for P = ceil(n / L) partitions) and into `words` (fixed_compress_worst_words
-// words); `scratch` holds fixed_compress_scratch_bytes(n) bytes; stats[0] receives the total bits,
-// stats[1] the widest field, stats[2] a DEVERR_* code (stats[0..3] zeroed here).
+// One column: values (n of dt, fixed partitions of L) into c's metadata arrays and tables
+// (allocated by the caller for P = ceil(n / L) partitions) and into `words`
+// (fixed_compress_worst_words words; its padding is left to the caller); `scratch` holds
+// fixed_compress_scratch_bytes(ntiles) bytes; stats[0] receives the total bits, stats[1] the
+// widest field, stats[2] a DEVERR_* code (stats[0..3] zeroed here).
 cudaError_t launch_fixed_compress(glc_dtype dt, const void* values, glc_column* c, int32_t L, uint32_t* words,
                                   void* scratch, unsigned long long* stats, cudaStream_t s) {
   FixedCompressArgs a{};
-  a.values = values;
-  a.n = c->n;
-  a.L = L;
-  a.parts_per_tile = kDecodeTile / L;
-  a.P = c->P;
-  a.ntiles = c->ntiles;
-  a.starts = c->d_start;
-  a.ends = c->d_end;
-  a.types = c->d_types;
-  a.params = c->d_params;
-  a.bits = c->d_bits;
-  a.offs = c->d_offs;
-  a.err = c->d_err;
-  a.desc = c->d_desc;
-  a.tiles = c->d_tiles;
-  a.words = words;
+  CfColumn& col = a.single;
+  col.values = values;
+  col.n = c->n;
+  col.L = L;
+  col.parts_per_tile = kDecodeTile / L;
+  col.P = c->P;
+  col.ntiles = c->ntiles;
+  col.item_base = 0;
+  col.nwords_alloc = 0;
+  col.starts = c->d_start;
+  col.ends = c->d_end;
+  col.types = c->d_types;
+  col.params = c->d_params;
+  col.bits = c->d_bits;
+  col.offs = c->d_offs;
+  col.err = c->d_err;
+  col.desc = c->d_desc;
+  col.tiles = c->d_tiles;
+  col.words = words;
+  col.words_cap = fixed_compress_worst_words(dt, c->n);
+  col.stats = stats;
+  a.nitems = c->ntiles;
   uint8_t* sp = reinterpret_cast<uint8_t*>(scratch);
   a.state = reinterpret_cast<unsigned long long*>(sp);
-  a.edge_head = reinterpret_cast<uint32_t*>(sp + (size_t)a.ntiles * 8);
-  a.edge_tail = a.edge_head + a.ntiles;
-  a.stats = stats;
+  a.edge_head = reinterpret_cast<uint32_t*>(sp + (size_t)a.nitems * 8);
+  a.edge_tail = a.edge_head + a.nitems;
+  a.status = stats + 2;
   cudaError_t e;
-  if ((e = cudaMemsetAsync(a.state, 0, (size_t)a.ntiles * 8, s)) != cudaSuccess) return e;
+  if ((e = cudaMemsetAsync(a.state, 0, (size_t)a.nitems * 8, s)) != cudaSuccess) return e;
   if ((e = cudaMemsetAsync(stats, 0, 4 * sizeof(unsigned long long), s)) != cudaSuccess) return e;
-  const int num_sms = c->ctx ? c->ctx->num_sms : 148;
-  switch (dt) {
-    case GLC_I32: return launch_fixed_compress_t<int32_t>(a, num_sms, s);
-    case GLC_I64: return launch_fixed_compress_t<int64_t>(a, num_sms, s);
-    case GLC_U64: return launch_fixed_compress_t<uint64_t>(a, num_sms, s);
-    case GLC_U32: return launch_fixed_compress_t<uint32_t>(a, num_sms, s);
-  }
-  return cudaErrorInvalidValue;
+  return launch_fixed_compress_dt(dt, a, c->ctx ? c->ctx->num_sms : 148, s);
+}
+
+// Many columns of one element type in one launch: cols (device, ncols entries, each with its own
+// arrays, stats zeroed and nwords_alloc set) and owner (device, nitems entries: the column of each
+// item, items in column order).  scratch: fixed_compress_scratch_bytes(nitems) bytes; status: a
+// DEVERR_* word.
+cudaError_t launch_fixed_compress_batch(glc_dtype dt, const CfColumn* cols, const int32_t* owner, int64_t nitems,
+                                        void* scratch, unsigned long long* status, int num_sms, cudaStream_t s) {
+  if (nitems <= 0) return cudaSuccess;
+  FixedCompressArgs a{};
+  a.cols = cols;
+  a.owner = owner;
+  a.nitems = nitems;
+  uint8_t* sp = reinterpret_cast<uint8_t*>(scratch);
+  a.state = reinterpret_cast<unsigned long long*>(sp);
+  a.edge_head = reinterpret_cast<uint32_t*>(sp + (size_t)nitems * 8);
+  a.edge_tail = a.edge_head + nitems;
+  a.status = status;
+  cudaError_t e;
+  if ((e = cudaMemsetAsync(a.state, 0, (size_t)nitems * 8, s)) != cudaSuccess) return e;
+  return launch_fixed_compress_dt(dt, a, num_sms, s);
 }
 
 }  // namespace glc

@@ -189,11 +189,36 @@ cudaError_t launch_fit(glc_dtype dt, const void* values, glc_column* c, void* sc
                        int64_t* d_stats, cudaStream_t s);
 cudaError_t launch_desc_and_tiles(glc_column* c, cudaStream_t s);
 // compress_fixed.cu: one-pass compression of fixed partitions of L values, L a divisor of 4096 and >= 256
+// One column of a launch (its arrays are the column's own, or its slices of a batch's arrays).
+struct CfColumn {
+  const void* values;
+  int64_t n;
+  int32_t L;
+  int32_t parts_per_tile;  // 4096 / L
+  int64_t P, ntiles;
+  int64_t item_base;       // work item of the column's tile 0
+  int64_t nwords_alloc;    // > 0: the edge pass also zeroes the words [total words, nwords_alloc)
+  int64_t words_cap;       // words the column's word array holds: nothing is written past it
+  int32_t* starts;
+  int32_t* ends;
+  int32_t* types;
+  double* params;
+  int32_t* bits;
+  int64_t* offs;
+  int64_t* err;
+  PartDesc* desc;
+  TileInfo* tiles;
+  uint32_t* words;             // the column's words (interior words of each tile)
+  unsigned long long* stats;   // [0] total bits (written by the last tile), [1] widest field
+};
+
 bool fixed_compress_supported(int64_t n, int32_t L);
 int64_t fixed_compress_worst_words(glc_dtype dt, int64_t n);
-size_t fixed_compress_scratch_bytes(int64_t n);
+size_t fixed_compress_scratch_bytes(int64_t nitems);  // nitems = 4096-value tiles of the launch
 cudaError_t launch_fixed_compress(glc_dtype dt, const void* values, glc_column* c, int32_t L, uint32_t* words,
                                   void* scratch, unsigned long long* stats, cudaStream_t s);
+cudaError_t launch_fixed_compress_batch(glc_dtype dt, const CfColumn* cols, const int32_t* owner, int64_t nitems,
+                                        void* scratch, unsigned long long* status, int num_sms, cudaStream_t s);
 cudaError_t launch_validate(const glc_column* c, int* d_bad, cudaStream_t s);
 cudaError_t launch_max_bits(const glc_column* c, int64_t* d_out, cudaStream_t s);
 // pack.cu: one column's arrays for the packer
