@@ -76,27 +76,43 @@ __device__ __forceinline__ unsigned long long ld_volatile_u64(const unsigned lon
 
 // Sum of the bits of all tiles before t (thread 0 of the compute warps).  Posts t's own count
 // first, so later tiles can look past t before t knows its prefix.  false when a wait gave up.
-// `state` is the column's first item's status; t the tile within the column.
+// Sum of the bits of all tiles before t in its column (`state` = the status of the column's tile
+// 0), by one warp: every lane reads one predecessor's status, 32 at a time (the warp-wide window of
+// the decoupled look-back), until the window holds an inclusive prefix; the aggregates between it
+// and t are added.  The warp waits (bounded) while a predecessor in the window has posted nothing.
+// Lane 0 posts t's own count first and its inclusive prefix at the end.  false when a wait gave up.
 __device__ __forceinline__ bool cf_look_back(unsigned long long* state, int64_t t, unsigned long long agg,
                                              unsigned long long* prefix) {
+  const int lane = threadIdx.x & 31;
   if (t == 0) {
-    atomicExch(state, kLbInc | agg);
+    if (lane == 0) atomicExch(state, kLbInc | agg);
     *prefix = 0;
     return true;
   }
-  atomicExch(state + t, kLbAgg | agg);
+  if (lane == 0) atomicExch(state + t, kLbAgg | agg);
   unsigned long long acc = 0;
-  int64_t k = t - 1;
+  int64_t hi = t - 1;
   const uint64_t t0 = global_ns();
   long long it = 0;
   bool ok = true;
   while (true) {
-    const unsigned long long s = ld_volatile_u64(state + k);
-    if (s & kLbInc) { acc += s & kLbVal; break; }
-    if (s & kLbAgg) { acc += s & kLbVal; k--; continue; }  // k > 0 here: tile 0 posts its prefix at once
-    if (++it > kSpinLimit || ((it & 255) == 0 && global_ns() - t0 > 2000000000ull)) { ok = false; break; }
+    const int64_t k = hi - lane;
+    // below tile 0 nothing is added (tile 0 posts its inclusive prefix, so the window stops there)
+    const unsigned long long sv = k >= 0 ? ld_volatile_u64(state + k) : kLbInc;
+    if (__any_sync(FULL_MASK, (sv & (kLbAgg | kLbInc)) == 0)) {
+      if (++it > kSpinLimit || ((it & 255) == 0 && global_ns() - t0 > 2000000000ull)) { ok = false; break; }
+      continue;
+    }
+    const unsigned inc = __ballot_sync(FULL_MASK, (sv & kLbInc) != 0);
+    const int stop = inc ? __ffs(inc) - 1 : 32;  // the nearest inclusive prefix in the window
+    unsigned long long v = lane <= stop ? (sv & kLbVal) : 0ull;
+#pragma unroll
+    for (int m = 16; m > 0; m >>= 1) v += __shfl_xor_sync(FULL_MASK, v, m);
+    acc += v;
+    if (inc) break;
+    hi -= 32;
   }
-  atomicExch(state + t, kLbInc | (acc + agg));
+  if (lane == 0) atomicExch(state + t, kLbInc | (acc + agg));
   *prefix = acc;
   return ok;
 }
@@ -118,7 +134,7 @@ fixed_compress_kernel(FixedCompressArgs a) {
   __shared__ long long s_err[kCfMaxParts];
   __shared__ int s_bl[kCfMaxParts + 1];
   __shared__ unsigned long long s_bit0;
-  __shared__ int s_ok;
+  __shared__ int s_ok, s_bmax;
 
   if (threadIdx.x == 0) {
     for (int st = 0; st < kCfStages; st++) {
@@ -316,7 +332,7 @@ fixed_compress_kernel(FixedCompressArgs a) {
       s_mb[p] = b > 1 ? 0xffffffffu / (uint32_t)b + 1u : 0u;
     }
     cf_sync();
-    if (tid == 0) {  // tile-relative bit ranges, the look-back, the tile's table entry
+    if (tid == 0) {  // tile-relative bit ranges
       int acc = 0, bmax = 0;
       for (int p = 0; p < np; p++) {
         s_bl[p] = acc;
@@ -324,9 +340,15 @@ fixed_compress_kernel(FixedCompressArgs a) {
         bmax = s_b[p] > bmax ? s_b[p] : bmax;
       }
       s_bl[np] = acc;
+      s_bmax = bmax;
+    }
+    cf_sync();
+    if (tid < 32) {  // the look-back (warp 0), the tile's table entry
+      const int acc = s_bl[np], bmax = s_bmax;
       unsigned long long prefix = 0;
-      if (!cf_look_back(a.state + col.item_base, t, (unsigned long long)acc, &prefix))
-        atomicExch(a.status, (unsigned long long)DEVERR_TIMEOUT);
+      const bool lb_ok = cf_look_back(a.state + col.item_base, t, (unsigned long long)acc, &prefix);
+      if (tid == 0) {
+      if (!lb_ok) atomicExch(a.status, (unsigned long long)DEVERR_TIMEOUT);
       s_bit0 = prefix;
       TileInfo ti;
       ti.bit_lo = (int64_t)prefix;
@@ -341,6 +363,7 @@ fixed_compress_kernel(FixedCompressArgs a) {
         col.stats[0] = prefix + acc;
       }
       if (bmax > 0) atomicMax(col.stats + 1, (unsigned long long)bmax);
+      }
     }
     cf_sync();
     const unsigned long long bit0 = s_bit0;
