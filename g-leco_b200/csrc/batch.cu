@@ -717,14 +717,20 @@ glc_status glc_batch_compress(glc_ctx* ctx, const glc_dtype* dtypes, const void*
                              s)) != cudaSuccess ||
         (e = cudaStreamSynchronize(s)) != cudaSuccess)
       return bail(bcuda(ctx, e, "batch compress: sizes"));
+    // the smallest compressed size; within 0.1 % of it, the length the tuner found to decode
+    // fastest for the element type and the column's mean field width (when the table holds one)
     for (int i = 0; i < nc && fixed_partition_len == 0; i++) {
-      int64_t best = INT64_MAX;
+      int64_t size[3], best = INT64_MAX;
       for (int k = 0; k < 3; k++) {
         const int64_t cand = kCandidates[k];
         const int64_t P = ns[i] > 0 ? (ns[i] + cand - 1) / cand : 0;
-        const int64_t size = 64 * P + 120 + (int64_t)(hbits[3 * i + k] + 7) / 8;  // api/G-LeCo.cuh:589-603
-        if (size < best) { best = size; len[i] = (int32_t)cand; }
+        size[k] = 64 * P + 120 + (int64_t)(hbits[3 * i + k] + 7) / 8;  // api/G-LeCo.cuh:589-603
+        if (size[k] < best) { best = size[k]; len[i] = (int32_t)cand; }
       }
+      const int mean_bits = ns[i] > 0 ? (int)((hbits[3 * i + 2] + ns[i] - 1) / ns[i]) : 0;
+      const int tuned = tune_entry(ctx, dtypes[i], mean_bits, 0).partition_len;
+      for (int k = 0; k < 3; k++)
+        if (kCandidates[k] == tuned && size[k] * 1000 <= best * 1001) len[i] = tuned;
     }
     int64_t total = 0;
     glc_status st = compress_one_pass(ctx, b, dtypes, values, ns, nc, len, hbits, s, &total);

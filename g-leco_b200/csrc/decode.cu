@@ -103,9 +103,10 @@ struct Cursor {
   bool nonneg;    // theta0 >= 0 and theta1 >= 0: predictions at x >= 0 are never negative
 };
 
-template <typename T, bool PLAIN, bool RESID, int kUnroll = 2>
+template <typename T, bool PLAIN, bool RESID, int kUnroll = 2, int CW = kConsumerWarps>
 __device__ __forceinline__ void decode_tile(const DecodeArgs& a, const StageInfo& si, const uint8_t* stage,
                                             const PartDesc* sdesc) {
+  constexpr int kThreads = CW * 32;  // consumer threads of the CTA
   typedef typename std::conditional<RESID, int64_t, T>::type OutT;
   // values per thread-vector: 32 bytes for 4-byte outputs (two 16-byte stores; the per-vector
   // cursor and address work is then shared by 8 values), 16 bytes for 8-byte outputs
@@ -251,15 +252,15 @@ __device__ __forceinline__ void decode_tile(const DecodeArgs& a, const StageInfo
   };
 
   if (E0 == tile_e0 && E1 - E0 == kDecodeTile) {  // full tile: every vector is in range
-    constexpr int kIters = kDecodeTile / V / kConsumers;
+    constexpr int kIters = kDecodeTile / V / kThreads;
 #pragma unroll kUnroll
     for (int it = 0; it < kIters; it++) {
-      const int e = Ea + (it * kConsumers + tid) * V;
+      const int e = Ea + (it * kThreads + tid) * V;
       if (c.idx < 0 || e >= c.next) seek(e);
       if (e <= c.next - V) fast_vec(e); else general_vec(e);  // e + V - 1 < next, without overflow
     }
   } else {
-    for (int j = tid; j < nvec; j += kConsumers) {
+    for (int j = tid; j < nvec; j += kThreads) {
       const int e = Ea + j * V;
       // e + V <= E1 and e + V - 1 < next, written so that they cannot overflow at n = 2^31 - 1
       if (e >= E0 && e <= E1 - V) {
@@ -271,8 +272,9 @@ __device__ __forceinline__ void decode_tile(const DecodeArgs& a, const StageInfo
   }
 }
 
-template <typename T, bool PLAIN, bool RESID, int kStages, int kUnroll>
-__global__ void __launch_bounds__(kPCThreads) decode_kernel(DecodeArgs a) {
+// CW consumer warps per CTA (8, or 4 for a tuned choice of the packed decode) + one producer warp.
+template <typename T, bool PLAIN, bool RESID, int kStages, int kUnroll, int CW = kConsumerWarps>
+__global__ void __launch_bounds__(CW * 32 + 32) decode_kernel(DecodeArgs a) {
   extern __shared__ __align__(128) uint8_t smem[];
   __shared__ __align__(128) PartDesc s_desc[kStages][kTileDescs];
   __shared__ __align__(8) uint64_t full[kStages], empty[kStages];
@@ -282,13 +284,13 @@ __global__ void __launch_bounds__(kPCThreads) decode_kernel(DecodeArgs a) {
   if (threadIdx.x == 0) {
     for (int s = 0; s < kStages; s++) {
       mbar_init(&full[s], 1);
-      mbar_init(&empty[s], kConsumerWarps);
+      mbar_init(&empty[s], CW);
     }
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   __syncthreads();
 
-  if (warp == kConsumerWarps) {  // ---- producer ----
+  if (warp == CW) {  // ---- producer ----
     if (lane != 0) return;
     for (int k = 0;; k++) {
       const int s = k % kStages;
@@ -347,7 +349,7 @@ __global__ void __launch_bounds__(kPCThreads) decode_kernel(DecodeArgs a) {
     }
     const StageInfo si = s_info[s];
     if (si.tile >= a.t_end) break;
-    decode_tile<T, PLAIN, RESID, kUnroll>(a, si, smem + (size_t)s * a.stage_bytes, &s_desc[s][0]);
+    decode_tile<T, PLAIN, RESID, kUnroll, CW>(a, si, smem + (size_t)s * a.stage_bytes, &s_desc[s][0]);
     __syncwarp();
     if (lane == 0) mbar_arrive(&empty[s]);
   }
@@ -586,14 +588,15 @@ int batch_stage_bytes(int max_bits) {
   return (int)(words * 4);
 }
 
-template <typename T, bool PLAIN, bool RESID, int kStages, int kUnroll>
+template <typename T, bool PLAIN, bool RESID, int kStages, int kUnroll, int CW = kConsumerWarps>
 static cudaError_t run_decode(glc_ctx* ctx, const DecodeArgs& a, cudaStream_t s) {
   const size_t smem = (size_t)kStages * a.stage_bytes;
-  void (*kern)(DecodeArgs) = decode_kernel<T, PLAIN, RESID, kStages, kUnroll>;
+  constexpr int kBlock = CW * 32 + 32;
+  void (*kern)(DecodeArgs) = decode_kernel<T, PLAIN, RESID, kStages, kUnroll, CW>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   int per_sm = 0;
-  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kPCThreads, smem);
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kBlock, smem);
   if (e != cudaSuccess) return e;
   if (per_sm < 1) per_sm = 1;
   const int64_t ntile = a.t_end - a.t_begin;
@@ -601,27 +604,35 @@ static cudaError_t run_decode(glc_ctx* ctx, const DecodeArgs& a, cudaStream_t s)
   if (grid > ntile) grid = ntile;
   if (grid < 1) return cudaSuccess;
   if ((e = cudaMemsetAsync(a.counter, 0, sizeof(int), s)) != cudaSuccess) return e;
-  kern<<<(unsigned)grid, kPCThreads, smem, s>>>(a);
+  kern<<<(unsigned)grid, kBlock, smem, s>>>(a);
   return cudaGetLastError();
 }
 
-// The unroll depth is a tuning choice of the packed value decode (the path every full and range
-// decode takes); the residual and pre-unpacked variants keep depth 2.
+// The unroll depth and the consumer warps per CTA (threads per tile) are tuning choices of the
+// packed value decode (the path every full and range decode takes); the residual and pre-unpacked
+// variants keep depth 2 and 8 warps.
+template <typename T, int kStages, int CW>
+static cudaError_t decode_packed(glc_ctx* ctx, const DecodeArgs& a, int unroll, cudaStream_t s) {
+  if (unroll == 1) return run_decode<T, false, false, kStages, 1, CW>(ctx, a, s);
+  if (unroll == 4) return run_decode<T, false, false, kStages, 4, CW>(ctx, a, s);
+  return run_decode<T, false, false, kStages, 2, CW>(ctx, a, s);
+}
+
 template <typename T, int kStages>
-static cudaError_t decode_staged(glc_ctx* ctx, const DecodeArgs& a, int plain, int resid, int unroll, cudaStream_t s) {
+static cudaError_t decode_staged(glc_ctx* ctx, const DecodeArgs& a, int plain, int resid, int unroll, int warps,
+                                 cudaStream_t s) {
   if (plain) return resid ? run_decode<T, true, true, kStages, 2>(ctx, a, s) : run_decode<T, true, false, kStages, 2>(ctx, a, s);
   if (resid) return run_decode<T, false, true, kStages, 2>(ctx, a, s);
-  if (unroll == 1) return run_decode<T, false, false, kStages, 1>(ctx, a, s);
-  if (unroll == 4) return run_decode<T, false, false, kStages, 4>(ctx, a, s);
-  return run_decode<T, false, false, kStages, 2>(ctx, a, s);
+  if (warps == 4) return decode_packed<T, kStages, 4>(ctx, a, unroll, s);
+  return decode_packed<T, kStages, kConsumerWarps>(ctx, a, unroll, s);
 }
 
 template <typename T>
 static cudaError_t decode_typed(glc_ctx* ctx, const DecodeArgs& a, int plain, int resid, int stages, int unroll,
-                                cudaStream_t s) {
-  if (stages == 2) return decode_staged<T, 2>(ctx, a, plain, resid, unroll, s);
-  if (stages == 4) return decode_staged<T, 4>(ctx, a, plain, resid, unroll, s);
-  return decode_staged<T, 3>(ctx, a, plain, resid, unroll, s);
+                                int warps, cudaStream_t s) {
+  if (stages == 2) return decode_staged<T, 2>(ctx, a, plain, resid, unroll, warps, s);
+  if (stages == 4) return decode_staged<T, 4>(ctx, a, plain, resid, unroll, warps, s);
+  return decode_staged<T, 3>(ctx, a, plain, resid, unroll, warps, s);
 }
 
 // Launch shape overrides for tuning sweeps (ring depth, stage capacity in words).
@@ -677,7 +688,8 @@ cudaError_t launch_decode_scratch(const glc_column* c, int64_t lo, int64_t hi, v
 }
 
 cudaError_t launch_decode_shape(glc_ctx* ctx, const glc_column* c, int plain_src, int residual_out, int64_t lo,
-                                int64_t hi, void* out_base, int stages, int unroll, int cap_words, cudaStream_t s) {
+                                int64_t hi, void* out_base, int stages, int unroll, int cap_words, int warps,
+                                cudaStream_t s) {
   if (hi <= lo || c->n <= 0) return cudaSuccess;
   if (((uintptr_t)out_base & 15) != 0) return cudaErrorMisalignedAddress;  // 16-byte vector stores
   DecodeArgs a;
@@ -707,23 +719,25 @@ cudaError_t launch_decode_shape(glc_ctx* ctx, const glc_column* c, int plain_src
     a.stage_bytes = (int)(words * 4);
   }
   switch (c->dtype) {
-    case GLC_I32: return decode_typed<int32_t>(ctx, a, plain_src, residual_out, stages, unroll, s);
-    case GLC_I64: return decode_typed<int64_t>(ctx, a, plain_src, residual_out, stages, unroll, s);
-    case GLC_U64: return decode_typed<uint64_t>(ctx, a, plain_src, residual_out, stages, unroll, s);
-    case GLC_U32: return decode_typed<uint32_t>(ctx, a, plain_src, residual_out, stages, unroll, s);
+    case GLC_I32: return decode_typed<int32_t>(ctx, a, plain_src, residual_out, stages, unroll, warps, s);
+    case GLC_I64: return decode_typed<int64_t>(ctx, a, plain_src, residual_out, stages, unroll, warps, s);
+    case GLC_U64: return decode_typed<uint64_t>(ctx, a, plain_src, residual_out, stages, unroll, warps, s);
+    case GLC_U32: return decode_typed<uint32_t>(ctx, a, plain_src, residual_out, stages, unroll, warps, s);
   }
   return cudaErrorInvalidValue;
 }
 
-// Ring depth, unroll depth and stage capacity from the context's tuning table for the column's
-// element type and widest field (GLC_DECODE_STAGES / _UNROLL / _CAP_WORDS override them, for sweeps).
+// Ring depth, unroll depth, stage capacity and consumer warps from the context's tuning table for
+// the column's element type and widest field (GLC_DECODE_STAGES / _UNROLL / _CAP_WORDS / _WARPS
+// override them, for sweeps).
 cudaError_t launch_decode(glc_ctx* ctx, const glc_column* c, int plain_src, int residual_out, int64_t lo, int64_t hi,
                           void* out_base, cudaStream_t s) {
   const TuneEntry& t = tune_entry(ctx, c->dtype, c->max_bits, plain_src);
   const int stages = env_int("GLC_DECODE_STAGES", t.decode_stages);
   const int unroll = env_int("GLC_DECODE_UNROLL", t.decode_unroll);
   const int cap = env_int("GLC_DECODE_CAP_WORDS", t.decode_cap_words);
-  return launch_decode_shape(ctx, c, plain_src, residual_out, lo, hi, out_base, stages, unroll, cap, s);
+  const int warps = env_int("GLC_DECODE_WARPS", t.decode_warps);
+  return launch_decode_shape(ctx, c, plain_src, residual_out, lo, hi, out_base, stages, unroll, cap, warps, s);
 }
 
 }  // namespace glc

@@ -51,9 +51,11 @@ struct TuneEntry {
   int32_t ra_shape;       // random-access launch shape (0..4)
   int32_t measured;       // 1 when set by a measurement
   int32_t decode_cap_words;  // largest tile staged in shared memory, in words (0 = built-in)
-  int32_t reserved;
+  int32_t decode_warps;      // consumer warps per CTA of the packed decode: 4 or 8 (0 = 8)
   float decode_gbs;       // decoded GB/s of the chosen decode shape (when measured)
   float ra_glookups;      // G lookups/s of the chosen random-access shape (when measured)
+  int32_t partition_len;  // fixed length (1024, 2048, 4096) whose column decoded fastest (0 = not measured)
+  int32_t reserved;
 };
 inline int tune_bucket(int bits) {
   return bits <= 8 ? 0 : bits <= 16 ? 1 : bits <= 24 ? 2 : bits <= 32 ? 3 : bits <= 48 ? 4 : 5;
@@ -255,7 +257,8 @@ cudaError_t launch_decode(glc_ctx* ctx, const glc_column* c, int plain_src, int 
                           int64_t hi, void* out_base, cudaStream_t s);
 // decode.cu: the same with an explicit ring depth and unroll depth (the tuner's candidates)
 cudaError_t launch_decode_shape(glc_ctx* ctx, const glc_column* c, int plain_src, int residual_out, int64_t lo,
-                                int64_t hi, void* out_base, int stages, int unroll, int cap_words, cudaStream_t s);
+                                int64_t hi, void* out_base, int stages, int unroll, int cap_words, int warps,
+                                cudaStream_t s);
 constexpr int kStageCapWordsMax = 8192 + 16;  // a whole tile of 64-bit fields
 // decode.cu: packed-source value decode with caller-supplied scratch; the counter must be zero.
 cudaError_t launch_decode_scratch(const glc_column* c, int64_t lo, int64_t hi, void* out_base, int* counter,

@@ -7,7 +7,11 @@
 //     (1, 2, 4): the values each CTA keeps in flight per tile; for fields wider than 32 bits also
 //     the largest tile staged in shared memory (6160 words, or a whole tile of 64-bit fields at
 //     the cost of fewer CTAs per SM; larger tiles are read from global memory);
-//   - the random-access launch shape (lookups per thread x CTAs per SM, five candidates).
+//   - the consumer warps per CTA of the packed decode (4 or 8: the threads that share a tile);
+//   - the random-access launch shape (lookups per thread x CTAs per SM, five candidates);
+//   - the fixed partition length (1024, 2048, 4096) whose column decodes fastest; the batched
+//     compress prefers it when two lengths give the same size (the length is otherwise chosen per
+//     column by the exact compressed size).
 // glc_autotune times every candidate on a synthetic fixed-partitioned column whose fields have the
 // bucket's width (48M values, larger than L2) and keeps the fastest; the table can be written to
 // and read from a text file keyed by the device (name, SM count, compute capability).
@@ -23,7 +27,7 @@ using namespace glc;
 
 namespace {
 
-constexpr int kTuneVersion = 2;
+constexpr int kTuneVersion = 3;
 constexpr int64_t kTuneValues = 48ll << 20;
 constexpr int64_t kTuneLookups = 16ll << 20;
 constexpr int kNoiseBits[kTuneBuckets] = {5, 13, 21, 29, 45, 59};  // fields of 6..60 bits
@@ -74,8 +78,8 @@ bool tune_save(const glc_ctx* ctx, const char* path) {
     for (int b = 0; b < kTuneBuckets; b++)
       for (int p = 0; p < 2; p++) {
         const TuneEntry& t = ctx->tune[d][b][p];
-        fprintf(f, "%d %d %d %d %d %d %d %.3f %.4f\n", d, b, p, t.decode_stages, t.decode_unroll, t.ra_shape,
-                t.decode_cap_words, t.decode_gbs, t.ra_glookups);
+        fprintf(f, "%d %d %d %d %d %d %d %d %d %.3f %.4f\n", d, b, p, t.decode_stages, t.decode_unroll, t.ra_shape,
+                t.decode_cap_words, t.decode_warps, t.partition_len, t.decode_gbs, t.ra_glookups);
       }
   if (fclose(f) != 0) {
     remove(tmp.c_str());
@@ -124,6 +128,8 @@ void glc::tune_defaults(glc_ctx* ctx) {
         t.ra_shape = p ? 3 : (b <= 3 ? 4 : (b == 4 ? 0 : 3));
         t.measured = 0;
         t.decode_cap_words = (wide_type && !p && b == kTuneBuckets - 1) ? kStageCapWordsMax : 0;
+        t.decode_warps = 0;
+        t.partition_len = 0;
         t.reserved = 0;
         t.decode_gbs = 0.f;
         t.ra_glookups = 0.f;
@@ -142,12 +148,16 @@ bool glc::tune_load(glc_ctx* ctx, const char* path) {
   TuneEntry tab[4][kTuneBuckets][2];
   int seen = 0;
   while (ok && fgets(line, sizeof line, f)) {
-    int d, b, p, st, un, ra, cap;
+    int d, b, p, st, un, ra, cap, wp, pl;
     float gbs, gl;
-    if (sscanf(line, "%d %d %d %d %d %d %d %f %f", &d, &b, &p, &st, &un, &ra, &cap, &gbs, &gl) != 9) { ok = false; break; }
+    if (sscanf(line, "%d %d %d %d %d %d %d %d %d %f %f", &d, &b, &p, &st, &un, &ra, &cap, &wp, &pl, &gbs, &gl) != 11) {
+      ok = false;
+      break;
+    }
     if (d < 0 || d > 3 || b < 0 || b >= kTuneBuckets || p < 0 || p > 1 || st < 2 || st > 4 ||
-        (un != 1 && un != 2 && un != 4) || ra < 0 || ra > 4 || cap < 0 || cap > kStageCapWordsMax) { ok = false; break; }
-    tab[d][b][p] = TuneEntry{st, un, ra, 1, cap, 0, gbs, gl};
+        (un != 1 && un != 2 && un != 4) || ra < 0 || ra > 4 || cap < 0 || cap > kStageCapWordsMax ||
+        (wp != 0 && wp != 4 && wp != 8) || (pl != 0 && pl != 1024 && pl != 2048 && pl != 4096)) { ok = false; break; }
+    tab[d][b][p] = TuneEntry{st, un, ra, 1, cap, wp, gbs, gl, pl, 0};
     seen++;
   }
   fclose(f);
@@ -162,8 +172,8 @@ glc_status glc_tune_get(const glc_ctx* ctx, glc_dtype dtype, int32_t field_bits,
                         glc_tune_entry* out) {
   if (!ctx || !out || (int)dtype < 0 || (int)dtype > 3 || field_bits < 0 || field_bits > 64) return GLC_ERR_INVALID_ARG;
   const TuneEntry& t = tune_entry(ctx, dtype, field_bits, preunpacked);
-  *out = glc_tune_entry{t.decode_stages, t.decode_unroll, t.ra_shape, t.measured, t.decode_cap_words, 0,
-                        t.decode_gbs, t.ra_glookups};
+  *out = glc_tune_entry{t.decode_stages, t.decode_unroll, t.ra_shape, t.measured, t.decode_cap_words,
+                        t.decode_warps, t.decode_gbs, t.ra_glookups, t.partition_len, 0};
   return GLC_OK;
 }
 
@@ -172,11 +182,13 @@ glc_status glc_tune_set(glc_ctx* ctx, glc_dtype dtype, int32_t field_bits, int32
   if (!ctx || !e || (int)dtype < 0 || (int)dtype > 3 || field_bits < 0 || field_bits > 64) return GLC_ERR_INVALID_ARG;
   if (e->decode_stages < 2 || e->decode_stages > 4 || (e->decode_unroll != 1 && e->decode_unroll != 2 &&
       e->decode_unroll != 4) || e->ra_shape < 0 || e->ra_shape > 4 || e->decode_cap_words < 0 ||
-      e->decode_cap_words > kStageCapWordsMax)
+      e->decode_cap_words > kStageCapWordsMax || (e->decode_warps != 0 && e->decode_warps != 4 &&
+      e->decode_warps != 8) || (e->partition_len != 0 && e->partition_len != 1024 && e->partition_len != 2048 &&
+      e->partition_len != 4096))
     return tfail(ctx, GLC_ERR_INVALID_ARG, "tune entry out of range");
   ctx->tune[(int)dtype][tune_bucket(field_bits)][preunpacked ? 1 : 0] =
-      TuneEntry{e->decode_stages, e->decode_unroll, e->ra_shape, e->measured, e->decode_cap_words, 0, e->decode_gbs,
-                e->ra_glookups};
+      TuneEntry{e->decode_stages, e->decode_unroll, e->ra_shape, e->measured, e->decode_cap_words, e->decode_warps,
+                e->decode_gbs, e->ra_glookups, e->partition_len, 0};
   return GLC_OK;
 }
 
@@ -220,21 +232,25 @@ glc_status glc_autotune(glc_ctx* ctx, const char* cache_path, int32_t flags) {
         float best_ms = 1e30f;
         for (int cap : {0, kStageCapWordsMax}) {
           if (cap && (plain || col->max_bits <= 32)) continue;  // only tiles of wide fields exceed the default
-          for (int stages = 2; stages <= 4; stages++)
-            for (int unroll : {1, 2, 4}) {
-              if (plain && unroll != 2) continue;  // the pre-unpacked decode has no unroll choice
-              const float ms = time_launches([&] {
-                return launch_decode_shape(ctx, col, plain, 0, 0, kTuneValues, out, stages, unroll, cap, s);
-              }, s, e0, e1);
-              if (ms < 0.f) { st = tfail(ctx, GLC_ERR_CUDA, "autotune: decode launch failed"); break; }
-              if (ms < best_ms) {
-                best_ms = ms;
-                best.decode_stages = stages;
-                best.decode_unroll = unroll;
-                best.decode_cap_words = cap;
-                best.decode_gbs = (float)(dtype_size(dt) * (double)kTuneValues / (ms * 1e6));
+          for (int warps : {8, 4}) {
+            if (plain && warps != 8) continue;  // the pre-unpacked decode keeps 8 warps
+            for (int stages = 2; stages <= 4; stages++)
+              for (int unroll : {1, 2, 4}) {
+                if (plain && unroll != 2) continue;  // the pre-unpacked decode has no unroll choice
+                const float ms = time_launches([&] {
+                  return launch_decode_shape(ctx, col, plain, 0, 0, kTuneValues, out, stages, unroll, cap, warps, s);
+                }, s, e0, e1);
+                if (ms < 0.f) { st = tfail(ctx, GLC_ERR_CUDA, "autotune: decode launch failed"); break; }
+                if (ms < best_ms) {
+                  best_ms = ms;
+                  best.decode_stages = stages;
+                  best.decode_unroll = unroll;
+                  best.decode_cap_words = cap;
+                  best.decode_warps = warps;
+                  best.decode_gbs = (float)(dtype_size(dt) * (double)kTuneValues / (ms * 1e6));
+                }
               }
-            }
+          }
         }
         float best_ra = 1e30f;
         for (int shape = 0; shape < 5 && st == GLC_OK; shape++) {
@@ -252,6 +268,26 @@ glc_status glc_autotune(glc_ctx* ctx, const char* cache_path, int32_t flags) {
         tab[d][bucket][plain] = best;
       }
       glc_column_free(col);
+      // partition length: the same column at 1024 and 2048 values per partition, decoded with the
+      // packed shape just chosen; the fastest of the three lengths is kept
+      if (st == GLC_OK) {
+        TuneEntry& tp = tab[d][bucket][0];
+        int best_len = 4096;
+        float best_len_ms = (float)(dtype_size(dt) * (double)kTuneValues / (tp.decode_gbs * 1e6));
+        for (int L : {2048, 1024}) {
+          glc_column* cl = nullptr;
+          if ((st = glc_compress(ctx, dt, vals, kTuneValues, 0, GLC_PART_FIXED, L, &cl, nullptr, s)) != GLC_OK) break;
+          const float ms = time_launches([&] {
+            return launch_decode_shape(ctx, cl, 0, 0, 0, kTuneValues, out, tp.decode_stages, tp.decode_unroll,
+                                       tp.decode_cap_words, tp.decode_warps, s);
+          }, s, e0, e1);
+          glc_column_free(cl);
+          if (ms < 0.f) { st = tfail(ctx, GLC_ERR_CUDA, "autotune: decode launch failed"); break; }
+          if (ms < best_len_ms) { best_len_ms = ms; best_len = L; }
+        }
+        tp.partition_len = best_len;
+        tab[d][bucket][1].partition_len = best_len;
+      }
       if (st == GLC_OK) st = glc_sync(ctx, s);  // a device-side wait that gave up fails the tuning
     }
     if (st == GLC_OK && nb < kTuneBuckets)  // wider buckets of 4-byte types reuse the 32-bit choice

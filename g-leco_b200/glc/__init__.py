@@ -66,8 +66,9 @@ class ColumnInfo(ctypes.Structure):
 
 class TuneEntry(ctypes.Structure):
     _fields_ = [("decode_stages", ctypes.c_int32), ("decode_unroll", ctypes.c_int32), ("ra_shape", ctypes.c_int32),
-                ("measured", ctypes.c_int32), ("decode_cap_words", ctypes.c_int32), ("reserved", ctypes.c_int32),
-                ("decode_gbs", ctypes.c_float), ("ra_glookups", ctypes.c_float)]
+                ("measured", ctypes.c_int32), ("decode_cap_words", ctypes.c_int32), ("decode_warps", ctypes.c_int32),
+                ("decode_gbs", ctypes.c_float), ("ra_glookups", ctypes.c_float), ("partition_len", ctypes.c_int32),
+                ("reserved", ctypes.c_int32)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -217,8 +218,8 @@ def tune_get(ctx: "Context", dtype: int, field_bits: int, preunpacked: bool = Fa
 
 
 def tune_set(ctx: "Context", dtype: int, field_bits: int, preunpacked: bool, stages: int, unroll: int, ra_shape: int,
-             cap_words: int = 0):
-    e = TuneEntry(stages, unroll, ra_shape, 0, cap_words, 0, 0.0, 0.0)
+             cap_words: int = 0, warps: int = 0, partition_len: int = 0):
+    e = TuneEntry(stages, unroll, ra_shape, 0, cap_words, warps, 0.0, 0.0, partition_len, 0)
     ctx.check(ctx.lib.glc_tune_set(ctx.handle, dtype, field_bits, 1 if preunpacked else 0, ctypes.byref(e)))
 
 

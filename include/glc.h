@@ -281,17 +281,22 @@ typedef struct glc_tune_entry {
   int32_t measured;       /* 1 when chosen by glc_autotune, 0 for the built-in default */
   int32_t decode_cap_words; /* largest tile staged in shared memory, in 32-bit words: 0 = 6160
                              (48-bit fields), up to 8208 (a whole tile of 64-bit fields) */
-  int32_t reserved;       /* 0 */
+  int32_t decode_warps;   /* consumer warps per CTA of the packed decode (the threads that share a
+                             4096-value tile): 4 or 8 (0 = 8) */
   float decode_gbs;       /* decoded GB/s of the chosen shape on the tuning column */
   float ra_glookups;      /* G lookups/s of the chosen random-access shape */
+  int32_t partition_len;  /* fixed partition length (1024, 2048, 4096) whose column decoded fastest;
+                             glc_batch_compress prefers it between lengths of equal size (0 = none) */
+  int32_t reserved;       /* 0 */
 } glc_tune_entry;
 
 enum { GLC_TUNE_FORCE = 1 };
 
-/* Time every candidate decode shape (ring depth x unroll depth) and random-access shape on this
- * context's device, per element type, widest-field bucket (<= 8, 16, 24, 32, 48, 64 bits) and
- * residual source (packed, pre-unpacked), each on a synthetic fixed-partitioned column of 48M
- * values with fields of that width, and keep the fastest in the context (about 2 s).  With
+/* Time every candidate decode shape (ring depth x unroll depth x consumer warps x stage capacity)
+ * and random-access shape on this context's device, per element type, widest-field bucket (<= 8,
+ * 16, 24, 32, 48, 64 bits) and residual source (packed, pre-unpacked), each on a synthetic
+ * fixed-partitioned column of 48M values with fields of that width, and the partition length
+ * (1024, 2048, 4096) whose column decodes fastest; keep the fastest in the context (a few seconds).  With
  * cache_path, results already stored there for this device (name, SM count, compute capability)
  * are loaded instead (unless GLC_TUNE_FORCE), and new results are written there.  A context also
  * loads the file named by the GLC_TUNE_CACHE environment variable when it is created. */

@@ -26,9 +26,9 @@ def _column_values(dt, n, noise_bits, seed):
     return ((1 << 40) + 1000 * i + rng.integers(0, 1 << noise_bits, n)).astype(np.int64)
 
 
-def _set_all(ctx, dt, plain, stages, unroll, ra_shape):
+def _set_all(ctx, dt, plain, stages, unroll, ra_shape, warps=0):
     for b in (8, 16, 24, 32, 48, 64):  # every bucket, whatever the column's widest field
-        glc.tune_set(ctx, dt, b, plain, stages, unroll, ra_shape)
+        glc.tune_set(ctx, dt, b, plain, stages, unroll, ra_shape, warps=warps)
 
 
 @pytest.mark.parametrize("dt", [glc.I32, glc.I64, glc.U64, glc.U32])
@@ -48,12 +48,21 @@ def test_every_shape_is_bit_exact(dt, mode):
         src = glc.SRC_PREUNPACKED if plain else glc.SRC_PACKED
         for stages in (2, 3, 4):
             for unroll in ((1, 2, 4) if not plain else (2,)):
-                _set_all(ctx, dt, plain, stages, unroll, 0)
-                out.fill_(0)
-                torch.cuda.synchronize()  # the library runs on its own stream
-                glc.decompress_into(ctx, col, out.data_ptr(), source=src)
-                ctx.sync()
-                assert np.array_equal(out.cpu().numpy().view(NP[dt]), v), (plain, stages, unroll)
+                for warps in ((8, 4) if not plain else (8,)):  # consumer warps per CTA
+                    _set_all(ctx, dt, plain, stages, unroll, 0, warps)
+                    out.fill_(0)
+                    torch.cuda.synchronize()  # the library runs on its own stream
+                    glc.decompress_into(ctx, col, out.data_ptr(), source=src)
+                    ctx.sync()
+                    assert np.array_equal(out.cpu().numpy().view(NP[dt]), v), (plain, stages, unroll, warps)
+        # a range decode with a partial first and last tile on 4 warps
+        if not plain:
+            _set_all(ctx, dt, plain, 3, 2, 0, 4)
+            part = torch.zeros(len(v), dtype=TH[dt], device="cuda:0")
+            torch.cuda.synchronize()
+            glc.decompress_range_into(ctx, col, 1001, 200_003, part.data_ptr() + 1001 * v.itemsize, source=src)
+            ctx.sync()
+            assert np.array_equal(part.cpu().numpy().view(NP[dt])[1001:201_004], v[1001:201_004])
         for ra_shape in range(5):
             _set_all(ctx, dt, plain, 2, 2, ra_shape)
             ra.fill_(0)
@@ -77,13 +86,15 @@ def test_autotune_measures_and_caches(tmp_path):
                 e = glc.tune_get(ctx, dt, b, plain)
                 assert e.measured == 1 and e.decode_gbs > 0 and e.ra_glookups > 0
                 assert e.decode_stages in (2, 3, 4) and e.decode_unroll in (1, 2, 4) and 0 <= e.ra_shape <= 4
-                got[(dt, b, plain)] = (e.decode_stages, e.decode_unroll, e.ra_shape)
+                assert e.decode_warps in (4, 8) and e.partition_len in (1024, 2048, 4096)
+                got[(dt, b, plain)] = (e.decode_stages, e.decode_unroll, e.ra_shape, e.decode_warps, e.partition_len)
     # a second context loads the file instead of measuring
     ctx2 = glc.Context(0)
     glc.autotune(ctx2, path)
     for (dt, b, plain), shape in got.items():
         e = glc.tune_get(ctx2, dt, b, plain)
-        assert e.measured == 1 and (e.decode_stages, e.decode_unroll, e.ra_shape) == shape
+        assert e.measured == 1 and (e.decode_stages, e.decode_unroll, e.ra_shape, e.decode_warps,
+                                    e.partition_len) == shape
     # a file written for another device is ignored by a new context
     with open(path) as f:
         lines = f.read().splitlines()
