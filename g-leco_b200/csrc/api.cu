@@ -300,36 +300,27 @@ static glc_status compress_impl(glc_ctx* ctx, glc_dtype dtype, const void* dev_v
   }
   CK(alloc_meta(c, s), "compress: metadata allocation");
   if (mode == GLC_PART_FIXED && fixed_compress_supported(n, fixed_len)) {
-    // one pass over the values: fit, widths, offsets, tables and words in one kernel; the words go
-    // to a worst-case buffer and the used ones into the column's exact-size array
-    uint32_t* wtmp = nullptr;
+    // one read of the values: fit, widths and words of every tile (into scratch slots), a scan of
+    // the tiles' bits; then, with the total known, the words placed into an exact-size array
     void* scratch = nullptr;
-    CK(pool_alloc(ctx, &wtmp, 4 * (size_t)fixed_compress_worst_words(dtype, n), s), "compress: word buffer");
-    cudaError_t e = pool_alloc(ctx, &scratch, fixed_compress_scratch_bytes((n + kDecodeTile - 1) / kDecodeTile), s);
-    if (e == cudaSuccess)
-      e = launch_fixed_compress(dtype, dev_values, c, fixed_len, wtmp, scratch, (unsigned long long*)ctx->d_stats, s);
+    CK(pool_alloc(ctx, &scratch, fixed_compress_scratch_bytes(dtype, c->ntiles), s), "compress: scratch");
+    unsigned long long* st = (unsigned long long*)ctx->d_stats;
+    cudaError_t e = launch_fixed_compress(dtype, dev_values, c, fixed_len, scratch, st, s);
     if (e == cudaSuccess) e = cudaMemcpyAsync(ctx->h_stats, ctx->d_stats, 3 * sizeof(int64_t), cudaMemcpyDeviceToHost, s);
-    if (scratch) cudaFreeAsync(scratch, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-    if (e != cudaSuccess) {
-      cudaFreeAsync(wtmp, s);
-      return cuda_fail(ctx, e, "compress: one-pass fixed compression");
+    if (e == cudaSuccess && ctx->h_stats[2] != DEVERR_NONE) {
+      cudaFreeAsync(scratch, s);
+      return fail(ctx, GLC_ERR_TIMEOUT, "compress: a device-side wait gave up");
     }
-    if (ctx->h_stats[2] != DEVERR_NONE) {
-      cudaFreeAsync(wtmp, s);
-      return ctx->h_stats[2] == DEVERR_TIMEOUT ? fail(ctx, GLC_ERR_TIMEOUT, "compress: a device-side wait gave up")
-                                               : fail(ctx, GLC_ERR_CUDA, "compress: words beyond their array");
+    if (e == cudaSuccess) {
+      c->total_bits = ctx->h_stats[0];
+      c->max_bits = (int32_t)ctx->h_stats[1];
+      set_word_counts(c);
+      e = col_alloc(c, &c->d_words, 4 * c->nwords_alloc, s);
     }
-    c->total_bits = ctx->h_stats[0];
-    c->max_bits = (int32_t)ctx->h_stats[1];
-    set_word_counts(c);
-    e = col_alloc(c, &c->d_words, 4 * c->nwords_alloc, s);
-    if (e == cudaSuccess && c->nwords > 0)
-      e = cudaMemcpyAsync(c->d_words, wtmp, 4 * (size_t)c->nwords, cudaMemcpyDeviceToDevice, s);
-    if (e == cudaSuccess)
-      e = cudaMemsetAsync(c->d_words + c->nwords, 0, 4 * (size_t)(c->nwords_alloc - c->nwords), s);
-    cudaFreeAsync(wtmp, s);
-    if (e != cudaSuccess) return cuda_fail(ctx, e, "compress: words");
+    if (e == cudaSuccess) e = launch_fixed_place(dtype, c, fixed_len, scratch, st, s);
+    cudaFreeAsync(scratch, s);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "compress: one-pass fixed compression");
     c->reported_size = reported_size(c->P, c->total_bits);
     return GLC_OK;
   }

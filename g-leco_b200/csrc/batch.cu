@@ -608,14 +608,17 @@ glc_status compress_one_pass(glc_ctx* ctx, glc_batch* b, const glc_dtype* dtypes
     int64_t* d_ib;
     int32_t* d_owner;
     uint8_t* scratch;
-    if ((e = dalloc(b, &d_g, g.size())) || (e = dalloc(b, &d_ib, ib.size())) || (e = dalloc(b, &d_owner, nitems)) ||
-        (e = dalloc(b, &scratch, fixed_compress_scratch_bytes(nitems))))
+    if ((e = dalloc(b, &d_g, g.size())) || (e = dalloc(b, &d_ib, ib.size())) || (e = dalloc(b, &d_owner, nitems)))
       return bcuda(ctx, e, "batch compress: allocation");
+    // the tiles' slots are scratch: from the context's pool, returned after the launch
+    BCK(cudaMallocFromPoolAsync((void**)&scratch, fixed_compress_scratch_bytes(dt, nitems), ctx->pool, s),
+        "batch compress: scratch");
     BCK(cudaMemcpyAsync(d_g, g.data(), sizeof(CfColumn) * g.size(), cudaMemcpyHostToDevice, s), "batch compress: columns");
     BCK(cudaMemcpyAsync(d_ib, ib.data(), sizeof(int64_t) * ib.size(), cudaMemcpyHostToDevice, s), "batch compress: columns");
     BCK(launch_pack_item_owner(d_ib, (int)g.size(), d_owner, s), "batch compress: work list");
-    BCK(launch_fixed_compress_batch(dt, d_g, d_owner, nitems, scratch, stats + 2 * (size_t)nc, ctx->num_sms, s),
-        "batch compress: one-pass compress");
+    e = launch_fixed_compress_batch(dt, d_g, d_owner, nitems, scratch, stats + 2 * (size_t)nc, ctx->num_sms, s);
+    cudaFreeAsync(scratch, s);
+    BCK(e, "batch compress: one-pass compress");
     BCK(cudaStreamSynchronize(s), "batch compress: sync");  // the host vectors above are reused next
   }
   std::vector<unsigned long long> hs(2 * (size_t)nc + 1);

@@ -18,20 +18,22 @@
 //     B  the residual of every value (fma prediction, round half away from zero, saturating
 //        cast; calculateDelta) written over the staged value (8-byte types) or into a residual
 //        array (4-byte types), and max |residual| per partition -> the partition's bit width;
-//     -  the tile's first bit: a decoupled look-back over per-tile status words (each tile posts
-//        its bit count, then its inclusive prefix once known; Merrill & Garland, "Single-pass
-//        parallel prefix scan with decoupled look-back", 2016);
-//     C  the tile's words from the residual fields, one thread per word; a word the tile shares
-//        with a neighbouring tile goes to a side table (edge_head / edge_tail) and
-//        fixed_edges_kernel merges it afterwards, so no word is written twice and nothing needs
-//        zeroing first;
-//     -  the partitions' metadata (the reference's SoA), their 32-byte descriptors and the
-//        tile's decode-table entry.
+//     C  the tile's words from the residual fields, one thread per word, into the tile's own
+//        slot of a scratch array (slots of the worst-case size of a tile, bit offsets relative to
+//        the tile), with the partitions' metadata (the reference's SoA), their descriptors and
+//        the tile's decode-table entry, all with tile-relative bit offsets, and the tile's bit
+//        count;
+//   then an exclusive scan of the tiles' bit counts gives every tile's first bit, and
+//   fixed_place_kernel (one CTA per tile) writes each word of the column once -- the word holding
+//   bit 32 W is built by the tile that holds that bit, from its slot with a funnel shift, ORed
+//   with the first bits of any later tiles that start inside it -- and adds the tile's first bit
+//   to its partitions' offsets, descriptors and decode-table entry.  No tile waits for another.
 //
-// The words go to a buffer of the worst-case size (64 bits per value for 8-byte types, 33 for
-// 4-byte types); the caller copies the used words into the column's exact-size array.
+// The column's word array is allocated at its exact size between the two kernels (the scan gives
+// the total); the slots cost one extra write and read of the compressed bits.
 #include <type_traits>
 #include "glc_internal.h"
+#include "glc_scan.cuh"
 #include "glc_tma.cuh"
 
 namespace glc {
@@ -49,10 +51,6 @@ template <typename T> __host__ __device__ constexpr int cf_smem_bytes() {
   return kCfStages * cf_stage_bytes<T>() + (sizeof(T) == 4 ? kDecodeTile * 8 : 0);
 }
 
-// Look-back status of a tile: top two bits 1 = its own bit count posted, 2 = its inclusive prefix
-// posted; the low 62 bits hold the count.  Zero at launch.
-constexpr unsigned long long kLbAgg = 1ull << 62, kLbInc = 2ull << 62, kLbVal = (1ull << 62) - 1;
-
 // A launch: work item i = one 4096-value tile of column owner[i] (every column of one element
 // type, tiles in order), or of `single` when cols is null.
 struct FixedCompressArgs {
@@ -60,61 +58,51 @@ struct FixedCompressArgs {
   const int32_t* owner;
   CfColumn single;
   int64_t nitems;
-  uint32_t* edge_head;        // per item: its bits of a first word it shares with an earlier tile
-  uint32_t* edge_tail;        // per item: its bits of a last word it shares with a later tile
-  unsigned long long* state;  // per item look-back status, zero at launch
-  unsigned long long* status; // DEVERR_* when a bounded wait gave up
+  uint32_t* slots;            // item i's words at slots + i * slot_words (tile-relative bits)
+  int64_t slot_words;
+  int64_t* tile_bits;         // per item: bits of the tile (nitems + 1 entries: the scan's input)
+  const int64_t* tile_first;  // per item: exclusive scan of tile_bits over the launch (nitems + 1)
+  unsigned long long* status; // DEVERR_* when a bounded wait gave up or a column's words overflow
 };
 
 __device__ __forceinline__ void cf_sync() { asm volatile("bar.sync 1, %0;" ::"n"(kCfThreads) : "memory"); }
 
-__device__ __forceinline__ unsigned long long ld_volatile_u64(const unsigned long long* p) {
-  unsigned long long v;
-  asm volatile("ld.volatile.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
-  return v;
-}
-
-// Sum of the bits of all tiles before t (thread 0 of the compute warps).  Posts t's own count
-// first, so later tiles can look past t before t knows its prefix.  false when a wait gave up.
-// Sum of the bits of all tiles before t in its column (`state` = the status of the column's tile
-// 0), by one warp: every lane reads one predecessor's status, 32 at a time (the warp-wide window of
-// the decoupled look-back), until the window holds an inclusive prefix; the aggregates between it
-// and t are added.  The warp waits (bounded) while a predecessor in the window has posted nothing.
-// Lane 0 posts t's own count first and its inclusive prefix at the end.  false when a wait gave up.
-__device__ __forceinline__ bool cf_look_back(unsigned long long* state, int64_t t, unsigned long long agg,
-                                             unsigned long long* prefix) {
-  const int lane = threadIdx.x & 31;
-  if (t == 0) {
-    if (lane == 0) atomicExch(state, kLbInc | agg);
-    *prefix = 0;
-    return true;
-  }
-  if (lane == 0) atomicExch(state + t, kLbAgg | agg);
-  unsigned long long acc = 0;
-  int64_t hi = t - 1;
-  const uint64_t t0 = global_ns();
-  long long it = 0;
-  bool ok = true;
-  while (true) {
-    const int64_t k = hi - lane;
-    // below tile 0 nothing is added (tile 0 posts its inclusive prefix, so the window stops there)
-    const unsigned long long sv = k >= 0 ? ld_volatile_u64(state + k) : kLbInc;
-    if (__any_sync(FULL_MASK, (sv & (kLbAgg | kLbInc)) == 0)) {
-      if (++it > kSpinLimit || ((it & 255) == 0 && global_ns() - t0 > 2000000000ull)) { ok = false; break; }
-      continue;
+// The producer lane of a launch: stages item blockIdx.x + k * gridDim.x of the work list into stage
+// k % kCfStages (its values, from the 16-byte block that holds the first one), with the item, its
+// column and the offset of its first value in the stage; an item of -1 marks the end.
+template <typename T>
+__device__ __forceinline__ void cf_produce(const FixedCompressArgs& a, uint8_t* smem, uint64_t* full, uint64_t* empty,
+                                           int64_t* s_stile, int* s_shead, int* s_scol) {
+  int64_t item = blockIdx.x;
+  for (int k = 0;; k++, item += gridDim.x) {
+    const int st = k % kCfStages;
+    if (k >= kCfStages && !mbar_wait_bounded(&empty[st], (uint32_t)((k / kCfStages) - 1) & 1u)) {
+      atomicExch(a.status, (unsigned long long)DEVERR_TIMEOUT);
+      s_stile[st] = -1;  // the compute warps stop at this stage (or time out on it)
+      mbar_arrive(&full[st]);
+      return;
     }
-    const unsigned inc = __ballot_sync(FULL_MASK, (sv & kLbInc) != 0);
-    const int stop = inc ? __ffs(inc) - 1 : 32;  // the nearest inclusive prefix in the window
-    unsigned long long v = lane <= stop ? (sv & kLbVal) : 0ull;
-#pragma unroll
-    for (int m = 16; m > 0; m >>= 1) v += __shfl_xor_sync(FULL_MASK, v, m);
-    acc += v;
-    if (inc) break;
-    hi -= 32;
+    if (item >= a.nitems) {
+      s_stile[st] = -1;
+      mbar_arrive(&full[st]);  // no copy: completes the phase, the compute warps see the end
+      return;
+    }
+    const int c = a.owner ? a.owner[item] : 0;
+    const CfColumn& col = a.cols ? a.cols[c] : a.single;
+    const int64_t e0 = (item - col.item_base) * kDecodeTile;
+    const int cnt = (int)((col.n - e0) < kDecodeTile ? (col.n - e0) : kDecodeTile);
+    const uintptr_t addr = reinterpret_cast<uintptr_t>(reinterpret_cast<const T*>(col.values) + e0);
+    const int head = (int)(addr & 15);
+    s_stile[st] = item;
+    s_shead[st] = head;
+    s_scol[st] = c;
+    // the copy covers the 16-byte blocks that hold the tile's values, never another page
+    const uint32_t bytes = (uint32_t)((head + (int64_t)cnt * (int64_t)sizeof(T) + 15) & ~15ll);
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    mbar_arrive_expect_tx(&full[st], bytes);
+    tma_bulk_load(smem + (size_t)st * cf_stage_bytes<T>(), reinterpret_cast<const void*>(addr - head), bytes,
+                  &full[st]);
   }
-  if (lane == 0) atomicExch(state + t, kLbInc | (acc + agg));
-  *prefix = acc;
-  return ok;
 }
 
 template <typename T> __global__ void __launch_bounds__(kCfCTA)
@@ -133,8 +121,7 @@ fixed_compress_kernel(FixedCompressArgs a) {
   __shared__ uint32_t s_mb[kCfMaxParts];
   __shared__ long long s_err[kCfMaxParts];
   __shared__ int s_bl[kCfMaxParts + 1];
-  __shared__ unsigned long long s_bit0;
-  __shared__ int s_ok, s_bmax;
+  __shared__ int s_ok;
 
   if (threadIdx.x == 0) {
     for (int st = 0; st < kCfStages; st++) {
@@ -146,37 +133,8 @@ fixed_compress_kernel(FixedCompressArgs a) {
   __syncthreads();
 
   if (threadIdx.x >= kCfThreads) {  // ---- producer ----
-    if (threadIdx.x != kCfThreads) return;
-    int64_t item = blockIdx.x;
-    for (int k = 0;; k++, item += gridDim.x) {
-      const int st = k % kCfStages;
-      if (k >= kCfStages && !mbar_wait_bounded(&empty[st], (uint32_t)((k / kCfStages) - 1) & 1u)) {
-        atomicExch(a.status, (unsigned long long)DEVERR_TIMEOUT);
-        s_stile[st] = -1;  // the compute warps stop at this stage (or time out on it)
-        mbar_arrive(&full[st]);
-        return;
-      }
-      if (item >= a.nitems) {
-        s_stile[st] = -1;
-        mbar_arrive(&full[st]);  // no copy: completes the phase, the compute warps see the end
-        return;
-      }
-      const int c = a.owner ? a.owner[item] : 0;
-      const CfColumn& col = a.cols ? a.cols[c] : a.single;
-      const int64_t e0 = (item - col.item_base) * kDecodeTile;
-      const int cnt = (int)((col.n - e0) < kDecodeTile ? (col.n - e0) : kDecodeTile);
-      const uintptr_t addr = reinterpret_cast<uintptr_t>(reinterpret_cast<const T*>(col.values) + e0);
-      const int head = (int)(addr & 15);
-      s_stile[st] = item;
-      s_shead[st] = head;
-      s_scol[st] = c;
-      // the copy covers the 16-byte blocks that hold the tile's values, never another page
-      const uint32_t bytes = (uint32_t)((head + (int64_t)cnt * (int64_t)sizeof(T) + 15) & ~15ll);
-      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-      mbar_arrive_expect_tx(&full[st], bytes);
-      tma_bulk_load(smem + (size_t)st * cf_stage_bytes<T>(), reinterpret_cast<const void*>(addr - head), bytes,
-                    &full[st]);
-    }
+    if (threadIdx.x == kCfThreads) cf_produce<T>(a, smem, full, empty, s_stile, s_shead, s_scol);
+    return;
   }
 
   // ---- compute warps ----
@@ -332,7 +290,7 @@ fixed_compress_kernel(FixedCompressArgs a) {
       s_mb[p] = b > 1 ? 0xffffffffu / (uint32_t)b + 1u : 0u;
     }
     cf_sync();
-    if (tid == 0) {  // tile-relative bit ranges
+    if (tid == 0) {  // tile-relative bit ranges, the tile's bit count and decode-table entry
       int acc = 0, bmax = 0;
       for (int p = 0; p < np; p++) {
         s_bl[p] = acc;
@@ -340,39 +298,20 @@ fixed_compress_kernel(FixedCompressArgs a) {
         bmax = s_b[p] > bmax ? s_b[p] : bmax;
       }
       s_bl[np] = acc;
-      s_bmax = bmax;
-    }
-    cf_sync();
-    if (tid < 32) {  // the look-back (warp 0), the tile's table entry
-      const int acc = s_bl[np], bmax = s_bmax;
-      unsigned long long prefix = 0;
-      const bool lb_ok = cf_look_back(a.state + col.item_base, t, (unsigned long long)acc, &prefix);
-      if (tid == 0) {
-      if (!lb_ok) atomicExch(a.status, (unsigned long long)DEVERR_TIMEOUT);
-      s_bit0 = prefix;
+      a.tile_bits[item] = acc;
       TileInfo ti;
-      ti.bit_lo = (int64_t)prefix;
+      ti.bit_lo = 0;  // the tile's first bit is added by fixed_place_kernel
       ti.p_first = (int32_t)(t * col.parts_per_tile);
       ti.p_last = (int32_t)(t * col.parts_per_tile + np - 1);
       col.tiles[t] = ti;
-      if (t == col.ntiles - 1) {
-        TileInfo te;
-        te.bit_lo = (int64_t)(prefix + acc);
-        te.p_first = te.p_last = (int32_t)(col.P - 1);
-        col.tiles[col.ntiles] = te;
-        col.stats[0] = prefix + acc;
-      }
       if (bmax > 0) atomicMax(col.stats + 1, (unsigned long long)bmax);
-      }
     }
     cf_sync();
-    const unsigned long long bit0 = s_bit0;
-    if (tid < np) {  // the partitions' metadata and descriptors
+    if (tid < np) {  // the partitions' metadata and descriptors (offsets relative to the tile)
       const int p = tid;
       const int64_t gp = t * col.parts_per_tile + p;
       const int32_t start = (int32_t)(e0 + (int64_t)p * L);
       const int type = s_direct[p] ? MODEL_DIRECT_COPY : MODEL_LINEAR;
-      const int64_t off = (int64_t)bit0 + s_bl[p];
       col.starts[gp] = start;
       col.ends[gp] = start + s_len[p];
       col.types[gp] = type;
@@ -381,33 +320,27 @@ fixed_compress_kernel(FixedCompressArgs a) {
       col.params[4 * gp + 2] = 0.0;
       col.params[4 * gp + 3] = 0.0;
       col.bits[gp] = s_b[p];
-      col.offs[gp] = off;
+      col.offs[gp] = s_bl[p];
       col.err[gp] = s_err[p];
       PartDesc d;
       d.theta0 = s_t0[p];
       d.theta1 = s_t1[p];
-      d.bit_off = off;
+      d.bit_off = s_bl[p];
       d.start = start;
       d.bits_type = (s_b[p] & 0xff) | (type << 8);
       col.desc[gp] = d;
     }
 
-    // ---- C: words.  Word w covers tile-relative bits [32 w - sh0, 32 w - sh0 + 32). ----
+    // ---- C: the tile's words into its slot; word w holds tile bits [32 w, 32 w + 32) ----
     {
-      const int sh0 = (int)(bit0 & 31);
       const int tb = s_bl[np];
-      const int nw = tb > 0 ? (sh0 + tb + 31) >> 5 : 0;
-      const bool first_partial = sh0 != 0;
-      const bool last_partial = ((bit0 + (unsigned long long)tb) & 31) != 0;
+      const int nw = (tb + 31) >> 5;
       const uint32_t* f32 = reinterpret_cast<const uint32_t*>(res);  // low half of residual j at 2 j
-      uint32_t* out = col.words + (bit0 >> 5);
-      // never past the word array (the caller sized it; a disagreement is reported, not written)
-      const bool fits = (int64_t)((bit0 + (unsigned long long)tb + 31) >> 5) <= col.words_cap;
-      if (!fits && tid == 0) atomicExch(a.status, (unsigned long long)DEVERR_BOUNDS);
+      uint32_t* out = a.slots + item * a.slot_words;
       int qi = 0;
-      for (int w = fits ? tid : nw; w < nw; w += kCfThreads) {
-        const int wb = 32 * w - sh0;
-        int pos = wb > 0 ? wb : 0;
+      for (int w = tid; w < nw; w += kCfThreads) {
+        const int wb = 32 * w;
+        int pos = wb;
         const int wend = wb + 32 < tb ? wb + 32 : tb;
         uint32_t word = 0u;
         while (pos < wend) {
@@ -433,9 +366,7 @@ fixed_compress_kernel(FixedCompressArgs a) {
           }
           pos = qend;
         }
-        if (w == 0 && first_partial) a.edge_head[item] = word;
-        else if (w == nw - 1 && last_partial) a.edge_tail[item] = word;
-        else out[w] = word;
+        out[w] = word;
       }
     }
     cf_sync();  // every compute thread is done with stage st and the residual array
@@ -443,32 +374,262 @@ fixed_compress_kernel(FixedCompressArgs a) {
   }
 }
 
-// The words shared by neighbouring tiles.  Word W holding a tile's last bit, when that tile also
-// holds W's first bit, is written here by that tile's thread: its own bits (edge_tail) OR the
-// first bits of every later tile of the column that starts inside W (edge_head; tiles without
-// bits are skipped).  The column's last tile also zeroes the padding words after its bitstream.
-__global__ void fixed_edges_kernel(FixedCompressArgs a) {
-  const int64_t item = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (item >= a.nitems) return;
-  const CfColumn& col = a.cols ? a.cols[a.owner ? a.owner[item] : 0] : a.single;
-  const int64_t t = item - col.item_base;
-  const TileInfo* tiles = col.tiles;
-  const int64_t b0 = tiles[t].bit_lo, b1 = tiles[t + 1].bit_lo;
-  if (t == col.ntiles - 1 && col.nwords_alloc > 0)
-    for (int64_t w = (b1 + 31) >> 5; w < col.nwords_alloc && w < col.words_cap; w++) col.words[w] = 0u;
-  if (b1 == b0 || (b1 & 31) == 0) return;     // no bits, or a complete last word (already written)
-  const int64_t wi = b1 >> 5;
-  if (wi >= col.words_cap) return;            // reported by the compress kernel
-  if (b0 > (wi << 5)) return;                 // the tile starts inside W: an earlier tile owns it
-  uint32_t word = a.edge_tail[item];
-  for (int64_t u = t + 1; u < col.ntiles; u++) {
-    const int64_t c0 = tiles[u].bit_lo, c1 = tiles[u + 1].bit_lo;
-    if (c1 == c0) continue;
-    if ((c0 >> 5) != wi) break;
-    word |= a.edge_head[col.item_base + u];
-    if (c1 > ((wi + 1) << 5) || (c1 & 31) == 0) break;  // u goes past W
+// The partition-length choice of the batched compress, one tile per step (the same staging as
+// fixed_compress_kernel): the tile's four 1024-value quarters, its two halves and the whole tile
+// are fitted from exact per-quarter sums (the index offsets of a half or the tile added exactly),
+// every value's residual is measured against the three lines that cover it, and the bits of each
+// candidate length are added into the column's choice_bits[0..2] (1024, 2048, 4096).  The widths
+// are the ones the compress at that length computes, so the column's size is exact.
+template <typename T> __global__ void __launch_bounds__(kCfCTA)
+choose_lengths_kernel(FixedCompressArgs a) {
+  extern __shared__ __align__(128) uint8_t smem[];
+  __shared__ __align__(8) uint64_t full[kCfStages], empty[kCfStages];
+  __shared__ int64_t s_stile[kCfStages];
+  __shared__ int s_shead[kCfStages];
+  __shared__ int s_scol[kCfStages];
+  typedef typename HalfSums<T>::Acc Acc;
+  __shared__ Acc s_acc[8][4];
+  __shared__ int s_ovf[8];
+  __shared__ unsigned long long s_m[8][3];
+  __shared__ double s_t0[7], s_t1[7];
+  __shared__ int s_dir[7], s_safe[7], s_len[7];
+  __shared__ int s_ok;
+  if (threadIdx.x == 0) {
+    for (int st = 0; st < kCfStages; st++) {
+      mbar_init(&full[st], 1);
+      mbar_init(&empty[st], 1);
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
-  col.words[wi] = word;
+  __syncthreads();
+  if (threadIdx.x >= kCfThreads) {  // ---- producer ----
+    if (threadIdx.x == kCfThreads) cf_produce<T>(a, smem, full, empty, s_stile, s_shead, s_scol);
+    return;
+  }
+  const int tid = threadIdx.x, warp = tid >> 5;
+  const int q = tid >> 6;          // this thread's quarter (64 threads, 16 values each)
+  const int r = tid & 63;
+  for (int k = 0;; k++) {
+    const int st = k % kCfStages;
+    const uint32_t par = (uint32_t)(k / kCfStages) & 1u;
+    if (tid == 0) {
+      s_ok = mbar_wait_bounded(&full[st], par);
+      if (!s_ok) {
+        atomicExch(a.status, (unsigned long long)DEVERR_TIMEOUT);
+        mbar_wait_bounded(&full[st], par);  // a copy in flight lands before the CTA exits
+      }
+    }
+    cf_sync();
+    if (!s_ok) return;
+    mbar_try_wait(&full[st], par);
+    const int64_t item = s_stile[st];
+    if (item < 0) return;
+    const CfColumn& col = a.cols[s_scol[st]];
+    const int64_t e0 = (item - col.item_base) * kDecodeTile;
+    const int cnt = (int)((col.n - e0) < kDecodeTile ? (col.n - e0) : kDecodeTile);
+    const T* x = reinterpret_cast<const T*>(smem + (size_t)st * cf_stage_bytes<T>() + s_shead[st]);
+    const int qlen = (cnt - 1024 * q) < 0 ? 0 : ((cnt - 1024 * q) < 1024 ? (cnt - 1024 * q) : 1024);
+    const T* xq = x + 1024 * q;
+    {  // exact sums per quarter (two warps each)
+      HalfSums<T> hs;
+      int ovf = 0;
+#pragma unroll 4
+      for (int m = 0; m < kCfPerThread; m++) {
+        const int i = r + 64 * m;
+        if (i < qlen) {
+          const T y = xq[i];
+          ovf |= overflows_double<T>(y) ? 1 : 0;
+          hs.add(y, i);
+        }
+      }
+      Acc c0 = hs.s_lo, c1 = hs.s_hi, c2 = hs.x_lo, c3 = hs.x_hi;
+#pragma unroll
+      for (int msk = 16; msk > 0; msk >>= 1) {
+        c0 += __shfl_xor_sync(FULL_MASK, c0, msk);
+        if (sizeof(T) == 8) c1 += __shfl_xor_sync(FULL_MASK, c1, msk);
+        c2 += __shfl_xor_sync(FULL_MASK, c2, msk);
+        if (sizeof(T) == 8) c3 += __shfl_xor_sync(FULL_MASK, c3, msk);
+        ovf |= __shfl_xor_sync(FULL_MASK, ovf, msk);
+      }
+      if ((tid & 31) == 0) {
+        s_acc[warp][0] = c0;
+        s_acc[warp][1] = c1;
+        s_acc[warp][2] = c2;
+        s_acc[warp][3] = c3;
+        s_ovf[warp] = ovf;
+      }
+    }
+    cf_sync();
+    if (tid < 7) {  // line l: 0 = the tile, 1-2 = its halves, 3-6 = its quarters
+      const int l = tid;
+      const int q0 = l == 0 ? 0 : (l < 3 ? (l - 1) * 2 : l - 3);
+      const int q1 = l == 0 ? 4 : (l < 3 ? q0 + 2 : q0 + 1);
+      i128 sy = 0, sxy = 0;
+      int ovf = 0;
+      for (int qq = q0; qq < q1; qq++) {
+        HalfSums<T> hs;
+        for (int w = 2 * qq; w < 2 * qq + 2; w++) {
+          hs.s_lo += s_acc[w][0];
+          hs.s_hi += s_acc[w][1];
+          hs.x_lo += s_acc[w][2];
+          hs.x_hi += s_acc[w][3];
+          ovf |= s_ovf[w];
+        }
+        const i128 qy = hs.sy();
+        sy += qy;
+        sxy += hs.sxy() + (i128)(1024 * (qq - q0)) * qy;  // quarter index -> line index
+      }
+      int len = cnt - 1024 * q0;
+      len = len < 0 ? 0 : (len < 1024 * (q1 - q0) ? len : 1024 * (q1 - q0));
+      double t0 = 0.0, t1 = 0.0;
+      if (len > 0 && !ovf) solve_line(len, sy, sxy, t0, t1);
+      s_t0[l] = t0;
+      s_t1[l] = t1;
+      s_dir[l] = ovf;
+      s_len[l] = len;
+      s_safe[l] = len > 0 && !ovf && line_fp64_safe<T>(t0, t1, 0, len - 1);
+    }
+    cf_sync();
+    {  // max |residual| of each value against its quarter's, its half's and the tile's line
+      const int ls[3] = {3 + q, 1 + (q >> 1), 0};
+      const int off[3] = {0, 1024 * (q & 1), 1024 * q};
+      unsigned long long mx[3] = {0, 0, 0};
+      if (qlen > 0) {
+        bool fast = s_safe[ls[0]] && s_safe[ls[1]] && s_safe[ls[2]];
+        if (fast) {
+          double md[3] = {0.0, 0.0, 0.0};
+#pragma unroll 2
+          for (int m = 0; m < kCfPerThread; m++) {
+            const int i = r + 64 * m;
+            if (i < qlen) {
+              const T y = xq[i];
+              fast &= value_fp64_safe<T>(y);
+#pragma unroll
+              for (int c = 0; c < 3; c++) {
+                const T pr = predict_from<T>(__fma_rn(s_t1[ls[c]], (double)(i + off[c]), s_t0[ls[c]]));
+                md[c] = fmax(md[c], fabs(__ll2double_rn((long long)y - (long long)pr)));
+              }
+            }
+          }
+#pragma unroll
+          for (int c = 0; c < 3; c++) mx[c] = (unsigned long long)md[c];
+        }
+        if (!fast) {  // exact integer residuals (saturating for uint64)
+          for (int c = 0; c < 3; c++) mx[c] = 0;
+          for (int m = 0; m < kCfPerThread; m++) {
+            const int i = r + 64 * m;
+            if (i >= qlen) continue;
+            const T y = xq[i];
+            for (int c = 0; c < 3; c++) {
+              if (s_dir[ls[c]]) continue;
+              const long long d =
+                  calc_delta<T>(y, predict_from<T>(__fma_rn(s_t1[ls[c]], (double)(i + off[c]), s_t0[ls[c]])));
+              const unsigned long long ad = (unsigned long long)abs_ref(d);
+              mx[c] = ad > mx[c] ? ad : mx[c];
+            }
+          }
+        }
+      }
+#pragma unroll
+      for (int c = 0; c < 3; c++) {
+#pragma unroll
+        for (int msk = 16; msk > 0; msk >>= 1) {
+          const unsigned long long o = __shfl_xor_sync(FULL_MASK, mx[c], msk);
+          mx[c] = o > mx[c] ? o : mx[c];
+        }
+      }
+      if ((tid & 31) == 0) {
+        s_m[warp][0] = mx[0];
+        s_m[warp][1] = mx[1];
+        s_m[warp][2] = mx[2];
+      }
+    }
+    cf_sync();
+    if (tid == 0) {
+      unsigned long long add[3] = {0, 0, 0};
+      for (int l = 0; l < 7; l++) {
+        if (s_len[l] <= 0) continue;
+        const int c = l == 0 ? 2 : (l < 3 ? 1 : 0);                      // index into s_m's lines
+        const int w0 = l == 0 ? 0 : (l < 3 ? 4 * (l - 1) : 2 * (l - 3));  // the line's warps
+        const int w1 = l == 0 ? 8 : (l < 3 ? w0 + 4 : w0 + 2);
+        unsigned long long m = 0;
+        for (int w = w0; w < w1; w++) m = s_m[w][c] > m ? s_m[w][c] : m;
+        const int b = s_dir[l] ? (int)sizeof(T) * 8 : bits_for((long long)m);
+        add[l == 0 ? 2 : (l < 3 ? 1 : 0)] += (unsigned long long)s_len[l] * (unsigned long long)b;
+      }
+      for (int c = 0; c < 3; c++)
+        if (add[c]) atomicAdd(col.choice_bits + c, add[c]);
+    }
+    cf_sync();  // every compute thread is done with stage st
+    if (tid == 0) mbar_arrive(&empty[st]);
+  }
+}
+
+// Places every tile of the launch in its column, one CTA per tile: the tile's first bit F (the
+// scan of the tiles' bits, relative to the column's first tile) is added to its partitions'
+// offsets and descriptors and to its decode-table entry, and the words whose first bit lies in the
+// tile are written -- from the tile's slot with a funnel shift, ORed with the first bits of every
+// later tile of the column that starts inside the same word (tiles without bits are skipped).  The
+// column's last tile writes the final decode-table entry and the total, and zeroes the padding.
+__global__ void __launch_bounds__(256) fixed_place_kernel(FixedCompressArgs a) {
+  for (int64_t item = blockIdx.x; item < a.nitems; item += gridDim.x) {
+    const CfColumn& col = a.cols ? a.cols[a.owner ? a.owner[item] : 0] : a.single;
+    const int64_t t = item - col.item_base;
+    const int64_t base = a.tile_first[col.item_base];
+    const int64_t first = a.tile_first[item] - base;
+    const int64_t bits = a.tile_bits[item];
+    const int64_t col_end = col.item_base + col.ntiles;  // the column's items are [item_base, col_end)
+    const int64_t total = a.tile_first[col_end - 1] - base + a.tile_bits[col_end - 1];
+    const int64_t e0 = t * kDecodeTile;
+    const int cnt = (int)((col.n - e0) < kDecodeTile ? (col.n - e0) : kDecodeTile);
+    const int np = (cnt + col.L - 1) / col.L;
+    if ((int)threadIdx.x < np) {
+      const int64_t gp = t * col.parts_per_tile + threadIdx.x;
+      col.offs[gp] += first;
+      col.desc[gp].bit_off += first;
+    }
+    if (threadIdx.x == 0) {
+      col.tiles[t].bit_lo = first;
+      if (t == col.ntiles - 1) {
+        TileInfo te;
+        te.bit_lo = total;
+        te.p_first = te.p_last = (int32_t)(col.P - 1);
+        col.tiles[col.ntiles] = te;
+        col.stats[0] = (unsigned long long)total;
+      }
+    }
+    const int64_t w_begin = (first + 31) >> 5, w_end = (first + bits + 31) >> 5;
+    if (w_end > col.words_cap) {  // the caller sized the array from another count: report, write nothing
+      if (threadIdx.x == 0) atomicExch(a.status, (unsigned long long)DEVERR_BOUNDS);
+      continue;
+    }
+    const uint32_t* slot = a.slots + item * a.slot_words;
+    for (int64_t w = w_begin + threadIdx.x; w < w_end; w += blockDim.x) {
+      const int64_t lb = 32 * w - first;  // tile bit of the word's bit 0 (0 <= lb < bits)
+      const int64_t k = lb >> 5;
+      const int r = (int)(lb & 31);
+      uint32_t v = r ? __funnelshift_r(slot[k], slot[k + 1], r) : slot[k];
+      const int64_t avail = bits - lb;
+      if (avail < 32) {  // the tile ends inside the word: the next tiles' first bits follow
+        v &= (1u << avail) - 1u;
+        int64_t pos = first + bits;  // column bit where the next tile starts
+        for (int64_t u = item + 1; u < col_end && pos < 32 * w + 32; u++) {
+          const int64_t ub = a.tile_bits[u];
+          if (ub == 0) continue;
+          const int64_t take = (32 * w + 32 - pos) < ub ? (32 * w + 32 - pos) : ub;
+          uint32_t f = a.slots[u * a.slot_words];
+          if (take < 32) f &= (1u << take) - 1u;
+          v |= f << (pos - 32 * w);
+          pos += ub;
+        }
+      }
+      col.words[w] = v;
+    }
+    if (t == col.ntiles - 1 && col.nwords_alloc > 0) {
+      const int64_t wt = (total + 31) >> 5;
+      for (int64_t w = wt + threadIdx.x; w < col.nwords_alloc && w < col.words_cap; w += blockDim.x) col.words[w] = 0u;
+    }
+  }
 }
 
 template <typename T> static cudaError_t launch_fixed_compress_t(const FixedCompressArgs& a, int num_sms, cudaStream_t s) {
@@ -487,13 +648,10 @@ template <typename T> static cudaError_t launch_fixed_compress_t(const FixedComp
       cudaSuccess)
     return e;
   if (per_sm < 1) per_sm = 1;
-  // every CTA resident at once: a tile's look-back waits only on tiles that resident CTAs own
   int64_t grid = (int64_t)per_sm * num_sms;
   if (grid > a.nitems) grid = a.nitems;
   if (grid < 1) grid = 1;
   fixed_compress_kernel<T><<<(unsigned)grid, kCfCTA, smem, s>>>(a);
-  if ((e = cudaGetLastError()) != cudaSuccess) return e;
-  fixed_edges_kernel<<<(unsigned)((a.nitems + 255) / 256), 256, 0, s>>>(a);
   return cudaGetLastError();
 }
 
@@ -507,24 +665,98 @@ static cudaError_t launch_fixed_compress_dt(glc_dtype dt, const FixedCompressArg
   return cudaErrorInvalidValue;
 }
 
+template <typename T> static cudaError_t launch_choose_t(const FixedCompressArgs& a, int num_sms, cudaStream_t s) {
+  constexpr int smem = kCfStages * cf_stage_bytes<T>();
+  static PerDeviceFlag attr_set;
+  const int dev = current_device();
+  cudaError_t e;
+  if (!attr_set.test(dev)) {
+    if ((e = cudaFuncSetAttribute(choose_lengths_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) !=
+        cudaSuccess)
+      return e;
+    attr_set.set(dev);
+  }
+  int per_sm = 0;
+  if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, choose_lengths_kernel<T>, kCfCTA, smem)) !=
+      cudaSuccess)
+    return e;
+  if (per_sm < 1) per_sm = 1;
+  int64_t grid = (int64_t)per_sm * num_sms;
+  if (grid > a.nitems) grid = a.nitems;
+  if (grid < 1) grid = 1;
+  choose_lengths_kernel<T><<<(unsigned)grid, kCfCTA, smem, s>>>(a);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_choose_lengths(glc_dtype dt, const CfColumn* cols, const int32_t* owner, int64_t nitems,
+                                  unsigned long long* status, int num_sms, cudaStream_t s) {
+  if (nitems <= 0) return cudaSuccess;
+  FixedCompressArgs a{};
+  a.cols = cols;
+  a.owner = owner;
+  a.nitems = nitems;
+  a.status = status;
+  switch (dt) {
+    case GLC_I32: return launch_choose_t<int32_t>(a, num_sms, s);
+    case GLC_I64: return launch_choose_t<int64_t>(a, num_sms, s);
+    case GLC_U64: return launch_choose_t<uint64_t>(a, num_sms, s);
+    case GLC_U32: return launch_choose_t<uint32_t>(a, num_sms, s);
+  }
+  return cudaErrorInvalidValue;
+}
+
 bool fixed_compress_supported(int64_t n, int32_t L) {
   return n > 0 && L >= kCfMinLen && L <= kDecodeTile && (kDecodeTile % L) == 0;
 }
 
-int64_t fixed_compress_worst_words(glc_dtype dt, int64_t n) {
-  const int64_t per_value = (dt == GLC_I64 || dt == GLC_U64) ? 64 : 33;  // widest field of the type
-  return (n * per_value + 31) / 32 + 8;
+// Words of one tile's slot: the widest fields of the type (64 bits for 8-byte types, 33 for 4-byte
+// ones) plus the word the placing funnel shift reads after the last, rounded to 16 bytes.
+int64_t fixed_compress_slot_words(glc_dtype dt) {
+  const int64_t per_value = (dt == GLC_I64 || dt == GLC_U64) ? 64 : 33;
+  return ((kDecodeTile * per_value + 31) / 32 + 1 + 3) & ~3ll;
 }
 
-size_t fixed_compress_scratch_bytes(int64_t nitems) { return (size_t)nitems * 16 + 64; }
+// Scratch of a launch over nitems tiles: slots, the tiles' bits, their scan and its tile sums.
+size_t fixed_compress_scratch_bytes(glc_dtype dt, int64_t nitems) {
+  return (size_t)nitems * fixed_compress_slot_words(dt) * 4 + (size_t)(nitems + 1) * 16 +
+         (size_t)(scan_num_tiles(nitems + 1) + 1) * 8 + 256;
+}
+
+static void carve(FixedCompressArgs& a, glc_dtype dt, void* scratch) {
+  uint8_t* sp = reinterpret_cast<uint8_t*>(scratch);
+  a.slot_words = fixed_compress_slot_words(dt);
+  a.slots = reinterpret_cast<uint32_t*>(sp);
+  sp += (size_t)a.nitems * a.slot_words * 4;
+  a.tile_bits = reinterpret_cast<int64_t*>(sp);
+  sp += (size_t)(a.nitems + 1) * 8;
+  a.tile_first = reinterpret_cast<int64_t*>(sp);
+}
+
+// Pass 1 for one launch: fit, residuals and each tile's words into its slot, the tiles' bits, and
+// their exclusive scan (tile_first[nitems] = all the launch's bits).
+static cudaError_t compress_pass(glc_dtype dt, FixedCompressArgs& a, void* scratch, int num_sms, cudaStream_t s) {
+  carve(a, dt, scratch);
+  cudaError_t e;
+  if ((e = launch_fixed_compress_dt(dt, a, num_sms, s)) != cudaSuccess) return e;
+  int64_t* first = const_cast<int64_t*>(a.tile_first);
+  int64_t* tmp = first + a.nitems + 1;
+  return exclusive_scan<int64_t>(a.tile_bits, first, a.nitems, first + a.nitems, tmp, s);
+}
+
+static cudaError_t place_pass(const FixedCompressArgs& a, int num_sms, cudaStream_t s) {
+  int64_t grid = a.nitems < (int64_t)num_sms * 16 ? a.nitems : (int64_t)num_sms * 16;
+  if (grid < 1) grid = 1;
+  fixed_place_kernel<<<(unsigned)grid, 256, 0, s>>>(a);
+  return cudaGetLastError();
+}
 
 // One column: values (n of dt, fixed partitions of L) into c's metadata arrays and tables
-// (allocated by the caller for P = ceil(n / L) partitions) and into `words`
-// (fixed_compress_worst_words words; its padding is left to the caller); `scratch` holds
-// fixed_compress_scratch_bytes(ntiles) bytes; stats[0] receives the total bits, stats[1] the
-// widest field, stats[2] a DEVERR_* code (stats[0..3] zeroed here).
-cudaError_t launch_fixed_compress(glc_dtype dt, const void* values, glc_column* c, int32_t L, uint32_t* words,
-                                  void* scratch, unsigned long long* stats, cudaStream_t s) {
+// (allocated by the caller for P = ceil(n / L) partitions); scratch holds
+// fixed_compress_scratch_bytes(dt, ntiles) bytes.  Pass 1 leaves stats[0] = the column's total bits,
+// stats[1] = its widest field, stats[2] = a DEVERR_* code (stats[0..3] zeroed here); the caller
+// reads them, allocates the words and calls launch_fixed_place.
+cudaError_t launch_fixed_compress(glc_dtype dt, const void* values, glc_column* c, int32_t L, void* scratch,
+                                  unsigned long long* stats, cudaStream_t s) {
   FixedCompressArgs a{};
   CfColumn& col = a.single;
   col.values = values;
@@ -534,7 +766,6 @@ cudaError_t launch_fixed_compress(glc_dtype dt, const void* values, glc_column* 
   col.P = c->P;
   col.ntiles = c->ntiles;
   col.item_base = 0;
-  col.nwords_alloc = 0;
   col.starts = c->d_start;
   col.ends = c->d_end;
   col.types = c->d_types;
@@ -544,25 +775,44 @@ cudaError_t launch_fixed_compress(glc_dtype dt, const void* values, glc_column* 
   col.err = c->d_err;
   col.desc = c->d_desc;
   col.tiles = c->d_tiles;
-  col.words = words;
-  col.words_cap = fixed_compress_worst_words(dt, c->n);
   col.stats = stats;
   a.nitems = c->ntiles;
-  uint8_t* sp = reinterpret_cast<uint8_t*>(scratch);
-  a.state = reinterpret_cast<unsigned long long*>(sp);
-  a.edge_head = reinterpret_cast<uint32_t*>(sp + (size_t)a.nitems * 8);
-  a.edge_tail = a.edge_head + a.nitems;
   a.status = stats + 2;
   cudaError_t e;
-  if ((e = cudaMemsetAsync(a.state, 0, (size_t)a.nitems * 8, s)) != cudaSuccess) return e;
   if ((e = cudaMemsetAsync(stats, 0, 4 * sizeof(unsigned long long), s)) != cudaSuccess) return e;
-  return launch_fixed_compress_dt(dt, a, c->ctx ? c->ctx->num_sms : 148, s);
+  if ((e = compress_pass(dt, a, scratch, c->ctx ? c->ctx->num_sms : 148, s)) != cudaSuccess) return e;
+  // the total: the scan's grand total (the column is the whole launch)
+  return cudaMemcpyAsync(stats, a.tile_first + a.nitems, sizeof(int64_t), cudaMemcpyDeviceToDevice, s);
 }
 
-// Many columns of one element type in one launch: cols (device, ncols entries, each with its own
-// arrays, stats zeroed and nwords_alloc set) and owner (device, nitems entries: the column of each
-// item, items in column order).  scratch: fixed_compress_scratch_bytes(nitems) bytes; status: a
-// DEVERR_* word.
+// Pass 2 for one column: its words into c->d_words (c->nwords_alloc words), its offsets, descriptors
+// and decode-table entries completed.  Same arguments as launch_fixed_compress.
+cudaError_t launch_fixed_place(glc_dtype dt, glc_column* c, int32_t L, void* scratch, unsigned long long* stats,
+                               cudaStream_t s) {
+  FixedCompressArgs a{};
+  CfColumn& col = a.single;
+  col.n = c->n;
+  col.L = L;
+  col.parts_per_tile = kDecodeTile / L;
+  col.P = c->P;
+  col.ntiles = c->ntiles;
+  col.item_base = 0;
+  col.nwords_alloc = c->nwords_alloc;
+  col.words_cap = c->nwords_alloc;
+  col.offs = c->d_offs;
+  col.desc = c->d_desc;
+  col.tiles = c->d_tiles;
+  col.words = c->d_words;
+  col.stats = stats;
+  a.nitems = c->ntiles;
+  a.status = stats + 2;
+  carve(a, dt, scratch);
+  return place_pass(a, c->ctx ? c->ctx->num_sms : 148, s);
+}
+
+// Many columns of one element type: cols (device, each with its own arrays, its exact word array
+// and words_cap, stats zeroed) and owner (device, nitems entries: the column of each item, items in
+// column order); both passes in stream order.  scratch: fixed_compress_scratch_bytes(dt, nitems).
 cudaError_t launch_fixed_compress_batch(glc_dtype dt, const CfColumn* cols, const int32_t* owner, int64_t nitems,
                                         void* scratch, unsigned long long* status, int num_sms, cudaStream_t s) {
   if (nitems <= 0) return cudaSuccess;
@@ -570,14 +820,10 @@ cudaError_t launch_fixed_compress_batch(glc_dtype dt, const CfColumn* cols, cons
   a.cols = cols;
   a.owner = owner;
   a.nitems = nitems;
-  uint8_t* sp = reinterpret_cast<uint8_t*>(scratch);
-  a.state = reinterpret_cast<unsigned long long*>(sp);
-  a.edge_head = reinterpret_cast<uint32_t*>(sp + (size_t)nitems * 8);
-  a.edge_tail = a.edge_head + nitems;
   a.status = status;
   cudaError_t e;
-  if ((e = cudaMemsetAsync(a.state, 0, (size_t)nitems * 8, s)) != cudaSuccess) return e;
-  return launch_fixed_compress_dt(dt, a, num_sms, s);
+  if ((e = compress_pass(dt, a, scratch, num_sms, s)) != cudaSuccess) return e;
+  return place_pass(a, num_sms, s);
 }
 
 }  // namespace glc

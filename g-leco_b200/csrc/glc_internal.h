@@ -212,15 +212,22 @@ struct CfColumn {
   TileInfo* tiles;
   uint32_t* words;             // the column's words (interior words of each tile)
   unsigned long long* stats;   // [0] total bits (written by the last tile), [1] widest field
+  unsigned long long* choice_bits;  // length choice: the column's bits at lengths 1024, 2048, 4096
 };
 
 bool fixed_compress_supported(int64_t n, int32_t L);
-int64_t fixed_compress_worst_words(glc_dtype dt, int64_t n);
-size_t fixed_compress_scratch_bytes(int64_t nitems);  // nitems = 4096-value tiles of the launch
-cudaError_t launch_fixed_compress(glc_dtype dt, const void* values, glc_column* c, int32_t L, uint32_t* words,
-                                  void* scratch, unsigned long long* stats, cudaStream_t s);
+int64_t fixed_compress_slot_words(glc_dtype dt);
+size_t fixed_compress_scratch_bytes(glc_dtype dt, int64_t nitems);  // nitems = 4096-value tiles of the launch
+cudaError_t launch_fixed_compress(glc_dtype dt, const void* values, glc_column* c, int32_t L, void* scratch,
+                                  unsigned long long* stats, cudaStream_t s);
+cudaError_t launch_fixed_place(glc_dtype dt, glc_column* c, int32_t L, void* scratch, unsigned long long* stats,
+                               cudaStream_t s);
 cudaError_t launch_fixed_compress_batch(glc_dtype dt, const CfColumn* cols, const int32_t* owner, int64_t nitems,
                                         void* scratch, unsigned long long* status, int num_sms, cudaStream_t s);
+// The exact bits of every column of one element type at partition lengths 1024, 2048 and 4096
+// (added into each column's choice_bits, zeroed by the caller), in one read of the values.
+cudaError_t launch_choose_lengths(glc_dtype dt, const CfColumn* cols, const int32_t* owner, int64_t nitems,
+                                  unsigned long long* status, int num_sms, cudaStream_t s);
 cudaError_t launch_validate(const glc_column* c, int* d_bad, cudaStream_t s);
 cudaError_t launch_max_bits(const glc_column* c, int64_t* d_out, cudaStream_t s);
 // pack.cu: one column's arrays for the packer
