@@ -188,176 +188,6 @@ batch_fit_kernel(const FitCol* __restrict__ cols, const int64_t* __restrict__ pa
   widths[p] = len * b;
 }
 
-// Choice of the partition length, one read of the values: one CTA per 4096-value chunk of a
-// column fits the chunk (length 4096), its two halves (2048) and its four quarters (1024) from
-// exact per-quarter sums, then measures all seven lines in one residual pass.  Partitions of each
-// candidate length start at multiples of that length, so the halves and quarters are exactly the
-// 2048- and 1024-value partitions, and the bits equal those of three separate fits.
-// col_bits[3 c + k] receives the column's residual bits for length 1024 << k.
-template <typename T>
-__device__ void choose_chunk(const T* __restrict__ v, int64_t len, unsigned long long* __restrict__ col_bits) {
-  constexpr int W = kFitCTA / 32;
-  __shared__ i128 s_y[W][4], s_xy[W][4];
-  __shared__ int s_ov[W];
-  __shared__ double s_t0[7], s_t1[7];
-  __shared__ int s_over, s_lover[7];
-  __shared__ long long s_m[W][7];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  i128 y[4], xy[4];
-  int ov = 0;
-#pragma unroll
-  for (int q = 0; q < 4; q++) {
-    HalfSums<T> hs;  // exact 64-bit partials of the quarter
-#pragma unroll
-    for (int k = 0; k < 1024 / kFitCTA; k++) {
-      const int64_t i = q * 1024 + k * kFitCTA + threadIdx.x;
-      if (i < len) {
-        const T x = __ldg(v + i);
-        if (overflows_double<T>(x)) ov |= 1 << q;
-        hs.add(x, (int)i);  // chunk-relative position; lines subtract their start below
-      }
-    }
-    y[q] = hs.sy();
-    xy[q] = hs.sxy();
-  }
-#pragma unroll
-  for (int q = 0; q < 4; q++) {
-    y[q] = warp_sum_i128(y[q]);
-    xy[q] = warp_sum_i128(xy[q]);
-  }
-  ov = __reduce_or_sync(FULL_MASK, ov);
-  if (lane == 0) {
-#pragma unroll
-    for (int q = 0; q < 4; q++) { s_y[warp][q] = y[q]; s_xy[warp][q] = xy[q]; }
-    s_ov[warp] = ov;
-  }
-  __syncthreads();
-  if (threadIdx.x < 7) {  // one thread per line: 0 = the chunk, 1-2 = halves, 3-6 = quarters
-    const int l = threadIdx.x;
-    const int q0 = l == 0 ? 0 : (l < 3 ? (l - 1) * 2 : l - 3);
-    const int q1 = l == 0 ? 4 : (l < 3 ? q0 + 2 : q0 + 1);
-    int o = 0;
-    for (int w = 0; w < W; w++) o |= s_ov[w];
-    int lo = 0;
-    for (int q = q0; q < q1; q++) lo |= (o >> q) & 1;
-    const int64_t a = q0 * 1024, b = q1 * 1024 < len ? q1 * 1024 : len;
-    double t0 = 0.0, t1 = 0.0;
-    if (b > a && !lo) {
-      i128 sy = 0, sxy = 0;
-      for (int w = 0; w < W; w++)
-        for (int q = q0; q < q1; q++) { sy += s_y[w][q]; sxy += s_xy[w][q]; }
-      solve_line(b - a, sy, sxy - (i128)a * sy, t0, t1);
-    }
-    s_t0[l] = t0;
-    s_t1[l] = t1;
-    s_lover[l] = lo;
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    int over = 0;
-    for (int l = 0; l < 7; l++) over |= s_lover[l] << l;
-    s_over = over;
-  }
-  __syncthreads();
-  const int over = s_over;
-  // lines whose predictions stay inside the FP64-exact bounds over their values (glc_device.cuh)
-  int safe = 0;
-#pragma unroll
-  for (int l = 0; l < 7; l++) {
-    const int q0 = l == 0 ? 0 : (l < 3 ? (l - 1) * 2 : l - 3);
-    const int q1 = l == 0 ? 4 : (l < 3 ? q0 + 2 : q0 + 1);
-    const int64_t a = q0 * 1024, b = q1 * 1024 < len ? q1 * 1024 : len;
-    if (b > a && !((over >> l) & 1) && line_fp64_safe<T>(s_t0[l], s_t1[l], 0, b - a - 1)) safe |= 1 << l;
-  }
-  long long m[7] = {0, 0, 0, 0, 0, 0, 0};
-  double md[7] = {0, 0, 0, 0, 0, 0, 0};
-  bool ok = true;
-  const double tid_d = (double)threadIdx.x;
-#pragma unroll
-  for (int q = 0; q < 4; q++) {
-    const int lh = 1 + (q >> 1), lq = 3 + q;
-#pragma unroll
-    for (int k = 0; k < 1024 / kFitCTA; k++) {
-      const int64_t i = q * 1024 + k * kFitCTA + threadIdx.x;
-      if (i < len) {
-        const T x = __ldg(v + i);
-        ok &= value_fp64_safe<T>(x);
-        const double id = tid_d + (double)(q * 1024 + k * kFitCTA);
-        const double yd = (double)(long long)x;
-        const int ls[3] = {0, lh, lq};
-        const int base[3] = {0, (q >> 1) * 2048, q * 1024};
-#pragma unroll
-        for (int t = 0; t < 3; t++) {
-          const int l = ls[t];
-          if ((over >> l) & 1) continue;
-          if ((safe >> l) & 1) {
-            md[l] = fmax(md[l], abs_resid_fp64(yd, __fma_rn(s_t1[l], id - (double)base[t], s_t0[l])));
-          } else {
-            const long long d = abs_ref(calc_delta<T>(x, predict<T>(s_t0[l], s_t1[l], i - base[t])));
-            m[l] = d > m[l] ? d : m[l];
-          }
-        }
-      }
-    }
-  }
-  if (ok) {
-#pragma unroll
-    for (int l = 0; l < 7; l++)
-      if ((safe >> l) & 1) m[l] = (long long)md[l];
-  } else {  // this thread holds a value beyond 2^51: its FP64-measured lines again, exactly
-    for (int i = threadIdx.x; i < len; i += kFitCTA) {
-      const T x = __ldg(v + i);
-      const int q = i >> 10;
-      const int ls[3] = {0, 1 + (q >> 1), 3 + q};
-      const int base[3] = {0, (q >> 1) * 2048, q * 1024};
-      for (int t = 0; t < 3; t++) {
-        const int l = ls[t];
-        if (!((safe >> l) & 1)) continue;
-        const long long d = abs_ref(calc_delta<T>(x, predict<T>(s_t0[l], s_t1[l], i - base[t])));
-        m[l] = d > m[l] ? d : m[l];
-      }
-    }
-  }
-#pragma unroll
-  for (int l = 0; l < 7; l++) {
-    const long long t = warp_max_ll(m[l]);
-    if (lane == 0) s_m[warp][l] = t;
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    unsigned long long add[3] = {0, 0, 0};
-    for (int l = 0; l < 7; l++) {
-      const int q0 = l == 0 ? 0 : (l < 3 ? (l - 1) * 2 : l - 3);
-      const int q1 = l == 0 ? 4 : (l < 3 ? q0 + 2 : q0 + 1);
-      const int64_t a = q0 * 1024, b = q1 * 1024 < len ? q1 * 1024 : len;
-      if (b <= a) continue;
-      long long t = 0;
-      for (int w = 0; w < W; w++) t = s_m[w][l] > t ? s_m[w][l] : t;
-      const int bits = ((over >> l) & 1) ? (int)sizeof(T) * 8 : bits_for(t);
-      add[l == 0 ? 2 : (l < 3 ? 1 : 0)] += (unsigned long long)((b - a) * bits);
-    }
-    for (int k = 0; k < 3; k++)
-      if (add[k]) atomicAdd(col_bits + k, add[k]);
-  }
-}
-
-// One CTA per 4096-value chunk of any column (cols[] laid out with length 4096).
-__global__ void __launch_bounds__(kFitCTA)
-batch_choose_kernel(const FitCol* __restrict__ cols, const int64_t* __restrict__ part_base, int ncols,
-                    unsigned long long* __restrict__ col_bits) {
-  const int64_t p = blockIdx.x;
-  const int c = col_of(part_base, ncols, p);
-  const FitCol fc = cols[c];
-  const int64_t s = (p - fc.part_base) * 4096;
-  const int64_t len = (s + 4096 < fc.n ? s + 4096 : fc.n) - s;
-  switch (fc.dtype) {
-    case GLC_I32: choose_chunk<int32_t>((const int32_t*)fc.values + s, len, col_bits + 3 * c); break;
-    case GLC_I64: choose_chunk<int64_t>((const int64_t*)fc.values + s, len, col_bits + 3 * c); break;
-    case GLC_U64: choose_chunk<uint64_t>((const uint64_t*)fc.values + s, len, col_bits + 3 * c); break;
-    default: choose_chunk<uint32_t>((const uint32_t*)fc.values + s, len, col_bits + 3 * c); break;
-  }
-}
-
 // Global exclusive bit prefix -> column-local offsets; col_stats[c] = {total bits, max bits}.
 __global__ void batch_local_offsets_kernel(const int64_t* __restrict__ gofs, const int64_t* __restrict__ part_base,
                                            const int32_t* __restrict__ bits, int ncols, int64_t P,
@@ -702,24 +532,51 @@ glc_status glc_batch_compress(glc_ctx* ctx, const glc_dtype* dtypes, const void*
     return ee;
   };
   if ((e = dalloc(b, &d_fc, nc)) != cudaSuccess || (e = dalloc(b, &d_pb, nc + 1)) != cudaSuccess ||
-      (e = dalloc(b, &d_colbits, 3 * (size_t)nc)) != cudaSuccess)
+      (e = dalloc(b, &d_colbits, 3 * (size_t)nc + 1)) != cudaSuccess)
     return bail(bcuda(ctx, e, "batch compress: allocation"));
   // lengths 1024 / 2048 / 4096: the choice pass measures the exact bits of all three, and the
   // one-pass kernel compresses every column at its chosen length
   const bool one_pass = fixed_partition_len == 0 || fixed_partition_len == 1024 || fixed_partition_len == 2048 ||
                         fixed_partition_len == 4096;
   std::vector<unsigned long long> hbits(3 * (size_t)nc);
-  if (one_pass) {  // one pass measures all three candidate lengths
-    std::vector<int32_t> L(nc, 4096);
-    if ((e = upload_layout(L)) != cudaSuccess) return bail(bcuda(ctx, e, "batch compress: layout"));
-    if ((e = cudaMemsetAsync(d_colbits, 0, sizeof(unsigned long long) * 3 * nc, s)) != cudaSuccess)
+  if (one_pass) {  // one read of every column measures all three candidate lengths
+    if ((e = cudaMemsetAsync(d_colbits, 0, sizeof(unsigned long long) * (3 * (size_t)nc + 1), s)) != cudaSuccess)
       return bail(bcuda(ctx, e, "batch compress: sizes"));
-    if (pb[nc] > 0) batch_choose_kernel<<<(unsigned)pb[nc], kFitCTA, 0, s>>>(d_fc, d_pb, nc, d_colbits);
-    if ((e = cudaGetLastError()) != cudaSuccess ||
-        (e = cudaMemcpyAsync(hbits.data(), d_colbits, sizeof(unsigned long long) * 3 * nc, cudaMemcpyDeviceToHost,
+    for (glc_dtype dt : {GLC_I32, GLC_I64, GLC_U64, GLC_U32}) {  // one launch per element type
+      std::vector<CfColumn> g;
+      std::vector<int64_t> ib(1, 0);
+      for (int i = 0; i < nc; i++) {
+        if (dtypes[i] != dt || ns[i] == 0) continue;
+        CfColumn f{};
+        f.values = values[i];
+        f.n = ns[i];
+        f.ntiles = (ns[i] + kDecodeTile - 1) / kDecodeTile;
+        f.item_base = ib.back();
+        f.choice_bits = d_colbits + 3 * (size_t)i;
+        g.push_back(f);
+        ib.push_back(ib.back() + f.ntiles);
+      }
+      if (g.empty()) continue;
+      CfColumn* d_g;
+      int64_t* d_ib;
+      int32_t* d_owner;
+      if ((e = dalloc(b, &d_g, g.size())) || (e = dalloc(b, &d_ib, ib.size())) || (e = dalloc(b, &d_owner, ib.back())))
+        return bail(bcuda(ctx, e, "batch compress: allocation"));
+      if ((e = cudaMemcpyAsync(d_g, g.data(), sizeof(CfColumn) * g.size(), cudaMemcpyHostToDevice, s)) ||
+          (e = cudaMemcpyAsync(d_ib, ib.data(), sizeof(int64_t) * ib.size(), cudaMemcpyHostToDevice, s)) ||
+          (e = launch_pack_item_owner(d_ib, (int)g.size(), d_owner, s)) ||
+          (e = launch_choose_lengths(dt, d_g, d_owner, ib.back(), d_colbits + 3 * (size_t)nc, ctx->num_sms, s)) ||
+          (e = cudaStreamSynchronize(s)))  // the host vectors are reused by the next type
+        return bail(bcuda(ctx, e, "batch compress: length choice"));
+    }
+    unsigned long long choice_status = 0;
+    if ((e = cudaMemcpyAsync(hbits.data(), d_colbits, sizeof(unsigned long long) * 3 * nc, cudaMemcpyDeviceToHost,
                              s)) != cudaSuccess ||
+        (e = cudaMemcpyAsync(&choice_status, d_colbits + 3 * (size_t)nc, sizeof(unsigned long long),
+                             cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
         (e = cudaStreamSynchronize(s)) != cudaSuccess)
       return bail(bcuda(ctx, e, "batch compress: sizes"));
+    if (choice_status != DEVERR_NONE) return bail(bfail(ctx, GLC_ERR_TIMEOUT, "batch compress: a device-side wait gave up"));
     // the smallest compressed size; within 0.1 % of it, the length the tuner found to decode
     // fastest for the element type and the column's mean field width (when the table holds one)
     for (int i = 0; i < nc && fixed_partition_len == 0; i++) {
