@@ -240,23 +240,26 @@ fixed_compress_kernel(FixedCompressArgs a) {
         } else {
           const double t0 = s_t0[p], t1 = s_t1[p];
           bool exact_fp64 = s_safe[p] != 0;
-          double md = 0.0;
           if (exact_fp64) {
-            // |y| < 2^51 and the predictions inside pred_fp64_safe's bounds: y - pred is below 2^52,
-            // so the integer difference is calculateDelta and its double is exact
+            // |y| < 2^51 and the predictions inside pred_fp64_safe's bounds: the prediction is
+            // predict_small (no conversion instruction), y - pred is below 2^52 and is
+            // calculateDelta; the index advances as an exact double
+            long long dmax = 0, dmin = 0;
+            double xd = (double)r_me;
+            const double xstep = (double)g;
 #pragma unroll 4
-            for (int m = 0; m < kCfPerThread; m++) {
+            for (int m = 0; m < kCfPerThread; m++, xd += xstep) {
               const int i = r_me + g * m;
               if (i < my_len) {
                 const T y = xp[i];
                 exact_fp64 &= value_fp64_safe<T>(y);
-                const T pr = predict_from<T>(__fma_rn(t1, (double)i, t0));
-                const long long d = (long long)y - (long long)pr;
+                const long long d = (long long)y - predict_small(__fma_rn(t1, xd, t0));
                 rp[i] = d;
-                md = fmax(md, fabs(__ll2double_rn(d)));
+                dmax = d > dmax ? d : dmax;
+                dmin = d < dmin ? d : dmin;
               }
             }
-            mx = (unsigned long long)md;
+            mx = (unsigned long long)(dmax > -dmin ? dmax : -dmin);
           }
           if (!exact_fp64) {  // the general residual (saturating for uint64), and its exact magnitude
             mx = 0;
@@ -496,8 +499,15 @@ choose_lengths_kernel(FixedCompressArgs a) {
       unsigned long long mx[3] = {0, 0, 0};
       if (qlen > 0) {
         bool fast = s_safe[ls[0]] && s_safe[ls[1]] && s_safe[ls[2]];
-        if (fast) {
-          double md[3] = {0.0, 0.0, 0.0};
+        if (fast) {  // predict_small and exact integer residuals (see fixed_compress_kernel)
+          long long dmax[3] = {0, 0, 0}, dmin[3] = {0, 0, 0};
+          double t0[3], t1[3], xd[3];
+#pragma unroll
+          for (int c = 0; c < 3; c++) {
+            t0[c] = s_t0[ls[c]];
+            t1[c] = s_t1[ls[c]];
+            xd[c] = (double)(r + off[c]);
+          }
 #pragma unroll 2
           for (int m = 0; m < kCfPerThread; m++) {
             const int i = r + 64 * m;
@@ -506,13 +516,16 @@ choose_lengths_kernel(FixedCompressArgs a) {
               fast &= value_fp64_safe<T>(y);
 #pragma unroll
               for (int c = 0; c < 3; c++) {
-                const T pr = predict_from<T>(__fma_rn(s_t1[ls[c]], (double)(i + off[c]), s_t0[ls[c]]));
-                md[c] = fmax(md[c], fabs(__ll2double_rn((long long)y - (long long)pr)));
+                const long long d = (long long)y - predict_small(__fma_rn(t1[c], xd[c], t0[c]));
+                dmax[c] = d > dmax[c] ? d : dmax[c];
+                dmin[c] = d < dmin[c] ? d : dmin[c];
               }
             }
+#pragma unroll
+            for (int c = 0; c < 3; c++) xd[c] += 64.0;
           }
 #pragma unroll
-          for (int c = 0; c < 3; c++) mx[c] = (unsigned long long)md[c];
+          for (int c = 0; c < 3; c++) mx[c] = (unsigned long long)(dmax[c] > -dmin[c] ? dmax[c] : -dmin[c]);
         }
         if (!fast) {  // exact integer residuals (saturating for uint64)
           for (int c = 0; c < 3; c++) mx[c] = 0;
@@ -572,23 +585,27 @@ choose_lengths_kernel(FixedCompressArgs a) {
 // later tile of the column that starts inside the same word (tiles without bits are skipped).  The
 // column's last tile writes the final decode-table entry and the total, and zeroes the padding.
 __global__ void __launch_bounds__(256) fixed_place_kernel(FixedCompressArgs a) {
-  for (int64_t item = blockIdx.x; item < a.nitems; item += gridDim.x) {
+  // one warp per tile (many tiles in flight per SM: the copy is bound by the memory latency of
+  // each tile's few words)
+  const int lane = threadIdx.x & 31;
+  const int64_t nwarps = (int64_t)gridDim.x * (blockDim.x >> 5);
+  for (int64_t item = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); item < a.nitems; item += nwarps) {
     const CfColumn& col = a.cols ? a.cols[a.owner ? a.owner[item] : 0] : a.single;
     const int64_t t = item - col.item_base;
     const int64_t base = a.tile_first[col.item_base];
     const int64_t first = a.tile_first[item] - base;
     const int64_t bits = a.tile_bits[item];
     const int64_t col_end = col.item_base + col.ntiles;  // the column's items are [item_base, col_end)
-    const int64_t total = a.tile_first[col_end - 1] - base + a.tile_bits[col_end - 1];
     const int64_t e0 = t * kDecodeTile;
     const int cnt = (int)((col.n - e0) < kDecodeTile ? (col.n - e0) : kDecodeTile);
     const int np = (cnt + col.L - 1) / col.L;
-    if ((int)threadIdx.x < np) {
-      const int64_t gp = t * col.parts_per_tile + threadIdx.x;
+    if (lane < np) {
+      const int64_t gp = t * col.parts_per_tile + lane;
       col.offs[gp] += first;
       col.desc[gp].bit_off += first;
     }
-    if (threadIdx.x == 0) {
+    const int64_t total = a.tile_first[col_end - 1] - base + a.tile_bits[col_end - 1];
+    if (lane == 0) {
       col.tiles[t].bit_lo = first;
       if (t == col.ntiles - 1) {
         TileInfo te;
@@ -600,14 +617,16 @@ __global__ void __launch_bounds__(256) fixed_place_kernel(FixedCompressArgs a) {
     }
     const int64_t w_begin = (first + 31) >> 5, w_end = (first + bits + 31) >> 5;
     if (w_end > col.words_cap) {  // the caller sized the array from another count: report, write nothing
-      if (threadIdx.x == 0) atomicExch(a.status, (unsigned long long)DEVERR_BOUNDS);
+      if (lane == 0) atomicExch(a.status, (unsigned long long)DEVERR_BOUNDS);
       continue;
     }
     const uint32_t* slot = a.slots + item * a.slot_words;
-    for (int64_t w = w_begin + threadIdx.x; w < w_end; w += blockDim.x) {
+    const int r = (int)((32 * w_begin - first) & 31);  // the same shift for every word of the tile
+    const int64_t k0 = (32 * w_begin - first) >> 5;
+#pragma unroll 4
+    for (int64_t w = w_begin + lane; w < w_end; w += 32) {
       const int64_t lb = 32 * w - first;  // tile bit of the word's bit 0 (0 <= lb < bits)
-      const int64_t k = lb >> 5;
-      const int r = (int)(lb & 31);
+      const int64_t k = k0 + (w - w_begin);
       uint32_t v = r ? __funnelshift_r(slot[k], slot[k + 1], r) : slot[k];
       const int64_t avail = bits - lb;
       if (avail < 32) {  // the tile ends inside the word: the next tiles' first bits follow
@@ -627,7 +646,7 @@ __global__ void __launch_bounds__(256) fixed_place_kernel(FixedCompressArgs a) {
     }
     if (t == col.ntiles - 1 && col.nwords_alloc > 0) {
       const int64_t wt = (total + 31) >> 5;
-      for (int64_t w = wt + threadIdx.x; w < col.nwords_alloc && w < col.words_cap; w += blockDim.x) col.words[w] = 0u;
+      for (int64_t w = wt + lane; w < col.nwords_alloc && w < col.words_cap; w += 32) col.words[w] = 0u;
     }
   }
 }
@@ -744,7 +763,8 @@ static cudaError_t compress_pass(glc_dtype dt, FixedCompressArgs& a, void* scrat
 }
 
 static cudaError_t place_pass(const FixedCompressArgs& a, int num_sms, cudaStream_t s) {
-  int64_t grid = a.nitems < (int64_t)num_sms * 16 ? a.nitems : (int64_t)num_sms * 16;
+  const int64_t need = (a.nitems + 7) / 8;  // eight tiles (warps) per CTA
+  int64_t grid = need < (int64_t)num_sms * 16 ? need : (int64_t)num_sms * 16;
   if (grid < 1) grid = 1;
   fixed_place_kernel<<<(unsigned)grid, 256, 0, s>>>(a);
   return cudaGetLastError();

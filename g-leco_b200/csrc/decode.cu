@@ -101,6 +101,8 @@ struct Cursor {
   uint32_t base;  // bit of value e (relative to the stage) = base + e * bits  (mod 2^32)
   int start, next, bits, type, idx;
   bool nonneg;    // theta0 >= 0 and theta1 >= 0: predictions at x >= 0 are never negative
+  bool small;     // nonneg, and every prediction of the partition in this tile inside
+                  // pred_fp64_safe's bounds: the prediction needs no conversion instruction
 };
 
 template <typename T, bool PLAIN, bool RESID, int kUnroll = 2, int CW = kConsumerWarps>
@@ -141,6 +143,9 @@ __device__ __forceinline__ void decode_tile(const DecodeArgs& a, const StageInfo
     c.base = (uint32_t)(d.bit_off - stage_bit0) - (uint32_t)d.start * (uint32_t)c.bits;
     c.next = (k + 1 < np) ? (cached ? sdesc[k + 1].start : __ldg(a.starts + pf + k + 1)) : INT_MAX;
     c.idx = k;
+    // the partition's last index in this tile; with theta0, theta1 >= 0 its prediction is the largest
+    const int hi = (c.next < E1 ? c.next : E1) - 1 - c.start;
+    c.small = c.nonneg && pred_fp64_safe<T>(__fma_rn(c.t1, (double)(hi > 0 ? hi : 0), c.t0));
   };
   auto seek = [&](int e) {  // position the cursor on the partition holding value e
     int k;
@@ -218,6 +223,18 @@ __device__ __forceinline__ void decode_tile(const DecodeArgs& a, const StageInfo
       if (RESID) {
 #pragma unroll
         for (int u = 0; u < V; u++) vals[u] = (OutT)rr[u];
+      } else if (c.small) {
+        // theta0, theta1 >= 0 and predictions below 2^51 (and inside the type): round half away
+        // by the constant bias, truncate by adding 2^52 rounded toward zero (trunc_small) and
+        // read the integer from the sum's low bits -- no conversion instruction
+        const double bias = __longlong_as_double(0x3FDFFFFFFFFFFFFFll);
+#pragma unroll
+        for (int u = 0; u < V; u++) {
+          const double pr = __fma_rn(c.t1, u ? x0 + (double)u : x0, c.t0);
+          const long long m = __double_as_longlong(__dadd_rz(__dadd_rn(pr, bias), 4503599627370496.0));
+          const T pred = sizeof(T) == 8 ? (T)(m & 0xFFFFFFFFFFFFFll) : (T)(uint32_t)m;
+          vals[u] = (OutT)apply_delta<T>(pred, (long long)rr[u]);
+        }
       } else if (c.nonneg) {  // theta0, theta1 >= 0: every prediction is >= 0, one rounding bias
         const double bias = __longlong_as_double(0x3FDFFFFFFFFFFFFFll);
 #pragma unroll

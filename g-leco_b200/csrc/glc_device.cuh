@@ -76,6 +76,20 @@ template <typename T> __device__ __forceinline__ T predict_from(double p) {
   return sat_cast<T>(__dadd_rn(p, half_away_bias(p)));
 }
 
+// trunc(t) for |t| < 2^52 without a conversion instruction (conversions between 64-bit integers
+// and doubles issue on the narrow XU pipe): the magic-number method -- adding 2^52 with t's sign,
+// rounded toward zero, lands in [2^52, 2^53), where doubles are the integers, so the low 52 bits
+// of the sum hold |trunc(t)| exactly.
+__device__ __forceinline__ long long trunc_small(double t) {
+  const double m = __dadd_rz(t, copysign(4503599627370496.0, t));
+  const long long mag = __double_as_longlong(m) & 0xFFFFFFFFFFFFFll;
+  return t < 0.0 ? -mag : mag;
+}
+
+// predict_from<T>(p) for a prediction argument inside pred_fp64_safe's bounds (then |p| < 2^51
+// and the result needs no saturation): round half away from zero, by trunc_small.
+__device__ __forceinline__ long long predict_small(double p) { return trunc_small(__dadd_rn(p, half_away_bias(p))); }
+
 template <typename T> __device__ __forceinline__ T predict(double theta0, double theta1, int64_t i) {
   return predict_from<T>(__fma_rn(theta1, __ll2double_rn(i), theta0));
 }
