@@ -421,10 +421,15 @@ glc_status compress_one_pass(glc_ctx* ctx, glc_batch* b, const glc_dtype* dtypes
     f.words = c->d_words;
     f.stats = stats + 2 * i;
   }
-  // one launch per element type over the tiles of that type's columns, in column order
+  // one launch per element type over the tiles of that type's columns, in column order; the host
+  // tables stay alive until the stream is synchronised
+  std::vector<std::vector<CfColumn>> keep_g;
+  std::vector<std::vector<int64_t>> keep_ib;
   for (glc_dtype dt : {GLC_I32, GLC_I64, GLC_U64, GLC_U32}) {
-    std::vector<CfColumn> g;
-    std::vector<int64_t> ib(1, 0);
+    keep_g.emplace_back();
+    keep_ib.emplace_back(1, 0);
+    std::vector<CfColumn>& g = keep_g.back();
+    std::vector<int64_t>& ib = keep_ib.back();
     for (int i = 0; i < nc; i++) {
       if (dtypes[i] != dt || ns[i] == 0) continue;
       CfColumn f = hc[i];
@@ -449,7 +454,6 @@ glc_status compress_one_pass(glc_ctx* ctx, glc_batch* b, const glc_dtype* dtypes
     e = launch_fixed_compress_batch(dt, d_g, d_owner, nitems, scratch, stats + 2 * (size_t)nc, ctx->num_sms, s);
     cudaFreeAsync(scratch, s);
     BCK(e, "batch compress: one-pass compress");
-    BCK(cudaStreamSynchronize(s), "batch compress: sync");  // the host vectors above are reused next
   }
   std::vector<unsigned long long> hs(2 * (size_t)nc + 1);
   BCK(cudaMemcpyAsync(hs.data(), stats, sizeof(unsigned long long) * hs.size(), cudaMemcpyDeviceToHost, s),
@@ -542,9 +546,14 @@ glc_status glc_batch_compress(glc_ctx* ctx, const glc_dtype* dtypes, const void*
   if (one_pass) {  // one read of every column measures all three candidate lengths
     if ((e = cudaMemsetAsync(d_colbits, 0, sizeof(unsigned long long) * (3 * (size_t)nc + 1), s)) != cudaSuccess)
       return bail(bcuda(ctx, e, "batch compress: sizes"));
-    for (glc_dtype dt : {GLC_I32, GLC_I64, GLC_U64, GLC_U32}) {  // one launch per element type
-      std::vector<CfColumn> g;
-      std::vector<int64_t> ib(1, 0);
+    // one launch per element type; the host tables stay alive until the stream is synchronised
+    std::vector<std::vector<CfColumn>> keep_g;
+    std::vector<std::vector<int64_t>> keep_ib;
+    for (glc_dtype dt : {GLC_I32, GLC_I64, GLC_U64, GLC_U32}) {
+      keep_g.emplace_back();
+      keep_ib.emplace_back(1, 0);
+      std::vector<CfColumn>& g = keep_g.back();
+      std::vector<int64_t>& ib = keep_ib.back();
       for (int i = 0; i < nc; i++) {
         if (dtypes[i] != dt || ns[i] == 0) continue;
         CfColumn f{};
@@ -565,8 +574,7 @@ glc_status glc_batch_compress(glc_ctx* ctx, const glc_dtype* dtypes, const void*
       if ((e = cudaMemcpyAsync(d_g, g.data(), sizeof(CfColumn) * g.size(), cudaMemcpyHostToDevice, s)) ||
           (e = cudaMemcpyAsync(d_ib, ib.data(), sizeof(int64_t) * ib.size(), cudaMemcpyHostToDevice, s)) ||
           (e = launch_pack_item_owner(d_ib, (int)g.size(), d_owner, s)) ||
-          (e = launch_choose_lengths(dt, d_g, d_owner, ib.back(), d_colbits + 3 * (size_t)nc, ctx->num_sms, s)) ||
-          (e = cudaStreamSynchronize(s)))  // the host vectors are reused by the next type
+          (e = launch_choose_lengths(dt, d_g, d_owner, ib.back(), d_colbits + 3 * (size_t)nc, ctx->num_sms, s)))
         return bail(bcuda(ctx, e, "batch compress: length choice"));
     }
     unsigned long long choice_status = 0;
