@@ -41,6 +41,26 @@ struct glc_batch {
   cudaStream_t alloc_stream = nullptr;        // stream of the pool allocations in `storage`
   int* d_err = nullptr;
   cudaGraphExec_t graph = nullptr;
+  // batches compressed by the one-pass kernel (lengths 1024 / 2048 / 4096): what
+  // glc_batch_recompress needs -- the columns' element types, sizes and lengths, and after its
+  // first call word arrays of the widest size, the launch tables and scratch of each element type
+  bool one_pass = false;
+  std::vector<glc_dtype> dtypes;
+  std::vector<int64_t> ns;
+  std::vector<int32_t> lens;
+  struct ReGroup {
+    glc_dtype dt;
+    std::vector<int> cols;  // batch columns of this type with values
+    CfColumn* d_tab = nullptr;
+    int32_t* d_owner = nullptr;
+    int64_t nitems = 0;
+    void* scratch = nullptr;
+  };
+  std::vector<ReGroup> re;
+  std::vector<const void*> re_values;      // the values the launch tables point at
+  unsigned long long* re_stats = nullptr;  // 2 per column (total bits, widest field), then a status
+  cudaGraphExec_t re_graph = nullptr;
+  bool re_stale = false;                   // the host-side column sizes await glc_batch_sync
 };
 
 namespace {
@@ -274,6 +294,7 @@ template <typename V> cudaError_t dalloc(glc_batch* b, V** p, size_t count) {
 
 void free_batch(glc_batch* b) {
   if (b->graph) cudaGraphExecDestroy(b->graph);
+  if (b->re_graph) cudaGraphExecDestroy(b->re_graph);
   if (b->owns_columns)
     for (glc_column* c : b->cols) delete c;  // views: their arrays are in storage
   for (void* q : b->storage) cudaFreeAsync(q, b->ctx->own_stream);
@@ -470,7 +491,111 @@ glc_status compress_one_pass(glc_ctx* ctx, glc_batch* b, const glc_dtype* dtypes
     total += c->reported_size;
   }
   if (total_size) *total_size = total;
+  b->one_pass = true;
+  b->dtypes.assign(dtypes, dtypes + nc);
+  b->ns.assign(ns, ns + nc);
+  b->lens = len;
   return GLC_OK;
+}
+
+// Word arrays of the widest size for every column, launch tables and scratch per element type
+// (glc_batch_recompress's first call).
+glc_status recompress_setup(glc_ctx* ctx, glc_batch* b, cudaStream_t s) {
+  const int nc = (int)b->cols.size();
+  std::vector<int64_t> cap(nc), wb(nc + 1, 0);
+  for (int i = 0; i < nc; i++) {
+    cap[i] = b->ns[i] > 0 ? ((fixed_compress_worst_words(b->dtypes[i], b->ns[i]) + 3) & ~3ll) : 4;
+    wb[i + 1] = wb[i] + cap[i];
+  }
+  uint32_t* words;
+  cudaError_t e;
+  if ((e = dalloc(b, &words, wb[nc])) || (e = dalloc(b, &b->re_stats, 2 * (size_t)nc + 1)))
+    return bcuda(ctx, e, "batch recompress: allocation");
+  for (int i = 0; i < nc; i++) {
+    glc_column* c = b->cols[i];
+    c->d_words = words + wb[i];
+    c->nwords_alloc = cap[i];
+  }
+  for (glc_dtype dt : {GLC_I32, GLC_I64, GLC_U64, GLC_U32}) {
+    glc_batch::ReGroup g;
+    g.dt = dt;
+    for (int i = 0; i < nc; i++)
+      if (b->dtypes[i] == dt && b->ns[i] > 0) {
+        g.cols.push_back(i);
+        g.nitems += b->cols[i]->ntiles;
+      }
+    if (g.cols.empty()) continue;
+    if ((e = dalloc(b, &g.d_tab, g.cols.size())) || (e = dalloc(b, &g.d_owner, g.nitems)) ||
+        (e = dalloc(b, (uint8_t**)&g.scratch, fixed_compress_scratch_bytes(dt, g.nitems))))
+      return bcuda(ctx, e, "batch recompress: allocation");
+    b->re.push_back(g);
+  }
+  // the decode reads the new word arrays
+  std::vector<BatchColumn> h(nc);
+  for (int i = 0; i < nc; i++) {
+    const glc_column* c = b->cols[i];
+    h[i] = BatchColumn{c->d_desc, c->d_start, c->d_tiles, c->d_words, c->n, (int32_t)c->dtype, c->max_bits};
+  }
+  BCK(cudaMemcpyAsync(b->d_cols, h.data(), sizeof(BatchColumn) * nc, cudaMemcpyHostToDevice, s), "batch recompress");
+  BCK(cudaStreamSynchronize(s), "batch recompress");
+  return GLC_OK;
+}
+
+// The launch tables of every element type for these values (columns' arrays, widest word arrays).
+glc_status recompress_tables(glc_ctx* ctx, glc_batch* b, const void* const* values, cudaStream_t s) {
+  for (glc_batch::ReGroup& g : b->re) {
+    std::vector<CfColumn> tab;
+    std::vector<int64_t> ib(1, 0);
+    for (int i : g.cols) {
+      const glc_column* c = b->cols[i];
+      CfColumn f{};
+      f.values = values[i];
+      f.n = c->n;
+      f.L = b->lens[i];
+      f.parts_per_tile = kDecodeTile / f.L;
+      f.P = c->P;
+      f.ntiles = c->ntiles;
+      f.item_base = ib.back();
+      f.nwords_alloc = c->nwords_alloc;
+      f.words_cap = c->nwords_alloc;
+      f.starts = c->d_start;
+      f.ends = c->d_end;
+      f.types = c->d_types;
+      f.params = c->d_params;
+      f.bits = c->d_bits;
+      f.offs = c->d_offs;
+      f.err = c->d_err;
+      f.desc = c->d_desc;
+      f.tiles = c->d_tiles;
+      f.words = c->d_words;
+      f.stats = b->re_stats + 2 * (size_t)i;
+      tab.push_back(f);
+      ib.push_back(ib.back() + f.ntiles);
+    }
+    int64_t* d_ib;
+    cudaError_t e;
+    if ((e = dalloc(b, &d_ib, ib.size()))) return bcuda(ctx, e, "batch recompress: allocation");
+    BCK(cudaMemcpyAsync(g.d_tab, tab.data(), sizeof(CfColumn) * tab.size(), cudaMemcpyHostToDevice, s),
+        "batch recompress: tables");
+    BCK(cudaMemcpyAsync(d_ib, ib.data(), sizeof(int64_t) * ib.size(), cudaMemcpyHostToDevice, s),
+        "batch recompress: tables");
+    BCK(launch_pack_item_owner(d_ib, (int)tab.size(), g.d_owner, s), "batch recompress: work list");
+    BCK(cudaStreamSynchronize(s), "batch recompress: tables");
+  }
+  b->re_values.assign(values, values + b->cols.size());
+  return GLC_OK;
+}
+
+// The launches of one recompress (stream-ordered, nothing read back; capturable).
+cudaError_t recompress_launches(glc_ctx* ctx, glc_batch* b, cudaStream_t s) {
+  const size_t nc = b->cols.size();
+  cudaError_t e = cudaMemsetAsync(b->re_stats, 0, sizeof(unsigned long long) * (2 * nc + 1), s);
+  for (const glc_batch::ReGroup& g : b->re) {
+    if (e != cudaSuccess) break;
+    e = launch_fixed_compress_batch(g.dt, g.d_tab, g.d_owner, g.nitems, g.scratch, b->re_stats + 2 * nc, ctx->num_sms,
+                                    s);
+  }
+  return e;
 }
 
 }  // namespace
@@ -778,6 +903,99 @@ glc_status glc_batch_decompress(glc_ctx* ctx, glc_batch* b, void* const* outs, i
     if (e != cudaSuccess) { b->graph = nullptr; return bcuda(ctx, e, "batch decode: instantiate"); }
   }
   BCK(cudaGraphLaunch(b->graph, s), "batch decode: graph launch");
+  return GLC_OK;
+}
+
+glc_status glc_batch_recompress(glc_ctx* ctx, glc_batch* b, const void* const* values, int use_graph,
+                                glc_stream stream) {
+  if (!ctx || !b || !values) return bfail(ctx, GLC_ERR_INVALID_ARG, "bad batch arguments");
+  if (!b->one_pass)
+    return bfail(ctx, GLC_ERR_UNSUPPORTED, "recompress needs a batch compressed at lengths 1024 / 2048 / 4096");
+  for (size_t i = 0; i < b->cols.size(); i++)
+    if (b->ns[i] > 0 && (!values[i] || ((uintptr_t)values[i] % dtype_size(b->dtypes[i])) != 0))
+      return bfail(ctx, GLC_ERR_INVALID_ARG, "null or misaligned values for a column of the batch");
+  glc::DeviceScope device_scope(ctx->device);
+  cudaStream_t s = stream ? (cudaStream_t)stream : ctx->own_stream;
+  glc_status st;
+  if (b->re.empty() && !b->cols.empty()) {
+    if ((st = recompress_setup(ctx, b, s)) != GLC_OK) return st;
+  }
+  bool same = b->re_values.size() == b->cols.size();
+  for (size_t i = 0; same && i < b->cols.size(); i++) same = b->re_values[i] == values[i];
+  if (!same) {
+    if (b->re_graph) {
+      cudaGraphExecDestroy(b->re_graph);
+      b->re_graph = nullptr;
+    }
+    if ((st = recompress_tables(ctx, b, values, s)) != GLC_OK) return st;
+  }
+  // until glc_batch_sync, the decode stages the widest tiles the element types allow
+  int widest = 0;
+  for (glc_dtype dt : b->dtypes) widest = std::max(widest, dtype_size(dt) == 8 ? 64 : 33);
+  if (b->max_bits != widest && b->graph) {
+    cudaGraphExecDestroy(b->graph);
+    b->graph = nullptr;
+  }
+  b->max_bits = widest;
+  b->re_stale = true;
+  if (!use_graph) {
+    BCK(recompress_launches(ctx, b, s), "batch recompress");
+    return GLC_OK;
+  }
+  if (!b->re_graph) {
+    cudaGraph_t g = nullptr;
+    BCK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "batch recompress: capture");
+    cudaError_t e = recompress_launches(ctx, b, s);
+    cudaError_t e2 = cudaStreamEndCapture(s, &g);
+    if (e != cudaSuccess) { if (g) cudaGraphDestroy(g); return bcuda(ctx, e, "batch recompress: capture"); }
+    if (e2 != cudaSuccess) return bcuda(ctx, e2, "batch recompress: capture");
+    e = cudaGraphInstantiate(&b->re_graph, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) { b->re_graph = nullptr; return bcuda(ctx, e, "batch recompress: instantiate"); }
+  }
+  BCK(cudaGraphLaunch(b->re_graph, s), "batch recompress: graph launch");
+  return GLC_OK;
+}
+
+glc_status glc_batch_sync(glc_ctx* ctx, glc_batch* b, glc_stream stream, int64_t* compressed_size_bytes) {
+  if (!ctx || !b) return bfail(ctx, GLC_ERR_INVALID_ARG, "bad batch arguments");
+  glc::DeviceScope device_scope(ctx->device);
+  cudaStream_t s = stream ? (cudaStream_t)stream : ctx->own_stream;
+  const size_t nc = b->cols.size();
+  int64_t total = 0;
+  if (b->re_stale) {
+    std::vector<unsigned long long> hs(2 * nc + 1);
+    BCK(cudaMemcpyAsync(hs.data(), b->re_stats, sizeof(unsigned long long) * hs.size(), cudaMemcpyDeviceToHost, s),
+        "batch sync");
+    BCK(cudaStreamSynchronize(s), "batch sync");
+    if (hs[2 * nc] == DEVERR_TIMEOUT) return bfail(ctx, GLC_ERR_TIMEOUT, "batch recompress: a device-side wait gave up");
+    if (hs[2 * nc] != DEVERR_NONE) return bfail(ctx, GLC_ERR_CUDA, "batch recompress: words beyond their array");
+    std::vector<BatchColumn> h(nc);
+    int mb = 0;
+    for (size_t i = 0; i < nc; i++) {
+      glc_column* c = b->cols[i];
+      if (c->n > 0) {
+        c->total_bits = (int64_t)hs[2 * i];
+        c->max_bits = (int32_t)hs[2 * i + 1];
+        c->nwords = (c->total_bits + 31) / 32;
+        c->reported_size = 64 * c->P + 120 + (c->total_bits + 7) / 8;  // api/G-LeCo.cuh:589-603
+      }
+      mb = std::max(mb, c->max_bits);
+      h[i] = BatchColumn{c->d_desc, c->d_start, c->d_tiles, c->d_words, c->n, (int32_t)c->dtype, c->max_bits};
+    }
+    BCK(cudaMemcpyAsync(b->d_cols, h.data(), sizeof(BatchColumn) * nc, cudaMemcpyHostToDevice, s), "batch sync");
+    BCK(cudaStreamSynchronize(s), "batch sync");
+    if (mb != b->max_bits && b->graph) {
+      cudaGraphExecDestroy(b->graph);
+      b->graph = nullptr;
+    }
+    b->max_bits = mb;
+    b->re_stale = false;
+  } else {
+    BCK(cudaStreamSynchronize(s), "batch sync");
+  }
+  for (glc_column* c : b->cols) total += c->reported_size;
+  if (compressed_size_bytes) *compressed_size_bytes = total;
   return GLC_OK;
 }
 

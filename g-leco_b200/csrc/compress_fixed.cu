@@ -644,9 +644,11 @@ __global__ void __launch_bounds__(256) fixed_place_kernel(FixedCompressArgs a) {
       }
       col.words[w] = v;
     }
-    if (t == col.ntiles - 1 && col.nwords_alloc > 0) {
+    if (t == col.ntiles - 1 && col.nwords_alloc > 0) {  // the decoders' zeroed read-ahead after the bitstream
       const int64_t wt = (total + 31) >> 5;
-      for (int64_t w = wt + lane; w < col.nwords_alloc && w < col.words_cap; w += 32) col.words[w] = 0u;
+      int64_t pad_end = ((wt + 3) & ~3ll) + 8;
+      pad_end = pad_end < col.nwords_alloc ? pad_end : col.nwords_alloc;
+      for (int64_t w = wt + lane; w < pad_end && w < col.words_cap; w += 32) col.words[w] = 0u;
     }
   }
 }
@@ -722,6 +724,11 @@ cudaError_t launch_choose_lengths(glc_dtype dt, const CfColumn* cols, const int3
     case GLC_U32: return launch_choose_t<uint32_t>(a, num_sms, s);
   }
   return cudaErrorInvalidValue;
+}
+
+int64_t fixed_compress_worst_words(glc_dtype dt, int64_t n) {
+  const int64_t per_value = (dt == GLC_I64 || dt == GLC_U64) ? 64 : 33;  // widest field of the type
+  return (n * per_value + 31) / 32 + 12;  // + the decoders' zeroed read-ahead
 }
 
 bool fixed_compress_supported(int64_t n, int32_t L) {

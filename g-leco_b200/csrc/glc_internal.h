@@ -217,6 +217,7 @@ struct CfColumn {
 
 bool fixed_compress_supported(int64_t n, int32_t L);
 int64_t fixed_compress_slot_words(glc_dtype dt);
+int64_t fixed_compress_worst_words(glc_dtype dt, int64_t n);  // the widest fields of the type, + padding
 size_t fixed_compress_scratch_bytes(glc_dtype dt, int64_t nitems);  // nitems = 4096-value tiles of the launch
 cudaError_t launch_fixed_compress(glc_dtype dt, const void* values, glc_column* c, int32_t L, void* scratch,
                                   unsigned long long* stats, cudaStream_t s);

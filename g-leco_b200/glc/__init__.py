@@ -36,7 +36,7 @@ EXPORTS = [
     "glc_decompress_range", "glc_random_access", "glc_preunpack", "glc_blob_size", "glc_serialize",
     "glc_deserialize", "glc_attach_blob", "glc_decode_blob_to_host", "glc_decompress_range_noalloc",
     "glc_batch_create", "glc_batch_compress",
-    "glc_batch_column", "glc_batch_decompress", "glc_batch_free", "glc_server_create", "glc_server_destroy",
+    "glc_batch_column", "glc_batch_decompress", "glc_batch_recompress", "glc_batch_sync", "glc_batch_free", "glc_server_create", "glc_server_destroy",
     "glc_server_admit", "glc_server_admit_blob", "glc_server_evict", "glc_server_submit", "glc_server_poll",
     "glc_server_drain", "glc_server_get_stats", "glc_server_now_ns", "glc_server_columns",
     "glc_autotune", "glc_tune_get", "glc_tune_set",
@@ -147,6 +147,8 @@ def load() -> ctypes.CDLL:
         "glc_batch_compress": ([vp, vp, vp, vp, i32, i32, pvp, pi64, vp], c_int),
         "glc_batch_column": ([vp, i32, pvp], c_int),
         "glc_batch_decompress": ([vp, vp, vp, c_int, vp], c_int),
+        "glc_batch_recompress": ([vp, vp, vp, c_int, vp], c_int),
+        "glc_batch_sync": ([vp, vp, vp, pi64], c_int),
         "glc_batch_free": ([vp], c_int),
         "glc_server_create": ([vp, ctypes.POINTER(ServerConfig), pvp], c_int),
         "glc_server_destroy": ([vp], c_int),
@@ -434,6 +436,21 @@ class Batch:
         arr = (ctypes.c_void_p * n)(*out_ptrs)
         self.ctx.check(self.ctx.lib.glc_batch_decompress(self.ctx.handle, self.handle, arr, 1 if use_graph else 0,
                                                          ctypes.c_void_p(stream)))
+
+    def recompress(self, dptrs, use_graph: bool = False, stream: int = 0):
+        """glc_batch_recompress: new values for the same columns, each at the length chosen before."""
+        n = len(self.columns)
+        vp = (ctypes.c_void_p * n)(*dptrs)
+        self.ctx.check(self.ctx.lib.glc_batch_recompress(self.ctx.handle, self.handle, vp, 1 if use_graph else 0,
+                                                         ctypes.c_void_p(stream)))
+
+    def sync(self, stream: int = 0) -> int:
+        """glc_batch_sync: the columns' sizes after recompress; returns the total compressed size."""
+        size = ctypes.c_int64()
+        self.ctx.check(self.ctx.lib.glc_batch_sync(self.ctx.handle, self.handle, ctypes.c_void_p(stream),
+                                                   ctypes.byref(size)))
+        self.compressed_size = size.value
+        return size.value
 
     def free(self):
         if self.handle:

@@ -240,6 +240,24 @@ GLC_API glc_status glc_batch_column(const glc_batch* batch, int32_t i, glc_colum
 GLC_API glc_status glc_batch_decompress(glc_ctx* ctx, glc_batch* batch, void* const* outs, int use_graph,
                                         glc_stream stream);
 
+/* Compress new values into a batch that glc_batch_compress made at lengths 1024 / 2048 / 4096
+ * (fixed_partition_len 0, 1024, 2048 or 4096): the same columns -- element types and sizes in the
+ * same order -- with values at new device addresses (aligned to the element size), every column
+ * at the partition length the batch chose for it.  Nothing is read back to the host and nothing is
+ * allocated after the first call (which gives the batch word arrays for the widest fields of each
+ * element type), so the call is stream-ordered; with use_graph != 0 it is captured in a CUDA graph
+ * on the first such call and replayed while `values` stay the same.  The columns' device arrays are
+ * rewritten in place; their host-side sizes (glc_column_get_info, glc_blob_size, glc_serialize,
+ * the compressed size) are brought up to date by glc_batch_sync.  No counterpart in the reference,
+ * whose every compress is one host round trip per column (api/G-LeCo.cuh:349-614). */
+GLC_API glc_status glc_batch_recompress(glc_ctx* ctx, glc_batch* batch, const void* const* values, int use_graph,
+                                        glc_stream stream);
+
+/* Wait for the batch's work on `stream`, then read the columns' sizes written by the last
+ * glc_batch_recompress (GLC_ERR_TIMEOUT if a bounded wait of it gave up); *compressed_size_bytes
+ * (may be NULL) receives the sum of the columns' reported sizes. */
+GLC_API glc_status glc_batch_sync(glc_ctx* ctx, glc_batch* batch, glc_stream stream, int64_t* compressed_size_bytes);
+
 GLC_API glc_status glc_batch_free(glc_batch* batch);
 
 /* ---- allocation-free range decode (no counterpart in the reference) --------------------- */

@@ -140,3 +140,53 @@ def test_batch_column_random_access_and_range():
     with pytest.raises(glc.GlcError):
         ctx.check(ctx.lib.glc_column_free(batch.columns[0].handle))  # owned by the batch
     batch.free()
+
+
+@pytest.mark.parametrize("use_graph", [False, True])
+def test_batch_recompress_new_values(oracle, use_graph):
+    """glc_batch_recompress: new values for the same columns, each at the length the batch chose;
+    after glc_batch_sync every column equals glc_compress of the new values at that length, and the
+    batched decode returns them.  With a CUDA graph the second call replays the first's capture on
+    other values written into the same device buffers."""
+    ctx = glc.Context(0)
+    cols = _columns(24, seed=5)
+    dev = [_to_device(v) for _, v in cols]
+    batch = glc.Batch.compress(ctx, [d for d, _ in cols], [t.data_ptr() for t in dev], [len(v) for _, v in cols],
+                               fixed_len=0)
+    lens = [bc.info().fixed_partition_len for bc in batch.columns]
+    for round_ in range(2):
+        fresh = _columns(24, seed=100 + round_)
+        for (dt, v), (_, w), t in zip(cols, fresh, dev):  # the same sizes, other values, same buffers
+            w = np.resize(w, len(v)).astype(v.dtype) if len(v) else v
+            t.copy_(_to_device(w))
+        torch.cuda.synchronize()
+        batch.recompress([t.data_ptr() for t in dev], use_graph=use_graph)
+        total = batch.sync()
+        want_total = 0
+        outs = []
+        for (dt, v), t, bc, L in zip(cols, dev, batch.columns, lens):
+            host = t.cpu().numpy().view(v.dtype)
+            if len(v) == 0:
+                outs.append(torch.zeros(16, dtype=torch.uint8, device="cuda:0"))
+                continue
+            info = bc.info()
+            assert info.fixed_partition_len == L
+            single = glc.compress_device(ctx, dt, host.ctypes.data, len(host), glc.FIXED, fixed_len=L, host=True)
+            assert glc.serialize_host(ctx, bc) == glc.serialize_host(ctx, single)
+            assert info.compressed_size_bytes == single.info().compressed_size_bytes
+            want_total += info.compressed_size_bytes
+            single.free()
+            outs.append(torch.zeros(len(v) + 8, dtype=DT[dt][1], device="cuda:0"))
+        assert total == want_total
+        torch.cuda.synchronize()
+        batch.decompress([o.data_ptr() for o in outs], use_graph=use_graph)
+        ctx.sync()
+        for (dt, v), t, o in zip(cols, dev, outs):
+            if len(v):
+                assert torch.equal(o[:len(v)], t)
+    # the last recompress against the oracle, column by column
+    for (dt, v), t, bc, L in zip(cols, dev, batch.columns, lens):
+        if len(v):
+            host = t.cpu().numpy().view(v.dtype)
+            assert glc.serialize_host(ctx, bc) == oracle.serialize(oracle.compress(host, "fixed", L))
+    batch.free()
