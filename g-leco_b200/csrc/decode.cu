@@ -105,7 +105,10 @@ struct Cursor {
                   // pred_fp64_safe's bounds: the prediction needs no conversion instruction
 };
 
-template <typename T, bool PLAIN, bool RESID, int kUnroll = 2, int CW = kConsumerWarps>
+// SMALL: 4-byte outputs may take the conversion-free prediction (off in the batch kernel, whose
+// one body serves every element type and would otherwise need more registers than its occupancy
+// allows).
+template <typename T, bool PLAIN, bool RESID, int kUnroll = 2, int CW = kConsumerWarps, bool SMALL = true>
 __device__ __forceinline__ void decode_tile(const DecodeArgs& a, const StageInfo& si, const uint8_t* stage,
                                             const PartDesc* sdesc) {
   constexpr int kThreads = CW * 32;  // consumer threads of the CTA
@@ -145,7 +148,7 @@ __device__ __forceinline__ void decode_tile(const DecodeArgs& a, const StageInfo
     c.idx = k;
     // 4-byte outputs (8 values per vector, so the conversions dominate): the partition's last index
     // in this tile; with theta0, theta1 >= 0 its prediction is the largest
-    if (sizeof(T) == 4) {
+    if (SMALL && sizeof(T) == 4) {
       const int hi = (c.next < E1 ? c.next : E1) - 1 - c.start;
       c.small = c.nonneg && pred_fp64_safe<T>(__fma_rn(c.t1, (double)(hi > 0 ? hi : 0), c.t0));
     } else {
@@ -228,7 +231,7 @@ __device__ __forceinline__ void decode_tile(const DecodeArgs& a, const StageInfo
       if (RESID) {
 #pragma unroll
         for (int u = 0; u < V; u++) vals[u] = (OutT)rr[u];
-      } else if (sizeof(T) == 4 && c.small) {
+      } else if (SMALL && sizeof(T) == 4 && c.small) {
         // theta0, theta1 >= 0 and predictions below 2^51 (and inside the type): round half away
         // by the constant bias, truncate by adding 2^52 rounded toward zero (trunc_small) and
         // read the integer from the sum's low bits -- no conversion instruction
@@ -464,7 +467,7 @@ __device__ __forceinline__ void batch_body(const BatchDecodeArgs& b, int g, uint
     a.out_base = w.out_base;
     a.stage_bytes = b.stage_bytes;
     a.first_wait_tests = -1;
-    decode_tile<T, false, false>(a, si, smem + (size_t)s * b.stage_bytes, &s_desc[s][0]);
+    decode_tile<T, false, false, 2, kConsumerWarps, false>(a, si, smem + (size_t)s * b.stage_bytes, &s_desc[s][0]);
     __syncwarp();
     if (lane == 0) mbar_arrive(&empty[s]);
   }

@@ -115,7 +115,12 @@ template <typename T> __device__ __forceinline__ bool line_fp64_safe(double t0, 
   return pred_fp64_safe<T>(__fma_rn(t1, (double)i0, t0)) && pred_fp64_safe<T>(__fma_rn(t1, (double)i1, t0));
 }
 __device__ __forceinline__ double abs_resid_fp64(double yd, double x) {
-  return fabs(__dsub_rn(yd, trunc(__dadd_rn(x, half_away_bias(x)))));
+  // trunc(t) by the magic number c = +-2^52 (trunc_small): m = t + c rounded toward zero is
+  // c + trunc(t) exactly, and (yd + c) - m = yd - trunc(t) is exact (|yd| < 2^51), so no
+  // rounding instruction is needed
+  const double t = __dadd_rn(x, half_away_bias(x));
+  const double c = copysign(4503599627370496.0, t);
+  return fabs(__dsub_rn(__dadd_rn(yd, c), __dadd_rz(t, c)));
 }
 
 // Exact sums of y and j * y over the values a thread adds (j < 2^14, at most 2^10 values per
@@ -124,13 +129,17 @@ template <typename T> struct HalfSums {
   typedef typename std::conditional<TypeTraits<T>::is_signed, int64_t, uint64_t>::type Acc;
   Acc s_lo = 0, s_hi = 0, x_lo = 0, x_hi = 0;
   __device__ __forceinline__ void add(T y, int j) {
-    if (sizeof(T) == 8) {
-      const uint32_t yl = (uint32_t)(uint64_t)y;
-      const Acc yh = TypeTraits<T>::is_signed ? (Acc)(int32_t)((int64_t)y >> 32) : (Acc)(uint32_t)((uint64_t)y >> 32);
+    if (sizeof(T) == 8) {  // j >= 0: 32 x 32 -> 64-bit products
+      const uint32_t yl = (uint32_t)(uint64_t)y, yh = (uint32_t)((uint64_t)y >> 32);
       s_lo += (Acc)yl;
-      s_hi += yh;
-      x_lo += (Acc)((uint64_t)(uint32_t)j * yl);
-      x_hi += (Acc)j * yh;
+      x_lo += (Acc)((uint64_t)(uint32_t)j * (uint64_t)yl);
+      if (TypeTraits<T>::is_signed) {
+        s_hi += (Acc)(int32_t)yh;
+        x_hi += (Acc)((long long)j * (long long)(int32_t)yh);
+      } else {
+        s_hi += (Acc)yh;
+        x_hi += (Acc)((uint64_t)(uint32_t)j * (uint64_t)yh);
+      }
     } else {
       s_lo += (Acc)y;
       x_lo += (Acc)j * (Acc)y;

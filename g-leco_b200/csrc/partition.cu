@@ -116,12 +116,14 @@ __device__ __forceinline__ void split_bands(const T* __restrict__ v, int64_t s, 
       const T y = __ldg(v + s + o0 + lane);
       vals_ok &= TypeTraits<T>::is_signed ? ((long long)y > -(1ll << 51) && (long long)y < (1ll << 51))
                                           : ((uint64_t)y < (1ull << 51));
-      const double yd = (double)(long long)y;
+      // yd + 2^52 (exact for |y| < 2^51); with predictions >= -0.25 the truncation is the sum
+      // with 2^52 rounded toward zero (trunc_small), and their difference is y - pred exactly
+      const double yc = __dadd_rn((double)(long long)y, 4503599627370496.0);
 #pragma unroll
       for (int k = B; k < kNumSizes; k++) {
         const double2 t = *reinterpret_cast<const double2*>(th[k]);  // broadcast shared-memory load
-        const double pred = trunc(__dadd_rn(__fma_rn(t.y, od, t.x), kBias));
-        md[k] = fmax(md[k], fabs(__dsub_rn(yd, pred)));
+        const double m = __dadd_rz(__dadd_rn(__fma_rn(t.y, od, t.x), kBias), 4503599627370496.0);
+        md[k] = fmax(md[k], fabs(__dsub_rn(yc, m)));
       }
     }
     split_bands<B + 1, T>(v, s, lane, th, md, vals_ok);
@@ -201,9 +203,7 @@ split_kernel(const T* __restrict__ v, RangeSums rs, int32_t* __restrict__ nb_nex
       for (int k = 0; k < kNumSizes; k++) {
         if (k < band || k >= ncand) continue;
         const double2 th = *reinterpret_cast<const double2*>(&s_th[warp][k][0]);
-        const double x = __fma_rn(th.y, od, th.x);
-        const double pred = trunc(__dadd_rn(x, half_away_bias(x)));
-        md[k] = fmax(md[k], fabs(__dsub_rn(yd, pred)));
+        md[k] = fmax(md[k], abs_resid_fp64(yd, __fma_rn(th.y, od, th.x)));
       }
     }
     fast = __all_sync(FULL_MASK, vals_ok);
