@@ -46,9 +46,14 @@ constexpr int kCfMaxParts = kDecodeTile / kCfMinLen;  // 16 partitions per tile 
 constexpr int kCfPerThread = kDecodeTile / kCfThreads;  // 16 values per thread
 constexpr int kCfMaxSegs = 16;                        // reduction segments (half-warps at L = 256)
 
-template <typename T> __host__ __device__ constexpr int cf_stage_bytes() { return kDecodeTile * (int)sizeof(T) + 16; }
-template <typename T> __host__ __device__ constexpr int cf_smem_bytes() {
-  return kCfStages * cf_stage_bytes<T>() + (sizeof(T) == 4 ? kDecodeTile * 8 : 0);
+// The work area of the packing: the transposed fields (32 x 129 words) and the staged words (4096
+// plus a pad word per 32), or the 64-bit residuals of the wide-field path (4096 x 8 bytes).
+constexpr int kCfWorkBytes = (32 * 129 + kDecodeTile + kDecodeTile / 32) * 4;
+static_assert(kCfWorkBytes >= kDecodeTile * 8, "the work area holds a tile's 64-bit residuals");
+// A stage holds a tile's values from the 16-byte block of the first one; for 8-byte types it is
+// also the work area of its tile.
+template <typename T> __host__ __device__ constexpr int cf_stage_bytes() {
+  return sizeof(T) == 8 ? kCfWorkBytes : kDecodeTile * (int)sizeof(T) + 16;
 }
 
 // A launch: work item i = one 4096-value tile of column owner[i] (every column of one element
@@ -68,15 +73,15 @@ struct FixedCompressArgs {
 __device__ __forceinline__ void cf_sync() { asm volatile("bar.sync 1, %0;" ::"n"(kCfThreads) : "memory"); }
 
 // The producer lane of a launch: stages item blockIdx.x + k * gridDim.x of the work list into stage
-// k % kCfStages (its values, from the 16-byte block that holds the first one), with the item, its
+// k % S (its values, from the 16-byte block that holds the first one), with the item, its
 // column and the offset of its first value in the stage; an item of -1 marks the end.
-template <typename T>
+template <typename T, int S>
 __device__ __forceinline__ void cf_produce(const FixedCompressArgs& a, uint8_t* smem, uint64_t* full, uint64_t* empty,
                                            int64_t* s_stile, int* s_shead, int* s_scol) {
   int64_t item = blockIdx.x;
   for (int k = 0;; k++, item += gridDim.x) {
-    const int st = k % kCfStages;
-    if (k >= kCfStages && !mbar_wait_bounded(&empty[st], (uint32_t)((k / kCfStages) - 1) & 1u)) {
+    const int st = k % S;
+    if (k >= S && !mbar_wait_sleep(&empty[st], (uint32_t)((k / S) - 1) & 1u)) {
       atomicExch(a.status, (unsigned long long)DEVERR_TIMEOUT);
       s_stile[st] = -1;  // the compute warps stop at this stage (or time out on it)
       mbar_arrive(&full[st]);
@@ -105,297 +110,657 @@ __device__ __forceinline__ void cf_produce(const FixedCompressArgs& a, uint8_t* 
   }
 }
 
-template <typename T> __global__ void __launch_bounds__(kCfCTA)
-fixed_compress_kernel(FixedCompressArgs a) {
+// ---- pieces of the compute warps -----------------------------------------------------------
+
+constexpr double kMagic = 6755399441055744.0;        // K = 1.5 * 2^52: the bits of K + v are 0x4338... + v, |v| <= 2^51
+constexpr double kHalfBias = 0x1.fffffffffffffp-2;    // 0.5 - 2^-54
+constexpr int kFtStride = 129;                        // transposed fields: field f of 32-value group G at f * 129 + G
+constexpr int kFtWords = 32 * kFtStride;
+constexpr int kStgWords = kDecodeTile + kDecodeTile / 32;  // a tile's words, one pad word after every 32
+
+// How a partition's residuals are computed (uniform per partition, so per thread):
+//   CF_DIRECT   direct copy (a uint64 value above 2^53): the field is the value;
+//   CF_NONNEG   |y| < 2^51 and predictions in [-0.25, 2^51] (4-byte types: inside the type): in
+//               FP64 with K: K + y from the bits, K + pred = (x + (0.5 - 2^-54)) + K rounded toward
+//               zero, their difference is y - pred exactly;
+//   CF_NONPOS   the mirror for signed types, predictions in [-2^51, 0.25]: K - pred =
+//               ((0.5 - 2^-54) - x) + K rounded toward zero;
+//   CF_OFFSET   8-byte types with predictions in [2^50, 2^62] within 2^50 of c = trunc(theta0):
+//               x - c and x - c + 0.5 are exact, pred = c + floor(x - c + 0.5), y - c by integer
+//               arithmetic (a thread whose |y - c| reaches 2^51 recomputes its values in general);
+//   CF_GENERAL  predict_from / calc_delta / abs_ref per value.
+// Each gives calc_delta<T>(y, predict_from<T>(fma(theta1, i, theta0))) exactly; the field is its
+// low 32 bits (the low bits of (y - pred) + K), which is all the packing of a width <= 31 reads.
+enum : int { CF_DIRECT = 0, CF_NONNEG = 1, CF_NONPOS = 2, CF_GENERAL = 3, CF_OFFSET = 4 };
+
+// Exact sum over a reduction segment of W lanes (32, or 16 at L = 256) of values |v| < 2^48: for a
+// whole warp two redux sums of the 24-bit limbs (each limb's sum stays below 2^29).
+__device__ __forceinline__ long long seg_sum48(long long v, int W) {
+  if (W == 32) {
+    const unsigned lo = __reduce_add_sync(FULL_MASK, (unsigned)v & 0xFFFFFFu);
+    const int hi = __reduce_add_sync(FULL_MASK, (int)(v >> 24));
+    return (long long)hi * 16777216ll + (long long)lo;
+  }
+  for (int msk = W >> 1; msk > 0; msk >>= 1) v += __shfl_xor_sync(FULL_MASK, v, msk);
+  return v;
+}
+__device__ __forceinline__ unsigned seg_max_u32(unsigned v, int W) {
+  if (W == 32) return __reduce_max_sync(FULL_MASK, v);
+  for (int msk = W >> 1; msk > 0; msk >>= 1) {
+    const unsigned o = __shfl_xor_sync(FULL_MASK, v, msk);
+    v = o > v ? o : v;
+  }
+  return v;
+}
+__device__ __forceinline__ unsigned seg_or_u32(unsigned v, int W) {
+  if (W == 32) return __reduce_or_sync(FULL_MASK, v);
+  for (int msk = W >> 1; msk > 0; msk >>= 1) v |= __shfl_xor_sync(FULL_MASK, v, msk);
+  return v;
+}
+__device__ __forceinline__ unsigned long long seg_max_u64(unsigned long long v, int W) {
+  const unsigned hi = seg_max_u32((unsigned)(v >> 32), W);
+  const unsigned lo = seg_max_u32((unsigned)(v >> 32) == hi ? (unsigned)v : 0u, W);
+  return ((unsigned long long)hi << 32) | lo;
+}
+
+// Per value, for the range tests of the partition: uint64 keeps the max of the high words, above
+// 2^21 when some value exceeds 2^53 (direct copy; exactly 2^21 is decided by a rescan of the
+// partition, cf_any_above_2_53) and below 2^19 iff every value is below 2^51; int64 keeps the OR of
+// hi ^ (hi >> 31), below 2^19 iff every value is in [-2^51, 2^51); 4-byte values always fit.
+template <typename T> __device__ __forceinline__ void value_flag(uint32_t& f, T y) {
+  if (sizeof(T) == 8) {
+    const uint32_t hi = (uint32_t)((uint64_t)y >> 32);
+    if (TypeTraits<T>::is_signed) f |= hi ^ (uint32_t)((int32_t)hi >> 31);
+    else f = hi > f ? hi : f;
+  }
+}
+// Whether a uint64 partition whose largest high word is exactly 2^21 holds a value above 2^53.
+template <typename T> __device__ __noinline__ bool cf_any_above_2_53(const T* __restrict__ xp, int len) {
+  for (int i = 0; i < len; i++)
+    if ((uint64_t)xp[i] > (1ull << 53)) return true;
+  return false;
+}
+// Direct copy for the range flag of a partition (the reference copies a uint64 partition with a
+// value above 2^53 directly).
+template <typename T> __device__ __forceinline__ bool cf_overflows(uint32_t flag, const T* __restrict__ xp, int len) {
+  if (TypeTraits<T>::is_signed || sizeof(T) != 8) return false;
+  return flag > 0x200000u || (flag == 0x200000u && cf_any_above_2_53<T>(xp, len));
+}
+
+// K + y as a double from the bits of y (|y| <= 2^51).
+template <typename T> __device__ __forceinline__ double magic_of(T y) {
+  if (sizeof(T) == 8) {
+    const uint64_t u = (uint64_t)y;
+    return __hiloint2double((int)((uint32_t)(u >> 32) + 0x43380000u), (int)(uint32_t)u);
+  } else if (TypeTraits<T>::is_signed) {
+    return __hiloint2double((int)(0x43380000u + (uint32_t)((int32_t)y >> 31)), (int)y);
+  } else {
+    return __hiloint2double(0x43380000, (int)(uint32_t)y);
+  }
+}
+__device__ __forceinline__ uint32_t low_field(double d) { return (uint32_t)__double2loint(__dadd_rn(d, kMagic)); }
+
+template <typename T, bool FULL>
+__device__ __forceinline__ void cf_sums(const T* __restrict__ xp, int r, int g, int len, HalfSums<T>& hs,
+                                        uint32_t& flag) {
+#pragma unroll
+  for (int m = 0; m < kCfPerThread; m++) {
+    const int i = r + g * m;
+    if (FULL || i < len) {
+      const T y = xp[i];
+      hs.add(y, i);
+      value_flag<T>(flag, y);
+    }
+  }
+}
+
+template <typename T, bool FULL, bool NEG>
+__device__ __forceinline__ unsigned long long cf_resid_sign(const T* __restrict__ xp, int r, int g, int len,
+                                                            double t0, double t1, uint32_t (&fl)[kCfPerThread]) {
+  double dm = 0.0, xd = (double)r;
+  const double gd = (double)g;
+#pragma unroll
+  for (int m = 0; m < kCfPerThread; m++) {
+    const int i = r + g * m;
+    fl[m] = 0u;
+    if (FULL || i < len) {
+      const double yc = magic_of<T>(xp[i]);
+      const double x = __fma_rn(t1, xd, t0);
+      double d;
+      if (!NEG) {
+        d = __dsub_rn(yc, __dadd_rz(__dadd_rn(x, kHalfBias), kMagic));  // (K + y) - (K + pred)
+      } else {
+        d = __dadd_rn(__dsub_rn(yc, 2.0 * kMagic), __dadd_rz(__dsub_rn(kHalfBias, x), kMagic));  // (y - K) + (K - pred)
+      }
+      dm = fmax(dm, fabs(d));
+      fl[m] = low_field(d);
+    }
+    xd = __dadd_rn(xd, gd);
+  }
+  return (unsigned long long)dm;
+}
+
+template <typename T, bool FULL>
+__device__ __forceinline__ bool cf_resid_offset(const T* __restrict__ xp, int r, int g, int len, double t0,
+                                                double t1, double c, long long ci, uint32_t (&fl)[kCfPerThread],
+                                                unsigned long long& mx) {
+  double dm = 0.0, xd = (double)r;
+  const double gd = (double)g;
+  uint32_t range = 0u;
+#pragma unroll
+  for (int m = 0; m < kCfPerThread; m++) {
+    const int i = r + g * m;
+    fl[m] = 0u;
+    if (FULL || i < len) {
+      const uint64_t yo = (uint64_t)xp[i] - (uint64_t)ci;  // y - c
+      const uint32_t yh = (uint32_t)(yo >> 32);
+      range |= yh ^ (uint32_t)((int32_t)yh >> 31);
+      const double yk = __hiloint2double((int)(yh + 0x43380000u), (int)(uint32_t)yo);  // K + (y - c)
+      const double v = __dadd_rn(__dsub_rn(__fma_rn(t1, xd, t0), c), 0.5);          // x - c + 0.5
+      const double d = __dsub_rn(yk, __dadd_rz(v, kMagic));                          // - (K + pred - c)
+      dm = fmax(dm, fabs(d));
+      fl[m] = low_field(d);
+    }
+    xd = __dadd_rn(xd, gd);
+  }
+  mx = (unsigned long long)dm;
+  return range < 0x80000u;  // every |y - c| below 2^51 (y - c in [-2^51, 2^51))
+}
+
+template <typename T>
+__device__ __forceinline__ unsigned long long cf_resid_general(const T* __restrict__ xp, int r, int g, int len,
+                                                               double t0, double t1, uint32_t (&fl)[kCfPerThread]) {
+  unsigned long long mx = 0;
+#pragma unroll
+  for (int m = 0; m < kCfPerThread; m++) {
+    const int i = r + g * m;
+    fl[m] = 0u;
+    if (i < len) {
+      const long long d = calc_delta<T>(xp[i], predict_from<T>(__fma_rn(t1, (double)i, t0)));
+      fl[m] = (uint32_t)d;
+      const unsigned long long ad = (unsigned long long)abs_ref(d);
+      mx = ad > mx ? ad : mx;
+    }
+  }
+  return mx;
+}
+
+// The residual mode of a partition from its line and the range test of its values.
+template <typename T>
+__device__ __forceinline__ int cf_mode(double t0, double t1, int len, bool vsafe, double& c, long long& ci) {
+  const double xa = t0, xb = __fma_rn(t1, (double)(len - 1), t0);  // the ends (fma is monotone in i)
+  const double lo = fmin(xa, xb), hi = fmax(xa, xb);
+  constexpr double kS = 2251799813685248.0;  // 2^51
+  const double hi_ok = sizeof(T) == 4 ? (TypeTraits<T>::is_signed ? 2147483646.0 : 4294967294.0) : kS;
+  const double lo_ok = sizeof(T) == 4 ? -2147483647.0 : -kS;
+  if (vsafe && lo >= -0.25 && hi <= hi_ok) return CF_NONNEG;
+  if (TypeTraits<T>::is_signed && vsafe && hi <= 0.25 && lo >= lo_ok) return CF_NONPOS;
+  if (sizeof(T) == 8 && lo >= 1125899906842624.0 && hi <= 4611686018427387904.0) {  // [2^50, 2^62]
+    c = trunc(t0);
+    if (fabs(__dsub_rn(xb, c)) < 562949953421312.0) {  // 2^49
+      ci = __double2ll_rz(c);
+      return CF_OFFSET;
+    }
+  }
+  return CF_GENERAL;
+}
+
+// Packs the 32 fields of one group (width B, 1..31, at fg[f * kFtStride]) into B words at staged
+// word o onward (staged word k at stg[k + k / 32]).
+template <int B>
+__device__ __forceinline__ void cf_pack_group(const uint32_t* __restrict__ fg, uint32_t* __restrict__ stg, int o) {
+  constexpr uint32_t kMask = (1u << B) - 1u;
+  uint32_t w = 0u;
+#pragma unroll
+  for (int f = 0; f < 32; f++) {
+    const uint32_t v = fg[f * kFtStride] & kMask;
+    const int sh = (f * B) & 31;
+    w |= v << sh;
+    if (sh + B >= 32) {
+      const int k = o + ((f * B) >> 5);
+      stg[k + (k >> 5)] = w;
+      w = sh + B > 32 ? v >> (32 - sh) : 0u;
+    }
+  }
+}
+
+__device__ __noinline__ void cf_pack_dispatch(int b, const uint32_t* __restrict__ fg, uint32_t* __restrict__ stg,
+                                              int o) {
+  switch (b) {
+#define GLC_CF_PACK(B) \
+  case B: cf_pack_group<B>(fg, stg, o); break;
+    GLC_CF_PACK(1) GLC_CF_PACK(2) GLC_CF_PACK(3) GLC_CF_PACK(4) GLC_CF_PACK(5) GLC_CF_PACK(6) GLC_CF_PACK(7)
+    GLC_CF_PACK(8) GLC_CF_PACK(9) GLC_CF_PACK(10) GLC_CF_PACK(11) GLC_CF_PACK(12) GLC_CF_PACK(13) GLC_CF_PACK(14)
+    GLC_CF_PACK(15) GLC_CF_PACK(16) GLC_CF_PACK(17) GLC_CF_PACK(18) GLC_CF_PACK(19) GLC_CF_PACK(20)
+    GLC_CF_PACK(21) GLC_CF_PACK(22) GLC_CF_PACK(23) GLC_CF_PACK(24) GLC_CF_PACK(25) GLC_CF_PACK(26)
+    GLC_CF_PACK(27) GLC_CF_PACK(28) GLC_CF_PACK(29) GLC_CF_PACK(30) GLC_CF_PACK(31)
+#undef GLC_CF_PACK
+    default: break;  // width 0: no words
+  }
+}
+
+// Word w of a partition of width B (1..64) whose exact residuals are rp[0, len): the tile-relative
+// bits [32 w, 32 w + 32) of its fields, from the field holding bit 32 w and the ceil(31 / B) after
+// it at most (fields past len are zero).  One thread per word, B known at compile time.
+template <int B>
+__device__ __forceinline__ void cf_words(const long long* rp, int len, int nwp, uint32_t* __restrict__ out, int tid) {
+  constexpr int kMore = (31 + B - 1) / B;
+  for (int w = tid; w < nwp; w += kCfThreads) {
+    int j = (32 * w) / B;
+    const int s = 32 * w - j * B;
+    if (B <= 32) {
+      constexpr uint32_t kMask = B >= 32 ? 0xffffffffu : ((1u << (B & 31)) - 1u);
+      const uint32_t* r32 = reinterpret_cast<const uint32_t*>(rp);  // low half of residual j at 2 j
+      uint32_t v = (r32[2 * j] & kMask) >> s;
+      int have = B - s;
+#pragma unroll
+      for (int e = 0; e < kMore; e++) {
+        if (have < 32) {
+          ++j;
+          if (j < len) v |= (r32[2 * j] & kMask) << have;
+          have += B;
+        }
+      }
+      out[w] = v;
+    } else {
+      constexpr uint64_t kMask = B >= 64 ? ~0ull : ((1ull << (B & 63)) - 1ull);
+      uint64_t v = ((uint64_t)rp[j] & kMask) >> s;
+      if (B - s < 32 && j + 1 < len) v |= ((uint64_t)rp[j + 1] & kMask) << (B - s);
+      out[w] = (uint32_t)v;
+    }
+  }
+}
+
+__device__ __noinline__ void cf_words_dispatch(int b, const long long* rp, int len, uint32_t* __restrict__ out,
+                                               int tid) {
+  const int nwp = (int)(((long long)len * b + 31) >> 5);
+  switch (b) {
+#define GLC_CF_WORDS(B) \
+  case B: cf_words<B>(rp, len, nwp, out, tid); break;
+    GLC_CF_WORDS(1) GLC_CF_WORDS(2) GLC_CF_WORDS(3) GLC_CF_WORDS(4) GLC_CF_WORDS(5) GLC_CF_WORDS(6)
+    GLC_CF_WORDS(7) GLC_CF_WORDS(8) GLC_CF_WORDS(9) GLC_CF_WORDS(10) GLC_CF_WORDS(11) GLC_CF_WORDS(12)
+    GLC_CF_WORDS(13) GLC_CF_WORDS(14) GLC_CF_WORDS(15) GLC_CF_WORDS(16) GLC_CF_WORDS(17) GLC_CF_WORDS(18)
+    GLC_CF_WORDS(19) GLC_CF_WORDS(20) GLC_CF_WORDS(21) GLC_CF_WORDS(22) GLC_CF_WORDS(23) GLC_CF_WORDS(24)
+    GLC_CF_WORDS(25) GLC_CF_WORDS(26) GLC_CF_WORDS(27) GLC_CF_WORDS(28) GLC_CF_WORDS(29) GLC_CF_WORDS(30)
+    GLC_CF_WORDS(31) GLC_CF_WORDS(32) GLC_CF_WORDS(33) GLC_CF_WORDS(34) GLC_CF_WORDS(35) GLC_CF_WORDS(36)
+    GLC_CF_WORDS(37) GLC_CF_WORDS(38) GLC_CF_WORDS(39) GLC_CF_WORDS(40) GLC_CF_WORDS(41) GLC_CF_WORDS(42)
+    GLC_CF_WORDS(43) GLC_CF_WORDS(44) GLC_CF_WORDS(45) GLC_CF_WORDS(46) GLC_CF_WORDS(47) GLC_CF_WORDS(48)
+    GLC_CF_WORDS(49) GLC_CF_WORDS(50) GLC_CF_WORDS(51) GLC_CF_WORDS(52) GLC_CF_WORDS(53) GLC_CF_WORDS(54)
+    GLC_CF_WORDS(55) GLC_CF_WORDS(56) GLC_CF_WORDS(57) GLC_CF_WORDS(58) GLC_CF_WORDS(59) GLC_CF_WORDS(60)
+    GLC_CF_WORDS(61) GLC_CF_WORDS(62) GLC_CF_WORDS(63) GLC_CF_WORDS(64)
+#undef GLC_CF_WORDS
+    default: break;  // width 0: no words
+  }
+}
+
+// The exact residuals of one thread's values (value i of its partition at xp[i], written to rp[i];
+// for 8-byte types rp is xp, each value read before its residual replaces it).  The FP64 modes give
+// y - pred as an exact integer-valued double, converted once; the others use the integer formula.
+template <typename T>
+__device__ __forceinline__ void cf_store_resid(const T* xp, long long* rp, int r, int g, int len, int mode, double t0,
+                                               double t1) {
+  for (int m = 0; m < kCfPerThread; m++) {
+    const int i = r + g * m;
+    if (i >= len) break;
+    const T y = xp[i];
+    long long d;
+    if (mode == CF_DIRECT) {
+      d = (long long)(uint64_t)y;  // the field is the value itself (zero-extended)
+    } else if (mode == CF_NONNEG) {
+      const double x = __fma_rn(t1, (double)i, t0);
+      d = __double2ll_rn(__dsub_rn(magic_of<T>(y), __dadd_rz(__dadd_rn(x, kHalfBias), kMagic)));
+    } else if (TypeTraits<T>::is_signed && mode == CF_NONPOS) {
+      const double x = __fma_rn(t1, (double)i, t0);
+      d = __double2ll_rn(
+          __dadd_rn(__dsub_rn(magic_of<T>(y), 2.0 * kMagic), __dadd_rz(__dsub_rn(kHalfBias, x), kMagic)));
+    } else {
+      d = calc_delta<T>(y, predict_from<T>(__fma_rn(t1, (double)i, t0)));
+    }
+    rp[i] = d;
+  }
+}
+
+// The compress kernel's CTA: eight compute warps, the producer warp and the solver warp.  Per step
+// k the compute warps take the sums of tile k + 1 and the residuals, widths and words of tile k,
+// while the solver warp fits the lines of tile k + 1 (one lane per partition) and the producer
+// stages tile k + 2: the fit's long dependency chain (128-bit arithmetic, two divisions) runs beside
+// the compute warps instead of between two of their barriers.  Every wait is bounded.
+constexpr int kCfFixStages = 3;
+constexpr int kCfFixCTA = kCfThreads + 64;
+
+template <typename T> __host__ __device__ constexpr int cf_fix_smem_bytes() {
+  return kCfFixStages * cf_stage_bytes<T>() + (sizeof(T) == 4 ? kCfWorkBytes : 0);
+}
+
+// A tile as a step sees it.
+struct CfGeom {
+  const CfColumn* col;
+  int64_t t, e0;
+  int L, g, W, cnt, np, segs_per_part;
+  int lg_L, lg_g, lg_W;  // L, g and W are powers of two: divisions are shifts
+};
+__device__ __forceinline__ CfGeom cf_geom(const FixedCompressArgs& a, int64_t item, int c) {
+  CfGeom q;
+  q.col = a.cols ? a.cols + c : &a.single;
+  q.t = item - q.col->item_base;
+  q.e0 = q.t * kDecodeTile;
+  const int64_t left = q.col->n - q.e0;
+  q.cnt = (int)(left < kDecodeTile ? left : kDecodeTile);
+  q.L = q.col->L;
+  q.lg_L = 31 - __clz(q.L);
+  q.g = q.L >> 4;
+  q.lg_g = q.lg_L - 4;
+  q.W = q.g < 32 ? q.g : 32;
+  q.lg_W = q.lg_g < 5 ? q.lg_g : 5;
+  q.np = (q.cnt + q.L - 1) >> q.lg_L;
+  q.segs_per_part = q.g >> q.lg_W;
+  return q;
+}
+
+// Two CTAs per SM (96 registers; three stages of 33 KB for 8-byte types).
+template <typename T> __global__ void __launch_bounds__(kCfFixCTA, 2)
+fixed_compress_kernel(const __grid_constant__ FixedCompressArgs a) {
+  constexpr int S = kCfFixStages;
   extern __shared__ __align__(128) uint8_t smem[];
-  __shared__ __align__(8) uint64_t full[kCfStages], empty[kCfStages];
-  __shared__ int64_t s_stile[kCfStages];   // work item staged in each stage (-1: the end)
-  __shared__ int s_shead[kCfStages];
-  __shared__ int s_scol[kCfStages];
-  typedef typename HalfSums<T>::Acc Acc;
-  __shared__ Acc s_acc[kCfMaxSegs][4];
-  __shared__ int s_ovf[kCfMaxSegs];
+  __shared__ __align__(8) uint64_t full[S], empty[S], sums[S], lines[S];
+  __shared__ int64_t s_stile[S];   // work item staged in each stage (-1: the end)
+  __shared__ int s_shead[S];
+  __shared__ int s_scol[S];
+  __shared__ long long s_acc[S][kCfMaxSegs][4];   // per stage: the segments' exact partial sums
+  __shared__ uint32_t s_flag[S][kCfMaxSegs];      // and range flags
+  __shared__ double s_t0[S][kCfMaxParts], s_t1[S][kCfMaxParts], s_c[S][kCfMaxParts];  // the solver's lines
+  __shared__ long long s_ci[S][kCfMaxParts];
+  __shared__ int s_mode[S][kCfMaxParts];
   __shared__ unsigned long long s_mx[kCfMaxSegs];
-  __shared__ double s_t0[kCfMaxParts], s_t1[kCfMaxParts];
-  __shared__ int s_direct[kCfMaxParts], s_safe[kCfMaxParts], s_len[kCfMaxParts], s_b[kCfMaxParts];
-  __shared__ uint32_t s_mb[kCfMaxParts];
-  __shared__ long long s_err[kCfMaxParts];
+  __shared__ int s_b[kCfMaxParts];
   __shared__ int s_bl[kCfMaxParts + 1];
-  __shared__ int s_ok;
+  __shared__ int s_ok, s_fast;
 
   if (threadIdx.x == 0) {
-    for (int st = 0; st < kCfStages; st++) {
+    for (int st = 0; st < S; st++) {
       mbar_init(&full[st], 1);
       mbar_init(&empty[st], 1);
+      mbar_init(&sums[st], kCfThreads / 32);
+      mbar_init(&lines[st], 1);
     }
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   __syncthreads();
 
-  if (threadIdx.x >= kCfThreads) {  // ---- producer ----
-    if (threadIdx.x == kCfThreads) cf_produce<T>(a, smem, full, empty, s_stile, s_shead, s_scol);
+  const int tid = threadIdx.x, lane = tid & 31;
+  if (tid >= kCfThreads + 32) {  // ---- solver warp ----
+    for (int k = 0;; k++) {
+      const int st = k % S;
+      int ok = 1;
+      if (lane == 0) {
+        ok = mbar_wait_sleep(&sums[st], (uint32_t)(k / S) & 1u);
+        if (!ok) atomicExch(a.status, (unsigned long long)DEVERR_TIMEOUT);
+      }
+      if (!__shfl_sync(FULL_MASK, ok, 0)) return;
+      const int64_t item = s_stile[st];
+      if (item < 0) return;
+      const CfGeom q = cf_geom(a, item, s_scol[st]);
+      if (lane < q.np) {  // lane p fits partition p (fit.cu's arithmetic) and picks its residual mode
+        const int p = lane;
+        long long a0 = 0, a1 = 0, a2 = 0, a3 = 0;
+        uint32_t flag = 0;
+        for (int s = p * q.segs_per_part; s < (p + 1) * q.segs_per_part; s++) {
+          a0 += s_acc[st][s][0];
+          a1 += s_acc[st][s][1];
+          a2 += s_acc[st][s][2];
+          a3 += s_acc[st][s][3];
+          flag = TypeTraits<T>::is_signed ? (flag | s_flag[st][s]) : (s_flag[st][s] > flag ? s_flag[st][s] : flag);
+        }
+        const int len = (q.cnt - p * q.L) < q.L ? (q.cnt - p * q.L) : q.L;
+        const T* xp = reinterpret_cast<const T*>(smem + (size_t)st * cf_stage_bytes<T>() + s_shead[st]) + p * q.L;
+        const bool ovf = cf_overflows<T>(flag, xp, len);  // a value above 2^53: direct copy
+        const bool vsafe = sizeof(T) == 4 || flag < 0x80000u;
+        double t0 = 0.0, t1 = 0.0, c = 0.0;
+        long long ci = 0;
+        int mode = CF_DIRECT;
+        if (!ovf) {
+          solve_line(len, (i128)a0 + (i128)a1 * ((i128)1 << 32), (i128)a2 + (i128)a3 * ((i128)1 << 32), t0, t1);
+          mode = cf_mode<T>(t0, t1, len, vsafe, c, ci);
+        }
+        s_t0[st][p] = t0;
+        s_t1[st][p] = t1;
+        s_c[st][p] = c;
+        s_ci[st][p] = ci;
+        s_mode[st][p] = mode;
+      }
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&lines[st]);
+    }
+  }
+  if (tid >= kCfThreads) {  // ---- producer ----
+    if (tid == kCfThreads) cf_produce<T, S>(a, smem, full, empty, s_stile, s_shead, s_scol);
     return;
   }
 
   // ---- compute warps ----
-  const int tid = threadIdx.x;
-  for (int k = 0;; k++) {
-    const int st = k % kCfStages;
-    const uint32_t par = (uint32_t)(k / kCfStages) & 1u;
+  // the exact sums of the tile in stage st into s_acc[st] / s_flag[st], then each warp arrives on
+  // sums[st] (an end marker is passed on unsummed, so the solver sees the end too)
+  auto stage_sums = [&](int st) {
+    const int64_t item = s_stile[st];
+    if (item >= 0) {
+      const CfGeom q = cf_geom(a, item, s_scol[st]);
+      const int p_me = tid >> q.lg_g, r_me = tid & (q.g - 1);
+      const int my_len = p_me < q.np ? ((q.cnt - p_me * q.L) < q.L ? (q.cnt - p_me * q.L) : q.L) : 0;
+      const T* xp = reinterpret_cast<const T*>(smem + (size_t)st * cf_stage_bytes<T>() + s_shead[st]) + p_me * q.L;
+      HalfSums<T> hs;
+      uint32_t flag = 0;
+      if (my_len == q.L) cf_sums<T, true>(xp, r_me, q.g, q.L, hs, flag);
+      else if (my_len > 0) cf_sums<T, false>(xp, r_me, q.g, my_len, hs, flag);
+      // every partial is below 2^48 in magnitude (16 values, i < 2^12, 32-bit halves)
+      const long long c0 = seg_sum48((long long)hs.s_lo, q.W);
+      const long long c1 = sizeof(T) == 8 ? seg_sum48((long long)hs.s_hi, q.W) : 0;
+      const long long c2 = seg_sum48((long long)hs.x_lo, q.W);
+      const long long c3 = sizeof(T) == 8 ? seg_sum48((long long)hs.x_hi, q.W) : 0;
+      flag = TypeTraits<T>::is_signed ? seg_or_u32(flag, q.W) : seg_max_u32(flag, q.W);
+      if ((tid & (q.W - 1)) == 0) {
+        const int seg = tid >> q.lg_W;
+        s_acc[st][seg][0] = c0;
+        s_acc[st][seg][1] = c1;
+        s_acc[st][seg][2] = c2;
+        s_acc[st][seg][3] = c3;
+        s_flag[st][seg] = flag;
+      }
+    }
+    __syncwarp();
+    if (lane == 0) mbar_arrive(&sums[st]);
+  };
+  // tid 0 waits for a phase; every compute thread learns the outcome after the barrier
+  auto wait_all = [&](uint64_t* bar, uint32_t par) {
     if (tid == 0) {
-      s_ok = mbar_wait_bounded(&full[st], par);
+      s_ok = mbar_wait_sleep(bar, par);
+      if (!s_ok) atomicExch(a.status, (unsigned long long)DEVERR_TIMEOUT);
+    }
+  };
+
+  if (tid == 0) {
+    s_ok = mbar_wait_sleep(&full[0], 0);
+    if (!s_ok) {
+      atomicExch(a.status, (unsigned long long)DEVERR_TIMEOUT);
+      mbar_wait_bounded(&full[0], 0);  // a copy in flight lands before the CTA exits
+    }
+  }
+  cf_sync();
+  if (!s_ok) return;
+  mbar_try_wait(&full[0], 0);  // the phase is complete: orders this thread's reads after the copy
+  if (s_stile[0] < 0) return;
+  stage_sums(0);
+
+  for (int k = 0;; k++) {
+    const int st = k % S, st1 = (k + 1) % S;
+    const uint32_t par = (uint32_t)(k / S) & 1u, par1 = (uint32_t)((k + 1) / S) & 1u;
+    // the next tile's values and this tile's lines
+    if (tid == 0) {
+      s_ok = mbar_wait_sleep(&full[st1], par1);
       if (!s_ok) {
         atomicExch(a.status, (unsigned long long)DEVERR_TIMEOUT);
-        mbar_wait_bounded(&full[st], par);  // a copy in flight lands before the CTA exits
+        mbar_wait_bounded(&full[st1], par1);  // a copy in flight lands before the CTA exits
+      } else {
+        wait_all(&lines[st], par);
       }
     }
     cf_sync();
     if (!s_ok) return;
-    mbar_try_wait(&full[st], par);  // the phase is complete: orders this thread's reads after the copy
+    mbar_try_wait(&full[st1], par1);
+    mbar_try_wait(&lines[st], par);
+    const int64_t item1 = s_stile[st1];
+    stage_sums(st1);
+
     const int64_t item = s_stile[st];
-    if (item < 0) return;
-    const CfColumn& col = a.cols ? a.cols[s_scol[st]] : a.single;
-    const int64_t t = item - col.item_base;  // the tile within its column
-    const int L = col.L;
-    const int g = L >> 4;                     // threads per partition (16 values each)
-    const int W = g < 32 ? g : 32;            // lanes of one reduction segment
-    const int seg = tid / W;                  // reduction segment of this thread
-    const int segs_per_part = g / W;
-    const int p_me = tid / g;                 // this thread's partition within the tile
-    const int r_me = tid - p_me * g;          // and its first value there
+    const CfGeom q = cf_geom(a, item, s_scol[st]);
+    const CfColumn& col = *q.col;
+    const int L = q.L, g = q.g, W = q.W, np = q.np, cnt = q.cnt;
+    const int64_t t = q.t, e0 = q.e0;
+    const int seg = tid >> q.lg_W, segs_per_part = q.segs_per_part;
+    const int p_me = tid >> q.lg_g, r_me = tid & (g - 1);
     uint8_t* stage = smem + (size_t)st * cf_stage_bytes<T>();
     T* x = reinterpret_cast<T*>(stage + s_shead[st]);
-    // residuals: over the values for 8-byte types, in their own array for 4-byte types
-    int64_t* res = sizeof(T) == 8 ? reinterpret_cast<int64_t*>(x)
-                                  : reinterpret_cast<int64_t*>(smem + (size_t)kCfStages * cf_stage_bytes<T>());
-    const int64_t e0 = t * kDecodeTile;
-    const int cnt = (int)((col.n - e0) < kDecodeTile ? (col.n - e0) : kDecodeTile);
-    const int np = (cnt + L - 1) / L;  // partitions in this tile (the last may be short)
+    // the fields and staged words of the fast packing: over the stage for 8-byte types (its values
+    // are dead by then), in the work area for 4-byte types
+    uint8_t* work = sizeof(T) == 8 ? stage : smem + (size_t)S * cf_stage_bytes<T>();
     const int my_len = p_me < np ? ((cnt - p_me * L) < L ? (cnt - p_me * L) : L) : 0;
     const T* xp = x + p_me * L;
 
-    // ---- A: exact sums of y and i * y (i = index within the partition), overflow flag ----
+    // ---- B: residual of every value: its low 32 bits kept, max |residual| per partition ----
+    uint32_t fl[kCfPerThread];
     {
-      HalfSums<T> hs;
-      int ovf = 0;
-#pragma unroll 4
-      for (int m = 0; m < kCfPerThread; m++) {
-        const int i = r_me + g * m;
-        if (i < my_len) {
-          const T y = xp[i];
-          ovf |= overflows_double<T>(y) ? 1 : 0;
-          hs.add(y, i);
-        }
-      }
-      Acc c0 = hs.s_lo, c1 = hs.s_hi, c2 = hs.x_lo, c3 = hs.x_hi;
-      for (int msk = W >> 1; msk > 0; msk >>= 1) {
-        c0 += __shfl_xor_sync(FULL_MASK, c0, msk);
-        if (sizeof(T) == 8) c1 += __shfl_xor_sync(FULL_MASK, c1, msk);
-        c2 += __shfl_xor_sync(FULL_MASK, c2, msk);
-        if (sizeof(T) == 8) c3 += __shfl_xor_sync(FULL_MASK, c3, msk);
-        ovf |= __shfl_xor_sync(FULL_MASK, ovf, msk);
-      }
-      if ((tid & (W - 1)) == 0) {
-        s_acc[seg][0] = c0;
-        s_acc[seg][1] = c1;
-        s_acc[seg][2] = c2;
-        s_acc[seg][3] = c3;
-        s_ovf[seg] = ovf;
-      }
-    }
-    cf_sync();
-    if (tid < np) {  // one thread per partition: the line (fit.cu's arithmetic)
-      const int p = tid;
-      HalfSums<T> hs;
-      int ovf = 0;
-      for (int q = p * segs_per_part; q < (p + 1) * segs_per_part; q++) {
-        hs.s_lo += s_acc[q][0];
-        hs.s_hi += s_acc[q][1];
-        hs.x_lo += s_acc[q][2];
-        hs.x_hi += s_acc[q][3];
-        ovf |= s_ovf[q];
-      }
-      const int len = (cnt - p * L) < L ? (cnt - p * L) : L;
-      double t0 = 0.0, t1 = 0.0;
-      if (!ovf) solve_line(len, hs.sy(), hs.sxy(), t0, t1);
-      s_t0[p] = t0;
-      s_t1[p] = t1;
-      s_direct[p] = ovf;
-      s_len[p] = len;
-      s_safe[p] = !ovf && line_fp64_safe<T>(t0, t1, 0, len - 1);
-    }
-    cf_sync();
-
-    // ---- B: residual of every value, max |residual| per partition ----
-    {
-      const int p = p_me;
       unsigned long long mx = 0;
+#pragma unroll
+      for (int m = 0; m < kCfPerThread; m++) fl[m] = 0u;
       if (my_len > 0) {
-        int64_t* rp = res + p_me * L;
-        if (s_direct[p]) {  // direct copy: the field is the value itself (zero-extended)
-          for (int m = 0; m < kCfPerThread; m++) {
-            const int i = r_me + g * m;
-            if (i < my_len) rp[i] = (int64_t)(uint64_t)xp[i];
-          }
-        } else {
-          const double t0 = s_t0[p], t1 = s_t1[p];
-          bool exact_fp64 = s_safe[p] != 0;
-          if (exact_fp64) {
-            // |y| < 2^51 and the predictions inside pred_fp64_safe's bounds: the prediction is
-            // predict_small (no conversion instruction), y - pred is below 2^52 and is
-            // calculateDelta; the index advances as an exact double
-            long long dmax = 0, dmin = 0;
-            double xd = (double)r_me;
-            const double xstep = (double)g;
-#pragma unroll 4
-            for (int m = 0; m < kCfPerThread; m++, xd += xstep) {
-              const int i = r_me + g * m;
-              if (i < my_len) {
-                const T y = xp[i];
-                exact_fp64 &= value_fp64_safe<T>(y);
-                const long long d = (long long)y - predict_small(__fma_rn(t1, xd, t0));
-                rp[i] = d;
-                dmax = d > dmax ? d : dmax;
-                dmin = d < dmin ? d : dmin;
-              }
-            }
-            mx = (unsigned long long)(dmax > -dmin ? dmax : -dmin);
-          }
-          if (!exact_fp64) {  // the general residual (saturating for uint64), and its exact magnitude
-            mx = 0;
-            for (int m = 0; m < kCfPerThread; m++) {
-              const int i = r_me + g * m;
-              if (i < my_len) {
-                const T y = xp[i];
-                const long long d = calc_delta<T>(y, predict_from<T>(__fma_rn(t1, (double)i, t0)));
-                rp[i] = d;
-                const unsigned long long ad = (unsigned long long)abs_ref(d);
-                mx = ad > mx ? ad : mx;
-              }
-            }
-          }
+        const int mode = s_mode[st][p_me];
+        const double t0 = s_t0[st][p_me], t1 = s_t1[st][p_me];
+        bool general = mode == CF_GENERAL;
+        if (mode == CF_NONNEG) {
+          mx = my_len == L ? cf_resid_sign<T, true, false>(xp, r_me, g, L, t0, t1, fl)
+                           : cf_resid_sign<T, false, false>(xp, r_me, g, my_len, t0, t1, fl);
+        } else if (TypeTraits<T>::is_signed && mode == CF_NONPOS) {
+          mx = my_len == L ? cf_resid_sign<T, true, true>(xp, r_me, g, L, t0, t1, fl)
+                           : cf_resid_sign<T, false, true>(xp, r_me, g, my_len, t0, t1, fl);
+        } else if (sizeof(T) == 8 && mode == CF_OFFSET) {
+          const double c = s_c[st][p_me];
+          const long long ci = s_ci[st][p_me];
+          general = !(my_len == L ? cf_resid_offset<T, true>(xp, r_me, g, L, t0, t1, c, ci, fl, mx)
+                                  : cf_resid_offset<T, false>(xp, r_me, g, my_len, t0, t1, c, ci, fl, mx));
         }
+        if (general) mx = cf_resid_general<T>(xp, r_me, g, my_len, t0, t1, fl);
       }
-      for (int msk = W >> 1; msk > 0; msk >>= 1) {
-        const unsigned long long o = __shfl_xor_sync(FULL_MASK, mx, msk);
-        mx = o > mx ? o : mx;
-      }
+      mx = seg_max_u64(mx, W);
       if ((tid & (W - 1)) == 0) s_mx[seg] = mx;
     }
     cf_sync();
-    if (tid < np) {
-      const int p = tid;
-      unsigned long long mx = 0;
-      for (int q = p * segs_per_part; q < (p + 1) * segs_per_part; q++) mx = s_mx[q] > mx ? s_mx[q] : mx;
-      const int b = s_direct[p] ? (int)sizeof(T) * 8 : bits_for((long long)mx);
-      s_err[p] = s_direct[p] ? 0 : (long long)mx;
-      s_b[p] = b;
-      s_mb[p] = b > 1 ? 0xffffffffu / (uint32_t)b + 1u : 0u;
-    }
-    cf_sync();
-    if (tid == 0) {  // tile-relative bit ranges, the tile's bit count and decode-table entry
-      int acc = 0, bmax = 0;
-      for (int p = 0; p < np; p++) {
-        s_bl[p] = acc;
-        acc += s_len[p] * s_b[p];
-        bmax = s_b[p] > bmax ? s_b[p] : bmax;
+    if (tid < 32) {  // widths, tile-relative bit ranges (a warp scan), descriptors, the tile's bits
+      const int p = lane;
+      int b = 0, nb = 0;
+      unsigned long long err = 0;
+      if (p < np) {
+        unsigned long long m = 0;
+        for (int s = p * segs_per_part; s < (p + 1) * segs_per_part; s++) m = s_mx[s] > m ? s_mx[s] : m;
+        const bool direct = s_mode[st][p] == CF_DIRECT;
+        b = direct ? (int)sizeof(T) * 8 : bits_for((long long)m);
+        err = direct ? 0 : m;
+        nb = ((cnt - p * L) < L ? (cnt - p * L) : L) * b;
       }
-      s_bl[np] = acc;
-      a.tile_bits[item] = acc;
-      TileInfo ti;
-      ti.bit_lo = 0;  // the tile's first bit is added by fixed_place_kernel
-      ti.p_first = (int32_t)(t * col.parts_per_tile);
-      ti.p_last = (int32_t)(t * col.parts_per_tile + np - 1);
-      col.tiles[t] = ti;
-      if (bmax > 0) atomicMax(col.stats + 1, (unsigned long long)bmax);
+      int inc = nb;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int v = __shfl_up_sync(FULL_MASK, inc, o);
+        if (lane >= o) inc += v;
+      }
+      const int bl = inc - nb;
+      const int bmax = (int)__reduce_max_sync(FULL_MASK, (unsigned)b);
+      const int total = __shfl_sync(FULL_MASK, inc, 31);
+      if (p < np) {
+        s_bl[p] = bl;
+        s_b[p] = b;
+        // the descriptor with the tile-relative offset and the max error; fixed_place_kernel
+        // completes the offset and writes the other metadata arrays from the descriptor
+        const int64_t gp = t * col.parts_per_tile + p;
+        PartDesc d;
+        d.theta0 = s_t0[st][p];
+        d.theta1 = s_t1[st][p];
+        d.bit_off = bl;
+        d.start = (int32_t)(e0 + (int64_t)p * L);
+        d.bits_type = (b & 0xff) | ((s_mode[st][p] == CF_DIRECT ? MODEL_DIRECT_COPY : MODEL_LINEAR) << 8);
+        col.desc[gp] = d;
+        col.err[gp] = (long long)err;
+      }
+      if (lane == 0) {
+        s_bl[np] = total;
+        s_fast = bmax <= 31;
+        a.tile_bits[item] = total;
+        if (bmax > 0) atomicMax(col.stats + 1, (unsigned long long)bmax);
+      }
     }
     cf_sync();
-    if (tid < np) {  // the partitions' metadata and descriptors (offsets relative to the tile)
-      const int p = tid;
-      const int64_t gp = t * col.parts_per_tile + p;
-      const int32_t start = (int32_t)(e0 + (int64_t)p * L);
-      const int type = s_direct[p] ? MODEL_DIRECT_COPY : MODEL_LINEAR;
-      col.starts[gp] = start;
-      col.ends[gp] = start + s_len[p];
-      col.types[gp] = type;
-      col.params[4 * gp] = s_t0[p];
-      col.params[4 * gp + 1] = s_t1[p];
-      col.params[4 * gp + 2] = 0.0;
-      col.params[4 * gp + 3] = 0.0;
-      col.bits[gp] = s_b[p];
-      col.offs[gp] = s_bl[p];
-      col.err[gp] = s_err[p];
-      PartDesc d;
-      d.theta0 = s_t0[p];
-      d.theta1 = s_t1[p];
-      d.bit_off = s_bl[p];
-      d.start = start;
-      d.bits_type = (s_b[p] & 0xff) | (type << 8);
-      col.desc[gp] = d;
-    }
 
-    // ---- C: the tile's words into its slot; word w holds tile bits [32 w, 32 w + 32) ----
-    {
-      const int tb = s_bl[np];
-      const int nw = (tb + 31) >> 5;
-      const uint32_t* f32 = reinterpret_cast<const uint32_t*>(res);  // low half of residual j at 2 j
-      uint32_t* out = a.slots + item * a.slot_words;
-      int qi = 0;
-      for (int w = tid; w < nw; w += kCfThreads) {
-        const int wb = 32 * w;
-        int pos = wb;
-        const int wend = wb + 32 < tb ? wb + 32 : tb;
-        uint32_t word = 0u;
-        while (pos < wend) {
-          while (s_bl[qi + 1] <= pos) qi++;  // the partition holding bit pos (empty ranges skipped)
-          const int b = s_b[qi], bl = s_bl[qi];
-          const int qend = s_bl[qi + 1] < wend ? s_bl[qi + 1] : wend;
-          const int jj = b > 1 ? (int)__umulhi((uint32_t)(pos - bl), s_mb[qi]) : pos - bl;
-          int fb = bl + jj * b;  // start of the field holding bit pos
-          int j = qi * L + jj;
-          if (b <= 32) {
-            const uint32_t mask = b == 32 ? 0xffffffffu : ((1u << b) - 1u);
-            for (; fb < qend; fb += b, j++) {
-              const uint32_t f = f32[2 * j] & mask;
-              const int sh = fb - wb;
-              word |= sh >= 0 ? (f << sh) : (f >> -sh);
-            }
-          } else {
-            for (; fb < qend; fb += b, j++) {
-              const uint64_t f = low_bits((uint64_t)res[j], b);
-              const int sh = fb - wb;
-              word |= sh >= 0 ? (uint32_t)(f << sh) : (uint32_t)(f >> -sh);
-            }
-          }
-          pos = qend;
+    uint32_t* out = a.slots + item * a.slot_words;
+    if (s_fast) {
+      // ---- C (every width <= 31): fields transposed, one thread packs each 32-value group into
+      // its `width` words (every partition starts on a word: L is a multiple of 32), staged, then
+      // copied to the slot with coalesced stores ----
+      uint32_t* fT = reinterpret_cast<uint32_t*>(work);
+      uint32_t* stg = fT + kFtWords;
+      if (g >= 32) {  // g a multiple of 32: position j = p_me L + r_me + g m has j % 32 = lane
+        uint32_t* fp = fT + lane * kFtStride + ((p_me * L + r_me) >> 5);
+        const int step = g >> 5;
+#pragma unroll
+        for (int m = 0; m < kCfPerThread; m++) fp[m * step] = fl[m];
+      } else {
+#pragma unroll
+        for (int m = 0; m < kCfPerThread; m++) {
+          const int j = p_me * L + r_me + g * m;  // position in the tile (the threads cover all 4096)
+          fT[(j & 31) * kFtStride + (j >> 5)] = fl[m];
         }
-        out[w] = word;
       }
+      cf_sync();
+      if (tid < ((cnt + 31) >> 5)) {
+        const int G = tid, p = G >> (q.lg_L - 5);  // L / 32 groups per partition
+        cf_pack_dispatch(s_b[p], fT + G, stg, (s_bl[p] >> 5) + (G - (p << (q.lg_L - 5))) * s_b[p]);
+      }
+      cf_sync();
+      const int nw = (s_bl[np] + 31) >> 5;
+      for (int w = tid; w < nw; w += kCfThreads) out[w] = stg[w + (w >> 5)];
+    } else {
+      // ---- C (a width above 31): the exact 64-bit residuals over the values (8-byte types) or in
+      // the work area, then per partition one thread per word of the slot ----
+      long long* res = sizeof(T) == 8 ? reinterpret_cast<long long*>(x) : reinterpret_cast<long long*>(work);
+      if (my_len > 0)
+        cf_store_resid<T>(xp, res + p_me * L, r_me, g, my_len, s_mode[st][p_me], s_t0[st][p_me], s_t1[st][p_me]);
+      cf_sync();
+      for (int p = 0; p < np; p++)
+        cf_words_dispatch(s_b[p], res + p * L, (cnt - p * L) < L ? (cnt - p * L) : L, out + (s_bl[p] >> 5), tid);
     }
-    cf_sync();  // every compute thread is done with stage st and the residual array
+    cf_sync();  // every compute thread is done with stage st and the work area
     if (tid == 0) mbar_arrive(&empty[st]);
+    if (item1 < 0) return;
   }
 }
 
 // The partition-length choice of the batched compress, one tile per step (the same staging as
 // fixed_compress_kernel): the tile's four 1024-value quarters, its two halves and the whole tile
 // are fitted from exact per-quarter sums (the index offsets of a half or the tile added exactly),
-// every value's residual is measured against the three lines that cover it, and the bits of each
-// candidate length are added into the column's choice_bits[0..2] (1024, 2048, 4096).  The widths
-// are the ones the compress at that length computes, so the column's size is exact.
-template <typename T> __global__ void __launch_bounds__(kCfCTA)
+// every value's residual is measured against the three lines that cover it (with the residual
+// modes of fixed_compress_kernel), and the bits of each candidate length are added into the
+// column's choice_bits[0..2] (1024, 2048, 4096).  The widths are the ones the compress at that
+// length computes, so the column's size is exact.
+template <typename T> __global__ void __launch_bounds__(kCfCTA, 2)
 choose_lengths_kernel(FixedCompressArgs a) {
   extern __shared__ __align__(128) uint8_t smem[];
   __shared__ __align__(8) uint64_t full[kCfStages], empty[kCfStages];
   __shared__ int64_t s_stile[kCfStages];
   __shared__ int s_shead[kCfStages];
   __shared__ int s_scol[kCfStages];
-  typedef typename HalfSums<T>::Acc Acc;
-  __shared__ Acc s_acc[8][4];
-  __shared__ int s_ovf[8];
+  __shared__ long long s_acc[8][4];
+  __shared__ uint32_t s_flag[8];
   __shared__ unsigned long long s_m[8][3];
-  __shared__ double s_t0[7], s_t1[7];
-  __shared__ int s_dir[7], s_safe[7], s_len[7];
+  __shared__ double s_t0[7], s_t1[7], s_c[7];
+  __shared__ long long s_ci[7];
+  __shared__ int s_mode[7], s_len[7];
   __shared__ int s_ok;
   if (threadIdx.x == 0) {
     for (int st = 0; st < kCfStages; st++) {
@@ -406,7 +771,7 @@ choose_lengths_kernel(FixedCompressArgs a) {
   }
   __syncthreads();
   if (threadIdx.x >= kCfThreads) {  // ---- producer ----
-    if (threadIdx.x == kCfThreads) cf_produce<T>(a, smem, full, empty, s_stile, s_shead, s_scol);
+    if (threadIdx.x == kCfThreads) cf_produce<T, kCfStages>(a, smem, full, empty, s_stile, s_shead, s_scol);
     return;
   }
   const int tid = threadIdx.x, warp = tid >> 5;
@@ -416,7 +781,7 @@ choose_lengths_kernel(FixedCompressArgs a) {
     const int st = k % kCfStages;
     const uint32_t par = (uint32_t)(k / kCfStages) & 1u;
     if (tid == 0) {
-      s_ok = mbar_wait_bounded(&full[st], par);
+      s_ok = mbar_wait_sleep(&full[st], par);
       if (!s_ok) {
         atomicExch(a.status, (unsigned long long)DEVERR_TIMEOUT);
         mbar_wait_bounded(&full[st], par);  // a copy in flight lands before the CTA exits
@@ -433,33 +798,22 @@ choose_lengths_kernel(FixedCompressArgs a) {
     const T* x = reinterpret_cast<const T*>(smem + (size_t)st * cf_stage_bytes<T>() + s_shead[st]);
     const int qlen = (cnt - 1024 * q) < 0 ? 0 : ((cnt - 1024 * q) < 1024 ? (cnt - 1024 * q) : 1024);
     const T* xq = x + 1024 * q;
-    {  // exact sums per quarter (two warps each)
+    {  // exact sums per quarter (two warps each) and the range flags
       HalfSums<T> hs;
-      int ovf = 0;
-#pragma unroll 4
-      for (int m = 0; m < kCfPerThread; m++) {
-        const int i = r + 64 * m;
-        if (i < qlen) {
-          const T y = xq[i];
-          ovf |= overflows_double<T>(y) ? 1 : 0;
-          hs.add(y, i);
-        }
-      }
-      Acc c0 = hs.s_lo, c1 = hs.s_hi, c2 = hs.x_lo, c3 = hs.x_hi;
-#pragma unroll
-      for (int msk = 16; msk > 0; msk >>= 1) {
-        c0 += __shfl_xor_sync(FULL_MASK, c0, msk);
-        if (sizeof(T) == 8) c1 += __shfl_xor_sync(FULL_MASK, c1, msk);
-        c2 += __shfl_xor_sync(FULL_MASK, c2, msk);
-        if (sizeof(T) == 8) c3 += __shfl_xor_sync(FULL_MASK, c3, msk);
-        ovf |= __shfl_xor_sync(FULL_MASK, ovf, msk);
-      }
+      uint32_t flag = 0;
+      if (qlen == 1024) cf_sums<T, true>(xq, r, 64, 1024, hs, flag);
+      else if (qlen > 0) cf_sums<T, false>(xq, r, 64, qlen, hs, flag);
+      const long long c0 = seg_sum48((long long)hs.s_lo, 32);
+      const long long c1 = sizeof(T) == 8 ? seg_sum48((long long)hs.s_hi, 32) : 0;
+      const long long c2 = seg_sum48((long long)hs.x_lo, 32);
+      const long long c3 = sizeof(T) == 8 ? seg_sum48((long long)hs.x_hi, 32) : 0;
+      flag = TypeTraits<T>::is_signed ? seg_or_u32(flag, 32) : seg_max_u32(flag, 32);
       if ((tid & 31) == 0) {
         s_acc[warp][0] = c0;
         s_acc[warp][1] = c1;
         s_acc[warp][2] = c2;
         s_acc[warp][3] = c3;
-        s_ovf[warp] = ovf;
+        s_flag[warp] = flag;
       }
     }
     cf_sync();
@@ -468,29 +822,37 @@ choose_lengths_kernel(FixedCompressArgs a) {
       const int q0 = l == 0 ? 0 : (l < 3 ? (l - 1) * 2 : l - 3);
       const int q1 = l == 0 ? 4 : (l < 3 ? q0 + 2 : q0 + 1);
       i128 sy = 0, sxy = 0;
-      int ovf = 0;
+      uint32_t flag = 0;
       for (int qq = q0; qq < q1; qq++) {
-        HalfSums<T> hs;
+        long long a0 = 0, a1 = 0, a2 = 0, a3 = 0;
         for (int w = 2 * qq; w < 2 * qq + 2; w++) {
-          hs.s_lo += s_acc[w][0];
-          hs.s_hi += s_acc[w][1];
-          hs.x_lo += s_acc[w][2];
-          hs.x_hi += s_acc[w][3];
-          ovf |= s_ovf[w];
+          a0 += s_acc[w][0];
+          a1 += s_acc[w][1];
+          a2 += s_acc[w][2];
+          a3 += s_acc[w][3];
+          flag = TypeTraits<T>::is_signed ? (flag | s_flag[w]) : (s_flag[w] > flag ? s_flag[w] : flag);
         }
-        const i128 qy = hs.sy();
+        const i128 qy = (i128)a0 + (i128)a1 * ((i128)1 << 32);
         sy += qy;
-        sxy += hs.sxy() + (i128)(1024 * (qq - q0)) * qy;  // quarter index -> line index
+        sxy += (i128)a2 + (i128)a3 * ((i128)1 << 32) + (i128)(1024 * (qq - q0)) * qy;  // quarter index -> line index
       }
       int len = cnt - 1024 * q0;
       len = len < 0 ? 0 : (len < 1024 * (q1 - q0) ? len : 1024 * (q1 - q0));
-      double t0 = 0.0, t1 = 0.0;
-      if (len > 0 && !ovf) solve_line(len, sy, sxy, t0, t1);
+      const bool ovf = len > 0 && cf_overflows<T>(flag, x + 1024 * q0, len);
+      const bool vsafe = sizeof(T) == 4 || flag < 0x80000u;
+      double t0 = 0.0, t1 = 0.0, c = 0.0;
+      long long ci = 0;
+      int mode = CF_DIRECT;
+      if (len > 0 && !ovf) {
+        solve_line(len, sy, sxy, t0, t1);
+        mode = cf_mode<T>(t0, t1, len, vsafe, c, ci);
+      }
       s_t0[l] = t0;
       s_t1[l] = t1;
-      s_dir[l] = ovf;
+      s_c[l] = c;
+      s_ci[l] = ci;
+      s_mode[l] = mode;
       s_len[l] = len;
-      s_safe[l] = len > 0 && !ovf && line_fp64_safe<T>(t0, t1, 0, len - 1);
     }
     cf_sync();
     {  // max |residual| of each value against its quarter's, its half's and the tile's line
@@ -498,59 +860,55 @@ choose_lengths_kernel(FixedCompressArgs a) {
       const int off[3] = {0, 1024 * (q & 1), 1024 * q};
       unsigned long long mx[3] = {0, 0, 0};
       if (qlen > 0) {
-        bool fast = s_safe[ls[0]] && s_safe[ls[1]] && s_safe[ls[2]];
-        if (fast) {  // predict_small and exact integer residuals (see fixed_compress_kernel)
-          long long dmax[3] = {0, 0, 0}, dmin[3] = {0, 0, 0};
-          double t0[3], t1[3], xd[3];
+        if (s_mode[ls[0]] == CF_NONNEG && s_mode[ls[1]] == CF_NONNEG && s_mode[ls[2]] == CF_NONNEG) {
+          // the common case in one pass: each value read once, K + y shared by the three lines
+          double t0[3], t1[3], xd[3], dm[3];
 #pragma unroll
           for (int c = 0; c < 3; c++) {
             t0[c] = s_t0[ls[c]];
             t1[c] = s_t1[ls[c]];
             xd[c] = (double)(r + off[c]);
+            dm[c] = 0.0;
           }
-#pragma unroll 2
+#pragma unroll
           for (int m = 0; m < kCfPerThread; m++) {
             const int i = r + 64 * m;
             if (i < qlen) {
-              const T y = xq[i];
-              fast &= value_fp64_safe<T>(y);
+              const double yc = magic_of<T>(xq[i]);
 #pragma unroll
               for (int c = 0; c < 3; c++) {
-                const long long d = (long long)y - predict_small(__fma_rn(t1[c], xd[c], t0[c]));
-                dmax[c] = d > dmax[c] ? d : dmax[c];
-                dmin[c] = d < dmin[c] ? d : dmin[c];
+                const double d = __dsub_rn(yc, __dadd_rz(__dadd_rn(__fma_rn(t1[c], xd[c], t0[c]), kHalfBias), kMagic));
+                dm[c] = fmax(dm[c], fabs(d));
               }
             }
 #pragma unroll
-            for (int c = 0; c < 3; c++) xd[c] += 64.0;
+            for (int c = 0; c < 3; c++) xd[c] = __dadd_rn(xd[c], 64.0);
           }
 #pragma unroll
-          for (int c = 0; c < 3; c++) mx[c] = (unsigned long long)(dmax[c] > -dmin[c] ? dmax[c] : -dmin[c]);
-        }
-        if (!fast) {  // exact integer residuals (saturating for uint64)
-          for (int c = 0; c < 3; c++) mx[c] = 0;
-          for (int m = 0; m < kCfPerThread; m++) {
-            const int i = r + 64 * m;
-            if (i >= qlen) continue;
-            const T y = xq[i];
-            for (int c = 0; c < 3; c++) {
-              if (s_dir[ls[c]]) continue;
-              const long long d =
-                  calc_delta<T>(y, predict_from<T>(__fma_rn(s_t1[ls[c]], (double)(i + off[c]), s_t0[ls[c]])));
-              const unsigned long long ad = (unsigned long long)abs_ref(d);
-              mx[c] = ad > mx[c] ? ad : mx[c];
+          for (int c = 0; c < 3; c++) mx[c] = (unsigned long long)dm[c];
+        } else {
+#pragma unroll
+          for (int c = 0; c < 3; c++) {
+            // the line's index of value i of the quarter is i + off: read through a pointer moved back by off
+            const int l = ls[c], mode = s_mode[l];
+            const T* xl = xq - off[c];
+            const int rl = r + off[c], ll = qlen + off[c];
+            const double t0 = s_t0[l], t1 = s_t1[l];
+            uint32_t fl[kCfPerThread];  // unused: only the maxima count here
+            bool general = mode == CF_GENERAL;
+            if (mode == CF_NONNEG) {
+              mx[c] = cf_resid_sign<T, false, false>(xl, rl, 64, ll, t0, t1, fl);
+            } else if (TypeTraits<T>::is_signed && mode == CF_NONPOS) {
+              mx[c] = cf_resid_sign<T, false, true>(xl, rl, 64, ll, t0, t1, fl);
+            } else if (sizeof(T) == 8 && mode == CF_OFFSET) {
+              general = !cf_resid_offset<T, false>(xl, rl, 64, ll, t0, t1, s_c[l], s_ci[l], fl, mx[c]);
             }
+            if (general) mx[c] = cf_resid_general<T>(xl, rl, 64, ll, t0, t1, fl);
           }
         }
       }
 #pragma unroll
-      for (int c = 0; c < 3; c++) {
-#pragma unroll
-        for (int msk = 16; msk > 0; msk >>= 1) {
-          const unsigned long long o = __shfl_xor_sync(FULL_MASK, mx[c], msk);
-          mx[c] = o > mx[c] ? o : mx[c];
-        }
-      }
+      for (int c = 0; c < 3; c++) mx[c] = seg_max_u64(mx[c], 32);
       if ((tid & 31) == 0) {
         s_m[warp][0] = mx[0];
         s_m[warp][1] = mx[1];
@@ -567,8 +925,8 @@ choose_lengths_kernel(FixedCompressArgs a) {
         const int w1 = l == 0 ? 8 : (l < 3 ? w0 + 4 : w0 + 2);
         unsigned long long m = 0;
         for (int w = w0; w < w1; w++) m = s_m[w][c] > m ? s_m[w][c] : m;
-        const int b = s_dir[l] ? (int)sizeof(T) * 8 : bits_for((long long)m);
-        add[l == 0 ? 2 : (l < 3 ? 1 : 0)] += (unsigned long long)s_len[l] * (unsigned long long)b;
+        const int b = s_mode[l] == CF_DIRECT ? (int)sizeof(T) * 8 : bits_for((long long)m);
+        add[c] += (unsigned long long)s_len[l] * (unsigned long long)b;
       }
       for (int c = 0; c < 3; c++)
         if (add[c]) atomicAdd(col.choice_bits + c, add[c]);
@@ -580,33 +938,57 @@ choose_lengths_kernel(FixedCompressArgs a) {
 
 // Places every tile of the launch in its column, one CTA per tile: the tile's first bit F (the
 // scan of the tiles' bits, relative to the column's first tile) is added to its partitions'
-// offsets and descriptors and to its decode-table entry, and the words whose first bit lies in the
+// descriptors, whose fields also fill the other metadata arrays (starts, ends, types, params,
+// bits, offsets), the tile's decode-table entry is written, and the words whose first bit lies in the
 // tile are written -- from the tile's slot with a funnel shift, ORed with the first bits of every
 // later tile of the column that starts inside the same word (tiles without bits are skipped).  The
 // column's last tile writes the final decode-table entry and the total, and zeroes the padding.
-__global__ void __launch_bounds__(256) fixed_place_kernel(FixedCompressArgs a) {
-  // one warp per tile (many tiles in flight per SM: the copy is bound by the memory latency of
-  // each tile's few words)
-  const int lane = threadIdx.x & 31;
-  const int64_t nwarps = (int64_t)gridDim.x * (blockDim.x >> 5);
-  for (int64_t item = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); item < a.nitems; item += nwarps) {
+//
+// Word w of the column, when its bits all lie in the tile, is funnelshift(slot[i], slot[i + 1], r)
+// with i = w - (first word the tile owns) and r = -F mod 32: each thread loads kPlaceUnroll slot
+// words before it uses one (the copy is bound by memory latency, so many loads are kept in
+// flight), and takes slot[i + 1] from the next lane.
+constexpr int kPlaceThreads = 256;
+constexpr int kPlaceUnroll = 4;
+constexpr int kPlaceVec = 4;
+
+__global__ void __launch_bounds__(kPlaceThreads, 4) fixed_place_kernel(FixedCompressArgs a) {
+  const int tid = threadIdx.x, lane = tid & 31;
+  for (int64_t item = blockIdx.x; item < a.nitems; item += gridDim.x) {
     const CfColumn& col = a.cols ? a.cols[a.owner ? a.owner[item] : 0] : a.single;
     const int64_t t = item - col.item_base;
+    const int64_t col_end = col.item_base + col.ntiles;  // the column's items are [item_base, col_end)
     const int64_t base = a.tile_first[col.item_base];
     const int64_t first = a.tile_first[item] - base;
     const int64_t bits = a.tile_bits[item];
-    const int64_t col_end = col.item_base + col.ntiles;  // the column's items are [item_base, col_end)
+    uint32_t* __restrict__ words = col.words;
     const int64_t e0 = t * kDecodeTile;
     const int cnt = (int)((col.n - e0) < kDecodeTile ? (col.n - e0) : kDecodeTile);
     const int np = (cnt + col.L - 1) / col.L;
-    if (lane < np) {
-      const int64_t gp = t * col.parts_per_tile + lane;
-      col.offs[gp] += first;
-      col.desc[gp].bit_off += first;
+    if (tid < np) {  // the tile's partitions: their metadata arrays from the descriptor
+      const int64_t gp = t * col.parts_per_tile + tid;
+      PartDesc d = col.desc[gp];
+      const int64_t off = d.bit_off + first;
+      const int len = (cnt - tid * col.L) < col.L ? (cnt - tid * col.L) : col.L;
+      d.bit_off = off;
+      col.desc[gp] = d;
+      col.starts[gp] = d.start;
+      col.ends[gp] = d.start + len;
+      col.types[gp] = d.bits_type >> 8;
+      col.params[4 * gp] = d.theta0;
+      col.params[4 * gp + 1] = d.theta1;
+      col.params[4 * gp + 2] = 0.0;
+      col.params[4 * gp + 3] = 0.0;
+      col.bits[gp] = d.bits_type & 0xff;
+      col.offs[gp] = off;
     }
     const int64_t total = a.tile_first[col_end - 1] - base + a.tile_bits[col_end - 1];
-    if (lane == 0) {
-      col.tiles[t].bit_lo = first;
+    if (tid == 0) {
+      TileInfo ti;
+      ti.bit_lo = first;
+      ti.p_first = (int32_t)(t * col.parts_per_tile);
+      ti.p_last = (int32_t)(t * col.parts_per_tile + np - 1);
+      col.tiles[t] = ti;
       if (t == col.ntiles - 1) {
         TileInfo te;
         te.bit_lo = total;
@@ -615,22 +997,62 @@ __global__ void __launch_bounds__(256) fixed_place_kernel(FixedCompressArgs a) {
         col.stats[0] = (unsigned long long)total;
       }
     }
+    // words [w_begin, w_end) have their first bit in the tile; [w_begin, w_begin + nfull) lie in it
     const int64_t w_begin = (first + 31) >> 5, w_end = (first + bits + 31) >> 5;
     if (w_end > col.words_cap) {  // the caller sized the array from another count: report, write nothing
-      if (lane == 0) atomicExch(a.status, (unsigned long long)DEVERR_BOUNDS);
+      if (tid == 0) atomicExch(a.status, (unsigned long long)DEVERR_BOUNDS);
       continue;
     }
-    const uint32_t* slot = a.slots + item * a.slot_words;
-    const int r = (int)((32 * w_begin - first) & 31);  // the same shift for every word of the tile
-    const int64_t k0 = (32 * w_begin - first) >> 5;
-#pragma unroll 4
-    for (int64_t w = w_begin + lane; w < w_end; w += 32) {
-      const int64_t lb = 32 * w - first;  // tile bit of the word's bit 0 (0 <= lb < bits)
-      const int64_t k = k0 + (w - w_begin);
-      uint32_t v = r ? __funnelshift_r(slot[k], slot[k + 1], r) : slot[k];
-      const int64_t avail = bits - lb;
-      if (avail < 32) {  // the tile ends inside the word: the next tiles' first bits follow
-        v &= (1u << avail) - 1u;
+    const uint32_t* __restrict__ slot = a.slots + item * a.slot_words;
+    if ((first & 127) == 0 && ((bits & 31) == 0 || item == col_end - 1) &&
+        (reinterpret_cast<uintptr_t>(words + w_begin) & 15) == 0) {
+      // the usual case: every partition holds L * width bits with L a multiple of 256, so every
+      // tile starts on a 16-byte boundary of its column and only a column's last tile ends inside
+      // a word -- a vector copy of the slot's first nw words
+      const int64_t nw = w_end - w_begin;
+      const uint4* __restrict__ src = reinterpret_cast<const uint4*>(slot);
+      uint4* __restrict__ dst = reinterpret_cast<uint4*>(words + w_begin);
+      const int64_t n4 = nw >> 2;
+      for (int64_t i0 = 0; i0 < n4; i0 += (int64_t)kPlaceThreads * kPlaceVec) {
+        uint4 v[kPlaceVec];
+#pragma unroll
+        for (int u = 0; u < kPlaceVec; u++) {
+          const int64_t i = i0 + tid + u * kPlaceThreads;
+          if (i < n4) v[u] = __ldg(src + i);
+        }
+#pragma unroll
+        for (int u = 0; u < kPlaceVec; u++) {
+          const int64_t i = i0 + tid + u * kPlaceThreads;
+          if (i < n4) dst[i] = v[u];
+        }
+      }
+      if (tid < (int)(nw & 3)) words[w_begin + 4 * n4 + tid] = slot[4 * n4 + tid];
+    } else {
+      const int64_t nfull = ((first + bits) >> 5) - w_begin;  // may be negative: the tile owns no full word
+      const int r = (int)((32 * w_begin - first) & 31);
+      // slot words [0, nfull] are read (the one after the last full word feeds its funnel shift; the
+      // slot holds one word more than the widest tile's bits)
+      for (int64_t i0 = 0; i0 < nfull; i0 += (int64_t)kPlaceThreads * kPlaceUnroll) {
+        uint32_t lo[kPlaceUnroll], hi[kPlaceUnroll];
+#pragma unroll
+        for (int u = 0; u < kPlaceUnroll; u++) {
+          const int64_t i = i0 + tid + u * kPlaceThreads;
+          lo[u] = i <= nfull ? __ldg(slot + i) : 0u;
+          hi[u] = (lane == 31 && i + 1 <= nfull) ? __ldg(slot + i + 1) : 0u;
+        }
+#pragma unroll
+        for (int u = 0; u < kPlaceUnroll; u++) {
+          const uint32_t nx = __shfl_down_sync(FULL_MASK, lo[u], 1);
+          const uint32_t h = lane == 31 ? hi[u] : nx;
+          const int64_t i = i0 + tid + u * kPlaceThreads;
+          if (i < nfull) words[w_begin + i] = __funnelshift_r(lo[u], h, r);
+        }
+      }
+      if (tid == 0 && w_end > w_begin && ((first + bits) & 31) != 0) {
+        // the tile ends inside its last word: that word's tile bits, then the next tiles' first bits
+        const int64_t w = w_end - 1, i = w - w_begin;
+        const int64_t avail = first + bits - 32 * w;  // 1..31 tile bits in the word
+        uint32_t v = __funnelshift_r(slot[i], slot[i + 1], r) & ((1u << avail) - 1u);
         int64_t pos = first + bits;  // column bit where the next tile starts
         for (int64_t u = item + 1; u < col_end && pos < 32 * w + 32; u++) {
           const int64_t ub = a.tile_bits[u];
@@ -641,20 +1063,20 @@ __global__ void __launch_bounds__(256) fixed_place_kernel(FixedCompressArgs a) {
           v |= f << (pos - 32 * w);
           pos += ub;
         }
+        words[w] = v;
       }
-      col.words[w] = v;
     }
     if (t == col.ntiles - 1 && col.nwords_alloc > 0) {  // the decoders' zeroed read-ahead after the bitstream
       const int64_t wt = (total + 31) >> 5;
       int64_t pad_end = ((wt + 3) & ~3ll) + 8;
       pad_end = pad_end < col.nwords_alloc ? pad_end : col.nwords_alloc;
-      for (int64_t w = wt + lane; w < pad_end && w < col.words_cap; w += 32) col.words[w] = 0u;
+      for (int64_t w = wt + tid; w < pad_end && w < col.words_cap; w += kPlaceThreads) words[w] = 0u;
     }
   }
 }
 
 template <typename T> static cudaError_t launch_fixed_compress_t(const FixedCompressArgs& a, int num_sms, cudaStream_t s) {
-  constexpr int smem = cf_smem_bytes<T>();
+  constexpr int smem = cf_fix_smem_bytes<T>();
   static PerDeviceFlag attr_set;  // per instantiation and device
   const int dev = current_device();
   cudaError_t e;
@@ -665,14 +1087,14 @@ template <typename T> static cudaError_t launch_fixed_compress_t(const FixedComp
     attr_set.set(dev);
   }
   int per_sm = 0;
-  if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fixed_compress_kernel<T>, kCfCTA, smem)) !=
+  if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fixed_compress_kernel<T>, kCfFixCTA, smem)) !=
       cudaSuccess)
     return e;
   if (per_sm < 1) per_sm = 1;
   int64_t grid = (int64_t)per_sm * num_sms;
   if (grid > a.nitems) grid = a.nitems;
   if (grid < 1) grid = 1;
-  fixed_compress_kernel<T><<<(unsigned)grid, kCfCTA, smem, s>>>(a);
+  fixed_compress_kernel<T><<<(unsigned)grid, kCfFixCTA, smem, s>>>(a);
   return cudaGetLastError();
 }
 
@@ -770,10 +1192,10 @@ static cudaError_t compress_pass(glc_dtype dt, FixedCompressArgs& a, void* scrat
 }
 
 static cudaError_t place_pass(const FixedCompressArgs& a, int num_sms, cudaStream_t s) {
-  const int64_t need = (a.nitems + 7) / 8;  // eight tiles (warps) per CTA
-  int64_t grid = need < (int64_t)num_sms * 16 ? need : (int64_t)num_sms * 16;
+  const int64_t cap = (int64_t)num_sms * 4;  // four CTAs of 256 threads per SM
+  int64_t grid = a.nitems < cap ? a.nitems : cap;
   if (grid < 1) grid = 1;
-  fixed_place_kernel<<<(unsigned)grid, 256, 0, s>>>(a);
+  fixed_place_kernel<<<(unsigned)grid, kPlaceThreads, 0, s>>>(a);
   return cudaGetLastError();
 }
 
@@ -826,6 +1248,11 @@ cudaError_t launch_fixed_place(glc_dtype dt, glc_column* c, int32_t L, void* scr
   col.item_base = 0;
   col.nwords_alloc = c->nwords_alloc;
   col.words_cap = c->nwords_alloc;
+  col.starts = c->d_start;
+  col.ends = c->d_end;
+  col.types = c->d_types;
+  col.params = c->d_params;
+  col.bits = c->d_bits;
   col.offs = c->d_offs;
   col.desc = c->d_desc;
   col.tiles = c->d_tiles;

@@ -61,6 +61,18 @@ __device__ __forceinline__ uint64_t global_ns() {
   return t;
 }
 
+// try_wait with a suspend-time hint: the thread may sleep in the barrier up to `ns` nanoseconds
+// (woken when the phase completes) instead of returning at once.
+__device__ __forceinline__ bool mbar_try_wait_hint(uint64_t* bar, uint32_t parity, uint32_t ns) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity), "r"(ns)
+      : "memory");
+  return ok != 0;
+}
+
 // Wait for the phase of parity `parity` on `bar`, giving up after ~2 s of wall time.
 __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity) {
   if (mbar_try_wait(bar, parity)) return true;
@@ -68,6 +80,19 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity
   for (long long it = 0; it < kSpinLimit; ++it) {
     if (mbar_try_wait(bar, parity)) return true;
     if ((it & 255) == 0 && global_ns() - t0 > 2000000000ull) return false;
+  }
+  return false;
+}
+
+// The same bounded wait for waits that are usually long (a producer waiting for a free stage): the
+// thread sleeps in the barrier between tests instead of polling, so it takes no issue slots from
+// the warps that work meanwhile.
+__device__ __forceinline__ bool mbar_wait_sleep(uint64_t* bar, uint32_t parity) {
+  if (mbar_try_wait(bar, parity)) return true;
+  const uint64_t t0 = global_ns();
+  for (long long it = 0; it < kSpinLimit; ++it) {
+    if (mbar_try_wait_hint(bar, parity, 20000u)) return true;
+    if (global_ns() - t0 > 2000000000ull) return false;
   }
   return false;
 }
