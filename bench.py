@@ -732,12 +732,13 @@ def run_batch(args):
     # batched compress (partition length picked per column) vs a per-column compress loop; best of
     # 3 calls each (the first call also grows the context's memory pool)
     batch_compress_ms, loop_compress_ms, batch, singles = 1e30, 1e30, None, None
+    col_ptrs = np.array([c.data_ptr() for c in cols], dtype=np.uint64)
     for rep in range(3):
         if batch is not None:
             batch.free()
         torch.cuda.synchronize(dev)
         e0.record(stream)
-        batch = glc.Batch.compress(ctx, dtypes, [c.data_ptr() for c in cols], ns, fixed_len=0, stream=sh)
+        batch = glc.Batch.compress(ctx, dtypes, col_ptrs, ns, fixed_len=0, stream=sh)
         e1.record(stream)
         torch.cuda.synchronize(dev)
         batch_compress_ms = min(batch_compress_ms, e0.elapsed_time(e1))
@@ -761,7 +762,7 @@ def run_batch(args):
     for rep in range(5):
         torch.cuda.synchronize(dev)
         e0.record(stream)
-        batch.recompress([c.data_ptr() for c in cols], use_graph=True, stream=sh)
+        batch.recompress(col_ptrs, use_graph=True, stream=sh)
         e1.record(stream)
         torch.cuda.synchronize(dev)
         recompress_ms = min(recompress_ms, e0.elapsed_time(e1))
@@ -772,7 +773,7 @@ def run_batch(args):
         offs.append(o)
         o += (c.numel() * c.element_size() + 255) // 256 * 256
     out = torch.empty(o, dtype=torch.uint8, device=dev)
-    ptrs = [out.data_ptr() + x for x in offs]
+    ptrs = np.array([out.data_ptr() + x for x in offs], dtype=np.uint64)
 
     def step():
         batch.decompress(ptrs, use_graph=True, stream=sh)
@@ -792,7 +793,7 @@ def run_batch(args):
     clk = clocks.stop()
     # the same decode as a per-column launch loop (same kernels, one launch chain per column)
     def loop():
-        for col, p in zip(singles, ptrs):
+        for col, p in zip(singles, ptrs.tolist()):
             glc.decompress_into(ctx, col, p, glc.SRC_PACKED, stream=sh)
     loop()
     torch.cuda.synchronize(dev)

@@ -7,27 +7,24 @@
 // setBitOffsetsKernel and packDeltasKernelOptimized, compression/CompressionKernels.cuh:45-372,
 // which read the values four times) with ONE persistent kernel that reads every value once:
 //
-//   producer warp   stages tile t's values in shared memory with cp.async.bulk, two tiles ahead
-//                   (full/empty mbarriers, bounded waits);
-//   compute warps   per tile, with every partition inside the tile (L divides 4096):
-//     A  exact sums per partition from 64-bit partials of 32-bit halves, and the overflow flag
-//        that selects direct copy; a group of L/16 threads owns a partition, 16 values each,
-//        so one reduction per group gives the partition's sums;
-//     -  one thread per partition solves the line from the exact sums (the same arithmetic as
-//        fit.cu, so the result is identical bit for bit);
-//     B  the residual of every value (fma prediction, round half away from zero, saturating
-//        cast; calculateDelta) written over the staged value (8-byte types) or into a residual
-//        array (4-byte types), and max |residual| per partition -> the partition's bit width;
-//     C  the tile's words from the residual fields, one thread per word, into the tile's own
-//        slot of a scratch array (slots of the worst-case size of a tile, bit offsets relative to
-//        the tile), with the partitions' metadata (the reference's SoA), their descriptors and
-//        the tile's decode-table entry, all with tile-relative bit offsets, and the tile's bit
-//        count;
+//   producer warp   stages tile t's values in shared memory with cp.async.bulk, three stages
+//                   (full/empty mbarriers, bounded waits that sleep in the barrier);
+//   solver warp     fits the lines of tile k + 1 from its exact sums (one lane per partition, the
+//                   same arithmetic as fit.cu, so the result is identical bit for bit) and picks
+//                   each partition's residual mode, while the compute warps work on tile k;
+//   compute warps   per step, with every partition inside the tile (L divides 4096):
+//     A  exact sums of tile k + 1 per partition from 64-bit partials of 32-bit halves, and the
+//        range flags (direct copy; FP64-safe values); a group of L/16 threads owns a partition,
+//        16 values each;
+//     B  the residual of every value of tile k (fma prediction, round half away from zero,
+//        saturating cast; calculateDelta -- in FP64 without conversion instructions where the
+//        line and the values allow it) and max |residual| per partition -> the bit widths;
+//     C  the tile's words into its own slot of a scratch array (slots of the worst-case size of
+//        a tile, bit offsets relative to the tile), the partitions' descriptors with
+//        tile-relative offsets and their max errors, and the tile's bit count;
 //   then an exclusive scan of the tiles' bit counts gives every tile's first bit, and
-//   fixed_place_kernel (one CTA per tile) writes each word of the column once -- the word holding
-//   bit 32 W is built by the tile that holds that bit, from its slot with a funnel shift, ORed
-//   with the first bits of any later tiles that start inside it -- and adds the tile's first bit
-//   to its partitions' offsets, descriptors and decode-table entry.  No tile waits for another.
+//   fixed_place_kernel (one CTA per tile) copies each tile's words to their place in the column
+//   and writes the metadata arrays from the descriptors.  No tile waits for another.
 //
 // The column's word array is allocated at its exact size between the two kernels (the scan gives
 // the total); the slots cost one extra write and read of the compressed bits.
@@ -39,8 +36,6 @@
 namespace glc {
 
 constexpr int kCfThreads = 256;                       // compute threads (8 warps)
-constexpr int kCfCTA = kCfThreads + 32;               // + the producer warp
-constexpr int kCfStages = 2;
 constexpr int kCfMinLen = 256;
 constexpr int kCfMaxParts = kDecodeTile / kCfMinLen;  // 16 partitions per tile at L = 256
 constexpr int kCfPerThread = kDecodeTile / kCfThreads;  // 16 values per thread
@@ -741,64 +736,110 @@ fixed_compress_kernel(const __grid_constant__ FixedCompressArgs a) {
   }
 }
 
-// The partition-length choice of the batched compress, one tile per step (the same staging as
-// fixed_compress_kernel): the tile's four 1024-value quarters, its two halves and the whole tile
-// are fitted from exact per-quarter sums (the index offsets of a half or the tile added exactly),
-// every value's residual is measured against the three lines that cover it (with the residual
-// modes of fixed_compress_kernel), and the bits of each candidate length are added into the
-// column's choice_bits[0..2] (1024, 2048, 4096).  The widths are the ones the compress at that
-// length computes, so the column's size is exact.
-template <typename T> __global__ void __launch_bounds__(kCfCTA, 2)
-choose_lengths_kernel(FixedCompressArgs a) {
+// The partition-length choice of the batched compress, one tile per step with the CTA layout of
+// fixed_compress_kernel (eight compute warps, a producer warp staging tiles three ahead, a solver
+// warp): the tile's four 1024-value quarters, its two halves and the whole tile are fitted from
+// exact per-quarter sums (the index offsets of a half or the tile added exactly) by the solver warp
+// while the compute warps measure the previous tile; every value's residual is measured against the
+// three lines that cover it (with the residual modes of fixed_compress_kernel), and the bits of each
+// candidate length are added into the column's choice_bits[0..2] (1024, 2048, 4096).  The widths
+// are the ones the compress at that length computes, so the column's size is exact.
+template <typename T> __global__ void __launch_bounds__(kCfFixCTA, 2)
+choose_lengths_kernel(const __grid_constant__ FixedCompressArgs a) {
+  constexpr int S = kCfFixStages;
   extern __shared__ __align__(128) uint8_t smem[];
-  __shared__ __align__(8) uint64_t full[kCfStages], empty[kCfStages];
-  __shared__ int64_t s_stile[kCfStages];
-  __shared__ int s_shead[kCfStages];
-  __shared__ int s_scol[kCfStages];
-  __shared__ long long s_acc[8][4];
-  __shared__ uint32_t s_flag[8];
+  __shared__ __align__(8) uint64_t full[S], empty[S], sums[S], lines[S];
+  __shared__ int64_t s_stile[S];
+  __shared__ int s_shead[S];
+  __shared__ int s_scol[S];
+  __shared__ long long s_acc[S][8][4];
+  __shared__ uint32_t s_flag[S][8];
+  __shared__ double s_t0[S][7], s_t1[S][7], s_c[S][7];
+  __shared__ long long s_ci[S][7];
+  __shared__ int s_mode[S][7], s_len[S][7];
   __shared__ unsigned long long s_m[8][3];
-  __shared__ double s_t0[7], s_t1[7], s_c[7];
-  __shared__ long long s_ci[7];
-  __shared__ int s_mode[7], s_len[7];
   __shared__ int s_ok;
   if (threadIdx.x == 0) {
-    for (int st = 0; st < kCfStages; st++) {
+    for (int st = 0; st < S; st++) {
       mbar_init(&full[st], 1);
       mbar_init(&empty[st], 1);
+      mbar_init(&sums[st], kCfThreads / 32);
+      mbar_init(&lines[st], 1);
     }
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   __syncthreads();
-  if (threadIdx.x >= kCfThreads) {  // ---- producer ----
-    if (threadIdx.x == kCfThreads) cf_produce<T, kCfStages>(a, smem, full, empty, s_stile, s_shead, s_scol);
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  if (tid >= kCfThreads + 32) {  // ---- solver warp: line l = 0 the tile, 1-2 its halves, 3-6 its quarters ----
+    for (int k = 0;; k++) {
+      const int st = k % S;
+      int ok = 1;
+      if (lane == 0) {
+        ok = mbar_wait_sleep(&sums[st], (uint32_t)(k / S) & 1u);
+        if (!ok) atomicExch(a.status, (unsigned long long)DEVERR_TIMEOUT);
+      }
+      if (!__shfl_sync(FULL_MASK, ok, 0)) return;
+      const int64_t item = s_stile[st];
+      if (item < 0) return;
+      if (lane < 7) {
+        const CfColumn& col = a.cols[s_scol[st]];
+        const int64_t e0 = (item - col.item_base) * kDecodeTile;
+        const int cnt = (int)((col.n - e0) < kDecodeTile ? (col.n - e0) : kDecodeTile);
+        const int l = lane;
+        const int q0 = l == 0 ? 0 : (l < 3 ? (l - 1) * 2 : l - 3);
+        const int q1 = l == 0 ? 4 : (l < 3 ? q0 + 2 : q0 + 1);
+        i128 sy = 0, sxy = 0;
+        uint32_t flag = 0;
+        for (int qq = q0; qq < q1; qq++) {
+          long long a0 = 0, a1 = 0, a2 = 0, a3 = 0;
+          for (int w = 2 * qq; w < 2 * qq + 2; w++) {
+            a0 += s_acc[st][w][0];
+            a1 += s_acc[st][w][1];
+            a2 += s_acc[st][w][2];
+            a3 += s_acc[st][w][3];
+            flag = TypeTraits<T>::is_signed ? (flag | s_flag[st][w]) : (s_flag[st][w] > flag ? s_flag[st][w] : flag);
+          }
+          const i128 qy = (i128)a0 + (i128)a1 * ((i128)1 << 32);
+          sy += qy;
+          sxy += (i128)a2 + (i128)a3 * ((i128)1 << 32) + (i128)(1024 * (qq - q0)) * qy;  // quarter index -> line index
+        }
+        int len = cnt - 1024 * q0;
+        len = len < 0 ? 0 : (len < 1024 * (q1 - q0) ? len : 1024 * (q1 - q0));
+        const T* x = reinterpret_cast<const T*>(smem + (size_t)st * cf_stage_bytes<T>() + s_shead[st]);
+        const bool ovf = len > 0 && cf_overflows<T>(flag, x + 1024 * q0, len);
+        const bool vsafe = sizeof(T) == 4 || flag < 0x80000u;
+        double t0 = 0.0, t1 = 0.0, c = 0.0;
+        long long ci = 0;
+        int mode = CF_DIRECT;
+        if (len > 0 && !ovf) {
+          solve_line(len, sy, sxy, t0, t1);
+          mode = cf_mode<T>(t0, t1, len, vsafe, c, ci);
+        }
+        s_t0[st][l] = t0;
+        s_t1[st][l] = t1;
+        s_c[st][l] = c;
+        s_ci[st][l] = ci;
+        s_mode[st][l] = mode;
+        s_len[st][l] = len;
+      }
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&lines[st]);
+    }
+  }
+  if (tid >= kCfThreads) {  // ---- producer ----
+    if (tid == kCfThreads) cf_produce<T, S>(a, smem, full, empty, s_stile, s_shead, s_scol);
     return;
   }
-  const int tid = threadIdx.x, warp = tid >> 5;
-  const int q = tid >> 6;          // this thread's quarter (64 threads, 16 values each)
-  const int r = tid & 63;
-  for (int k = 0;; k++) {
-    const int st = k % kCfStages;
-    const uint32_t par = (uint32_t)(k / kCfStages) & 1u;
-    if (tid == 0) {
-      s_ok = mbar_wait_sleep(&full[st], par);
-      if (!s_ok) {
-        atomicExch(a.status, (unsigned long long)DEVERR_TIMEOUT);
-        mbar_wait_bounded(&full[st], par);  // a copy in flight lands before the CTA exits
-      }
-    }
-    cf_sync();
-    if (!s_ok) return;
-    mbar_try_wait(&full[st], par);
+  // ---- compute warps: thread tid measures values r + 64 m of quarter q ----
+  const int q = tid >> 6, r = tid & 63;
+  auto stage_sums = [&](int st) {  // exact sums per quarter (two warps each) and the range flags
     const int64_t item = s_stile[st];
-    if (item < 0) return;
-    const CfColumn& col = a.cols[s_scol[st]];
-    const int64_t e0 = (item - col.item_base) * kDecodeTile;
-    const int cnt = (int)((col.n - e0) < kDecodeTile ? (col.n - e0) : kDecodeTile);
-    const T* x = reinterpret_cast<const T*>(smem + (size_t)st * cf_stage_bytes<T>() + s_shead[st]);
-    const int qlen = (cnt - 1024 * q) < 0 ? 0 : ((cnt - 1024 * q) < 1024 ? (cnt - 1024 * q) : 1024);
-    const T* xq = x + 1024 * q;
-    {  // exact sums per quarter (two warps each) and the range flags
+    if (item >= 0) {
+      const CfColumn& col = a.cols[s_scol[st]];
+      const int64_t e0 = (item - col.item_base) * kDecodeTile;
+      const int cnt = (int)((col.n - e0) < kDecodeTile ? (col.n - e0) : kDecodeTile);
+      const int qlen = (cnt - 1024 * q) < 0 ? 0 : ((cnt - 1024 * q) < 1024 ? (cnt - 1024 * q) : 1024);
+      const T* xq = reinterpret_cast<const T*>(smem + (size_t)st * cf_stage_bytes<T>() + s_shead[st]) + 1024 * q;
       HalfSums<T> hs;
       uint32_t flag = 0;
       if (qlen == 1024) cf_sums<T, true>(xq, r, 64, 1024, hs, flag);
@@ -808,65 +849,70 @@ choose_lengths_kernel(FixedCompressArgs a) {
       const long long c2 = seg_sum48((long long)hs.x_lo, 32);
       const long long c3 = sizeof(T) == 8 ? seg_sum48((long long)hs.x_hi, 32) : 0;
       flag = TypeTraits<T>::is_signed ? seg_or_u32(flag, 32) : seg_max_u32(flag, 32);
-      if ((tid & 31) == 0) {
-        s_acc[warp][0] = c0;
-        s_acc[warp][1] = c1;
-        s_acc[warp][2] = c2;
-        s_acc[warp][3] = c3;
-        s_flag[warp] = flag;
+      if (lane == 0) {
+        s_acc[st][warp][0] = c0;
+        s_acc[st][warp][1] = c1;
+        s_acc[st][warp][2] = c2;
+        s_acc[st][warp][3] = c3;
+        s_flag[st][warp] = flag;
+      }
+    }
+    __syncwarp();
+    if (lane == 0) mbar_arrive(&sums[st]);
+  };
+
+  if (tid == 0) {
+    s_ok = mbar_wait_sleep(&full[0], 0);
+    if (!s_ok) {
+      atomicExch(a.status, (unsigned long long)DEVERR_TIMEOUT);
+      mbar_wait_bounded(&full[0], 0);  // a copy in flight lands before the CTA exits
+    }
+  }
+  cf_sync();
+  if (!s_ok) return;
+  mbar_try_wait(&full[0], 0);
+  if (s_stile[0] < 0) return;
+  stage_sums(0);
+
+  for (int k = 0;; k++) {
+    const int st = k % S, st1 = (k + 1) % S;
+    const uint32_t par = (uint32_t)(k / S) & 1u, par1 = (uint32_t)((k + 1) / S) & 1u;
+    if (tid == 0) {
+      s_ok = mbar_wait_sleep(&full[st1], par1);
+      if (!s_ok) {
+        atomicExch(a.status, (unsigned long long)DEVERR_TIMEOUT);
+        mbar_wait_bounded(&full[st1], par1);  // a copy in flight lands before the CTA exits
+      } else {
+        s_ok = mbar_wait_sleep(&lines[st], par);
+        if (!s_ok) atomicExch(a.status, (unsigned long long)DEVERR_TIMEOUT);
       }
     }
     cf_sync();
-    if (tid < 7) {  // line l: 0 = the tile, 1-2 = its halves, 3-6 = its quarters
-      const int l = tid;
-      const int q0 = l == 0 ? 0 : (l < 3 ? (l - 1) * 2 : l - 3);
-      const int q1 = l == 0 ? 4 : (l < 3 ? q0 + 2 : q0 + 1);
-      i128 sy = 0, sxy = 0;
-      uint32_t flag = 0;
-      for (int qq = q0; qq < q1; qq++) {
-        long long a0 = 0, a1 = 0, a2 = 0, a3 = 0;
-        for (int w = 2 * qq; w < 2 * qq + 2; w++) {
-          a0 += s_acc[w][0];
-          a1 += s_acc[w][1];
-          a2 += s_acc[w][2];
-          a3 += s_acc[w][3];
-          flag = TypeTraits<T>::is_signed ? (flag | s_flag[w]) : (s_flag[w] > flag ? s_flag[w] : flag);
-        }
-        const i128 qy = (i128)a0 + (i128)a1 * ((i128)1 << 32);
-        sy += qy;
-        sxy += (i128)a2 + (i128)a3 * ((i128)1 << 32) + (i128)(1024 * (qq - q0)) * qy;  // quarter index -> line index
-      }
-      int len = cnt - 1024 * q0;
-      len = len < 0 ? 0 : (len < 1024 * (q1 - q0) ? len : 1024 * (q1 - q0));
-      const bool ovf = len > 0 && cf_overflows<T>(flag, x + 1024 * q0, len);
-      const bool vsafe = sizeof(T) == 4 || flag < 0x80000u;
-      double t0 = 0.0, t1 = 0.0, c = 0.0;
-      long long ci = 0;
-      int mode = CF_DIRECT;
-      if (len > 0 && !ovf) {
-        solve_line(len, sy, sxy, t0, t1);
-        mode = cf_mode<T>(t0, t1, len, vsafe, c, ci);
-      }
-      s_t0[l] = t0;
-      s_t1[l] = t1;
-      s_c[l] = c;
-      s_ci[l] = ci;
-      s_mode[l] = mode;
-      s_len[l] = len;
-    }
-    cf_sync();
+    if (!s_ok) return;
+    mbar_try_wait(&full[st1], par1);
+    mbar_try_wait(&lines[st], par);
+    const int64_t item1 = s_stile[st1];
+    stage_sums(st1);
+
+    const int64_t item = s_stile[st];
+    const CfColumn& col = a.cols[s_scol[st]];
+    const int64_t e0 = (item - col.item_base) * kDecodeTile;
+    const int cnt = (int)((col.n - e0) < kDecodeTile ? (col.n - e0) : kDecodeTile);
+    const T* x = reinterpret_cast<const T*>(smem + (size_t)st * cf_stage_bytes<T>() + s_shead[st]);
+    const int qlen = (cnt - 1024 * q) < 0 ? 0 : ((cnt - 1024 * q) < 1024 ? (cnt - 1024 * q) : 1024);
+    const T* xq = x + 1024 * q;
     {  // max |residual| of each value against its quarter's, its half's and the tile's line
       const int ls[3] = {3 + q, 1 + (q >> 1), 0};
       const int off[3] = {0, 1024 * (q & 1), 1024 * q};
       unsigned long long mx[3] = {0, 0, 0};
       if (qlen > 0) {
-        if (s_mode[ls[0]] == CF_NONNEG && s_mode[ls[1]] == CF_NONNEG && s_mode[ls[2]] == CF_NONNEG) {
+        if (s_mode[st][ls[0]] == CF_NONNEG && s_mode[st][ls[1]] == CF_NONNEG && s_mode[st][ls[2]] == CF_NONNEG) {
           // the common case in one pass: each value read once, K + y shared by the three lines
           double t0[3], t1[3], xd[3], dm[3];
 #pragma unroll
           for (int c = 0; c < 3; c++) {
-            t0[c] = s_t0[ls[c]];
-            t1[c] = s_t1[ls[c]];
+            t0[c] = s_t0[st][ls[c]];
+            t1[c] = s_t1[st][ls[c]];
             xd[c] = (double)(r + off[c]);
             dm[c] = 0.0;
           }
@@ -890,10 +936,10 @@ choose_lengths_kernel(FixedCompressArgs a) {
 #pragma unroll
           for (int c = 0; c < 3; c++) {
             // the line's index of value i of the quarter is i + off: read through a pointer moved back by off
-            const int l = ls[c], mode = s_mode[l];
+            const int l = ls[c], mode = s_mode[st][l];
             const T* xl = xq - off[c];
             const int rl = r + off[c], ll = qlen + off[c];
-            const double t0 = s_t0[l], t1 = s_t1[l];
+            const double t0 = s_t0[st][l], t1 = s_t1[st][l];
             uint32_t fl[kCfPerThread];  // unused: only the maxima count here
             bool general = mode == CF_GENERAL;
             if (mode == CF_NONNEG) {
@@ -901,7 +947,7 @@ choose_lengths_kernel(FixedCompressArgs a) {
             } else if (TypeTraits<T>::is_signed && mode == CF_NONPOS) {
               mx[c] = cf_resid_sign<T, false, true>(xl, rl, 64, ll, t0, t1, fl);
             } else if (sizeof(T) == 8 && mode == CF_OFFSET) {
-              general = !cf_resid_offset<T, false>(xl, rl, 64, ll, t0, t1, s_c[l], s_ci[l], fl, mx[c]);
+              general = !cf_resid_offset<T, false>(xl, rl, 64, ll, t0, t1, s_c[st][l], s_ci[st][l], fl, mx[c]);
             }
             if (general) mx[c] = cf_resid_general<T>(xl, rl, 64, ll, t0, t1, fl);
           }
@@ -909,7 +955,7 @@ choose_lengths_kernel(FixedCompressArgs a) {
       }
 #pragma unroll
       for (int c = 0; c < 3; c++) mx[c] = seg_max_u64(mx[c], 32);
-      if ((tid & 31) == 0) {
+      if (lane == 0) {
         s_m[warp][0] = mx[0];
         s_m[warp][1] = mx[1];
         s_m[warp][2] = mx[2];
@@ -919,20 +965,21 @@ choose_lengths_kernel(FixedCompressArgs a) {
     if (tid == 0) {
       unsigned long long add[3] = {0, 0, 0};
       for (int l = 0; l < 7; l++) {
-        if (s_len[l] <= 0) continue;
+        if (s_len[st][l] <= 0) continue;
         const int c = l == 0 ? 2 : (l < 3 ? 1 : 0);                      // index into s_m's lines
         const int w0 = l == 0 ? 0 : (l < 3 ? 4 * (l - 1) : 2 * (l - 3));  // the line's warps
         const int w1 = l == 0 ? 8 : (l < 3 ? w0 + 4 : w0 + 2);
         unsigned long long m = 0;
         for (int w = w0; w < w1; w++) m = s_m[w][c] > m ? s_m[w][c] : m;
-        const int b = s_mode[l] == CF_DIRECT ? (int)sizeof(T) * 8 : bits_for((long long)m);
-        add[c] += (unsigned long long)s_len[l] * (unsigned long long)b;
+        const int b = s_mode[st][l] == CF_DIRECT ? (int)sizeof(T) * 8 : bits_for((long long)m);
+        add[c] += (unsigned long long)s_len[st][l] * (unsigned long long)b;
       }
       for (int c = 0; c < 3; c++)
         if (add[c]) atomicAdd(col.choice_bits + c, add[c]);
     }
-    cf_sync();  // every compute thread is done with stage st
+    cf_sync();  // every compute thread is done with stage st (and with s_m)
     if (tid == 0) mbar_arrive(&empty[st]);
+    if (item1 < 0) return;
   }
 }
 
@@ -1109,7 +1156,7 @@ static cudaError_t launch_fixed_compress_dt(glc_dtype dt, const FixedCompressArg
 }
 
 template <typename T> static cudaError_t launch_choose_t(const FixedCompressArgs& a, int num_sms, cudaStream_t s) {
-  constexpr int smem = kCfStages * cf_stage_bytes<T>();
+  constexpr int smem = kCfFixStages * cf_stage_bytes<T>();
   static PerDeviceFlag attr_set;
   const int dev = current_device();
   cudaError_t e;
@@ -1120,14 +1167,14 @@ template <typename T> static cudaError_t launch_choose_t(const FixedCompressArgs
     attr_set.set(dev);
   }
   int per_sm = 0;
-  if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, choose_lengths_kernel<T>, kCfCTA, smem)) !=
+  if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, choose_lengths_kernel<T>, kCfFixCTA, smem)) !=
       cudaSuccess)
     return e;
   if (per_sm < 1) per_sm = 1;
   int64_t grid = (int64_t)per_sm * num_sms;
   if (grid > a.nitems) grid = a.nitems;
   if (grid < 1) grid = 1;
-  choose_lengths_kernel<T><<<(unsigned)grid, kCfCTA, smem, s>>>(a);
+  choose_lengths_kernel<T><<<(unsigned)grid, kCfFixCTA, smem, s>>>(a);
   return cudaGetLastError();
 }
 

@@ -396,6 +396,35 @@ class BorrowedColumn(Column):
         self.handle = None
 
 
+class _BatchColumns:
+    """The columns of a compressed batch, as BorrowedColumn handles fetched on first access (a batch
+    of thousands of columns is not walked on every compress)."""
+
+    def __init__(self, ctx: Context, handle: ctypes.c_void_p, n: int):
+        self._ctx, self._handle, self._n = ctx, handle, n
+        self._cache = {}
+
+    def __len__(self):
+        return self._n
+
+    def __getitem__(self, i):
+        if isinstance(i, slice):
+            return [self[k] for k in range(*i.indices(self._n))]
+        if i < 0:
+            i += self._n
+        if not 0 <= i < self._n:
+            raise IndexError(i)
+        c = self._cache.get(i)
+        if c is None:
+            h = ctypes.c_void_p()
+            self._ctx.check(self._ctx.lib.glc_batch_column(self._handle, i, ctypes.byref(h)))
+            c = self._cache[i] = BorrowedColumn(self._ctx, h)
+        return c
+
+    def __iter__(self):
+        return (self[i] for i in range(self._n))
+
+
 class Batch:
     """Many columns per launch: batched compress and one-launch decode (glc_batch_*)."""
 
@@ -407,19 +436,14 @@ class Batch:
     @classmethod
     def compress(cls, ctx: Context, dtypes, dptrs, ns, fixed_len: int = 0, stream: int = 0):
         n = len(dtypes)
-        dt = (ctypes.c_int * n)(*dtypes)
-        vp = (ctypes.c_void_p * n)(*dptrs)
-        nn = (ctypes.c_int64 * n)(*ns)
+        dt = np.ascontiguousarray(dtypes, dtype=np.int32)
+        vp = np.ascontiguousarray(dptrs, dtype=np.uint64)
+        nn = np.ascontiguousarray(ns, dtype=np.int64)
         h = ctypes.c_void_p()
         size = ctypes.c_int64()
-        ctx.check(ctx.lib.glc_batch_compress(ctx.handle, dt, vp, nn, n, fixed_len, ctypes.byref(h), ctypes.byref(size),
-                                             ctypes.c_void_p(stream)))
-        cols = []
-        for i in range(n):
-            c = ctypes.c_void_p()
-            ctx.check(ctx.lib.glc_batch_column(h, i, ctypes.byref(c)))
-            cols.append(BorrowedColumn(ctx, c))
-        b = cls(ctx, h, cols)
+        ctx.check(ctx.lib.glc_batch_compress(ctx.handle, dt.ctypes.data, vp.ctypes.data, nn.ctypes.data, n, fixed_len,
+                                             ctypes.byref(h), ctypes.byref(size), ctypes.c_void_p(stream)))
+        b = cls(ctx, h, _BatchColumns(ctx, h, n))
         b.compressed_size = size.value
         return b
 
@@ -432,17 +456,17 @@ class Batch:
         return cls(ctx, h, list(columns))
 
     def decompress(self, out_ptrs, use_graph: bool = False, stream: int = 0):
-        n = len(self.columns)
-        arr = (ctypes.c_void_p * n)(*out_ptrs)
-        self.ctx.check(self.ctx.lib.glc_batch_decompress(self.ctx.handle, self.handle, arr, 1 if use_graph else 0,
-                                                         ctypes.c_void_p(stream)))
+        arr = np.ascontiguousarray(out_ptrs, dtype=np.uint64)
+        assert len(arr) == len(self.columns)
+        self.ctx.check(self.ctx.lib.glc_batch_decompress(self.ctx.handle, self.handle, arr.ctypes.data,
+                                                         1 if use_graph else 0, ctypes.c_void_p(stream)))
 
     def recompress(self, dptrs, use_graph: bool = False, stream: int = 0):
         """glc_batch_recompress: new values for the same columns, each at the length chosen before."""
-        n = len(self.columns)
-        vp = (ctypes.c_void_p * n)(*dptrs)
-        self.ctx.check(self.ctx.lib.glc_batch_recompress(self.ctx.handle, self.handle, vp, 1 if use_graph else 0,
-                                                         ctypes.c_void_p(stream)))
+        vp = np.ascontiguousarray(dptrs, dtype=np.uint64)
+        assert len(vp) == len(self.columns)
+        self.ctx.check(self.ctx.lib.glc_batch_recompress(self.ctx.handle, self.handle, vp.ctypes.data,
+                                                         1 if use_graph else 0, ctypes.c_void_p(stream)))
 
     def sync(self, stream: int = 0) -> int:
         """glc_batch_sync: the columns' sizes after recompress; returns the total compressed size."""
