@@ -346,6 +346,19 @@ def run_random_access(args):
     per_lookup = 4 + 8 + 32
     peak, peak_kind = measured_peak()
     achieved = per_lookup * lookups_s / 1e9
+    # the ceiling of this access pattern: a plain 8-byte gather (torch.index_select) of the same
+    # positions from the raw values, an array as large as the pre-unpacked residuals (512 MB)
+    d_pos64 = d_pos.long()
+    gout = torch.empty(q, dtype=torch.int64, device=dev)
+    for _ in range(3):
+        torch.index_select(d_vals, 0, d_pos64, out=gout)
+    e0.record(stream)
+    for _ in range(args.steps):
+        torch.index_select(d_vals, 0, d_pos64, out=gout)
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    gather_s = q / (e0.elapsed_time(e1) / args.steps / 1e3)
+    del d_pos64, gout
     # end to end: pinned host positions in, pinned host values out, through the C ABI
     h_pos = torch.from_numpy(pos).pin_memory()
     h_out = torch.empty(q, dtype=torch.int64).pin_memory()
@@ -387,6 +400,10 @@ def run_random_access(args):
         "config": {"workload": f"timestamps_i64_64M_fixed4096_lookups100M_{args.mode}", "values": n, "lookups": q,
                    "partitions": info.num_partitions, "bits_per_value": round(info.total_bits / n, 3),
                    "position_mix": "50% uniform, 50% Zipf(1.1) over partitions", "bit_exact": ok and e2e_ok,
+                   "gather_ceiling": {"value": round(gather_s, 1), "unit": "lookups/s",
+                                      "what": "torch.index_select of the same positions from the raw 512 MB int64 "
+                                              "values (8 B random gather, no decoding)",
+                                      "frac": round(lookups_s / gather_s, 4)},
                    "l2": "positions and outputs larger than L2 (no flush)"},
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4), "peak_kind": peak_kind, "traffic": None,
