@@ -418,13 +418,17 @@ __device__ __forceinline__ void cf_store_resid(const T* xp, long long* rp, int r
 // The compress kernel's CTA: eight compute warps, the producer warp and the solver warp.  Per step
 // k the compute warps take the sums of tile k + 1 and the residuals, widths and words of tile k,
 // while the solver warp fits the lines of tile k + 1 (one lane per partition) and the producer
-// stages tile k + 2: the fit's long dependency chain (128-bit arithmetic, two divisions) runs beside
-// the compute warps instead of between two of their barriers.  Every wait is bounded.
-constexpr int kCfFixStages = 3;
+// stages the next tile as soon as a stage is free: the fit's long dependency chain (128-bit
+// arithmetic, two divisions) runs beside the compute warps instead of between two of their
+// barriers.  Every wait is bounded.  The compress kernel runs two stages at three CTAs per SM (64
+// registers; measured 5 % faster than three stages at two CTAs per SM: other CTAs cover the load
+// of the next tile); the length choice, with heavier per-value work, three stages at two.
+constexpr int kCfCompressStages = 2;
+constexpr int kCfChooseStages = 3;
 constexpr int kCfFixCTA = kCfThreads + 64;
 
-template <typename T> __host__ __device__ constexpr int cf_fix_smem_bytes() {
-  return kCfFixStages * cf_stage_bytes<T>() + (sizeof(T) == 4 ? kCfWorkBytes : 0);
+template <typename T> __host__ __device__ constexpr int cf_fix_smem_bytes(int stages) {
+  return stages * cf_stage_bytes<T>() + (sizeof(T) == 4 ? kCfWorkBytes : 0);
 }
 
 // A tile as a step sees it.
@@ -452,10 +456,9 @@ __device__ __forceinline__ CfGeom cf_geom(const FixedCompressArgs& a, int64_t it
   return q;
 }
 
-// Two CTAs per SM (96 registers; three stages of 33 KB for 8-byte types).
-template <typename T> __global__ void __launch_bounds__(kCfFixCTA, 2)
+template <typename T> __global__ void __launch_bounds__(kCfFixCTA, 3)
 fixed_compress_kernel(const __grid_constant__ FixedCompressArgs a) {
-  constexpr int S = kCfFixStages;
+  constexpr int S = kCfCompressStages;
   extern __shared__ __align__(128) uint8_t smem[];
   __shared__ __align__(8) uint64_t full[S], empty[S], sums[S], lines[S];
   __shared__ int64_t s_stile[S];   // work item staged in each stage (-1: the end)
@@ -746,7 +749,7 @@ fixed_compress_kernel(const __grid_constant__ FixedCompressArgs a) {
 // are the ones the compress at that length computes, so the column's size is exact.
 template <typename T> __global__ void __launch_bounds__(kCfFixCTA, 2)
 choose_lengths_kernel(const __grid_constant__ FixedCompressArgs a) {
-  constexpr int S = kCfFixStages;
+  constexpr int S = kCfChooseStages;
   extern __shared__ __align__(128) uint8_t smem[];
   __shared__ __align__(8) uint64_t full[S], empty[S], sums[S], lines[S];
   __shared__ int64_t s_stile[S];
@@ -1123,7 +1126,7 @@ __global__ void __launch_bounds__(kPlaceThreads, 4) fixed_place_kernel(FixedComp
 }
 
 template <typename T> static cudaError_t launch_fixed_compress_t(const FixedCompressArgs& a, int num_sms, cudaStream_t s) {
-  constexpr int smem = cf_fix_smem_bytes<T>();
+  constexpr int smem = cf_fix_smem_bytes<T>(kCfCompressStages);
   static PerDeviceFlag attr_set;  // per instantiation and device
   const int dev = current_device();
   cudaError_t e;
@@ -1156,7 +1159,7 @@ static cudaError_t launch_fixed_compress_dt(glc_dtype dt, const FixedCompressArg
 }
 
 template <typename T> static cudaError_t launch_choose_t(const FixedCompressArgs& a, int num_sms, cudaStream_t s) {
-  constexpr int smem = kCfFixStages * cf_stage_bytes<T>();
+  constexpr int smem = kCfChooseStages * cf_stage_bytes<T>();
   static PerDeviceFlag attr_set;
   const int dev = current_device();
   cudaError_t e;

@@ -88,7 +88,8 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity
 // thread sleeps in the barrier between tests instead of polling, so it takes no issue slots from
 // the warps that work meanwhile.
 __device__ __forceinline__ bool mbar_wait_sleep(uint64_t* bar, uint32_t parity) {
-  if (mbar_try_wait(bar, parity)) return true;
+  for (int i = 0; i < 8; i++)  // a phase about to complete is taken without sleeping
+    if (mbar_try_wait(bar, parity)) return true;
   const uint64_t t0 = global_ns();
   for (long long it = 0; it < kSpinLimit; ++it) {
     if (mbar_try_wait_hint(bar, parity, 20000u)) return true;
