@@ -365,9 +365,24 @@ glc_status build_work(glc_ctx* ctx, glc_batch* b, void* const* outs, cudaStream_
 // so the same widths), so every array is allocated at its exact size before one launch per element
 // type fits, offsets, packs and tabulates all of that type's columns.  The values are read twice
 // in all: once by the choice, once by this launch.
+// The length choice's pass over one element type, which also packed every tile at length 4096:
+// its column table and work list (the choice's item numbering), the tiles' slots and bits
+// (scratch), their descriptors and max errors, and each column's widest field at 4096.
+struct PrePacked {
+  glc_dtype dt;
+  int64_t nitems = 0;
+  std::vector<int> cols;          // the batch's column index of each entry of the table
+  std::vector<int64_t> item_base; // per entry
+  int32_t* d_owner = nullptr;
+  void* scratch = nullptr;        // from the context's pool, returned after the place
+  PartDesc* tdesc = nullptr;
+  long long* terr = nullptr;
+};
+
 glc_status compress_one_pass(glc_ctx* ctx, glc_batch* b, const glc_dtype* dtypes, const void* const* values,
                              const int64_t* ns, int nc, const std::vector<int32_t>& len,
-                             const std::vector<unsigned long long>& hbits, cudaStream_t s, int64_t* total_size) {
+                             const std::vector<unsigned long long>& hbits, cudaStream_t s, int64_t* total_size,
+                             std::vector<PrePacked>* pre, unsigned long long* pre_stats) {
   std::vector<int64_t> pb(nc + 1, 0), wb(nc + 1, 0), eb(nc + 1, 0);
   std::vector<glc_column*> cols(nc, nullptr);
   for (int i = 0; i < nc; i++) {
@@ -442,17 +457,53 @@ glc_status compress_one_pass(glc_ctx* ctx, glc_batch* b, const glc_dtype* dtypes
     f.words = c->d_words;
     f.stats = stats + 2 * i;
   }
-  // one launch per element type over the tiles of that type's columns, in column order; the host
-  // tables stay alive until the stream is synchronised
+  // a column the length choice already packed (it keeps length 4096) is only placed
+  std::vector<char> prepacked(nc, 0);
+  if (pre)
+    for (const PrePacked& pp : *pre)
+      for (int i : pp.cols) prepacked[i] = len[i] == 4096;
+  // one launch per element type over the tiles of that type's other columns, in column order; the
+  // host tables stay alive until the stream is synchronised
   std::vector<std::vector<CfColumn>> keep_g;
   std::vector<std::vector<int64_t>> keep_ib;
+  if (pre) {
+    for (PrePacked& pp : *pre) {
+      keep_g.emplace_back();
+      std::vector<CfColumn>& tab = keep_g.back();
+      bool any = false;
+      for (size_t k = 0; k < pp.cols.size(); k++) {
+        CfColumn f{};
+        const int i = pp.cols[k];
+        if (prepacked[i]) {
+          f = hc[i];
+          any = true;
+        }
+        f.n = ns[i];
+        f.ntiles = (ns[i] + kDecodeTile - 1) / kDecodeTile;
+        f.item_base = pp.item_base[k];  // words stay null for a column placed elsewhere: skipped
+        tab.push_back(f);
+      }
+      cudaError_t ee = cudaSuccess;
+      if (any) {
+        CfColumn* d_tab;
+        if ((e = dalloc(b, &d_tab, tab.size())) != cudaSuccess) return bcuda(ctx, e, "batch compress: allocation");
+        ee = cudaMemcpyAsync(d_tab, tab.data(), sizeof(CfColumn) * tab.size(), cudaMemcpyHostToDevice, s);
+        if (ee == cudaSuccess)
+          ee = launch_place_prepacked(pp.dt, d_tab, pp.d_owner, pp.nitems, pp.scratch, pp.tdesc, pp.terr,
+                                      stats + 2 * (size_t)nc, ctx->num_sms, s);
+      }
+      cudaFreeAsync(pp.scratch, s);
+      pp.scratch = nullptr;
+      BCK(ee, "batch compress: place of the columns packed by the length choice");
+    }
+  }
   for (glc_dtype dt : {GLC_I32, GLC_I64, GLC_U64, GLC_U32}) {
     keep_g.emplace_back();
     keep_ib.emplace_back(1, 0);
     std::vector<CfColumn>& g = keep_g.back();
     std::vector<int64_t>& ib = keep_ib.back();
     for (int i = 0; i < nc; i++) {
-      if (dtypes[i] != dt || ns[i] == 0) continue;
+      if (dtypes[i] != dt || ns[i] == 0 || prepacked[i]) continue;
       CfColumn f = hc[i];
       f.item_base = ib.back();
       g.push_back(f);
@@ -476,10 +527,15 @@ glc_status compress_one_pass(glc_ctx* ctx, glc_batch* b, const glc_dtype* dtypes
     cudaFreeAsync(scratch, s);
     BCK(e, "batch compress: one-pass compress");
   }
-  std::vector<unsigned long long> hs(2 * (size_t)nc + 1);
+  std::vector<unsigned long long> hs(2 * (size_t)nc + 1), hp(pre_stats ? 2 * (size_t)nc : 0);
   BCK(cudaMemcpyAsync(hs.data(), stats, sizeof(unsigned long long) * hs.size(), cudaMemcpyDeviceToHost, s),
       "batch compress: stats");
+  if (pre_stats)
+    BCK(cudaMemcpyAsync(hp.data(), pre_stats, sizeof(unsigned long long) * hp.size(), cudaMemcpyDeviceToHost, s),
+        "batch compress: stats");
   BCK(cudaStreamSynchronize(s), "batch compress: sync");
+  for (int i = 0; i < nc && pre_stats; i++)
+    if (prepacked[i]) hs[2 * (size_t)i + 1] = hp[2 * (size_t)i + 1];  // widest field at 4096
   if (hs[2 * (size_t)nc] == DEVERR_TIMEOUT) return bfail(ctx, GLC_ERR_TIMEOUT, "batch compress: a device-side wait gave up");
   if (hs[2 * (size_t)nc] != DEVERR_NONE) return bfail(ctx, GLC_ERR_CUDA, "batch compress: words beyond their array");
   int64_t total = 0;
@@ -668,17 +724,33 @@ glc_status glc_batch_compress(glc_ctx* ctx, const glc_dtype* dtypes, const void*
   const bool one_pass = fixed_partition_len == 0 || fixed_partition_len == 1024 || fixed_partition_len == 2048 ||
                         fixed_partition_len == 4096;
   std::vector<unsigned long long> hbits(3 * (size_t)nc);
+  std::vector<PrePacked> pre;
   if (one_pass) {  // one read of every column measures all three candidate lengths
     if ((e = cudaMemsetAsync(d_colbits, 0, sizeof(unsigned long long) * (3 * (size_t)nc + 1), s)) != cudaSuccess)
       return bail(bcuda(ctx, e, "batch compress: sizes"));
-    // one launch per element type; the host tables stay alive until the stream is synchronised
+    // one launch per element type, which also packs every tile at length 4096 (kept by most
+    // columns); the host tables stay alive until the stream is synchronised
     std::vector<std::vector<CfColumn>> keep_g;
     std::vector<std::vector<int64_t>> keep_ib;
+    const bool pack = fixed_partition_len == 0 || fixed_partition_len == 4096;
+    unsigned long long* pre_stats = nullptr;  // per column: [1] widest field at 4096
+    if (pack) {
+      if ((e = dalloc(b, &pre_stats, 2 * (size_t)nc)) != cudaSuccess ||
+          (e = cudaMemsetAsync(pre_stats, 0, sizeof(unsigned long long) * 2 * (size_t)nc, s)) != cudaSuccess)
+        return bail(bcuda(ctx, e, "batch compress: allocation"));
+    }
+    auto release_pre = [&]() {
+      for (PrePacked& pp : pre)
+        if (pp.scratch) cudaFreeAsync(pp.scratch, s);
+      pre.clear();
+    };
     for (glc_dtype dt : {GLC_I32, GLC_I64, GLC_U64, GLC_U32}) {
       keep_g.emplace_back();
       keep_ib.emplace_back(1, 0);
       std::vector<CfColumn>& g = keep_g.back();
       std::vector<int64_t>& ib = keep_ib.back();
+      PrePacked pp;
+      pp.dt = dt;
       for (int i = 0; i < nc; i++) {
         if (dtypes[i] != dt || ns[i] == 0) continue;
         CfColumn f{};
@@ -687,6 +759,9 @@ glc_status glc_batch_compress(glc_ctx* ctx, const glc_dtype* dtypes, const void*
         f.ntiles = (ns[i] + kDecodeTile - 1) / kDecodeTile;
         f.item_base = ib.back();
         f.choice_bits = d_colbits + 3 * (size_t)i;
+        f.stats = pack ? pre_stats + 2 * (size_t)i : nullptr;
+        pp.cols.push_back(i);
+        pp.item_base.push_back(ib.back());
         g.push_back(f);
         ib.push_back(ib.back() + f.ntiles);
       }
@@ -695,12 +770,24 @@ glc_status glc_batch_compress(glc_ctx* ctx, const glc_dtype* dtypes, const void*
       int64_t* d_ib;
       int32_t* d_owner;
       if ((e = dalloc(b, &d_g, g.size())) || (e = dalloc(b, &d_ib, ib.size())) || (e = dalloc(b, &d_owner, ib.back())))
-        return bail(bcuda(ctx, e, "batch compress: allocation"));
+        return release_pre(), bail(bcuda(ctx, e, "batch compress: allocation"));
+      pp.nitems = ib.back();
+      pp.d_owner = d_owner;
+      if (pack) {
+        if ((e = dalloc(b, &pp.tdesc, pp.nitems)) || (e = dalloc(b, &pp.terr, pp.nitems)) ||
+            (e = cudaMallocFromPoolAsync(&pp.scratch, fixed_compress_scratch_bytes(dt, pp.nitems), ctx->pool, s)))
+          return release_pre(), bail(bcuda(ctx, e, "batch compress: allocation"));
+      }
+      void* scratch = pp.scratch;
+      PartDesc* tdesc = pp.tdesc;
+      long long* terr = pp.terr;
+      if (pack) pre.push_back(std::move(pp));
       if ((e = cudaMemcpyAsync(d_g, g.data(), sizeof(CfColumn) * g.size(), cudaMemcpyHostToDevice, s)) ||
           (e = cudaMemcpyAsync(d_ib, ib.data(), sizeof(int64_t) * ib.size(), cudaMemcpyHostToDevice, s)) ||
           (e = launch_pack_item_owner(d_ib, (int)g.size(), d_owner, s)) ||
-          (e = launch_choose_lengths(dt, d_g, d_owner, ib.back(), d_colbits + 3 * (size_t)nc, ctx->num_sms, s)))
-        return bail(bcuda(ctx, e, "batch compress: length choice"));
+          (e = launch_choose_lengths(dt, d_g, d_owner, ib.back(), d_colbits + 3 * (size_t)nc, ctx->num_sms, s,
+                                     scratch, tdesc, terr)))
+        return release_pre(), bail(bcuda(ctx, e, "batch compress: length choice"));
     }
     unsigned long long choice_status = 0;
     if ((e = cudaMemcpyAsync(hbits.data(), d_colbits, sizeof(unsigned long long) * 3 * nc, cudaMemcpyDeviceToHost,
@@ -708,8 +795,9 @@ glc_status glc_batch_compress(glc_ctx* ctx, const glc_dtype* dtypes, const void*
         (e = cudaMemcpyAsync(&choice_status, d_colbits + 3 * (size_t)nc, sizeof(unsigned long long),
                              cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
         (e = cudaStreamSynchronize(s)) != cudaSuccess)
-      return bail(bcuda(ctx, e, "batch compress: sizes"));
-    if (choice_status != DEVERR_NONE) return bail(bfail(ctx, GLC_ERR_TIMEOUT, "batch compress: a device-side wait gave up"));
+      return release_pre(), bail(bcuda(ctx, e, "batch compress: sizes"));
+    if (choice_status != DEVERR_NONE)
+      return release_pre(), bail(bfail(ctx, GLC_ERR_TIMEOUT, "batch compress: a device-side wait gave up"));
     // the smallest compressed size; within 0.1 % of it, the length the tuner found to decode
     // fastest for the element type and the column's mean field width (when the table holds one)
     for (int i = 0; i < nc && fixed_partition_len == 0; i++) {
@@ -726,7 +814,9 @@ glc_status glc_batch_compress(glc_ctx* ctx, const glc_dtype* dtypes, const void*
         if (kCandidates[k] == tuned && size[k] * 1000 <= best * 1001) len[i] = tuned;
     }
     int64_t total = 0;
-    glc_status st = compress_one_pass(ctx, b, dtypes, values, ns, nc, len, hbits, s, &total);
+    glc_status st = compress_one_pass(ctx, b, dtypes, values, ns, nc, len, hbits, s, &total, pack ? &pre : nullptr,
+                                      pre_stats);
+    release_pre();  // what the place did not return (an error on the way)
     if (st == GLC_OK) st = finish_batch(ctx, b, s);
     if (st != GLC_OK) return bail(st);
     if (compressed_size_bytes) *compressed_size_bytes = total;

@@ -63,6 +63,8 @@ struct FixedCompressArgs {
   int64_t* tile_bits;         // per item: bits of the tile (nitems + 1 entries: the scan's input)
   const int64_t* tile_first;  // per item: exclusive scan of tile_bits over the launch (nitems + 1)
   unsigned long long* status; // DEVERR_* when a bounded wait gave up or a column's words overflow
+  PartDesc* tdesc;            // the length choice that also packs at 4096: per item, the tile's one
+  long long* terr;            // partition's descriptor (tile-relative offset) and max error
 };
 
 __device__ __forceinline__ void cf_sync() { asm volatile("bar.sync 1, %0;" ::"n"(kCfThreads) : "memory"); }
@@ -746,8 +748,11 @@ fixed_compress_kernel(const __grid_constant__ FixedCompressArgs a) {
 // while the compute warps measure the previous tile; every value's residual is measured against the
 // three lines that cover it (with the residual modes of fixed_compress_kernel), and the bits of each
 // candidate length are added into the column's choice_bits[0..2] (1024, 2048, 4096).  The widths
-// are the ones the compress at that length computes, so the column's size is exact.
-template <typename T> __global__ void __launch_bounds__(kCfFixCTA, 2)
+// are the ones the compress at that length computes, so the column's size is exact.  With PACK the
+// tile is also compressed at length 4096 -- the usual choice -- exactly as fixed_compress_kernel
+// would (the tile's line from the same exact sums, the same residual modes and packing): its words
+// into its slot, its descriptor and max error into tdesc / terr, its bits into tile_bits.
+template <typename T, bool PACK> __global__ void __launch_bounds__(kCfFixCTA, 2)
 choose_lengths_kernel(const __grid_constant__ FixedCompressArgs a) {
   constexpr int S = kCfChooseStages;
   extern __shared__ __align__(128) uint8_t smem[];
@@ -761,7 +766,7 @@ choose_lengths_kernel(const __grid_constant__ FixedCompressArgs a) {
   __shared__ long long s_ci[S][7];
   __shared__ int s_mode[S][7], s_len[S][7];
   __shared__ unsigned long long s_m[8][3];
-  __shared__ int s_ok;
+  __shared__ int s_ok, s_b0;
   if (threadIdx.x == 0) {
     for (int st = 0; st < S; st++) {
       mbar_init(&full[st], 1);
@@ -904,6 +909,9 @@ choose_lengths_kernel(const __grid_constant__ FixedCompressArgs a) {
     const T* x = reinterpret_cast<const T*>(smem + (size_t)st * cf_stage_bytes<T>() + s_shead[st]);
     const int qlen = (cnt - 1024 * q) < 0 ? 0 : ((cnt - 1024 * q) < 1024 ? (cnt - 1024 * q) : 1024);
     const T* xq = x + 1024 * q;
+    uint32_t fl[kCfPerThread];  // PACK: the low 32 bits of each value's residual against the tile's line
+#pragma unroll
+    for (int m = 0; m < kCfPerThread; m++) fl[m] = 0u;
     {  // max |residual| of each value against its quarter's, its half's and the tile's line
       const int ls[3] = {3 + q, 1 + (q >> 1), 0};
       const int off[3] = {0, 1024 * (q & 1), 1024 * q};
@@ -928,6 +936,7 @@ choose_lengths_kernel(const __grid_constant__ FixedCompressArgs a) {
               for (int c = 0; c < 3; c++) {
                 const double d = __dsub_rn(yc, __dadd_rz(__dadd_rn(__fma_rn(t1[c], xd[c], t0[c]), kHalfBias), kMagic));
                 dm[c] = fmax(dm[c], fabs(d));
+                if (PACK && c == 2) fl[m] = low_field(d);
               }
             }
 #pragma unroll
@@ -943,16 +952,17 @@ choose_lengths_kernel(const __grid_constant__ FixedCompressArgs a) {
             const T* xl = xq - off[c];
             const int rl = r + off[c], ll = qlen + off[c];
             const double t0 = s_t0[st][l], t1 = s_t1[st][l];
-            uint32_t fl[kCfPerThread];  // unused: only the maxima count here
+            uint32_t fd[kCfPerThread];  // the quarter's and the half's fields are not kept
+            uint32_t (&f)[kCfPerThread] = (PACK && c == 2) ? fl : fd;
             bool general = mode == CF_GENERAL;
             if (mode == CF_NONNEG) {
-              mx[c] = cf_resid_sign<T, false, false>(xl, rl, 64, ll, t0, t1, fl);
+              mx[c] = cf_resid_sign<T, false, false>(xl, rl, 64, ll, t0, t1, f);
             } else if (TypeTraits<T>::is_signed && mode == CF_NONPOS) {
-              mx[c] = cf_resid_sign<T, false, true>(xl, rl, 64, ll, t0, t1, fl);
+              mx[c] = cf_resid_sign<T, false, true>(xl, rl, 64, ll, t0, t1, f);
             } else if (sizeof(T) == 8 && mode == CF_OFFSET) {
-              general = !cf_resid_offset<T, false>(xl, rl, 64, ll, t0, t1, s_c[st][l], s_ci[st][l], fl, mx[c]);
+              general = !cf_resid_offset<T, false>(xl, rl, 64, ll, t0, t1, s_c[st][l], s_ci[st][l], f, mx[c]);
             }
-            if (general) mx[c] = cf_resid_general<T>(xl, rl, 64, ll, t0, t1, fl);
+            if (general) mx[c] = cf_resid_general<T>(xl, rl, 64, ll, t0, t1, f);
           }
         }
       }
@@ -979,8 +989,51 @@ choose_lengths_kernel(const __grid_constant__ FixedCompressArgs a) {
       }
       for (int c = 0; c < 3; c++)
         if (add[c]) atomicAdd(col.choice_bits + c, add[c]);
+      if (PACK) {  // the tile as one partition of 4096: its width, descriptor, max error and bits
+        unsigned long long m = 0;
+        for (int w = 0; w < 8; w++) m = s_m[w][2] > m ? s_m[w][2] : m;
+        const bool direct = s_mode[st][0] == CF_DIRECT;
+        const int b = direct ? (int)sizeof(T) * 8 : bits_for((long long)m);
+        PartDesc d;
+        d.theta0 = s_t0[st][0];
+        d.theta1 = s_t1[st][0];
+        d.bit_off = 0;
+        d.start = (int32_t)e0;
+        d.bits_type = (b & 0xff) | ((direct ? MODEL_DIRECT_COPY : MODEL_LINEAR) << 8);
+        a.tdesc[item] = d;
+        a.terr[item] = direct ? 0 : (long long)m;
+        a.tile_bits[item] = (int64_t)cnt * b;
+        if (b > 0) atomicMax(col.stats + 1, (unsigned long long)b);
+        s_b0 = b;
+      }
     }
-    cf_sync();  // every compute thread is done with stage st (and with s_m)
+    cf_sync();  // every compute thread is done with s_m (and, without PACK, with stage st)
+    if (PACK) {  // the tile's words at length 4096 into its slot (as fixed_compress_kernel)
+      const int b = s_b0;
+      uint8_t* stage = smem + (size_t)st * cf_stage_bytes<T>();
+      uint8_t* work = sizeof(T) == 8 ? stage : smem + (size_t)S * cf_stage_bytes<T>();
+      uint32_t* out = a.slots + item * a.slot_words;
+      if (b <= 31) {
+        uint32_t* fT = reinterpret_cast<uint32_t*>(work);
+        uint32_t* stg = fT + kFtWords;
+        uint32_t* fp = fT + lane * kFtStride + ((1024 * q + r) >> 5);  // position 1024 q + r + 64 m: j % 32 = lane
+#pragma unroll
+        for (int m = 0; m < kCfPerThread; m++) fp[2 * m] = fl[m];
+        cf_sync();
+        if (tid < ((cnt + 31) >> 5)) cf_pack_dispatch(b, fT + tid, stg, tid * b);
+        cf_sync();
+        const int nw = (int)(((long long)cnt * b + 31) >> 5);
+        for (int w = tid; w < nw; w += kCfThreads) out[w] = stg[w + (w >> 5)];
+      } else {
+        long long* res = sizeof(T) == 8 ? reinterpret_cast<long long*>(const_cast<T*>(x))
+                                        : reinterpret_cast<long long*>(work);
+        if (qlen > 0)
+          cf_store_resid<T>(x, res, 1024 * q + r, 64, cnt, s_mode[st][0], s_t0[st][0], s_t1[st][0]);
+        cf_sync();
+        cf_words_dispatch(b, res, cnt, out, tid);
+      }
+      cf_sync();  // every compute thread is done with stage st and the work area
+    }
     if (tid == 0) mbar_arrive(&empty[st]);
     if (item1 < 0) return;
   }
@@ -1006,6 +1059,7 @@ __global__ void __launch_bounds__(kPlaceThreads, 4) fixed_place_kernel(FixedComp
   const int tid = threadIdx.x, lane = tid & 31;
   for (int64_t item = blockIdx.x; item < a.nitems; item += gridDim.x) {
     const CfColumn& col = a.cols ? a.cols[a.owner ? a.owner[item] : 0] : a.single;
+    if (!col.words) continue;  // a column this launch does not place
     const int64_t t = item - col.item_base;
     const int64_t col_end = col.item_base + col.ntiles;  // the column's items are [item_base, col_end)
     const int64_t base = a.tile_first[col.item_base];
@@ -1017,7 +1071,13 @@ __global__ void __launch_bounds__(kPlaceThreads, 4) fixed_place_kernel(FixedComp
     const int np = (cnt + col.L - 1) / col.L;
     if (tid < np) {  // the tile's partitions: their metadata arrays from the descriptor
       const int64_t gp = t * col.parts_per_tile + tid;
-      PartDesc d = col.desc[gp];
+      PartDesc d;
+      if (a.tdesc) {  // packed by the length choice: the tile is one partition
+        d = a.tdesc[item];
+        col.err[gp] = a.terr[item];
+      } else {
+        d = col.desc[gp];
+      }
       const int64_t off = d.bit_off + first;
       const int len = (cnt - tid * col.L) < col.L ? (cnt - tid * col.L) : col.L;
       d.bit_off = off;
@@ -1158,42 +1218,51 @@ static cudaError_t launch_fixed_compress_dt(glc_dtype dt, const FixedCompressArg
   return cudaErrorInvalidValue;
 }
 
-template <typename T> static cudaError_t launch_choose_t(const FixedCompressArgs& a, int num_sms, cudaStream_t s) {
-  constexpr int smem = kCfChooseStages * cf_stage_bytes<T>();
+template <typename T, bool PACK> static cudaError_t launch_choose_t(const FixedCompressArgs& a, int num_sms, cudaStream_t s) {
+  constexpr int smem = PACK ? cf_fix_smem_bytes<T>(kCfChooseStages) : kCfChooseStages * cf_stage_bytes<T>();
   static PerDeviceFlag attr_set;
   const int dev = current_device();
   cudaError_t e;
   if (!attr_set.test(dev)) {
-    if ((e = cudaFuncSetAttribute(choose_lengths_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) !=
-        cudaSuccess)
+    if ((e = cudaFuncSetAttribute(choose_lengths_kernel<T, PACK>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  smem)) != cudaSuccess)
       return e;
     attr_set.set(dev);
   }
   int per_sm = 0;
-  if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, choose_lengths_kernel<T>, kCfFixCTA, smem)) !=
+  if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, choose_lengths_kernel<T, PACK>, kCfFixCTA, smem)) !=
       cudaSuccess)
     return e;
   if (per_sm < 1) per_sm = 1;
   int64_t grid = (int64_t)per_sm * num_sms;
   if (grid > a.nitems) grid = a.nitems;
   if (grid < 1) grid = 1;
-  choose_lengths_kernel<T><<<(unsigned)grid, kCfFixCTA, smem, s>>>(a);
+  choose_lengths_kernel<T, PACK><<<(unsigned)grid, kCfFixCTA, smem, s>>>(a);
   return cudaGetLastError();
 }
 
+static void carve(FixedCompressArgs& a, glc_dtype dt, void* scratch);
+
 cudaError_t launch_choose_lengths(glc_dtype dt, const CfColumn* cols, const int32_t* owner, int64_t nitems,
-                                  unsigned long long* status, int num_sms, cudaStream_t s) {
+                                  unsigned long long* status, int num_sms, cudaStream_t s, void* scratch,
+                                  PartDesc* tdesc, long long* terr) {
   if (nitems <= 0) return cudaSuccess;
   FixedCompressArgs a{};
   a.cols = cols;
   a.owner = owner;
   a.nitems = nitems;
   a.status = status;
+  const bool pack = scratch != nullptr;
+  if (pack) {
+    carve(a, dt, scratch);
+    a.tdesc = tdesc;
+    a.terr = terr;
+  }
   switch (dt) {
-    case GLC_I32: return launch_choose_t<int32_t>(a, num_sms, s);
-    case GLC_I64: return launch_choose_t<int64_t>(a, num_sms, s);
-    case GLC_U64: return launch_choose_t<uint64_t>(a, num_sms, s);
-    case GLC_U32: return launch_choose_t<uint32_t>(a, num_sms, s);
+    case GLC_I32: return pack ? launch_choose_t<int32_t, true>(a, num_sms, s) : launch_choose_t<int32_t, false>(a, num_sms, s);
+    case GLC_I64: return pack ? launch_choose_t<int64_t, true>(a, num_sms, s) : launch_choose_t<int64_t, false>(a, num_sms, s);
+    case GLC_U64: return pack ? launch_choose_t<uint64_t, true>(a, num_sms, s) : launch_choose_t<uint64_t, false>(a, num_sms, s);
+    case GLC_U32: return pack ? launch_choose_t<uint32_t, true>(a, num_sms, s) : launch_choose_t<uint32_t, false>(a, num_sms, s);
   }
   return cudaErrorInvalidValue;
 }
@@ -1312,6 +1381,27 @@ cudaError_t launch_fixed_place(glc_dtype dt, glc_column* c, int32_t L, void* scr
   a.status = stats + 2;
   carve(a, dt, scratch);
   return place_pass(a, c->ctx ? c->ctx->num_sms : 148, s);
+}
+
+// The columns packed at 4096 by launch_choose_lengths (same cols layout and owner list, same
+// scratch, tdesc and terr): the scan of the tiles' bits and the place of every column whose words
+// are set in cols (the others are skipped).
+cudaError_t launch_place_prepacked(glc_dtype dt, const CfColumn* cols, const int32_t* owner, int64_t nitems,
+                                   void* scratch, PartDesc* tdesc, long long* terr, unsigned long long* status,
+                                   int num_sms, cudaStream_t s) {
+  if (nitems <= 0) return cudaSuccess;
+  FixedCompressArgs a{};
+  a.cols = cols;
+  a.owner = owner;
+  a.nitems = nitems;
+  a.status = status;
+  a.tdesc = tdesc;
+  a.terr = terr;
+  carve(a, dt, scratch);
+  int64_t* first = const_cast<int64_t*>(a.tile_first);
+  cudaError_t e = exclusive_scan<int64_t>(a.tile_bits, first, a.nitems, first + a.nitems, first + a.nitems + 1, s);
+  if (e != cudaSuccess) return e;
+  return place_pass(a, num_sms, s);
 }
 
 // Many columns of one element type: cols (device, each with its own arrays, its exact word array

@@ -227,8 +227,15 @@ cudaError_t launch_fixed_compress_batch(glc_dtype dt, const CfColumn* cols, cons
                                         void* scratch, unsigned long long* status, int num_sms, cudaStream_t s);
 // The exact bits of every column of one element type at partition lengths 1024, 2048 and 4096
 // (added into each column's choice_bits, zeroed by the caller), in one read of the values.
+// With scratch (fixed_compress_scratch_bytes(dt, nitems)) the same pass also compresses every tile
+// at length 4096: its words into its slot, its descriptor and max error into tdesc / terr (nitems
+// each); launch_place_prepacked then places the columns that keep length 4096.
 cudaError_t launch_choose_lengths(glc_dtype dt, const CfColumn* cols, const int32_t* owner, int64_t nitems,
-                                  unsigned long long* status, int num_sms, cudaStream_t s);
+                                  unsigned long long* status, int num_sms, cudaStream_t s, void* scratch = nullptr,
+                                  PartDesc* tdesc = nullptr, long long* terr = nullptr);
+cudaError_t launch_place_prepacked(glc_dtype dt, const CfColumn* cols, const int32_t* owner, int64_t nitems,
+                                   void* scratch, PartDesc* tdesc, long long* terr, unsigned long long* status,
+                                   int num_sms, cudaStream_t s);
 cudaError_t launch_validate(const glc_column* c, int* d_bad, cudaStream_t s);
 cudaError_t launch_max_bits(const glc_column* c, int64_t* d_out, cudaStream_t s);
 // pack.cu: one column's arrays for the packer
