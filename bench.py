@@ -759,7 +759,7 @@ def run_batch(args):
         e1.record(stream)
         torch.cuda.synchronize(dev)
         batch_compress_ms = min(batch_compress_ms, e0.elapsed_time(e1))
-    for rep in range(3):
+    for rep in range(0 if args.no_loops else 3):
         if singles is not None:
             for sgl in singles:
                 sgl.free()
@@ -812,15 +812,17 @@ def run_batch(args):
     def loop():
         for col, p in zip(singles, ptrs.tolist()):
             glc.decompress_into(ctx, col, p, glc.SRC_PACKED, stream=sh)
-    loop()
-    torch.cuda.synchronize(dev)
-    e0.record(stream)
-    reps = max(1, min(args.steps, 5))
-    for _ in range(reps):
+    loop_ms = float("nan")
+    if not args.no_loops:
         loop()
-    e1.record(stream)
-    torch.cuda.synchronize(dev)
-    loop_ms = e0.elapsed_time(e1) / reps
+        torch.cuda.synchronize(dev)
+        e0.record(stream)
+        reps = max(1, min(args.steps, 5))
+        for _ in range(reps):
+            loop()
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        loop_ms = e0.elapsed_time(e1) / reps
     # end to end: batched decode + one device-to-host copy of every column into pinned memory
     h_out = torch.empty(o, dtype=torch.uint8).pin_memory()
     e0.record(stream)
@@ -840,9 +842,11 @@ def run_batch(args):
         "config": {"workload": f"batch_{args.columns}_columns_mixed", "columns": args.columns,
                    "raw_bytes": raw_bytes, "compressed_bytes": comp_bytes,
                    "compression_ratio": round(raw_bytes / comp_bytes, 3),
-                   "per_column_loop_ms": round(loop_ms, 3), "per_column_loop_gbs": round(raw_bytes / loop_ms / 1e6, 2),
-                   "speedup_vs_per_column_loop": round(loop_ms / ms, 2),
-                   "batch_compress_ms": round(batch_compress_ms, 2), "per_column_compress_loop_ms": round(loop_compress_ms, 2),
+                   "per_column_loop_ms": None if args.no_loops else round(loop_ms, 3),
+                   "per_column_loop_gbs": None if args.no_loops else round(raw_bytes / loop_ms / 1e6, 2),
+                   "speedup_vs_per_column_loop": None if args.no_loops else round(loop_ms / ms, 2),
+                   "batch_compress_ms": round(batch_compress_ms, 2),
+                   "per_column_compress_loop_ms": None if args.no_loops else round(loop_compress_ms, 2),
                    "batch_recompress_graph_ms": round(recompress_ms, 3),
                    "batch_recompress_gbs": round((raw_bytes + comp_bytes) / recompress_ms / 1e6, 1),
                    "compress_timing": "best of 3 calls each (CUDA events on the calling stream)",
@@ -856,7 +860,7 @@ def run_batch(args):
         "gpu_launches": args.steps, "clocks": clk, "cpu_baseline": None,
     }
     print(json.dumps(line), flush=True)
-    for sgl in singles:
+    for sgl in singles or []:
         sgl.free()
     batch.free()
     ctx.close()
@@ -1230,6 +1234,8 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--columns", type=int, default=4096, help="c4 batch: number of columns")
+    ap.add_argument("--no-loops", action="store_true",
+                    help="c4 batch: skip the per-column comparison loops (a short launch list for ncu)")
     ap.add_argument("--workload", default="c2_decode",
                     choices=["c1_plain", "c2_decode", "c3_random_access", "c4_batch", "c5_serving", "compress",
                              "decode_i32"],
