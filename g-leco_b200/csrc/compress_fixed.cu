@@ -68,6 +68,15 @@ struct FixedCompressArgs {
 };
 
 __device__ __forceinline__ void cf_sync() { asm volatile("bar.sync 1, %0;" ::"n"(kCfThreads) : "memory"); }
+// cf_sync that also returns whether any compute thread passed true.
+__device__ __forceinline__ bool cf_sync_or(bool v) {
+  uint32_t r;
+  asm volatile("{\n .reg .pred p, q;\n setp.ne.u32 q, %1, 0;\n bar.red.or.pred p, 1, %2, q;\n selp.u32 %0, 1, 0, p;\n}\n"
+               : "=r"(r)
+               : "r"((uint32_t)v), "n"(kCfThreads)
+               : "memory");
+  return r != 0;
+}
 
 // The producer lane of a launch: stages item blockIdx.x + k * gridDim.x of the work list into stage
 // k % S (its values, from the 16-byte block that holds the first one), with the item, its
@@ -474,7 +483,7 @@ fixed_compress_kernel(const __grid_constant__ FixedCompressArgs a) {
   __shared__ unsigned long long s_mx[kCfMaxSegs];
   __shared__ int s_b[kCfMaxParts];
   __shared__ int s_bl[kCfMaxParts + 1];
-  __shared__ int s_ok, s_fast;
+  __shared__ int s_ok;
 
   if (threadIdx.x == 0) {
     for (int st = 0; st < S; st++) {
@@ -627,6 +636,7 @@ fixed_compress_kernel(const __grid_constant__ FixedCompressArgs a) {
 
     // ---- B: residual of every value: its low 32 bits kept, max |residual| per partition ----
     uint32_t fl[kCfPerThread];
+    bool wide;
     {
       unsigned long long mx = 0;
 #pragma unroll
@@ -651,8 +661,10 @@ fixed_compress_kernel(const __grid_constant__ FixedCompressArgs a) {
       }
       mx = seg_max_u64(mx, W);
       if ((tid & (W - 1)) == 0) s_mx[seg] = mx;
+      // a width above 31 anywhere in the tile (a max |residual| of 2^30 or more, or direct copy)
+      wide = my_len > 0 && (s_mode[st][p_me] == CF_DIRECT || mx >= (1ull << 30));
     }
-    cf_sync();
+    wide = cf_sync_or(wide);
     if (tid < 32) {  // widths, tile-relative bit ranges (a warp scan), descriptors, the tile's bits
       const int p = lane;
       int b = 0, nb = 0;
@@ -691,15 +703,15 @@ fixed_compress_kernel(const __grid_constant__ FixedCompressArgs a) {
       }
       if (lane == 0) {
         s_bl[np] = total;
-        s_fast = bmax <= 31;
         a.tile_bits[item] = total;
         if (bmax > 0) atomicMax(col.stats + 1, (unsigned long long)bmax);
       }
     }
-    cf_sync();
+    // (the widths are not needed by the field writes or the residual recompute below: they run
+    // beside warp 0's section and one barrier covers both)
 
     uint32_t* out = a.slots + item * a.slot_words;
-    if (s_fast) {
+    if (!wide) {
       // ---- C (every width <= 31): fields transposed, one thread packs each 32-value group into
       // its `width` words (every partition starts on a word: L is a multiple of 32), staged, then
       // copied to the slot with coalesced stores ----
