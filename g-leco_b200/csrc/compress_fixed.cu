@@ -206,18 +206,55 @@ template <typename T> __device__ __forceinline__ double magic_of(T y) {
 }
 __device__ __forceinline__ uint32_t low_field(double d) { return (uint32_t)__double2loint(__dadd_rn(d, kMagic)); }
 
+__device__ __forceinline__ uint64_t madw_u(uint32_t a, uint32_t b, uint64_t c) {
+  uint64_t d;
+  asm("mad.wide.u32 %0, %1, %2, %3;" : "=l"(d) : "r"(a), "r"(b), "l"(c));
+  return d;
+}
+__device__ __forceinline__ int64_t madw_s(int32_t a, int32_t b, int64_t c) {
+  int64_t d;
+  asm("mad.wide.s32 %0, %1, %2, %3;" : "=l"(d) : "r"(a), "r"(b), "l"(c));
+  return d;
+}
+
+// The HalfSums of a thread's values y_m = xp[r + g m] (m < 16), without the index per value:
+// sum (r + g m) y_m = r sum y_m + g sum m y_m, each sum accumulated by one 32 x 32 -> 64-bit
+// multiply-add per value and half (m is a compile-time constant); every partial stays below 2^48.
 template <typename T, bool FULL>
 __device__ __forceinline__ void cf_sums(const T* __restrict__ xp, int r, int g, int len, HalfSums<T>& hs,
                                         uint32_t& flag) {
+  typedef typename HalfSums<T>::Acc Acc;
+  Acc s_lo = 0, s_hi = 0, t_lo = 0, t_hi = 0;
+  const T* p = xp + r;
 #pragma unroll
   for (int m = 0; m < kCfPerThread; m++) {
-    const int i = r + g * m;
-    if (FULL || i < len) {
-      const T y = xp[i];
-      hs.add(y, i);
+    if (FULL || r + g * m < len) {
+      const T y = p[g * m];
       value_flag<T>(flag, y);
+      if (sizeof(T) == 8) {
+        const uint32_t yl = (uint32_t)(uint64_t)y, yh = (uint32_t)((uint64_t)y >> 32);
+        s_lo = (Acc)madw_u(yl, 1u, (uint64_t)s_lo);
+        if (m) t_lo = (Acc)madw_u(yl, (uint32_t)m, (uint64_t)t_lo);
+        if (TypeTraits<T>::is_signed) {
+          s_hi = (Acc)madw_s((int32_t)yh, 1, (int64_t)s_hi);
+          if (m) t_hi = (Acc)madw_s((int32_t)yh, m, (int64_t)t_hi);
+        } else {
+          s_hi = (Acc)madw_u(yh, 1u, (uint64_t)s_hi);
+          if (m) t_hi = (Acc)madw_u(yh, (uint32_t)m, (uint64_t)t_hi);
+        }
+      } else if (TypeTraits<T>::is_signed) {
+        s_lo = (Acc)madw_s((int32_t)y, 1, (int64_t)s_lo);
+        if (m) t_lo = (Acc)madw_s((int32_t)y, m, (int64_t)t_lo);
+      } else {
+        s_lo = (Acc)madw_u((uint32_t)y, 1u, (uint64_t)s_lo);
+        if (m) t_lo = (Acc)madw_u((uint32_t)y, (uint32_t)m, (uint64_t)t_lo);
+      }
     }
   }
+  hs.s_lo += s_lo;
+  hs.s_hi += s_hi;
+  hs.x_lo += (Acc)r * s_lo + (Acc)g * t_lo;
+  hs.x_hi += (Acc)r * s_hi + (Acc)g * t_hi;
 }
 
 template <typename T, bool FULL, bool NEG>
