@@ -367,7 +367,7 @@ __device__ __forceinline__ void cf_pack_group(const uint32_t* __restrict__ fg, u
   }
 }
 
-__device__ __noinline__ void cf_pack_dispatch(int b, const uint32_t* __restrict__ fg, uint32_t* __restrict__ stg,
+__device__ __forceinline__ void cf_pack_dispatch(int b, const uint32_t* __restrict__ fg, uint32_t* __restrict__ stg,
                                               int o) {
   switch (b) {
 #define GLC_CF_PACK(B) \
@@ -470,7 +470,8 @@ __device__ __forceinline__ void cf_store_resid(const T* xp, long long* rp, int r
 // arithmetic, two divisions) runs beside the compute warps instead of between two of their
 // barriers.  Every wait is bounded.  The compress kernel runs two stages at three CTAs per SM (64
 // registers; measured 5 % faster than three stages at two CTAs per SM: other CTAs cover the load
-// of the next tile); the length choice, with heavier per-value work, three stages at two.
+// of the next tile); the length choice, with heavier per-value work, three stages at two (two
+// stages at three CTAs per SM fit its registers too, but measured 3 % slower).
 constexpr int kCfCompressStages = 2;
 constexpr int kCfChooseStages = 3;
 constexpr int kCfFixCTA = kCfThreads + 64;
