@@ -28,6 +28,8 @@ def _columns(ncols, seed=0, max_len=300_000):
         if dt in (glc.I32, glc.U32):
             slope = int(rng.integers(0, 400))
             v = (int(rng.integers(0, 1 << 20)) + slope * i + noise) % (1 << 31)
+            if c % 13 in (5, 8):  # unpredictable values: fields of 32-33 bits (the wide-field packing)
+                v = rng.integers(0, 1 << 31, n)
         else:
             slope = int(rng.integers(0, 10_000))
             v = int(rng.integers(0, 1 << 40)) + slope * i + noise
@@ -41,7 +43,7 @@ def _to_device(values):
     return torch.from_numpy(values.view(np.int64) if values.dtype.itemsize == 8 else values.view(np.int32)).cuda()
 
 
-@pytest.mark.parametrize("fixed_len", [0, 1024, 3000])
+@pytest.mark.parametrize("fixed_len", [0, 1024, 4096, 3000])
 def test_batch_compress_matches_single_column(oracle, fixed_len):
     ctx = glc.Context(0)
     cols = _columns(40, seed=fixed_len)
