@@ -1037,36 +1037,41 @@ choose_lengths_kernel(const __grid_constant__ FixedCompressArgs a) {
       }
     }
     cf_sync();
-    if (tid == 0) {
+    if (tid < 32) {  // lane l < 7: line l's width and bits; the three lengths' sums by shuffles
+      const int l = lane;
       unsigned long long add[3] = {0, 0, 0};
-      for (int l = 0; l < 7; l++) {
-        if (s_len[st][l] <= 0) continue;
+      int b_line = 0;
+      unsigned long long m_line = 0;
+      if (l < 7 && s_len[st][l] > 0) {
         const int c = l == 0 ? 2 : (l < 3 ? 1 : 0);                      // index into s_m's lines
         const int w0 = l == 0 ? 0 : (l < 3 ? 4 * (l - 1) : 2 * (l - 3));  // the line's warps
         const int w1 = l == 0 ? 8 : (l < 3 ? w0 + 4 : w0 + 2);
-        unsigned long long m = 0;
-        for (int w = w0; w < w1; w++) m = s_m[w][c] > m ? s_m[w][c] : m;
-        const int b = s_mode[st][l] == CF_DIRECT ? (int)sizeof(T) * 8 : bits_for((long long)m);
-        add[c] += (unsigned long long)s_len[st][l] * (unsigned long long)b;
+        for (int w = w0; w < w1; w++) m_line = s_m[w][c] > m_line ? s_m[w][c] : m_line;
+        b_line = s_mode[st][l] == CF_DIRECT ? (int)sizeof(T) * 8 : bits_for((long long)m_line);
+        add[c] = (unsigned long long)s_len[st][l] * (unsigned long long)b_line;
       }
+#pragma unroll
       for (int c = 0; c < 3; c++)
-        if (add[c]) atomicAdd(col.choice_bits + c, add[c]);
-      if (PACK) {  // the tile as one partition of 4096: its width, descriptor, max error and bits
-        unsigned long long m = 0;
-        for (int w = 0; w < 8; w++) m = s_m[w][2] > m ? s_m[w][2] : m;
-        const bool direct = s_mode[st][0] == CF_DIRECT;
-        const int b = direct ? (int)sizeof(T) * 8 : bits_for((long long)m);
-        PartDesc d;
-        d.theta0 = s_t0[st][0];
-        d.theta1 = s_t1[st][0];
-        d.bit_off = 0;
-        d.start = (int32_t)e0;
-        d.bits_type = (b & 0xff) | ((direct ? MODEL_DIRECT_COPY : MODEL_LINEAR) << 8);
-        a.tdesc[item] = d;
-        a.terr[item] = direct ? 0 : (long long)m;
-        a.tile_bits[item] = (int64_t)cnt * b;
-        if (b > 0) atomicMax(col.stats + 1, (unsigned long long)b);
-        s_b0 = b;
+#pragma unroll
+        for (int o = 4; o > 0; o >>= 1) add[c] += __shfl_xor_sync(FULL_MASK, add[c], o);  // lanes 0-7
+      if (lane == 0) {
+        for (int c = 0; c < 3; c++)
+          if (add[c]) atomicAdd(col.choice_bits + c, add[c]);
+        if (PACK) {  // the tile as one partition of 4096 (line 0): width, descriptor, max error, bits
+          const bool direct = s_mode[st][0] == CF_DIRECT;
+          const int b = b_line;
+          PartDesc d;
+          d.theta0 = s_t0[st][0];
+          d.theta1 = s_t1[st][0];
+          d.bit_off = 0;
+          d.start = (int32_t)e0;
+          d.bits_type = (b & 0xff) | ((direct ? MODEL_DIRECT_COPY : MODEL_LINEAR) << 8);
+          a.tdesc[item] = d;
+          a.terr[item] = direct ? 0 : (long long)m_line;
+          a.tile_bits[item] = (int64_t)cnt * b;
+          if (b > 0) atomicMax(col.stats + 1, (unsigned long long)b);
+          s_b0 = b;
+        }
       }
     }
     cf_sync();  // every compute thread is done with s_m (and, without PACK, with stage st)
