@@ -382,57 +382,27 @@ __device__ __forceinline__ void cf_pack_dispatch(int b, const uint32_t* __restri
   }
 }
 
-// Word w of a partition of width B (1..64) whose exact residuals are rp[0, len): the tile-relative
-// bits [32 w, 32 w + 32) of its fields, from the field holding bit 32 w and the ceil(31 / B) after
-// it at most (fields past len are zero).  One thread per word, B known at compile time.
-template <int B>
-__device__ __forceinline__ void cf_words(const long long* rp, int len, int nwp, uint32_t* __restrict__ out, int tid) {
-  constexpr int kMore = (31 + B - 1) / B;
-  for (int w = tid; w < nwp; w += kCfThreads) {
-    int j = (32 * w) / B;
-    const int s = 32 * w - j * B;
-    if (B <= 32) {
-      constexpr uint32_t kMask = B >= 32 ? 0xffffffffu : ((1u << (B & 31)) - 1u);
-      const uint32_t* r32 = reinterpret_cast<const uint32_t*>(rp);  // low half of residual j at 2 j
-      uint32_t v = (r32[2 * j] & kMask) >> s;
-      int have = B - s;
-#pragma unroll
-      for (int e = 0; e < kMore; e++) {
-        if (have < 32) {
-          ++j;
-          if (j < len) v |= (r32[2 * j] & kMask) << have;
-          have += B;
-        }
-      }
-      out[w] = v;
-    } else {
-      constexpr uint64_t kMask = B >= 64 ? ~0ull : ((1ull << (B & 63)) - 1ull);
-      uint64_t v = ((uint64_t)rp[j] & kMask) >> s;
-      if (B - s < 32 && j + 1 < len) v |= ((uint64_t)rp[j + 1] & kMask) << (B - s);
-      out[w] = (uint32_t)v;
-    }
-  }
-}
-
+// The words of a partition of width b (1..64) whose exact residuals are rp[0, len), one thread per
+// word: word w holds the partition's bits [32 w, 32 w + 32), from the field holding bit 32 w and
+// the following ones (fields past len are zero).  One routine for every width (the wide-field path
+// is taken by a few tiles; a copy per width made the kernels' code several times larger than the
+// instruction cache).
 __device__ __noinline__ void cf_words_dispatch(int b, const long long* rp, int len, uint32_t* __restrict__ out,
                                                int tid) {
+  if (b <= 0) return;
   const int nwp = (int)(((long long)len * b + 31) >> 5);
-  switch (b) {
-#define GLC_CF_WORDS(B) \
-  case B: cf_words<B>(rp, len, nwp, out, tid); break;
-    GLC_CF_WORDS(1) GLC_CF_WORDS(2) GLC_CF_WORDS(3) GLC_CF_WORDS(4) GLC_CF_WORDS(5) GLC_CF_WORDS(6)
-    GLC_CF_WORDS(7) GLC_CF_WORDS(8) GLC_CF_WORDS(9) GLC_CF_WORDS(10) GLC_CF_WORDS(11) GLC_CF_WORDS(12)
-    GLC_CF_WORDS(13) GLC_CF_WORDS(14) GLC_CF_WORDS(15) GLC_CF_WORDS(16) GLC_CF_WORDS(17) GLC_CF_WORDS(18)
-    GLC_CF_WORDS(19) GLC_CF_WORDS(20) GLC_CF_WORDS(21) GLC_CF_WORDS(22) GLC_CF_WORDS(23) GLC_CF_WORDS(24)
-    GLC_CF_WORDS(25) GLC_CF_WORDS(26) GLC_CF_WORDS(27) GLC_CF_WORDS(28) GLC_CF_WORDS(29) GLC_CF_WORDS(30)
-    GLC_CF_WORDS(31) GLC_CF_WORDS(32) GLC_CF_WORDS(33) GLC_CF_WORDS(34) GLC_CF_WORDS(35) GLC_CF_WORDS(36)
-    GLC_CF_WORDS(37) GLC_CF_WORDS(38) GLC_CF_WORDS(39) GLC_CF_WORDS(40) GLC_CF_WORDS(41) GLC_CF_WORDS(42)
-    GLC_CF_WORDS(43) GLC_CF_WORDS(44) GLC_CF_WORDS(45) GLC_CF_WORDS(46) GLC_CF_WORDS(47) GLC_CF_WORDS(48)
-    GLC_CF_WORDS(49) GLC_CF_WORDS(50) GLC_CF_WORDS(51) GLC_CF_WORDS(52) GLC_CF_WORDS(53) GLC_CF_WORDS(54)
-    GLC_CF_WORDS(55) GLC_CF_WORDS(56) GLC_CF_WORDS(57) GLC_CF_WORDS(58) GLC_CF_WORDS(59) GLC_CF_WORDS(60)
-    GLC_CF_WORDS(61) GLC_CF_WORDS(62) GLC_CF_WORDS(63) GLC_CF_WORDS(64)
-#undef GLC_CF_WORDS
-    default: break;  // width 0: no words
+  const uint32_t mb = 0xffffffffu / (uint32_t)b + 1u;  // 32 w / b by a multiply-high (32 w < 2^18)
+  const uint64_t mask = b >= 64 ? ~0ull : ((1ull << b) - 1ull);
+  for (int w = tid; w < nwp; w += kCfThreads) {
+    int j = b > 1 ? (int)__umulhi((uint32_t)(32 * w), mb) : 32 * w;
+    const int s = 32 * w - j * b;
+    uint64_t v = ((uint64_t)rp[j] & mask) >> s;
+    int have = b - s;
+    while (have < 32 && ++j < len) {
+      v |= ((uint64_t)rp[j] & mask) << have;
+      have += b;
+    }
+    out[w] = (uint32_t)v;
   }
 }
 
