@@ -29,6 +29,7 @@ struct glc_batch {
   glc_ctx* ctx = nullptr;
   std::vector<glc_column*> cols;  // views into `storage` when the batch compressed them
   bool owns_columns = false;
+  glc_column* col_block = nullptr;  // the owned columns, when allocated as one array
   std::vector<void*> storage;     // device allocations owned by the batch
   BatchColumn* d_cols = nullptr;
   int max_bits = 0;
@@ -295,8 +296,9 @@ template <typename V> cudaError_t dalloc(glc_batch* b, V** p, size_t count) {
 void free_batch(glc_batch* b) {
   if (b->graph) cudaGraphExecDestroy(b->graph);
   if (b->re_graph) cudaGraphExecDestroy(b->re_graph);
-  if (b->owns_columns)
-    for (glc_column* c : b->cols) delete c;  // views: their arrays are in storage
+  if (b->col_block) delete[] b->col_block;  // views: their arrays are in storage
+  else if (b->owns_columns)
+    for (glc_column* c : b->cols) delete c;
   for (void* q : b->storage) cudaFreeAsync(q, b->ctx->own_stream);
   if (!b->storage.empty()) cudaStreamSynchronize(b->ctx->own_stream);
   if (b->d_cols) cudaFree(b->d_cols);
@@ -379,31 +381,30 @@ struct PrePacked {
   long long* terr = nullptr;
 };
 
-glc_status compress_one_pass(glc_ctx* ctx, glc_batch* b, const glc_dtype* dtypes, const void* const* values,
-                             const int64_t* ns, int nc, const std::vector<int32_t>& len,
-                             const std::vector<unsigned long long>& hbits, cudaStream_t s, int64_t* total_size,
-                             std::vector<PrePacked>* pre, unsigned long long* pre_stats) {
-  std::vector<int64_t> pb(nc + 1, 0), wb(nc + 1, 0), eb(nc + 1, 0);
-  std::vector<glc_column*> cols(nc, nullptr);
+// What the one-pass batched compress sets up before the lengths are known (so that it overlaps the
+// length choice on the device): the columns, their partition arrays sized for the shortest
+// candidate length (a column's arrays are a prefix of its region), the decode tables, the status
+// words, and each column's launch-table entry without its length-dependent fields.
+struct OnePassPrep {
+  std::vector<CfColumn> hc;
+  unsigned long long* stats = nullptr;  // 2 per column, then the status word
+};
+
+glc_status prepare_one_pass(glc_ctx* ctx, glc_batch* b, const glc_dtype* dtypes, const void* const* values,
+                            const int64_t* ns, int nc, int32_t shortest_len, cudaStream_t s, OnePassPrep* prep) {
+  std::vector<int64_t> pb(nc + 1, 0), eb(nc + 1, 0);
+  glc_column* block = new (std::nothrow) glc_column[nc > 0 ? nc : 1];
+  if (!block) return GLC_ERR_OOM;
+  b->col_block = block;
   for (int i = 0; i < nc; i++) {
-    glc_column* c = new (std::nothrow) glc_column();
-    if (!c) return GLC_ERR_OOM;
-    cols[i] = c;
+    glc_column* c = block + i;
     b->cols.push_back(c);
     c->ctx = ctx;
     c->view = true;
     c->dtype = dtypes[i];
     c->n = ns[i];
-    c->fixed_len = len[i];
-    c->P = c->n > 0 ? (c->n + len[i] - 1) / len[i] : 0;
-    const int k = len[i] == 1024 ? 0 : (len[i] == 2048 ? 1 : 2);
-    c->total_bits = c->n > 0 ? (int64_t)hbits[3 * (size_t)i + k] : 0;
-    c->nwords = (c->total_bits + 31) / 32;
-    c->nwords_alloc = ((c->nwords + 3) & ~3ll) + 8;
     c->ntiles = (c->n + kDecodeTile - 1) / kDecodeTile;
-    c->reported_size = c->n ? 64 * c->P + 120 + (c->total_bits + 7) / 8 : 0;  // api/G-LeCo.cuh:589-603
-    pb[i + 1] = pb[i] + c->P;
-    wb[i + 1] = wb[i] + c->nwords_alloc;
+    pb[i + 1] = pb[i] + (c->n > 0 ? (c->n + shortest_len - 1) / shortest_len : 0);
     eb[i + 1] = eb[i] + (c->n ? c->ntiles + 1 : 0);
   }
   const int64_t P = pb[nc];
@@ -411,19 +412,19 @@ glc_status compress_one_pass(glc_ctx* ctx, glc_batch* b, const glc_dtype* dtypes
   double* params;
   int64_t *offs, *errs;
   PartDesc* desc;
-  uint32_t* words;
   TileInfo* tiles;
-  unsigned long long* stats;  // 2 per column, then the status word
+  unsigned long long* stats;
   cudaError_t e;
   if ((e = dalloc(b, &starts, P)) || (e = dalloc(b, &ends, P)) || (e = dalloc(b, &types, P)) ||
       (e = dalloc(b, &bits, P)) || (e = dalloc(b, &params, 4 * P)) || (e = dalloc(b, &offs, P)) ||
-      (e = dalloc(b, &errs, P)) || (e = dalloc(b, &desc, P)) || (e = dalloc(b, &words, wb[nc])) ||
-      (e = dalloc(b, &tiles, eb[nc])) || (e = dalloc(b, &stats, 2 * (size_t)nc + 1)))
+      (e = dalloc(b, &errs, P)) || (e = dalloc(b, &desc, P)) || (e = dalloc(b, &tiles, eb[nc])) ||
+      (e = dalloc(b, &stats, 2 * (size_t)nc + 1)))
     return bcuda(ctx, e, "batch compress: allocation");
   BCK(cudaMemsetAsync(stats, 0, sizeof(unsigned long long) * (2 * (size_t)nc + 1), s), "batch compress: stats");
-  std::vector<CfColumn> hc(nc);
+  prep->stats = stats;
+  prep->hc.assign(nc, CfColumn{});
   for (int i = 0; i < nc; i++) {
-    glc_column* c = cols[i];
+    glc_column* c = block + i;
     const int64_t p0 = pb[i];
     c->d_start = starts + p0;
     c->d_end = ends + p0;
@@ -433,18 +434,11 @@ glc_status compress_one_pass(glc_ctx* ctx, glc_batch* b, const glc_dtype* dtypes
     c->d_offs = offs + p0;
     c->d_err = errs + p0;
     c->d_desc = desc + p0;
-    c->d_words = words + wb[i];
     c->d_tiles = tiles + eb[i];
-    CfColumn& f = hc[i];
-    f = CfColumn{};
+    CfColumn& f = prep->hc[i];
     f.values = values[i];
     f.n = c->n;
-    f.L = len[i];
-    f.parts_per_tile = kDecodeTile / len[i];
-    f.P = c->P;
     f.ntiles = c->ntiles;
-    f.nwords_alloc = c->nwords_alloc;
-    f.words_cap = c->nwords_alloc;
     f.starts = c->d_start;
     f.ends = c->d_end;
     f.types = c->d_types;
@@ -454,8 +448,44 @@ glc_status compress_one_pass(glc_ctx* ctx, glc_batch* b, const glc_dtype* dtypes
     f.err = c->d_err;
     f.desc = c->d_desc;
     f.tiles = c->d_tiles;
-    f.words = c->d_words;
     f.stats = stats + 2 * i;
+  }
+  return GLC_OK;
+}
+
+glc_status compress_one_pass(glc_ctx* ctx, glc_batch* b, const glc_dtype* dtypes, const void* const* values,
+                             const int64_t* ns, int nc, const std::vector<int32_t>& len,
+                             const std::vector<unsigned long long>& hbits, cudaStream_t s, int64_t* total_size,
+                             std::vector<PrePacked>* pre, unsigned long long* pre_stats, OnePassPrep& prep) {
+  (void)values;
+  std::vector<int64_t> wb(nc + 1, 0);
+  for (int i = 0; i < nc; i++) {  // the length-dependent fields
+    glc_column* c = b->cols[i];
+    c->fixed_len = len[i];
+    c->P = c->n > 0 ? (c->n + len[i] - 1) / len[i] : 0;
+    const int k = len[i] == 1024 ? 0 : (len[i] == 2048 ? 1 : 2);
+    c->total_bits = c->n > 0 ? (int64_t)hbits[3 * (size_t)i + k] : 0;
+    c->nwords = (c->total_bits + 31) / 32;
+    c->nwords_alloc = ((c->nwords + 3) & ~3ll) + 8;
+    c->reported_size = c->n ? 64 * c->P + 120 + (c->total_bits + 7) / 8 : 0;  // api/G-LeCo.cuh:589-603
+    wb[i + 1] = wb[i] + c->nwords_alloc;
+  }
+  uint32_t* words;
+  cudaError_t e;
+  if ((e = dalloc(b, &words, wb[nc])) != cudaSuccess) return bcuda(ctx, e, "batch compress: allocation");
+  unsigned long long* stats = prep.stats;
+  std::vector<CfColumn>& hc = prep.hc;
+  std::vector<glc_column*> cols(b->cols.begin(), b->cols.end());
+  for (int i = 0; i < nc; i++) {
+    glc_column* c = cols[i];
+    c->d_words = words + wb[i];
+    CfColumn& f = hc[i];
+    f.L = len[i];
+    f.parts_per_tile = kDecodeTile / len[i];
+    f.P = c->P;
+    f.nwords_alloc = c->nwords_alloc;
+    f.words_cap = c->nwords_alloc;
+    f.words = c->d_words;
   }
   // a column the length choice already packed (it keeps length 4096) is only placed
   std::vector<char> prepacked(nc, 0);
@@ -789,6 +819,13 @@ glc_status glc_batch_compress(glc_ctx* ctx, const glc_dtype* dtypes, const void*
                                      scratch, tdesc, terr)))
         return release_pre(), bail(bcuda(ctx, e, "batch compress: length choice"));
     }
+    // everything that does not depend on the lengths, while the choice runs on the device
+    OnePassPrep prep;
+    {
+      const glc_status ps = prepare_one_pass(ctx, b, dtypes, values, ns, nc,
+                                             fixed_partition_len ? fixed_partition_len : kCandidates[0], s, &prep);
+      if (ps != GLC_OK) return release_pre(), bail(ps);
+    }
     unsigned long long choice_status = 0;
     if ((e = cudaMemcpyAsync(hbits.data(), d_colbits, sizeof(unsigned long long) * 3 * nc, cudaMemcpyDeviceToHost,
                              s)) != cudaSuccess ||
@@ -815,7 +852,7 @@ glc_status glc_batch_compress(glc_ctx* ctx, const glc_dtype* dtypes, const void*
     }
     int64_t total = 0;
     glc_status st = compress_one_pass(ctx, b, dtypes, values, ns, nc, len, hbits, s, &total, pack ? &pre : nullptr,
-                                      pre_stats);
+                                      pre_stats, prep);
     release_pre();  // what the place did not return (an error on the way)
     if (st == GLC_OK) st = finish_batch(ctx, b, s);
     if (st != GLC_OK) return bail(st);
