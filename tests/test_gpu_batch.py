@@ -78,6 +78,41 @@ def test_batch_compress_matches_single_column(oracle, fixed_len):
     batch.free()
 
 
+def _mode_columns(n=150_001, seed=5):
+    """Columns whose residuals take each arithmetic form of the compress kernels: predictions
+    above 2^51 (nanosecond timestamps), non-positive lines, lines through zero, uint64 values at
+    and just above 2^53 (tiles kept in the line form and tiles copied), 32-bit extremes."""
+    rng = np.random.default_rng(seed)
+    i = np.arange(n, dtype=np.int64)
+    ns = (1_700_000_000_000_000_000 + np.cumsum(rng.integers(900_000, 1_100_000, n))).astype(np.int64)
+    down = (-10 ** 12 - np.cumsum(rng.integers(0, 100_000, n))).astype(np.int64)
+    cross = (-(n // 2) * 37 + 37 * i + rng.integers(-300, 300, n)).astype(np.int64)
+    edge = (np.uint64(2 ** 53) - np.uint64(n)) + i.astype(np.uint64) * np.uint64(2)
+    edge[:4096] = np.minimum(edge[:4096], np.uint64(2 ** 53))
+    edge[4095] = np.uint64(2 ** 53)
+    high = (np.uint64(1) << np.uint64(51)) + i.astype(np.uint64) * np.uint64(1_000_003)
+    i32 = rng.integers(np.iinfo(np.int32).min, np.iinfo(np.int32).max, n, dtype=np.int64).astype(np.int32)
+    u32 = (np.uint32(0xFFFFFFF0) - (i % 7).astype(np.uint32)).astype(np.uint32)
+    return [(glc.I64, ns), (glc.I64, down), (glc.I64, cross), (glc.U64, edge), (glc.U64, high), (glc.I32, i32),
+            (glc.U32, u32), (glc.U64, ns.view(np.uint64)), (glc.I64, cross[: 4096 * 3 + 11])]
+
+
+@pytest.mark.parametrize("fixed_len", [0, 4096, 256])
+def test_batch_compress_residual_forms(oracle, fixed_len):
+    ctx = glc.Context(0)
+    cols = _mode_columns()
+    dev = [_to_device(v) for _, v in cols]
+    batch = glc.Batch.compress(ctx, [d for d, _ in cols], [t.data_ptr() for t in dev], [len(v) for _, v in cols],
+                               fixed_len=fixed_len)
+    for (dt, v), bc in zip(cols, batch.columns):
+        L = bc.info().fixed_partition_len
+        if not fixed_len:
+            sizes = [oracle.compress(v, "fixed", cand).reported_size() for cand in (1024, 2048, 4096)]
+            assert L == (1024, 2048, 4096)[int(np.argmin(sizes))], (L, sizes)
+        assert glc.serialize_host(ctx, bc) == oracle.serialize(oracle.compress(v, "fixed", L))
+    batch.free()
+
+
 @pytest.mark.parametrize("use_graph", [False, True])
 def test_batch_decode(use_graph):
     ctx = glc.Context(0)

@@ -61,6 +61,21 @@ def _data(kind: str, n: int, seed: int = 1):
                 v[pos:pos + run] = 12345 * np.arange(len(seg)) + rng.integers(0, 1 << w, len(seg))
             pos += run
         return v
+    if kind == "i64_ns":  # nanosecond timestamps near 2^60: predictions far above 2^51 (offset residuals)
+        return (1_700_000_000_000_000_000 + np.cumsum(rng.integers(900_000, 1_100_000, n))).astype(np.int64)
+    if kind == "u64_high":  # a smooth line in [2^51, 2^52]
+        return ((np.uint64(1) << np.uint64(51)) + i.astype(np.uint64) * np.uint64(1_000_003)
+                + rng.integers(0, 1 << 16, n).astype(np.uint64))
+    if kind == "u64_2p53":  # values across 2^53: some tiles hold 2^53 itself (not copied), some 2^53 + 1 (copied)
+        v = (np.uint64(2 ** 53) - np.uint64(n)) + i.astype(np.uint64) * np.uint64(2)
+        for t0 in range(0, n, 4096 * 3):
+            v[t0:t0 + 4096] = np.minimum(v[t0:t0 + 4096], np.uint64(2 ** 53))
+            v[min(t0 + 4095, n - 1)] = np.uint64(2 ** 53)
+        return v
+    if kind == "i64_negwalk":  # a falling line of negative values (non-positive predictions)
+        return (-10 ** 12 - np.cumsum(rng.integers(0, 100_000, n))).astype(np.int64)
+    if kind == "i64_cross":  # lines crossing zero
+        return (-(n // 2) * 37 + 37 * i + rng.integers(-300, 300, n)).astype(np.int64)
     if kind == "u32_extreme":
         v = rng.integers(0, 2 ** 32, n, dtype=np.int64).astype(np.uint32)
         v[:: 3] = np.iinfo(np.uint32).max
@@ -70,7 +85,7 @@ def _data(kind: str, n: int, seed: int = 1):
 
 
 KINDS = ["i32_linear", "i32_neg", "i64_walk", "i64_extreme", "u64_piecewise", "u64_big", "u32_noise", "u32_const",
-         "timestamps", "i64_runs"]
+         "timestamps", "i64_runs", "i64_ns", "u64_high", "u64_2p53", "i64_negwalk", "i64_cross"]
 
 
 def _codec(values):
