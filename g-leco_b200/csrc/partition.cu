@@ -41,6 +41,7 @@ constexpr int kMaxJumpBlocks = 29;  // 3712 / 128
 constexpr int kRangeBlocks = 1024;
 constexpr int kMaxMergeRounds = 64;
 constexpr int kPairChunk = 4096;
+constexpr int32_t kUnknown = -1;  // best end of a start not evaluated
 
 struct SumPair {  // trivially constructible: SumPair() value-initialises to zero
   i128 y;
@@ -104,8 +105,27 @@ __device__ __forceinline__ double part_cost(int64_t len, int bits) {
 // range known at compile time, no per-candidate test.  Used when all 14 candidates exist and every
 // prediction is >= -0.25 (so round-half-away is trunc(x + 0.5 - 2^-54) with a constant addend)
 // and the values are below 2^51: all quantities are exact integers in FP64.
-template <int B, typename T>
-__device__ __forceinline__ void split_bands(const T* __restrict__ v, int64_t s, int lane, const double (*th)[2],
+// A value of the start's reach: from global memory (read-only path) or from the warp's staged copy.
+template <bool SMEM, typename T> __device__ __forceinline__ T ld_val(const T* p) {
+  if constexpr (SMEM) return *p;
+  else return __ldg(p);
+}
+
+// Copies vals[0, count) to win[0, count) with asynchronous copies (cp.async, element-sized, so any
+// element-aligned input works); the caller waits with cp_async_wait_all + __syncwarp.
+template <typename T>
+__device__ __forceinline__ void stage_reach(const T* __restrict__ vals, T* win, int count, int lane) {
+  for (int o = lane; o < count; o += 32) {
+    const uint32_t dst = (uint32_t)__cvta_generic_to_shared(win + o);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(dst), "l"(vals + o), "n"((int)sizeof(T))
+                 : "memory");
+  }
+  asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+template <int B, bool SMEM, typename T>
+__device__ __forceinline__ void split_bands(const T* __restrict__ vs, int lane, const double (*th)[2],
                                             double (&md)[kNumSizes], bool& vals_ok) {
   if constexpr (B < kNumSizes) {
     constexpr int lo = B == 0 ? 0 : split_size(B - 1), hi = split_size(B);
@@ -113,7 +133,7 @@ __device__ __forceinline__ void split_bands(const T* __restrict__ v, int64_t s, 
     double od = (double)(lo + lane);
 #pragma unroll 2
     for (int o0 = lo; o0 < hi; o0 += 32, od += 32.0) {
-      const T y = __ldg(v + s + o0 + lane);
+      const T y = ld_val<SMEM>(vs + o0 + lane);
       vals_ok &= TypeTraits<T>::is_signed ? ((long long)y > -(1ll << 51) && (long long)y < (1ll << 51))
                                           : ((uint64_t)y < (1ull << 51));
       // yd + 2^52 (exact for |y| < 2^51); with predictions >= -0.25 the truncation is the sum
@@ -126,25 +146,60 @@ __device__ __forceinline__ void split_bands(const T* __restrict__ v, int64_t s, 
         md[k] = fmax(md[k], fabs(__dsub_rn(yc, m)));
       }
     }
-    split_bands<B + 1, T>(v, s, lane, th, md, vals_ok);
+    split_bands<B + 1, SMEM, T>(vs, lane, th, md, vals_ok);
   }
 }
 
 
-template <typename T> __global__ void __launch_bounds__(256)
-split_kernel(const T* __restrict__ v, RangeSums rs, int32_t* __restrict__ nb_next) {
-  __shared__ __align__(16) double s_th[8][kNumSizes][2];
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int64_t j = (int64_t)blockIdx.x * 8 + warp;
-  if (j >= rs.nb) return;
+// The same band loops for 8-byte values beyond 2^51, measured from an offset: with every
+// prediction argument x in [2^51, 2^62] (a multiple of 0.5 there, and no saturation) and within
+// 2^50 of the integer d = c, and every value within 2^50 of c, the prediction is
+// round_half_away(x) = floor(x + 0.5) (trunc(x + 0.5 - 2^-54) at a spacing of 0.5 or more), so
+// pred - c = floor((x - d) + 0.5), where x - d and the + 0.5 are exact and the floor is the sum
+// with 1.5 * 2^52 rounded down; y - c is an exact 64-bit difference below 2^50.
+template <int B, bool SMEM, typename T>
+__device__ __forceinline__ void split_bands_off(const T* __restrict__ vs, int lane, const double (*th)[2], double d,
+                                                long long c, double (&md)[kNumSizes], bool& vals_ok) {
+  if constexpr (B < kNumSizes) {
+    constexpr int lo = B == 0 ? 0 : split_size(B - 1), hi = split_size(B);
+    constexpr double kM = 6755399441055744.0;  // 1.5 * 2^52
+    double od = (double)(lo + lane);
+#pragma unroll 2
+    for (int o0 = lo; o0 < hi; o0 += 32, od += 32.0) {
+      const long long yv = (long long)ld_val<SMEM>(vs + o0 + lane);
+      const long long dy = yv - c;  // no overflow: c in [2^51, 2^62], checked values >= 0
+      vals_ok &= yv >= 0 && dy > -(1ll << 50) && dy < (1ll << 50);
+      const double yc = __dadd_rn((double)dy, kM);
+#pragma unroll
+      for (int k = B; k < kNumSizes; k++) {
+        const double2 t = *reinterpret_cast<const double2*>(th[k]);
+        const double x = __fma_rn(t.y, od, t.x);
+        const double m = __dadd_rd(__dadd_rn(__dsub_rn(x, d), 0.5), kM);
+        md[k] = fmax(md[k], fabs(__dsub_rn(yc, m)));
+      }
+    }
+    split_bands_off<B + 1, SMEM, T>(vs, lane, th, d, c, md, vals_ok);
+  }
+}
+
+// Best end (as a block index; nb for the end of the column) of the start at block j.  One warp:
+// every lane takes part and returns the same result; th is the warp's own table of lines.  SMEM:
+// the start's reach (up to 3712 values) is first copied to win (the warp's own buffer) with all
+// copies in flight at once, for walks where one warp evaluates starts one after another.
+template <typename T, bool SMEM>
+__device__ __forceinline__ int32_t split_best_block(const T* __restrict__ v, const RangeSums& rs, int64_t j, int lane,
+                                                    double (*th)[2], T* win) {
   const int64_t s = j * kMinPart;
   const int64_t max_size = (rs.n - s < kMinPart * 32) ? rs.n - s : kMinPart * 32;
   int ncand = 0;
 #pragma unroll
   for (int k = 0; k < kNumSizes; k++) ncand += (c_sizes[k] <= max_size) ? 1 : 0;
-  if (ncand == 0) {  // fewer than 128 values left: the rest is one partition
-    if (lane == 0) nb_next[j] = (int32_t)rs.nb;
-    return;
+  if (ncand == 0) return (int32_t)rs.nb;  // fewer than 128 values left: the rest is one partition
+  __syncwarp();  // the previous start's lines and values are no longer read
+  const T* vs = v + s;
+  if constexpr (SMEM) {
+    stage_reach<T>(v + s, win, c_sizes[ncand - 1], lane);
+    vs = win;
   }
   // Fast path: when every value of the start's reach and every candidate's prediction (checked
   // at both ends of the candidate: fma(theta1, o, theta0) is monotone in o) lie well inside
@@ -156,15 +211,18 @@ split_kernel(const T* __restrict__ v, RangeSums rs, int32_t* __restrict__ nb_nex
   const double lo_ok = TypeTraits<T>::is_signed ? (sizeof(T) == 4 ? -2147483647.0 : -kSafe) : -0.25;
   const double hi_ok = sizeof(T) == 4 ? (TypeTraits<T>::is_signed ? 2147483646.0 : 4294967294.0) : kSafe;
   bool cand_ok = true, cand_nonneg = true;
+  double xa = 0.0, xb = 0.0;  // each candidate's prediction argument at its two ends
   if (lane < ncand) {
     double t0, t1;
     rs.line(s, s + c_sizes[lane], t0, t1);
-    s_th[warp][lane][0] = t0;
-    s_th[warp][lane][1] = t1;
-    const double xa = t0, xb = __fma_rn(t1, (double)(c_sizes[lane] - 1), t0);
+    th[lane][0] = t0;
+    th[lane][1] = t1;
+    xa = t0;
+    xb = __fma_rn(t1, (double)(c_sizes[lane] - 1), t0);
     cand_ok = xa >= lo_ok && xa <= hi_ok && xb >= lo_ok && xb <= hi_ok;
     cand_nonneg = xa >= -0.25 && xb >= -0.25;
   }
+  if constexpr (SMEM) cp_async_wait_all();
   __syncwarp();
   long long m[kNumSizes];
 #pragma unroll
@@ -177,11 +235,34 @@ split_kernel(const T* __restrict__ v, RangeSums rs, int32_t* __restrict__ nb_nex
 #pragma unroll
     for (int k = 0; k < kNumSizes; k++) md[k] = 0.0;
     bool vals_ok = true;
-    split_bands<0, T>(v, s, lane, s_th[warp], md, vals_ok);
+    split_bands<0, SMEM, T>(vs, lane, th, md, vals_ok);
     if (__all_sync(FULL_MASK, vals_ok)) {
 #pragma unroll
       for (int k = 0; k < kNumSizes; k++) m[k] = (long long)md[k];
       banded = true;
+    }
+  }
+  if constexpr (sizeof(T) == 8 && SMEM) {  // (walks only: it would cost the all-starts kernel occupancy)
+    if (!fast && ncand == kNumSizes) {  // values beyond 2^51: the offset form, when it applies
+      constexpr double kLo = 2251799813685248.0, kHi = 4611686018427387904.0, kNear = 1125899906842624.0;
+      const double x0 = __shfl_sync(FULL_MASK, xa, 0);
+      const bool d_ok = x0 >= kLo && x0 <= kHi;
+      const double d = d_ok ? trunc(x0) : 0.0;
+      const bool cand_off = lane >= ncand || (xa >= kLo && xa <= kHi && xb >= kLo && xb <= kHi &&
+                                              fabs(xa - d) <= kNear && fabs(xb - d) <= kNear);
+      if (__all_sync(FULL_MASK, d_ok && cand_off)) {
+        double md[kNumSizes];
+#pragma unroll
+        for (int k = 0; k < kNumSizes; k++) md[k] = 0.0;
+        bool vals_ok = true;
+        split_bands_off<0, SMEM, T>(vs, lane, th, d, (long long)d, md, vals_ok);
+        if (__all_sync(FULL_MASK, vals_ok)) {
+#pragma unroll
+          for (int k = 0; k < kNumSizes; k++) m[k] = (long long)md[k];
+          banded = true;
+          fast = true;  // measured
+        }
+      }
     }
   }
   if (fast && !banded) {
@@ -195,15 +276,15 @@ split_kernel(const T* __restrict__ v, RangeSums rs, int32_t* __restrict__ nb_nex
     double od = (double)lane;
     for (int o0 = 0; o0 < total; o0 += 32, od += 32.0) {
       while (c_sizes[band] <= o0) band++;
-      const T y = __ldg(v + s + o0 + lane);
+      const T y = ld_val<SMEM>(vs + o0 + lane);
       const long long yv = (long long)y;
       vals_ok &= TypeTraits<T>::is_signed ? (yv > -(1ll << 51) && yv < (1ll << 51)) : ((uint64_t)y < (1ull << 51));
       const double yd = (double)yv;  // exact when vals_ok (a start where it is not is measured again below)
 #pragma unroll
       for (int k = 0; k < kNumSizes; k++) {
         if (k < band || k >= ncand) continue;
-        const double2 th = *reinterpret_cast<const double2*>(&s_th[warp][k][0]);
-        md[k] = fmax(md[k], abs_resid_fp64(yd, __fma_rn(th.y, od, th.x)));
+        const double2 tk = *reinterpret_cast<const double2*>(&th[k][0]);
+        md[k] = fmax(md[k], abs_resid_fp64(yd, __fma_rn(tk.y, od, tk.x)));
       }
     }
     fast = __all_sync(FULL_MASK, vals_ok);
@@ -217,11 +298,11 @@ split_kernel(const T* __restrict__ v, RangeSums rs, int32_t* __restrict__ nb_nex
     for (int o0 = 0; o0 < total; o0 += 32) {
       while (c_sizes[band] <= o0) band++;
       const int o = o0 + lane;
-      const T y = __ldg(v + s + o);
+      const T y = ld_val<SMEM>(vs + o);
 #pragma unroll
       for (int k = 0; k < kNumSizes; k++) {
         if (k < band || k >= ncand) continue;
-        const long long d = abs_ref(calc_delta<T>(y, predict<T>(s_th[warp][k][0], s_th[warp][k][1], o)));
+        const long long d = abs_ref(calc_delta<T>(y, predict<T>(th[k][0], th[k][1], o)));
         m[k] = d > m[k] ? d : m[k];
       }
     }
@@ -235,10 +316,19 @@ split_kernel(const T* __restrict__ v, RangeSums rs, int32_t* __restrict__ nb_nex
     const double cpe = __ddiv_rn(part_cost(c_sizes[k], bits_for(mk)), (double)c_sizes[k]);
     if (cpe < best_cpe) { best_cpe = cpe; best = k; }
   }
-  if (lane == 0) {
-    const int64_t e = s + c_sizes[best];
-    nb_next[j] = (int32_t)(e >= rs.n ? rs.nb : e / kMinPart);
-  }
+  const int64_t e = s + c_sizes[best];
+  return (int32_t)(e >= rs.n ? rs.nb : e / kMinPart);
+}
+
+// Best end of every 128-aligned start not evaluated yet (one warp per start).
+template <typename T> __global__ void __launch_bounds__(256)
+split_kernel(const T* __restrict__ v, RangeSums rs, int32_t* __restrict__ nb_next) {
+  __shared__ __align__(16) double s_th[8][kNumSizes][2];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int64_t j = (int64_t)blockIdx.x * 8 + warp;
+  if (j >= rs.nb || nb_next[j] != kUnknown) return;
+  const int32_t e = split_best_block<T, false>(v, rs, j, lane, s_th[warp], nullptr);
+  if (lane == 0) nb_next[j] = e;
 }
 
 // ---- walk from 0 ---------------------------------------------------------------------------
@@ -254,13 +344,113 @@ __global__ void chain_exit_kernel(const int32_t* __restrict__ nb_next, int64_t n
   exits[t] = (node >= nb) ? kEnd : (int32_t)(node - lim);
 }
 
-__global__ void chain_link_kernel(const int32_t* __restrict__ exits, int64_t nr, int32_t* __restrict__ entries) {
-  if (blockIdx.x != 0 || threadIdx.x != 0) return;
-  int32_t e = 0;
-  for (int64_t r = 0; r < nr; r++) {
-    entries[r] = e;
-    if (e != kEnd) e = exits[r * kMaxJumpBlocks + e];
+// ---- lazy walk: evaluate only the starts a walk can reach --------------------------------------
+// The walk from 0 visits one start in ~25 on piecewise-linear data.  Each range is walked from its
+// first block, and again from the block where the previous range's first walk leaves it (the
+// walk from 0 usually enters there: walks from nearby starts meet where the data changes
+// slope).  The ranges are then chained through the exits of the starts these walks visited; if
+// the walk from 0 enters a range at a start no walk visited, every start is evaluated instead.
+
+constexpr int kWalkWarps = 1;  // one warp per CTA: the few range walks spread evenly over the SMs
+
+// Walk of each range from its first block (one warp per range).
+template <typename T> __global__ void __launch_bounds__(kWalkWarps * 32)
+walk_first_kernel(const T* __restrict__ v, RangeSums rs, int64_t nr, int32_t* __restrict__ nb_next,
+                  int32_t* __restrict__ exit_first) {
+  __shared__ __align__(16) double s_th[kWalkWarps][kNumSizes][2];
+  __shared__ __align__(16) T s_win[kWalkWarps][kMinPart * kMaxJumpBlocks];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int64_t r = (int64_t)blockIdx.x * kWalkWarps + warp;
+  if (r >= nr) return;
+  const int64_t lim = (r + 1) * kRangeBlocks < rs.nb ? (r + 1) * kRangeBlocks : rs.nb;
+  int64_t node = r * kRangeBlocks;
+  while (node < lim) {
+    const int32_t nx = split_best_block<T, true>(v, rs, node, lane, s_th[warp], s_win[warp]);
+    if (lane == 0) nb_next[node] = nx;
+    node = nx;
   }
+  if (lane == 0) exit_first[r] = (int32_t)node;
+}
+
+// The exit block of every start on the first walk of each range, then the walk from the block
+// where the previous range's first walk leaves, evaluated until it meets the first walk (whose
+// starts are the only ones of the range evaluated so far), and the exit of its starts.
+template <typename T> __global__ void __launch_bounds__(kWalkWarps * 32)
+walk_entry_kernel(const T* __restrict__ v, RangeSums rs, int64_t nr, int32_t* __restrict__ nb_next,
+                  const int32_t* __restrict__ exit_first, int32_t* __restrict__ cexit) {
+  __shared__ __align__(16) double s_th[kWalkWarps][kNumSizes][2];
+  __shared__ __align__(16) T s_win[kWalkWarps][kMinPart * kMaxJumpBlocks];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int64_t r = (int64_t)blockIdx.x * kWalkWarps + warp;
+  if (r >= nr) return;
+  const int64_t lim = (r + 1) * kRangeBlocks < rs.nb ? (r + 1) * kRangeBlocks : rs.nb;
+  const int32_t ex0 = exit_first[r];
+  if (lane == 0)
+    for (int64_t p = r * kRangeBlocks; p < lim; p = nb_next[p]) cexit[p] = ex0;
+  if (r == 0) return;
+  const int64_t x = exit_first[r - 1];  // in [r * kRangeBlocks, r * kRangeBlocks + 29) or past the end
+  if (x >= lim) return;
+  int64_t node = x;
+  while (node < lim) {
+    int32_t nx = lane == 0 ? nb_next[node] : 0;
+    nx = __shfl_sync(FULL_MASK, nx, 0);
+    if (nx != kUnknown) break;  // met the first walk
+    nx = split_best_block<T, true>(v, rs, node, lane, s_th[warp], s_win[warp]);
+    if (lane == 0) nb_next[node] = nx;
+    node = nx;
+  }
+  const int32_t exb = node < lim ? ex0 : (int32_t)node;
+  if (lane == 0)
+    for (int64_t p = x; p < lim && cexit[p] == kUnknown; p = nb_next[p]) cexit[p] = exb;
+}
+
+// Chains the ranges (one warp): entries[r] = the block offset at which the walk from 0 enters
+// range r (kEnd past the end of the column).  LAZY: exits from cexit (absolute blocks, kUnknown
+// where no walk passed; *fail = the first range entered at such a start, or -1); otherwise from
+// the exit table of every entry offset (relative offsets, kEnd).  The exits of eight ranges'
+// 29 entry offsets are loaded together, one lane per offset, ahead of the dependent chain.
+template <bool LAZY>
+__global__ void chain_link_kernel(const int32_t* __restrict__ exits, int64_t nb, int64_t nr,
+                                  int32_t* __restrict__ entries, int64_t* __restrict__ fail) {
+  if (blockIdx.x != 0 || threadIdx.x >= 32) return;
+  const int lane = threadIdx.x;
+  constexpr int kAhead = 8;
+  int32_t e = 0;
+  for (int64_t r0 = 0; r0 < nr; r0 += kAhead) {
+    int32_t c[kAhead];
+#pragma unroll
+    for (int q = 0; q < kAhead; q++) {
+      const int64_t r = r0 + q;
+      c[q] = kUnknown;
+      if (r < nr && lane < kMaxJumpBlocks) {
+        if (LAZY) {
+          const int64_t b = r * kRangeBlocks + lane;
+          if (b < nb) c[q] = exits[b];
+        } else {
+          c[q] = exits[r * kMaxJumpBlocks + lane];
+        }
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < kAhead; q++) {
+      const int64_t r = r0 + q;
+      if (r >= nr) break;
+      if (lane == 0) entries[r] = e;
+      if (e == kEnd) continue;
+      const int32_t ex = __shfl_sync(FULL_MASK, c[q], e);
+      if (!LAZY) {
+        e = ex;
+        continue;
+      }
+      if (ex == kUnknown) {  // no walk passed this entry: the caller evaluates every start
+        for (int64_t k = r + lane; k < nr; k += 32) entries[k] = kEnd;
+        if (lane == 0) *fail = r;
+        return;
+      }
+      e = (int64_t)ex >= nb ? kEnd : (int32_t)(ex - (r + 1) * kRangeBlocks);
+    }
+  }
+  if (LAZY && lane == 0) *fail = -1;
 }
 
 __global__ void chain_mark_kernel(const int32_t* __restrict__ nb_next, const int32_t* __restrict__ entries, int64_t nb,
@@ -432,7 +622,8 @@ static cudaError_t partition_typed(glc_ctx* ctx, const T* v, int64_t n, int32_t*
   bytes += al(sizeof(SumPair) * (scan_num_tiles(nb) + 1));     // scan tiles (pair)
   bytes += al(sizeof(int32_t) * nb);                           // nb_next
   bytes += al(sizeof(int32_t) * nr * kMaxJumpBlocks);          // exits
-  bytes += al(sizeof(int32_t) * nr);                           // entries
+  bytes += al(sizeof(int32_t) * nr) * 2;                       // entries, exit_first
+  bytes += al(sizeof(int32_t) * nb);                           // cexit
   bytes += al(sizeof(int64_t) * (nb + 1)) * 2;                 // flags, idx
   bytes += al(sizeof(int64_t) * (scan_num_tiles(nb) + 1));     // scan tiles (i64)
   bytes += al(sizeof(int32_t) * mmax) * 4;                     // ps, pe, ps2, pe2
@@ -451,6 +642,8 @@ static cudaError_t partition_typed(glc_ctx* ctx, const T* v, int64_t n, int32_t*
   int32_t* nb_next = (int32_t*)take(sizeof(int32_t) * nb);
   int32_t* exits = (int32_t*)take(sizeof(int32_t) * nr * kMaxJumpBlocks);
   int32_t* entries = (int32_t*)take(sizeof(int32_t) * nr);
+  int32_t* exit_first = (int32_t*)take(sizeof(int32_t) * nr);
+  int32_t* cexit = (int32_t*)take(sizeof(int32_t) * nb);
   int64_t* flags = (int64_t*)take(sizeof(int64_t) * (nb + 1));
   int64_t* idx = (int64_t*)take(sizeof(int64_t) * (nb + 1));
   int64_t* itiles = (int64_t*)take(sizeof(int64_t) * (scan_num_tiles(nb) + 1));
@@ -470,7 +663,7 @@ static cudaError_t partition_typed(glc_ctx* ctx, const T* v, int64_t n, int32_t*
   int64_t* nch = (int64_t*)take(sizeof(int64_t) * (mmax + 1));
   int64_t* base = (int64_t*)take(sizeof(int64_t) * (mmax + 1));
   long long* perr = (long long*)take(sizeof(long long) * mmax);
-  int64_t* dsc = (int64_t*)take(sizeof(int64_t) * 4);  // [0] total chunks, [1] m, [2] any (int)
+  int64_t* dsc = (int64_t*)take(sizeof(int64_t) * 4);  // [0] total chunks, [1] m, [2] any (int), [3] walk fail
   RangeSums rs{pre, n, nb};
 
   auto fail = [&](cudaError_t ee) { cudaFreeAsync(buf, s); return ee; };
@@ -478,16 +671,31 @@ static cudaError_t partition_typed(glc_ctx* ctx, const T* v, int64_t n, int32_t*
 
   block_sums_kernel<T><<<grid(nb * 32, 256), 256, 0, s>>>(v, n, nb, pre);
   if ((e = exclusive_scan<SumPair>(pre, pre, nb, pre + nb, ptiles, s)) != cudaSuccess) return fail(e);
-  split_kernel<T><<<grid(nb, 8), 256, 0, s>>>(v, rs, nb_next);
-  chain_exit_kernel<<<grid(nr * kMaxJumpBlocks, 128), 128, 0, s>>>(nb_next, nb, nr, exits);
-  chain_link_kernel<<<1, 1, 0, s>>>(exits, nr, entries);
-  if ((e = cudaMemsetAsync(flags, 0, sizeof(int64_t) * (nb + 1), s)) != cudaSuccess) return fail(e);
-  chain_mark_kernel<<<grid(nr, 128), 128, 0, s>>>(nb_next, entries, nb, nr, flags);
-  if ((e = exclusive_scan<int64_t>(flags, idx, nb, dsc + 1, itiles, s)) != cudaSuccess) return fail(e);
-  chain_compact_kernel<<<grid(nb, 256), 256, 0, s>>>(flags, idx, nb_next, nb, n, ps, pe);
-  if ((e = cudaGetLastError()) != cudaSuccess) return fail(e);
-  if ((e = cudaMemcpyAsync(ctx->h_stats, dsc + 1, sizeof(int64_t), cudaMemcpyDeviceToHost, s)) != cudaSuccess) return fail(e);
-  if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return fail(e);
+  // the walk from 0: first only the starts that the walks of the ranges visit
+  if ((e = cudaMemsetAsync(nb_next, 0xff, sizeof(int32_t) * nb, s)) != cudaSuccess) return fail(e);
+  if ((e = cudaMemsetAsync(cexit, 0xff, sizeof(int32_t) * nb, s)) != cudaSuccess) return fail(e);
+  walk_first_kernel<T><<<grid(nr, kWalkWarps), kWalkWarps * 32, 0, s>>>(v, rs, nr, nb_next, exit_first);
+  walk_entry_kernel<T><<<grid(nr, kWalkWarps), kWalkWarps * 32, 0, s>>>(v, rs, nr, nb_next, exit_first, cexit);
+  chain_link_kernel<true><<<1, 32, 0, s>>>(cexit, nb, nr, entries, dsc + 3);
+  auto mark_and_compact = [&]() -> cudaError_t {
+    cudaError_t ee = cudaMemsetAsync(flags, 0, sizeof(int64_t) * (nb + 1), s);
+    if (ee != cudaSuccess) return ee;
+    chain_mark_kernel<<<grid(nr, 128), 128, 0, s>>>(nb_next, entries, nb, nr, flags);
+    if ((ee = exclusive_scan<int64_t>(flags, idx, nb, dsc + 1, itiles, s)) != cudaSuccess) return ee;
+    chain_compact_kernel<<<grid(nb, 256), 256, 0, s>>>(flags, idx, nb_next, nb, n, ps, pe);
+    if ((ee = cudaGetLastError()) != cudaSuccess) return ee;
+    // dsc[1] = partitions, dsc[3] = first range the walks did not cover
+    if ((ee = cudaMemcpyAsync(ctx->h_stats, dsc + 1, 3 * sizeof(int64_t), cudaMemcpyDeviceToHost, s)) != cudaSuccess)
+      return ee;
+    return cudaStreamSynchronize(s);
+  };
+  if ((e = mark_and_compact()) != cudaSuccess) return fail(e);
+  if (ctx->h_stats[2] >= 0) {  // the walk from 0 left the visited starts: evaluate all of them
+    split_kernel<T><<<grid(nb, 8), 256, 0, s>>>(v, rs, nb_next);
+    chain_exit_kernel<<<grid(nr * kMaxJumpBlocks, 128), 128, 0, s>>>(nb_next, nb, nr, exits);
+    chain_link_kernel<false><<<1, 32, 0, s>>>(exits, nb, nr, entries, nullptr);
+    if ((e = mark_and_compact()) != cudaSuccess) return fail(e);
+  }
   int64_t m = ctx->h_stats[0];
   if (m <= 0 || m > mmax) {
     if (err) *err = "partitioner produced an invalid split";
