@@ -482,21 +482,13 @@ __global__ void chain_compact_kernel(const int64_t* __restrict__ flags, const in
 struct LineJob {  // one range whose max |delta| is needed
   int32_t a, b;
   double t0, t1;
+  double sum;  // pairs: the two partitions' costs (a merge must cost less); partitions: +inf
 };
-
-__device__ __forceinline__ int64_t owner_last_le(const int64_t* __restrict__ base, int64_t cnt, int64_t c) {
-  int64_t lo = 0, hi = cnt - 1;
-  while (lo < hi) {
-    int64_t mid = (lo + hi + 1) >> 1;
-    if (base[mid] <= c) lo = mid; else hi = mid - 1;
-  }
-  return lo;
-}
 
 // chunks of each job (0 for jobs that are cached)
 __global__ void job_setup_kernel(const int32_t* __restrict__ ps, const int32_t* __restrict__ pe, int64_t m, int pairs,
-                                 const uint8_t* __restrict__ cached, RangeSums rs, LineJob* __restrict__ jobs,
-                                 int64_t* __restrict__ nch, long long* __restrict__ err) {
+                                 const uint8_t* __restrict__ cached, const double* __restrict__ pc, RangeSums rs,
+                                 LineJob* __restrict__ jobs, int64_t* __restrict__ nch, long long* __restrict__ err) {
   const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int64_t njobs = pairs ? m - 1 : m;
   if (k >= njobs) return;
@@ -504,33 +496,44 @@ __global__ void job_setup_kernel(const int32_t* __restrict__ ps, const int32_t* 
   jb.a = ps[k];
   jb.b = pairs ? pe[k + 1] : pe[k];
   rs.line(jb.a, jb.b, jb.t0, jb.t1);
+  jb.sum = pairs ? __dadd_rn(pc[k], pc[k + 1]) : __longlong_as_double(0x7ff0000000000000ll);
   jobs[k] = jb;
   err[k] = 0;
   const bool skip = cached && cached[k];
   nch[k] = skip ? 0 : ((int64_t)jb.b - jb.a + kPairChunk - 1) / kPairChunk;
 }
 
-template <typename T> __global__ void __launch_bounds__(256)
-job_err_kernel(const T* __restrict__ v, const LineJob* __restrict__ jobs, const int64_t* __restrict__ base,
-               int64_t njobs, const int64_t* __restrict__ total_chunks, long long* __restrict__ err) {
-  const int64_t c = blockIdx.x;
-  if (c >= *total_chunks) return;
-  const int64_t k = owner_last_le(base, njobs, c);
-  const LineJob jb = jobs[k];
-  const int64_t off0 = (c - base[k]) * kPairChunk;
+// Max |delta| of a job's line over chunk q of the job (256 threads, no CTA barrier: warps may
+// skip a chunk independently), folded into *errk by each warp.
+template <typename T>
+__device__ __forceinline__ void job_chunk(const T* __restrict__ v, const LineJob& jb, int64_t q, long long* errk) {
+  const int64_t off0 = q * kPairChunk;
   const int64_t len = (int64_t)jb.b - jb.a;
   const int64_t off1 = off0 + kPairChunk < len ? off0 + kPairChunk : len;
   long long mm = 0;
   bool exact = true;
   if (off1 > off0 && line_fp64_safe<T>(jb.t0, jb.t1, off0, off1 - 1)) {  // exact in FP64 (glc_device.cuh)
-    double md = 0.0, od = (double)(off0 + threadIdx.x);
-    bool ok = true;
-    for (int64_t o = off0 + threadIdx.x; o < off1; o += 256, od += 256.0) {
-      const T y = __ldg(v + jb.a + o);
-      ok &= value_fp64_safe<T>(y);
-      md = fmax(md, abs_resid_fp64((double)(long long)y, __fma_rn(jb.t1, od, jb.t0)));
+    static_assert(kPairChunk == 16 * 256, "16 values per thread");
+    T ys[16];
+#pragma unroll
+    for (int u = 0; u < 16; u++) {  // all loads in flight before the arithmetic
+      const int64_t o = off0 + threadIdx.x + u * 256;
+      ys[u] = o < off1 ? __ldg(v + jb.a + o) : (T)0;
     }
-    if (ok) { mm = (long long)md; exact = false; }
+    double md = 0.0;
+    bool ok = true;
+#pragma unroll
+    for (int u = 0; u < 16; u++) {
+      const int64_t o = off0 + threadIdx.x + u * 256;
+      if (o < off1) {
+        ok &= value_fp64_safe<T>(ys[u]);
+        md = fmax(md, abs_resid_fp64((double)(long long)ys[u], __fma_rn(jb.t1, (double)o, jb.t0)));
+      }
+    }
+    if (ok) {  // this thread's values were all inside the exact range
+      mm = (long long)md;
+      exact = false;
+    }
   }
   if (exact)
     for (int64_t o = off0 + threadIdx.x; o < off1; o += 256) {
@@ -538,13 +541,32 @@ job_err_kernel(const T* __restrict__ v, const LineJob* __restrict__ jobs, const 
       mm = d > mm ? d : mm;
     }
   mm = warp_max_ll(mm);
-  __shared__ long long s_m[8];
-  if ((threadIdx.x & 31) == 0) s_m[threadIdx.x >> 5] = mm;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    long long t = 0;
-    for (int w = 0; w < 8; w++) t = s_m[w] > t ? s_m[w] : t;
-    if (t > 0) atomicMax(err + k, t);
+  if ((threadIdx.x & 31) == 0 && mm > 0) atomicMax(errk, mm);
+}
+
+// A pair whose partial max |delta| already makes the merge cost at least the two partitions'
+// costs is not merged whatever the rest of it holds (the score stays unprofitable, also when it
+// is kept for the next round), so its remaining chunks are skipped.  One warp decides.
+__device__ __forceinline__ bool job_settled(const LineJob& jb, const long long* errk) {
+  long long e = 0;
+  if ((threadIdx.x & 31) == 0) e = *(const volatile long long*)errk;
+  e = __shfl_sync(FULL_MASK, e, 0);
+  return !(part_cost((int64_t)jb.b - jb.a, bits_for(e)) < jb.sum);
+}
+
+// Max |delta| of every job still to measure: persistent CTAs, one job at a time, its chunks in
+// order (each warp stops at the first chunk after which the pair is settled).
+template <typename T> __global__ void __launch_bounds__(256, 4)
+job_err_kernel(const T* __restrict__ v, const LineJob* __restrict__ jobs, const int64_t* __restrict__ nch,
+               int64_t njobs, long long* __restrict__ err) {
+  for (int64_t k = blockIdx.x; k < njobs; k += gridDim.x) {
+    const int64_t nc = nch[k];  // 0: kept from the previous round
+    if (nc == 0) continue;
+    const LineJob jb = jobs[k];
+    for (int64_t q = 0; q < nc; q++) {
+      if (q > 0 && job_settled(jb, err + k)) break;
+      job_chunk<T>(v, jb, q, err + k);
+    }
   }
 }
 
@@ -630,7 +652,7 @@ static cudaError_t partition_typed(glc_ctx* ctx, const T* v, int64_t n, int32_t*
   bytes += al(sizeof(double) * mmax) * 5;                      // pc, pc2, mc, cmc, cmc2
   bytes += al(sizeof(uint8_t) * mmax) * 3;                     // prof, cached, cached2
   bytes += al(sizeof(LineJob) * mmax);                         // jobs
-  bytes += al(sizeof(int64_t) * (mmax + 1)) * 2;               // nch, base
+  bytes += al(sizeof(int64_t) * (mmax + 1));                   // nch
   bytes += al(sizeof(long long) * mmax);                       // err
   bytes += al(sizeof(int64_t) * 4);                            // device scalars
   char* buf = nullptr;
@@ -661,9 +683,8 @@ static cudaError_t partition_typed(glc_ctx* ctx, const T* v, int64_t n, int32_t*
   uint8_t* cached2 = (uint8_t*)take(mmax);
   LineJob* jobs = (LineJob*)take(sizeof(LineJob) * mmax);
   int64_t* nch = (int64_t*)take(sizeof(int64_t) * (mmax + 1));
-  int64_t* base = (int64_t*)take(sizeof(int64_t) * (mmax + 1));
   long long* perr = (long long*)take(sizeof(long long) * mmax);
-  int64_t* dsc = (int64_t*)take(sizeof(int64_t) * 4);  // [0] total chunks, [1] m, [2] any (int), [3] walk fail
+  int64_t* dsc = (int64_t*)take(sizeof(int64_t) * 4);  // [0] unused, [1] m, [2] any (int), [3] walk fail
   RangeSums rs{pre, n, nb};
 
   auto fail = [&](cudaError_t ee) { cudaFreeAsync(buf, s); return ee; };
@@ -705,12 +726,9 @@ static cudaError_t partition_typed(glc_ctx* ctx, const T* v, int64_t n, int32_t*
 
   // costs of the split partitions
   auto run_jobs = [&](int64_t cnt, int pairs, const uint8_t* cache) -> cudaError_t {
-    job_setup_kernel<<<grid(cnt, 256), 256, 0, s>>>(ps, pe, m, pairs, cache, rs, jobs, nch, perr);
-    cudaError_t ee = exclusive_scan<int64_t>(nch, base, cnt, dsc, itiles, s);
-    if (ee != cudaSuccess) return ee;
-    // each value lies in at most two jobs, so the chunks number at most 2n/4096 + jobs
-    const int64_t cap = 2 * n / kPairChunk + cnt + 1;
-    job_err_kernel<T><<<(unsigned)cap, 256, 0, s>>>(v, jobs, base, cnt, dsc, perr);
+    job_setup_kernel<<<grid(cnt, 256), 256, 0, s>>>(ps, pe, m, pairs, cache, pc, rs, jobs, nch, perr);
+    const int64_t resident = (int64_t)ctx->num_sms * 4;  // 256-thread CTAs, four per SM
+    job_err_kernel<T><<<(unsigned)(cnt < resident ? cnt : resident), 256, 0, s>>>(v, jobs, nch, cnt, perr);
     return cudaGetLastError();
   };
   if ((e = run_jobs(m, 0, nullptr)) != cudaSuccess) return fail(e);
