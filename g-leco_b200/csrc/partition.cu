@@ -9,12 +9,15 @@
 //
 // Split.  The reference walks from 0: at start s it tries sizes 128..3712 (steps of 128 up to
 // 640, then 256 up to 2176, then 512; CpuPartitioner.cuh:150-175), keeps the first size with
-// the lowest cost per value and jumps there.  Every start on that walk is a multiple of 128,
-// so the best end of EVERY 128-aligned start is computed in parallel (one warp per start; each
-// value is loaded once and scored against all candidate lines that contain it), and the walk
-// is recovered afterwards: the starts are cut into ranges of 1024 blocks, the exit of each
-// possible entry point of a range is computed in parallel, one thread chains the ranges, and
-// each range marks its walk.
+// the lowest cost per value and jumps there.  Every start on that walk is a multiple of 128 and
+// the best end of a start depends on nothing else, so the walk is cut into ranges of 1024
+// blocks: each range is walked from its first block and from the block where the previous
+// range's first walk leaves it (one warp per range, each start's best end evaluated on the way:
+// each value of its reach scored against all candidate lines that contain it), one warp chains
+// the ranges through the exits of the visited starts, and each range marks its walk.  When the
+// walk from 0 enters a range at a start no walk visited, the best end of every start is
+// evaluated (one warp per start) and the ranges are chained through the exits of all their
+// possible entry points instead.
 //
 // Merge.  The reference absorbs right neighbours left to right while the merged cost is lower
 // (CpuPartitioner.cuh:198-242).  Here merging runs in rounds: every adjacent pair is scored,
@@ -407,14 +410,14 @@ walk_entry_kernel(const T* __restrict__ v, RangeSums rs, int64_t nr, int32_t* __
 // Chains the ranges (one warp): entries[r] = the block offset at which the walk from 0 enters
 // range r (kEnd past the end of the column).  LAZY: exits from cexit (absolute blocks, kUnknown
 // where no walk passed; *fail = the first range entered at such a start, or -1); otherwise from
-// the exit table of every entry offset (relative offsets, kEnd).  The exits of eight ranges'
+// the exit table of every entry offset (relative offsets, kEnd).  The exits of 32 ranges.
 // 29 entry offsets are loaded together, one lane per offset, ahead of the dependent chain.
 template <bool LAZY>
 __global__ void chain_link_kernel(const int32_t* __restrict__ exits, int64_t nb, int64_t nr,
                                   int32_t* __restrict__ entries, int64_t* __restrict__ fail) {
   if (blockIdx.x != 0 || threadIdx.x >= 32) return;
   const int lane = threadIdx.x;
-  constexpr int kAhead = 8;
+  constexpr int kAhead = 32;
   int32_t e = 0;
   for (int64_t r0 = 0; r0 < nr; r0 += kAhead) {
     int32_t c[kAhead];
