@@ -41,7 +41,7 @@ __host__ __device__ constexpr int split_size(int k) {
 static_assert(split_size(0) == 128 && split_size(4) == 640 && split_size(5) == 896 && split_size(10) == 2176 &&
               split_size(11) == 2688 && split_size(13) == 3712, "candidate sizes");
 constexpr int kMaxJumpBlocks = 29;  // 3712 / 128
-constexpr int kRangeBlocks = 1024;
+constexpr int kRangeBlocks = 2048;
 constexpr int kMaxMergeRounds = 64;
 constexpr int kPairChunk = 4096;
 constexpr int32_t kUnknown = -1;  // best end of a start not evaluated

@@ -128,6 +128,21 @@ def test_variable_compress_bit_exact(oracle, kind, n):
     _check_column(codec, col, v, ocol, oracle)
 
 
+@pytest.mark.parametrize("kind", ["timestamps", "i32_linear", "u64_piecewise", "u64_high", "i64_ns", "i64_cross"])
+def test_variable_walks_over_many_ranges(oracle, kind):
+    """1.5M values span 6 ranges of 2048 blocks of the split walk: lines without slope changes
+    (the ranges' walks never meet, so every start is evaluated), piecewise lines (only the starts
+    the walks visit), and values beyond 2^51 (the walks' offset form)."""
+    v = _data(kind, 1_500_000, seed=7)
+    codec = _codec(v)
+    col, size = codec.compress(v, True)
+    s, e = oracle.partition_variable(v)
+    ocol = oracle.compress(v, starts=s, ends=e)
+    assert col.num_partitions == len(s)
+    assert size == ocol.reported_size()
+    _check_column(codec, col, v, ocol, oracle)
+
+
 def test_partitioner_matches_oracle_large(oracle, glc_ctx):
     v = W.piecewise_linear(3_000_000, seed=5)
     ds, de = glc.partition_variable(glc_ctx, v)
