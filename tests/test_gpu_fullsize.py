@@ -1,6 +1,12 @@
 """Full-size workloads, checked through size-independent properties: every value round-trips
 bit-exactly (compared on the device), lookups equal direct indexing, and the batched and
-per-column paths agree.  Inputs are generated on the device with the workloads' distributions."""
+per-column paths agree; the 200M decode-benchmark column's blobs also equal the oracle's (SHA-256
+digests in tests/golden/c2_oracle_blobs.json, made by tests/golden/make_c2_oracle_blobs.py).
+Inputs are generated on the device with the workloads' distributions."""
+import hashlib
+import json
+import os
+
 import numpy as np
 import pytest
 import torch
@@ -44,6 +50,31 @@ def test_piecewise_u64_200m_variable_round_trip():
     assert torch.equal(out, d)
     col.free()
     back.free()
+
+
+@pytest.mark.parametrize("mode", ["variable", "fixed4096"])
+def test_piecewise_u64_200m_blob_equals_oracle(mode):
+    """The whole 200M-value blob of the decode benchmark's column (device partitioner and compress,
+    or the one-pass fixed compress) is byte for byte the oracle's."""
+    with open(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "c2_oracle_blobs.json")) as f:
+        fx = json.load(f)
+    ctx = _ctx()
+    v = W.piecewise_linear(fx["values"], seed=fx["seed"])
+    d = torch.from_numpy(v.view(np.int64)).cuda()
+    s = torch.cuda.current_stream().cuda_stream
+    torch.cuda.synchronize()
+    if mode == "variable":
+        col = glc.compress_device(ctx, glc.U64, d.data_ptr(), len(v), glc.VARIABLE, stream=s)
+    else:
+        col = glc.compress_device(ctx, glc.U64, d.data_ptr(), len(v), glc.FIXED, fixed_len=4096, stream=s)
+    ctx.sync()
+    info = col.info()
+    assert info.num_partitions == fx[mode]["partitions"]
+    assert info.compressed_size_bytes == fx[mode]["reported_size"]
+    blob = glc.serialize_host(ctx, col)
+    col.free()
+    assert len(blob) == fx[mode]["blob_bytes"]
+    assert hashlib.sha256(blob).hexdigest() == fx[mode]["blob_sha256"]
 
 
 @pytest.mark.parametrize("mode", ["packed", "preunpacked"])
