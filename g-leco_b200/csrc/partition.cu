@@ -191,12 +191,13 @@ __device__ __forceinline__ void split_bands_off(const T* __restrict__ vs, int la
 // copies in flight at once, for walks where one warp evaluates starts one after another.
 template <typename T, bool SMEM>
 __device__ __forceinline__ int32_t split_best_block(const T* __restrict__ v, const RangeSums& rs, int64_t j, int lane,
-                                                    double (*th)[2], T* win) {
+                                                    double (*th)[2], T* win, long long& best_err) {
   const int64_t s = j * kMinPart;
   const int64_t max_size = (rs.n - s < kMinPart * 32) ? rs.n - s : kMinPart * 32;
   int ncand = 0;
 #pragma unroll
   for (int k = 0; k < kNumSizes; k++) ncand += (c_sizes[k] <= max_size) ? 1 : 0;
+  best_err = -1;  // not measured
   if (ncand == 0) return (int32_t)rs.nb;  // fewer than 128 values left: the rest is one partition
   __syncwarp();  // the previous start's lines and values are no longer read
   const T* vs = v + s;
@@ -317,21 +318,26 @@ __device__ __forceinline__ int32_t split_best_block(const T* __restrict__ v, con
     if (k >= ncand) continue;
     const long long mk = warp_max_ll(m[k]);
     const double cpe = __ddiv_rn(part_cost(c_sizes[k], bits_for(mk)), (double)c_sizes[k]);
-    if (cpe < best_cpe) { best_cpe = cpe; best = k; }
+    if (cpe < best_cpe) { best_cpe = cpe; best = k; best_err = mk; }
   }
   const int64_t e = s + c_sizes[best];
   return (int32_t)(e >= rs.n ? rs.nb : e / kMinPart);
 }
 
-// Best end of every 128-aligned start not evaluated yet (one warp per start).
+// Best end of every 128-aligned start not evaluated yet (one warp per start), and the max |delta|
+// of the partition it makes (nb_err: -1 where not measured).
 template <typename T> __global__ void __launch_bounds__(256)
-split_kernel(const T* __restrict__ v, RangeSums rs, int32_t* __restrict__ nb_next) {
+split_kernel(const T* __restrict__ v, RangeSums rs, int32_t* __restrict__ nb_next, long long* __restrict__ nb_err) {
   __shared__ __align__(16) double s_th[8][kNumSizes][2];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int64_t j = (int64_t)blockIdx.x * 8 + warp;
   if (j >= rs.nb || nb_next[j] != kUnknown) return;
-  const int32_t e = split_best_block<T, false>(v, rs, j, lane, s_th[warp], nullptr);
-  if (lane == 0) nb_next[j] = e;
+  long long err;
+  const int32_t e = split_best_block<T, false>(v, rs, j, lane, s_th[warp], nullptr, err);
+  if (lane == 0) {
+    nb_next[j] = e;
+    nb_err[j] = err;
+  }
 }
 
 // ---- walk from 0 ---------------------------------------------------------------------------
@@ -359,7 +365,7 @@ constexpr int kWalkWarps = 1;  // one warp per CTA: the few range walks spread e
 // Walk of each range from its first block (one warp per range).
 template <typename T> __global__ void __launch_bounds__(kWalkWarps * 32)
 walk_first_kernel(const T* __restrict__ v, RangeSums rs, int64_t nr, int32_t* __restrict__ nb_next,
-                  int32_t* __restrict__ exit_first) {
+                  long long* __restrict__ nb_err, int32_t* __restrict__ exit_first) {
   __shared__ __align__(16) double s_th[kWalkWarps][kNumSizes][2];
   __shared__ __align__(16) T s_win[kWalkWarps][kMinPart * kMaxJumpBlocks];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -368,8 +374,12 @@ walk_first_kernel(const T* __restrict__ v, RangeSums rs, int64_t nr, int32_t* __
   const int64_t lim = (r + 1) * kRangeBlocks < rs.nb ? (r + 1) * kRangeBlocks : rs.nb;
   int64_t node = r * kRangeBlocks;
   while (node < lim) {
-    const int32_t nx = split_best_block<T, true>(v, rs, node, lane, s_th[warp], s_win[warp]);
-    if (lane == 0) nb_next[node] = nx;
+    long long err;
+    const int32_t nx = split_best_block<T, true>(v, rs, node, lane, s_th[warp], s_win[warp], err);
+    if (lane == 0) {
+      nb_next[node] = nx;
+      nb_err[node] = err;
+    }
     node = nx;
   }
   if (lane == 0) exit_first[r] = (int32_t)node;
@@ -380,7 +390,7 @@ walk_first_kernel(const T* __restrict__ v, RangeSums rs, int64_t nr, int32_t* __
 // starts are the only ones of the range evaluated so far), and the exit of its starts.
 template <typename T> __global__ void __launch_bounds__(kWalkWarps * 32)
 walk_entry_kernel(const T* __restrict__ v, RangeSums rs, int64_t nr, int32_t* __restrict__ nb_next,
-                  const int32_t* __restrict__ exit_first, int32_t* __restrict__ cexit) {
+                  long long* __restrict__ nb_err, const int32_t* __restrict__ exit_first, int32_t* __restrict__ cexit) {
   __shared__ __align__(16) double s_th[kWalkWarps][kNumSizes][2];
   __shared__ __align__(16) T s_win[kWalkWarps][kMinPart * kMaxJumpBlocks];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -398,8 +408,12 @@ walk_entry_kernel(const T* __restrict__ v, RangeSums rs, int64_t nr, int32_t* __
     int32_t nx = lane == 0 ? nb_next[node] : 0;
     nx = __shfl_sync(FULL_MASK, nx, 0);
     if (nx != kUnknown) break;  // met the first walk
-    nx = split_best_block<T, true>(v, rs, node, lane, s_th[warp], s_win[warp]);
-    if (lane == 0) nb_next[node] = nx;
+    long long err;
+    nx = split_best_block<T, true>(v, rs, node, lane, s_th[warp], s_win[warp], err);
+    if (lane == 0) {
+      nb_next[node] = nx;
+      nb_err[node] = err;
+    }
     node = nx;
   }
   const int32_t exb = node < lim ? ex0 : (int32_t)node;
@@ -470,15 +484,19 @@ __global__ void chain_mark_kernel(const int32_t* __restrict__ nb_next, const int
   }
 }
 
+// The walk's partitions in order, with the max |delta| their start's evaluation measured for them
+// (-1 for a last partition of fewer than 128 values, which no evaluation measured).
 __global__ void chain_compact_kernel(const int64_t* __restrict__ flags, const int64_t* __restrict__ idx,
-                                     const int32_t* __restrict__ nb_next, int64_t nb, int64_t n,
-                                     int32_t* __restrict__ ps, int32_t* __restrict__ pe) {
+                                     const int32_t* __restrict__ nb_next, const long long* __restrict__ nb_err,
+                                     int64_t nb, int64_t n, int32_t* __restrict__ ps, int32_t* __restrict__ pe,
+                                     long long* __restrict__ kerr) {
   const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= nb || !flags[j]) return;
   const int64_t k = idx[j];
   ps[k] = (int32_t)(j * kMinPart);
   const int64_t e = (int64_t)nb_next[j] * kMinPart;
   pe[k] = (int32_t)(e > n ? n : e);
+  kerr[k] = nb_err[j];
 }
 
 // ---- costs of partitions ---------------------------------------------------------------
@@ -489,9 +507,12 @@ struct LineJob {  // one range whose max |delta| is needed
 };
 
 // chunks of each job (0 for jobs that are cached)
+// known (partitions only): a max |delta| already measured (the split evaluation of the
+// partition's start, same line and values), or -1.
 __global__ void job_setup_kernel(const int32_t* __restrict__ ps, const int32_t* __restrict__ pe, int64_t m, int pairs,
-                                 const uint8_t* __restrict__ cached, const double* __restrict__ pc, RangeSums rs,
-                                 LineJob* __restrict__ jobs, int64_t* __restrict__ nch, long long* __restrict__ err) {
+                                 const uint8_t* __restrict__ cached, const long long* __restrict__ known,
+                                 const double* __restrict__ pc, RangeSums rs, LineJob* __restrict__ jobs,
+                                 int64_t* __restrict__ nch, long long* __restrict__ err) {
   const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int64_t njobs = pairs ? m - 1 : m;
   if (k >= njobs) return;
@@ -501,8 +522,9 @@ __global__ void job_setup_kernel(const int32_t* __restrict__ ps, const int32_t* 
   rs.line(jb.a, jb.b, jb.t0, jb.t1);
   jb.sum = pairs ? __dadd_rn(pc[k], pc[k + 1]) : __longlong_as_double(0x7ff0000000000000ll);
   jobs[k] = jb;
-  err[k] = 0;
-  const bool skip = cached && cached[k];
+  const long long kn = known ? known[k] : -1;
+  err[k] = kn >= 0 ? kn : 0;
+  const bool skip = (cached && cached[k]) || kn >= 0;
   nch[k] = skip ? 0 : ((int64_t)jb.b - jb.a + kPairChunk - 1) / kPairChunk;
 }
 
@@ -649,6 +671,8 @@ static cudaError_t partition_typed(glc_ctx* ctx, const T* v, int64_t n, int32_t*
   bytes += al(sizeof(int32_t) * nr * kMaxJumpBlocks);          // exits
   bytes += al(sizeof(int32_t) * nr) * 2;                       // entries, exit_first
   bytes += al(sizeof(int32_t) * nb);                           // cexit
+  bytes += al(sizeof(long long) * nb);                         // nb_err
+  bytes += al(sizeof(long long) * mmax);                       // kerr
   bytes += al(sizeof(int64_t) * (nb + 1)) * 2;                 // flags, idx
   bytes += al(sizeof(int64_t) * (scan_num_tiles(nb) + 1));     // scan tiles (i64)
   bytes += al(sizeof(int32_t) * mmax) * 4;                     // ps, pe, ps2, pe2
@@ -669,6 +693,8 @@ static cudaError_t partition_typed(glc_ctx* ctx, const T* v, int64_t n, int32_t*
   int32_t* entries = (int32_t*)take(sizeof(int32_t) * nr);
   int32_t* exit_first = (int32_t*)take(sizeof(int32_t) * nr);
   int32_t* cexit = (int32_t*)take(sizeof(int32_t) * nb);
+  long long* nb_err = (long long*)take(sizeof(long long) * nb);
+  long long* kerr = (long long*)take(sizeof(long long) * mmax);
   int64_t* flags = (int64_t*)take(sizeof(int64_t) * (nb + 1));
   int64_t* idx = (int64_t*)take(sizeof(int64_t) * (nb + 1));
   int64_t* itiles = (int64_t*)take(sizeof(int64_t) * (scan_num_tiles(nb) + 1));
@@ -698,15 +724,16 @@ static cudaError_t partition_typed(glc_ctx* ctx, const T* v, int64_t n, int32_t*
   // the walk from 0: first only the starts that the walks of the ranges visit
   if ((e = cudaMemsetAsync(nb_next, 0xff, sizeof(int32_t) * nb, s)) != cudaSuccess) return fail(e);
   if ((e = cudaMemsetAsync(cexit, 0xff, sizeof(int32_t) * nb, s)) != cudaSuccess) return fail(e);
-  walk_first_kernel<T><<<grid(nr, kWalkWarps), kWalkWarps * 32, 0, s>>>(v, rs, nr, nb_next, exit_first);
-  walk_entry_kernel<T><<<grid(nr, kWalkWarps), kWalkWarps * 32, 0, s>>>(v, rs, nr, nb_next, exit_first, cexit);
+  walk_first_kernel<T><<<grid(nr, kWalkWarps), kWalkWarps * 32, 0, s>>>(v, rs, nr, nb_next, nb_err, exit_first);
+  walk_entry_kernel<T><<<grid(nr, kWalkWarps), kWalkWarps * 32, 0, s>>>(v, rs, nr, nb_next, nb_err, exit_first,
+                                                                          cexit);
   chain_link_kernel<true><<<1, 32, 0, s>>>(cexit, nb, nr, entries, dsc + 3);
   auto mark_and_compact = [&]() -> cudaError_t {
     cudaError_t ee = cudaMemsetAsync(flags, 0, sizeof(int64_t) * (nb + 1), s);
     if (ee != cudaSuccess) return ee;
     chain_mark_kernel<<<grid(nr, 128), 128, 0, s>>>(nb_next, entries, nb, nr, flags);
     if ((ee = exclusive_scan<int64_t>(flags, idx, nb, dsc + 1, itiles, s)) != cudaSuccess) return ee;
-    chain_compact_kernel<<<grid(nb, 256), 256, 0, s>>>(flags, idx, nb_next, nb, n, ps, pe);
+    chain_compact_kernel<<<grid(nb, 256), 256, 0, s>>>(flags, idx, nb_next, nb_err, nb, n, ps, pe, kerr);
     if ((ee = cudaGetLastError()) != cudaSuccess) return ee;
     // dsc[1] = partitions, dsc[3] = first range the walks did not cover
     if ((ee = cudaMemcpyAsync(ctx->h_stats, dsc + 1, 3 * sizeof(int64_t), cudaMemcpyDeviceToHost, s)) != cudaSuccess)
@@ -715,7 +742,7 @@ static cudaError_t partition_typed(glc_ctx* ctx, const T* v, int64_t n, int32_t*
   };
   if ((e = mark_and_compact()) != cudaSuccess) return fail(e);
   if (ctx->h_stats[2] >= 0) {  // the walk from 0 left the visited starts: evaluate all of them
-    split_kernel<T><<<grid(nb, 8), 256, 0, s>>>(v, rs, nb_next);
+    split_kernel<T><<<grid(nb, 8), 256, 0, s>>>(v, rs, nb_next, nb_err);
     chain_exit_kernel<<<grid(nr * kMaxJumpBlocks, 128), 128, 0, s>>>(nb_next, nb, nr, exits);
     chain_link_kernel<false><<<1, 32, 0, s>>>(exits, nb, nr, entries, nullptr);
     if ((e = mark_and_compact()) != cudaSuccess) return fail(e);
@@ -727,19 +754,20 @@ static cudaError_t partition_typed(glc_ctx* ctx, const T* v, int64_t n, int32_t*
     return cudaErrorUnknown;
   }
 
-  // costs of the split partitions
-  auto run_jobs = [&](int64_t cnt, int pairs, const uint8_t* cache) -> cudaError_t {
-    job_setup_kernel<<<grid(cnt, 256), 256, 0, s>>>(ps, pe, m, pairs, cache, pc, rs, jobs, nch, perr);
+  // max |delta| of each job's line (partitions, or adjacent pairs of the merge rounds)
+  auto run_jobs = [&](int64_t cnt, int pairs, const uint8_t* cache, const long long* known) -> cudaError_t {
+    job_setup_kernel<<<grid(cnt, 256), 256, 0, s>>>(ps, pe, m, pairs, cache, known, pc, rs, jobs, nch, perr);
     const int64_t resident = (int64_t)ctx->num_sms * 4;  // 256-thread CTAs, four per SM
     job_err_kernel<T><<<(unsigned)(cnt < resident ? cnt : resident), 256, 0, s>>>(v, jobs, nch, cnt, perr);
     return cudaGetLastError();
   };
-  if ((e = run_jobs(m, 0, nullptr)) != cudaSuccess) return fail(e);
+  // costs of the split partitions: their max |delta| came with the split evaluation
+  if ((e = run_jobs(m, 0, nullptr, kerr)) != cudaSuccess) return fail(e);
   part_cost_kernel<<<grid(m, 256), 256, 0, s>>>(jobs, perr, m, pc);
   if ((e = cudaMemsetAsync(cached, 0, mmax, s)) != cudaSuccess) return fail(e);
 
   for (int round = 0; round < kMaxMergeRounds && m >= 2; round++) {
-    if ((e = run_jobs(m - 1, 1, cached)) != cudaSuccess) return fail(e);
+    if ((e = run_jobs(m - 1, 1, cached, nullptr)) != cudaSuccess) return fail(e);
     if ((e = cudaMemsetAsync(dsc + 2, 0, sizeof(int64_t), s)) != cudaSuccess) return fail(e);
     pair_score_kernel<<<grid(m - 1, 256), 256, 0, s>>>(jobs, perr, cached, cmc, pc, m, mc, prof, (int*)(dsc + 2));
     merge_heads_kernel<<<grid(m, 256), 256, 0, s>>>(prof, m, round, flags);
