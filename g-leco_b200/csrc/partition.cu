@@ -10,14 +10,15 @@
 // Split.  The reference walks from 0: at start s it tries sizes 128..3712 (steps of 128 up to
 // 640, then 256 up to 2176, then 512; CpuPartitioner.cuh:150-175), keeps the first size with
 // the lowest cost per value and jumps there.  Every start on that walk is a multiple of 128 and
-// the best end of a start depends on nothing else, so the walk is cut into ranges of 1024
+// the best end of a start depends on nothing else, so the walk is cut into ranges of 2048
 // blocks: each range is walked from its first block and from the block where the previous
 // range's first walk leaves it (one warp per range, each start's best end evaluated on the way:
 // each value of its reach scored against all candidate lines that contain it), one warp chains
 // the ranges through the exits of the visited starts, and each range marks its walk.  When the
 // walk from 0 enters a range at a start no walk visited, the best end of every start is
 // evaluated (one warp per start) and the ranges are chained through the exits of all their
-// possible entry points instead.
+// possible entry points instead.  The max |delta| each evaluation measured for the partition it
+// chose is kept, so the split partitions' costs need no second pass over the values.
 //
 // Merge.  The reference absorbs right neighbours left to right while the merged cost is lower
 // (CpuPartitioner.cuh:198-242).  Here merging runs in rounds: every adjacent pair is scored,
