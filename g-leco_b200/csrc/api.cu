@@ -281,6 +281,14 @@ static glc_status compress_impl(glc_ctx* ctx, glc_dtype dtype, const void* dev_v
   c->sync_free = true;
   int32_t* tmp_s = nullptr;
   int32_t* tmp_e = nullptr;
+  long long* part_err = nullptr;  // variable partitions: each partition's max |delta|, measured by the partitioner
+  struct StreamFree {  // returned to the pool after the stream's work so far, on every exit
+    void** p;
+    cudaStream_t s;
+    ~StreamFree() {
+      if (*p) cudaFreeAsync(*p, s);
+    }
+  } part_err_free{reinterpret_cast<void**>(&part_err), s};
   if (mode == GLC_PART_FIXED) {
     c->P = (n + fixed_len - 1) / fixed_len;
     c->fixed_len = fixed_len;
@@ -293,7 +301,7 @@ static glc_status compress_impl(glc_ctx* ctx, glc_dtype dtype, const void* dev_v
   } else {
     std::string perr;
     int64_t P = 0;
-    cudaError_t e = launch_partition_variable(ctx, dtype, dev_values, n, &tmp_s, &tmp_e, &P, s, &perr);
+    cudaError_t e = launch_partition_variable(ctx, dtype, dev_values, n, &tmp_s, &tmp_e, &P, s, &perr, &part_err);
     if (e != cudaSuccess) return perr.empty() ? cuda_fail(ctx, e, "variable partitioner") : fail(ctx, GLC_ERR_CUDA, perr);
     c->P = P;
     c->fixed_len = 0;
@@ -335,7 +343,7 @@ static glc_status compress_impl(glc_ctx* ctx, glc_dtype dtype, const void* dev_v
   const size_t sb = fit_scratch_bytes(nullptr, n, c->P);
   void* scratch = nullptr;
   CK(pool_alloc(ctx, &scratch, sb, s), "compress: scratch allocation");
-  cudaError_t e = launch_fit(dtype, dev_values, c, scratch, sb, ctx->d_stats, s);
+  cudaError_t e = launch_fit(dtype, dev_values, c, scratch, sb, ctx->d_stats, s, part_err);
   if (e == cudaSuccess) e = cudaMemcpyAsync(ctx->h_stats, ctx->d_stats, 4 * sizeof(int64_t), cudaMemcpyDeviceToHost, s);
   cudaFreeAsync(scratch, s);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);

@@ -450,8 +450,20 @@ static cudaError_t launch_fit_stream(const T* v, const FitStreamArgs& a, int num
   return cudaGetLastError();
 }
 
+// A partition longer than one chunk whose max |delta| the variable partitioner measured against
+// the same exact least-squares line takes it from there (direct-copy partitions keep 0).
+__global__ void fit_known_err_kernel(const int32_t* __restrict__ starts, const int32_t* __restrict__ ends,
+                                     const int32_t* __restrict__ types, const long long* __restrict__ known, int64_t P,
+                                     int64_t* __restrict__ err) {
+  const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= P) return;
+  if ((int64_t)ends[p] - starts[p] <= kFitChunk || types[p] == MODEL_DIRECT_COPY) return;
+  err[p] = known[p];
+}
+
 template <typename T>
-static cudaError_t fit_typed(const T* v, glc_column* c, void* scratch, int64_t* d_stats, cudaStream_t s) {
+static cudaError_t fit_typed(const T* v, glc_column* c, void* scratch, int64_t* d_stats, cudaStream_t s,
+                             const long long* known_err) {
   const int64_t P = c->P, n = c->n;
   const int64_t ncmax = n / kFitChunk + P + 1;
   char* sp = (char*)scratch;
@@ -487,9 +499,11 @@ static cudaError_t fit_typed(const T* v, glc_column* c, void* scratch, int64_t* 
     chunk_count_kernel<<<pg, 256, 0, s>>>(c->d_start, c->d_end, P, nch);
     if ((e = exclusive_scan<int64_t>(nch, base, P, nchunks, tiles, s)) != cudaSuccess) return e;
     chunk_owner_kernel<<<pg, 256, 0, s>>>(base, nch, P, owner);
-    multi_count_kernel<<<pg, 256, 0, s>>>(c->d_start, c->d_end, nch, P, nm);
-    if ((e = exclusive_scan<int64_t>(nm, mbase, P, nmulti, tiles, s)) != cudaSuccess) return e;
-    chunk_owner_kernel<<<pg, 256, 0, s>>>(mbase, nm, P, owner_m);
+    if (!known_err) {  // the chunks of the second pass (partitions longer than one chunk)
+      multi_count_kernel<<<pg, 256, 0, s>>>(c->d_start, c->d_end, nch, P, nm);
+      if ((e = exclusive_scan<int64_t>(nm, mbase, P, nmulti, tiles, s)) != cudaSuccess) return e;
+      chunk_owner_kernel<<<pg, 256, 0, s>>>(mbase, nm, P, owner_m);
+    }
   }
 
   FitStreamArgs a{c->d_start, c->d_end, nchunks, owner, base, P, sy, sxy, ovf, base,
@@ -497,11 +511,15 @@ static cudaError_t fit_typed(const T* v, glc_column* c, void* scratch, int64_t* 
   if ((e = launch_fit_stream<T, 0>(v, a, num_sms, s)) != cudaSuccess) return e;
   FitChunkArgs fa{c->d_start, c->d_end, base, nchunks, owner, P, sy, sxy, ovf};
   fit_solve_kernel<T><<<pg, 256, 0, s>>>(fa, nch, c->d_types, c->d_params, c->d_err);
-  FitStreamArgs am = a;
-  am.count = nmulti;
-  am.owner = owner_m;
-  am.base = mbase;
-  if ((e = launch_fit_stream<T, 1>(v, am, num_sms, s)) != cudaSuccess) return e;
+  if (known_err && c->fixed_len == 0) {
+    fit_known_err_kernel<<<pg, 256, 0, s>>>(c->d_start, c->d_end, c->d_types, known_err, P, c->d_err);
+  } else {
+    FitStreamArgs am = a;
+    am.count = nmulti;
+    am.owner = owner_m;
+    am.base = mbase;
+    if ((e = launch_fit_stream<T, 1>(v, am, num_sms, s)) != cudaSuccess) return e;
+  }
   fit_bits_kernel<T><<<pg, 256, 0, s>>>(c->d_start, c->d_end, c->d_types, c->d_err, c->d_bits, widths, P,
                                          (unsigned long long*)(d_stats + 1), (unsigned long long*)(d_stats + 3));
   // bit offsets = exclusive scan of len*bits; stats[0] = total bits
@@ -511,12 +529,12 @@ static cudaError_t fit_typed(const T* v, glc_column* c, void* scratch, int64_t* 
 }
 
 cudaError_t launch_fit(glc_dtype dt, const void* values, glc_column* c, void* scratch, size_t, int64_t* d_stats,
-                       cudaStream_t s) {
+                       cudaStream_t s, const long long* known_err) {
   switch (dt) {
-    case GLC_I32: return fit_typed<int32_t>((const int32_t*)values, c, scratch, d_stats, s);
-    case GLC_I64: return fit_typed<int64_t>((const int64_t*)values, c, scratch, d_stats, s);
-    case GLC_U64: return fit_typed<uint64_t>((const uint64_t*)values, c, scratch, d_stats, s);
-    case GLC_U32: return fit_typed<uint32_t>((const uint32_t*)values, c, scratch, d_stats, s);
+    case GLC_I32: return fit_typed<int32_t>((const int32_t*)values, c, scratch, d_stats, s, known_err);
+    case GLC_I64: return fit_typed<int64_t>((const int64_t*)values, c, scratch, d_stats, s, known_err);
+    case GLC_U64: return fit_typed<uint64_t>((const uint64_t*)values, c, scratch, d_stats, s, known_err);
+    case GLC_U32: return fit_typed<uint32_t>((const uint32_t*)values, c, scratch, d_stats, s, known_err);
   }
   return cudaErrorInvalidValue;
 }

@@ -187,8 +187,10 @@ template <typename P> inline cudaError_t pool_alloc(glc_ctx* ctx, P** p, size_t 
 cudaError_t launch_fixed_partitions(int32_t* starts, int32_t* ends, int64_t n, int32_t len, int64_t P, cudaStream_t s);
 size_t fit_scratch_bytes(const int32_t* unused, int64_t n, int64_t P);
 // Fits every partition of c (starts/ends set); d_stats[0] = total bits, d_stats[1] = max bits.
+// known_err: each partition's max |delta| against its exact least-squares line when already
+// measured (the variable partitioner's), so partitions longer than one chunk need no second pass.
 cudaError_t launch_fit(glc_dtype dt, const void* values, glc_column* c, void* scratch, size_t scratch_bytes,
-                       int64_t* d_stats, cudaStream_t s);
+                       int64_t* d_stats, cudaStream_t s, const long long* known_err = nullptr);
 cudaError_t launch_desc_and_tiles(glc_column* c, cudaStream_t s);
 // compress_fixed.cu: one-pass compression of fixed partitions of L values, L a divisor of 4096 and >= 256
 // One column of a launch (its arrays are the column's own, or its slices of a batch's arrays).
@@ -346,10 +348,11 @@ struct RARequest {
 };
 cudaError_t launch_multi_lookup(const RAColumn* cols, const RARequest* reqs, int nreq, int64_t total, int num_sms,
                                 cudaStream_t s);
-// partition.cu: allocates *d_starts / *d_ends (cudaMallocAsync on s)
+// partition.cu: allocates *d_starts / *d_ends (and, when d_err is given, *d_err: each partition's
+// max |delta| against its exact least-squares line) from the context's pool on s
 cudaError_t launch_partition_variable(glc_ctx* ctx, glc_dtype dt, const void* values, int64_t n,
                                       int32_t** d_starts, int32_t** d_ends, int64_t* P, cudaStream_t s,
-                                      std::string* err);
+                                      std::string* err, long long** d_err = nullptr);
 // partition_v6.cu: the reference's GPU partitioner boundaries (pool-allocated starts/ends)
 constexpr int32_t kV6Base = 2048;  // base size compress passes (api/G-LeCo.cuh:384-387)
 cudaError_t launch_partition_v6(glc_ctx* ctx, glc_dtype dt, const void* values, int64_t n, int32_t base,

@@ -509,11 +509,12 @@ struct LineJob {  // one range whose max |delta| is needed
 
 // chunks of each job (0 for jobs that are cached)
 // known (partitions only): a max |delta| already measured (the split evaluation of the
-// partition's start, same line and values), or -1.
+// partition's start, same line and values), or -1.  A pair kept from the previous round (cached)
+// keeps its max |delta| too (cached_err).
 __global__ void job_setup_kernel(const int32_t* __restrict__ ps, const int32_t* __restrict__ pe, int64_t m, int pairs,
-                                 const uint8_t* __restrict__ cached, const long long* __restrict__ known,
-                                 const double* __restrict__ pc, RangeSums rs, LineJob* __restrict__ jobs,
-                                 int64_t* __restrict__ nch, long long* __restrict__ err) {
+                                 const uint8_t* __restrict__ cached, const long long* __restrict__ cached_err,
+                                 const long long* __restrict__ known, const double* __restrict__ pc, RangeSums rs,
+                                 LineJob* __restrict__ jobs, int64_t* __restrict__ nch, long long* __restrict__ err) {
   const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int64_t njobs = pairs ? m - 1 : m;
   if (k >= njobs) return;
@@ -524,8 +525,9 @@ __global__ void job_setup_kernel(const int32_t* __restrict__ ps, const int32_t* 
   jb.sum = pairs ? __dadd_rn(pc[k], pc[k + 1]) : __longlong_as_double(0x7ff0000000000000ll);
   jobs[k] = jb;
   const long long kn = known ? known[k] : -1;
-  err[k] = kn >= 0 ? kn : 0;
-  const bool skip = (cached && cached[k]) || kn >= 0;
+  const bool kept = cached && cached[k];
+  err[k] = kn >= 0 ? kn : (kept ? cached_err[k] : 0);
+  const bool skip = kept || kn >= 0;
   nch[k] = skip ? 0 : ((int64_t)jb.b - jb.a + kPairChunk - 1) / kPairChunk;
 }
 
@@ -637,7 +639,9 @@ __global__ void merge_scatter_kernel(const int32_t* __restrict__ ps, const int32
                                      const uint8_t* __restrict__ prof, const int64_t* __restrict__ head,
                                      const int64_t* __restrict__ idx, int64_t m, int round,
                                      int32_t* __restrict__ ps2, int32_t* __restrict__ pe2, double* __restrict__ pc2,
-                                     uint8_t* __restrict__ cached2, double* __restrict__ cmc2) {
+                                     uint8_t* __restrict__ cached2, double* __restrict__ cmc2,
+                                     const long long* __restrict__ pair_err, const long long* __restrict__ part_err,
+                                     long long* __restrict__ part_err2, long long* __restrict__ cerr2) {
   const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= m || !head[k]) return;
   const int64_t d = idx[k];
@@ -645,22 +649,25 @@ __global__ void merge_scatter_kernel(const int32_t* __restrict__ ps, const int32
   ps2[d] = ps[k];
   pe2[d] = sel ? pe[k + 1] : pe[k];
   pc2[d] = sel ? mc[k] : pc[k];
+  part_err2[d] = sel ? pair_err[k] : part_err[k];  // a merged pair was measured in full (never settled early)
   // the score of (this part, next part) survives when neither changed
   const int64_t nxt = sel ? k + 2 : k + 1;  // old index of the next head
   const bool keep = !sel && nxt < m && !selected(prof, m, nxt, round);
   cached2[d] = keep ? 1 : 0;
   cmc2[d] = keep ? mc[k] : 0.0;
+  cerr2[d] = keep ? pair_err[k] : 0;
 }
 
 static inline size_t al(size_t x) { return (x + 255) & ~(size_t)255; }
 
 template <typename T>
 static cudaError_t partition_typed(glc_ctx* ctx, const T* v, int64_t n, int32_t** out_s, int32_t** out_e, int64_t* outP,
-                                   cudaStream_t s, std::string* err) {
+                                   cudaStream_t s, std::string* err, long long** out_err) {
   cudaError_t e;
   *out_s = nullptr;
   *out_e = nullptr;
   *outP = 0;
+  if (out_err) *out_err = nullptr;
   if (n <= 0) return cudaSuccess;
   const int64_t nb = (n + kMinPart - 1) / kMinPart;
   const int64_t nr = (nb + kRangeBlocks - 1) / kRangeBlocks;
@@ -674,6 +681,7 @@ static cudaError_t partition_typed(glc_ctx* ctx, const T* v, int64_t n, int32_t*
   bytes += al(sizeof(int32_t) * nb);                           // cexit
   bytes += al(sizeof(long long) * nb);                         // nb_err
   bytes += al(sizeof(long long) * mmax);                       // kerr
+  bytes += al(sizeof(long long) * mmax) * 4;                   // part_err, part_err2, cerr, cerr2
   bytes += al(sizeof(int64_t) * (nb + 1)) * 2;                 // flags, idx
   bytes += al(sizeof(int64_t) * (scan_num_tiles(nb) + 1));     // scan tiles (i64)
   bytes += al(sizeof(int32_t) * mmax) * 4;                     // ps, pe, ps2, pe2
@@ -696,6 +704,10 @@ static cudaError_t partition_typed(glc_ctx* ctx, const T* v, int64_t n, int32_t*
   int32_t* cexit = (int32_t*)take(sizeof(int32_t) * nb);
   long long* nb_err = (long long*)take(sizeof(long long) * nb);
   long long* kerr = (long long*)take(sizeof(long long) * mmax);
+  long long* part_err = (long long*)take(sizeof(long long) * mmax);
+  long long* part_err2 = (long long*)take(sizeof(long long) * mmax);
+  long long* cerr = (long long*)take(sizeof(long long) * mmax);
+  long long* cerr2 = (long long*)take(sizeof(long long) * mmax);
   int64_t* flags = (int64_t*)take(sizeof(int64_t) * (nb + 1));
   int64_t* idx = (int64_t*)take(sizeof(int64_t) * (nb + 1));
   int64_t* itiles = (int64_t*)take(sizeof(int64_t) * (scan_num_tiles(nb) + 1));
@@ -757,7 +769,7 @@ static cudaError_t partition_typed(glc_ctx* ctx, const T* v, int64_t n, int32_t*
 
   // max |delta| of each job's line (partitions, or adjacent pairs of the merge rounds)
   auto run_jobs = [&](int64_t cnt, int pairs, const uint8_t* cache, const long long* known) -> cudaError_t {
-    job_setup_kernel<<<grid(cnt, 256), 256, 0, s>>>(ps, pe, m, pairs, cache, known, pc, rs, jobs, nch, perr);
+    job_setup_kernel<<<grid(cnt, 256), 256, 0, s>>>(ps, pe, m, pairs, cache, cerr, known, pc, rs, jobs, nch, perr);
     const int64_t resident = (int64_t)ctx->num_sms * 4;  // 256-thread CTAs, four per SM
     job_err_kernel<T><<<(unsigned)(cnt < resident ? cnt : resident), 256, 0, s>>>(v, jobs, nch, cnt, perr);
     return cudaGetLastError();
@@ -765,6 +777,9 @@ static cudaError_t partition_typed(glc_ctx* ctx, const T* v, int64_t n, int32_t*
   // costs of the split partitions: their max |delta| came with the split evaluation
   if ((e = run_jobs(m, 0, nullptr, kerr)) != cudaSuccess) return fail(e);
   part_cost_kernel<<<grid(m, 256), 256, 0, s>>>(jobs, perr, m, pc);
+  // each partition's max |delta| travels with it through the merge rounds (for the fit)
+  if ((e = cudaMemcpyAsync(part_err, perr, sizeof(long long) * m, cudaMemcpyDeviceToDevice, s)) != cudaSuccess)
+    return fail(e);
   if ((e = cudaMemsetAsync(cached, 0, mmax, s)) != cudaSuccess) return fail(e);
 
   for (int round = 0; round < kMaxMergeRounds && m >= 2; round++) {
@@ -774,7 +789,7 @@ static cudaError_t partition_typed(glc_ctx* ctx, const T* v, int64_t n, int32_t*
     merge_heads_kernel<<<grid(m, 256), 256, 0, s>>>(prof, m, round, flags);
     if ((e = exclusive_scan<int64_t>(flags, idx, m, dsc + 1, itiles, s)) != cudaSuccess) return fail(e);
     merge_scatter_kernel<<<grid(m, 256), 256, 0, s>>>(ps, pe, pc, mc, prof, flags, idx, m, round, ps2, pe2, pc2,
-                                                       cached2, cmc2);
+                                                       cached2, cmc2, perr, part_err, part_err2, cerr2);
     if ((e = cudaGetLastError()) != cudaSuccess) return fail(e);
     if ((e = cudaMemcpyAsync(ctx->h_stats, dsc + 1, 2 * sizeof(int64_t), cudaMemcpyDeviceToHost, s)) != cudaSuccess)
       return fail(e);
@@ -787,6 +802,8 @@ static cudaError_t partition_typed(glc_ctx* ctx, const T* v, int64_t n, int32_t*
     std::swap(pc, pc2);
     std::swap(cached, cached2);
     std::swap(cmc, cmc2);
+    std::swap(part_err, part_err2);
+    std::swap(cerr, cerr2);
     m = m2;
   }
 
@@ -799,6 +816,16 @@ static cudaError_t partition_typed(glc_ctx* ctx, const T* v, int64_t n, int32_t*
   }
   cudaMemcpyAsync(rs_out, ps, sizeof(int32_t) * m, cudaMemcpyDeviceToDevice, s);
   cudaMemcpyAsync(re_out, pe, sizeof(int32_t) * m, cudaMemcpyDeviceToDevice, s);
+  if (out_err) {
+    long long* er_out = nullptr;
+    if ((e = pool_alloc(ctx, &er_out, sizeof(long long) * m, s)) != cudaSuccess) {
+      cudaFreeAsync(rs_out, s);
+      cudaFreeAsync(re_out, s);
+      return fail(e);
+    }
+    cudaMemcpyAsync(er_out, part_err, sizeof(long long) * m, cudaMemcpyDeviceToDevice, s);
+    *out_err = er_out;
+  }
   cudaFreeAsync(buf, s);
   *out_s = rs_out;
   *out_e = re_out;
@@ -807,12 +834,13 @@ static cudaError_t partition_typed(glc_ctx* ctx, const T* v, int64_t n, int32_t*
 }
 
 cudaError_t launch_partition_variable(glc_ctx* ctx, glc_dtype dt, const void* values, int64_t n, int32_t** d_starts,
-                                      int32_t** d_ends, int64_t* P, cudaStream_t s, std::string* err) {
+                                      int32_t** d_ends, int64_t* P, cudaStream_t s, std::string* err,
+                                      long long** d_err) {
   switch (dt) {
-    case GLC_I32: return partition_typed<int32_t>(ctx, (const int32_t*)values, n, d_starts, d_ends, P, s, err);
-    case GLC_I64: return partition_typed<int64_t>(ctx, (const int64_t*)values, n, d_starts, d_ends, P, s, err);
-    case GLC_U64: return partition_typed<uint64_t>(ctx, (const uint64_t*)values, n, d_starts, d_ends, P, s, err);
-    case GLC_U32: return partition_typed<uint32_t>(ctx, (const uint32_t*)values, n, d_starts, d_ends, P, s, err);
+    case GLC_I32: return partition_typed<int32_t>(ctx, (const int32_t*)values, n, d_starts, d_ends, P, s, err, d_err);
+    case GLC_I64: return partition_typed<int64_t>(ctx, (const int64_t*)values, n, d_starts, d_ends, P, s, err, d_err);
+    case GLC_U64: return partition_typed<uint64_t>(ctx, (const uint64_t*)values, n, d_starts, d_ends, P, s, err, d_err);
+    case GLC_U32: return partition_typed<uint32_t>(ctx, (const uint32_t*)values, n, d_starts, d_ends, P, s, err, d_err);
   }
   return cudaErrorInvalidValue;
 }
